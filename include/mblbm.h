@@ -1,0 +1,213 @@
+/*
+ * mblbm.h - C ABI of the B200-native multi-block D2Q9 BGK lattice-Boltzmann step.
+ *
+ * The entry points replace the host call surface of the reference program
+ * (zhangya9741/Multi-block-LBM-GPU): geometry set-up, block and interface
+ * initialisation, the recursive level scheduler, momentum-exchange drag, the
+ * relative L2 change and the Tecplot writer.  Each declaration cites the
+ * reference function it replaces as file:line within that project.
+ *
+ * Conventions (differ from the reference, which has only void functions):
+ *   - every function returns int: MB_OK (0) or a negative MB_ERR_* code;
+ *   - no function writes a file except mb_write_tecplot / mb_append_*;
+ *   - all device work is enqueued on the caller's stream (mb_stream is a
+ *     cudaStream_t passed as void*; NULL = legacy default stream);
+ *   - a context is used by one host thread at a time.
+ *
+ * Types mirror the reference structs field by field so that tables written
+ * for the reference (geo/geometry.h) map one-to-one.
+ */
+#ifndef MBLBM_H
+#define MBLBM_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MB_ABI_VERSION 1
+
+/* ---- limits of the fixed-size tables ---------------------------------- */
+#define MB_MAX_LEVEL 8
+#define MB_MAX_AREA 64
+#define MB_MAX_LINE 128  /* coarse-fine lines (number_line)            */
+#define MB_MAX_LINE2 128 /* same-level lines (number_line2, even)      */
+
+/* ---- error codes ------------------------------------------------------- */
+#define MB_OK 0
+#define MB_ERR_INVALID -1     /* bad argument or table                   */
+#define MB_ERR_CUDA -2        /* a CUDA runtime call failed              */
+#define MB_ERR_NOMEM -3       /* device or host allocation failed        */
+#define MB_ERR_GEOMETRY -4    /* layout violates a geometry rule         */
+#define MB_ERR_UNSUPPORTED -5 /* feature or size outside this build      */
+#define MB_ERR_NUMERIC -6     /* NaN / Inf detected in the state         */
+#define MB_ERR_TIMEOUT -7     /* a bounded device wait gave up           */
+#define MB_ERR_STATE -8       /* call out of order (e.g. step before init)*/
+#define MB_ERR_NODEVICE -9    /* no CUDA device / extension unusable     */
+
+/* ---- storage precisions of the distributions -------------------------- */
+#define MB_PREC_F64 0  /* FP64 storage and arithmetic (reference precision)  */
+#define MB_PREC_F32 1  /* FP32 storage and arithmetic (plain form)           */
+#define MB_PREC_F16S 2 /* FP16 storage of f - w (shifted), FP32 arithmetic   */
+
+/* ---- cell type codes, values as in lbm/lbm.h:26-32 -------------------- */
+#define MB_FLUID 0
+#define MB_SOLID_SBB 1
+#define MB_C_BOUNDARY 9
+
+/* ---- obstacle kinds ---------------------------------------------------- */
+#define MB_OBST_CIRCLE 0  /* (x-CX)^2+(y-CY)^2 < R^2, lbm/init_block.h:28    */
+#define MB_OBST_ELLIPSE 1 /* rotated ellipse (batched cases; no reference)  */
+
+typedef void *mb_stream; /* cudaStream_t */
+
+/* P4 (lbm/data_type_lbm.h:15-20) */
+typedef struct {
+  int xstart, xend, ystart, yend;
+} mb_p4;
+/* P4d (lbm/data_type_lbm.h:26-31) */
+typedef struct {
+  double xstart, xend, ystart, yend;
+} mb_p4d;
+/* P4d4i: fractional zone plus integer move (lbm/data_type_lbm.h:32-36) */
+typedef struct {
+  mb_p4d reduced;
+  mb_p4 move;
+} mb_zone;
+/* P3i: (coarse block, fine block, direction) (lbm/data_type_lbm.h:21-25) */
+typedef struct {
+  int nc, nf, direction;
+} mb_p3i;
+
+/* Block layout: the tables of geo/geometry.h:55-100 as runtime data. */
+typedef struct {
+  int LEVEL;
+  int mi[MB_MAX_LEVEL];
+  int number_area, number_line, number_line2;
+  int ASP[MB_MAX_LEVEL + 1];
+  mb_zone AreaZone[MB_MAX_AREA];
+  int LTCFFCP[MB_MAX_LEVEL + 1];
+  int LS3CFFCP[MB_MAX_LEVEL + 1];
+  int LCCP[MB_MAX_LEVEL + 1];
+  mb_p3i NeborCF[MB_MAX_LINE];
+  mb_p3i NeborCC[MB_MAX_LINE2];
+} mb_layout;
+
+/* Physical parameters: the globals of parameters.h:23-52 as runtime data. */
+typedef struct {
+  double Re;        /* parameters.h:24 */
+  double rho0;      /* parameters.h:27 */
+  int LX, LY;       /* parameters.h:32-33 */
+  int R, CX, CY;    /* parameters.h:36-40 */
+  double U0[2];     /* parameters.h:48 */
+  int obstacle;     /* MB_OBST_* */
+  double ell_cx, ell_cy, ell_a, ell_b, ell_angle; /* MB_OBST_ELLIPSE only */
+  int drag_area;    /* block used for drag; -1 = last block (Multi-block-LBM.cu:127) */
+} mb_config;
+
+/* AREA (lbm/data_type_lbm.h:43-51) */
+typedef struct {
+  int m, nx, ny;
+  double base_x, base_y, tau, rv_tau;
+} mb_area;
+
+/* Inf_Ff_store (multi/data_type_multi.h:15-22) */
+typedef struct {
+  int areac_n, Nc;
+  mb_p4 line_C;
+  int areaf_n, Nf;
+  mb_p4 line_F;
+} mb_line;
+
+/* Everything geo_init() produces (geo/init_geo.h:10-14). */
+typedef struct {
+  mb_layout layout;
+  mb_config config;
+  mb_p4 AreaDefine[MB_MAX_AREA];
+  mb_area Areas[MB_MAX_AREA];
+  mb_line Line_Inf_C[MB_MAX_LINE];
+  mb_line Line_Inf_F[MB_MAX_LINE];
+  mb_line Line_Inf_CC[MB_MAX_LINE2];
+} mb_geometry;
+
+typedef struct mb_ctx mb_ctx;
+
+/* ---- library ------------------------------------------------------------ */
+int mb_version(void);
+const char *mb_error_string(int code);
+
+/* ---- layouts and geometry (host only, no device needed) --------------- */
+/* Built-in tables "1_1", "2_2", "2_5", "4_9" of geo/geometry.h:7-147. */
+int mb_layout_builtin(const char *name, mb_layout *out);
+/* Nested rectangular frames: level 0 covers [0,LX-1]x[0,LY-1]; level l>0
+ * covers the integer box boxes[4(l-1)..] = {xs, xe, ys, ye} (coarse cells),
+ * refined by ratio 2 per level.  Each non-finest level is split into four
+ * blocks (top, bottom, left, right) that overlap their neighbours by one
+ * coarse cell, the pattern of geo/geometry.h:55-100 (_GEO_2_5). */
+int mb_layout_nested(int LX, int LY, int nlevels, const int *boxes, mb_layout *out);
+/* geo_init() + Line_init() (geo/init_geo.h:17-165). */
+int mb_geo_init(const mb_layout *layout, const mb_config *cfg, mb_geometry *geo);
+/* Checks that every C_BOUNDARY cell is the target of some transfer line. */
+int mb_geo_check_coverage(const mb_geometry *geo, int *n_uncovered);
+
+/* ---- context ------------------------------------------------------------- */
+/* Allocates all device state (Multi-block-LBM.cu:26-113). */
+int mb_create(const mb_geometry *geo, int precision, mb_ctx **out);
+int mb_destroy(mb_ctx *ctx);
+/* init_General (lbm/init_block.h:2), init_Fstore / init_tri_A
+ * (multi/init_multi.h:3,30), sum_N_drag + fdrag_store (lbm/force_block.h:50,78). */
+int mb_init(mb_ctx *ctx, mb_stream stream);
+/* n coarse steps of evolution(level 0) (evolution.h:2-65).  The last coarse
+ * step of every call leaves rho/ux/uy of all cells up to date, as the
+ * reference's stb2 does each step; earlier steps keep only the macroscopic
+ * values that interface transfers read. use_graph: 1 = replay a CUDA graph of
+ * the dependency DAG (default), 0 = launch the kernels one by one. */
+int mb_step(mb_ctx *ctx, int n_coarse, mb_stream stream);
+int mb_set_graph_mode(mb_ctx *ctx, int use_graph);
+/* Compiles the plans (and CUDA graphs) that mb_step(ctx, n) will replay from
+ * the current state, so the step call itself spends no host time on them. */
+int mb_prepare(mb_ctx *ctx, int n_coarse);
+/* evolution_area_stb (multi/FH/evolution_block.h:121) on one block. */
+int mb_block_step(mb_ctx *ctx, int area, mb_stream stream);
+/* Single interface operations, for per-kernel checks. */
+int mb_c_c_boundary_transfer(mb_ctx *ctx, int line_cc, mb_stream stream);       /* assit_multi.h:2   */
+int mb_space_interpolation(mb_ctx *ctx, int line, mb_stream stream);            /* assit_multi.h:187 */
+int mb_temporal_interpolation(mb_ctx *ctx, int line, double xm, mb_stream s);   /* assit_multi.h:213 */
+int mb_c_f_boundary_transfer(mb_ctx *ctx, int line, mb_stream stream);          /* assit_multi.h:249 */
+int mb_f_c_boundary_transfer(mb_ctx *ctx, int line, mb_stream stream);          /* assit_multi.h:273 */
+int mb_rotate_markers(mb_ctx *ctx, int line);                                   /* evolution.h:41-46 */
+
+/* ---- diagnostics ----------------------------------------------------------- */
+/* getDrag_block (lbm/force_block.h:180-216) without the file: force[2], Cd, Cl.
+ * Blocks until the value is on the host. */
+int mb_drag(mb_ctx *ctx, double force[2], double *cd, double *cl, mb_stream stream);
+int mb_drag_link_count(mb_ctx *ctx, int *n_links);
+/* error_L2 (lbm/error_L2.h:57-91) without the file; updates u_prev. */
+int mb_error_L2(mb_ctx *ctx, double *e, mb_stream stream);
+/* Scans every block for NaN / Inf; *bad = number of bad values. */
+int mb_check_finite(mb_ctx *ctx, long long *bad, mb_stream stream);
+
+/* ---- host field access (FP64 host buffers, row-major i + j*nx) ------------ */
+/* Any pointer may be NULL.  F is 9*nx*ny (plane k at k*nx*ny).  Synchronous. */
+int mb_copy_fields(mb_ctx *ctx, int area, double *rho, double *ux, double *uy, double *F,
+                   int *solid, mb_stream stream);
+int mb_set_fields(mb_ctx *ctx, int area, const double *rho, const double *ux,
+                  const double *uy, const double *F, mb_stream stream);
+/* Tecplot POINT file in the layout of output/output.h:2-38. */
+int mb_write_tecplot(mb_ctx *ctx, const char *path);
+/* Line "t\tCd\tCl\t" / "t\terr" appended as in force_block.h:212-215 / error_L2.h:85-88. */
+int mb_append_drag(const char *path, int t, double cd, double cl);
+int mb_append_error_L2(const char *path, int t, double e);
+
+/* ---- introspection ------------------------------------------------------- */
+/* Number of kernels launched by the last mb_step call, and in one coarse step. */
+int mb_stats(mb_ctx *ctx, long long *kernels_last_step_call, long long *kernels_per_coarse_step,
+             long long *cell_updates_per_coarse_step);
+/* Times the fused block-step kernel of one level alone (n launches, CUDA events
+ * on the given stream); returns mean ms per launch and bytes moved per launch. */
+int mb_time_block_step(mb_ctx *ctx, int level, int n, mb_stream stream, double *ms_per_launch,
+                       double *alg_bytes_per_launch, long long *cells_per_launch);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MBLBM_H */

@@ -1,0 +1,944 @@
+// mblbm.cu - device context, plan execution (direct or CUDA graph) and the C ABI.
+//
+// Replaces main() of zhangya9741/Multi-block-LBM-GPU (Multi-block-LBM.cu:19-230)
+// as a library: allocation, initialisation, the coarse time step of
+// evolution() and the per-step diagnostics, each behind an extern "C" entry
+// point that returns a status code and enqueues work on the caller's stream.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/mblbm.h"
+#include "kernels.cuh"
+#include "mblbm_internal.h"
+
+using namespace mblbm;
+using namespace mblbm::dev;
+
+#define MB_CUDA(call)                                                                          \
+  do {                                                                                         \
+    cudaError_t e_ = (call);                                                                   \
+    if (e_ != cudaSuccess) {                                                                   \
+      std::fprintf(stderr, "mblbm: %s failed: %s (%s:%d)\n", #call, cudaGetErrorString(e_),    \
+                   __FILE__, __LINE__);                                                        \
+      return MB_ERR_CUDA;                                                                      \
+    }                                                                                          \
+  } while (0)
+
+namespace {
+
+size_t prec_bytes(int prec) { return prec == MB_PREC_F64 ? 8 : (prec == MB_PREC_F32 ? 4 : 2); }
+size_t real_bytes(int prec) { return prec == MB_PREC_F64 ? 8 : 4; }
+
+struct DevPlanNode {
+  NodeKind kind;
+  // launch
+  void *func = nullptr;
+  dim3 grid, block;
+  size_t smem = 0;
+  // parameter blocks (one of them used)
+  StbParams stb;
+  RecParams rec;
+  SplParams spl;
+  void *args[1];
+  std::vector<int> deps;
+};
+
+struct CompiledPlan {
+  std::vector<PlanNode> nodes;
+  std::vector<DevPlanNode> dn;
+  std::vector<void *> dev_allocs;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  SchedState end;
+  long long kernels = 0;
+  ~CompiledPlan() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    for (void *p : dev_allocs) cudaFree(p);
+  }
+};
+
+}  // namespace
+
+struct mb_ctx {
+  int prec = MB_PREC_F32;
+  int device = 0;
+  mb_geometry geo{};
+  int nblk = 0;
+  std::vector<BlockLayout> bl;
+  std::vector<std::vector<uint8_t>> hflags;
+  // device state
+  std::vector<IfBlk> blk;  // host mirror of the device block table
+  IfBlk *d_blk = nullptr;
+  std::vector<void *> allocs;
+  void *d_slots = nullptr;
+  long long n_slot_points = 0;
+  std::vector<SplLine> spl_lines;
+  SplLineDev *d_spl_lines = nullptr;
+  // drag
+  int drag_area = 0;
+  int n_drag = 0;
+  DragLink *d_links = nullptr;
+  double *d_drag_out = nullptr;
+  double *h_drag_out = nullptr;  // pinned
+  // L2
+  L2Blk *d_l2blk = nullptr;
+  double2 *d_l2_partial = nullptr;
+  unsigned int *d_l2_ticket = nullptr;
+  double *d_l2_out = nullptr;
+  double *h_l2_out = nullptr;  // pinned
+  int l2_grid = 0;
+  long long total_cells = 0;
+  // misc scratch
+  unsigned long long *d_count = nullptr;
+  double *d_stage = nullptr;
+  size_t stage_elems = 0;
+  double feqc[9]{};
+  // scheduler
+  SchedState state;
+  bool inited = false;
+  int use_graph = 1;
+  int period = 1;
+  std::map<std::string, std::unique_ptr<CompiledPlan>> plans;
+  long long kernels_last_call = 0;
+  long long kernels_per_step = 0;
+  long long updates_per_step = 0;
+};
+
+namespace {
+
+template <typename T>
+int dalloc(mb_ctx *c, T **p, size_t n) {
+  void *q = nullptr;
+  if (cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T)) != cudaSuccess) return MB_ERR_NOMEM;
+  c->allocs.push_back(q);
+  *p = (T *)q;
+  return MB_OK;
+}
+
+int launch_grid(long long n, int threads) { return (int)std::min<long long>((n + threads - 1) / threads, 148LL * 64); }
+
+// ---- templated dispatch over precision -------------------------------------
+template <template <int> class K, typename... A>
+void *kfunc(int prec) {
+  if (prec == MB_PREC_F64) return K<MB_PREC_F64>::ptr();
+  if (prec == MB_PREC_F32) return K<MB_PREC_F32>::ptr();
+  return K<MB_PREC_F16S>::ptr();
+}
+template <int P> struct KStb { static void *ptr() { return (void *)k_block_step<P>; } };
+template <int P> struct KRec { static void *ptr() { return (void *)k_records<P>; } };
+template <int P> struct KSpl1 { static void *ptr() { return (void *)k_spline<P, 1>; } };
+template <int P> struct KSpl2 { static void *ptr() { return (void *)k_spline<P, 2>; } };
+template <int P> struct KDrag { static void *ptr() { return (void *)k_drag<P>; } };
+template <int P> struct KL2 { static void *ptr() { return (void *)k_error_l2<P>; } };
+
+int max_spline_rows(int prec) { return prec == MB_PREC_F64 ? SPL_THREADS : 2 * SPL_THREADS; }
+
+// ---- node lowering ------------------------------------------------------------
+StbParams make_stb(mb_ctx *c, int a0, int a1, uint64_t parity, int macro_all, int write_macros) {
+  StbParams p{};
+  p.nblk = a1 - a0;
+  p.macro_all = macro_all;
+  p.write_macros = write_macros;
+  for (int k = 0; k < 9; k++) p.feqc[k] = c->feqc[k];
+  p.rho0 = c->geo.config.rho0;
+  p.u0x = c->geo.config.U0[0];
+  p.u0y = c->geo.config.U0[1];
+  long long cell = 0;
+  for (int a = a0; a < a1; a++) {
+    const IfBlk &B = c->blk[a];
+    const int cur = (parity >> a) & 1;
+    StbBlk &s = p.b[a - a0];
+    s.Fin = B.F[cur];
+    s.Fout = B.F[cur ^ 1];
+    s.rho = B.rho;
+    s.ux = B.ux;
+    s.uy = B.uy;
+    s.flags = B.flags;
+    s.nx = B.nx;
+    s.ny = B.ny;
+    s.pitch = B.pitch;
+    s.plane = B.plane;
+    s.cell0 = cell;
+    s.rv_tau = c->geo.Areas[a].rv_tau;
+    cell += (long long)B.nx * B.ny;
+  }
+  p.total = cell;
+  return p;
+}
+
+int lower_plan(mb_ctx *c, CompiledPlan &cp) {
+  cp.dn.resize(cp.nodes.size());
+  for (size_t q = 0; q < cp.nodes.size(); q++) {
+    const PlanNode &n = cp.nodes[q];
+    DevPlanNode &d = cp.dn[q];
+    d.kind = n.kind;
+    d.deps = n.deps;
+    if (n.kind == NK_STB) {
+      d.stb = make_stb(c, n.a0, n.a1, n.parity, n.macro_all, 1);
+      d.func = kfunc<KStb>(c->prec);
+      d.block = dim3(256);
+      d.grid = dim3((unsigned)((d.stb.total + 255) / 256));
+      d.args[0] = &d.stb;
+    } else if (n.kind == NK_REC) {
+      RecDev *dr = nullptr;
+      if (cudaMalloc(&dr, n.recs.size() * sizeof(RecDev)) != cudaSuccess) return MB_ERR_NOMEM;
+      cp.dev_allocs.push_back(dr);
+      if (cudaMemcpy(dr, n.recs.data(), n.recs.size() * sizeof(RecDev), cudaMemcpyHostToDevice) != cudaSuccess)
+        return MB_ERR_CUDA;
+      d.rec = RecParams{};
+      d.rec.recs = dr;
+      d.rec.n = (int)n.recs.size();
+      d.rec.blk = c->d_blk;
+      d.rec.slots = c->d_slots;
+      std::memcpy(d.rec.tw, n.tw, sizeof(n.tw));
+      d.func = kfunc<KRec>(c->prec);
+      d.block = dim3(256);
+      d.grid = dim3((unsigned)((n.recs.size() + 255) / 256));
+      d.args[0] = &d.rec;
+    } else {
+      std::vector<SplTaskDev> tasks(n.spl.size());
+      int maxN = 0;
+      for (size_t t = 0; t < n.spl.size(); t++) {
+        tasks[t] = {n.spl[t].line, n.spl[t].src_buf, n.spl[t].m0, n.spl[t].mask_off};
+        maxN = std::max(maxN, c->spl_lines[n.spl[t].line].Nc);
+      }
+      SplTaskDev *dt = nullptr;
+      uint8_t *dm = nullptr;
+      if (cudaMalloc(&dt, tasks.size() * sizeof(SplTaskDev)) != cudaSuccess) return MB_ERR_NOMEM;
+      cp.dev_allocs.push_back(dt);
+      if (cudaMalloc(&dm, std::max<size_t>(n.spl_mask.size(), 1)) != cudaSuccess) return MB_ERR_NOMEM;
+      cp.dev_allocs.push_back(dm);
+      MB_CUDA(cudaMemcpy(dt, tasks.data(), tasks.size() * sizeof(SplTaskDev), cudaMemcpyHostToDevice));
+      if (!n.spl_mask.empty()) MB_CUDA(cudaMemcpy(dm, n.spl_mask.data(), n.spl_mask.size(), cudaMemcpyHostToDevice));
+      d.spl.tasks = dt;
+      d.spl.lines = c->d_spl_lines;
+      d.spl.mask = dm;
+      d.spl.blk = c->d_blk;
+      d.spl.slots = c->d_slots;
+      const int rows = (maxN + SPL_THREADS - 1) / SPL_THREADS;
+      d.func = rows <= 1 ? kfunc<KSpl1>(c->prec) : kfunc<KSpl2>(c->prec);
+      d.block = dim3(SPL_THREADS);
+      d.grid = dim3((unsigned)tasks.size());
+      d.smem = (size_t)15 * maxN * real_bytes(c->prec);
+      d.args[0] = &d.spl;
+    }
+  }
+  cp.kernels = (long long)cp.dn.size();
+  return MB_OK;
+}
+
+int run_direct(CompiledPlan &cp, cudaStream_t s) {
+  for (auto &d : cp.dn) {
+    if (d.grid.x == 0) continue;
+    MB_CUDA(cudaLaunchKernel(d.func, d.grid, d.block, d.args, d.smem, s));
+  }
+  return MB_OK;
+}
+
+int build_graph(CompiledPlan &cp) {
+  MB_CUDA(cudaGraphCreate(&cp.graph, 0));
+  std::vector<cudaGraphNode_t> gn(cp.dn.size(), nullptr);
+  for (size_t q = 0; q < cp.dn.size(); q++) {
+    DevPlanNode &d = cp.dn[q];
+    std::vector<cudaGraphNode_t> deps;
+    for (int p : d.deps)
+      if (gn[p]) deps.push_back(gn[p]);
+    cudaKernelNodeParams kp{};
+    kp.func = d.func;
+    kp.gridDim = d.grid.x ? d.grid : dim3(1);
+    kp.blockDim = d.block;
+    kp.sharedMemBytes = (unsigned)d.smem;
+    kp.kernelParams = d.args;
+    kp.extra = nullptr;
+    if (d.grid.x == 0) continue;
+    MB_CUDA(cudaGraphAddKernelNode(&gn[q], cp.graph, deps.data(), deps.size(), &kp));
+  }
+  MB_CUDA(cudaGraphInstantiate(&cp.exec, cp.graph, 0));
+  return MB_OK;
+}
+
+int set_smem_limits(int prec) {
+  const int bytes = 15 * max_spline_rows(prec) * (int)real_bytes(prec);
+  void *f1 = kfunc<KSpl1>(prec), *f2 = kfunc<KSpl2>(prec);
+  MB_CUDA(cudaFuncSetAttribute(f1, cudaFuncAttributeMaxDynamicSharedMemorySize, std::min(bytes, 227 * 1024)));
+  MB_CUDA(cudaFuncSetAttribute(f2, cudaFuncAttributeMaxDynamicSharedMemorySize, std::min(bytes, 227 * 1024)));
+  return MB_OK;
+}
+
+CompiledPlan *get_plan(mb_ctx *c, int n, bool final_macros, int *err) {
+  std::string key = c->state.key() + "/" + std::to_string(n) + (final_macros ? "F" : "P");
+  auto it = c->plans.find(key);
+  if (it != c->plans.end()) return it->second.get();
+  auto cp = std::make_unique<CompiledPlan>();
+  PlanCompiler pc(c->geo, c->bl, c->hflags, c->spl_lines);
+  SchedState s = c->state;
+  cp->nodes = pc.compile(s, n, final_macros);
+  cp->end = s;
+  *err = lower_plan(c, *cp);
+  if (*err) return nullptr;
+  CompiledPlan *raw = cp.get();
+  c->plans[key] = std::move(cp);
+  return raw;
+}
+
+int exec_plan(mb_ctx *c, CompiledPlan *cp, cudaStream_t s) {
+  int e;
+  if (c->use_graph) {
+    if (!cp->exec) {
+      e = build_graph(*cp);
+      if (e) return e;
+    }
+    MB_CUDA(cudaGraphLaunch(cp->exec, s));
+  } else {
+    e = run_direct(*cp, s);
+    if (e) return e;
+  }
+  c->state = cp->end;
+  c->kernels_last_call += cp->kernels;
+  return MB_OK;
+}
+
+int exec_nodes_once(mb_ctx *c, std::vector<PlanNode> nodes, cudaStream_t s) {
+  CompiledPlan cp;
+  cp.nodes = std::move(nodes);
+  int e = lower_plan(c, cp);
+  if (e) return e;
+  e = run_direct(cp, s);
+  if (e) return e;
+  // the temporary device buffers are freed by ~CompiledPlan after the work completes
+  MB_CUDA(cudaStreamSynchronize(s));
+  return MB_OK;
+}
+
+}  // namespace
+
+// =============================================================================
+// C ABI
+// =============================================================================
+extern "C" int mb_create(const mb_geometry *geo, int precision, mb_ctx **out) {
+  if (!geo || !out) return MB_ERR_INVALID;
+  *out = nullptr;
+  if (precision != MB_PREC_F64 && precision != MB_PREC_F32 && precision != MB_PREC_F16S) return MB_ERR_INVALID;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return MB_ERR_NODEVICE;
+  auto c = std::make_unique<mb_ctx>();
+  c->prec = precision;
+  cudaGetDevice(&c->device);
+  c->geo = *geo;
+  const mb_layout &L = geo->layout;
+  const mb_config &cfg = geo->config;
+  c->nblk = L.number_area;
+  if (c->nblk < 1 || c->nblk > MB_MAX_AREA || c->nblk > 255) return MB_ERR_INVALID;
+  const size_t sb = prec_bytes(precision), rb = real_bytes(precision);
+  const int pitch_align = (int)(128 / sb);
+
+  // feq(rho0, U0): init_General state and the block-edge equilibrium
+  for (int k = 0; k < 9; k++) {
+    const double eu = ex(k) * cfg.U0[0] + ey(k) * cfg.U0[1];
+    const double uv = cfg.U0[0] * cfg.U0[0] + cfg.U0[1] * cfg.U0[1];
+    c->feqc[k] = wd(k) * cfg.rho0 * (1.0 + 3.0 * eu + 4.5 * eu * eu - 1.5 * uv);
+  }
+
+  // block layouts and flags
+  c->bl.resize(c->nblk);
+  c->hflags.resize(c->nblk);
+  for (int a = 0; a < c->nblk; a++) {
+    const mb_area &A = geo->Areas[a];
+    BlockLayout &b = c->bl[a];
+    b.nx = A.nx;
+    b.ny = A.ny;
+    if ((long long)A.nx * A.ny > (1LL << 31) / 2) return MB_ERR_UNSUPPORTED;
+    b.pitch = (A.nx + pitch_align - 1) / pitch_align * pitch_align;
+    const long long pe = (long long)b.pitch * b.ny;
+    b.plane = (pe + 127) / 128 * 128;
+    auto &fl = c->hflags[a];
+    fl.assign((size_t)b.plane, CT_PAD);
+    for (int j = 0; j < A.ny; j++)
+      for (int i = 0; i < A.nx; i++) {
+        const int t = cell_type(*geo, a, i, j);
+        uint8_t v = t == MB_FLUID ? CT_FLUID : (t == MB_SOLID_SBB ? CT_SOLID : CT_COPY);
+        if (i == 0 || j == 0 || i == A.nx - 1 || j == A.ny - 1) v |= CF_EDGE;
+        fl[(size_t)j * b.pitch + i] = v;
+      }
+  }
+  mark_macro_sources(*geo, c->bl, c->hflags);
+
+  // coarse-fine line table for the spline kernel; slots: 3 x 9 values per fine point
+  c->spl_lines.resize(L.number_line);
+  long long slot_pts = 0;
+  for (int b = 0; b < L.number_line; b++) {
+    const mb_line &l = geo->Line_Inf_C[b];
+    SplLine &s = c->spl_lines[b];
+    s.coarse = l.areac_n;
+    s.fine = l.areaf_n;
+    s.Nc = l.Nc;
+    s.Nf = l.Nf;
+    const mb_area &ac = geo->Areas[l.areac_n], &af = geo->Areas[l.areaf_n];
+    s.r = af.m / ac.m;
+    const bool vc = l.line_C.xstart == l.line_C.xend, vf = l.line_F.xstart == l.line_F.xend;
+    s.ci0 = l.line_C.xstart; s.cj0 = l.line_C.ystart; s.cdi = vc ? 0 : 1; s.cdj = vc ? 1 : 0;
+    s.fi0 = l.line_F.xstart; s.fj0 = l.line_F.ystart; s.fdi = vf ? 0 : 1; s.fdj = vf ? 1 : 0;
+    s.slot0 = (int)slot_pts;
+    s.para = (af.tau - 1.0) / (s.r * (ac.tau - 1.0));
+    if (l.Nc < 2 || l.Nf < 1 || s.r < 1) return MB_ERR_GEOMETRY;
+    if ((long long)(l.Nf - 1) > (long long)s.r * (l.Nc - 1)) return MB_ERR_GEOMETRY;
+    if (l.Nc > max_spline_rows(precision)) return MB_ERR_UNSUPPORTED;
+    slot_pts += l.Nf;
+  }
+  c->n_slot_points = slot_pts;
+
+  // device allocations (Multi-block-LBM.cu:26-113, without x/y/force/f arrays)
+  int e;
+  c->blk.resize(c->nblk);
+  for (int a = 0; a < c->nblk; a++) {
+    IfBlk &B = c->blk[a];
+    const BlockLayout &b = c->bl[a];
+    for (int q = 0; q < 2; q++) {
+      void *p;
+      if (cudaMalloc(&p, (size_t)9 * b.plane * sb) != cudaSuccess) return MB_ERR_NOMEM;
+      c->allocs.push_back(p);
+      B.F[q] = p;
+    }
+    void *m[5];
+    for (int q = 0; q < 5; q++) {
+      if (cudaMalloc(&m[q], (size_t)b.plane * rb) != cudaSuccess) return MB_ERR_NOMEM;
+      c->allocs.push_back(m[q]);
+    }
+    B.rho = m[0]; B.ux = m[1]; B.uy = m[2]; B.upx = m[3]; B.upy = m[4];
+    uint8_t *fl;
+    if ((e = dalloc(c.get(), &fl, (size_t)b.plane))) return e;
+    MB_CUDA(cudaMemcpy(fl, c->hflags[a].data(), (size_t)b.plane, cudaMemcpyHostToDevice));
+    B.flags = fl;
+    B.nx = b.nx; B.ny = b.ny; B.pitch = b.pitch; B.m = geo->Areas[a].m;
+    B.plane = b.plane;
+    B.tau = geo->Areas[a].tau;
+  }
+  if ((e = dalloc(c.get(), &c->d_blk, c->nblk))) return e;
+  MB_CUDA(cudaMemcpy(c->d_blk, c->blk.data(), c->nblk * sizeof(IfBlk), cudaMemcpyHostToDevice));
+  {
+    void *p;
+    if (cudaMalloc(&p, std::max<long long>(slot_pts, 1) * 27 * rb) != cudaSuccess) return MB_ERR_NOMEM;
+    c->allocs.push_back(p);
+    c->d_slots = p;
+  }
+  if ((e = dalloc(c.get(), &c->d_spl_lines, std::max(L.number_line, 1)))) return e;
+  if (L.number_line) {
+    std::vector<SplLineDev> sd(L.number_line);
+    for (int b = 0; b < L.number_line; b++) {
+      const SplLine &s = c->spl_lines[b];
+      sd[b] = {s.coarse, s.fine, s.Nc, s.Nf, s.r, s.ci0, s.cj0, s.cdi, s.cdj, s.fi0, s.fj0, s.fdi, s.fdj, s.slot0, s.para};
+    }
+    MB_CUDA(cudaMemcpy(c->d_spl_lines, sd.data(), sd.size() * sizeof(SplLineDev), cudaMemcpyHostToDevice));
+  }
+
+  // drag links (fdrag_store, force_block.h:78-127): i-outer, j-inner, k
+  c->drag_area = cfg.drag_area < 0 ? c->nblk - 1 : cfg.drag_area;
+  if (c->drag_area >= c->nblk) return MB_ERR_INVALID;
+  {
+    const int a = c->drag_area;
+    const BlockLayout &b = c->bl[a];
+    const auto &fl = c->hflags[a];
+    std::vector<DragLink> links;
+    for (int i = 0; i < b.nx; i++)
+      for (int j = 0; j < b.ny; j++) {
+        const long long cs = (long long)j * b.pitch + i;
+        if ((fl[cs] & 3) != CT_SOLID) continue;
+        for (int k = 0; k < 9; k++) {
+          const int id = i - ex(k), jd = j - ey(k);
+          if (id < 0 || id > b.nx - 1 || jd < 0 || jd > b.ny - 1) continue;
+          const long long cf = (long long)jd * b.pitch + id;
+          if ((fl[cf] & 3) != CT_FLUID) continue;
+          links.push_back({(int32_t)cs, (int32_t)cf, k, (fl[cf] & CF_EDGE) ? 1 : 0});
+        }
+      }
+    c->n_drag = (int)links.size();
+    if ((e = dalloc(c.get(), &c->d_links, links.size()))) return e;
+    if (!links.empty())
+      MB_CUDA(cudaMemcpy(c->d_links, links.data(), links.size() * sizeof(DragLink), cudaMemcpyHostToDevice));
+    if ((e = dalloc(c.get(), &c->d_drag_out, 2))) return e;
+    MB_CUDA(cudaMallocHost(&c->h_drag_out, 2 * sizeof(double)));
+  }
+
+  // L2 tables and scratch
+  {
+    std::vector<L2Blk> lb(c->nblk);
+    long long cell = 0;
+    for (int a = 0; a < c->nblk; a++) {
+      lb[a] = {cell, c->bl[a].nx, c->bl[a].pitch, 1.0 / geo->Areas[a].m};
+      cell += (long long)c->bl[a].nx * c->bl[a].ny;
+    }
+    c->total_cells = cell;
+    if ((e = dalloc(c.get(), &c->d_l2blk, c->nblk))) return e;
+    MB_CUDA(cudaMemcpy(c->d_l2blk, lb.data(), lb.size() * sizeof(L2Blk), cudaMemcpyHostToDevice));
+    c->l2_grid = (int)std::min<long long>((cell + 255) / 256, 148LL * 8);
+    if ((e = dalloc(c.get(), &c->d_l2_partial, c->l2_grid))) return e;
+    if ((e = dalloc(c.get(), &c->d_l2_ticket, 1))) return e;
+    MB_CUDA(cudaMemset(c->d_l2_ticket, 0, sizeof(unsigned int)));
+    if ((e = dalloc(c.get(), &c->d_l2_out, 2))) return e;
+    MB_CUDA(cudaMallocHost(&c->h_l2_out, 2 * sizeof(double)));
+  }
+  if ((e = dalloc(c.get(), &c->d_count, 1))) return e;
+
+  // scheduler state (Multi-block-LBM.cu:45-47 markers)
+  c->state.parity.assign(c->nblk, 0);
+  c->state.marker.assign(L.number_line, {2, 1, 0});
+  {
+    // period of the (parity, marker) state over coarse steps
+    PlanCompiler pc(c->geo, c->bl, c->hflags, c->spl_lines);
+    SchedState s = c->state;
+    int per = 0;
+    for (int n = 1; n <= 12; n++) {
+      SchedState t = s;
+      (void)pc;
+      // advance symbolically by one coarse step without building nodes
+      for (int l = 0; l < L.LEVEL; l++) {
+        int steps = 1;
+        for (int q = 1; q <= l; q++) steps *= L.mi[q];
+        if (steps & 1)
+          for (int a = L.ASP[l]; a < L.ASP[l + 1]; a++) t.parity[a] ^= 1;
+        if (l != L.LEVEL - 1) {
+          const int rot = steps % 3;
+          for (int b = L.LS3CFFCP[l]; b < L.LS3CFFCP[l + 1]; b++)
+            for (int r = 0; r < rot; r++)
+              for (int p = 0; p < 3; p++) t.marker[b][p] = t.marker[b][p] == 0 ? 2 : t.marker[b][p] - 1;
+        }
+      }
+      s = t;
+      if (s == c->state) { per = n; break; }
+    }
+    c->period = per > 0 ? per : 6;
+  }
+  {
+    long long upd = 0;
+    for (int l = 0; l < L.LEVEL; l++) {
+      long long steps = 1;
+      for (int q = 1; q <= l; q++) steps *= L.mi[q];
+      for (int a = L.ASP[l]; a < L.ASP[l + 1]; a++) upd += steps * (long long)c->bl[a].nx * c->bl[a].ny;
+    }
+    c->updates_per_step = upd;
+  }
+  if ((e = set_smem_limits(precision))) return e;
+  *out = c.release();
+  return MB_OK;
+}
+
+extern "C" int mb_destroy(mb_ctx *c) {
+  if (!c) return MB_ERR_INVALID;
+  cudaDeviceSynchronize();
+  c->plans.clear();
+  for (void *p : c->allocs) cudaFree(p);
+  if (c->h_drag_out) cudaFreeHost(c->h_drag_out);
+  if (c->h_l2_out) cudaFreeHost(c->h_l2_out);
+  delete c;
+  return MB_OK;
+}
+
+extern "C" int mb_set_graph_mode(mb_ctx *c, int use_graph) {
+  if (!c) return MB_ERR_INVALID;
+  c->use_graph = use_graph ? 1 : 0;
+  return MB_OK;
+}
+
+// init_General (lbm/init_block.h:2-51), init_Fstore and init_tri_A
+// (multi/init_multi.h:3-51): uniform rho0/U0 with f = F = feq, u_prev = U0,
+// every ring slot = the fine edge F (= feq), the spline matrix is implicit.
+extern "C" int mb_init(mb_ctx *c, mb_stream stream) {
+  if (!c) return MB_ERR_INVALID;
+  cudaStream_t s = (cudaStream_t)stream;
+  const mb_config &cfg = c->geo.config;
+  const int th = 256;
+  for (int a = 0; a < c->nblk; a++) {
+    const IfBlk &B = c->blk[a];
+    const long long n = B.plane;
+    for (int q = 0; q < 2; q++) {
+      const int gr = launch_grid(9 * n, th);
+      const double *f = c->feqc;
+      if (c->prec == MB_PREC_F64)
+        k_fill_planes<MB_PREC_F64><<<gr, th, 0, s>>>((double *)B.F[q], n, f[0], f[1], f[2], f[3], f[4], f[5], f[6], f[7], f[8]);
+      else if (c->prec == MB_PREC_F32)
+        k_fill_planes<MB_PREC_F32><<<gr, th, 0, s>>>((float *)B.F[q], n, f[0], f[1], f[2], f[3], f[4], f[5], f[6], f[7], f[8]);
+      else
+        k_fill_planes<MB_PREC_F16S><<<gr, th, 0, s>>>((__half *)B.F[q], n, f[0], f[1], f[2], f[3], f[4], f[5], f[6], f[7], f[8]);
+    }
+    const int gr = launch_grid(n, th);
+    if (c->prec == MB_PREC_F64) {
+      k_fill<double><<<gr, th, 0, s>>>((double *)B.rho, n, cfg.rho0);
+      k_fill<double><<<gr, th, 0, s>>>((double *)B.ux, n, cfg.U0[0]);
+      k_fill<double><<<gr, th, 0, s>>>((double *)B.uy, n, cfg.U0[1]);
+      k_fill<double><<<gr, th, 0, s>>>((double *)B.upx, n, cfg.U0[0]);
+      k_fill<double><<<gr, th, 0, s>>>((double *)B.upy, n, cfg.U0[1]);
+    } else {
+      k_fill<float><<<gr, th, 0, s>>>((float *)B.rho, n, (float)cfg.rho0);
+      k_fill<float><<<gr, th, 0, s>>>((float *)B.ux, n, (float)cfg.U0[0]);
+      k_fill<float><<<gr, th, 0, s>>>((float *)B.uy, n, (float)cfg.U0[1]);
+      k_fill<float><<<gr, th, 0, s>>>((float *)B.upx, n, (float)cfg.U0[0]);
+      k_fill<float><<<gr, th, 0, s>>>((float *)B.upy, n, (float)cfg.U0[1]);
+    }
+  }
+  if (c->n_slot_points > 0) {
+    // slot layout [point][slot][k]: fill k-periodic values through a host pattern
+    const long long n = c->n_slot_points * 27;
+    const size_t rb = real_bytes(c->prec);
+    std::vector<unsigned char> host((size_t)n * rb);
+    for (long long q = 0; q < n; q++) {
+      const double v = c->feqc[q % 9];
+      if (rb == 8) std::memcpy(&host[q * 8], &v, 8);
+      else { const float fv = (float)v; std::memcpy(&host[q * 4], &fv, 4); }
+    }
+    MB_CUDA(cudaMemcpyAsync(c->d_slots, host.data(), host.size(), cudaMemcpyHostToDevice, s));
+    MB_CUDA(cudaStreamSynchronize(s));
+  }
+  MB_CUDA(cudaGetLastError());
+  c->state.parity.assign(c->nblk, 0);
+  c->state.marker.assign(c->geo.layout.number_line, {2, 1, 0});
+  c->inited = true;
+  return MB_OK;
+}
+
+extern "C" int mb_step(mb_ctx *c, int n, mb_stream stream) {
+  if (!c || n < 0) return MB_ERR_INVALID;
+  if (!c->inited) return MB_ERR_STATE;
+  cudaStream_t s = (cudaStream_t)stream;
+  c->kernels_last_call = 0;
+  int remaining = n;
+  const int G = c->period;
+  while (remaining > 0) {
+    int chunk;
+    bool fin;
+    if (remaining - 1 >= G) { chunk = G; fin = false; }
+    else if (remaining > 1) { chunk = 1; fin = false; }
+    else { chunk = 1; fin = true; }
+    int err = 0;
+    CompiledPlan *cp = get_plan(c, chunk, fin, &err);
+    if (!cp) return err ? err : MB_ERR_INVALID;
+    if ((err = exec_plan(c, cp, s))) return err;
+    remaining -= chunk;
+  }
+  {
+    int err = 0;
+    SchedState save = c->state;
+    CompiledPlan *cp = get_plan(c, 1, true, &err);
+    if (cp) c->kernels_per_step = cp->kernels;
+    c->state = save;
+  }
+  MB_CUDA(cudaGetLastError());
+  return MB_OK;
+}
+
+// Compiles (and instantiates as graphs) every plan mb_step(n) will replay from
+// the current state, so that a later mb_step spends no host time on it.
+extern "C" int mb_prepare(mb_ctx *c, int n) {
+  if (!c || n < 0) return MB_ERR_INVALID;
+  if (!c->inited) return MB_ERR_STATE;
+  const SchedState save = c->state;
+  int remaining = n, err = 0;
+  const int G = c->period;
+  while (remaining > 0) {
+    int chunk;
+    bool fin;
+    if (remaining - 1 >= G) { chunk = G; fin = false; }
+    else if (remaining > 1) { chunk = 1; fin = false; }
+    else { chunk = 1; fin = true; }
+    CompiledPlan *cp = get_plan(c, chunk, fin, &err);
+    if (!cp) { c->state = save; return err ? err : MB_ERR_INVALID; }
+    if (c->use_graph && !cp->exec && (err = build_graph(*cp))) { c->state = save; return err; }
+    c->state = cp->end;
+    remaining -= chunk;
+  }
+  c->state = save;
+  return MB_OK;
+}
+
+extern "C" int mb_block_step(mb_ctx *c, int area, mb_stream stream) {
+  if (!c || area < 0 || area >= c->nblk) return MB_ERR_INVALID;
+  if (!c->inited) return MB_ERR_STATE;
+  PlanNode nd;
+  nd.kind = NK_STB;
+  nd.a0 = area;
+  nd.a1 = area + 1;
+  nd.macro_all = 1;
+  for (int a = 0; a < c->nblk; a++)
+    if (c->state.parity[a]) nd.parity |= 1ull << a;
+  int e = exec_nodes_once(c, {nd}, (cudaStream_t)stream);
+  if (e) return e;
+  c->state.parity[area] ^= 1;
+  return MB_OK;
+}
+
+static int single_op(mb_ctx *c, int kind, int index, double xm, mb_stream stream) {
+  if (!c) return MB_ERR_INVALID;
+  if (!c->inited) return MB_ERR_STATE;
+  PlanCompiler pc(c->geo, c->bl, c->hflags, c->spl_lines);
+  return exec_nodes_once(c, pc.compile_single(kind, index, xm, c->state), (cudaStream_t)stream);
+}
+
+extern "C" int mb_c_c_boundary_transfer(mb_ctx *c, int line, mb_stream s) {
+  if (!c || line < 0 || line >= c->geo.layout.number_line2) return MB_ERR_INVALID;
+  return single_op(c, Op::CC, line, 0, s);
+}
+extern "C" int mb_space_interpolation(mb_ctx *c, int line, mb_stream s) {
+  if (!c || line < 0 || line >= c->geo.layout.number_line) return MB_ERR_INVALID;
+  return single_op(c, Op::SPL, line, 0, s);
+}
+extern "C" int mb_temporal_interpolation(mb_ctx *c, int line, double xm, mb_stream s) {
+  if (!c || line < 0 || line >= c->geo.layout.number_line) return MB_ERR_INVALID;
+  return single_op(c, Op::TEMPORAL, line, xm, s);
+}
+extern "C" int mb_c_f_boundary_transfer(mb_ctx *c, int line, mb_stream s) {
+  if (!c || line < 0 || line >= c->geo.layout.number_line) return MB_ERR_INVALID;
+  return single_op(c, Op::CF, line, 0, s);
+}
+extern "C" int mb_f_c_boundary_transfer(mb_ctx *c, int line, mb_stream s) {
+  if (!c || line < 0 || line >= c->geo.layout.number_line) return MB_ERR_INVALID;
+  return single_op(c, Op::FC, line, 0, s);
+}
+extern "C" int mb_rotate_markers(mb_ctx *c, int line) {
+  if (!c || line < 0 || line >= c->geo.layout.number_line) return MB_ERR_INVALID;
+  auto &m = c->state.marker[line];
+  for (int p = 0; p < 3; p++) m[p] = m[p] == 0 ? 2 : m[p] - 1;
+  return MB_OK;
+}
+
+// getDrag_block (lbm/force_block.h:180-216): momentum exchange over the
+// stored links of the drag block, Cd = Fx/(rho0 |U0|^2 m R).
+extern "C" int mb_drag(mb_ctx *c, double force[2], double *cd, double *cl, mb_stream stream) {
+  if (!c || !force) return MB_ERR_INVALID;
+  if (!c->inited) return MB_ERR_STATE;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int a = c->drag_area;
+  const IfBlk &B = c->blk[a];
+  DragParams p{};
+  p.links = c->d_links;
+  p.n = c->n_drag;
+  p.F = B.F[c->state.parity[a] ^ 1];
+  p.plane = B.plane;
+  for (int k = 0; k < 9; k++) p.feqc[k] = c->feqc[k];
+  p.out = c->d_drag_out;
+  void *args[] = {&p};
+  MB_CUDA(cudaLaunchKernel(kfunc<KDrag>(c->prec), dim3(1), dim3(1024), args, 0, s));
+  MB_CUDA(cudaMemcpyAsync(c->h_drag_out, c->d_drag_out, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  MB_CUDA(cudaStreamSynchronize(s));
+  force[0] = c->h_drag_out[0];
+  force[1] = c->h_drag_out[1];
+  const mb_config &cfg = c->geo.config;
+  const double u0 = std::sqrt(cfg.U0[0] * cfg.U0[0] + cfg.U0[1] * cfg.U0[1]);
+  const double den = cfg.rho0 * u0 * u0 * c->geo.Areas[a].m * cfg.R;
+  if (cd) *cd = force[0] / den;
+  if (cl) *cl = force[1] / den;
+  return MB_OK;
+}
+
+extern "C" int mb_drag_link_count(mb_ctx *c, int *n) {
+  if (!c || !n) return MB_ERR_INVALID;
+  *n = c->n_drag;
+  return MB_OK;
+}
+
+// error_L2 (lbm/error_L2.h:57-91)
+extern "C" int mb_error_L2(mb_ctx *c, double *e, mb_stream stream) {
+  if (!c || !e) return MB_ERR_INVALID;
+  if (!c->inited) return MB_ERR_STATE;
+  cudaStream_t s = (cudaStream_t)stream;
+  L2Params p{};
+  p.blocks = c->d_l2blk;
+  p.blk = c->d_blk;
+  p.nblk = c->nblk;
+  p.total = c->total_cells;
+  p.partial = c->d_l2_partial;
+  p.ticket = c->d_l2_ticket;
+  p.out = c->d_l2_out;
+  void *args[] = {&p};
+  MB_CUDA(cudaLaunchKernel(kfunc<KL2>(c->prec), dim3(c->l2_grid), dim3(256), args, 0, s));
+  MB_CUDA(cudaMemcpyAsync(c->h_l2_out, c->d_l2_out, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  MB_CUDA(cudaStreamSynchronize(s));
+  *e = std::sqrt(c->h_l2_out[0]) / std::sqrt(c->h_l2_out[1]);
+  return MB_OK;
+}
+
+extern "C" int mb_check_finite(mb_ctx *c, long long *bad, mb_stream stream) {
+  if (!c || !bad) return MB_ERR_INVALID;
+  cudaStream_t s = (cudaStream_t)stream;
+  MB_CUDA(cudaMemsetAsync(c->d_count, 0, sizeof(unsigned long long), s));
+  for (int a = 0; a < c->nblk; a++) {
+    const IfBlk &B = c->blk[a];
+    const void *F = B.F[c->state.parity[a]];
+    const int gr = launch_grid((long long)B.nx * B.ny, 256);
+    if (c->prec == MB_PREC_F64)
+      k_count_nonfinite<MB_PREC_F64><<<gr, 256, 0, s>>>((const double *)F, B.plane, B.flags, B.nx, B.ny, B.pitch, c->d_count);
+    else if (c->prec == MB_PREC_F32)
+      k_count_nonfinite<MB_PREC_F32><<<gr, 256, 0, s>>>((const float *)F, B.plane, B.flags, B.nx, B.ny, B.pitch, c->d_count);
+    else
+      k_count_nonfinite<MB_PREC_F16S><<<gr, 256, 0, s>>>((const __half *)F, B.plane, B.flags, B.nx, B.ny, B.pitch, c->d_count);
+  }
+  unsigned long long h = 0;
+  MB_CUDA(cudaMemcpyAsync(&h, c->d_count, sizeof(h), cudaMemcpyDeviceToHost, s));
+  MB_CUDA(cudaStreamSynchronize(s));
+  *bad = (long long)h;
+  return h ? MB_ERR_NUMERIC : MB_OK;
+}
+
+static int ensure_stage(mb_ctx *c, size_t elems) {
+  if (c->stage_elems >= elems) return MB_OK;
+  if (c->d_stage) cudaFree(c->d_stage);
+  c->d_stage = nullptr;
+  c->stage_elems = 0;
+  if (cudaMalloc(&c->d_stage, elems * sizeof(double)) != cudaSuccess) return MB_ERR_NOMEM;
+  c->stage_elems = elems;
+  return MB_OK;
+}
+
+extern "C" int mb_copy_fields(mb_ctx *c, int a, double *rho, double *ux, double *uy, double *F, int *solid,
+                              mb_stream stream) {
+  if (!c || a < 0 || a >= c->nblk) return MB_ERR_INVALID;
+  cudaStream_t s = (cudaStream_t)stream;
+  const IfBlk &B = c->blk[a];
+  const long long n = (long long)B.nx * B.ny;
+  int e = ensure_stage(c, (size_t)9 * n);
+  if (e) return e;
+  const int gr = launch_grid(9 * n, 256);
+  if (F) {
+    const void *Fs = B.F[c->state.parity[a]];
+    if (c->prec == MB_PREC_F64) k_planes_to_f64<MB_PREC_F64><<<gr, 256, 0, s>>>((const double *)Fs, B.plane, B.nx, B.ny, B.pitch, c->d_stage);
+    else if (c->prec == MB_PREC_F32) k_planes_to_f64<MB_PREC_F32><<<gr, 256, 0, s>>>((const float *)Fs, B.plane, B.nx, B.ny, B.pitch, c->d_stage);
+    else k_planes_to_f64<MB_PREC_F16S><<<gr, 256, 0, s>>>((const __half *)Fs, B.plane, B.nx, B.ny, B.pitch, c->d_stage);
+    MB_CUDA(cudaMemcpyAsync(F, c->d_stage, 9 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    MB_CUDA(cudaStreamSynchronize(s));
+  }
+  void *M[3] = {B.rho, B.ux, B.uy};
+  double *H[3] = {rho, ux, uy};
+  for (int q = 0; q < 3; q++) {
+    if (!H[q]) continue;
+    if (c->prec == MB_PREC_F64) k_field_to_f64<double><<<gr, 256, 0, s>>>((const double *)M[q], B.nx, B.ny, B.pitch, c->d_stage);
+    else k_field_to_f64<float><<<gr, 256, 0, s>>>((const float *)M[q], B.nx, B.ny, B.pitch, c->d_stage);
+    MB_CUDA(cudaMemcpyAsync(H[q], c->d_stage, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    MB_CUDA(cudaStreamSynchronize(s));
+  }
+  if (solid) {
+    const auto &fl = c->hflags[a];
+    for (int j = 0; j < B.ny; j++)
+      for (int i = 0; i < B.nx; i++) {
+        const int t = fl[(size_t)j * B.pitch + i] & 3;
+        solid[(size_t)j * B.nx + i] = t == CT_FLUID ? MB_FLUID : (t == CT_SOLID ? MB_SOLID_SBB : MB_C_BOUNDARY);
+      }
+  }
+  MB_CUDA(cudaGetLastError());
+  return MB_OK;
+}
+
+extern "C" int mb_set_fields(mb_ctx *c, int a, const double *rho, const double *ux, const double *uy,
+                             const double *F, mb_stream stream) {
+  if (!c || a < 0 || a >= c->nblk) return MB_ERR_INVALID;
+  cudaStream_t s = (cudaStream_t)stream;
+  const IfBlk &B = c->blk[a];
+  const long long n = (long long)B.nx * B.ny;
+  int e = ensure_stage(c, (size_t)9 * n);
+  if (e) return e;
+  const int gr = launch_grid(9 * n, 256);
+  if (F) {
+    MB_CUDA(cudaMemcpyAsync(c->d_stage, F, 9 * n * sizeof(double), cudaMemcpyHostToDevice, s));
+    void *Fd = B.F[c->state.parity[a]];
+    if (c->prec == MB_PREC_F64) k_f64_to_planes<MB_PREC_F64><<<gr, 256, 0, s>>>((double *)Fd, B.plane, B.nx, B.ny, B.pitch, c->d_stage);
+    else if (c->prec == MB_PREC_F32) k_f64_to_planes<MB_PREC_F32><<<gr, 256, 0, s>>>((float *)Fd, B.plane, B.nx, B.ny, B.pitch, c->d_stage);
+    else k_f64_to_planes<MB_PREC_F16S><<<gr, 256, 0, s>>>((__half *)Fd, B.plane, B.nx, B.ny, B.pitch, c->d_stage);
+    MB_CUDA(cudaStreamSynchronize(s));
+  }
+  void *M[3] = {B.rho, B.ux, B.uy};
+  const double *H[3] = {rho, ux, uy};
+  for (int q = 0; q < 3; q++) {
+    if (!H[q]) continue;
+    MB_CUDA(cudaMemcpyAsync(c->d_stage, H[q], n * sizeof(double), cudaMemcpyHostToDevice, s));
+    if (c->prec == MB_PREC_F64) k_f64_to_field<double><<<gr, 256, 0, s>>>((double *)M[q], B.nx, B.ny, B.pitch, c->d_stage);
+    else k_f64_to_field<float><<<gr, 256, 0, s>>>((float *)M[q], B.nx, B.ny, B.pitch, c->d_stage);
+    MB_CUDA(cudaStreamSynchronize(s));
+  }
+  MB_CUDA(cudaGetLastError());
+  return MB_OK;
+}
+
+// output (output/output.h:2-38): Tecplot POINT zones with %g values
+extern "C" int mb_write_tecplot(mb_ctx *c, const char *path) {
+  if (!c || !path) return MB_ERR_INVALID;
+  FILE *fp = std::fopen(path, "w");
+  if (!fp) return MB_ERR_INVALID;
+  std::fprintf(fp, "Title= \"LBM 2D\"\n");
+  std::fprintf(fp, "VARIABLES= \"X\",\"Y\",\"solid\",\"rho\",\"U\",\"V\",\n");
+  int err = MB_OK;
+  for (int a = 0; a < c->nblk && err == MB_OK; a++) {
+    const mb_area &A = c->geo.Areas[a];
+    const size_t n = (size_t)A.nx * A.ny;
+    std::vector<double> rho(n), ux(n), uy(n);
+    std::vector<int> solid(n);
+    err = mb_copy_fields(c, a, rho.data(), ux.data(), uy.data(), nullptr, solid.data(), nullptr);
+    if (err) break;
+    std::fprintf(fp, "ZONE T= \"zone_level%d\",I= %d,J= %d,F=POINT\n", a, A.nx, A.ny);
+    const double dx = 1.0 / A.m;
+    for (int j = 0; j < A.ny; j++)
+      for (int i = 0; i < A.nx; i++) {
+        const size_t q = (size_t)j * A.nx + i;
+        std::fprintf(fp, "%g\t%g\t%d\t%g\t%g\t%g\n", i * dx + A.base_x, j * dx + A.base_y, solid[q], rho[q], ux[q],
+                     uy[q]);
+      }
+  }
+  std::fclose(fp);
+  return err;
+}
+
+extern "C" int mb_stats(mb_ctx *c, long long *kl, long long *kps, long long *ups) {
+  if (!c) return MB_ERR_INVALID;
+  if (kl) *kl = c->kernels_last_call;
+  if (kps) *kps = c->kernels_per_step;
+  if (ups) *ups = c->updates_per_step;
+  return MB_OK;
+}
+
+extern "C" int mb_time_block_step(mb_ctx *c, int level, int n, mb_stream stream, double *ms, double *bytes,
+                                  long long *cells) {
+  if (!c || level < 0 || level >= c->geo.layout.LEVEL || n < 1) return MB_ERR_INVALID;
+  if (!c->inited) return MB_ERR_STATE;
+  cudaStream_t s = (cudaStream_t)stream;
+  const mb_layout &L = c->geo.layout;
+  uint64_t par = 0;
+  for (int a = 0; a < c->nblk; a++)
+    if (c->state.parity[a]) par |= 1ull << a;
+  std::vector<StbParams> ps;
+  long long tot = 0;
+  for (int a0 = L.ASP[level]; a0 < L.ASP[level + 1]; a0 += STB_MAX_BLOCKS) {
+    const int a1 = std::min(L.ASP[level + 1], a0 + STB_MAX_BLOCKS);
+    ps.push_back(make_stb(c, a0, a1, par, 0, 0));
+    tot += ps.back().total;
+  }
+  void *fn = kfunc<KStb>(c->prec);
+  cudaEvent_t e0, e1;
+  MB_CUDA(cudaEventCreate(&e0));
+  MB_CUDA(cudaEventCreate(&e1));
+  for (int w = 0; w < 3; w++)
+    for (auto &p : ps) {
+      void *args[] = {&p};
+      MB_CUDA(cudaLaunchKernel(fn, dim3((unsigned)((p.total + 255) / 256)), dim3(256), args, 0, s));
+    }
+  MB_CUDA(cudaEventRecord(e0, s));
+  for (int it = 0; it < n; it++)
+    for (auto &p : ps) {
+      void *args[] = {&p};
+      MB_CUDA(cudaLaunchKernel(fn, dim3((unsigned)((p.total + 255) / 256)), dim3(256), args, 0, s));
+    }
+  MB_CUDA(cudaEventRecord(e1, s));
+  MB_CUDA(cudaEventSynchronize(e1));
+  float t = 0;
+  MB_CUDA(cudaEventElapsedTime(&t, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (ms) *ms = t / n;
+  if (bytes) *bytes = (double)tot * 18.0 * (double)prec_bytes(c->prec);
+  if (cells) *cells = tot;
+  return MB_OK;
+}

@@ -1,0 +1,126 @@
+// mblbm_internal.h - host-side internal types shared by the geometry, plan
+// compiler and CUDA context translation units.
+#pragma once
+#include <array>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/mblbm.h"
+
+namespace mblbm {
+
+// cell classes in the per-cell flag byte (bits 0-1), plus attribute bits
+enum : uint8_t {
+  CT_FLUID = 0,
+  CT_SOLID = 1,
+  CT_COPY = 2,  // C_BOUNDARY (never streamed or collided; evolution_block.h:17,44,90)
+  CT_PAD = 3,   // row padding beyond nx
+  CF_EDGE = 4,  // i==0 || j==0 || i==nx-1 || j==ny-1
+  CF_MACRO = 8, // rho/ux/uy of this FLUID cell are read by an interface op
+};
+
+bool obstacle_contains(const mb_config &c, double x, double y);
+int cell_type(const mb_geometry &g, int a, int i, int j);
+
+// One interface point operation (16 bytes, the unit of the record kernel).
+enum : uint8_t { REC_CC = 0, REC_TEMPORAL = 1, REC_CF = 2, REC_FC = 3 };
+enum : uint8_t {
+  RB_SRC_BUF = 1,   // current F buffer of the source block
+  RB_DST_BUF = 2,   // current F buffer of the target block
+  RB_WRITE_F = 4,   // write the distributions (cleared when a later op of the batch overwrites them)
+  RB_WRITE_M = 8,   // write rho/ux/uy
+  RB_WIDX_SHIFT = 4 // 2 bits: index of the temporal weight triple
+};
+struct Rec {
+  uint8_t type;
+  uint8_t bits;
+  uint8_t dst_block;
+  uint8_t src_block;
+  uint8_t m0, m1, m2, pad;
+  int32_t dst_cell;  // j*pitch + i in the target block
+  int32_t src;       // source cell (j*pitch + i) or slot point id
+};
+static_assert(sizeof(Rec) == 16, "Rec must be 16 bytes");
+
+// Static description of a coarse-fine line for the spline kernel.
+struct SplLine {
+  int coarse, fine;      // block ids
+  int Nc, Nf, r;
+  int ci0, cj0, cdi, cdj;  // coarse source line: start and unit step
+  int fi0, fj0, fdi, fdj;  // fine edge line
+  int slot0;             // point id of fine point 0 in the slot array
+  double para;           // (tau_f - 1) / (r (tau_c - 1)), assit_multi.h:176
+};
+
+// One line of a spline node.
+struct SplTask {
+  int line;       // index into the SplLine table
+  int src_buf;    // current F buffer of the coarse block
+  int m0;         // slot written (marker[0] at the time of the call)
+  int mask_off;   // offset into the node's M-write mask (-1: write all points)
+};
+
+enum NodeKind { NK_STB = 0, NK_REC = 1, NK_SPL = 2 };
+
+struct PlanNode {
+  NodeKind kind;
+  int level = -1;             // STB
+  int a0 = 0, a1 = 0;         // STB: block range [a0, a1)
+  uint64_t parity = 0;        // STB: current buffer of each block before the step
+  int macro_all = 0;          // STB: write rho/u of every FLUID cell
+  std::vector<Rec> recs;      // REC
+  double tw[4][3] = {};       // REC: temporal weight triples (a, b, c)
+  int ntw = 0;
+  std::vector<SplTask> spl;   // SPL
+  std::vector<uint8_t> spl_mask;
+  std::vector<int> deps;      // earlier nodes this one waits for (transitively reduced)
+  std::string label;
+};
+
+// Symbolic scheduler state: current buffer per block and ring markers per line.
+struct SchedState {
+  std::vector<int> parity;             // per block
+  std::vector<std::array<int, 3>> marker;  // per coarse-fine line
+  bool operator==(const SchedState &o) const { return parity == o.parity && marker == o.marker; }
+  std::string key() const;
+};
+
+struct BlockLayout {
+  int nx, ny, pitch;
+  long long plane;  // elements between planes k and k+1
+};
+
+// One call of the reference scheduler: a block step of a level or one line op.
+struct Op {
+  enum Kind { STB = 0, CC = 1, TEMPORAL = 2, CF = 3, FC = 4, SPL = 5 } kind;
+  int level = -1, line = -1;
+  double xm = 0;
+  int macro_all = 0;
+  std::vector<int> parity;  // current buffer of every block at the call
+  std::array<int, 3> mk{};  // ring markers of the line at the call
+};
+
+// Compiles n coarse steps of evolution() (evolution.h:2-65) starting from
+// state s into plan nodes with dependency edges; advances s.  final_macros:
+// the last sub-step of every level writes rho/u of all FLUID cells.
+struct PlanCompiler {
+  const mb_geometry &g;
+  const std::vector<BlockLayout> &bl;
+  const std::vector<std::vector<uint8_t>> &flags;  // per block, pitched
+  const std::vector<SplLine> &spl_lines;
+  PlanCompiler(const mb_geometry &g_, const std::vector<BlockLayout> &bl_,
+               const std::vector<std::vector<uint8_t>> &fl, const std::vector<SplLine> &sl)
+      : g(g_), bl(bl_), flags(fl), spl_lines(sl) {}
+  std::vector<PlanNode> compile(SchedState &s, int n_coarse, bool final_macros) const;
+  // one reference call (Op::Kind, level or line index) at state s, state unchanged
+  std::vector<PlanNode> compile_single(int kind, int index, double xm, const SchedState &s) const;
+  // line ops expanded into launches (REC / SPL batches, STB nodes) with DAG edges
+  std::vector<PlanNode> build(const std::vector<Op> &ops) const;
+};
+
+// Cells whose rho/ux/uy an interface op reads (the CF_MACRO attribute).
+void mark_macro_sources(const mb_geometry &g, const std::vector<BlockLayout> &bl,
+                        std::vector<std::vector<uint8_t>> &flags);
+
+}  // namespace mblbm

@@ -1,0 +1,589 @@
+// plan.cpp - plan compiler: the reference level scheduler as a dependency DAG.
+//
+// evolution() (evolution.h:2-65 of zhangya9741/Multi-block-LBM-GPU) issues,
+// per level and sub-step, temporal interpolation, the block step of every
+// block of the level, same-level copies, spatial interpolation with ring
+// rotation, recursion into the next level and the fine-to-coarse transfers,
+// one kernel per line on the default stream.  Here the same sequence is
+// replayed symbolically (parities of the ping-pong buffers and ring markers
+// are tracked on the host), every line op is expanded into point records,
+// consecutive ops are merged into one launch when no point of the launch
+// reads what an earlier op of it writes (or the other way round), and the
+// launches become nodes of a DAG whose edges are exactly the read/write
+// conflicts.  Replaying the DAG in any topological order gives the values of
+// the sequential order.
+#include <algorithm>
+#include <cstdio>
+#include <map>
+#include <set>
+#include <unordered_map>
+#include <unordered_set>
+
+#include "mblbm_internal.h"
+
+namespace mblbm {
+
+std::string SchedState::key() const {
+  std::string k;
+  for (int p : parity) k.push_back(char('0' + p));
+  k.push_back('|');
+  for (auto &m : marker) {
+    k.push_back(char('0' + m[0]));
+    k.push_back(char('0' + m[1]));
+    k.push_back(char('0' + m[2]));
+  }
+  return k;
+}
+
+namespace {
+
+// resource kinds of an access key
+enum : uint64_t { RK_F0 = 0, RK_F1 = 1, RK_M = 2, RK_SLOT = 3 };
+
+inline uint64_t key(uint64_t kind, uint64_t owner, uint64_t idx) { return (kind << 56) | (owner << 48) | idx; }
+inline uint32_t summ(uint64_t k) { return uint32_t(k >> 48); }  // kind<<8 | owner
+inline uint64_t fkey(int buf, int block, long long cell) { return key(buf ? RK_F1 : RK_F0, block, cell); }
+
+struct Whole {
+  uint32_t s;       // kind<<8 | block
+  bool fluid_only;  // only FLUID cells of the block (rho/u written by the block step)
+};
+
+struct Access {
+  std::unordered_set<uint64_t> r, w;
+  std::vector<Whole> wr, ww;
+  std::set<uint32_t> rs, ws;  // summaries of r / w keys and whole entries
+  void read(uint64_t k) { r.insert(k); rs.insert(summ(k)); }
+  void write(uint64_t k) { w.insert(k); ws.insert(summ(k)); }
+  void read_whole(uint32_t s) { wr.push_back({s, false}); rs.insert(s); }
+  void write_whole(uint32_t s, bool fo) { ww.push_back({s, fo}); ws.insert(s); }
+  void merge(const Access &o) {
+    for (auto k : o.r) r.insert(k);
+    for (auto k : o.w) w.insert(k);
+    wr.insert(wr.end(), o.wr.begin(), o.wr.end());
+    ww.insert(ww.end(), o.ww.begin(), o.ww.end());
+    rs.insert(o.rs.begin(), o.rs.end());
+    ws.insert(o.ws.begin(), o.ws.end());
+  }
+};
+
+bool sets_intersect(const std::set<uint32_t> &a, const std::set<uint32_t> &b) {
+  auto i = a.begin();
+  auto j = b.begin();
+  while (i != a.end() && j != b.end()) {
+    if (*i == *j) return true;
+    if (*i < *j) ++i; else ++j;
+  }
+  return false;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// CF_MACRO marks: FLUID cells whose rho/ux/uy are read by c_c (source line),
+// init_Spline3 (coarse line) or f_c (fine points).
+// ---------------------------------------------------------------------------
+static void mark_line(const mb_geometry &g, const std::vector<BlockLayout> &bl,
+                      std::vector<std::vector<uint8_t>> &flags, int a, const mb_p4 &p, int n, int stride) {
+  for (int ip = 0; ip < n; ip++) {
+    int i, j;
+    if (p.xstart == p.xend) { i = p.xstart; j = p.ystart + ip * stride; }
+    else { i = p.xstart + ip * stride; j = p.ystart; }
+    if (i < 0 || j < 0 || i >= bl[a].nx || j >= bl[a].ny) continue;
+    flags[a][(size_t)j * bl[a].pitch + i] |= CF_MACRO;
+  }
+  (void)g;
+}
+
+void mark_macro_sources(const mb_geometry &g, const std::vector<BlockLayout> &bl,
+                        std::vector<std::vector<uint8_t>> &flags) {
+  const mb_layout &L = g.layout;
+  for (int c = 0; c < L.number_line2; c++) {
+    const mb_line &l = g.Line_Inf_CC[c];
+    mark_line(g, bl, flags, l.areac_n, l.line_C, l.Nc, 1);
+  }
+  for (int b = 0; b < L.number_line; b++) {
+    const mb_line &lc = g.Line_Inf_C[b];
+    mark_line(g, bl, flags, lc.areac_n, lc.line_C, lc.Nc, 1);
+    const mb_line &lf = g.Line_Inf_F[b];
+    const int r = g.Areas[lf.areaf_n].m / g.Areas[lf.areac_n].m;
+    mark_line(g, bl, flags, lf.areaf_n, lf.line_F, lf.Nc, r);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// symbolic evolution (evolution.h:2-65)
+// ---------------------------------------------------------------------------
+static void emit(const mb_geometry &g, int level, SchedState &s, std::vector<Op> &ops, bool final_chain) {
+  const mb_layout &L = g.layout;
+  if (level == L.LEVEL) return;
+  for (int i = 0; i < L.mi[level]; i++) {
+    if (!(level == 0 || i == 0)) {
+      for (int b = L.LTCFFCP[level]; b < L.LTCFFCP[level + 1]; b++) {
+        Op o;
+        o.kind = Op::TEMPORAL;
+        o.line = b;
+        o.level = level;
+        o.xm = 1.0 * i / L.mi[level];
+        o.parity = s.parity;
+        o.mk = s.marker[b];
+        ops.push_back(o);
+      }
+    }
+    const bool last = final_chain && (i == L.mi[level] - 1);
+    {
+      Op o;
+      o.kind = Op::STB;
+      o.level = level;
+      o.parity = s.parity;
+      o.macro_all = last ? 1 : 0;
+      ops.push_back(o);
+      for (int a = L.ASP[level]; a < L.ASP[level + 1]; a++) s.parity[a] ^= 1;
+    }
+    if (L.number_line2 != 0) {
+      for (int c = L.LCCP[level]; c < L.LCCP[level + 1]; c++) {
+        Op o;
+        o.kind = Op::CC;
+        o.line = c;
+        o.level = level;
+        o.parity = s.parity;
+        ops.push_back(o);
+      }
+    }
+    if (level != L.LEVEL - 1) {
+      for (int b = L.LS3CFFCP[level]; b < L.LS3CFFCP[level + 1]; b++) {
+        Op o;
+        o.kind = Op::SPL;
+        o.line = b;
+        o.level = level;
+        o.parity = s.parity;
+        o.mk = s.marker[b];
+        ops.push_back(o);
+        for (int p = 0; p < 3; p++) s.marker[b][p] = (s.marker[b][p] == 0) ? 2 : s.marker[b][p] - 1;
+      }
+    }
+    emit(g, level + 1, s, ops, last);
+    if (level != 0 && i == L.mi[level] - 1) {
+      for (int b = L.LTCFFCP[level]; b < L.LTCFFCP[level + 1]; b++) {
+        Op o;
+        o.kind = Op::CF;
+        o.line = b;
+        o.level = level;
+        o.parity = s.parity;
+        o.mk = s.marker[b];
+        ops.push_back(o);
+        o.kind = Op::FC;
+        ops.push_back(o);
+      }
+    }
+  }
+}
+
+static inline void line_pt(const mb_p4 &p, int ip, int stride, int &i, int &j) {
+  if (p.xstart == p.xend) { i = p.xstart; j = p.ystart + ip * stride; }
+  else { i = p.xstart + ip * stride; j = p.ystart; }
+}
+
+std::vector<PlanNode> PlanCompiler::compile(SchedState &s, int n_coarse, bool final_macros) const {
+  std::vector<Op> ops;
+  for (int n = 0; n < n_coarse; n++) emit(g, 0, s, ops, final_macros && n == n_coarse - 1);
+  return build(ops);
+}
+
+std::vector<PlanNode> PlanCompiler::compile_single(int kind, int index, double xm, const SchedState &s) const {
+  Op o;
+  o.kind = Op::Kind(kind);
+  o.parity = s.parity;
+  if (kind == Op::STB) {
+    o.level = index;
+    o.macro_all = 1;
+  } else {
+    o.line = index;
+    if (kind != Op::CC) o.mk = s.marker[index];
+    o.xm = xm;
+  }
+  std::vector<Op> ops{o};
+  return build(ops);
+}
+
+std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
+  const mb_layout &L = g.layout;
+  auto pitch_cell = [&](int a, int i, int j) -> long long { return (long long)j * bl[a].pitch + i; };
+  auto is_fluid = [&](int a, long long cell) { return (flags[a][cell] & 3) == CT_FLUID; };
+
+  // One write of an op (the F part or the M part of a record, or the rho/u
+  // write of a spline point) with the reads it needs.
+  struct Part {
+    int node, idx;
+    uint8_t bit;  // RB_WRITE_F / RB_WRITE_M of record idx, or 0: spline mask entry idx
+    uint64_t wkey;
+    std::vector<uint64_t> rkeys;
+    bool live = true;
+  };
+  struct OpInfo {
+    bool stb = false;
+    int level = -1;
+    std::vector<int> parity;
+    std::vector<Part> parts;
+    std::vector<uint64_t> always_r, always_w;  // spline: gathered cells / written slot
+    int node = -1;
+  };
+  std::vector<OpInfo> info(ops.size());
+  std::vector<PlanNode> nodes;
+  std::vector<Access> acc;  // forward (unpruned) sets: used only to decide batching
+  int open = -1;
+
+  // ---- forward: expand ops into records and batch them ---------------------
+  for (size_t oi = 0; oi < ops.size(); oi++) {
+    const Op &o = ops[oi];
+    OpInfo &I = info[oi];
+    if (o.kind == Op::STB) {
+      open = -1;
+      I.stb = true;
+      I.level = o.level;
+      I.parity = o.parity;
+      for (int a0 = L.ASP[o.level]; a0 < L.ASP[o.level + 1]; a0 += 16) {
+        PlanNode nd;
+        nd.kind = NK_STB;
+        nd.level = o.level;
+        nd.macro_all = o.macro_all;
+        const int a1 = std::min(L.ASP[o.level + 1], a0 + 16);
+        for (int a = a0; a < a1; a++)
+          if (o.parity[a]) nd.parity |= (1ull << a);
+        char lab[64];
+        std::snprintf(lab, sizeof lab, "stb L%d a%d-%d", o.level, a0, a1 - 1);
+        nd.label = lab;
+        nd.a0 = a0;
+        nd.a1 = a1;
+        nodes.push_back(nd);
+        acc.push_back(Access());
+      }
+      continue;
+    }
+    Access ac;
+    std::vector<Rec> recs;
+    struct RP { uint64_t wF, wM; std::vector<uint64_t> rF, rM; };
+    std::vector<RP> rparts;
+    std::vector<uint64_t> spl_wM;
+    SplTask task{};
+    const bool is_spl = (o.kind == Op::SPL);
+    double tw[3] = {0, 0, 0};
+
+    if (o.kind == Op::CC) {
+      const mb_line &l = g.Line_Inf_CC[o.line];
+      const int A = l.areac_n, B = l.areaf_n;
+      const int pA = o.parity[A], pB = o.parity[B];
+      for (int ip = 0; ip < l.Nc; ip++) {
+        int i1 = 0, j1 = 0, i2 = 0, j2 = 0;
+        if (l.line_C.xstart == l.line_C.xend) { i1 = l.line_C.xstart; j1 = l.line_C.ystart + ip; i2 = l.line_F.xstart; j2 = l.line_F.ystart + ip; }
+        if (l.line_C.ystart == l.line_C.yend) { i1 = l.line_C.xstart + ip; j1 = l.line_C.ystart; i2 = l.line_F.xstart + ip; j2 = l.line_F.ystart; }
+        const long long c1 = pitch_cell(A, i1, j1), c2 = pitch_cell(B, i2, j2);
+        Rec r{};
+        r.type = REC_CC;
+        r.bits = uint8_t((pA ? RB_SRC_BUF : 0) | (pB ? RB_DST_BUF : 0) | RB_WRITE_F | RB_WRITE_M);
+        r.dst_block = uint8_t(B);
+        r.src_block = uint8_t(A);
+        r.dst_cell = int32_t(c2);
+        r.src = int32_t(c1);
+        recs.push_back(r);
+        rparts.push_back({fkey(pB, B, c2), key(RK_M, B, c2), {fkey(pA, A, c1)}, {key(RK_M, A, c1)}});
+      }
+    } else if (o.kind == Op::TEMPORAL || o.kind == Op::CF) {
+      const mb_line &l = g.Line_Inf_C[o.line];
+      const int Fb = l.areaf_n, pF = o.parity[Fb];
+      const SplLine &sl = spl_lines[o.line];
+      std::vector<uint64_t> sr;
+      if (o.kind == Op::TEMPORAL) {
+        const double xm = o.xm;
+        tw[0] = 0.5 * (xm - 1.0) * xm;
+        tw[1] = (xm - 1.0) * (xm + 1.0);
+        tw[2] = 0.5 * xm * (xm + 1.0);
+        for (int p = 0; p < 3; p++) sr.push_back(key(RK_SLOT, o.line, o.mk[p]));
+      } else {
+        sr.push_back(key(RK_SLOT, o.line, o.mk[2]));
+      }
+      for (int ip = 0; ip < l.Nf; ip++) {
+        int i, j;
+        line_pt(l.line_F, ip, 1, i, j);
+        const long long c = pitch_cell(Fb, i, j);
+        Rec r{};
+        r.type = (o.kind == Op::TEMPORAL) ? REC_TEMPORAL : REC_CF;
+        r.bits = uint8_t((pF ? RB_DST_BUF : 0) | RB_WRITE_F);
+        r.dst_block = uint8_t(Fb);
+        r.src_block = uint8_t(Fb);
+        r.m0 = uint8_t(o.mk[0]);
+        r.m1 = uint8_t(o.mk[1]);
+        r.m2 = uint8_t(o.mk[2]);
+        r.dst_cell = int32_t(c);
+        r.src = sl.slot0 + ip;
+        recs.push_back(r);
+        rparts.push_back({fkey(pF, Fb, c), ~0ull, sr, {}});
+      }
+    } else if (o.kind == Op::FC) {
+      const mb_line &l = g.Line_Inf_F[o.line];
+      const int Cb = l.areac_n, Fb = l.areaf_n;
+      const int pC = o.parity[Cb], pF = o.parity[Fb];
+      const int r = g.Areas[Fb].m / g.Areas[Cb].m;
+      for (int ip = 0; ip < l.Nc; ip++) {
+        int ic, jc, i_f, j_f;
+        if (l.line_C.xstart == l.line_C.xend) { ic = l.line_C.xstart; jc = l.line_C.ystart + ip; i_f = l.line_F.xstart; j_f = l.line_F.ystart + r * ip; }
+        else { ic = l.line_C.xstart + ip; jc = l.line_C.ystart; i_f = l.line_F.xstart + r * ip; j_f = l.line_F.ystart; }
+        const long long cc = pitch_cell(Cb, ic, jc), cf = pitch_cell(Fb, i_f, j_f);
+        Rec rr{};
+        rr.type = REC_FC;
+        rr.bits = uint8_t((pF ? RB_SRC_BUF : 0) | (pC ? RB_DST_BUF : 0) | RB_WRITE_F | RB_WRITE_M);
+        rr.dst_block = uint8_t(Cb);
+        rr.src_block = uint8_t(Fb);
+        rr.dst_cell = int32_t(cc);
+        rr.src = int32_t(cf);
+        recs.push_back(rr);
+        rparts.push_back({fkey(pC, Cb, cc), key(RK_M, Cb, cc), {fkey(pF, Fb, cf), key(RK_M, Fb, cf)}, {key(RK_M, Fb, cf)}});
+      }
+    } else if (is_spl) {
+      const mb_line &l = g.Line_Inf_C[o.line];
+      const int Cb = l.areac_n, Fb = l.areaf_n, pC = o.parity[Cb];
+      for (int ip = 0; ip < l.Nc; ip++) {
+        int i, j;
+        line_pt(l.line_C, ip, 1, i, j);
+        const long long c = pitch_cell(Cb, i, j);
+        I.always_r.push_back(fkey(pC, Cb, c));
+        I.always_r.push_back(key(RK_M, Cb, c));
+      }
+      for (int ip = 0; ip < l.Nf; ip++) {
+        int i, j;
+        line_pt(l.line_F, ip, 1, i, j);
+        spl_wM.push_back(key(RK_M, Fb, pitch_cell(Fb, i, j)));
+      }
+      I.always_w.push_back(key(RK_SLOT, o.line, o.mk[0]));
+      task.line = o.line;
+      task.src_buf = pC;
+      task.m0 = o.mk[0];
+      task.mask_off = -1;
+    }
+    for (auto &rp : rparts) {
+      for (auto k : rp.rF) ac.read(k);
+      for (auto k : rp.rM) ac.read(k);
+      if (rp.wF != ~0ull) ac.write(rp.wF);
+      if (rp.wM != ~0ull) ac.write(rp.wM);
+    }
+    for (auto k : I.always_r) ac.read(k);
+    for (auto k : I.always_w) ac.write(k);
+    for (auto k : spl_wM) ac.write(k);
+
+    const NodeKind want = is_spl ? NK_SPL : NK_REC;
+    bool join = (open >= 0 && nodes[open].kind == want);
+    if (join && want == NK_REC && o.kind == Op::TEMPORAL) {
+      const PlanNode &nd = nodes[open];
+      bool found = false;
+      for (int t = 0; t < nd.ntw; t++)
+        if (nd.tw[t][0] == tw[0] && nd.tw[t][1] == tw[1] && nd.tw[t][2] == tw[2]) found = true;
+      if (!found && nd.ntw >= 4) join = false;
+    }
+    if (join) {
+      // a launch runs its points concurrently: no point may read what another writes
+      const Access &B = acc[open];
+      for (auto k : ac.r)
+        if (B.w.count(k)) { join = false; break; }
+      if (join)
+        for (auto k : ac.w)
+          if (B.r.count(k)) { join = false; break; }
+    }
+    if (!join) {
+      PlanNode nd;
+      nd.kind = want;
+      nd.label = is_spl ? "spl" : "rec";
+      nodes.push_back(nd);
+      acc.push_back(Access());
+      open = int(nodes.size()) - 1;
+    }
+    PlanNode &nd = nodes[open];
+    I.node = open;
+    if (want == NK_REC) {
+      int widx = 0;
+      if (o.kind == Op::TEMPORAL) {
+        widx = -1;
+        for (int t = 0; t < nd.ntw; t++)
+          if (nd.tw[t][0] == tw[0] && nd.tw[t][1] == tw[1] && nd.tw[t][2] == tw[2]) widx = t;
+        if (widx < 0) {
+          widx = nd.ntw++;
+          nd.tw[widx][0] = tw[0];
+          nd.tw[widx][1] = tw[1];
+          nd.tw[widx][2] = tw[2];
+        }
+      }
+      for (size_t q = 0; q < recs.size(); q++) {
+        Rec r = recs[q];
+        r.bits |= uint8_t(widx << RB_WIDX_SHIFT);
+        const int idx = int(nd.recs.size());
+        nd.recs.push_back(r);
+        const RP &rp = rparts[q];
+        I.parts.push_back({open, idx, RB_WRITE_F, rp.wF, rp.rF});
+        if (rp.wM != ~0ull) I.parts.push_back({open, idx, RB_WRITE_M, rp.wM, rp.rM});
+      }
+    } else {
+      task.mask_off = int(nd.spl_mask.size());
+      for (size_t q = 0; q < spl_wM.size(); q++) {
+        I.parts.push_back({open, task.mask_off + int(q), 0, spl_wM[q], {}});
+        nd.spl_mask.push_back(1);
+      }
+      nd.spl.push_back(task);
+    }
+    acc[open].merge(ac);
+  }
+
+  // ---- backward liveness: drop writes overwritten before any read ----------
+  // state of a key = kind of its nearest later access (true: a write).  Keys
+  // never touched later are read (the state after the plan is observable).
+  struct SummState {
+    bool dflt_write = false;        // default for keys of this (kind, block)
+    bool fluid_write = false;       // M only: default for FLUID cells
+    bool has_fluid = false;
+    std::unordered_map<uint64_t, bool> ov;
+  };
+  std::unordered_map<uint32_t, SummState> st;
+  auto state_of = [&](uint64_t k) -> bool {
+    auto it = st.find(summ(k));
+    if (it == st.end()) return false;
+    auto o2 = it->second.ov.find(k);
+    if (o2 != it->second.ov.end()) return o2->second;
+    if ((k >> 56) == RK_M && it->second.has_fluid) {
+      const int blk = int((k >> 48) & 0xff);
+      if (is_fluid(blk, (long long)(k & 0xffffffffffffull))) return it->second.fluid_write;
+    }
+    return it->second.dflt_write;
+  };
+  auto set_state = [&](uint64_t k, bool w) { st[summ(k)].ov[k] = w; };
+  for (int oi = int(ops.size()) - 1; oi >= 0; oi--) {
+    OpInfo &I = info[oi];
+    if (I.stb) {
+      for (int a = L.ASP[I.level]; a < L.ASP[I.level + 1]; a++) {
+        const int p = I.parity[a];
+        // writes F of buffer 1-p and rho/u of FLUID cells, reads F of buffer p
+        SummState &w = st[uint32_t(((p ? RK_F0 : RK_F1) << 8) | a)];
+        w.ov.clear();
+        w.dflt_write = true;
+        SummState &m = st[uint32_t((RK_M << 8) | a)];
+        for (auto it = m.ov.begin(); it != m.ov.end();) {
+          if (is_fluid(a, (long long)(it->first & 0xffffffffffffull))) it = m.ov.erase(it);
+          else ++it;
+        }
+        m.has_fluid = true;
+        m.fluid_write = true;
+        SummState &r = st[uint32_t(((p ? RK_F1 : RK_F0) << 8) | a)];
+        r.ov.clear();
+        r.dflt_write = false;
+      }
+      continue;
+    }
+    for (Part &pt : I.parts) pt.live = !state_of(pt.wkey);
+    for (Part &pt : I.parts)
+      if (pt.live) set_state(pt.wkey, true);
+    for (auto k : I.always_w) set_state(k, true);
+    for (Part &pt : I.parts)
+      if (pt.live)
+        for (auto k : pt.rkeys) set_state(k, false);
+    for (auto k : I.always_r) set_state(k, false);
+    for (Part &pt : I.parts) {
+      if (pt.live) continue;
+      PlanNode &nd = nodes[pt.node];
+      if (pt.bit) nd.recs[pt.idx].bits &= uint8_t(~pt.bit);
+      else nd.spl_mask.at(pt.idx) = 0;
+    }
+  }
+
+  // ---- final access sets from the surviving parts -----------------------------
+  std::vector<Access> fin(nodes.size());
+  for (size_t q = 0; q < nodes.size(); q++) {
+    if (nodes[q].kind != NK_STB) continue;
+    for (int a = nodes[q].a0; a < nodes[q].a1; a++) {
+      const int p = int((nodes[q].parity >> a) & 1);
+      fin[q].read_whole(uint32_t(((p ? RK_F1 : RK_F0) << 8) | a));
+      fin[q].write_whole(uint32_t(((p ? RK_F0 : RK_F1) << 8) | a), false);
+      fin[q].write_whole(uint32_t((RK_M << 8) | a), true);
+    }
+  }
+  for (auto &I : info) {
+    if (I.stb) continue;
+    Access &A = fin[I.node];
+    for (auto &pt : I.parts) {
+      if (!pt.live) continue;
+      A.write(pt.wkey);
+      for (auto k : pt.rkeys) A.read(k);
+    }
+    for (auto k : I.always_r) A.read(k);
+    for (auto k : I.always_w) A.write(k);
+  }
+  // drop records with nothing left to write, and nodes with nothing to do
+  std::vector<int> remap(nodes.size(), -1);
+  std::vector<PlanNode> kept;
+  std::vector<Access> kacc;
+  for (size_t q = 0; q < nodes.size(); q++) {
+    PlanNode &nd = nodes[q];
+    if (nd.kind == NK_REC) {
+      std::vector<Rec> live;
+      for (const Rec &r : nd.recs)
+        if (r.bits & (RB_WRITE_F | RB_WRITE_M)) live.push_back(r);
+      nd.recs.swap(live);
+      if (nd.recs.empty()) continue;
+    }
+    remap[q] = int(kept.size());
+    kept.push_back(std::move(nd));
+    kacc.push_back(std::move(fin[q]));
+  }
+  nodes.swap(kept);
+  acc.swap(kacc);
+
+  // ---- DAG edges: every earlier node that conflicts with a later one ------
+  const int n = int(nodes.size());
+  auto whole_hits_keys = [&](const Whole &wh, const std::unordered_set<uint64_t> &keys) {
+    for (auto k : keys) {
+      if (summ(k) != wh.s) continue;
+      if (!wh.fluid_only) return true;
+      const int blk = int((k >> 48) & 0xff);
+      if (is_fluid(blk, (long long)(k & 0xffffffffffffull))) return true;
+    }
+    return false;
+  };
+  auto conflict = [&](const Access &p, const Access &q) {
+    // quick reject on summaries
+    const bool wr = sets_intersect(p.ws, q.rs), rw = sets_intersect(p.rs, q.ws), ww = sets_intersect(p.ws, q.ws);
+    if (!wr && !rw && !ww) return false;
+    auto cross = [&](const std::unordered_set<uint64_t> &a, const std::unordered_set<uint64_t> &b) {
+      const auto &sm = a.size() < b.size() ? a : b;
+      const auto &lg = a.size() < b.size() ? b : a;
+      for (auto k : sm)
+        if (lg.count(k)) return true;
+      return false;
+    };
+    auto whole_vs = [&](const std::vector<Whole> &wa, const std::unordered_set<uint64_t> &kb,
+                        const std::vector<Whole> &wb) {
+      for (auto &x : wa) {
+        for (auto &y : wb)
+          if (x.s == y.s) return true;
+        if (whole_hits_keys(x, kb)) return true;
+      }
+      return false;
+    };
+    if (wr && (cross(p.w, q.r) || whole_vs(p.ww, q.r, q.wr) || whole_vs(q.wr, p.w, {}))) return true;
+    if (rw && (cross(p.r, q.w) || whole_vs(p.wr, q.w, q.ww) || whole_vs(q.ww, p.r, {}))) return true;
+    if (ww && (cross(p.w, q.w) || whole_vs(p.ww, q.w, q.ww) || whole_vs(q.ww, p.w, {}))) return true;
+    return false;
+  };
+  std::vector<std::vector<uint64_t>> reach(n, std::vector<uint64_t>((n + 63) / 64, 0));
+  for (int q = 0; q < n; q++) {
+    std::vector<int> direct;
+    for (int p = q - 1; p >= 0; p--)
+      if (conflict(acc[p], acc[q])) direct.push_back(p);
+    // transitive reduction (direct is in descending order)
+    for (int p : direct) {
+      if (reach[q][p >> 6] & (1ull << (p & 63))) continue;
+      nodes[q].deps.push_back(p);
+      reach[q][p >> 6] |= 1ull << (p & 63);
+      for (size_t w = 0; w < reach[q].size(); w++) reach[q][w] |= reach[p][w];
+    }
+    std::sort(nodes[q].deps.begin(), nodes[q].deps.end());
+  }
+  return nodes;
+}
+
+}  // namespace mblbm

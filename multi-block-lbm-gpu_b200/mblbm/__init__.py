@@ -1,0 +1,375 @@
+"""Python host-side mirror of the mblbm C ABI (include/mblbm.h).
+
+The names follow the reference program's host call surface
+(zhangya9741/Multi-block-LBM-GPU): ``geo_init`` (geo/init_geo.h:89),
+``evolution`` (evolution.h:2), ``error_L2`` (lbm/error_L2.h:57),
+``getDrag_block`` (lbm/force_block.h:180) and ``output``
+(output/output.h:2).  Everything runs through ``libmblbm.so``; there is no
+Python or CPU fallback: constructing a :class:`MultiBlockLBM` without the
+library or without a CUDA device raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libmblbm.so")
+
+MB_MAX_LEVEL = 8
+MB_MAX_AREA = 64
+MB_MAX_LINE = 128
+MB_MAX_LINE2 = 128
+
+MB_OK = 0
+PREC_F64, PREC_F32, PREC_F16S = 0, 1, 2
+PRECISIONS = {"f64": PREC_F64, "f32": PREC_F32, "f16s": PREC_F16S}
+FLUID, SOLID_SBB, C_BOUNDARY = 0, 1, 9
+OBST_CIRCLE, OBST_ELLIPSE = 0, 1
+
+
+class P4(C.Structure):
+    _fields_ = [("xstart", C.c_int), ("xend", C.c_int), ("ystart", C.c_int), ("yend", C.c_int)]
+
+
+class P4d(C.Structure):
+    _fields_ = [("xstart", C.c_double), ("xend", C.c_double), ("ystart", C.c_double), ("yend", C.c_double)]
+
+
+class Zone(C.Structure):
+    _fields_ = [("reduced", P4d), ("move", P4)]
+
+
+class P3i(C.Structure):
+    _fields_ = [("nc", C.c_int), ("nf", C.c_int), ("direction", C.c_int)]
+
+
+class Layout(C.Structure):
+    _fields_ = [
+        ("LEVEL", C.c_int),
+        ("mi", C.c_int * MB_MAX_LEVEL),
+        ("number_area", C.c_int),
+        ("number_line", C.c_int),
+        ("number_line2", C.c_int),
+        ("ASP", C.c_int * (MB_MAX_LEVEL + 1)),
+        ("AreaZone", Zone * MB_MAX_AREA),
+        ("LTCFFCP", C.c_int * (MB_MAX_LEVEL + 1)),
+        ("LS3CFFCP", C.c_int * (MB_MAX_LEVEL + 1)),
+        ("LCCP", C.c_int * (MB_MAX_LEVEL + 1)),
+        ("NeborCF", P3i * MB_MAX_LINE),
+        ("NeborCC", P3i * MB_MAX_LINE2),
+    ]
+
+
+class Config(C.Structure):
+    _fields_ = [
+        ("Re", C.c_double),
+        ("rho0", C.c_double),
+        ("LX", C.c_int),
+        ("LY", C.c_int),
+        ("R", C.c_int),
+        ("CX", C.c_int),
+        ("CY", C.c_int),
+        ("U0", C.c_double * 2),
+        ("obstacle", C.c_int),
+        ("ell_cx", C.c_double),
+        ("ell_cy", C.c_double),
+        ("ell_a", C.c_double),
+        ("ell_b", C.c_double),
+        ("ell_angle", C.c_double),
+        ("drag_area", C.c_int),
+    ]
+
+
+class Area(C.Structure):
+    _fields_ = [
+        ("m", C.c_int),
+        ("nx", C.c_int),
+        ("ny", C.c_int),
+        ("base_x", C.c_double),
+        ("base_y", C.c_double),
+        ("tau", C.c_double),
+        ("rv_tau", C.c_double),
+    ]
+
+
+class Line(C.Structure):
+    _fields_ = [("areac_n", C.c_int), ("Nc", C.c_int), ("line_C", P4), ("areaf_n", C.c_int), ("Nf", C.c_int), ("line_F", P4)]
+
+
+class Geometry(C.Structure):
+    _fields_ = [
+        ("layout", Layout),
+        ("config", Config),
+        ("AreaDefine", P4 * MB_MAX_AREA),
+        ("Areas", Area * MB_MAX_AREA),
+        ("Line_Inf_C", Line * MB_MAX_LINE),
+        ("Line_Inf_F", Line * MB_MAX_LINE),
+        ("Line_Inf_CC", Line * MB_MAX_LINE2),
+    ]
+
+
+# every symbol declared in include/mblbm.h, with its ctypes signature
+_vp = C.c_void_p
+_pd = C.POINTER(C.c_double)
+_pi = C.POINTER(C.c_int)
+_pll = C.POINTER(C.c_longlong)
+SIGNATURES = {
+    "mb_version": ([], C.c_int),
+    "mb_error_string": ([C.c_int], C.c_char_p),
+    "mb_layout_builtin": ([C.c_char_p, C.POINTER(Layout)], C.c_int),
+    "mb_layout_nested": ([C.c_int, C.c_int, C.c_int, _pi, C.POINTER(Layout)], C.c_int),
+    "mb_geo_init": ([C.POINTER(Layout), C.POINTER(Config), C.POINTER(Geometry)], C.c_int),
+    "mb_geo_check_coverage": ([C.POINTER(Geometry), _pi], C.c_int),
+    "mb_create": ([C.POINTER(Geometry), C.c_int, C.POINTER(_vp)], C.c_int),
+    "mb_destroy": ([_vp], C.c_int),
+    "mb_init": ([_vp, _vp], C.c_int),
+    "mb_step": ([_vp, C.c_int, _vp], C.c_int),
+    "mb_set_graph_mode": ([_vp, C.c_int], C.c_int),
+    "mb_prepare": ([_vp, C.c_int], C.c_int),
+    "mb_block_step": ([_vp, C.c_int, _vp], C.c_int),
+    "mb_c_c_boundary_transfer": ([_vp, C.c_int, _vp], C.c_int),
+    "mb_space_interpolation": ([_vp, C.c_int, _vp], C.c_int),
+    "mb_temporal_interpolation": ([_vp, C.c_int, C.c_double, _vp], C.c_int),
+    "mb_c_f_boundary_transfer": ([_vp, C.c_int, _vp], C.c_int),
+    "mb_f_c_boundary_transfer": ([_vp, C.c_int, _vp], C.c_int),
+    "mb_rotate_markers": ([_vp, C.c_int], C.c_int),
+    "mb_drag": ([_vp, _pd, _pd, _pd, _vp], C.c_int),
+    "mb_drag_link_count": ([_vp, _pi], C.c_int),
+    "mb_error_L2": ([_vp, _pd, _vp], C.c_int),
+    "mb_check_finite": ([_vp, _pll, _vp], C.c_int),
+    "mb_copy_fields": ([_vp, C.c_int, _pd, _pd, _pd, _pd, _pi, _vp], C.c_int),
+    "mb_set_fields": ([_vp, C.c_int, _pd, _pd, _pd, _pd, _vp], C.c_int),
+    "mb_write_tecplot": ([_vp, C.c_char_p], C.c_int),
+    "mb_append_drag": ([C.c_char_p, C.c_int, C.c_double, C.c_double], C.c_int),
+    "mb_append_error_L2": ([C.c_char_p, C.c_int, C.c_double], C.c_int),
+    "mb_stats": ([_vp, _pll, _pll, _pll], C.c_int),
+    "mb_time_block_step": ([_vp, C.c_int, C.c_int, _vp, _pd, _pd, _pll], C.c_int),
+}
+
+_lib = None
+
+
+class MBError(RuntimeError):
+    def __init__(self, code, what):
+        self.code = code
+        super().__init__(f"{what}: {load().mb_error_string(code).decode()} ({code})")
+
+
+def load(path=LIB_PATH):
+    """Loads libmblbm.so (raises OSError when it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(path):
+            raise OSError(f"{path} not built; run multi-block-lbm-gpu_b200/build.py")
+        lib = C.CDLL(path)
+        for name, (args, res) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = lib
+    return _lib
+
+
+def _check(code, what):
+    if code != MB_OK:
+        raise MBError(code, what)
+
+
+def _dp(a):
+    return None if a is None else a.ctypes.data_as(_pd)
+
+
+# ---------------------------------------------------------------------------
+# layouts and configurations
+# ---------------------------------------------------------------------------
+def layout_builtin(name):
+    """Tables of geo/geometry.h for _GEO_<name> ("1_1", "2_2", "2_5", "4_9")."""
+    L = Layout()
+    _check(load().mb_layout_builtin(name.encode(), C.byref(L)), f"mb_layout_builtin({name})")
+    return L
+
+
+def layout_nested(LX, LY, boxes):
+    """Nested-frame layout; boxes = [(xs, xe, ys, ye), ...] per refined level."""
+    flat = (C.c_int * max(1, 4 * len(boxes)))(*[v for b in boxes for v in b])
+    L = Layout()
+    _check(load().mb_layout_nested(LX, LY, len(boxes) + 1, flat, C.byref(L)), "mb_layout_nested")
+    return L
+
+
+def make_config(LX, LY, R, CX, CY, U0=(0.1, 0.0), Re=10.0, rho0=1.0, drag_area=-1, ellipse=None):
+    c = Config()
+    c.Re, c.rho0, c.LX, c.LY, c.R, c.CX, c.CY = float(Re), float(rho0), LX, LY, R, CX, CY
+    c.U0[0], c.U0[1] = float(U0[0]), float(U0[1])
+    c.obstacle = OBST_CIRCLE
+    c.drag_area = drag_area
+    if ellipse is not None:
+        c.obstacle = OBST_ELLIPSE
+        c.ell_cx, c.ell_cy, c.ell_a, c.ell_b, c.ell_angle = [float(v) for v in ellipse]
+    return c
+
+
+def geo_init(layout, config):
+    """geo_init() (geo/init_geo.h:89-165) -> Geometry."""
+    g = Geometry()
+    _check(load().mb_geo_init(C.byref(layout), C.byref(config), C.byref(g)), "mb_geo_init")
+    return g
+
+
+def coverage(geo):
+    n = C.c_int(0)
+    _check(load().mb_geo_check_coverage(C.byref(geo), C.byref(n)), "mb_geo_check_coverage")
+    return n.value
+
+
+# Workloads of the benchmark configurations (coarse cells).
+def config1_geometry():
+    """2-level cylinder, Re=40: 400x160 coarse, fine box [60,140]x[40,120], D=20 at (100,80), U0=0.05."""
+    L = layout_nested(400, 160, [(60, 140, 40, 120)])
+    return geo_init(L, make_config(400, 160, 10, 100, 80, U0=(0.05, 0.0), Re=40.0))
+
+
+def config2_geometry():
+    """3-level cylinder, Re=100: 4096x1024 coarse, level-1 box 512x256, level-2 box 256x128,
+    D=32 at (960,512), U0=0.04."""
+    L = layout_nested(4096, 1024, [(768, 1280, 384, 640), (896, 1152, 448, 576)])
+    return geo_init(L, make_config(4096, 1024, 16, 960, 512, U0=(0.04, 0.0), Re=100.0))
+
+
+def updates_per_coarse_step(geo):
+    L = geo.layout
+    tot = 0
+    for l in range(L.LEVEL):
+        steps = 1
+        for q in range(1, l + 1):
+            steps *= L.mi[q]
+        for a in range(L.ASP[l], L.ASP[l + 1]):
+            tot += steps * geo.Areas[a].nx * geo.Areas[a].ny
+    return tot
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        return None
+    if isinstance(stream, int):
+        return stream
+    return int(stream.cuda_stream)  # torch.cuda.Stream
+
+
+# ---------------------------------------------------------------------------
+# the solver context
+# ---------------------------------------------------------------------------
+class MultiBlockLBM:
+    """One multi-block simulation on the current CUDA device."""
+
+    def __init__(self, geo, precision="f32", graph=True):
+        self.lib = load()
+        self.geo = geo
+        self.precision = precision
+        h = C.c_void_p()
+        _check(self.lib.mb_create(C.byref(geo), PRECISIONS[precision], C.byref(h)), "mb_create")
+        self.h = h
+        if not graph:
+            _check(self.lib.mb_set_graph_mode(self.h, 0), "mb_set_graph_mode")
+        self.n = 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mb_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- reference call surface -------------------------------------------------
+    def init(self, stream=None):
+        _check(self.lib.mb_init(self.h, _stream_ptr(stream)), "mb_init")
+        self.n = 0
+
+    def evolution(self, n_coarse=1, stream=None):
+        _check(self.lib.mb_step(self.h, int(n_coarse), _stream_ptr(stream)), "mb_step")
+        self.n += n_coarse
+
+    def prepare(self, n_coarse):
+        """Compiles the plans and graphs that evolution(n_coarse) will replay."""
+        _check(self.lib.mb_prepare(self.h, int(n_coarse)), "mb_prepare")
+
+    def block_step(self, area, stream=None):
+        _check(self.lib.mb_block_step(self.h, area, _stream_ptr(stream)), "mb_block_step")
+
+    def c_c_boundary_transfer(self, line, stream=None):
+        _check(self.lib.mb_c_c_boundary_transfer(self.h, line, _stream_ptr(stream)), "mb_c_c_boundary_transfer")
+
+    def space_interpolation(self, line, stream=None):
+        _check(self.lib.mb_space_interpolation(self.h, line, _stream_ptr(stream)), "mb_space_interpolation")
+
+    def temporal_interpolation(self, line, xm, stream=None):
+        _check(self.lib.mb_temporal_interpolation(self.h, line, float(xm), _stream_ptr(stream)), "mb_temporal_interpolation")
+
+    def c_f_boundary_transfer(self, line, stream=None):
+        _check(self.lib.mb_c_f_boundary_transfer(self.h, line, _stream_ptr(stream)), "mb_c_f_boundary_transfer")
+
+    def f_c_boundary_transfer(self, line, stream=None):
+        _check(self.lib.mb_f_c_boundary_transfer(self.h, line, _stream_ptr(stream)), "mb_f_c_boundary_transfer")
+
+    def rotate_markers(self, line):
+        _check(self.lib.mb_rotate_markers(self.h, line), "mb_rotate_markers")
+
+    def getDrag_block(self, stream=None):
+        """Returns (Fx, Fy, Cd, Cl) as getDrag_block computes them."""
+        f = (C.c_double * 2)()
+        cd, cl = C.c_double(), C.c_double()
+        _check(self.lib.mb_drag(self.h, f, C.byref(cd), C.byref(cl), _stream_ptr(stream)), "mb_drag")
+        return f[0], f[1], cd.value, cl.value
+
+    def drag_links(self):
+        n = C.c_int()
+        _check(self.lib.mb_drag_link_count(self.h, C.byref(n)), "mb_drag_link_count")
+        return n.value
+
+    def error_L2(self, stream=None):
+        e = C.c_double()
+        _check(self.lib.mb_error_L2(self.h, C.byref(e), _stream_ptr(stream)), "mb_error_L2")
+        return e.value
+
+    def check_finite(self, stream=None):
+        bad = C.c_longlong()
+        self.lib.mb_check_finite(self.h, C.byref(bad), _stream_ptr(stream))
+        return bad.value
+
+    def fields(self, area, stream=None):
+        """Dict of FP64 host arrays rho, ux, uy (ny, nx), F (9, ny, nx), solid (ny, nx)."""
+        A = self.geo.Areas[area]
+        nx, ny = A.nx, A.ny
+        rho = np.empty((ny, nx))
+        ux = np.empty((ny, nx))
+        uy = np.empty((ny, nx))
+        F = np.empty((9, ny, nx))
+        solid = np.empty((ny, nx), dtype=np.int32)
+        _check(
+            self.lib.mb_copy_fields(self.h, area, _dp(rho), _dp(ux), _dp(uy), _dp(F), solid.ctypes.data_as(_pi), _stream_ptr(stream)),
+            "mb_copy_fields",
+        )
+        return {"rho": rho, "ux": ux, "uy": uy, "F": F, "solid": solid}
+
+    def set_fields(self, area, rho=None, ux=None, uy=None, F=None, stream=None):
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (rho, ux, uy, F)]
+        _check(self.lib.mb_set_fields(self.h, area, *[_dp(a) for a in arrs], _stream_ptr(stream)), "mb_set_fields")
+
+    def output(self, path):
+        _check(self.lib.mb_write_tecplot(self.h, path.encode()), "mb_write_tecplot")
+
+    def stats(self):
+        a, b, c = C.c_longlong(), C.c_longlong(), C.c_longlong()
+        _check(self.lib.mb_stats(self.h, C.byref(a), C.byref(b), C.byref(c)), "mb_stats")
+        return {"kernels_last_call": a.value, "kernels_per_coarse_step": b.value, "updates_per_coarse_step": c.value}
+
+    def time_block_step(self, level, n, stream=None):
+        ms, by, cells = C.c_double(), C.c_double(), C.c_longlong()
+        _check(self.lib.mb_time_block_step(self.h, level, n, _stream_ptr(stream), C.byref(ms), C.byref(by), C.byref(cells)),
+               "mb_time_block_step")
+        return ms.value, by.value, cells.value

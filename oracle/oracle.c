@@ -1,0 +1,830 @@
+/*
+ * oracle.c - FP64 CPU restatement of the reference multi-block D2Q9 step.
+ *
+ * TEST INFRASTRUCTURE ONLY (the checker): the product library never links,
+ * loads or calls this file.  Only tests/, __graft_entry__.smoke() and the
+ * cpu_baseline leg of bench.py use it.
+ *
+ * Each function below restates one reference function of
+ * zhangya9741/Multi-block-LBM-GPU (cited file:line) in plain C, keeping the
+ * FP64 operation order of the reference expressions, the structure-of-arrays
+ * layout (ixy = i + j*nx) and the quirks listed at each function.  OpenMP
+ * parallelises loops whose iterations are independent in the reference too,
+ * so results do not depend on the thread count.
+ */
+#include "oracle.h"
+
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define Q 9
+#define BLOCKX 16   /* _BLOCKX, parameters.h:9  */
+#define BLOCKY 16   /* _BLOCKY, parameters.h:10 */
+#define BLOCK1D 256 /* _BLOCK_1D, parameters.h:11 */
+
+/* D2Q9 tables, lbm/lbm.h:43-45 */
+static const double Wt[Q] = {4. / 9, 1. / 9, 1. / 9, 1. / 9, 1. / 9, 1. / 36, 1. / 36, 1. / 36, 1. / 36};
+static const int Ev[2 * Q] = {0, 1, 0, -1, 0, 1, -1, -1, 1, 0, 0, 1, 0, -1, 1, 1, -1, -1};
+static const int Opp[Q] = {0, 3, 4, 1, 2, 7, 8, 5, 6};
+
+typedef struct {
+  int *solid;
+  double *x, *y, *rho, *ux, *uy, *forcex, *forcey;
+  double *f[Q];
+  double *F[Q];
+} o_d2q9; /* D2Q9, lbm/data_type_lbm.h:7-14 */
+
+typedef struct {
+  int N;
+  int marker[3];
+  double *F[3][Q]; /* f_t1, f_t, f_t_1 (multi/data_type_multi.h:24-30) */
+} o_fstore;
+
+typedef struct {
+  int N;
+  double *l, *m, *u, *Varibs_M;
+  double *rho, *ux, *uy;
+  double *F[Q];
+} o_spline; /* FM_spline3, multi/data_type_multi.h:7-13 */
+
+struct orc_sim {
+  mb_geometry geo;
+  o_d2q9 pp[MB_MAX_AREA];
+  double *upx[MB_MAX_AREA], *upy[MB_MAX_AREA];
+  o_fstore t3[MB_MAX_LINE];
+  o_spline s3[MB_MAX_LINE];
+  int drag_area;
+  int n_drag;
+  int *drag; /* 3 * n_drag: i, j, k */
+  double U0_2;
+};
+
+void orc_set_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+#else
+  (void)n;
+#endif
+}
+
+/* feq, lbm/assit_func.h:2-9 */
+double orc_feq(int k, double rh, double uxx, double uyy) {
+  double eu, uv, feq0;
+  eu = Ev[k] * uxx + Ev[k + Q] * uyy;
+  uv = uxx * uxx + uyy * uyy;
+  feq0 = Wt[k] * rh * (1.0 + 3.0 * eu + 4.5 * eu * eu - 1.5 * uv);
+  return feq0;
+}
+
+/* Macros, lbm/assit_func.h:23-31 */
+static inline void macros(double *rh, double *uxx, double *uyy, const double *ft) {
+  *rh = ft[0] + ft[1] + ft[2] + ft[3] + ft[4] + ft[5] + ft[6] + ft[7] + ft[8];
+  *uxx = ft[1] - ft[3] + ft[5] - ft[6] - ft[7] + ft[8];
+  *uyy = ft[2] - ft[4] + ft[5] + ft[6] - ft[7] - ft[8];
+  *uxx = *uxx / *rh;
+  *uyy = *uyy / *rh;
+}
+
+/* ---------------------------------------------------------------------------
+ * Geometry: Line_init (geo/init_geo.h:17-86) and geo_init (:89-165)
+ * ------------------------------------------------------------------------- */
+static void line_init(int Direction, const mb_p4 *aD_C, const mb_area *aC, mb_line *lC,
+                      const mb_p4 *aD_F, const mb_area *aF, mb_line *lF) {
+  if (Direction == 0 || Direction == 1) {
+    lC->line_C.xstart = (Direction == 0 ? aC->m : aC->nx - 1 - aC->m);
+    lC->line_C.xend = lC->line_C.xstart;
+    lC->line_F.xstart = (Direction == 0 ? aF->nx - 1 : 0);
+    lC->line_F.xend = lC->line_F.xstart;
+    lF->line_C.xstart = (Direction == 0 ? 0 : aC->nx - 1);
+    lF->line_C.xend = lF->line_C.xstart;
+    lF->line_F.xstart = (Direction == 0 ? aF->nx - aF->m - 1 : aF->m);
+    lF->line_F.xend = lF->line_F.xstart;
+
+    lC->line_C.ystart = (aD_F->ystart - aD_C->ystart <= 0) ? 0 : (aD_F->ystart - aD_C->ystart) * aC->m;
+    lC->line_C.yend = (aD_F->yend - aD_C->yend >= 0) ? aC->ny - 1 : (aD_F->yend - aD_C->ystart) * aC->m;
+    lC->line_F.ystart = (aD_C->ystart - aD_F->ystart <= 0) ? 0 : (aD_C->ystart - aD_F->ystart) * aF->m;
+    lC->line_F.yend = (aD_C->yend - aD_F->yend >= 0) ? aF->ny - 1 : (aD_C->yend - aD_F->ystart) * aF->m;
+    lF->line_C.ystart = lC->line_C.ystart;
+    lF->line_C.yend = lC->line_C.yend;
+    lF->line_F.ystart = lC->line_F.ystart;
+    lF->line_F.yend = lC->line_F.yend;
+    lC->Nc = lC->line_C.yend - lC->line_C.ystart + 1;
+    lC->Nf = lC->line_F.yend - lC->line_F.ystart + 1;
+    lF->Nc = lC->Nc;
+    lF->Nf = lC->Nf;
+  } else if (Direction == 2 || Direction == 3) {
+    lC->line_C.ystart = (Direction == 2 ? aC->m : aC->ny - 1 - aC->m);
+    lC->line_C.yend = lC->line_C.ystart;
+    lC->line_F.ystart = (Direction == 2 ? aF->ny - 1 : 0);
+    lC->line_F.yend = lC->line_F.ystart;
+    lF->line_C.ystart = (Direction == 2 ? 0 : aC->ny - 1);
+    lF->line_C.yend = lF->line_C.ystart;
+    lF->line_F.ystart = (Direction == 2 ? aF->ny - aF->m - 1 : aF->m);
+    lF->line_F.yend = lF->line_F.ystart;
+
+    lC->line_C.xstart = (aD_F->xstart - aD_C->xstart <= 0) ? 0 : (aD_F->xstart - aD_C->xstart) * aC->m;
+    lC->line_C.xend = (aD_F->xend - aD_C->xend >= 0) ? aC->nx - 1 : (aD_F->xend - aD_C->xstart) * aC->m;
+    lC->line_F.xstart = (aD_C->xstart - aD_F->xstart <= 0) ? 0 : (aD_C->xstart - aD_F->xstart) * aF->m;
+    lC->line_F.xend = (aD_C->xend - aD_F->xend >= 0) ? aF->nx - 1 : (aD_C->xend - aD_F->xstart) * aF->m;
+    lF->line_C.xstart = lC->line_C.xstart;
+    lF->line_C.xend = lC->line_C.xend;
+    lF->line_F.xstart = lC->line_F.xstart;
+    lF->line_F.xend = lC->line_F.xend;
+    lC->Nc = lC->line_C.xend - lC->line_C.xstart + 1;
+    lC->Nf = lC->line_F.xend - lC->line_F.xstart + 1;
+    lF->Nc = lC->Nc;
+    lF->Nf = lC->Nf;
+  }
+}
+
+int orc_geo_init(const mb_layout *L, const mb_config *cfg, mb_geometry *g) {
+  if (!L || !cfg || !g) return MB_ERR_INVALID;
+  memset(g, 0, sizeof(*g));
+  g->layout = *L;
+  g->config = *cfg;
+  const int LX = cfg->LX, LY = cfg->LY;
+  for (int i = 0; i < L->number_area; i++) {
+    g->AreaDefine[i].xstart = (int)(L->AreaZone[i].reduced.xstart * (LX - 1)) + L->AreaZone[i].move.xstart;
+    g->AreaDefine[i].xend = (int)(L->AreaZone[i].reduced.xend * (LX - 1)) + L->AreaZone[i].move.xend;
+    g->AreaDefine[i].ystart = (int)(L->AreaZone[i].reduced.ystart * (LY - 1)) + L->AreaZone[i].move.ystart;
+    g->AreaDefine[i].yend = (int)(L->AreaZone[i].reduced.yend * (LY - 1)) + L->AreaZone[i].move.yend;
+  }
+  int mm = 1;
+  double U0_2 = sqrt(cfg->U0[0] * cfg->U0[0] + cfg->U0[1] * cfg->U0[1]);
+  double niu = U0_2 * 2 * cfg->R / cfg->Re;
+  double tau = 0.5 + 3.0 * niu;
+  double rv_tau = 1.0 / tau;
+  for (int i = 0; i < L->LEVEL; i++) {
+    mm *= L->mi[i];
+    tau = 0.5 + L->mi[i] * (tau - 0.5);
+    rv_tau = 1.0 / tau;
+    for (int j = L->ASP[i]; j < L->ASP[i + 1]; j++) {
+      g->Areas[j].m = mm;
+      g->Areas[j].nx = (g->AreaDefine[j].xend - g->AreaDefine[j].xstart) * mm + 1;
+      g->Areas[j].ny = (g->AreaDefine[j].yend - g->AreaDefine[j].ystart) * mm + 1;
+      g->Areas[j].base_x = g->AreaDefine[j].xstart;
+      g->Areas[j].base_y = g->AreaDefine[j].ystart;
+      g->Areas[j].tau = tau;
+      g->Areas[j].rv_tau = rv_tau;
+    }
+  }
+  for (int i = 0; i < L->number_line; i++) {
+    int nc = L->NeborCF[i].nc, nf = L->NeborCF[i].nf;
+    g->Line_Inf_C[i].areac_n = nc;
+    g->Line_Inf_C[i].areaf_n = nf;
+    g->Line_Inf_F[i].areac_n = nc;
+    g->Line_Inf_F[i].areaf_n = nf;
+    line_init(L->NeborCF[i].direction, &g->AreaDefine[nc], &g->Areas[nc], &g->Line_Inf_C[i],
+              &g->AreaDefine[nf], &g->Areas[nf], &g->Line_Inf_F[i]);
+  }
+  for (int i = 0; i + 1 < L->number_line2; i += 2) {
+    int nc = L->NeborCC[i].nc, nf = L->NeborCC[i].nf;
+    g->Line_Inf_CC[i].areac_n = nc;
+    g->Line_Inf_CC[i].areaf_n = nf;
+    line_init(L->NeborCC[i].direction, &g->AreaDefine[nc], &g->Areas[nc], &g->Line_Inf_CC[i],
+              &g->AreaDefine[nf], &g->Areas[nf], &g->Line_Inf_CC[i + 1]);
+    g->Line_Inf_CC[i + 1].areac_n = L->NeborCC[i + 1].nc;
+    g->Line_Inf_CC[i + 1].areaf_n = L->NeborCC[i + 1].nf;
+    mb_p4 tmp = g->Line_Inf_CC[i + 1].line_C;
+    g->Line_Inf_CC[i + 1].line_C = g->Line_Inf_CC[i + 1].line_F;
+    g->Line_Inf_CC[i + 1].line_F = tmp;
+  }
+  return MB_OK;
+}
+
+/* ---------------------------------------------------------------------------
+ * Allocation (Multi-block-LBM.cu:26-113)
+ * ------------------------------------------------------------------------- */
+static double *dalloc(size_t n) { return (double *)calloc(n ? n : 1, sizeof(double)); }
+
+orc_sim *orc_create(const mb_geometry *geo) {
+  orc_sim *s = (orc_sim *)calloc(1, sizeof(orc_sim));
+  if (!s) return NULL;
+  s->geo = *geo;
+  const mb_layout *L = &geo->layout;
+  for (int a = 0; a < L->number_area; a++) {
+    size_t N = (size_t)geo->Areas[a].nx * geo->Areas[a].ny;
+    o_d2q9 *p = &s->pp[a];
+    p->solid = (int *)calloc(N, sizeof(int));
+    p->x = dalloc(N); p->y = dalloc(N); p->rho = dalloc(N); p->ux = dalloc(N); p->uy = dalloc(N);
+    p->forcex = dalloc(N); p->forcey = dalloc(N);
+    for (int k = 0; k < Q; k++) { p->f[k] = dalloc(N); p->F[k] = dalloc(N); }
+    s->upx[a] = dalloc(N);
+    s->upy[a] = dalloc(N);
+  }
+  for (int b = 0; b < L->number_line; b++) {
+    o_fstore *t = &s->t3[b];
+    t->marker[0] = 2; t->marker[1] = 1; t->marker[2] = 0; /* Multi-block-LBM.cu:45-47 */
+    t->N = geo->Line_Inf_C[b].Nf;
+    for (int i = 0; i < 3; i++)
+      for (int k = 0; k < Q; k++) t->F[i][k] = dalloc(t->N);
+    o_spline *sp = &s->s3[b];
+    sp->N = geo->Line_Inf_C[b].Nc;
+    sp->l = dalloc(sp->N); sp->m = dalloc(sp->N); sp->u = dalloc(sp->N);
+    sp->Varibs_M = dalloc(12 * (size_t)sp->N);
+    sp->rho = dalloc(sp->N); sp->ux = dalloc(sp->N); sp->uy = dalloc(sp->N);
+    for (int k = 0; k < Q; k++) sp->F[k] = dalloc(sp->N);
+  }
+  s->drag_area = geo->config.drag_area < 0 ? L->number_area - 1 : geo->config.drag_area;
+  s->U0_2 = sqrt(geo->config.U0[0] * geo->config.U0[0] + geo->config.U0[1] * geo->config.U0[1]);
+  return s;
+}
+
+void orc_destroy(orc_sim *s) {
+  if (!s) return;
+  const mb_layout *L = &s->geo.layout;
+  for (int a = 0; a < L->number_area; a++) {
+    o_d2q9 *p = &s->pp[a];
+    free(p->solid); free(p->x); free(p->y); free(p->rho); free(p->ux); free(p->uy);
+    free(p->forcex); free(p->forcey);
+    for (int k = 0; k < Q; k++) { free(p->f[k]); free(p->F[k]); }
+    free(s->upx[a]); free(s->upy[a]);
+  }
+  for (int b = 0; b < L->number_line; b++) {
+    for (int i = 0; i < 3; i++)
+      for (int k = 0; k < Q; k++) free(s->t3[b].F[i][k]);
+    o_spline *sp = &s->s3[b];
+    free(sp->l); free(sp->m); free(sp->u); free(sp->Varibs_M);
+    free(sp->rho); free(sp->ux); free(sp->uy);
+    for (int k = 0; k < Q; k++) free(sp->F[k]);
+  }
+  free(s->drag);
+  free(s);
+}
+
+/* ---------------------------------------------------------------------------
+ * init_General (lbm/init_block.h:2-51).  The ellipse branch has no reference
+ * counterpart (batched cases only).
+ * ------------------------------------------------------------------------- */
+static int is_solid(const mb_config *c, double x, double y) {
+  if (c->obstacle == MB_OBST_ELLIPSE) {
+    double dx = x - c->ell_cx, dy = y - c->ell_cy;
+    double ca = cos(c->ell_angle), sa = sin(c->ell_angle);
+    double xr = ca * dx + sa * dy, yr = -sa * dx + ca * dy;
+    return (xr * xr) / (c->ell_a * c->ell_a) + (yr * yr) / (c->ell_b * c->ell_b) < 1.0;
+  }
+  return (x - c->CX) * (x - c->CX) + (y - c->CY) * (y - c->CY) < c->R * c->R;
+}
+
+static void init_general(orc_sim *s, int a) {
+  const mb_area *ar = &s->geo.Areas[a];
+  const mb_config *c = &s->geo.config;
+  o_d2q9 *pp = &s->pp[a];
+  const int nx = ar->nx, ny = ar->ny;
+#pragma omp parallel for schedule(static)
+  for (int j = 0; j < ny; j++)
+    for (int i = 0; i < nx; i++) {
+      int ixy = i + j * nx;
+      double dx = 1.0 / ar->m;
+      pp->x[ixy] = i * dx + ar->base_x;
+      pp->y[ixy] = j * dx + ar->base_y;
+      pp->rho[ixy] = c->rho0;
+      pp->ux[ixy] = c->U0[0];
+      pp->uy[ixy] = c->U0[1];
+      s->upx[a][ixy] = c->U0[0];
+      s->upy[a][ixy] = c->U0[1];
+      pp->forcex[ixy] = 0.0;
+      pp->forcey[ixy] = 0.0;
+      double X = pp->x[ixy], Y = pp->y[ixy];
+      if (is_solid(c, X, Y)) pp->solid[ixy] = MB_SOLID_SBB;
+      else if (Y == 0.0) pp->solid[ixy] = MB_FLUID;
+      else if (Y == c->LY - 1.0) pp->solid[ixy] = MB_FLUID;
+      else if (X == 0.0) pp->solid[ixy] = MB_FLUID;
+      else if (X == c->LX - 1.0) pp->solid[ixy] = MB_FLUID;
+      else if (i == 0 || j == 0 || i == nx - 1 || j == ny - 1) pp->solid[ixy] = MB_C_BOUNDARY;
+      else pp->solid[ixy] = MB_FLUID;
+      for (int k = 0; k < Q; k++) {
+        pp->F[k][ixy] = orc_feq(k, pp->rho[ixy], pp->ux[ixy], pp->uy[ixy]);
+        pp->f[k][ixy] = pp->F[k][ixy];
+      }
+    }
+}
+
+/* position of point ip on a line (the is==ie test of init_multi.h:14-15 and
+ * assit_multi.h:61-70) */
+static inline void line_point(const mb_p4 *p, int ip, int *i, int *j) {
+  if (p->xstart == p->xend) { *i = p->xstart; *j = p->ystart + ip; }
+  else { *i = p->xstart + ip; *j = p->ystart; }
+}
+
+/* init_Fstore (multi/init_multi.h:3-28) */
+static void init_fstore(orc_sim *s, int b) {
+  const mb_line *ln = &s->geo.Line_Inf_C[b];
+  const mb_area *af = &s->geo.Areas[ln->areaf_n];
+  o_d2q9 *pp = &s->pp[ln->areaf_n];
+  o_fstore *t = &s->t3[b];
+  for (int ip = 0; ip < t->N; ip++) {
+    int i, j;
+    line_point(&ln->line_F, ip, &i, &j);
+    int ixy = i + j * af->nx;
+    for (int k = 0; k < Q; k++) {
+      t->F[0][k][ip] = pp->F[k][ixy];
+      t->F[1][k][ip] = pp->F[k][ixy];
+      t->F[2][k][ip] = pp->F[k][ixy];
+    }
+  }
+}
+
+/* init_tri_A (multi/init_multi.h:30-51).  The reference writes l[ip+1]=0 from
+ * thread ip while thread ip+1 writes l[ip+1]=0.5; within a warp the later
+ * conditional store lands last.  The oracle takes that order (all unconditional
+ * stores first, then the conditional ones): natural end rows. */
+static void init_tri_a(orc_sim *s, int b) {
+  o_spline *sp = &s->s3[b];
+  const int N = s->geo.Line_Inf_C[b].Nc;
+  for (int ip = 0; ip < sp->N; ip++) { sp->l[ip] = 0.5; sp->m[ip] = 2.0; sp->u[ip] = 0.5; }
+  for (int ip = 0; ip < sp->N; ip++) {
+    if (ip == 0) sp->l[ip] = 0.0;
+    if (ip == N - 1) sp->u[ip] = 0.0;
+    if (ip == 0 || ip == N - 2) {
+      sp->u[ip] = 0.0;
+      if (ip + 1 < sp->N) sp->l[ip + 1] = 0.0;
+    }
+  }
+}
+
+/* ---------------------------------------------------------------------------
+ * Drag links: kernel_sum_N_drag + sum_N_drag + fdrag_store
+ * (lbm/force_block.h:2-127).  Enumeration is i-outer, j-inner, k.
+ * ------------------------------------------------------------------------- */
+static void drag_setup(orc_sim *s) {
+  const int a = s->drag_area;
+  const mb_area *ar = &s->geo.Areas[a];
+  const int *solid = s->pp[a].solid;
+  int n = 0;
+  for (int pass = 0; pass < 2; pass++) {
+    int ii = 0;
+    for (int i = 0; i < ar->nx; i++)
+      for (int j = 0; j < ar->ny; j++) {
+        int ixy = i + j * ar->nx;
+        if (solid[ixy] != MB_SOLID_SBB) continue;
+        for (int k = 0; k < Q; k++) {
+          int id = i - Ev[k], jd = j - Ev[k + Q];
+          if (id < 0 || id > ar->nx - 1 || jd < 0 || jd > ar->ny - 1) continue;
+          if (solid[id + jd * ar->nx] == MB_FLUID) {
+            if (pass == 1) { s->drag[3 * ii] = i; s->drag[3 * ii + 1] = j; s->drag[3 * ii + 2] = k; }
+            ii++;
+          }
+        }
+      }
+    if (pass == 0) { n = ii; s->n_drag = n; s->drag = (int *)calloc(3 * (size_t)(n ? n : 1), sizeof(int)); }
+  }
+}
+
+int orc_init(orc_sim *s) {
+  const mb_layout *L = &s->geo.layout;
+  for (int a = 0; a < L->number_area; a++) init_general(s, a);
+  drag_setup(s);
+  for (int b = 0; b < L->number_line; b++) { init_fstore(s, b); init_tri_a(s, b); }
+  return MB_OK;
+}
+
+/* ---------------------------------------------------------------------------
+ * Block step: evolution_area_stb1/2/3 (multi/FH/evolution_block.h:3-126)
+ * ------------------------------------------------------------------------- */
+void orc_block_step(orc_sim *s, int a) {
+  const mb_area area = s->geo.Areas[a];
+  const mb_config *c = &s->geo.config;
+  o_d2q9 *pp = &s->pp[a];
+  const int nx = area.nx, ny = area.ny;
+  /* stb1: pull stream; out-of-block neighbours keep the old f (:23-24) */
+#pragma omp parallel for schedule(static)
+  for (int j = 0; j < ny; j++)
+    for (int i = 0; i < nx; i++) {
+      int ixy = i + j * nx;
+      if (pp->solid[ixy] == MB_FLUID || pp->solid[ixy] == MB_SOLID_SBB) {
+        for (int k = 0; k < Q; k++) {
+          int id = i - Ev[k], jd = j - Ev[k + Q];
+          if (id < 0 || id > nx - 1 || jd < 0 || jd > ny - 1) continue;
+          pp->f[k][ixy] = pp->F[k][id + jd * nx];
+        }
+      }
+    }
+  /* stb2: equilibrium on block-edge FLUID cells (:47-57), else Macros (:60-70) */
+#pragma omp parallel for schedule(static)
+  for (int j = 0; j < ny; j++)
+    for (int i = 0; i < nx; i++) {
+      int ixy = i + j * nx;
+      if (pp->solid[ixy] != MB_FLUID) continue;
+      if (i == 0 || i == nx - 1 || j == 0 || j == ny - 1) {
+        pp->rho[ixy] = c->rho0;
+        pp->ux[ixy] = c->U0[0];
+        pp->uy[ixy] = c->U0[1];
+        for (int k = 0; k < Q; k++) pp->f[k][ixy] = orc_feq(k, c->rho0, c->U0[0], c->U0[1]);
+      } else {
+        double ft[Q], rh, ux, uy;
+        for (int k = 0; k < Q; k++) ft[k] = pp->f[k][ixy];
+        macros(&rh, &ux, &uy, ft);
+        pp->rho[ixy] = rh;
+        pp->ux[ixy] = ux;
+        pp->uy[ixy] = uy;
+      }
+    }
+  /* stb3: BGK with the (zero) forcing term (:90-111), on-node bounce-back (:113-117) */
+#pragma omp parallel for schedule(static)
+  for (int j = 0; j < ny; j++)
+    for (int i = 0; i < nx; i++) {
+      int ixy = i + j * nx;
+      double dt = 1.0 / area.m;
+      double ft[Q];
+      for (int k = 0; k < Q; k++) ft[k] = pp->f[k][ixy];
+      if (pp->solid[ixy] == MB_FLUID) {
+        double rh = pp->rho[ixy], ux = pp->ux[ixy], uy = pp->uy[ixy];
+        double fx = pp->forcex[ixy], fy = pp->forcey[ixy];
+        for (int k = 0; k < Q; k++) {
+          double vx = 3.0 * (Ev[k] - ux) + 9.0 * (Ev[k] * ux + Ev[k + Q] * uy) * Ev[k];
+          double vy = 3.0 * (Ev[k + Q] - uy) + 9.0 * (Ev[k] * ux + Ev[k + Q] * uy) * Ev[k + Q];
+          double Fk = (1.0 - 0.5 * area.rv_tau) * Wt[k] * (vx * fx + vy * fy);
+          pp->F[k][ixy] = ft[k] - (ft[k] - orc_feq(k, rh, ux, uy)) * area.rv_tau + dt * Fk;
+        }
+      } else if (pp->solid[ixy] == MB_SOLID_SBB) {
+        for (int k = 0; k < Q; k++) pp->F[k][ixy] = ft[Opp[k]];
+      }
+    }
+}
+
+/* ---------------------------------------------------------------------------
+ * Interface kernels (multi/FH/assit_multi.h)
+ * ------------------------------------------------------------------------- */
+/* c_c_boundary_transfer (:2-46): source line_C in areac_n, target line_F in areaf_n */
+void orc_c_c(orc_sim *s, int c) {
+  const mb_line *ln = &s->geo.Line_Inf_CC[c];
+  const int nx1 = s->geo.Areas[ln->areac_n].nx, nx2 = s->geo.Areas[ln->areaf_n].nx;
+  o_d2q9 *p1 = &s->pp[ln->areac_n], *p2 = &s->pp[ln->areaf_n];
+  const int xs1 = ln->line_C.xstart, xe1 = ln->line_C.xend, ys1 = ln->line_C.ystart, ye1 = ln->line_C.yend;
+  const int xs2 = ln->line_F.xstart, ys2 = ln->line_F.ystart;
+  for (int ip = 0; ip < ln->Nc; ip++) {
+    int i1 = 0, j1 = 0, i2 = 0, j2 = 0;
+    if (xs1 == xe1) { i1 = xs1; j1 = ys1 + ip; i2 = xs2; j2 = ys2 + ip; }
+    if (ys1 == ye1) { i1 = xs1 + ip; j1 = ys1; i2 = xs2 + ip; j2 = ys2; }
+    int ixy1 = i1 + j1 * nx1, ixy2 = i2 + j2 * nx2;
+    p2->rho[ixy2] = p1->rho[ixy1];
+    p2->ux[ixy2] = p1->ux[ixy1];
+    p2->uy[ixy2] = p1->uy[ixy1];
+    for (int k = 0; k < Q; k++) p2->F[k][ixy2] = p1->F[k][ixy1];
+  }
+}
+
+/* init_Spline3 (:48-116).  The reference reads neighbour points that other
+ * CTAs write in the same launch (:100-107) when Nc > 256; the oracle gathers
+ * the whole line first (the result of the reference when Nc <= 256). */
+static void init_spline3(orc_sim *s, int b) {
+  const mb_line *ln = &s->geo.Line_Inf_C[b];
+  const int nx = s->geo.Areas[ln->areac_n].nx;
+  o_d2q9 *pp = &s->pp[ln->areac_n];
+  o_spline *sp = &s->s3[b];
+  const int N = sp->N;
+  for (int ip = 0; ip < N; ip++) {
+    int i, j;
+    line_point(&ln->line_C, ip, &i, &j);
+    int ixy = i + j * nx;
+    sp->rho[ip] = pp->rho[ixy];
+    sp->ux[ip] = pp->ux[ixy];
+    sp->uy[ip] = pp->uy[ixy];
+    for (int k = 0; k < Q; k++) sp->F[k][ip] = pp->F[k][ixy];
+  }
+  double *V = sp->Varibs_M;
+  for (int ip = 0; ip < N; ip++) {
+    if (ip == 0 || ip == N - 1) {
+      V[ip] = 0.0;
+      V[N + ip] = 0.0;
+      V[2 * N + ip] = 0.0;
+      for (int k = 0; k < Q; k++) V[(3 + k) * N + ip] = 0.0;
+    } else {
+      V[ip] = (6.0 * sp->rho[ip] - 3.0 * sp->rho[ip - 1] - 3.0 * sp->rho[ip + 1]);
+      V[N + ip] = (6.0 * sp->ux[ip] - 3.0 * sp->ux[ip - 1] - 3.0 * sp->ux[ip + 1]);
+      V[2 * N + ip] = (6.0 * sp->uy[ip] - 3.0 * sp->uy[ip - 1] - 3.0 * sp->uy[ip + 1]);
+      for (int k = 0; k < Q; k++)
+        V[(3 + k) * N + ip] = (6.0 * sp->F[k][ip] - 3.0 * sp->F[k][ip - 1] - 3.0 * sp->F[k][ip + 1]);
+    }
+  }
+}
+
+/* cusparseDgtsv2 (assit_multi.h:194-205) is NVIDIA library code; the oracle
+ * solves the same diagonally dominant system (|2| > |0.5|+|0.5|) by the
+ * Thomas algorithm, which needs no pivoting.  B is column-major, ldb >= n. */
+void orc_gtsv(int n, int nrhs, const double *l, const double *m, const double *u, double *B, int ldb) {
+  double *cp = (double *)malloc(sizeof(double) * (n > 0 ? n : 1));
+  for (int r = 0; r < nrhs; r++) {
+    double *d = B + (size_t)r * ldb;
+    cp[0] = u[0] / m[0];
+    d[0] = d[0] / m[0];
+    for (int i = 1; i < n; i++) {
+      double den = m[i] - l[i] * cp[i - 1];
+      cp[i] = u[i] / den;
+      d[i] = (d[i] - l[i] * d[i - 1]) / den;
+    }
+    for (int i = n - 2; i >= 0; i--) d[i] = d[i] - cp[i] * d[i + 1];
+  }
+  free(cp);
+}
+
+/* Spline3_S (:118-134) including its 0.1666667 constant */
+double orc_spline3_s(double xx, double x_1, double h, double fi_1, double fi, double mi_1, double mi) {
+  double x, a, b, c, d;
+  x = x_1 + h;
+  a = mi_1 * (x - xx) * (x - xx) * (x - xx) * 0.1666667;
+  b = mi * (xx - x_1) * (xx - x_1) * (xx - x_1) * 0.1666667;
+  c = (fi_1 - mi_1 * h * h * 0.1666667) * (x - xx);
+  d = (fi - mi * h * h * 0.1666667) * (xx - x_1);
+  return (a + b + c + d);
+}
+
+/* calculate_Spline3_gpu (:136-185): writes fine-edge rho/ux/uy and slot marker[0] */
+static void calculate_spline3(orc_sim *s, int b) {
+  const mb_line *ln = &s->geo.Line_Inf_C[b];
+  const mb_area *ac = &s->geo.Areas[ln->areac_n], *af = &s->geo.Areas[ln->areaf_n];
+  o_d2q9 *pp = &s->pp[ln->areaf_n];
+  o_spline *sp = &s->s3[b];
+  double **lt3 = s->t3[b].F[s->t3[b].marker[0]];
+  const int N = sp->N;
+  const double *V = sp->Varibs_M;
+  const int r = af->m / ac->m;
+  for (int ip = 0; ip < ln->Nf; ip++) {
+    int i, j;
+    line_point(&ln->line_F, ip, &i, &j);
+    int ixy = i + j * af->nx;
+    double xx = (double)ip / (double)r;
+    int I;
+    if (ceil(xx) == 0) I = (int)(ceil(xx) + 1.0);
+    else I = (int)(ceil(xx));
+    double rho_t = orc_spline3_s(xx, (I - 1.0), 1.0, sp->rho[I - 1], sp->rho[I], V[I - 1], V[I]);
+    double ux_t = orc_spline3_s(xx, (I - 1.0), 1.0, sp->ux[I - 1], sp->ux[I], V[N + I - 1], V[N + I]);
+    double uy_t = orc_spline3_s(xx, (I - 1.0), 1.0, sp->uy[I - 1], sp->uy[I], V[2 * N + I - 1], V[2 * N + I]);
+    pp->rho[ixy] = rho_t;
+    pp->ux[ixy] = ux_t;
+    pp->uy[ixy] = uy_t;
+    double para = (af->tau - 1.0) / (r * (ac->tau - 1.0));
+    for (int k = 0; k < Q; k++) {
+      double ft = orc_spline3_s(xx, (I - 1.0), 1.0, sp->F[k][I - 1], sp->F[k][I], V[(3 + k) * N + I - 1],
+                                V[(3 + k) * N + I]);
+      double fe = orc_feq(k, rho_t, ux_t, uy_t);
+      lt3[k][ip] = fe + para * (ft - fe);
+    }
+  }
+}
+
+/* space_interpolation_Spline3 (:187-211) */
+void orc_space_interpolation(orc_sim *s, int b) {
+  o_spline *sp = &s->s3[b];
+  init_spline3(s, b);
+  orc_gtsv(sp->N, 12, sp->l, sp->m, sp->u, sp->Varibs_M, sp->N);
+  calculate_spline3(s, b);
+}
+
+/* temporal_interpolation (:213-247): F = a*F(t-1) - b*F(t) + c*F(t+1) on the fine edge */
+void orc_temporal(orc_sim *s, int b, double xm) {
+  const mb_line *ln = &s->geo.Line_Inf_C[b];
+  const int nx = s->geo.Areas[ln->areaf_n].nx;
+  o_d2q9 *pp = &s->pp[ln->areaf_n];
+  o_fstore *t = &s->t3[b];
+  double **Ft_1 = t->F[t->marker[0]], **Ft = t->F[t->marker[1]], **Ft1 = t->F[t->marker[2]];
+  double a = 0.5 * (xm - 1.0) * xm;
+  double bb = (xm - 1.0) * (xm + 1.0);
+  double c = 0.5 * xm * (xm + 1.0);
+  for (int ip = 0; ip < t->N; ip++) {
+    int i, j;
+    line_point(&ln->line_F, ip, &i, &j);
+    int ixy = i + j * nx;
+    for (int k = 0; k < Q; k++) pp->F[k][ixy] = a * Ft_1[k][ip] - bb * Ft[k][ip] + c * Ft1[k][ip];
+  }
+}
+
+/* c_f_boundary_transfer (:249-271): fine edge F <- slot marker[2] */
+void orc_c_f(orc_sim *s, int b) {
+  const mb_line *ln = &s->geo.Line_Inf_C[b];
+  const int nx = s->geo.Areas[ln->areaf_n].nx;
+  o_d2q9 *pp = &s->pp[ln->areaf_n];
+  o_fstore *t = &s->t3[b];
+  double **Ft = t->F[t->marker[2]];
+  for (int ip = 0; ip < t->N; ip++) {
+    int i, j;
+    line_point(&ln->line_F, ip, &i, &j);
+    int ixy = i + j * nx;
+    for (int k = 0; k < Q; k++) pp->F[k][ixy] = Ft[k][ip];
+  }
+}
+
+/* f_c_boundary_transfer (:273-314), on Line_Inf_F */
+void orc_f_c(orc_sim *s, int b) {
+  const mb_line *ln = &s->geo.Line_Inf_F[b];
+  const mb_area *ac = &s->geo.Areas[ln->areac_n], *af = &s->geo.Areas[ln->areaf_n];
+  o_d2q9 *pc = &s->pp[ln->areac_n], *pf = &s->pp[ln->areaf_n];
+  const int r = af->m / ac->m;
+  for (int ip = 0; ip < ln->Nc; ip++) {
+    int ic, jc, i_f, j_f;
+    if (ln->line_C.xstart == ln->line_C.xend) {
+      ic = ln->line_C.xstart; jc = ln->line_C.ystart + ip;
+      i_f = ln->line_F.xstart; j_f = ln->line_F.ystart + r * ip;
+    } else {
+      ic = ln->line_C.xstart + ip; jc = ln->line_C.ystart;
+      i_f = ln->line_F.xstart + r * ip; j_f = ln->line_F.ystart;
+    }
+    int ixyc = ic + jc * ac->nx, ixyf = i_f + j_f * af->nx;
+    pc->rho[ixyc] = pf->rho[ixyf];
+    pc->ux[ixyc] = pf->ux[ixyf];
+    pc->uy[ixyc] = pf->uy[ixyf];
+    double para = r * (ac->tau - 1.0) / (af->tau - 1.0);
+    for (int k = 0; k < Q; k++) {
+      double ft = pf->F[k][ixyf];
+      double fe = orc_feq(k, pf->rho[ixyf], pf->ux[ixyf], pf->uy[ixyf]);
+      pc->F[k][ixyc] = fe + para * (ft - fe);
+    }
+  }
+}
+
+/* ring rotation (evolution.h:41-46) */
+void orc_rotate_markers(orc_sim *s, int b) {
+  for (int p = 0; p < 3; p++) {
+    int bb = s->t3[b].marker[p] - 1;
+    s->t3[b].marker[p] = (bb == -1) ? 2 : bb;
+  }
+}
+
+/* ---------------------------------------------------------------------------
+ * Level scheduler: evolution (evolution.h:2-65)
+ * ------------------------------------------------------------------------- */
+static void evolution(orc_sim *s, int level) {
+  const mb_layout *L = &s->geo.layout;
+  /* The reference evaluates mi[LEVEL] (one past the table) before its
+   * level == LEVEL return (evolution.h:4-8); either way that call does nothing. */
+  if (level == L->LEVEL) return;
+  for (int i = 0; i < L->mi[level]; i++) {
+    if (!(level == 0 || i == 0)) {
+      for (int b = L->LTCFFCP[level]; b < L->LTCFFCP[level + 1]; b++)
+        orc_temporal(s, b, (1.0 * i / L->mi[level]));
+    }
+    for (int a = L->ASP[level]; a < L->ASP[level + 1]; a++) orc_block_step(s, a);
+    if (L->number_line2 != 0)
+      for (int c = L->LCCP[level]; c < L->LCCP[level + 1]; c++) orc_c_c(s, c);
+    if (level != L->LEVEL - 1) {
+      for (int b = L->LS3CFFCP[level]; b < L->LS3CFFCP[level + 1]; b++) {
+        orc_space_interpolation(s, b);
+        orc_rotate_markers(s, b);
+      }
+    }
+    evolution(s, level + 1);
+    if (level != 0 && i == L->mi[level] - 1) {
+      for (int b = L->LTCFFCP[level]; b < L->LTCFFCP[level + 1]; b++) {
+        orc_c_f(s, b);
+        orc_f_c(s, b);
+      }
+    }
+  }
+}
+
+void orc_evolution(orc_sim *s, int n) {
+  (void)n;
+  evolution(s, 0);
+}
+
+/* ---------------------------------------------------------------------------
+ * Diagnostics
+ * ------------------------------------------------------------------------- */
+int orc_drag_link_count(orc_sim *s) { return s->n_drag; }
+void orc_drag_links(orc_sim *s, int *ijk) { memcpy(ijk, s->drag, sizeof(int) * 3 * (size_t)s->n_drag); }
+
+/* kernel_sum_Force + getDrag_block (force_block.h:129-216): per-CTA shared-memory
+ * tree over 256 links, then an in-order host sum of the CTA partials. */
+void orc_drag(orc_sim *s, double force[2], double *cd, double *cl) {
+  const int a = s->drag_area;
+  const mb_area *ar = &s->geo.Areas[a];
+  const o_d2q9 *pp = &s->pp[a];
+  const int N = s->n_drag;
+  const int Bx = (int)ceil(N / (double)BLOCK1D);
+  double fxs[BLOCK1D], fys[BLOCK1D];
+  force[0] = 0.0;
+  force[1] = 0.0;
+  for (int bx = 0; bx < Bx; bx++) {
+    for (int tx = 0; tx < BLOCK1D; tx++) {
+      int ip = bx * BLOCK1D + tx;
+      fxs[tx] = 0.0;
+      fys[tx] = 0.0;
+      if (ip < N) {
+        int i = s->drag[3 * ip], j = s->drag[3 * ip + 1], k = s->drag[3 * ip + 2];
+        int id = i - Ev[k], jd = j - Ev[Q + k], kd = Opp[k];
+        int ixy = i + j * ar->nx, ixyd = id + jd * ar->nx;
+        fxs[tx] = (pp->f[k][ixy] * Ev[k] - pp->f[kd][ixyd] * Ev[kd]);
+        fys[tx] = (pp->f[k][ixy] * Ev[k + Q] - pp->f[kd][ixyd] * Ev[kd + Q]);
+      }
+    }
+    for (int st = BLOCK1D / 2; st > 0; st >>= 1)
+      for (int tx = 0; tx < st; tx++) { fxs[tx] += fxs[tx + st]; fys[tx] += fys[tx + st]; }
+    force[0] += fxs[0];
+    force[1] += fys[0];
+  }
+  const mb_config *c = &s->geo.config;
+  double den = c->rho0 * s->U0_2 * s->U0_2 * ar->m * c->R;
+  if (cd) *cd = force[0] / den;
+  if (cl) *cl = force[1] / den;
+}
+
+/* error_L2_area + error_L2 (lbm/error_L2.h:3-91): per 16x16 CTA tree sums, an
+ * in-order host sum per block, weights 1/m, u_prev <- u. */
+double orc_error_L2(orc_sim *s) {
+  const mb_layout *L = &s->geo.layout;
+  double uvp2_all = 0.0, uv2_all = 0.0;
+  for (int a = 0; a < L->number_area; a++) {
+    const mb_area *ar = &s->geo.Areas[a];
+    const int nx = ar->nx, ny = ar->ny;
+    const int Bx = (int)ceil(nx / (double)BLOCKX), By = (int)ceil(ny / (double)BLOCKY);
+    const int NB = Bx * By;
+    double *pv = (double *)malloc(sizeof(double) * 2 * (size_t)NB);
+    const double *ux = s->pp[a].ux, *uy = s->pp[a].uy;
+    double *upx = s->upx[a], *upy = s->upy[a];
+#pragma omp parallel for schedule(static)
+    for (int bip = 0; bip < NB; bip++) {
+      int bx = bip % Bx, by = bip / Bx;
+      double s1[BLOCKX * BLOCKY], s2[BLOCKX * BLOCKY];
+      for (int tip = 0; tip < BLOCKX * BLOCKY; tip++) {
+        int tx = tip % BLOCKX, ty = tip / BLOCKX;
+        int i = bx * BLOCKX + tx, j = by * BLOCKY + ty;
+        s1[tip] = 0.0;
+        s2[tip] = 0.0;
+        if (i <= nx - 1 && j <= ny - 1) {
+          int ixy = i + j * nx;
+          double uxt = ux[ixy], upxt = upx[ixy], uyt = uy[ixy], upyt = upy[ixy];
+          s1[tip] = (uxt - upxt) * (uxt - upxt) + (uyt - upyt) * (uyt - upyt);
+          s2[tip] = uxt * uxt + uyt * uyt;
+          upx[ixy] = uxt;
+          upy[ixy] = uyt;
+        }
+      }
+      for (int st = BLOCKX * BLOCKY / 2; st > 0; st >>= 1)
+        for (int t = 0; t < st; t++) { s1[t] += s1[t + st]; s2[t] += s2[t + st]; }
+      pv[2 * bip] = s1[0];
+      pv[2 * bip + 1] = s2[0];
+    }
+    double uvp2_area = 0.0, uv2_area = 0.0;
+    for (int i = 0; i < NB; i++) { uvp2_area += pv[2 * i]; uv2_area += pv[2 * i + 1]; }
+    free(pv);
+    uvp2_all += uvp2_area / ar->m;
+    uv2_all += uv2_area / ar->m;
+  }
+  return sqrt(uvp2_all) / sqrt(uv2_all);
+}
+
+/* ---------------------------------------------------------------------------
+ * Field access
+ * ------------------------------------------------------------------------- */
+void orc_get_fields(orc_sim *s, int a, double *rho, double *ux, double *uy, double *F, double *f, int *solid) {
+  const size_t N = (size_t)s->geo.Areas[a].nx * s->geo.Areas[a].ny;
+  const o_d2q9 *p = &s->pp[a];
+  if (rho) memcpy(rho, p->rho, N * sizeof(double));
+  if (ux) memcpy(ux, p->ux, N * sizeof(double));
+  if (uy) memcpy(uy, p->uy, N * sizeof(double));
+  if (solid) memcpy(solid, p->solid, N * sizeof(int));
+  for (int k = 0; k < Q; k++) {
+    if (F) memcpy(F + k * N, p->F[k], N * sizeof(double));
+    if (f) memcpy(f + k * N, p->f[k], N * sizeof(double));
+  }
+}
+
+void orc_set_fields(orc_sim *s, int a, const double *rho, const double *ux, const double *uy, const double *F,
+                    const double *f) {
+  const size_t N = (size_t)s->geo.Areas[a].nx * s->geo.Areas[a].ny;
+  o_d2q9 *p = &s->pp[a];
+  if (rho) memcpy(p->rho, rho, N * sizeof(double));
+  if (ux) memcpy(p->ux, ux, N * sizeof(double));
+  if (uy) memcpy(p->uy, uy, N * sizeof(double));
+  for (int k = 0; k < Q; k++) {
+    if (F) memcpy(p->F[k], F + k * N, N * sizeof(double));
+    if (f) memcpy(p->f[k], f + k * N, N * sizeof(double));
+  }
+}
+
+void orc_get_slots(orc_sim *s, int b, double *out) {
+  const int N = s->t3[b].N;
+  for (int t = 0; t < 3; t++)
+    for (int k = 0; k < Q; k++) memcpy(out + ((size_t)t * Q + k) * N, s->t3[b].F[t][k], N * sizeof(double));
+}
+
+void orc_get_markers(orc_sim *s, int b, int *m3) {
+  for (int p = 0; p < 3; p++) m3[p] = s->t3[b].marker[p];
+}
+
+/* output (output/output.h:2-38) */
+int orc_write_tecplot(orc_sim *s, const char *path) {
+  FILE *fp = fopen(path, "w");
+  if (!fp) return MB_ERR_INVALID;
+  fprintf(fp, "Title= \"LBM 2D\"\n");
+  fprintf(fp, "VARIABLES= \"X\",\"Y\",\"solid\",\"rho\",\"U\",\"V\",\n");
+  for (int a = 0; a < s->geo.layout.number_area; a++) {
+    const mb_area *ar = &s->geo.Areas[a];
+    const o_d2q9 *p = &s->pp[a];
+    fprintf(fp, "ZONE T= \"zone_level%d\",I= %d,J= %d,F=POINT\n", a, ar->nx, ar->ny);
+    for (int j = 0; j < ar->ny; j++)
+      for (int i = 0; i < ar->nx; i++) {
+        int ixy = i + j * ar->nx;
+        fprintf(fp, "%g\t%g\t%d\t%g\t%g\t%g\n", p->x[ixy], p->y[ixy], p->solid[ixy], p->rho[ixy], p->ux[ixy],
+                p->uy[ixy]);
+      }
+  }
+  fclose(fp);
+  return MB_OK;
+}

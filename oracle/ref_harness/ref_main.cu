@@ -1,0 +1,192 @@
+// ref_main.cu - driver that runs the reference's own CUDA code, unmodified.
+//
+// TEST INFRASTRUCTURE ONLY.  Compiled by oracle/ref_harness/make_ref.py from
+// the reference sources where they lie (zhangya9741/Multi-block-LBM-GPU, read
+// through -I), together with a generated header that supplies what
+// parameters.h and geo/geometry.h supply in the reference (physical constants
+// and the block tables).  The kernels, geo_init, evolution, error_L2 and
+// getDrag_block are the reference's; this file only replaces main()
+// (Multi-block-LBM.cu:19-230): it allocates and initialises the same way,
+// then either dumps full-precision results (golden mode) or times the step
+// loop with CUDA events (bench mode).
+#include "geo/init_geo.h"
+
+#include "lbm/assit_func.h"
+#include "lbm/error_L2.h"
+#include "lbm/force_block.h"
+#include "lbm/init_block.h"
+
+#include "multi/FH/assit_multi.h"
+#include "multi/FH/evolution_block.h"
+#include "multi/init_multi.h"
+
+#include "output/output.h"
+
+#include "evolution.h"
+
+#include <vector>
+
+static void put(FILE *fp, const void *p, size_t n) { fwrite(p, 1, n, fp); }
+
+int main(int argc, char **argv) {
+  if (argc < 3) {
+    fprintf(stderr, "usage: %s golden|bench nsteps [warmup]\n", argv[0]);
+    return 2;
+  }
+  const bool golden = strcmp(argv[1], "golden") == 0;
+  const int nsteps = atoi(argv[2]);
+  const int warm = argc > 3 ? atoi(argv[3]) : 0;
+
+  geo_init();
+
+  // allocation, as Multi-block-LBM.cu:26-113
+  D2Q9 Vh[number_area], Vd[number_area];
+  for (int a = 0; a < number_area; a++) {
+    size_t N = (size_t)Areas[a].nx * Areas[a].ny;
+    Vh[a].solid = (Lbi *)malloc(N * sizeof(Lbi));
+    cudaMalloc((void **)&Vd[a].solid, N * sizeof(Lbi));
+    Lbd **ph = &Vh[a].x, **pd = &Vd[a].x;
+    for (int b = 0; b < 1 + 3 * DMS + 2 * Q; b++) {
+      ph[b] = (Lbd *)malloc(N * sizeof(Lbd));
+      cudaMalloc((void **)&pd[b], N * sizeof(Lbd));
+    }
+  }
+  Ff_Store T3[number_line > 0 ? number_line : 1];
+  for (int a = 0; a < number_line; a++) {
+    T3[a].marker[0] = 2;
+    T3[a].marker[1] = 1;
+    T3[a].marker[2] = 0;
+    T3[a].N = Line_Inf_C[a].Nf;
+    F_k3 *ft = &T3[a].f_t1;
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < Q; j++) cudaMalloc((void **)&ft[i].F[j], T3[a].N * sizeof(Lbd));
+  }
+  cusparseHandle_t handle;
+  cusparseCreate(&handle);
+  FM_spline3 S3[number_line > 0 ? number_line : 1];
+  for (int a = 0; a < number_line; a++) {
+    S3[a].N = Line_Inf_C[a].Nc;
+    cudaMalloc((void **)&S3[a].l, S3[a].N * sizeof(Lbd));
+    cudaMalloc((void **)&S3[a].m, S3[a].N * sizeof(Lbd));
+    cudaMalloc((void **)&S3[a].u, S3[a].N * sizeof(Lbd));
+    cudaMalloc((void **)&S3[a].Varibs_M, 12 * S3[a].N * sizeof(Lbd));
+    Lbd **fM = &S3[a].rho;
+    for (int i = 0; i < 12; i++) cudaMalloc((void **)&fM[i], S3[a].N * sizeof(Lbd));
+  }
+  dim3 block(_BLOCKX, _BLOCKY, 1);
+  dim3 grid[number_area];
+  for (int i = 0; i < number_area; i++)
+    grid[i] = dim3(int(ceil(Areas[i].nx / double(_BLOCKX))), int(ceil(Areas[i].ny / double(_BLOCKY))), 1);
+  Lbd *upsx[number_area], *upsy[number_area];
+  Lbd *h_uvp2[number_area], *d_uvp2[number_area], *h_uv2[number_area], *d_uv2[number_area];
+  for (int a = 0; a < number_area; a++) {
+    size_t N = (size_t)Areas[a].nx * Areas[a].ny;
+    cudaMalloc((void **)&upsx[a], N * sizeof(Lbd));
+    cudaMalloc((void **)&upsy[a], N * sizeof(Lbd));
+    size_t sb = (size_t)grid[a].x * grid[a].y * sizeof(Lbd);
+    h_uvp2[a] = (Lbd *)malloc(sb);
+    cudaMalloc((void **)&d_uvp2[a], sb);
+    h_uv2[a] = (Lbd *)malloc(sb);
+    cudaMalloc((void **)&d_uv2[a], sb);
+  }
+
+  // initialisation, as Multi-block-LBM.cu:116-140
+  for (int a = 0; a < number_area; a++) init_General<<<grid[a], block>>>(Areas[a], Vd[a], upsx[a], upsy[a]);
+  Lbd Force[2];
+  const int last = number_area - 1;
+  Lbi N_drag = sum_N_drag(block, grid[last], Areas[last], Vd[last]);
+  Int3 *d_drag;
+  cudaMalloc((void **)&d_drag, (N_drag > 0 ? N_drag : 1) * sizeof(Int3));
+  fdrag_store(Areas[last], Vh[last], d_drag, Vd[last], N_drag);
+  for (int a = 0; a < number_line; a++) {
+    init_Fstore<<<int(ceil(T3[a].N / double(_BLOCK_1D))), _BLOCK_1D>>>(Areas[Line_Inf_C[a].areaf_n],
+                                                                     Vd[Line_Inf_C[a].areaf_n], Line_Inf_C[a], T3[a]);
+    init_tri_A<<<int(ceil(S3[a].N / double(_BLOCK_1D))), _BLOCK_1D>>>(Areas[Line_Inf_C[a].areac_n],
+                                                                     Vd[Line_Inf_C[a].areac_n], Line_Inf_C[a], S3[a]);
+  }
+  cudaDeviceSynchronize();
+
+  if (golden) {
+    FILE *fg = fopen("geometry.bin", "wb");
+    put(fg, AreaDefine, sizeof(AreaDefine));
+    put(fg, Areas, sizeof(Areas));
+    put(fg, Line_Inf_C, sizeof(Line_Inf_C));
+    put(fg, Line_Inf_F, sizeof(Line_Inf_F));
+    put(fg, Line_Inf_CC, sizeof(Line_Inf_CC));
+    fclose(fg);
+    std::vector<double> drag(2 * (size_t)nsteps);
+    for (int n = 0; n < nsteps; n++) {
+      evolution(n, ASP, LS3CFFCP, LTCFFCP, LCCP, 0, block, grid, Areas, Vh, Vd, Line_Inf_C, Line_Inf_F, Line_Inf_CC,
+                T3, S3, handle);
+      error_L2(n, number_area, block, grid, Areas, Vd, upsx, upsy, h_uvp2, d_uvp2, h_uv2, d_uv2);
+      getDrag_block(n, d_drag, Areas[last], Vd[last], Force, N_drag);
+      drag[2 * n] = Force[0];
+      drag[2 * n + 1] = Force[1];
+    }
+    cudaDeviceSynchronize();
+    FILE *fd = fopen("drag.bin", "wb");
+    put(fd, drag.data(), drag.size() * sizeof(double));
+    fclose(fd);
+    FILE *ff = fopen("fields.bin", "wb");
+    for (int a = 0; a < number_area; a++) {
+      size_t N = (size_t)Areas[a].nx * Areas[a].ny;
+      std::vector<double> h(N);
+      std::vector<int> s(N);
+      cudaMemcpy(s.data(), Vd[a].solid, N * sizeof(int), cudaMemcpyDeviceToHost);
+      put(ff, s.data(), N * sizeof(int));
+      Lbd **pd = &Vd[a].x;  // x, y, rho, ux, uy, forcex, forcey, f[9], F[9]
+      for (int b = 0; b < 1 + 3 * DMS + 2 * Q; b++) {
+        cudaMemcpy(h.data(), pd[b], N * sizeof(double), cudaMemcpyDeviceToHost);
+        put(ff, h.data(), N * sizeof(double));
+      }
+      cudaMemcpy(h.data(), upsx[a], N * sizeof(double), cudaMemcpyDeviceToHost);
+      put(ff, h.data(), N * sizeof(double));
+      cudaMemcpy(h.data(), upsy[a], N * sizeof(double), cudaMemcpyDeviceToHost);
+      put(ff, h.data(), N * sizeof(double));
+    }
+    for (int b = 0; b < number_line; b++) {
+      put(ff, T3[b].marker, sizeof(T3[b].marker));
+      F_k3 *ft = &T3[b].f_t1;
+      std::vector<double> h(T3[b].N);
+      for (int i = 0; i < 3; i++)
+        for (int k = 0; k < Q; k++) {
+          cudaMemcpy(h.data(), ft[i].F[k], T3[b].N * sizeof(double), cudaMemcpyDeviceToHost);
+          put(ff, h.data(), T3[b].N * sizeof(double));
+        }
+    }
+    fclose(ff);
+    output(nsteps, Areas, Vh, Vd);
+    printf("{\"n_drag\": %d, \"status\": \"%s\"}\n", N_drag, cudaGetErrorString(cudaGetLastError()));
+  } else {
+    for (int n = 0; n < warm; n++)
+      evolution(n, ASP, LS3CFFCP, LTCFFCP, LCCP, 0, block, grid, Areas, Vh, Vd, Line_Inf_C, Line_Inf_F, Line_Inf_CC,
+                T3, S3, handle);
+    cudaDeviceSynchronize();
+    cudaEvent_t e0, e1, e2;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventCreate(&e2);
+    cudaEventRecord(e0, 0);
+    for (int n = 0; n < nsteps; n++)
+      evolution(warm + n, ASP, LS3CFFCP, LTCFFCP, LCCP, 0, block, grid, Areas, Vh, Vd, Line_Inf_C, Line_Inf_F,
+                Line_Inf_CC, T3, S3, handle);
+    cudaEventRecord(e1, 0);
+    // the shipped main loop: step, error_L2 and getDrag_block (with their file appends) every step
+    for (int n = 0; n < nsteps; n++) {
+      evolution(warm + nsteps + n, ASP, LS3CFFCP, LTCFFCP, LCCP, 0, block, grid, Areas, Vh, Vd, Line_Inf_C,
+                Line_Inf_F, Line_Inf_CC, T3, S3, handle);
+      error_L2(n, number_area, block, grid, Areas, Vd, upsx, upsy, h_uvp2, d_uvp2, h_uv2, d_uv2);
+      getDrag_block(n, d_drag, Areas[last], Vd[last], Force, N_drag);
+    }
+    cudaEventRecord(e2, 0);
+    cudaEventSynchronize(e2);
+    float t1 = 0, t2 = 0;
+    cudaEventElapsedTime(&t1, e0, e1);
+    cudaEventElapsedTime(&t2, e1, e2);
+    printf("{\"ms_per_step\": %.6f, \"ms_per_step_diag\": %.6f, \"steps\": %d, \"warmup\": %d, \"Fx\": %.17g, "
+           "\"status\": \"%s\"}\n",
+           t1 / nsteps, t2 / nsteps, nsteps, warm, Force[0], cudaGetErrorString(cudaGetLastError()));
+  }
+  cusparseDestroy(handle);
+  return 0;
+}
