@@ -1,0 +1,322 @@
+"""Benchmark of the multi-block D2Q9 BGK step (MLUPS, % HBM roofline).
+
+Workload: the 3-level cylinder at Re=100, 4096x1024 coarse cells, level-1 box
+[768,1280]x[384,640], level-2 box [896,1152]x[448,576], D=32 at (960,512),
+U0=0.04 (6,986,527 cell updates per coarse step), FP32 storage of f - w.
+A step is one coarse time step of evolution() over all levels.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs under torchrun, one process per GPU, each GPU advancing its own
+independent case (weak scaling, no data-path collective).  Rank 0 prints one
+JSON line.  --impl reference times the reference program's own CUDA build
+(oracle/_ref/ref_c2: its kernels compiled unmodified, FP64) on the same
+workload; when that binary is absent it times the FP64 C oracle on the host.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "multi-block-lbm-gpu_b200"))
+
+METRIC = "multi-block D2Q9 MLUPS & % HBM roofline; time-to-Cd (±0.5%) vs plain FP32"
+WORKLOAD = "3-level cylinder Re=100, 4096x1024 coarse, L1 box 512x256, L2 box 256x128 coarse, D=32"
+BYTES_PER_UPDATE = {"f32": 72, "f32u": 72, "f16s": 36, "f64": 144}
+
+
+def peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def dram_traffic_per_launch(prec):
+    """dram__bytes_read.sum + dram__bytes_write.sum of one level-0 block-step
+    launch, from the committed ncu summary (None when absent)."""
+    path = os.path.join(REPO, "profiles", f"block_step_L0_config2_{prec}.md")
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_launch_full:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+class Clocks:
+    """nvidia-smi sampling (200 ms) while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = tempfile.mktemp(suffix=".csv")
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                v = [x.strip() for x in line.split(",")]
+                if len(v) >= 9 and v[1].isdigit():
+                    rows.append(v)
+        except OSError:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [int(r[1]) for r in rows]
+        loaded = [int(r[1]) for r in rows if float(r[3]) > 300] or sm
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for n, val in zip(names, r[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": int(rows[0][2]), "reasons": sorted(reasons),
+                "samples": len(rows)}
+
+
+def cpu_baseline(budget_s=12.0):
+    """The FP64 C oracle (OpenMP over all host cores) on the same workload,
+    bounded to about budget_s seconds of coarse steps."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import mblbm
+    import oracle
+
+    g = mblbm.config2_geometry()
+    oracle.set_threads(os.cpu_count())
+    o = oracle.Oracle(g)
+    o.init()
+    o.evolution(1)
+    t0 = time.perf_counter()
+    n = 0
+    while True:
+        o.evolution(1)
+        n += 1
+        if time.perf_counter() - t0 > budget_s or n >= 400:
+            break
+    dt = time.perf_counter() - t0
+    upd = mblbm.updates_per_coarse_step(g)
+    o.close()
+    return {"value": round(upd * n / dt / 1e6, 2), "unit": "MLUPS", "cores": os.cpu_count(), "kind": "port",
+            "sample": f"{n} coarse steps of the same workload after 1 warm-up step ({dt:.1f} s), FP64 C oracle, OpenMP"}
+
+
+def run_reference(args):
+    exe = os.path.join(REPO, "oracle", "_ref", "ref_c2")
+    import mblbm
+
+    upd = mblbm.updates_per_coarse_step(mblbm.config2_geometry())
+    base = {"metric": METRIC, "unit": "MLUPS", "impl": "reference", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "data": "synthetic",
+            "config": {"workload": WORKLOAD, "l2": "working set larger than L2"}}
+    if os.path.exists(exe):
+        wd = tempfile.mkdtemp()
+        r = subprocess.run([exe, "bench", str(args.steps), str(args.warmup)], cwd=wd, capture_output=True, text=True,
+                           timeout=1800)
+        js = json.loads(r.stdout.strip().splitlines()[-1])
+        v = upd / js["ms_per_step"] / 1e3
+        ve = upd / js["ms_per_step_diag"] / 1e3
+        base.update(value=round(v, 2), ms_per_step=js["ms_per_step"], dtype="f64",
+                    e2e={"value": round(ve, 2), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                         "what": "the reference's shipped loop: evolution + error_L2 + getDrag_block every step"},
+                    cpu_baseline={"value": round(v, 2), "unit": "MLUPS", "cores": 1, "kind": "reference",
+                                  "sample": f"reference CUDA build (kernels and host code unmodified, FP64, nvcc -arch=sm_100a) "
+                                            f"on cuda:0, {args.steps} timed coarse steps after {args.warmup}"})
+    else:
+        cb = cpu_baseline()
+        base.update(value=cb["value"], ms_per_step=round(upd / cb["value"] / 1e3, 4), dtype="f64", cpu_baseline=cb,
+                    e2e={"value": cb["value"], "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
+    print(json.dumps(base), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5000)
+    ap.add_argument("--warmup", type=int, default=12)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="f32", choices=["f32", "f32u", "f16s", "f64"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--roofline-only", type=int, default=0, metavar="N",
+                    help="init, 3 coarse steps, then N timed launches of the level-0 block step alone "
+                         "(the fixed launch order an ncu capture of that kernel needs); prints its roofline")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference(args)
+        return 0
+
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    import mblbm
+
+    geo = mblbm.config2_geometry()
+    upd = mblbm.updates_per_coarse_step(geo)
+    stream = torch.cuda.Stream()
+    sim = mblbm.MultiBlockLBM(geo, args.precision)
+    sim.init(stream)
+    if args.roofline_only:
+        sim.evolution(3, stream)
+        kms, kbytes, kcells = sim.time_block_step(0, args.roofline_only, stream)
+        peak, src = peaks()
+        print(json.dumps({"kernel": "k_block_step level 0", "ms_per_launch": kms, "alg_bytes_per_launch": kbytes,
+                          "cells": kcells, "achieved_gbs": kbytes / kms / 1e6, "frac": kbytes / kms / 1e6 / peak}))
+        return 0
+    sim.evolution(args.warmup, stream)
+    torch.cuda.synchronize()
+    sim.prepare(args.steps)  # plans and graphs of the timed call, compiled outside the timed region
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- timed region: K coarse steps, inputs resident in HBM ---------------
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        barrier()
+        e0.record(stream)
+        sim.evolution(args.steps, stream)
+        e1.record(stream)
+        barrier()
+    ms = e0.elapsed_time(e1)
+    kernels = sim.stats()["kernels_last_call"]
+
+    # ---- dominant kernel alone: level-0 block step, CUDA events on its stream
+    kms, kbytes, kcells = sim.time_block_step(0, 50, stream)
+    # ---- end to end through the C ABI with host buffers ----------------------
+    import numpy as np
+
+    A = [geo.Areas[a] for a in range(geo.layout.number_area)]
+    host = []
+    for a in A:
+        n = a.nx * a.ny
+        host.append({k: torch.empty(n * (9 if k == "F" else 1), dtype=torch.float64).pin_memory().numpy()
+                     for k in ("rho", "ux", "uy", "F")})
+    ref = mblbm.MultiBlockLBM(geo, args.precision)
+    ref.init(stream)
+    for i, h in enumerate(host):
+        f = ref.fields(i, stream)
+        for k in h:
+            h[k][:] = f[k].ravel()
+    ref.close()
+    sim2 = mblbm.MultiBlockLBM(geo, args.precision)
+    sim2.init(stream)
+    for _ in range(12):  # compiles the single-step plans of every scheduler phase
+        sim2.evolution(1, stream)
+        sim2.getDrag_block(stream)
+        sim2.error_L2(stream)
+    sim2.init(stream)
+    torch.cuda.synchronize()
+    h2d = sum(h[k].nbytes for h in host for k in h)
+    d2h = 0
+    barrier()
+    t0 = time.perf_counter()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for i, h in enumerate(host):
+        sim2.set_fields(i, h["rho"], h["ux"], h["uy"], h["F"], stream)
+    for _ in range(args.steps):
+        sim2.evolution(1, stream)
+        sim2.getDrag_block(stream)
+        sim2.error_L2(stream)
+        d2h += 32
+    out = [sim2.fields(i, stream) for i in range(len(A))]
+    d2h += sum(v.nbytes for f in out for k, v in f.items() if k != "solid")
+    f1.record(stream)
+    barrier()
+    ms_e2e = f0.elapsed_time(f1)
+    wall_e2e = time.perf_counter() - t0
+    sim2.close()
+
+    if dist:
+        t = torch.tensor([ms, ms_e2e], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, ms_e2e = float(t[0]), float(t[1])
+
+    if rank == 0:
+        peak, src = peaks()
+        achieved = kbytes / (kms * 1e-3) / 1e9
+        traffic = dram_traffic_per_launch(args.precision)
+        line = {
+            "metric": METRIC,
+            "value": round(world * upd * args.steps / (ms * 1e-3) / 1e6, 1),
+            "unit": "MLUPS",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": round(ms / args.steps, 5),
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": args.precision,
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "precision": args.precision, "cell_updates_per_step": upd,
+                       "l2": "working set larger than L2 (two FP32 state buffers of 5.1M cells = 370 MB); no flush",
+                       "parallelism": f"{world} independent cases, one per GPU"},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": src,
+                         "kernel": "k_block_step level 0", "alg_bytes_per_launch": kbytes, "cells_per_launch": kcells,
+                         "ms_per_launch": round(kms, 5), "bytes_per_update": BYTES_PER_UPDATE[args.precision]},
+            "e2e": {"value": round(world * upd * args.steps / (ms_e2e * 1e-3) / 1e6, 1), "unit": "MLUPS",
+                    "h2d_bytes_per_step": round(h2d / args.steps), "d2h_bytes_per_step": round(d2h / args.steps),
+                    "wall_s": round(wall_e2e, 3),
+                    "what": "C ABI with host buffers: state upload, per step mb_step + mb_drag + mb_error_L2 "
+                            "(as the reference loop), final field download"},
+            "gpu_launches": kernels,
+            "clocks": clk.summary(),
+        }
+        if not args.no_cpu_baseline and world == 1:
+            line["cpu_baseline"] = cpu_baseline()
+        print(json.dumps(line), flush=True)
+    sim.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

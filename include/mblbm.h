@@ -45,9 +45,10 @@ extern "C" {
 #define MB_ERR_NODEVICE -9    /* no CUDA device / extension unusable     */
 
 /* ---- storage precisions of the distributions -------------------------- */
-#define MB_PREC_F64 0  /* FP64 storage and arithmetic (reference precision)  */
-#define MB_PREC_F32 1  /* FP32 storage and arithmetic (plain form)           */
-#define MB_PREC_F16S 2 /* FP16 storage of f - w (shifted), FP32 arithmetic   */
+#define MB_PREC_F64 0  /* FP64 storage and arithmetic (reference precision)     */
+#define MB_PREC_F32 1  /* FP32 storage of f - w (shifted), FP32 arithmetic      */
+#define MB_PREC_F16S 2 /* FP16 storage of f - w (shifted), FP32 arithmetic      */
+#define MB_PREC_F32U 3 /* FP32 storage of f (unshifted), FP32 arithmetic        */
 
 /* ---- cell type codes, values as in lbm/lbm.h:26-32 -------------------- */
 #define MB_FLUID 0
@@ -163,6 +164,14 @@ int mb_init(mb_ctx *ctx, mb_stream stream);
  * the dependency DAG (default), 0 = launch the kernels one by one. */
 int mb_step(mb_ctx *ctx, int n_coarse, mb_stream stream);
 int mb_set_graph_mode(mb_ctx *ctx, int use_graph);
+/* Levels with at least `cells` cells update their interior (cells two or more
+ * from a block edge) and their rim as separate DAG nodes, so that the interior
+ * of the next coarse step overlaps the fine levels of this one.  Default 1e6;
+ * 0 splits every level. */
+int mb_set_split_cells(mb_ctx *ctx, long long cells);
+/* Block-step kernel of one level: 0 = one cell per thread (default),
+ * 1 = four cells per thread with vector loads.  Results are identical. */
+int mb_set_stb_variant(mb_ctx *ctx, int level, int variant);
 /* Compiles the plans (and CUDA graphs) that mb_step(ctx, n) will replay from
  * the current state, so the step call itself spends no host time on them. */
 int mb_prepare(mb_ctx *ctx, int n_coarse);

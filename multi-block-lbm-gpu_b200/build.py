@@ -60,6 +60,19 @@ def build_lib(force=False, verbose_ptxas=False):
     return LIB
 
 
+APP_SRC = os.path.join(HERE, "apps", "mblbm_run.c")
+APP = os.path.join(HERE, "apps", "mblbm_run")
+
+
+def build_app(force=False):
+    """The C driver (apps/mblbm_run.c), linked against libmblbm.so."""
+    if not force and _newer(APP, [APP_SRC, LIB]):
+        return APP
+    _run(["gcc", "-O2", "-std=c11", APP_SRC, "-o", APP, "-L" + os.path.dirname(LIB), "-lmblbm",
+          "-Wl,-rpath,$ORIGIN/../mblbm"])
+    return APP
+
+
 def build_oracle(force=False):
     src = os.path.join(ORACLE_DIR, "oracle.c")
     deps = [src, os.path.join(ORACLE_DIR, "oracle.h"), os.path.join(REPO, "include", "mblbm.h")]
@@ -72,6 +85,7 @@ def build_oracle(force=False):
 def build_all(force=False):
     build_oracle(force)
     build_lib(force)
+    build_app(force)
 
 
 if __name__ == "__main__":
@@ -83,3 +97,4 @@ if __name__ == "__main__":
     else:
         build_oracle(force)
         build_lib(force, verbose_ptxas="--ptxas" in sys.argv)
+        build_app(force)

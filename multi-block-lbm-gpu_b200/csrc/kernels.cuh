@@ -2,9 +2,10 @@
 //
 // Storage precisions (template parameter P):
 //   MB_PREC_F64  : double storage, double arithmetic (the reference's precision)
-//   MB_PREC_F32  : float storage, float arithmetic
-//   MB_PREC_F16S : half storage of h = f - w_k, float arithmetic in the
+//   MB_PREC_F32  : float storage of h = f - w_k, float arithmetic in the
 //                  shifted variables (rho = 1 + sum h)
+//   MB_PREC_F16S : half storage of h = f - w_k, float arithmetic as above
+//   MB_PREC_F32U : float storage of f itself, float arithmetic
 // Distributions live in structure-of-arrays planes: element (k, cell) of a
 // block is F[k*plane + j*pitch + i] with pitch a multiple of 128 bytes.
 #pragma once
@@ -25,20 +26,30 @@ __host__ __device__ constexpr double wd(int k) { return k == 0 ? 4. / 9 : (k <= 
 
 template <int P> struct Prec;
 template <> struct Prec<MB_PREC_F64> { using S = double; using R = double; static constexpr bool shifted = false; };
-template <> struct Prec<MB_PREC_F32> { using S = float; using R = float; static constexpr bool shifted = false; };
+template <> struct Prec<MB_PREC_F32> { using S = float; using R = float; static constexpr bool shifted = true; };
 template <> struct Prec<MB_PREC_F16S> { using S = __half; using R = float; static constexpr bool shifted = true; };
+template <> struct Prec<MB_PREC_F32U> { using S = float; using R = float; static constexpr bool shifted = false; };
 
 template <int P> __device__ __forceinline__ typename Prec<P>::R wk(int k) { return (typename Prec<P>::R)wd(k); }
 
-// value of distribution k from its stored form
+// stored word <-> arithmetic type
+__device__ __forceinline__ float to_r(__half h) { return __half2float(h); }
+__device__ __forceinline__ float to_r(float v) { return v; }
+__device__ __forceinline__ double to_r(double v) { return v; }
+template <typename S> __device__ __forceinline__ S from_r(float v);
+template <> __device__ __forceinline__ __half from_r<__half>(float v) { return __float2half_rn(v); }
+template <> __device__ __forceinline__ float from_r<float>(float v) { return v; }
+template <typename S> __device__ __forceinline__ S from_r(double v) { return (S)v; }
+
+// value of distribution k from its stored form (shifted forms store f - w_k)
 template <int P>
 __device__ __forceinline__ typename Prec<P>::R ld_f(const typename Prec<P>::S *p, long long idx, int k) {
-  if constexpr (Prec<P>::shifted) return __half2float(p[idx]) + wk<P>(k);
+  if constexpr (Prec<P>::shifted) return to_r(p[idx]) + wk<P>(k);
   else return p[idx];
 }
 template <int P>
 __device__ __forceinline__ void st_f(typename Prec<P>::S *p, long long idx, int k, typename Prec<P>::R v) {
-  if constexpr (Prec<P>::shifted) p[idx] = __float2half_rn(v - wk<P>(k));
+  if constexpr (Prec<P>::shifted) p[idx] = from_r<typename Prec<P>::S>(v - wk<P>(k));
   else p[idx] = v;
 }
 
@@ -63,34 +74,67 @@ struct StbBlk {
   const uint8_t *flags;
   int nx, ny, pitch, pad_;
   long long plane;
-  long long cell0;  // first linear cell index of this block in the launch
+  long long cell0;  // first linear cell index of this block in the launch (per-cell kernel)
   double rv_tau;
+  long long wt0;    // first warp tile of this block in the launch (quad kernel)
+  int tiles_x, row0;  // quad kernel: tiles of 128 cells per row, first row of the region
 };
 
 struct StbParams {
   int nblk;
   int macro_all;     // write rho/u of every FLUID cell (else only CF_MACRO cells)
   int write_macros;  // 0: never write rho/u (kernel timing only)
-  int pad_;
-  long long total;   // cells in the launch
+  int region;        // 0: all cells, 1: distance >= 2 from the block edge, 2: distance <= 1
+  long long total;   // cells in the launch (per-cell kernel) or warp tiles (quad kernel)
   double feqc[9];    // feq(rho0, U0): block-edge FLUID cells and stale f of edge solids
   double rho0, u0x, u0y;
   StbBlk b[STB_MAX_BLOCKS];
 };
 
+// FLUID interior cell: Macros (lbm/assit_func.h:23-31) and BGK (stb3 :103-111,
+// zero forcing term) on pulled values f (f itself, or h = f - w when shifted).
+// Writes the new distributions to out and rho/u to m.
 template <int P>
-__global__ void __launch_bounds__(256) k_block_step(const __grid_constant__ StbParams p) {
+__device__ __forceinline__ void stb_collide(const typename Prec<P>::R *f, typename Prec<P>::R rv,
+                                            typename Prec<P>::R *out, typename Prec<P>::R *m) {
+  using R = typename Prec<P>::R;
+  if constexpr (!Prec<P>::shifted) {
+    R rh = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8];
+    R ux = f[1] - f[3] + f[5] - f[6] - f[7] + f[8];
+    R uy = f[2] - f[4] + f[5] + f[6] - f[7] - f[8];
+    ux = ux / rh;
+    uy = uy / rh;
+    m[0] = rh;
+    m[1] = ux;
+    m[2] = uy;
+#pragma unroll
+    for (int k = 0; k < 9; k++) out[k] = f[k] - (f[k] - feq<R>(k, rh, ux, uy)) * rv;
+  } else {
+    // the same scheme in h = f - w: rho = 1 + sum h, j = sum e h, heq = feq - w
+    const R drh = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8];
+    const R rh = (R)1.0 + drh;
+    R ux = f[1] - f[3] + f[5] - f[6] - f[7] + f[8];
+    R uy = f[2] - f[4] + f[5] + f[6] - f[7] - f[8];
+    ux = ux / rh;
+    uy = uy / rh;
+    m[0] = rh;
+    m[1] = ux;
+    m[2] = uy;
+    const R uv = ux * ux + uy * uy;
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+      const R eu = (R)ex(k) * ux + (R)ey(k) * uy;
+      const R heq = wk<P>(k) * (drh + rh * ((R)3.0 * eu + (R)4.5 * eu * eu - (R)1.5 * uv));
+      out[k] = f[k] - (f[k] - heq) * rv;
+    }
+  }
+}
+
+// One cell of the block step: evolution_area_stb1/2/3 (multi/FH/evolution_block.h:3-119).
+template <int P>
+__device__ __forceinline__ void stb_cell(const StbParams &p, const StbBlk &B, int i, int j) {
   using R = typename Prec<P>::R;
   using S = typename Prec<P>::S;
-  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= p.total) return;
-  int t = 0;
-#pragma unroll 1
-  while (t + 1 < p.nblk && g >= p.b[t + 1].cell0) t++;
-  const StbBlk &B = p.b[t];
-  const int local = int(g - B.cell0);
-  const int j = local / B.nx;
-  const int i = local - j * B.nx;
   const long long c = (long long)j * B.pitch + i;
   const S *__restrict__ Fin = (const S *)B.Fin;
   S *__restrict__ Fout = (S *)B.Fout;
@@ -112,48 +156,16 @@ __global__ void __launch_bounds__(256) k_block_step(const __grid_constant__ StbP
     }
     R f[9];
 #pragma unroll
-    for (int k = 0; k < 9; k++) {
-      const long long src = k * plane + c - ((long long)ey(k) * B.pitch + ex(k));
-      if constexpr (Prec<P>::shifted) f[k] = __half2float(Fin[src]);  // h = f - w
-      else f[k] = Fin[src];
+    for (int k = 0; k < 9; k++) f[k] = to_r(Fin[k * plane + c - ((long long)ey(k) * B.pitch + ex(k))]);
+    R out[9], m[3];
+    stb_collide<P>(f, (R)B.rv_tau, out, m);
+    if (wm) {
+      ((R *)B.rho)[c] = m[0];
+      ((R *)B.ux)[c] = m[1];
+      ((R *)B.uy)[c] = m[2];
     }
-    const R rv = (R)B.rv_tau;
-    if constexpr (!Prec<P>::shifted) {
-      // Macros (lbm/assit_func.h:23-31)
-      R rh = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8];
-      R ux = f[1] - f[3] + f[5] - f[6] - f[7] + f[8];
-      R uy = f[2] - f[4] + f[5] + f[6] - f[7] - f[8];
-      ux = ux / rh;
-      uy = uy / rh;
-      if (wm) {
-        ((R *)B.rho)[c] = rh;
-        ((R *)B.ux)[c] = ux;
-        ((R *)B.uy)[c] = uy;
-      }
-      // BGK, stb3 :103-111 (the forcing term is zero)
 #pragma unroll
-      for (int k = 0; k < 9; k++) Fout[k * plane + c] = f[k] - (f[k] - feq<R>(k, rh, ux, uy)) * rv;
-    } else {
-      // same scheme in h = f - w: rho = 1 + sum h, j = sum e h, heq = feq - w
-      const R drh = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8];
-      const R rh = (R)1.0 + drh;
-      R ux = f[1] - f[3] + f[5] - f[6] - f[7] + f[8];
-      R uy = f[2] - f[4] + f[5] + f[6] - f[7] - f[8];
-      ux = ux / rh;
-      uy = uy / rh;
-      if (wm) {
-        ((R *)B.rho)[c] = rh;
-        ((R *)B.ux)[c] = ux;
-        ((R *)B.uy)[c] = uy;
-      }
-      const R uv = ux * ux + uy * uy;
-#pragma unroll
-      for (int k = 0; k < 9; k++) {
-        const R eu = (R)ex(k) * ux + (R)ey(k) * uy;
-        const R heq = wk<P>(k) * (drh + rh * ((R)3.0 * eu + (R)4.5 * eu * eu - (R)1.5 * uv));
-        Fout[k * plane + c] = __float2half_rn(f[k] - (f[k] - heq) * rv);
-      }
-    }
+    for (int k = 0; k < 9; k++) Fout[k * plane + c] = from_r<S>(out[k]);
     return;
   }
   if (type == 1) {  // SOLID_SBB: pull (stale f = feq(rho0,U0) off-block), then on-node bounce-back
@@ -164,7 +176,7 @@ __global__ void __launch_bounds__(256) k_block_step(const __grid_constant__ StbP
       if (id >= 0 && id < B.nx && jd >= 0 && jd < B.ny)
         fr[k] = Fin[k * plane + c - ((long long)ey(k) * B.pitch + ex(k))];
       else if constexpr (Prec<P>::shifted)
-        fr[k] = __float2half_rn((float)(p.feqc[k] - wd(k)));
+        fr[k] = from_r<S>((float)(p.feqc[k] - wd(k)));
       else
         fr[k] = (S)p.feqc[k];
     }
@@ -175,6 +187,155 @@ __global__ void __launch_bounds__(256) k_block_step(const __grid_constant__ StbP
   // C_BOUNDARY and row padding: untouched by the step, carried to the new buffer
 #pragma unroll
   for (int k = 0; k < 9; k++) Fout[k * plane + c] = Fin[k * plane + c];
+}
+
+
+template <int P>
+__global__ void __launch_bounds__(256) k_block_step(const __grid_constant__ StbParams p) {
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= p.total) return;
+  int t = 0;
+#pragma unroll 1
+  while (t + 1 < p.nblk && g >= p.b[t + 1].cell0) t++;
+  const StbBlk &B = p.b[t];
+  const int local = int(g - B.cell0);
+  int i, j;
+  if (p.region == 1) {  // interior rectangle [2, nx-3] x [2, ny-3]
+    const int w = B.nx - 4;
+    j = 2 + local / w;
+    i = 2 + (local - (j - 2) * w);
+  } else if (p.region == 2 && B.nx > 4 && B.ny > 4) {  // rows 0,1,ny-2,ny-1, then columns 0,1,nx-2,nx-1
+    if (local < 4 * B.nx) {
+      const int r = local / B.nx;
+      j = r < 2 ? r : B.ny - 4 + r;
+      i = local - r * B.nx;
+    } else {
+      const int l2 = local - 4 * B.nx, h = B.ny - 4;
+      const int q = l2 / h;
+      i = q < 2 ? q : B.nx - 4 + q;
+      j = 2 + (l2 - q * h);
+    }
+  } else {
+    j = local / B.nx;
+    i = local - j * B.nx;
+  }
+  stb_cell<P>(p, B, i, j);
+}
+
+// Four consecutive cells of a row in the stored form, as arithmetic values
+// (for shifted precisions these are h = f - w); quads start at i % 4 == 0.
+__device__ __forceinline__ void ld_quad(const float *p, float *v) {
+  const float4 x = *(const float4 *)p;
+  v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+}
+__device__ __forceinline__ void st_quad(float *p, const float *v) { *(float4 *)p = make_float4(v[0], v[1], v[2], v[3]); }
+__device__ __forceinline__ void ld_quad(const double *p, double *v) {
+  const double2 a = *(const double2 *)p, b = *(const double2 *)(p + 2);
+  v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+__device__ __forceinline__ void st_quad(double *p, const double *v) {
+  *(double2 *)p = make_double2(v[0], v[1]);
+  *(double2 *)(p + 2) = make_double2(v[2], v[3]);
+}
+__device__ __forceinline__ void ld_quad(const __half *p, float *v) {
+  const uint2 u = *(const uint2 *)p;
+  const float2 a = __half22float2(*(const __half2 *)&u.x), b = __half22float2(*(const __half2 *)&u.y);
+  v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+__device__ __forceinline__ void st_quad(__half *p, const float *v) {
+  const __half2 a = __floats2half2_rn(v[0], v[1]), b = __floats2half2_rn(v[2], v[3]);
+  uint2 u;
+  u.x = *(const uint32_t *)&a;
+  u.y = *(const uint32_t *)&b;
+  *(uint2 *)p = u;
+}
+
+// The block step on quads: a warp owns 128 consecutive cells of one row and
+// each lane four of them, moved with one vector load and store per
+// direction.  The +-1 shift of the pulled column comes from the neighbouring
+// lane (shuffle) and, at the two ends of the warp's span, from one scalar
+// load.  Quads that are all FLUID interior cells of the region take this
+// path; any other quad (block-edge rows and columns, solids, region borders,
+// row ends) runs the per-cell stb_cell for its cells.
+template <int P>
+__global__ void __launch_bounds__(256) k_block_step_q(const __grid_constant__ StbParams p) {
+  using R = typename Prec<P>::R;
+  using S = typename Prec<P>::S;
+  const long long wt = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (wt >= p.total) return;  // warp-uniform
+  int t = 0;
+#pragma unroll 1
+  while (t + 1 < p.nblk && wt >= p.b[t + 1].wt0) t++;
+  const StbBlk &B = p.b[t];
+  const int local = int(wt - B.wt0);
+  const int rr = local / B.tiles_x;
+  const int j = B.row0 + rr;
+  const int i0 = (local - rr * B.tiles_x) * 128 + 4 * lane;
+  const int clo = p.region == 1 ? 2 : 0, chi = p.region == 1 ? B.nx - 3 : B.nx - 1;
+  if (j == 0 || j == B.ny - 1) {  // no row on one side: per-cell path for the whole warp
+    for (int q = 0; q < 4; q++) {
+      const int i = i0 + q;
+      if (i >= clo && i <= chi) stb_cell<P>(p, B, i, j);
+    }
+    return;
+  }
+  const bool inrow = i0 < B.pitch;
+  const long long rowc = (long long)j * B.pitch;
+  const uint32_t fl4 = inrow ? *(const uint32_t *)(B.flags + rowc + i0) : 0x03030303u;
+  const bool fast = inrow && (fl4 & 0x07070707u) == 0u && i0 >= clo && i0 + 3 <= chi;
+  const S *__restrict__ Fin = (const S *)B.Fin;
+  // issue every load before any shuffle consumes one: nine quads and, for the
+  // six directions with a column shift, the cell just outside the warp's span
+  // (lane 0 for e_x = +1, lane 31 for e_x = -1)
+  R f[9][4];
+  R halo[9];
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    const S *rowp = Fin + k * B.plane + (long long)(j - ey(k)) * B.pitch;
+    f[k][0] = f[k][1] = f[k][2] = f[k][3] = (R)0;
+    if (inrow) ld_quad(rowp + i0, f[k]);
+    halo[k] = (R)0;
+    if (ex(k) == 1 && lane == 0 && inrow && i0 > 0) halo[k] = to_r(rowp[i0 - 1]);
+    if (ex(k) == -1 && lane == 31 && i0 + 4 < B.pitch) halo[k] = to_r(rowp[i0 + 4]);
+  }
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    if (ex(k) == 1) {  // cells i0..i0+3 pull from i0-1..i0+2
+      R pw = __shfl_up_sync(0xffffffffu, f[k][3], 1);
+      if (lane == 0) pw = halo[k];
+      f[k][3] = f[k][2]; f[k][2] = f[k][1]; f[k][1] = f[k][0]; f[k][0] = pw;
+    } else if (ex(k) == -1) {  // pull from i0+1..i0+4
+      R nw = __shfl_down_sync(0xffffffffu, f[k][0], 1);
+      if (lane == 31) nw = halo[k];
+      f[k][0] = f[k][1]; f[k][1] = f[k][2]; f[k][2] = f[k][3]; f[k][3] = nw;
+    }
+  }
+  if (fast) {
+    const R rv = (R)B.rv_tau;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      R fc[9], o[9], m[3];
+#pragma unroll
+      for (int k = 0; k < 9; k++) fc[k] = f[k][q];
+      stb_collide<P>(fc, rv, o, m);
+#pragma unroll
+      for (int k = 0; k < 9; k++) f[k][q] = o[k];
+      if (p.write_macros && (p.macro_all || ((fl4 >> (8 * q)) & 8u))) {
+        ((R *)B.rho)[rowc + i0 + q] = m[0];
+        ((R *)B.ux)[rowc + i0 + q] = m[1];
+        ((R *)B.uy)[rowc + i0 + q] = m[2];
+      }
+    }
+    S *__restrict__ Fout = (S *)B.Fout;
+#pragma unroll
+    for (int k = 0; k < 9; k++) st_quad(Fout + k * B.plane + rowc + i0, f[k]);
+  } else {
+    for (int q = 0; q < 4; q++) {
+      const int i = i0 + q;
+      if (i < B.nx && i >= clo && i <= chi) stb_cell<P>(p, B, i, j);
+    }
+  }
 }
 
 // ----------------------------------------------------------------------------
@@ -199,6 +360,7 @@ struct RecDev {
   uint8_t m0, m1, m2, pad;
   int32_t dst_cell, src;
 };
+constexpr int REC_THREADS = 64;
 struct RecParams {
   const RecDev *recs;
   int n, pad_;
@@ -206,20 +368,36 @@ struct RecParams {
   void *slots;
   double tw[4][3];
 };
+// Per-block fields the record kernel touches, as launch parameters: a record's
+// first access then depends on one load (the record), not on the block table.
+constexpr int REC_MAX_BLOCKS = 40;
+struct RecBlk {
+  void *F[2];
+  void *rho, *ux, *uy;
+  long long plane;
+  double tau;
+  int m, pad_;
+};
+struct RecParamsB {
+  RecParams r;
+  RecBlk b[REC_MAX_BLOCKS];
+};
+static_assert(sizeof(RecParamsB) <= 4096, "record launch parameters must fit the 4 KB parameter space");
 
 template <int P>
-__global__ void __launch_bounds__(256) k_records(const __grid_constant__ RecParams p) {
+__global__ void __launch_bounds__(REC_THREADS) k_records(const __grid_constant__ RecParamsB pb) {
   using R = typename Prec<P>::R;
   using S = typename Prec<P>::S;
+  const RecParams &p = pb.r;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= p.n) return;
   const RecDev r = p.recs[t];
-  const IfBlk &D = p.blk[r.dst_block];
+  const RecBlk &D = pb.b[r.dst_block];
   S *Fd = (S *)D.F[(r.bits >> 1) & 1];
   const long long dc = r.dst_cell;
   const bool wF = r.bits & 4, wM = r.bits & 8;
   if (r.type == 0) {  // same-level copy (assit_multi.h:2-46)
-    const IfBlk &A = p.blk[r.src_block];
+    const RecBlk &A = pb.b[r.src_block];
     const S *Fs = (const S *)A.F[r.bits & 1];
     const long long sc = r.src;
     if (wM) {
@@ -249,7 +427,7 @@ __global__ void __launch_bounds__(256) k_records(const __grid_constant__ RecPara
     return;
   }
   // f_c (:273-314): coarse edge <- fine point, f_neq scaled by r (tau_c-1)/(tau_f-1)
-  const IfBlk &Fb = p.blk[r.src_block];
+  const RecBlk &Fb = pb.b[r.src_block];
   const S *Fs = (const S *)Fb.F[r.bits & 1];
   const long long sc = r.src;
   const R rh = ((const R *)Fb.rho)[sc], ux = ((const R *)Fb.ux)[sc], uy = ((const R *)Fb.uy)[sc];
@@ -278,17 +456,11 @@ struct SplLineDev {
   int ci0, cj0, cdi, cdj;
   int fi0, fj0, fdi, fdj;
   int slot0;
+  int coef0;  // offset of the line's c' table (in units of 2 values per row)
   double para;
 };
 struct SplTaskDev {
   int line, src_buf, m0, mask_off;
-};
-struct SplParams {
-  const SplTaskDev *tasks;
-  const SplLineDev *lines;
-  const uint8_t *mask;
-  const IfBlk *blk;
-  void *slots;
 };
 
 // Spline3_S (:118-134), with its 0.1666667 constant
@@ -316,117 +488,111 @@ __device__ __forceinline__ void spl_gather(const SplLineDev &L, const IfBlk &C, 
   for (int k = 0; k < 9; k++) v[3 + k] = ld_f<P>(Fc, k * C.plane + c, k);
 }
 
-constexpr int SPL_THREADS = 1024;
+// Spatial interpolation, one warp per segment of SPL_SEG intervals of a
+// coarse-fine line.  The spline moments M solve the (0.5, 2, 0.5) system of
+// init_tri_A (multi/init_multi.h:30-51; decoupled natural end rows) by the
+// Thomas recurrences y_i = (d_i - l_i y_{i-1}) / den_i, x_i = y_i - c'_i x_{i+1}
+// (c'_i and 1/den_i of the whole system come from a per-line table).  Both
+// recurrences contract by 0.268 per row (2 - sqrt 3), so the moments a
+// segment needs are computed on a window of SPL_HALO rows either side of it,
+// started from zero: the truncation changes them by less than 0.268^HALO of
+// the data (1e-16 in FP64, 1e-9 in FP32), i.e. they equal the whole-line solve
+// to rounding.  Every segment is independent, so a line's gathers and solves
+// spread over many SMs.
+constexpr int SPL_SEG = 32;
+constexpr int SPL_WARPS = 4;
+template <typename R> struct SplHalo { static constexpr int v = 16; };
+template <> struct SplHalo<double> { static constexpr int v = 28; };
+template <typename R> __host__ __device__ constexpr int spl_win() { return SPL_SEG + 2 * SplHalo<R>::v + 4; }
 
-// Parallel cyclic reduction of A x_{i-1} + B x_i + C x_{i+1} = D_i for the 12
-// right-hand sides at once; the matrix is (0.5, 2, 0.5) with the decoupled
-// natural end rows of init_tri_A (multi/init_multi.h:30-51).  ROWS rows per
-// thread; shared memory holds A, B, C and D (15 N values).
-template <int P, int ROWS>
-__global__ void __launch_bounds__(SPL_THREADS) k_spline(const __grid_constant__ SplParams p) {
+struct SplSegDev {
+  int task, seg;
+};
+struct SplParamsW {
+  const SplTaskDev *tasks;
+  const SplSegDev *segs;
+  int nseg, pad_;
+  const SplLineDev *lines;
+  const uint8_t *mask;
+  const IfBlk *blk;
+  void *slots;
+  const void *coef;  // per line: c'_i (Nc values) then 1/den_i (Nc values), at 2 * line.coef0
+};
+
+template <int P>
+__global__ void __launch_bounds__(32 * SPL_WARPS) k_spline(const __grid_constant__ SplParamsW p) {
   using R = typename Prec<P>::R;
   using S = typename Prec<P>::S;
+  constexpr int H = SplHalo<R>::v;
+  constexpr int W = spl_win<R>();
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const SplTaskDev task = p.tasks[blockIdx.x];
+  typedef R Win[12][W];
+  Win *sf = (Win *)smem_raw;            // [warp] gathered fields
+  Win *sx = sf + SPL_WARPS;             // [warp] forward sweep, then the moments
+  R(*scf)[2][W] = (R(*)[2][W])(sx + SPL_WARPS);  // [warp] c'_i and 1/den_i of the window
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int sid = blockIdx.x * SPL_WARPS + warp;
+  if (sid >= p.nseg) return;
+  const SplSegDev sg = p.segs[sid];
+  const SplTaskDev task = p.tasks[sg.task];
   const SplLineDev L = p.lines[task.line];
   const int N = L.Nc;
-  R *A = (R *)smem_raw;
-  R *Bd = A + N;
-  R *Cu = Bd + N;
-  R *D = Cu + N;  // D[f*N + i]
   const IfBlk &C = p.blk[L.coarse];
   const S *Fc = (const S *)C.F[task.src_buf];
-  const int tid = threadIdx.x;
+  const R *cpt = (const R *)p.coef + 2LL * L.coef0;
+  const R *ivd = cpt + N;
 
-  // gather (the race-free reading of init_Spline3 :54-80)
-  for (int i = tid; i < N; i += blockDim.x) {
+  // intervals I in [Ilo, Ihi] (fine point ip uses rows I-1 and I, I = ceil(ip/r), at least 1)
+  const int Ilo = 1 + sg.seg * SPL_SEG, Ihi = min(N - 1, (sg.seg + 1) * SPL_SEG);
+  const int w0 = max(0, Ilo - 1 - H), w1 = min(N - 1, Ihi + H);  // rows solved
+  const int g0 = max(0, w0 - 1), g1 = min(N - 1, w1 + 1);        // rows gathered
+  for (int i = g0 + lane; i <= g1; i += 32) {
     R v[12];
     spl_gather<P>(L, C, Fc, i, v);
 #pragma unroll
-    for (int f = 0; f < 12; f++) D[f * N + i] = v[f];
+    for (int f = 0; f < 12; f++) sf[warp][f][i - g0] = v[f];
+    scf[warp][0][i - g0] = cpt[i];
+    scf[warp][1][i - g0] = ivd[i];
   }
-  __syncthreads();
-  // right-hand sides 6 f_i - 3 f_{i-1} - 3 f_{i+1}, zero at both ends (:82-107)
-  R rhs[ROWS][12];
-#pragma unroll
-  for (int q = 0; q < ROWS; q++) {
-    const int i = tid + q * blockDim.x;
-#pragma unroll
-    for (int f = 0; f < 12; f++) {
-      R v = 0;
-      if (i > 0 && i < N - 1) v = ((R)6.0 * D[f * N + i] - (R)3.0 * D[f * N + i - 1] - (R)3.0 * D[f * N + i + 1]);
-      rhs[q][f] = v;
+  __syncwarp();
+  if (lane < 12) {
+    const int f = lane;
+    const R *x = sf[warp][f] - g0;  // x[i] = field at row i
+    R *y = sx[warp][f] - g0;
+    const R *cp = scf[warp][0] - g0, *iv = scf[warp][1] - g0;
+    // right-hand sides 6 f_i - 3 f_{i-1} - 3 f_{i+1}, zero at both ends (assit_multi.h:82-107)
+    R yv = 0;
+#pragma unroll 4
+    for (int i = w0; i <= w1; i++) {
+      const R d = (i == 0 || i == N - 1) ? (R)0 : ((R)6.0 * x[i] - (R)3.0 * x[i - 1] - (R)3.0 * x[i + 1]);
+      const R l = (i <= 1 || i == N - 1) ? (R)0 : (R)0.5;
+      yv = (d - l * yv) * iv[i];
+      y[i] = yv;
+    }
+    R xv = 0;
+#pragma unroll 4
+    for (int i = w1; i >= w0; i--) {
+      xv = y[i] - cp[i] * xv;
+      y[i] = xv;
     }
   }
-  __syncthreads();
-#pragma unroll
-  for (int q = 0; q < ROWS; q++) {
-    const int i = tid + q * blockDim.x;
-    if (i < N) {
-      A[i] = (i == 0 || i == 1 || i == N - 1) ? (R)0 : (R)0.5;
-      Cu[i] = (i == 0 || i == N - 2 || i == N - 1) ? (R)0 : (R)0.5;
-      Bd[i] = (R)2.0;
-#pragma unroll
-      for (int f = 0; f < 12; f++) D[f * N + i] = rhs[q][f];
-    }
-  }
-  __syncthreads();
-  for (int s = 1; s < N; s <<= 1) {
-    R na[ROWS], nb[ROWS], nc[ROWS];
-#pragma unroll
-    for (int q = 0; q < ROWS; q++) {
-      const int i = tid + q * blockDim.x;
-      if (i >= N) continue;
-      const R a = A[i], c = Cu[i];
-      R al = 0, ga = 0, aa = 0, cc = 0, bb = Bd[i];
-      if (i - s >= 0) { al = -a / Bd[i - s]; aa = al * A[i - s]; bb += al * Cu[i - s]; }
-      if (i + s < N) { ga = -c / Bd[i + s]; cc = ga * Cu[i + s]; bb += ga * A[i + s]; }
-      na[q] = aa;
-      nb[q] = bb;
-      nc[q] = cc;
-#pragma unroll
-      for (int f = 0; f < 12; f++) {
-        R d = D[f * N + i];
-        if (i - s >= 0) d += al * D[f * N + i - s];
-        if (i + s < N) d += ga * D[f * N + i + s];
-        rhs[q][f] = d;
-      }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int q = 0; q < ROWS; q++) {
-      const int i = tid + q * blockDim.x;
-      if (i >= N) continue;
-      A[i] = na[q];
-      Bd[i] = nb[q];
-      Cu[i] = nc[q];
-#pragma unroll
-      for (int f = 0; f < 12; f++) D[f * N + i] = rhs[q][f];
-    }
-    __syncthreads();
-  }
-  for (int i = tid; i < N; i += blockDim.x) {
-    const R inv = Bd[i];
-#pragma unroll
-    for (int f = 0; f < 12; f++) D[f * N + i] = D[f * N + i] / inv;
-  }
-  __syncthreads();
+  __syncwarp();
 
-  // evaluate at the fine points (calculate_Spline3_gpu :136-185)
+  // evaluate the fine points of the segment (calculate_Spline3_gpu :136-185)
   const IfBlk &Fb = p.blk[L.fine];
   R *slots = (R *)p.slots;
   const R para = (R)L.para;
-  for (int ip = tid; ip < L.Nf; ip += blockDim.x) {
+  const int ip0 = (sg.seg == 0) ? 0 : L.r * (Ilo - 1) + 1;
+  const int ip1 = min(L.Nf - 1, L.r * Ihi);
+  for (int ip = ip0 + lane; ip <= ip1; ip += 32) {
     const R xx = (R)ip / (R)L.r;
     int I = (int)ceil(xx);
     if (I == 0) I = 1;
-    R v0[12], v1[12];
-    spl_gather<P>(L, C, Fc, I - 1, v0);
-    spl_gather<P>(L, C, Fc, I, v1);
     R out[12];
 #pragma unroll
     for (int f = 0; f < 12; f++)
-      out[f] = spline3_s<R>(xx, (R)(I - 1), (R)1.0, v0[f], v1[f], D[f * N + I - 1], D[f * N + I]);
+      out[f] = spline3_s<R>(xx, (R)(I - 1), (R)1.0, sf[warp][f][I - 1 - g0], sf[warp][f][I - g0],
+                            sx[warp][f][I - 1 - g0], sx[warp][f][I - g0]);
     const long long fc = (long long)(L.fj0 + ip * L.fdj) * Fb.pitch + (L.fi0 + ip * L.fdi);
     if (task.mask_off < 0 || p.mask[task.mask_off + ip]) {
       ((R *)Fb.rho)[fc] = out[0];

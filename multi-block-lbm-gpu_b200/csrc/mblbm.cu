@@ -34,7 +34,7 @@ using namespace mblbm::dev;
 
 namespace {
 
-size_t prec_bytes(int prec) { return prec == MB_PREC_F64 ? 8 : (prec == MB_PREC_F32 ? 4 : 2); }
+size_t prec_bytes(int prec) { return prec == MB_PREC_F64 ? 8 : (prec == MB_PREC_F16S ? 2 : 4); }
 size_t real_bytes(int prec) { return prec == MB_PREC_F64 ? 8 : 4; }
 
 struct DevPlanNode {
@@ -45,8 +45,9 @@ struct DevPlanNode {
   size_t smem = 0;
   // parameter blocks (one of them used)
   StbParams stb;
-  RecParams rec;
-  SplParams spl;
+  RecParamsB rec;
+  SplParamsW spl;
+  std::vector<SplSegDev> segs;
   void *args[1];
   std::vector<int> deps;
 };
@@ -83,6 +84,7 @@ struct mb_ctx {
   long long n_slot_points = 0;
   std::vector<SplLine> spl_lines;
   SplLineDev *d_spl_lines = nullptr;
+  void *d_spl_coef = nullptr;  // per line: c'_i and 1/den_i of the spline system
   // drag
   int drag_area = 0;
   int n_drag = 0;
@@ -107,6 +109,8 @@ struct mb_ctx {
   bool inited = false;
   int use_graph = 1;
   int period = 1;
+  long long split_cells = 1000000;
+  int stb_variant[MB_MAX_LEVEL] = {0};  // 0: one cell per thread, 1: quads (k_block_step_q)
   std::map<std::string, std::unique_ptr<CompiledPlan>> plans;
   long long kernels_last_call = 0;
   long long kernels_per_step = 0;
@@ -114,6 +118,28 @@ struct mb_ctx {
 };
 
 namespace {
+
+// Runs STMT with P bound to the runtime precision and S to its storage type.
+#define MB_DISPATCH(prec, STMT)                                     \
+  do {                                                              \
+    if ((prec) == MB_PREC_F64) {                                    \
+      constexpr int P = MB_PREC_F64;                                \
+      using S = double;                                             \
+      STMT;                                                         \
+    } else if ((prec) == MB_PREC_F32) {                             \
+      constexpr int P = MB_PREC_F32;                                \
+      using S = float;                                              \
+      STMT;                                                         \
+    } else if ((prec) == MB_PREC_F32U) {                            \
+      constexpr int P = MB_PREC_F32U;                               \
+      using S = float;                                              \
+      STMT;                                                         \
+    } else {                                                        \
+      constexpr int P = MB_PREC_F16S;                               \
+      using S = __half;                                             \
+      STMT;                                                         \
+    }                                                               \
+  } while (0)
 
 template <typename T>
 int dalloc(mb_ctx *c, T **p, size_t n) {
@@ -131,28 +157,43 @@ template <template <int> class K, typename... A>
 void *kfunc(int prec) {
   if (prec == MB_PREC_F64) return K<MB_PREC_F64>::ptr();
   if (prec == MB_PREC_F32) return K<MB_PREC_F32>::ptr();
+  if (prec == MB_PREC_F32U) return K<MB_PREC_F32U>::ptr();
   return K<MB_PREC_F16S>::ptr();
 }
 template <int P> struct KStb { static void *ptr() { return (void *)k_block_step<P>; } };
+template <int P> struct KStbQ { static void *ptr() { return (void *)k_block_step_q<P>; } };
 template <int P> struct KRec { static void *ptr() { return (void *)k_records<P>; } };
-template <int P> struct KSpl1 { static void *ptr() { return (void *)k_spline<P, 1>; } };
-template <int P> struct KSpl2 { static void *ptr() { return (void *)k_spline<P, 2>; } };
+template <int P> struct KSpl { static void *ptr() { return (void *)k_spline<P>; } };
 template <int P> struct KDrag { static void *ptr() { return (void *)k_drag<P>; } };
 template <int P> struct KL2 { static void *ptr() { return (void *)k_error_l2<P>; } };
 
-int max_spline_rows(int prec) { return prec == MB_PREC_F64 ? SPL_THREADS : 2 * SPL_THREADS; }
+// dynamic shared memory of k_spline per warp: two 12 x window arrays and the
+// window's c' and 1/den
+size_t spline_smem(int prec) {
+  return prec == MB_PREC_F64 ? (size_t)26 * SPL_WARPS * spl_win<double>() * sizeof(double)
+                             : (size_t)26 * SPL_WARPS * spl_win<float>() * sizeof(float);
+}
 
 // ---- node lowering ------------------------------------------------------------
-StbParams make_stb(mb_ctx *c, int a0, int a1, uint64_t parity, int macro_all, int write_macros) {
+// cells of a block in a block-step region (see StbRegion)
+long long region_cells(int nx, int ny, int region) {
+  const long long all = (long long)nx * ny;
+  const long long in = (nx > 4 && ny > 4) ? (long long)(nx - 4) * (ny - 4) : 0;
+  return region == STB_INTERIOR ? in : (region == STB_RIM ? all - in : all);
+}
+
+StbParams make_stb(mb_ctx *c, int a0, int a1, uint64_t parity, int macro_all, int write_macros,
+                   int region = STB_ALL) {
   StbParams p{};
   p.nblk = a1 - a0;
   p.macro_all = macro_all;
   p.write_macros = write_macros;
+  p.region = region;
   for (int k = 0; k < 9; k++) p.feqc[k] = c->feqc[k];
   p.rho0 = c->geo.config.rho0;
   p.u0x = c->geo.config.U0[0];
   p.u0y = c->geo.config.U0[1];
-  long long cell = 0;
+  long long cell = 0, wt = 0;
   for (int a = a0; a < a1; a++) {
     const IfBlk &B = c->blk[a];
     const int cur = (parity >> a) & 1;
@@ -169,10 +210,21 @@ StbParams make_stb(mb_ctx *c, int a0, int a1, uint64_t parity, int macro_all, in
     s.plane = B.plane;
     s.cell0 = cell;
     s.rv_tau = c->geo.Areas[a].rv_tau;
-    cell += (long long)B.nx * B.ny;
+    cell += region_cells(B.nx, B.ny, region);
+    // quad kernel: rows of the region in tiles of 128 cells
+    s.tiles_x = (B.nx + 127) / 128;
+    s.row0 = region == STB_INTERIOR ? 2 : 0;
+    const int nrows = region == STB_INTERIOR ? std::max(0, B.ny - 4) : B.ny;
+    s.wt0 = wt;
+    wt += (long long)s.tiles_x * nrows;
   }
-  p.total = cell;
+  p.total = region == STB_RIM ? cell : wt;
   return p;
+}
+
+// the rim is always stepped one cell per thread
+bool stb_uses_quads(const mb_ctx *c, int level, int region) {
+  return region != STB_RIM && c->stb_variant[level] == 1;
 }
 
 int lower_plan(mb_ctx *c, CompiledPlan &cp) {
@@ -183,10 +235,15 @@ int lower_plan(mb_ctx *c, CompiledPlan &cp) {
     d.kind = n.kind;
     d.deps = n.deps;
     if (n.kind == NK_STB) {
-      d.stb = make_stb(c, n.a0, n.a1, n.parity, n.macro_all, 1);
-      d.func = kfunc<KStb>(c->prec);
+      d.stb = make_stb(c, n.a0, n.a1, n.parity, n.macro_all, 1, n.region);
       d.block = dim3(256);
-      d.grid = dim3((unsigned)((d.stb.total + 255) / 256));
+      if (stb_uses_quads(c, n.level, n.region)) {
+        d.func = kfunc<KStbQ>(c->prec);
+        d.grid = dim3((unsigned)((d.stb.total + 7) / 8));  // 8 warp tiles per CTA
+      } else {
+        d.func = kfunc<KStb>(c->prec);
+        d.grid = dim3((unsigned)((d.stb.total + 255) / 256));
+      }
       d.args[0] = &d.stb;
     } else if (n.kind == NK_REC) {
       RecDev *dr = nullptr;
@@ -194,45 +251,56 @@ int lower_plan(mb_ctx *c, CompiledPlan &cp) {
       cp.dev_allocs.push_back(dr);
       if (cudaMemcpy(dr, n.recs.data(), n.recs.size() * sizeof(RecDev), cudaMemcpyHostToDevice) != cudaSuccess)
         return MB_ERR_CUDA;
-      d.rec = RecParams{};
-      d.rec.recs = dr;
-      d.rec.n = (int)n.recs.size();
-      d.rec.blk = c->d_blk;
-      d.rec.slots = c->d_slots;
-      std::memcpy(d.rec.tw, n.tw, sizeof(n.tw));
+      d.rec = RecParamsB{};
+      d.rec.r.recs = dr;
+      d.rec.r.n = (int)n.recs.size();
+      d.rec.r.blk = c->d_blk;
+      d.rec.r.slots = c->d_slots;
+      std::memcpy(d.rec.r.tw, n.tw, sizeof(n.tw));
+      for (int a = 0; a < c->nblk; a++) {
+        const IfBlk &B = c->blk[a];
+        d.rec.b[a] = {{B.F[0], B.F[1]}, B.rho, B.ux, B.uy, B.plane, B.tau, B.m, 0};
+      }
       d.func = kfunc<KRec>(c->prec);
-      d.block = dim3(256);
-      d.grid = dim3((unsigned)((n.recs.size() + 255) / 256));
+      d.block = dim3(REC_THREADS);  // small CTAs spread a launch's scattered accesses over many SMs
+      d.grid = dim3((unsigned)((n.recs.size() + REC_THREADS - 1) / REC_THREADS));
       d.args[0] = &d.rec;
     } else {
       std::vector<SplTaskDev> tasks(n.spl.size());
-      int maxN = 0;
       for (size_t t = 0; t < n.spl.size(); t++) {
         tasks[t] = {n.spl[t].line, n.spl[t].src_buf, n.spl[t].m0, n.spl[t].mask_off};
-        maxN = std::max(maxN, c->spl_lines[n.spl[t].line].Nc);
+        const int nseg = (c->spl_lines[n.spl[t].line].Nc - 1 + SPL_SEG - 1) / SPL_SEG;
+        for (int g = 0; g < nseg; g++) d.segs.push_back({(int)t, g});
       }
       SplTaskDev *dt = nullptr;
+      SplSegDev *dsg = nullptr;
       uint8_t *dm = nullptr;
       if (cudaMalloc(&dt, tasks.size() * sizeof(SplTaskDev)) != cudaSuccess) return MB_ERR_NOMEM;
       cp.dev_allocs.push_back(dt);
+      if (cudaMalloc(&dsg, d.segs.size() * sizeof(SplSegDev)) != cudaSuccess) return MB_ERR_NOMEM;
+      cp.dev_allocs.push_back(dsg);
       if (cudaMalloc(&dm, std::max<size_t>(n.spl_mask.size(), 1)) != cudaSuccess) return MB_ERR_NOMEM;
       cp.dev_allocs.push_back(dm);
       MB_CUDA(cudaMemcpy(dt, tasks.data(), tasks.size() * sizeof(SplTaskDev), cudaMemcpyHostToDevice));
+      MB_CUDA(cudaMemcpy(dsg, d.segs.data(), d.segs.size() * sizeof(SplSegDev), cudaMemcpyHostToDevice));
       if (!n.spl_mask.empty()) MB_CUDA(cudaMemcpy(dm, n.spl_mask.data(), n.spl_mask.size(), cudaMemcpyHostToDevice));
       d.spl.tasks = dt;
+      d.spl.segs = dsg;
+      d.spl.nseg = (int)d.segs.size();
       d.spl.lines = c->d_spl_lines;
       d.spl.mask = dm;
       d.spl.blk = c->d_blk;
       d.spl.slots = c->d_slots;
-      const int rows = (maxN + SPL_THREADS - 1) / SPL_THREADS;
-      d.func = rows <= 1 ? kfunc<KSpl1>(c->prec) : kfunc<KSpl2>(c->prec);
-      d.block = dim3(SPL_THREADS);
-      d.grid = dim3((unsigned)tasks.size());
-      d.smem = (size_t)15 * maxN * real_bytes(c->prec);
+      d.spl.coef = c->d_spl_coef;
+      d.func = kfunc<KSpl>(c->prec);
+      d.block = dim3(32 * SPL_WARPS);
+      d.grid = dim3((unsigned)((d.segs.size() + SPL_WARPS - 1) / SPL_WARPS));
+      d.smem = spline_smem(c->prec);
       d.args[0] = &d.spl;
     }
   }
-  cp.kernels = (long long)cp.dn.size();
+  cp.kernels = 0;
+  for (auto &d : cp.dn) cp.kernels += d.grid.x ? 1 : 0;
   return MB_OK;
 }
 
@@ -252,14 +320,17 @@ int build_graph(CompiledPlan &cp) {
     std::vector<cudaGraphNode_t> deps;
     for (int p : d.deps)
       if (gn[p]) deps.push_back(gn[p]);
+    if (d.grid.x == 0) {  // nothing to do, but later nodes may order through it
+      MB_CUDA(cudaGraphAddEmptyNode(&gn[q], cp.graph, deps.data(), deps.size()));
+      continue;
+    }
     cudaKernelNodeParams kp{};
     kp.func = d.func;
-    kp.gridDim = d.grid.x ? d.grid : dim3(1);
+    kp.gridDim = d.grid;
     kp.blockDim = d.block;
     kp.sharedMemBytes = (unsigned)d.smem;
     kp.kernelParams = d.args;
     kp.extra = nullptr;
-    if (d.grid.x == 0) continue;
     MB_CUDA(cudaGraphAddKernelNode(&gn[q], cp.graph, deps.data(), deps.size(), &kp));
   }
   MB_CUDA(cudaGraphInstantiate(&cp.exec, cp.graph, 0));
@@ -267,10 +338,8 @@ int build_graph(CompiledPlan &cp) {
 }
 
 int set_smem_limits(int prec) {
-  const int bytes = 15 * max_spline_rows(prec) * (int)real_bytes(prec);
-  void *f1 = kfunc<KSpl1>(prec), *f2 = kfunc<KSpl2>(prec);
-  MB_CUDA(cudaFuncSetAttribute(f1, cudaFuncAttributeMaxDynamicSharedMemorySize, std::min(bytes, 227 * 1024)));
-  MB_CUDA(cudaFuncSetAttribute(f2, cudaFuncAttributeMaxDynamicSharedMemorySize, std::min(bytes, 227 * 1024)));
+  MB_CUDA(cudaFuncSetAttribute(kfunc<KSpl>(prec), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)spline_smem(prec)));
   return MB_OK;
 }
 
@@ -280,6 +349,7 @@ CompiledPlan *get_plan(mb_ctx *c, int n, bool final_macros, int *err) {
   if (it != c->plans.end()) return it->second.get();
   auto cp = std::make_unique<CompiledPlan>();
   PlanCompiler pc(c->geo, c->bl, c->hflags, c->spl_lines);
+  pc.split_cells = c->split_cells;
   SchedState s = c->state;
   cp->nodes = pc.compile(s, n, final_macros);
   cp->end = s;
@@ -327,7 +397,8 @@ int exec_nodes_once(mb_ctx *c, std::vector<PlanNode> nodes, cudaStream_t s) {
 extern "C" int mb_create(const mb_geometry *geo, int precision, mb_ctx **out) {
   if (!geo || !out) return MB_ERR_INVALID;
   *out = nullptr;
-  if (precision != MB_PREC_F64 && precision != MB_PREC_F32 && precision != MB_PREC_F16S) return MB_ERR_INVALID;
+  if (precision != MB_PREC_F64 && precision != MB_PREC_F32 && precision != MB_PREC_F16S && precision != MB_PREC_F32U)
+    return MB_ERR_INVALID;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return MB_ERR_NODEVICE;
   auto c = std::make_unique<mb_ctx>();
@@ -337,7 +408,8 @@ extern "C" int mb_create(const mb_geometry *geo, int precision, mb_ctx **out) {
   const mb_layout &L = geo->layout;
   const mb_config &cfg = geo->config;
   c->nblk = L.number_area;
-  if (c->nblk < 1 || c->nblk > MB_MAX_AREA || c->nblk > 255) return MB_ERR_INVALID;
+  if (c->nblk < 1 || c->nblk > MB_MAX_AREA) return MB_ERR_INVALID;
+  if (c->nblk > REC_MAX_BLOCKS) return MB_ERR_UNSUPPORTED;
   const size_t sb = prec_bytes(precision), rb = real_bytes(precision);
   const int pitch_align = (int)(128 / sb);
 
@@ -391,7 +463,6 @@ extern "C" int mb_create(const mb_geometry *geo, int precision, mb_ctx **out) {
     s.para = (af.tau - 1.0) / (s.r * (ac.tau - 1.0));
     if (l.Nc < 2 || l.Nf < 1 || s.r < 1) return MB_ERR_GEOMETRY;
     if ((long long)(l.Nf - 1) > (long long)s.r * (l.Nc - 1)) return MB_ERR_GEOMETRY;
-    if (l.Nc > max_spline_rows(precision)) return MB_ERR_UNSUPPORTED;
     slot_pts += l.Nf;
   }
   c->n_slot_points = slot_pts;
@@ -432,12 +503,39 @@ extern "C" int mb_create(const mb_geometry *geo, int precision, mb_ctx **out) {
   }
   if ((e = dalloc(c.get(), &c->d_spl_lines, std::max(L.number_line, 1)))) return e;
   if (L.number_line) {
+    // LU coefficients of each line's system (init_tri_A rows): c'_i = u_i / den_i,
+    // den_i = 2 - l_i c'_{i-1}; stored as c' then 1/den, in the arithmetic type
     std::vector<SplLineDev> sd(L.number_line);
+    std::vector<double> coef;
     for (int b = 0; b < L.number_line; b++) {
       const SplLine &s = c->spl_lines[b];
-      sd[b] = {s.coarse, s.fine, s.Nc, s.Nf, s.r, s.ci0, s.cj0, s.cdi, s.cdj, s.fi0, s.fj0, s.fdi, s.fdj, s.slot0, s.para};
+      const int N = s.Nc;
+      sd[b] = {s.coarse, s.fine, s.Nc, s.Nf, s.r, s.ci0, s.cj0, s.cdi, s.cdj, s.fi0, s.fj0, s.fdi, s.fdj, s.slot0,
+               (int)(coef.size() / 2), s.para};
+      std::vector<double> cp(N), iv(N);
+      double prev = 0;
+      for (int i = 0; i < N; i++) {
+        const double l = (i <= 1 || i == N - 1) ? 0.0 : 0.5, u = (i == 0 || i >= N - 2) ? 0.0 : 0.5;
+        const double den = 2.0 - l * prev;
+        cp[i] = u / den;
+        iv[i] = 1.0 / den;
+        prev = cp[i];
+      }
+      coef.insert(coef.end(), cp.begin(), cp.end());
+      coef.insert(coef.end(), iv.begin(), iv.end());
     }
     MB_CUDA(cudaMemcpy(c->d_spl_lines, sd.data(), sd.size() * sizeof(SplLineDev), cudaMemcpyHostToDevice));
+    const size_t rb = real_bytes(precision);
+    std::vector<unsigned char> raw(coef.size() * rb);
+    for (size_t q = 0; q < coef.size(); q++) {
+      if (rb == 8) std::memcpy(&raw[q * 8], &coef[q], 8);
+      else { const float fv = (float)coef[q]; std::memcpy(&raw[q * 4], &fv, 4); }
+    }
+    void *pc;
+    if (cudaMalloc(&pc, raw.size()) != cudaSuccess) return MB_ERR_NOMEM;
+    c->allocs.push_back(pc);
+    c->d_spl_coef = pc;
+    MB_CUDA(cudaMemcpy(pc, raw.data(), raw.size(), cudaMemcpyHostToDevice));
   }
 
   // drag links (fdrag_store, force_block.h:78-127): i-outer, j-inner, k
@@ -542,6 +640,22 @@ extern "C" int mb_destroy(mb_ctx *c) {
   return MB_OK;
 }
 
+extern "C" int mb_set_split_cells(mb_ctx *c, long long cells) {
+  if (!c || cells < 0) return MB_ERR_INVALID;
+  cudaDeviceSynchronize();
+  c->split_cells = cells;
+  c->plans.clear();
+  return MB_OK;
+}
+
+extern "C" int mb_set_stb_variant(mb_ctx *c, int level, int variant) {
+  if (!c || level < 0 || level >= c->geo.layout.LEVEL || variant < 0 || variant > 1) return MB_ERR_INVALID;
+  cudaDeviceSynchronize();
+  c->stb_variant[level] = variant;
+  c->plans.clear();
+  return MB_OK;
+}
+
 extern "C" int mb_set_graph_mode(mb_ctx *c, int use_graph) {
   if (!c) return MB_ERR_INVALID;
   c->use_graph = use_graph ? 1 : 0;
@@ -562,12 +676,8 @@ extern "C" int mb_init(mb_ctx *c, mb_stream stream) {
     for (int q = 0; q < 2; q++) {
       const int gr = launch_grid(9 * n, th);
       const double *f = c->feqc;
-      if (c->prec == MB_PREC_F64)
-        k_fill_planes<MB_PREC_F64><<<gr, th, 0, s>>>((double *)B.F[q], n, f[0], f[1], f[2], f[3], f[4], f[5], f[6], f[7], f[8]);
-      else if (c->prec == MB_PREC_F32)
-        k_fill_planes<MB_PREC_F32><<<gr, th, 0, s>>>((float *)B.F[q], n, f[0], f[1], f[2], f[3], f[4], f[5], f[6], f[7], f[8]);
-      else
-        k_fill_planes<MB_PREC_F16S><<<gr, th, 0, s>>>((__half *)B.F[q], n, f[0], f[1], f[2], f[3], f[4], f[5], f[6], f[7], f[8]);
+      MB_DISPATCH(c->prec, (k_fill_planes<P><<<gr, th, 0, s>>>((S *)B.F[q], n, f[0], f[1], f[2], f[3], f[4], f[5],
+                                                               f[6], f[7], f[8])));
     }
     const int gr = launch_grid(n, th);
     if (c->prec == MB_PREC_F64) {
@@ -772,12 +882,8 @@ extern "C" int mb_check_finite(mb_ctx *c, long long *bad, mb_stream stream) {
     const IfBlk &B = c->blk[a];
     const void *F = B.F[c->state.parity[a]];
     const int gr = launch_grid((long long)B.nx * B.ny, 256);
-    if (c->prec == MB_PREC_F64)
-      k_count_nonfinite<MB_PREC_F64><<<gr, 256, 0, s>>>((const double *)F, B.plane, B.flags, B.nx, B.ny, B.pitch, c->d_count);
-    else if (c->prec == MB_PREC_F32)
-      k_count_nonfinite<MB_PREC_F32><<<gr, 256, 0, s>>>((const float *)F, B.plane, B.flags, B.nx, B.ny, B.pitch, c->d_count);
-    else
-      k_count_nonfinite<MB_PREC_F16S><<<gr, 256, 0, s>>>((const __half *)F, B.plane, B.flags, B.nx, B.ny, B.pitch, c->d_count);
+    MB_DISPATCH(c->prec, (k_count_nonfinite<P><<<gr, 256, 0, s>>>((const S *)F, B.plane, B.flags, B.nx, B.ny, B.pitch,
+                                                                    c->d_count)));
   }
   unsigned long long h = 0;
   MB_CUDA(cudaMemcpyAsync(&h, c->d_count, sizeof(h), cudaMemcpyDeviceToHost, s));
@@ -807,9 +913,7 @@ extern "C" int mb_copy_fields(mb_ctx *c, int a, double *rho, double *ux, double 
   const int gr = launch_grid(9 * n, 256);
   if (F) {
     const void *Fs = B.F[c->state.parity[a]];
-    if (c->prec == MB_PREC_F64) k_planes_to_f64<MB_PREC_F64><<<gr, 256, 0, s>>>((const double *)Fs, B.plane, B.nx, B.ny, B.pitch, c->d_stage);
-    else if (c->prec == MB_PREC_F32) k_planes_to_f64<MB_PREC_F32><<<gr, 256, 0, s>>>((const float *)Fs, B.plane, B.nx, B.ny, B.pitch, c->d_stage);
-    else k_planes_to_f64<MB_PREC_F16S><<<gr, 256, 0, s>>>((const __half *)Fs, B.plane, B.nx, B.ny, B.pitch, c->d_stage);
+    MB_DISPATCH(c->prec, (k_planes_to_f64<P><<<gr, 256, 0, s>>>((const S *)Fs, B.plane, B.nx, B.ny, B.pitch, c->d_stage)));
     MB_CUDA(cudaMemcpyAsync(F, c->d_stage, 9 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
     MB_CUDA(cudaStreamSynchronize(s));
   }
@@ -846,9 +950,7 @@ extern "C" int mb_set_fields(mb_ctx *c, int a, const double *rho, const double *
   if (F) {
     MB_CUDA(cudaMemcpyAsync(c->d_stage, F, 9 * n * sizeof(double), cudaMemcpyHostToDevice, s));
     void *Fd = B.F[c->state.parity[a]];
-    if (c->prec == MB_PREC_F64) k_f64_to_planes<MB_PREC_F64><<<gr, 256, 0, s>>>((double *)Fd, B.plane, B.nx, B.ny, B.pitch, c->d_stage);
-    else if (c->prec == MB_PREC_F32) k_f64_to_planes<MB_PREC_F32><<<gr, 256, 0, s>>>((float *)Fd, B.plane, B.nx, B.ny, B.pitch, c->d_stage);
-    else k_f64_to_planes<MB_PREC_F16S><<<gr, 256, 0, s>>>((__half *)Fd, B.plane, B.nx, B.ny, B.pitch, c->d_stage);
+    MB_DISPATCH(c->prec, (k_f64_to_planes<P><<<gr, 256, 0, s>>>((S *)Fd, B.plane, B.nx, B.ny, B.pitch, c->d_stage)));
     MB_CUDA(cudaStreamSynchronize(s));
   }
   void *M[3] = {B.rho, B.ux, B.uy};
@@ -914,22 +1016,26 @@ extern "C" int mb_time_block_step(mb_ctx *c, int level, int n, mb_stream stream,
   for (int a0 = L.ASP[level]; a0 < L.ASP[level + 1]; a0 += STB_MAX_BLOCKS) {
     const int a1 = std::min(L.ASP[level + 1], a0 + STB_MAX_BLOCKS);
     ps.push_back(make_stb(c, a0, a1, par, 0, 0));
-    tot += ps.back().total;
+    for (int a = a0; a < a1; a++) tot += (long long)c->blk[a].nx * c->blk[a].ny;
   }
-  void *fn = kfunc<KStb>(c->prec);
+  const bool quads = stb_uses_quads(c, level, STB_ALL);
+  void *fn = quads ? kfunc<KStbQ>(c->prec) : kfunc<KStb>(c->prec);
+  auto grid_of = [&](const StbParams &p) {
+    return quads ? dim3((unsigned)((p.total + 7) / 8)) : dim3((unsigned)((p.total + 255) / 256));
+  };
   cudaEvent_t e0, e1;
   MB_CUDA(cudaEventCreate(&e0));
   MB_CUDA(cudaEventCreate(&e1));
   for (int w = 0; w < 3; w++)
     for (auto &p : ps) {
       void *args[] = {&p};
-      MB_CUDA(cudaLaunchKernel(fn, dim3((unsigned)((p.total + 255) / 256)), dim3(256), args, 0, s));
+      MB_CUDA(cudaLaunchKernel(fn, grid_of(p), dim3(256), args, 0, s));
     }
   MB_CUDA(cudaEventRecord(e0, s));
   for (int it = 0; it < n; it++)
     for (auto &p : ps) {
       void *args[] = {&p};
-      MB_CUDA(cudaLaunchKernel(fn, dim3((unsigned)((p.total + 255) / 256)), dim3(256), args, 0, s));
+      MB_CUDA(cudaLaunchKernel(fn, grid_of(p), dim3(256), args, 0, s));
     }
   MB_CUDA(cudaEventRecord(e1, s));
   MB_CUDA(cudaEventSynchronize(e1));

@@ -62,11 +62,15 @@ struct SplTask {
 };
 
 enum NodeKind { NK_STB = 0, NK_REC = 1, NK_SPL = 2 };
+// cells a block-step node updates: all, those at distance >= 2 from the block
+// edge (they read nothing an interface op writes), or the distance <= 1 rim
+enum StbRegion { STB_ALL = 0, STB_INTERIOR = 1, STB_RIM = 2 };
 
 struct PlanNode {
   NodeKind kind;
   int level = -1;             // STB
   int a0 = 0, a1 = 0;         // STB: block range [a0, a1)
+  int region = STB_ALL;       // STB: StbRegion
   uint64_t parity = 0;        // STB: current buffer of each block before the step
   int macro_all = 0;          // STB: write rho/u of every FLUID cell
   std::vector<Rec> recs;      // REC
@@ -109,6 +113,8 @@ struct PlanCompiler {
   const std::vector<BlockLayout> &bl;
   const std::vector<std::vector<uint8_t>> &flags;  // per block, pitched
   const std::vector<SplLine> &spl_lines;
+  // levels with at least this many cells step their interior and rim as two nodes
+  long long split_cells = 1000000;
   PlanCompiler(const mb_geometry &g_, const std::vector<BlockLayout> &bl_,
                const std::vector<std::vector<uint8_t>> &fl, const std::vector<SplLine> &sl)
       : g(g_), bl(bl_), flags(fl), spl_lines(sl) {}

@@ -44,10 +44,15 @@ inline uint64_t key(uint64_t kind, uint64_t owner, uint64_t idx) { return (kind 
 inline uint32_t summ(uint64_t k) { return uint32_t(k >> 48); }  // kind<<8 | owner
 inline uint64_t fkey(int buf, int block, long long cell) { return key(buf ? RK_F1 : RK_F0, block, cell); }
 
+// A whole-block access of a block step: every cell of block `s & 0xff` whose
+// distance to the block edge lies in [dlo, dhi] (FLUID cells only if
+// fluid_only: the rho/u written by the step).
 struct Whole {
   uint32_t s;       // kind<<8 | block
-  bool fluid_only;  // only FLUID cells of the block (rho/u written by the block step)
+  bool fluid_only;
+  uint8_t dlo, dhi;
 };
+constexpr uint8_t DMAX = 255;
 
 struct Access {
   std::unordered_set<uint64_t> r, w;
@@ -55,8 +60,11 @@ struct Access {
   std::set<uint32_t> rs, ws;  // summaries of r / w keys and whole entries
   void read(uint64_t k) { r.insert(k); rs.insert(summ(k)); }
   void write(uint64_t k) { w.insert(k); ws.insert(summ(k)); }
-  void read_whole(uint32_t s) { wr.push_back({s, false}); rs.insert(s); }
-  void write_whole(uint32_t s, bool fo) { ww.push_back({s, fo}); ws.insert(s); }
+  void read_whole(uint32_t s, uint8_t dlo = 0, uint8_t dhi = DMAX) { wr.push_back({s, false, dlo, dhi}); rs.insert(s); }
+  void write_whole(uint32_t s, bool fo, uint8_t dlo = 0, uint8_t dhi = DMAX) {
+    ww.push_back({s, fo, dlo, dhi});
+    ws.insert(s);
+  }
   void merge(const Access &o) {
     for (auto k : o.r) r.insert(k);
     for (auto k : o.w) w.insert(k);
@@ -75,6 +83,13 @@ bool sets_intersect(const std::set<uint32_t> &a, const std::set<uint32_t> &b) {
     if (*i < *j) ++i; else ++j;
   }
   return false;
+}
+
+// distance ranges [lo, hi] a block-step region reads and writes
+void region_ranges(int region, uint8_t &rlo, uint8_t &rhi, uint8_t &wlo, uint8_t &whi) {
+  if (region == STB_INTERIOR) { rlo = 1; rhi = DMAX; wlo = 2; whi = DMAX; }
+  else if (region == STB_RIM) { rlo = 0; rhi = 2; wlo = 0; whi = 1; }
+  else { rlo = 0; rhi = DMAX; wlo = 0; whi = DMAX; }
 }
 
 }  // namespace
@@ -210,6 +225,18 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
   const mb_layout &L = g.layout;
   auto pitch_cell = [&](int a, int i, int j) -> long long { return (long long)j * bl[a].pitch + i; };
   auto is_fluid = [&](int a, long long cell) { return (flags[a][cell] & 3) == CT_FLUID; };
+  auto edge_dist = [&](int a, long long cell) -> int {
+    const int i = int(cell % bl[a].pitch), j = int(cell / bl[a].pitch);
+    return std::min(std::min(i, j), std::min(bl[a].nx - 1 - i, bl[a].ny - 1 - j));
+  };
+  auto covers = [&](const Whole &wh, uint64_t k) {
+    if (summ(k) != wh.s) return false;
+    const int blk = int((k >> 48) & 0xff);
+    const long long cell = (long long)(k & 0xffffffffffffull);
+    const int d = edge_dist(blk, cell);
+    if (d < wh.dlo || d > wh.dhi) return false;
+    return !wh.fluid_only || is_fluid(blk, cell);
+  };
 
   // One write of an op (the F part or the M part of a record, or the rho/u
   // write of a spline point) with the reads it needs.
@@ -242,21 +269,28 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
       I.stb = true;
       I.level = o.level;
       I.parity = o.parity;
+      long long level_cells = 0;
+      for (int a = L.ASP[o.level]; a < L.ASP[o.level + 1]; a++) level_cells += (long long)bl[a].nx * bl[a].ny;
+      const bool split = level_cells >= split_cells;
       for (int a0 = L.ASP[o.level]; a0 < L.ASP[o.level + 1]; a0 += 16) {
-        PlanNode nd;
-        nd.kind = NK_STB;
-        nd.level = o.level;
-        nd.macro_all = o.macro_all;
         const int a1 = std::min(L.ASP[o.level + 1], a0 + 16);
-        for (int a = a0; a < a1; a++)
-          if (o.parity[a]) nd.parity |= (1ull << a);
-        char lab[64];
-        std::snprintf(lab, sizeof lab, "stb L%d a%d-%d", o.level, a0, a1 - 1);
-        nd.label = lab;
-        nd.a0 = a0;
-        nd.a1 = a1;
-        nodes.push_back(nd);
-        acc.push_back(Access());
+        for (int region : split ? std::vector<int>{STB_RIM, STB_INTERIOR} : std::vector<int>{STB_ALL}) {
+          PlanNode nd;
+          nd.kind = NK_STB;
+          nd.level = o.level;
+          nd.macro_all = o.macro_all;
+          nd.region = region;
+          for (int a = a0; a < a1; a++)
+            if (o.parity[a]) nd.parity |= (1ull << a);
+          char lab[64];
+          std::snprintf(lab, sizeof lab, "stb L%d a%d-%d %s", o.level, a0, a1 - 1,
+                        region == STB_RIM ? "rim" : (region == STB_INTERIOR ? "int" : ""));
+          nd.label = lab;
+          nd.a0 = a0;
+          nd.a1 = a1;
+          nodes.push_back(nd);
+          acc.push_back(Access());
+        }
       }
       continue;
     }
@@ -434,10 +468,14 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
   // ---- backward liveness: drop writes overwritten before any read ----------
   // state of a key = kind of its nearest later access (true: a write).  Keys
   // never touched later are read (the state after the plan is observable).
+  // Block steps set the state of whole regions (layers, newest last); point
+  // accesses override single keys until a newer layer covers them.
+  struct Layer {
+    Whole w;
+    bool write;
+  };
   struct SummState {
-    bool dflt_write = false;        // default for keys of this (kind, block)
-    bool fluid_write = false;       // M only: default for FLUID cells
-    bool has_fluid = false;
+    std::vector<Layer> layers;
     std::unordered_map<uint64_t, bool> ov;
   };
   std::unordered_map<uint32_t, SummState> st;
@@ -446,32 +484,29 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
     if (it == st.end()) return false;
     auto o2 = it->second.ov.find(k);
     if (o2 != it->second.ov.end()) return o2->second;
-    if ((k >> 56) == RK_M && it->second.has_fluid) {
-      const int blk = int((k >> 48) & 0xff);
-      if (is_fluid(blk, (long long)(k & 0xffffffffffffull))) return it->second.fluid_write;
-    }
-    return it->second.dflt_write;
+    for (auto l = it->second.layers.rbegin(); l != it->second.layers.rend(); ++l)
+      if (covers(l->w, k)) return l->write;
+    return false;
   };
   auto set_state = [&](uint64_t k, bool w) { st[summ(k)].ov[k] = w; };
+  auto apply_layer = [&](const Whole &wh, bool write) {
+    SummState &ss = st[wh.s];
+    for (auto it = ss.ov.begin(); it != ss.ov.end();) {
+      if (covers(wh, it->first)) it = ss.ov.erase(it);
+      else ++it;
+    }
+    ss.layers.push_back({wh, write});
+  };
   for (int oi = int(ops.size()) - 1; oi >= 0; oi--) {
     OpInfo &I = info[oi];
     if (I.stb) {
+      // the op's nodes together write F of buffer 1-p and rho/u of FLUID
+      // cells and read F of buffer p, over the whole block
       for (int a = L.ASP[I.level]; a < L.ASP[I.level + 1]; a++) {
         const int p = I.parity[a];
-        // writes F of buffer 1-p and rho/u of FLUID cells, reads F of buffer p
-        SummState &w = st[uint32_t(((p ? RK_F0 : RK_F1) << 8) | a)];
-        w.ov.clear();
-        w.dflt_write = true;
-        SummState &m = st[uint32_t((RK_M << 8) | a)];
-        for (auto it = m.ov.begin(); it != m.ov.end();) {
-          if (is_fluid(a, (long long)(it->first & 0xffffffffffffull))) it = m.ov.erase(it);
-          else ++it;
-        }
-        m.has_fluid = true;
-        m.fluid_write = true;
-        SummState &r = st[uint32_t(((p ? RK_F1 : RK_F0) << 8) | a)];
-        r.ov.clear();
-        r.dflt_write = false;
+        apply_layer({uint32_t(((p ? RK_F0 : RK_F1) << 8) | a), false, 0, DMAX}, true);
+        apply_layer({uint32_t((RK_M << 8) | a), true, 0, DMAX}, true);
+        apply_layer({uint32_t(((p ? RK_F1 : RK_F0) << 8) | a), false, 0, DMAX}, false);
       }
       continue;
     }
@@ -495,11 +530,13 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
   std::vector<Access> fin(nodes.size());
   for (size_t q = 0; q < nodes.size(); q++) {
     if (nodes[q].kind != NK_STB) continue;
+    uint8_t rlo, rhi, wlo, whi;
+    region_ranges(nodes[q].region, rlo, rhi, wlo, whi);
     for (int a = nodes[q].a0; a < nodes[q].a1; a++) {
       const int p = int((nodes[q].parity >> a) & 1);
-      fin[q].read_whole(uint32_t(((p ? RK_F1 : RK_F0) << 8) | a));
-      fin[q].write_whole(uint32_t(((p ? RK_F0 : RK_F1) << 8) | a), false);
-      fin[q].write_whole(uint32_t((RK_M << 8) | a), true);
+      fin[q].read_whole(uint32_t(((p ? RK_F1 : RK_F0) << 8) | a), rlo, rhi);
+      fin[q].write_whole(uint32_t(((p ? RK_F0 : RK_F1) << 8) | a), false, wlo, whi);
+      fin[q].write_whole(uint32_t((RK_M << 8) | a), true, wlo, whi);
     }
   }
   for (auto &I : info) {
@@ -536,12 +573,8 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
   // ---- DAG edges: every earlier node that conflicts with a later one ------
   const int n = int(nodes.size());
   auto whole_hits_keys = [&](const Whole &wh, const std::unordered_set<uint64_t> &keys) {
-    for (auto k : keys) {
-      if (summ(k) != wh.s) continue;
-      if (!wh.fluid_only) return true;
-      const int blk = int((k >> 48) & 0xff);
-      if (is_fluid(blk, (long long)(k & 0xffffffffffffull))) return true;
-    }
+    for (auto k : keys)
+      if (covers(wh, k)) return true;
     return false;
   };
   auto conflict = [&](const Access &p, const Access &q) {
@@ -559,7 +592,7 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
                         const std::vector<Whole> &wb) {
       for (auto &x : wa) {
         for (auto &y : wb)
-          if (x.s == y.s) return true;
+          if (x.s == y.s && x.dlo <= y.dhi && y.dlo <= x.dhi) return true;
         if (whole_hits_keys(x, kb)) return true;
       }
       return false;

@@ -22,8 +22,9 @@ MB_MAX_LINE = 128
 MB_MAX_LINE2 = 128
 
 MB_OK = 0
-PREC_F64, PREC_F32, PREC_F16S = 0, 1, 2
-PRECISIONS = {"f64": PREC_F64, "f32": PREC_F32, "f16s": PREC_F16S}
+PREC_F64, PREC_F32, PREC_F16S, PREC_F32U = 0, 1, 2, 3
+# f32: FP32 storage of f - w (the product FP32 form); f32u: FP32 storage of f
+PRECISIONS = {"f64": PREC_F64, "f32": PREC_F32, "f16s": PREC_F16S, "f32u": PREC_F32U}
 FLUID, SOLID_SBB, C_BOUNDARY = 0, 1, 9
 OBST_CIRCLE, OBST_ELLIPSE = 0, 1
 
@@ -126,6 +127,8 @@ SIGNATURES = {
     "mb_init": ([_vp, _vp], C.c_int),
     "mb_step": ([_vp, C.c_int, _vp], C.c_int),
     "mb_set_graph_mode": ([_vp, C.c_int], C.c_int),
+    "mb_set_split_cells": ([_vp, C.c_longlong], C.c_int),
+    "mb_set_stb_variant": ([_vp, C.c_int, C.c_int], C.c_int),
     "mb_prepare": ([_vp, C.c_int], C.c_int),
     "mb_block_step": ([_vp, C.c_int, _vp], C.c_int),
     "mb_c_c_boundary_transfer": ([_vp, C.c_int, _vp], C.c_int),
@@ -293,6 +296,14 @@ class MultiBlockLBM:
     def evolution(self, n_coarse=1, stream=None):
         _check(self.lib.mb_step(self.h, int(n_coarse), _stream_ptr(stream)), "mb_step")
         self.n += n_coarse
+
+    def set_split_cells(self, cells):
+        """Levels with >= cells cells step interior and rim as separate graph nodes."""
+        _check(self.lib.mb_set_split_cells(self.h, int(cells)), "mb_set_split_cells")
+
+    def set_stb_variant(self, level, variant):
+        """Block-step kernel of a level: 0 one cell per thread, 1 four cells per thread."""
+        _check(self.lib.mb_set_stb_variant(self.h, int(level), int(variant)), "mb_set_stb_variant")
 
     def prepare(self, n_coarse):
         """Compiles the plans and graphs that evolution(n_coarse) will replay."""
