@@ -182,8 +182,12 @@ long long region_cells(int nx, int ny, int region) {
   return region == STB_INTERIOR ? in : (region == STB_RIM ? all - in : all);
 }
 
-StbParams make_stb(mb_ctx *c, int a0, int a1, uint64_t parity, int macro_all, int write_macros,
-                   int region = STB_ALL) {
+bool stb_uses_quads(const mb_ctx *c, int level, int region);
+
+// Launch parameters of a block-step node.  total counts cells for the
+// one-cell-per-thread kernel and warp tiles for the quad kernel (quads).
+StbParams make_stb(mb_ctx *c, int a0, int a1, uint64_t parity, int macro_all, int write_macros, int region,
+                   bool quads) {
   StbParams p{};
   p.nblk = a1 - a0;
   p.macro_all = macro_all;
@@ -218,7 +222,7 @@ StbParams make_stb(mb_ctx *c, int a0, int a1, uint64_t parity, int macro_all, in
     s.wt0 = wt;
     wt += (long long)s.tiles_x * nrows;
   }
-  p.total = region == STB_RIM ? cell : wt;
+  p.total = quads ? wt : cell;
   return p;
 }
 
@@ -235,9 +239,10 @@ int lower_plan(mb_ctx *c, CompiledPlan &cp) {
     d.kind = n.kind;
     d.deps = n.deps;
     if (n.kind == NK_STB) {
-      d.stb = make_stb(c, n.a0, n.a1, n.parity, n.macro_all, 1, n.region);
+      const bool quads = stb_uses_quads(c, n.level, n.region);
+      d.stb = make_stb(c, n.a0, n.a1, n.parity, n.macro_all, 1, n.region, quads);
       d.block = dim3(256);
-      if (stb_uses_quads(c, n.level, n.region)) {
+      if (quads) {
         d.func = kfunc<KStbQ>(c->prec);
         d.grid = dim3((unsigned)((d.stb.total + 7) / 8));  // 8 warp tiles per CTA
       } else {
@@ -1015,7 +1020,7 @@ extern "C" int mb_time_block_step(mb_ctx *c, int level, int n, mb_stream stream,
   long long tot = 0;
   for (int a0 = L.ASP[level]; a0 < L.ASP[level + 1]; a0 += STB_MAX_BLOCKS) {
     const int a1 = std::min(L.ASP[level + 1], a0 + STB_MAX_BLOCKS);
-    ps.push_back(make_stb(c, a0, a1, par, 0, 0));
+    ps.push_back(make_stb(c, a0, a1, par, 0, 0, STB_ALL, stb_uses_quads(c, level, STB_ALL)));
     for (int a = a0; a < a1; a++) tot += (long long)c->blk[a].nx * c->blk[a].ny;
   }
   const bool quads = stb_uses_quads(c, level, STB_ALL);
