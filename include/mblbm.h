@@ -207,6 +207,31 @@ int mb_write_tecplot(mb_ctx *ctx, const char *path);
 int mb_append_drag(const char *path, int t, double cd, double cl);
 int mb_append_error_L2(const char *path, int t, double e);
 
+/* ---- relative L2 change without any device allocation -------------------- */
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory: an application that owns the device through its own memory pool,
+ * or a time-stepping loop that must not pay the device-wide synchronisation
+ * of cudaMalloc/cudaFree.  The caller passes its own device arrays (FP64,
+ * dense) per segment and a device output of 3 doubles:
+ *   out[0] = sum over segments of weight * sum |u - u_prev|^2,
+ *   out[1] = sum of weight * sum |u|^2,   out[2] = sqrt(out[0]) / sqrt(out[1]),
+ * and u_prev <- u, the sums of error_L2 (lbm/error_L2.h:57-91) with weight
+ * 1/m per block.  Scratch is a fixed array inside the library (one copy per
+ * device, kept until exit); the first call on a device looks up its address
+ * and should come before any stream capture.  Calls share that array, so
+ * calls that overlap on the GPU race.  Returns MB_ERR_UNSUPPORTED beyond the
+ * limits below.  Asynchronous on `stream`. */
+#define MB_L2_NOALLOC_MAX_SEGMENTS 64
+#define MB_L2_NOALLOC_MAX_CTAS 1184
+#define MB_L2_NOALLOC_MAX_CELLS (1LL << 40)
+typedef struct {
+  const double *ux, *uy; /* current velocity, n values each (device) */
+  double *upx, *upy;     /* previous velocity (device); overwritten with ux, uy */
+  long long n;           /* cells in this segment */
+  double weight;         /* factor of this segment's sums */
+} mb_l2_segment;
+int mb_error_L2_noalloc(const mb_l2_segment *segs, int nseg, double *d_out, mb_stream stream);
+
 /* ---- introspection ------------------------------------------------------- */
 /* Number of kernels launched by the last mb_step call, and in one coarse step. */
 int mb_stats(mb_ctx *ctx, long long *kernels_last_step_call, long long *kernels_per_coarse_step,

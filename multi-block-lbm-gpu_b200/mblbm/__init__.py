@@ -110,6 +110,15 @@ class Geometry(C.Structure):
     ]
 
 
+class L2Segment(C.Structure):
+    """mb_l2_segment: device pointers of one segment for mb_error_L2_noalloc."""
+
+    _fields_ = [("ux", C.c_void_p), ("uy", C.c_void_p), ("upx", C.c_void_p), ("upy", C.c_void_p),
+                ("n", C.c_longlong), ("weight", C.c_double)]
+
+
+MB_L2_NOALLOC_MAX_SEGMENTS = 64
+
 # every symbol declared in include/mblbm.h, with its ctypes signature
 _vp = C.c_void_p
 _pd = C.POINTER(C.c_double)
@@ -148,6 +157,7 @@ SIGNATURES = {
     "mb_append_error_L2": ([C.c_char_p, C.c_int, C.c_double], C.c_int),
     "mb_stats": ([_vp, _pll, _pll, _pll], C.c_int),
     "mb_time_block_step": ([_vp, C.c_int, C.c_int, _vp, _pd, _pd, _pll], C.c_int),
+    "mb_error_L2_noalloc": ([C.POINTER(L2Segment), C.c_int, C.c_void_p, _vp], C.c_int),
 }
 
 _lib = None
@@ -250,6 +260,13 @@ def updates_per_coarse_step(geo):
         for a in range(L.ASP[l], L.ASP[l + 1]):
             tot += steps * geo.Areas[a].nx * geo.Areas[a].ny
     return tot
+
+
+def error_L2_noalloc(segments, d_out, stream=None):
+    """mb_error_L2_noalloc over [(ux, uy, upx, upy, n, weight), ...] device pointers;
+    writes sum w|u-up|^2, sum w|u|^2 and their root ratio to the 3 doubles at d_out."""
+    arr = (L2Segment * max(1, len(segments)))(*[L2Segment(*s) for s in segments])
+    return load().mb_error_L2_noalloc(arr, len(segments), d_out, _stream_ptr(stream))
 
 
 def _stream_ptr(stream):
