@@ -160,10 +160,12 @@ int mb_init(mb_ctx *ctx, mb_stream stream);
 /* n coarse steps of evolution(level 0) (evolution.h:2-65).  The last coarse
  * step of every call leaves rho/ux/uy of all cells up to date, as the
  * reference's stb2 does each step; earlier steps keep only the macroscopic
- * values that interface transfers read. use_graph: 1 = replay a CUDA graph of
- * the dependency DAG (default), 0 = launch the kernels one by one. */
+ * values that interface transfers read. */
 int mb_step(mb_ctx *ctx, int n_coarse, mb_stream stream);
-int mb_set_graph_mode(mb_ctx *ctx, int use_graph);
+/* 0: launch the kernels one by one; 1: replay CUDA graphs of the dependency
+ * DAG (default); 2: graphs whose kernel-to-kernel edges are programmatic, so a
+ * consumer is scheduled while its producers drain. */
+int mb_set_graph_mode(mb_ctx *ctx, int mode);
 /* Levels with at least `cells` cells update their interior (cells two or more
  * from a block edge) and their rim as separate DAG nodes, so that the interior
  * of the next coarse step overlaps the fine levels of this one.  Default 1e6;
@@ -172,6 +174,10 @@ int mb_set_split_cells(mb_ctx *ctx, long long cells);
 /* Block-step kernel of one level: 0 = one cell per thread (default),
  * 1 = four cells per thread with vector loads.  Results are identical. */
 int mb_set_stb_variant(mb_ctx *ctx, int level, int variant);
+/* Caps the grid of interior (bulk) block-step launches at ctas_per_sm CTAs of
+ * 256 threads per SM (0 = uncapped), leaving CTA slots on every SM for the
+ * fine-level kernels that run beside them. */
+int mb_set_bulk_occupancy(mb_ctx *ctx, int ctas_per_sm);
 /* Compiles the plans (and CUDA graphs) that mb_step(ctx, n) will replay from
  * the current state, so the step call itself spends no host time on them. */
 int mb_prepare(mb_ctx *ctx, int n_coarse);
@@ -206,6 +212,15 @@ int mb_write_tecplot(mb_ctx *ctx, const char *path);
 /* Line "t\tCd\tCl\t" / "t\terr" appended as in force_block.h:212-215 / error_L2.h:85-88. */
 int mb_append_drag(const char *path, int t, double cd, double cl);
 int mb_append_error_L2(const char *path, int t, double e);
+
+/* ---- checkpoint / restart (no counterpart in the reference) -------------- */
+/* The raw device state (both distribution buffers, rho/u, u_prev, ring slots,
+ * scheduler state) in a caller-provided host buffer of mb_checkpoint_size
+ * bytes; loading it into a context built from the same geometry and precision
+ * restarts bit-exactly.  Both calls synchronise the stream. */
+int mb_checkpoint_size(mb_ctx *ctx, long long *bytes);
+int mb_checkpoint_save(mb_ctx *ctx, void *host, long long bytes, mb_stream stream);
+int mb_checkpoint_load(mb_ctx *ctx, const void *host, long long bytes, mb_stream stream);
 
 /* ---- relative L2 change without any device allocation -------------------- */
 /* No counterpart in the reference.  For callers that cannot allocate device

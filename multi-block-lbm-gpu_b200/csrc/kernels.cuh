@@ -53,6 +53,13 @@ __device__ __forceinline__ void st_f(typename Prec<P>::S *p, long long idx, int 
   else p[idx] = v;
 }
 
+// Programmatic dependent launch: a kernel lets the next one in the graph be
+// scheduled as soon as every CTA has started (pdl_trigger), and waits for its
+// own producers to finish and flush (pdl_wait) before it reads their output.
+// Both are no-ops when the launch has no programmatic dependency.
+__device__ __forceinline__ void pdl_trigger() { cudaTriggerProgrammaticLaunchCompletion(); }
+__device__ __forceinline__ void pdl_wait() { cudaGridDependencySynchronize(); }
+
 // feq, lbm/assit_func.h:2-9
 template <typename R>
 __device__ __forceinline__ R feq(int k, R rh, R uxx, R uyy) {
@@ -191,9 +198,13 @@ __device__ __forceinline__ void stb_cell(const StbParams &p, const StbBlk &B, in
 
 
 template <int P>
-__global__ void __launch_bounds__(256) k_block_step(const __grid_constant__ StbParams p) {
-  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= p.total) return;
+__global__ void __launch_bounds__(256, P == MB_PREC_F64 ? 4 : 8) k_block_step(const __grid_constant__ StbParams p) {
+  pdl_trigger();
+  bool waited = false;
+  // grid-stride: a capped grid (bulk interior work) leaves CTA slots on every
+  // SM for kernels that run beside it
+  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < p.total;
+       g += (long long)gridDim.x * blockDim.x) {
   int t = 0;
 #pragma unroll 1
   while (t + 1 < p.nblk && g >= p.b[t + 1].cell0) t++;
@@ -219,7 +230,12 @@ __global__ void __launch_bounds__(256) k_block_step(const __grid_constant__ StbP
     j = local / B.nx;
     i = local - j * B.nx;
   }
+  if (!waited) {
+    pdl_wait();
+    waited = true;
+  }
   stb_cell<P>(p, B, i, j);
+  }
 }
 
 // Four consecutive cells of a row in the stored form, as arithmetic values
@@ -261,9 +277,11 @@ template <int P>
 __global__ void __launch_bounds__(256) k_block_step_q(const __grid_constant__ StbParams p) {
   using R = typename Prec<P>::R;
   using S = typename Prec<P>::S;
+  pdl_trigger();
   const long long wt = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (wt >= p.total) return;  // warp-uniform
+  pdl_wait();
   int t = 0;
 #pragma unroll 1
   while (t + 1 < p.nblk && wt >= p.b[t + 1].wt0) t++;
@@ -355,19 +373,7 @@ struct IfBlk {
 // Interface point records: c_c_boundary_transfer, temporal_interpolation,
 // c_f_boundary_transfer, f_c_boundary_transfer (multi/FH/assit_multi.h).
 // ----------------------------------------------------------------------------
-struct RecDev {
-  uint8_t type, bits, dst_block, src_block;
-  uint8_t m0, m1, m2, pad;
-  int32_t dst_cell, src;
-};
 constexpr int REC_THREADS = 64;
-struct RecParams {
-  const RecDev *recs;
-  int n, pad_;
-  const IfBlk *blk;
-  void *slots;
-  double tw[4][3];
-};
 // Per-block fields the record kernel touches, as launch parameters: a record's
 // first access then depends on one load (the record), not on the block table.
 constexpr int REC_MAX_BLOCKS = 40;
@@ -378,28 +384,51 @@ struct RecBlk {
   double tau;
   int m, pad_;
 };
-struct RecParamsB {
-  RecParams r;
-  RecBlk b[REC_MAX_BLOCKS];
+
+
+// One reference line op of a record launch.  Its points are affine in the
+// point index ip: target cell dst0 + ip*dstride, source (cell or slot point)
+// src0 + ip*sstride.  Points whose writes the plan dropped are marked in the
+// per-point mask (bits 4: F, 8: rho/u); has_mask = 0 means all writes live.
+constexpr int REC_MAX_OPS = 24;
+struct RecOp {
+  uint8_t type, dst_block, src_block, bits;  // bits: RB_* buffer bits and weight index
+  uint8_t m0, m1, m2, has_mask;
+  int32_t count, dst0, dstride, src0, sstride, mask_off;
 };
-static_assert(sizeof(RecParamsB) <= 4096, "record launch parameters must fit the 4 KB parameter space");
+struct RecOpsParams {
+  int nops, total;
+  int op_start[REC_MAX_OPS + 1];
+  RecOp ops[REC_MAX_OPS];
+  RecBlk b[REC_MAX_BLOCKS];
+  void *slots;
+  const uint8_t *mask;
+  double tw[4][3];
+};
+static_assert(sizeof(RecOpsParams) <= 4096, "record launch parameters must fit the 4 KB parameter space");
 
 template <int P>
-__global__ void __launch_bounds__(REC_THREADS) k_records(const __grid_constant__ RecParamsB pb) {
+__global__ void __launch_bounds__(REC_THREADS) k_records(const __grid_constant__ RecOpsParams p) {
   using R = typename Prec<P>::R;
   using S = typename Prec<P>::S;
-  const RecParams &p = pb.r;
+  pdl_trigger();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= p.n) return;
-  const RecDev r = p.recs[t];
-  const RecBlk &D = pb.b[r.dst_block];
-  S *Fd = (S *)D.F[(r.bits >> 1) & 1];
-  const long long dc = r.dst_cell;
-  const bool wF = r.bits & 4, wM = r.bits & 8;
-  if (r.type == 0) {  // same-level copy (assit_multi.h:2-46)
-    const RecBlk &A = pb.b[r.src_block];
-    const S *Fs = (const S *)A.F[r.bits & 1];
-    const long long sc = r.src;
+  if (t >= p.total) return;
+  int o = 0;
+#pragma unroll 1
+  while (o + 1 < p.nops && t >= p.op_start[o + 1]) o++;
+  const RecOp &op = p.ops[o];
+  const int ip = t - p.op_start[o];
+  const long long dc = (long long)op.dst0 + (long long)ip * op.dstride;
+  const long long sc = (long long)op.src0 + (long long)ip * op.sstride;
+  pdl_wait();
+  const uint8_t live = op.has_mask ? p.mask[op.mask_off + ip] : op.bits;
+  const bool wF = live & 4, wM = live & 8;
+  const RecBlk &D = p.b[op.dst_block];
+  S *Fd = (S *)D.F[(op.bits >> 1) & 1];
+  if (op.type == 0) {  // same-level copy (assit_multi.h:2-46)
+    const RecBlk &A = p.b[op.src_block];
+    const S *Fs = (const S *)A.F[op.bits & 1];
     if (wM) {
       ((R *)D.rho)[dc] = ((const R *)A.rho)[sc];
       ((R *)D.ux)[dc] = ((const R *)A.ux)[sc];
@@ -411,25 +440,24 @@ __global__ void __launch_bounds__(REC_THREADS) k_records(const __grid_constant__
     }
     return;
   }
-  if (r.type == 1 || r.type == 2) {  // temporal interpolation (:213-247) / c_f (:249-271)
+  if (op.type == 1 || op.type == 2) {  // temporal interpolation (:213-247) / c_f (:249-271)
     if (!wF) return;
-    const R *s = (const R *)p.slots + (long long)r.src * 27;
-    if (r.type == 1) {
-      const int wi = (r.bits >> 4) & 3;
+    const R *s = (const R *)p.slots + sc * 27;
+    if (op.type == 1) {
+      const int wi = (op.bits >> 4) & 3;
       const R a = (R)p.tw[wi][0], b = (R)p.tw[wi][1], cc = (R)p.tw[wi][2];
 #pragma unroll
       for (int k = 0; k < 9; k++)
-        st_f<P>(Fd, k * D.plane + dc, k, a * s[r.m0 * 9 + k] - b * s[r.m1 * 9 + k] + cc * s[r.m2 * 9 + k]);
+        st_f<P>(Fd, k * D.plane + dc, k, a * s[op.m0 * 9 + k] - b * s[op.m1 * 9 + k] + cc * s[op.m2 * 9 + k]);
     } else {
 #pragma unroll
-      for (int k = 0; k < 9; k++) st_f<P>(Fd, k * D.plane + dc, k, s[r.m2 * 9 + k]);
+      for (int k = 0; k < 9; k++) st_f<P>(Fd, k * D.plane + dc, k, s[op.m2 * 9 + k]);
     }
     return;
   }
   // f_c (:273-314): coarse edge <- fine point, f_neq scaled by r (tau_c-1)/(tau_f-1)
-  const RecBlk &Fb = pb.b[r.src_block];
-  const S *Fs = (const S *)Fb.F[r.bits & 1];
-  const long long sc = r.src;
+  const RecBlk &Fb = p.b[op.src_block];
+  const S *Fs = (const S *)Fb.F[op.bits & 1];
   const R rh = ((const R *)Fb.rho)[sc], ux = ((const R *)Fb.ux)[sc], uy = ((const R *)Fb.uy)[sc];
   if (wM) {
     ((R *)D.rho)[dc] = rh;
@@ -451,17 +479,6 @@ __global__ void __launch_bounds__(REC_THREADS) k_records(const __grid_constant__
 // Spatial interpolation: init_Spline3 + tridiagonal solve + calculate_Spline3_gpu
 // (assit_multi.h:48-211) for one coarse-fine line per CTA.
 // ----------------------------------------------------------------------------
-struct SplLineDev {
-  int coarse, fine, Nc, Nf, r;
-  int ci0, cj0, cdi, cdj;
-  int fi0, fj0, fdi, fdj;
-  int slot0;
-  int coef0;  // offset of the line's c' table (in units of 2 values per row)
-  double para;
-};
-struct SplTaskDev {
-  int line, src_buf, m0, mask_off;
-};
 
 // Spline3_S (:118-134), with its 0.1666667 constant
 template <typename R>
@@ -473,19 +490,6 @@ __device__ __forceinline__ R spline3_s(R xx, R x_1, R h, R fi_1, R fi, R mi_1, R
   const R c = (fi_1 - mi_1 * h * h * s6) * (x - xx);
   const R d = (fi - mi * h * h * s6) * (xx - x_1);
   return a + b + c + d;
-}
-
-// gather the 12 fields (rho, ux, uy, F0..F8) of coarse point ip
-template <int P>
-__device__ __forceinline__ void spl_gather(const SplLineDev &L, const IfBlk &C, const typename Prec<P>::S *Fc,
-                                           int ip, typename Prec<P>::R *v) {
-  using R = typename Prec<P>::R;
-  const long long c = (long long)(L.cj0 + ip * L.cdj) * C.pitch + (L.ci0 + ip * L.cdi);
-  v[0] = ((const R *)C.rho)[c];
-  v[1] = ((const R *)C.ux)[c];
-  v[2] = ((const R *)C.uy)[c];
-#pragma unroll
-  for (int k = 0; k < 9; k++) v[3 + k] = ld_f<P>(Fc, k * C.plane + c, k);
 }
 
 // Spatial interpolation, one warp per segment of SPL_SEG intervals of a
@@ -505,22 +509,46 @@ template <typename R> struct SplHalo { static constexpr int v = 16; };
 template <> struct SplHalo<double> { static constexpr int v = 28; };
 template <typename R> __host__ __device__ constexpr int spl_win() { return SPL_SEG + 2 * SplHalo<R>::v + 4; }
 
-struct SplSegDev {
-  int task, seg;
+// Everything a spline warp needs about its line, as launch parameters (no
+// dependent loads before the gather).
+constexpr int SPL_MAX_TASKS = 16;
+struct SplTaskP {
+  int Nc, Nf, r, slot0;
+  int ci0, cj0, cdi, cdj;  // coarse source line: start and unit step
+  int fi0, fj0, fdi, fdj;  // fine edge line
+  int coef0, m0, mask_off, seg0;
+  double para;
+  const void *Fc;          // current F buffer of the coarse block
+  const void *Mc[3];       // coarse rho, ux, uy
+  void *Mf[3];             // fine rho, ux, uy
+  long long cplane;
+  int cpitch, fpitch;
 };
-struct SplParamsW {
-  const SplTaskDev *tasks;
-  const SplSegDev *segs;
-  int nseg, pad_;
-  const SplLineDev *lines;
-  const uint8_t *mask;
-  const IfBlk *blk;
+struct SplParamsP {
+  int ntask, nseg;
+  SplTaskP t[SPL_MAX_TASKS];
   void *slots;
-  const void *coef;  // per line: c'_i (Nc values) then 1/den_i (Nc values), at 2 * line.coef0
+  const uint8_t *mask;
+  const void *coef;  // per line: c'_i (Nc values) then 1/den_i (Nc values), at 2 * coef0
 };
+static_assert(sizeof(SplParamsP) <= 4096, "spline launch parameters must fit the 4 KB parameter space");
+
+// the 12 fields (rho, ux, uy, F0..F8) of coarse point ip
+template <int P>
+__device__ __forceinline__ void spl_gather_p(const SplTaskP &T, int ip, typename Prec<P>::R *v) {
+  using R = typename Prec<P>::R;
+  using S = typename Prec<P>::S;
+  const long long c = (long long)(T.cj0 + ip * T.cdj) * T.cpitch + (T.ci0 + ip * T.cdi);
+  v[0] = ((const R *)T.Mc[0])[c];
+  v[1] = ((const R *)T.Mc[1])[c];
+  v[2] = ((const R *)T.Mc[2])[c];
+  const S *F = (const S *)T.Fc;
+#pragma unroll
+  for (int k = 0; k < 9; k++) v[3 + k] = ld_f<P>(F, k * T.cplane + c, k);
+}
 
 template <int P>
-__global__ void __launch_bounds__(32 * SPL_WARPS) k_spline(const __grid_constant__ SplParamsW p) {
+__global__ void __launch_bounds__(32 * SPL_WARPS) k_spline(const __grid_constant__ SplParamsP p) {
   using R = typename Prec<P>::R;
   using S = typename Prec<P>::S;
   constexpr int H = SplHalo<R>::v;
@@ -531,24 +559,26 @@ __global__ void __launch_bounds__(32 * SPL_WARPS) k_spline(const __grid_constant
   Win *sx = sf + SPL_WARPS;             // [warp] forward sweep, then the moments
   R(*scf)[2][W] = (R(*)[2][W])(sx + SPL_WARPS);  // [warp] c'_i and 1/den_i of the window
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  pdl_trigger();
   const int sid = blockIdx.x * SPL_WARPS + warp;
   if (sid >= p.nseg) return;
-  const SplSegDev sg = p.segs[sid];
-  const SplTaskDev task = p.tasks[sg.task];
-  const SplLineDev L = p.lines[task.line];
-  const int N = L.Nc;
-  const IfBlk &C = p.blk[L.coarse];
-  const S *Fc = (const S *)C.F[task.src_buf];
-  const R *cpt = (const R *)p.coef + 2LL * L.coef0;
+  int tk = 0;
+#pragma unroll 1
+  while (tk + 1 < p.ntask && sid >= p.t[tk + 1].seg0) tk++;
+  const SplTaskP &T = p.t[tk];
+  const int seg = sid - T.seg0;
+  const int N = T.Nc;
+  const R *cpt = (const R *)p.coef + 2LL * T.coef0;
   const R *ivd = cpt + N;
 
   // intervals I in [Ilo, Ihi] (fine point ip uses rows I-1 and I, I = ceil(ip/r), at least 1)
-  const int Ilo = 1 + sg.seg * SPL_SEG, Ihi = min(N - 1, (sg.seg + 1) * SPL_SEG);
+  const int Ilo = 1 + seg * SPL_SEG, Ihi = min(N - 1, (seg + 1) * SPL_SEG);
   const int w0 = max(0, Ilo - 1 - H), w1 = min(N - 1, Ihi + H);  // rows solved
   const int g0 = max(0, w0 - 1), g1 = min(N - 1, w1 + 1);        // rows gathered
+  pdl_wait();
   for (int i = g0 + lane; i <= g1; i += 32) {
     R v[12];
-    spl_gather<P>(L, C, Fc, i, v);
+    spl_gather_p<P>(T, i, v);
 #pragma unroll
     for (int f = 0; f < 12; f++) sf[warp][f][i - g0] = v[f];
     scf[warp][0][i - g0] = cpt[i];
@@ -579,13 +609,12 @@ __global__ void __launch_bounds__(32 * SPL_WARPS) k_spline(const __grid_constant
   __syncwarp();
 
   // evaluate the fine points of the segment (calculate_Spline3_gpu :136-185)
-  const IfBlk &Fb = p.blk[L.fine];
   R *slots = (R *)p.slots;
-  const R para = (R)L.para;
-  const int ip0 = (sg.seg == 0) ? 0 : L.r * (Ilo - 1) + 1;
-  const int ip1 = min(L.Nf - 1, L.r * Ihi);
+  const R para = (R)T.para;
+  const int ip0 = (seg == 0) ? 0 : T.r * (Ilo - 1) + 1;
+  const int ip1 = min(T.Nf - 1, T.r * Ihi);
   for (int ip = ip0 + lane; ip <= ip1; ip += 32) {
-    const R xx = (R)ip / (R)L.r;
+    const R xx = (R)ip / (R)T.r;
     int I = (int)ceil(xx);
     if (I == 0) I = 1;
     R out[12];
@@ -593,13 +622,13 @@ __global__ void __launch_bounds__(32 * SPL_WARPS) k_spline(const __grid_constant
     for (int f = 0; f < 12; f++)
       out[f] = spline3_s<R>(xx, (R)(I - 1), (R)1.0, sf[warp][f][I - 1 - g0], sf[warp][f][I - g0],
                             sx[warp][f][I - 1 - g0], sx[warp][f][I - g0]);
-    const long long fc = (long long)(L.fj0 + ip * L.fdj) * Fb.pitch + (L.fi0 + ip * L.fdi);
-    if (task.mask_off < 0 || p.mask[task.mask_off + ip]) {
-      ((R *)Fb.rho)[fc] = out[0];
-      ((R *)Fb.ux)[fc] = out[1];
-      ((R *)Fb.uy)[fc] = out[2];
+    const long long fc = (long long)(T.fj0 + ip * T.fdj) * T.fpitch + (T.fi0 + ip * T.fdi);
+    if (T.mask_off < 0 || p.mask[T.mask_off + ip]) {
+      ((R *)T.Mf[0])[fc] = out[0];
+      ((R *)T.Mf[1])[fc] = out[1];
+      ((R *)T.Mf[2])[fc] = out[2];
     }
-    R *sl = slots + ((long long)(L.slot0 + ip) * 3 + task.m0) * 9;
+    R *sl = slots + ((long long)(T.slot0 + ip) * 3 + T.m0) * 9;
 #pragma unroll
     for (int k = 0; k < 9; k++) {
       const R fe = feq<R>(k, out[0], out[1], out[2]);

@@ -39,15 +39,15 @@ size_t real_bytes(int prec) { return prec == MB_PREC_F64 ? 8 : 4; }
 
 struct DevPlanNode {
   NodeKind kind;
+  bool background = false;  // bandwidth-bound bulk work: lowest scheduling priority
   // launch
   void *func = nullptr;
   dim3 grid, block;
   size_t smem = 0;
   // parameter blocks (one of them used)
   StbParams stb;
-  RecParamsB rec;
-  SplParamsW spl;
-  std::vector<SplSegDev> segs;
+  RecOpsParams rec;
+  SplParamsP spl;
   void *args[1];
   std::vector<int> deps;
 };
@@ -83,7 +83,7 @@ struct mb_ctx {
   void *d_slots = nullptr;
   long long n_slot_points = 0;
   std::vector<SplLine> spl_lines;
-  SplLineDev *d_spl_lines = nullptr;
+  std::vector<int> spl_coef0;  // per line: offset of its c' / 1/den table (units of 2 values)
   void *d_spl_coef = nullptr;  // per line: c'_i and 1/den_i of the spline system
   // drag
   int drag_area = 0;
@@ -111,6 +111,8 @@ struct mb_ctx {
   int period = 1;
   long long split_cells = 1000000;
   int stb_variant[MB_MAX_LEVEL] = {0};  // 0: one cell per thread, 1: quads (k_block_step_q)
+  int bulk_ctas_per_sm = 0;             // >0: cap interior (bulk) block-step grids at this many CTAs per SM
+  int num_sms = 148;
   std::map<std::string, std::unique_ptr<CompiledPlan>> plans;
   long long kernels_last_call = 0;
   long long kernels_per_step = 0;
@@ -241,65 +243,112 @@ int lower_plan(mb_ctx *c, CompiledPlan &cp) {
     if (n.kind == NK_STB) {
       const bool quads = stb_uses_quads(c, n.level, n.region);
       d.stb = make_stb(c, n.a0, n.a1, n.parity, n.macro_all, 1, n.region, quads);
+      d.background = (n.region == STB_INTERIOR);
       d.block = dim3(256);
       if (quads) {
         d.func = kfunc<KStbQ>(c->prec);
         d.grid = dim3((unsigned)((d.stb.total + 7) / 8));  // 8 warp tiles per CTA
       } else {
         d.func = kfunc<KStb>(c->prec);
-        d.grid = dim3((unsigned)((d.stb.total + 255) / 256));
+        long long ctas = (d.stb.total + 255) / 256;
+        if (d.background && c->bulk_ctas_per_sm > 0)
+          ctas = std::min<long long>(ctas, (long long)c->bulk_ctas_per_sm * c->num_sms);
+        d.grid = dim3((unsigned)ctas);
       }
       d.args[0] = &d.stb;
     } else if (n.kind == NK_REC) {
-      RecDev *dr = nullptr;
-      if (cudaMalloc(&dr, n.recs.size() * sizeof(RecDev)) != cudaSuccess) return MB_ERR_NOMEM;
-      cp.dev_allocs.push_back(dr);
-      if (cudaMemcpy(dr, n.recs.data(), n.recs.size() * sizeof(RecDev), cudaMemcpyHostToDevice) != cudaSuccess)
-        return MB_ERR_CUDA;
-      d.rec = RecParamsB{};
-      d.rec.r.recs = dr;
-      d.rec.r.n = (int)n.recs.size();
-      d.rec.r.blk = c->d_blk;
-      d.rec.r.slots = c->d_slots;
-      std::memcpy(d.rec.r.tw, n.tw, sizeof(n.tw));
+      if ((int)n.ops.size() > REC_MAX_OPS) return MB_ERR_UNSUPPORTED;
+      d.rec = RecOpsParams{};
+      std::vector<uint8_t> mask;
+      int total = 0;
+      for (size_t o = 0; o < n.ops.size(); o++) {
+        const int r0 = n.ops[o].first, cnt = n.ops[o].second;
+        const Rec &a = n.recs[r0];
+        RecOp &op = d.rec.ops[o];
+        op.type = a.type;
+        op.dst_block = a.dst_block;
+        op.src_block = a.src_block;
+        op.m0 = a.m0;
+        op.m1 = a.m1;
+        op.m2 = a.m2;
+        op.count = cnt;
+        op.dst0 = a.dst_cell;
+        op.src0 = a.src;
+        op.dstride = cnt > 1 ? n.recs[r0 + 1].dst_cell - a.dst_cell : 0;
+        op.sstride = cnt > 1 ? n.recs[r0 + 1].src - a.src : 0;
+        uint8_t full = 0, all_same = 1;
+        const uint8_t buf_bits = uint8_t(a.bits & ~(RB_WRITE_F | RB_WRITE_M));
+        for (int q = 0; q < cnt; q++) {
+          const Rec &r = n.recs[r0 + q];
+          // every op is a line: affine in the point index
+          if (r.dst_cell != op.dst0 + q * op.dstride || r.src != op.src0 + q * op.sstride ||
+              uint8_t(r.bits & ~(RB_WRITE_F | RB_WRITE_M)) != buf_bits)
+            return MB_ERR_INVALID;
+          full |= r.bits & (RB_WRITE_F | RB_WRITE_M);
+          if ((r.bits & (RB_WRITE_F | RB_WRITE_M)) != (a.bits & (RB_WRITE_F | RB_WRITE_M))) all_same = 0;
+        }
+        op.bits = all_same ? a.bits : uint8_t(buf_bits | full);
+        op.has_mask = all_same ? 0 : 1;
+        op.mask_off = (int)mask.size();
+        if (!all_same)
+          for (int q = 0; q < cnt; q++) mask.push_back(uint8_t(n.recs[r0 + q].bits & (RB_WRITE_F | RB_WRITE_M)));
+        d.rec.op_start[o] = total;
+        total += cnt;
+      }
+      d.rec.nops = (int)n.ops.size();
+      d.rec.op_start[n.ops.size()] = total;
+      d.rec.total = total;
+      uint8_t *dm = nullptr;
+      if (cudaMalloc(&dm, std::max<size_t>(mask.size(), 1)) != cudaSuccess) return MB_ERR_NOMEM;
+      cp.dev_allocs.push_back(dm);
+      if (!mask.empty()) MB_CUDA(cudaMemcpy(dm, mask.data(), mask.size(), cudaMemcpyHostToDevice));
+      d.rec.mask = dm;
+      d.rec.slots = c->d_slots;
+      std::memcpy(d.rec.tw, n.tw, sizeof(n.tw));
       for (int a = 0; a < c->nblk; a++) {
         const IfBlk &B = c->blk[a];
         d.rec.b[a] = {{B.F[0], B.F[1]}, B.rho, B.ux, B.uy, B.plane, B.tau, B.m, 0};
       }
       d.func = kfunc<KRec>(c->prec);
       d.block = dim3(REC_THREADS);  // small CTAs spread a launch's scattered accesses over many SMs
-      d.grid = dim3((unsigned)((n.recs.size() + REC_THREADS - 1) / REC_THREADS));
+      d.grid = dim3((unsigned)((total + REC_THREADS - 1) / REC_THREADS));
       d.args[0] = &d.rec;
     } else {
-      std::vector<SplTaskDev> tasks(n.spl.size());
+      if ((int)n.spl.size() > SPL_MAX_TASKS) return MB_ERR_UNSUPPORTED;
+      d.spl = SplParamsP{};
+      int nseg = 0;
       for (size_t t = 0; t < n.spl.size(); t++) {
-        tasks[t] = {n.spl[t].line, n.spl[t].src_buf, n.spl[t].m0, n.spl[t].mask_off};
-        const int nseg = (c->spl_lines[n.spl[t].line].Nc - 1 + SPL_SEG - 1) / SPL_SEG;
-        for (int g = 0; g < nseg; g++) d.segs.push_back({(int)t, g});
+        const SplLine &L = c->spl_lines[n.spl[t].line];
+        const IfBlk &Cb = c->blk[L.coarse], &Fb = c->blk[L.fine];
+        SplTaskP &T = d.spl.t[t];
+        T.Nc = L.Nc; T.Nf = L.Nf; T.r = L.r; T.slot0 = L.slot0;
+        T.ci0 = L.ci0; T.cj0 = L.cj0; T.cdi = L.cdi; T.cdj = L.cdj;
+        T.fi0 = L.fi0; T.fj0 = L.fj0; T.fdi = L.fdi; T.fdj = L.fdj;
+        T.coef0 = c->spl_coef0[n.spl[t].line];
+        T.m0 = n.spl[t].m0;
+        T.mask_off = n.spl[t].mask_off;
+        T.seg0 = nseg;
+        T.para = L.para;
+        T.Fc = Cb.F[n.spl[t].src_buf];
+        T.Mc[0] = Cb.rho; T.Mc[1] = Cb.ux; T.Mc[2] = Cb.uy;
+        T.Mf[0] = Fb.rho; T.Mf[1] = Fb.ux; T.Mf[2] = Fb.uy;
+        T.cplane = Cb.plane;
+        T.cpitch = Cb.pitch;
+        T.fpitch = Fb.pitch;
+        nseg += (L.Nc - 1 + SPL_SEG - 1) / SPL_SEG;
       }
-      SplTaskDev *dt = nullptr;
-      SplSegDev *dsg = nullptr;
+      d.spl.ntask = (int)n.spl.size();
+      d.spl.nseg = nseg;
       uint8_t *dm = nullptr;
-      if (cudaMalloc(&dt, tasks.size() * sizeof(SplTaskDev)) != cudaSuccess) return MB_ERR_NOMEM;
-      cp.dev_allocs.push_back(dt);
-      if (cudaMalloc(&dsg, d.segs.size() * sizeof(SplSegDev)) != cudaSuccess) return MB_ERR_NOMEM;
-      cp.dev_allocs.push_back(dsg);
       if (cudaMalloc(&dm, std::max<size_t>(n.spl_mask.size(), 1)) != cudaSuccess) return MB_ERR_NOMEM;
       cp.dev_allocs.push_back(dm);
-      MB_CUDA(cudaMemcpy(dt, tasks.data(), tasks.size() * sizeof(SplTaskDev), cudaMemcpyHostToDevice));
-      MB_CUDA(cudaMemcpy(dsg, d.segs.data(), d.segs.size() * sizeof(SplSegDev), cudaMemcpyHostToDevice));
       if (!n.spl_mask.empty()) MB_CUDA(cudaMemcpy(dm, n.spl_mask.data(), n.spl_mask.size(), cudaMemcpyHostToDevice));
-      d.spl.tasks = dt;
-      d.spl.segs = dsg;
-      d.spl.nseg = (int)d.segs.size();
-      d.spl.lines = c->d_spl_lines;
       d.spl.mask = dm;
-      d.spl.blk = c->d_blk;
       d.spl.slots = c->d_slots;
       d.spl.coef = c->d_spl_coef;
       d.func = kfunc<KSpl>(c->prec);
       d.block = dim3(32 * SPL_WARPS);
-      d.grid = dim3((unsigned)((d.segs.size() + SPL_WARPS - 1) / SPL_WARPS));
+      d.grid = dim3((unsigned)((nseg + SPL_WARPS - 1) / SPL_WARPS));
       d.smem = spline_smem(c->prec);
       d.args[0] = &d.spl;
     }
@@ -317,7 +366,19 @@ int run_direct(CompiledPlan &cp, cudaStream_t s) {
   return MB_OK;
 }
 
-int build_graph(CompiledPlan &cp) {
+// Interior nodes of split levels get the lowest priority and every other
+// kernel the highest: pending CTAs of the latency-bound fine-level chain are
+// then dispatched ahead of the queued bulk CTAs as SMs free up.
+int set_priority(cudaGraphNode_t node, bool background) {
+  int least = 0, greatest = 0;
+  MB_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+  cudaKernelNodeAttrValue v{};
+  v.priority = background ? least : greatest;
+  MB_CUDA(cudaGraphKernelNodeSetAttribute(node, cudaKernelNodeAttributePriority, &v));
+  return MB_OK;
+}
+
+int build_graph(CompiledPlan &cp, bool pdl) {
   MB_CUDA(cudaGraphCreate(&cp.graph, 0));
   std::vector<cudaGraphNode_t> gn(cp.dn.size(), nullptr);
   for (size_t q = 0; q < cp.dn.size(); q++) {
@@ -336,7 +397,28 @@ int build_graph(CompiledPlan &cp) {
     kp.sharedMemBytes = (unsigned)d.smem;
     kp.kernelParams = d.args;
     kp.extra = nullptr;
-    MB_CUDA(cudaGraphAddKernelNode(&gn[q], cp.graph, deps.data(), deps.size(), &kp));
+    if (!pdl) {
+      MB_CUDA(cudaGraphAddKernelNode(&gn[q], cp.graph, deps.data(), deps.size(), &kp));
+      if (int e = set_priority(gn[q], d.background)) return e;
+      continue;
+    }
+    // programmatic edges from kernel producers: this kernel is scheduled once
+    // every producer CTA has started and waits in-kernel for their completion
+    std::vector<cudaGraphNode_t> plain;
+    std::vector<cudaGraphNode_t> prog;
+    for (int p : d.deps) {
+      if (!gn[p]) continue;
+      (cp.dn[p].grid.x ? prog : plain).push_back(gn[p]);
+    }
+    MB_CUDA(cudaGraphAddKernelNode(&gn[q], cp.graph, plain.data(), plain.size(), &kp));
+    if (int e = set_priority(gn[q], d.background)) return e;
+    for (cudaGraphNode_t from : prog) {
+      cudaGraphEdgeData ed{};
+      ed.from_port = cudaGraphKernelNodePortProgrammatic;
+      ed.to_port = 0;
+      ed.type = cudaGraphDependencyTypeProgrammatic;
+      MB_CUDA(cudaGraphAddDependencies_v2(cp.graph, &from, &gn[q], &ed, 1));
+    }
   }
   MB_CUDA(cudaGraphInstantiate(&cp.exec, cp.graph, 0));
   return MB_OK;
@@ -369,7 +451,7 @@ int exec_plan(mb_ctx *c, CompiledPlan *cp, cudaStream_t s) {
   int e;
   if (c->use_graph) {
     if (!cp->exec) {
-      e = build_graph(*cp);
+      e = build_graph(*cp, c->use_graph == 2);
       if (e) return e;
     }
     MB_CUDA(cudaGraphLaunch(cp->exec, s));
@@ -409,6 +491,7 @@ extern "C" int mb_create(const mb_geometry *geo, int precision, mb_ctx **out) {
   auto c = std::make_unique<mb_ctx>();
   c->prec = precision;
   cudaGetDevice(&c->device);
+  cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device);
   c->geo = *geo;
   const mb_layout &L = geo->layout;
   const mb_config &cfg = geo->config;
@@ -506,17 +589,15 @@ extern "C" int mb_create(const mb_geometry *geo, int precision, mb_ctx **out) {
     c->allocs.push_back(p);
     c->d_slots = p;
   }
-  if ((e = dalloc(c.get(), &c->d_spl_lines, std::max(L.number_line, 1)))) return e;
   if (L.number_line) {
     // LU coefficients of each line's system (init_tri_A rows): c'_i = u_i / den_i,
     // den_i = 2 - l_i c'_{i-1}; stored as c' then 1/den, in the arithmetic type
-    std::vector<SplLineDev> sd(L.number_line);
     std::vector<double> coef;
+    c->spl_coef0.resize(L.number_line);
     for (int b = 0; b < L.number_line; b++) {
       const SplLine &s = c->spl_lines[b];
       const int N = s.Nc;
-      sd[b] = {s.coarse, s.fine, s.Nc, s.Nf, s.r, s.ci0, s.cj0, s.cdi, s.cdj, s.fi0, s.fj0, s.fdi, s.fdj, s.slot0,
-               (int)(coef.size() / 2), s.para};
+      c->spl_coef0[b] = (int)(coef.size() / 2);
       std::vector<double> cp(N), iv(N);
       double prev = 0;
       for (int i = 0; i < N; i++) {
@@ -529,7 +610,6 @@ extern "C" int mb_create(const mb_geometry *geo, int precision, mb_ctx **out) {
       coef.insert(coef.end(), cp.begin(), cp.end());
       coef.insert(coef.end(), iv.begin(), iv.end());
     }
-    MB_CUDA(cudaMemcpy(c->d_spl_lines, sd.data(), sd.size() * sizeof(SplLineDev), cudaMemcpyHostToDevice));
     const size_t rb = real_bytes(precision);
     std::vector<unsigned char> raw(coef.size() * rb);
     for (size_t q = 0; q < coef.size(); q++) {
@@ -661,9 +741,21 @@ extern "C" int mb_set_stb_variant(mb_ctx *c, int level, int variant) {
   return MB_OK;
 }
 
-extern "C" int mb_set_graph_mode(mb_ctx *c, int use_graph) {
-  if (!c) return MB_ERR_INVALID;
-  c->use_graph = use_graph ? 1 : 0;
+extern "C" int mb_set_bulk_occupancy(mb_ctx *c, int ctas_per_sm) {
+  if (!c || ctas_per_sm < 0) return MB_ERR_INVALID;
+  cudaDeviceSynchronize();
+  c->bulk_ctas_per_sm = ctas_per_sm;
+  c->plans.clear();
+  return MB_OK;
+}
+
+extern "C" int mb_set_graph_mode(mb_ctx *c, int mode) {
+  if (!c || mode < 0 || mode > 2) return MB_ERR_INVALID;
+  if (mode != c->use_graph) {
+    cudaDeviceSynchronize();
+    c->plans.clear();
+  }
+  c->use_graph = mode;
   return MB_OK;
 }
 
@@ -765,7 +857,7 @@ extern "C" int mb_prepare(mb_ctx *c, int n) {
     else { chunk = 1; fin = true; }
     CompiledPlan *cp = get_plan(c, chunk, fin, &err);
     if (!cp) { c->state = save; return err ? err : MB_ERR_INVALID; }
-    if (c->use_graph && !cp->exec && (err = build_graph(*cp))) { c->state = save; return err; }
+    if (c->use_graph && !cp->exec && (err = build_graph(*cp, c->use_graph == 2))) { c->state = save; return err; }
     c->state = cp->end;
     remaining -= chunk;
   }
@@ -968,6 +1060,122 @@ extern "C" int mb_set_fields(mb_ctx *c, int a, const double *rho, const double *
     MB_CUDA(cudaStreamSynchronize(s));
   }
   MB_CUDA(cudaGetLastError());
+  return MB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Checkpoint / restart.  The reference has none (its steady_<n>.dat files hold
+// no distributions).  A checkpoint is the raw device state: both distribution
+// buffers of every block (so the drag's read buffer survives too), rho/u and
+// u_prev, the ring slots and the scheduler state (buffer parities, ring
+// markers), behind a header that pins the layout, so a restart is bit-exact.
+// ---------------------------------------------------------------------------
+namespace {
+struct CkptHeader {
+  char magic[8];
+  int version, precision, nblk, nline;
+  long long slot_points, body_bytes;
+  unsigned long long geo_hash;
+};
+unsigned long long fnv1a(const void *p, size_t n) {
+  const unsigned char *b = (const unsigned char *)p;
+  unsigned long long h = 1469598103934665603ull;
+  for (size_t i = 0; i < n; i++) h = (h ^ b[i]) * 1099511628211ull;
+  return h;
+}
+size_t ckpt_bytes(const mb_ctx *c) {
+  size_t n = sizeof(CkptHeader);
+  for (int a = 0; a < c->nblk; a++) {
+    const IfBlk &B = c->blk[a];
+    n += 2 * 9 * (size_t)B.plane * prec_bytes(c->prec) + 5 * (size_t)B.plane * real_bytes(c->prec);
+  }
+  n += (size_t)c->n_slot_points * 27 * real_bytes(c->prec);
+  n += sizeof(int) * (c->nblk + 3 * c->geo.layout.number_line);
+  return n;
+}
+}  // namespace
+
+extern "C" int mb_checkpoint_size(mb_ctx *c, long long *bytes) {
+  if (!c || !bytes) return MB_ERR_INVALID;
+  *bytes = (long long)ckpt_bytes(c);
+  return MB_OK;
+}
+
+extern "C" int mb_checkpoint_save(mb_ctx *c, void *host, long long bytes, mb_stream stream) {
+  if (!c || !host) return MB_ERR_INVALID;
+  if (!c->inited) return MB_ERR_STATE;
+  if (bytes < (long long)ckpt_bytes(c)) return MB_ERR_INVALID;
+  cudaStream_t s = (cudaStream_t)stream;
+  unsigned char *o = (unsigned char *)host;
+  CkptHeader h{};
+  std::memcpy(h.magic, "MBLBMCK1", 8);
+  h.version = 1;
+  h.precision = c->prec;
+  h.nblk = c->nblk;
+  h.nline = c->geo.layout.number_line;
+  h.slot_points = c->n_slot_points;
+  h.body_bytes = (long long)(ckpt_bytes(c) - sizeof(CkptHeader));
+  h.geo_hash = fnv1a(&c->geo, sizeof(c->geo));
+  std::memcpy(o, &h, sizeof h);
+  o += sizeof h;
+  const size_t sb = prec_bytes(c->prec), rb = real_bytes(c->prec);
+  for (int a = 0; a < c->nblk; a++) {
+    const IfBlk &B = c->blk[a];
+    for (int q = 0; q < 2; q++) {
+      MB_CUDA(cudaMemcpyAsync(o, B.F[q], 9 * (size_t)B.plane * sb, cudaMemcpyDeviceToHost, s));
+      o += 9 * (size_t)B.plane * sb;
+    }
+    void *m[5] = {B.rho, B.ux, B.uy, B.upx, B.upy};
+    for (int q = 0; q < 5; q++) {
+      MB_CUDA(cudaMemcpyAsync(o, m[q], (size_t)B.plane * rb, cudaMemcpyDeviceToHost, s));
+      o += (size_t)B.plane * rb;
+    }
+  }
+  if (c->n_slot_points) {
+    MB_CUDA(cudaMemcpyAsync(o, c->d_slots, (size_t)c->n_slot_points * 27 * rb, cudaMemcpyDeviceToHost, s));
+    o += (size_t)c->n_slot_points * 27 * rb;
+  }
+  for (int a = 0; a < c->nblk; a++, o += sizeof(int)) std::memcpy(o, &c->state.parity[a], sizeof(int));
+  for (int b = 0; b < c->geo.layout.number_line; b++)
+    for (int p = 0; p < 3; p++, o += sizeof(int)) std::memcpy(o, &c->state.marker[b][p], sizeof(int));
+  MB_CUDA(cudaStreamSynchronize(s));
+  return MB_OK;
+}
+
+extern "C" int mb_checkpoint_load(mb_ctx *c, const void *host, long long bytes, mb_stream stream) {
+  if (!c || !host) return MB_ERR_INVALID;
+  if (bytes < (long long)sizeof(CkptHeader)) return MB_ERR_INVALID;
+  const unsigned char *o = (const unsigned char *)host;
+  CkptHeader h;
+  std::memcpy(&h, o, sizeof h);
+  if (std::memcmp(h.magic, "MBLBMCK1", 8) || h.version != 1 || h.precision != c->prec || h.nblk != c->nblk ||
+      h.nline != c->geo.layout.number_line || h.slot_points != c->n_slot_points ||
+      h.geo_hash != fnv1a(&c->geo, sizeof(c->geo)) || bytes < (long long)ckpt_bytes(c))
+    return MB_ERR_INVALID;
+  o += sizeof h;
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t sb = prec_bytes(c->prec), rb = real_bytes(c->prec);
+  for (int a = 0; a < c->nblk; a++) {
+    const IfBlk &B = c->blk[a];
+    for (int q = 0; q < 2; q++) {
+      MB_CUDA(cudaMemcpyAsync(B.F[q], o, 9 * (size_t)B.plane * sb, cudaMemcpyHostToDevice, s));
+      o += 9 * (size_t)B.plane * sb;
+    }
+    void *m[5] = {B.rho, B.ux, B.uy, B.upx, B.upy};
+    for (int q = 0; q < 5; q++) {
+      MB_CUDA(cudaMemcpyAsync(m[q], o, (size_t)B.plane * rb, cudaMemcpyHostToDevice, s));
+      o += (size_t)B.plane * rb;
+    }
+  }
+  if (c->n_slot_points) {
+    MB_CUDA(cudaMemcpyAsync(c->d_slots, o, (size_t)c->n_slot_points * 27 * rb, cudaMemcpyHostToDevice, s));
+    o += (size_t)c->n_slot_points * 27 * rb;
+  }
+  for (int a = 0; a < c->nblk; a++, o += sizeof(int)) std::memcpy(&c->state.parity[a], o, sizeof(int));
+  for (int b = 0; b < c->geo.layout.number_line; b++)
+    for (int p = 0; p < 3; p++, o += sizeof(int)) std::memcpy(&c->state.marker[b][p], o, sizeof(int));
+  MB_CUDA(cudaStreamSynchronize(s));
+  c->inited = true;
   return MB_OK;
 }
 

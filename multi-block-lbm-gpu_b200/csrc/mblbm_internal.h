@@ -53,6 +53,11 @@ struct SplLine {
   double para;           // (tau_f - 1) / (r (tau_c - 1)), assit_multi.h:176
 };
 
+// Launch limits of one record / spline node (the launch parameters hold
+// every op, line and block descriptor, see kernels.cuh).
+constexpr int PLAN_MAX_REC_OPS = 24;
+constexpr int PLAN_MAX_SPL_TASKS = 16;
+
 // One line of a spline node.
 struct SplTask {
   int line;       // index into the SplLine table
@@ -74,6 +79,7 @@ struct PlanNode {
   uint64_t parity = 0;        // STB: current buffer of each block before the step
   int macro_all = 0;          // STB: write rho/u of every FLUID cell
   std::vector<Rec> recs;      // REC
+  std::vector<std::pair<int, int>> ops;  // REC: (first record, count) of each reference line op
   double tw[4][3] = {};       // REC: temporal weight triples (a, b, c)
   int ntw = 0;
   std::vector<SplTask> spl;   // SPL

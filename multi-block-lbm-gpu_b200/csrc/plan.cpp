@@ -406,6 +406,8 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
 
     const NodeKind want = is_spl ? NK_SPL : NK_REC;
     bool join = (open >= 0 && nodes[open].kind == want);
+    if (join && want == NK_REC && int(nodes[open].ops.size()) >= PLAN_MAX_REC_OPS) join = false;
+    if (join && want == NK_SPL && int(nodes[open].spl.size()) >= PLAN_MAX_SPL_TASKS) join = false;
     if (join && want == NK_REC && o.kind == Op::TEMPORAL) {
       const PlanNode &nd = nodes[open];
       bool found = false;
@@ -445,6 +447,7 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
           nd.tw[widx][2] = tw[2];
         }
       }
+      nd.ops.push_back({int(nd.recs.size()), int(recs.size())});
       for (size_t q = 0; q < recs.size(); q++) {
         Rec r = recs[q];
         r.bits |= uint8_t(widx << RB_WIDX_SHIFT);
@@ -557,10 +560,19 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
   for (size_t q = 0; q < nodes.size(); q++) {
     PlanNode &nd = nodes[q];
     if (nd.kind == NK_REC) {
+      // ops keep their point ranges (each is affine in the point index); an op
+      // whose every write died is dropped whole
       std::vector<Rec> live;
-      for (const Rec &r : nd.recs)
-        if (r.bits & (RB_WRITE_F | RB_WRITE_M)) live.push_back(r);
+      std::vector<std::pair<int, int>> ops;
+      for (auto &op : nd.ops) {
+        bool any = false;
+        for (int r = op.first; r < op.first + op.second; r++) any |= (nd.recs[r].bits & (RB_WRITE_F | RB_WRITE_M)) != 0;
+        if (!any) continue;
+        ops.push_back({int(live.size()), op.second});
+        live.insert(live.end(), nd.recs.begin() + op.first, nd.recs.begin() + op.first + op.second);
+      }
       nd.recs.swap(live);
+      nd.ops.swap(ops);
       if (nd.recs.empty()) continue;
     }
     remap[q] = int(kept.size());

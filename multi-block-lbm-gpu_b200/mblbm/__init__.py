@@ -138,6 +138,7 @@ SIGNATURES = {
     "mb_set_graph_mode": ([_vp, C.c_int], C.c_int),
     "mb_set_split_cells": ([_vp, C.c_longlong], C.c_int),
     "mb_set_stb_variant": ([_vp, C.c_int, C.c_int], C.c_int),
+    "mb_set_bulk_occupancy": ([_vp, C.c_int], C.c_int),
     "mb_prepare": ([_vp, C.c_int], C.c_int),
     "mb_block_step": ([_vp, C.c_int, _vp], C.c_int),
     "mb_c_c_boundary_transfer": ([_vp, C.c_int, _vp], C.c_int),
@@ -158,6 +159,9 @@ SIGNATURES = {
     "mb_stats": ([_vp, _pll, _pll, _pll], C.c_int),
     "mb_time_block_step": ([_vp, C.c_int, C.c_int, _vp, _pd, _pd, _pll], C.c_int),
     "mb_error_L2_noalloc": ([C.POINTER(L2Segment), C.c_int, C.c_void_p, _vp], C.c_int),
+    "mb_checkpoint_size": ([_vp, _pll], C.c_int),
+    "mb_checkpoint_save": ([_vp, C.c_void_p, C.c_longlong, _vp], C.c_int),
+    "mb_checkpoint_load": ([_vp, C.c_void_p, C.c_longlong, _vp], C.c_int),
 }
 
 _lib = None
@@ -284,14 +288,17 @@ class MultiBlockLBM:
     """One multi-block simulation on the current CUDA device."""
 
     def __init__(self, geo, precision="f32", graph=True):
+        """graph: False launches kernels one by one, True replays CUDA graphs,
+        "pdl" replays graphs with programmatic kernel-to-kernel edges."""
         self.lib = load()
         self.geo = geo
         self.precision = precision
         h = C.c_void_p()
         _check(self.lib.mb_create(C.byref(geo), PRECISIONS[precision], C.byref(h)), "mb_create")
         self.h = h
-        if not graph:
-            _check(self.lib.mb_set_graph_mode(self.h, 0), "mb_set_graph_mode")
+        mode = 2 if graph == "pdl" else (1 if graph else 0)
+        if mode != 1:
+            _check(self.lib.mb_set_graph_mode(self.h, mode), "mb_set_graph_mode")
         self.n = 0
 
     def close(self):
@@ -321,6 +328,10 @@ class MultiBlockLBM:
     def set_stb_variant(self, level, variant):
         """Block-step kernel of a level: 0 one cell per thread, 1 four cells per thread."""
         _check(self.lib.mb_set_stb_variant(self.h, int(level), int(variant)), "mb_set_stb_variant")
+
+    def set_bulk_occupancy(self, ctas_per_sm):
+        """Cap interior block-step grids at ctas_per_sm CTAs per SM (0: uncapped)."""
+        _check(self.lib.mb_set_bulk_occupancy(self.h, int(ctas_per_sm)), "mb_set_bulk_occupancy")
 
     def prepare(self, n_coarse):
         """Compiles the plans and graphs that evolution(n_coarse) will replay."""
@@ -387,6 +398,18 @@ class MultiBlockLBM:
     def set_fields(self, area, rho=None, ux=None, uy=None, F=None, stream=None):
         arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (rho, ux, uy, F)]
         _check(self.lib.mb_set_fields(self.h, area, *[_dp(a) for a in arrs], _stream_ptr(stream)), "mb_set_fields")
+
+    def checkpoint(self, stream=None):
+        """The full device state as bytes (see mb_checkpoint_save)."""
+        n = C.c_longlong()
+        _check(self.lib.mb_checkpoint_size(self.h, C.byref(n)), "mb_checkpoint_size")
+        buf = np.empty(n.value, dtype=np.uint8)
+        _check(self.lib.mb_checkpoint_save(self.h, buf.ctypes.data, n.value, _stream_ptr(stream)), "mb_checkpoint_save")
+        return buf.tobytes()
+
+    def restore(self, data, stream=None):
+        buf = np.frombuffer(data, dtype=np.uint8)
+        _check(self.lib.mb_checkpoint_load(self.h, buf.ctypes.data, len(buf), _stream_ptr(stream)), "mb_checkpoint_load")
 
     def output(self, path):
         _check(self.lib.mb_write_tecplot(self.h, path.encode()), "mb_write_tecplot")
