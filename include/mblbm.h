@@ -164,15 +164,62 @@ int mb_init(mb_ctx *ctx, mb_stream stream);
 int mb_step(mb_ctx *ctx, int n_coarse, mb_stream stream);
 /* 0: launch the kernels one by one; 1: replay CUDA graphs of the dependency
  * DAG (default); 2: graphs whose kernel-to-kernel edges are programmatic, so a
- * consumer is scheduled while its producers drain. */
+ * consumer is scheduled while its producers drain; 3: one persistent
+ * executor launch per plan, which tracks the DAG on the device (CTAs claim
+ * work items of ready nodes; bulk interior work fills the fine-level chain's
+ * waits).  Results are identical in every mode. */
 int mb_set_graph_mode(mb_ctx *ctx, int mode);
+/* Mode 3: a CTA that finds no ready work for this long sets the context's
+ * error word and the launch ends; the next synchronising call (mb_sync,
+ * mb_drag, mb_error_L2, mb_check_finite, mb_copy_fields) returns
+ * MB_ERR_TIMEOUT once.  Default 2 s; at most 600 s.  No reference counterpart. */
+int mb_set_program_timeout(mb_ctx *ctx, double seconds);
+/* Mode 3: cells per work item of interior (bulk) and of all other block-step
+ * nodes (defaults 512 and 256); how many periods of the scheduler state (the
+ * coarse-step cycle after which buffer parities and ring markers repeat) one
+ * executor launch covers (default 2); at most how many CTAs execute bulk
+ * items at once (default 0: no limit), which keeps memory latency low for
+ * the fine-level chain.  No reference counterpart. */
+int mb_set_program_shape(mb_ctx *ctx, int bulk_cells, int urgent_cells, int periods_per_launch, int bulk_ctas);
+/* Mode 3 tracing: records one 48-byte entry per executed work item (global
+ * timer at the claim scan, at the start and at the end of the work; plan
+ * node, item, SM, CTA, launch number) into a device buffer of `capacity`
+ * records (0 turns tracing off).  mb_program_trace copies up to max_records
+ * of them to the host and empties the buffer.  No reference counterpart. */
+int mb_set_program_trace(mb_ctx *ctx, long long capacity);
+int mb_program_trace(mb_ctx *ctx, void *records, long long max_records, long long *n_records);
+/* Waits for the stream and reports an executor timeout (MB_ERR_TIMEOUT) of
+ * any earlier launch.  No reference counterpart. */
+int mb_sync(mb_ctx *ctx, mb_stream stream);
+/* One executor launch over a single empty node, for checking the timeout
+ * path: stall = 0 completes (MB_OK); stall = 1 gives the node a dependency
+ * that nothing satisfies, so the launch gives up after the timeout and the
+ * call returns MB_ERR_TIMEOUT with the context still usable.  Synchronous.
+ * No reference counterpart. */
+int mb_program_selftest(mb_ctx *ctx, int stall, mb_stream stream);
 /* Levels with at least `cells` cells update their interior (cells two or more
  * from a block edge) and their rim as separate DAG nodes, so that the interior
  * of the next coarse step overlaps the fine levels of this one.  Default 1e6;
  * 0 splits every level. */
 int mb_set_split_cells(mb_ctx *ctx, long long cells);
+/* Work granularity of interface nodes: points per record CTA (graph modes)
+ * or work item (mode 3), 32 (default) or 64; spline segments of 32 coarse
+ * intervals per CTA or work item, 1 (default) to 4.  Interface lines across
+ * rows touch one cache sector per value, so small units spread a node over
+ * many SMs' load/store units.  Results are identical. */
+int mb_set_interface_shape(mb_ctx *ctx, int rec_points, int spline_segments);
+/* Block-step nodes over at least `cells` cells (a whole level, or its
+ * interior or rim) load and store with evict-first cache hints, so that the
+ * streamed coarse level does not evict the fine levels' buffers from L2.
+ * Default 2e6; 0 never hints.  bulk = 1 also schedules such whole-level
+ * nodes as bulk work (lowest graph priority, executor bulk class), as the
+ * interiors of split levels always are.  Results are identical. */
+int mb_set_stream_cells(mb_ctx *ctx, long long cells, int bulk);
 /* Block-step kernel of one level: 0 = one cell per thread (default),
- * 1 = four cells per thread with vector loads.  Results are identical. */
+ * 1 = four cells per thread with vector loads, 2 = two cells per thread with
+ * the loads of both in flight together, 3 = row tiles of 256 cells per CTA
+ * with 32-bit offsets (whole levels and interiors; rims use 0).  Results are
+ * identical. */
 int mb_set_stb_variant(mb_ctx *ctx, int level, int variant);
 /* Caps the grid of interior (bulk) block-step launches at ctas_per_sm CTAs of
  * 256 threads per SM (0 = uncapped), leaving CTA slots on every SM for the

@@ -53,6 +53,18 @@ __device__ __forceinline__ void st_f(typename Prec<P>::S *p, long long idx, int 
   else p[idx] = v;
 }
 
+// Global loads and stores with an optional evict-first cache hint (.cs):
+// the coarse level streams several hundred MB per step and, hinted, leaves
+// the fine levels' buffers resident in L2.
+template <bool EF, typename T> __device__ __forceinline__ T ld_ef(const T *p) {
+  if constexpr (EF) return __ldcs(p);
+  else return *p;
+}
+template <bool EF, typename T> __device__ __forceinline__ void st_ef(T *p, T v) {
+  if constexpr (EF) __stcs(p, v);
+  else *p = v;
+}
+
 // Programmatic dependent launch: a kernel lets the next one in the graph be
 // scheduled as soon as every CTA has started (pdl_trigger), and waits for its
 // own producers to finish and flush (pdl_wait) before it reads their output.
@@ -84,7 +96,9 @@ struct StbBlk {
   long long cell0;  // first linear cell index of this block in the launch (per-cell kernel)
   double rv_tau;
   long long wt0;    // first warp tile of this block in the launch (quad kernel)
-  int tiles_x, row0;  // quad kernel: tiles of 128 cells per row, first row of the region
+  int tiles_x, row0;  // quad kernel: tiles of 128 cells per row; first row of the region (quad and row kernels)
+  int rt0, rtiles_x;  // row kernel: first row tile of this block in the launch, tiles of 256 cells per row
+  int col0, col1;     // row kernel: first and last column of the region
 };
 
 struct StbParams {
@@ -92,7 +106,9 @@ struct StbParams {
   int macro_all;     // write rho/u of every FLUID cell (else only CF_MACRO cells)
   int write_macros;  // 0: never write rho/u (kernel timing only)
   int region;        // 0: all cells, 1: distance >= 2 from the block edge, 2: distance <= 1
+  int evict_first;   // stream the blocks' buffers with evict-first cache hints
   long long total;   // cells in the launch (per-cell kernel) or warp tiles (quad kernel)
+  long long rtiles;  // row tiles in the launch (row kernel)
   double feqc[9];    // feq(rho0, U0): block-edge FLUID cells and stale f of edge solids
   double rho0, u0x, u0y;
   StbBlk b[STB_MAX_BLOCKS];
@@ -109,8 +125,14 @@ __device__ __forceinline__ void stb_collide(const typename Prec<P>::R *f, typena
     R rh = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8];
     R ux = f[1] - f[3] + f[5] - f[6] - f[7] + f[8];
     R uy = f[2] - f[4] + f[5] + f[6] - f[7] - f[8];
-    ux = ux / rh;
-    uy = uy / rh;
+    if constexpr (sizeof(R) == 8) {  // FP64: the reference's divisions
+      ux = ux / rh;
+      uy = uy / rh;
+    } else {  // FP32 arithmetic: one correctly rounded reciprocal
+      const R inv = __frcp_rn(rh);
+      ux = ux * inv;
+      uy = uy * inv;
+    }
     m[0] = rh;
     m[1] = ux;
     m[2] = uy;
@@ -122,8 +144,14 @@ __device__ __forceinline__ void stb_collide(const typename Prec<P>::R *f, typena
     const R rh = (R)1.0 + drh;
     R ux = f[1] - f[3] + f[5] - f[6] - f[7] + f[8];
     R uy = f[2] - f[4] + f[5] + f[6] - f[7] - f[8];
-    ux = ux / rh;
-    uy = uy / rh;
+    if constexpr (sizeof(R) == 8) {  // FP64: the reference's divisions
+      ux = ux / rh;
+      uy = uy / rh;
+    } else {  // FP32 arithmetic: one correctly rounded reciprocal
+      const R inv = __frcp_rn(rh);
+      ux = ux * inv;
+      uy = uy * inv;
+    }
     m[0] = rh;
     m[1] = ux;
     m[2] = uy;
@@ -137,42 +165,65 @@ __device__ __forceinline__ void stb_collide(const typename Prec<P>::R *f, typena
   }
 }
 
-// One cell of the block step: evolution_area_stb1/2/3 (multi/FH/evolution_block.h:3-119).
-template <int P>
-__device__ __forceinline__ void stb_cell(const StbParams &p, const StbBlk &B, int i, int j) {
+// Pulled values of cell (i, j): F_k at x - e_k, or the cell's own F_k where
+// x - e_k lies outside the block (those values are never used).  They do
+// not depend on the cell's flag byte, so the pulls and the flag load share
+// one memory round trip.
+template <int P, bool EF>
+__device__ __forceinline__ void stb_pull(const StbBlk &B, int i, int j, typename Prec<P>::S *raw) {
+  using S = typename Prec<P>::S;
+  const long long c = (long long)j * B.pitch + i;
+  // plain pointers: inside the persistent executor these buffers are written
+  // by earlier nodes of the same launch, so no non-coherent (read-only) loads
+  const S *Fin = (const S *)B.Fin;
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    const bool inb = (ex(k) != 1 || i > 0) && (ex(k) != -1 || i < B.nx - 1) && (ey(k) != 1 || j > 0) &&
+                     (ey(k) != -1 || j < B.ny - 1);
+    const long long off = inb ? ((long long)ey(k) * B.pitch + ex(k)) : 0;
+    raw[k] = ld_ef<EF>(Fin + (k * B.plane + c - off));
+  }
+}
+
+// One cell of the block step, evolution_area_stb1/2/3
+// (multi/FH/evolution_block.h:3-119), from its pulled values and flag byte.
+template <int P, bool EF>
+__device__ __forceinline__ void stb_finish(const StbParams &p, const StbBlk &B, int i, int j,
+                                           const typename Prec<P>::S *raw, uint8_t fl) {
   using R = typename Prec<P>::R;
   using S = typename Prec<P>::S;
   const long long c = (long long)j * B.pitch + i;
-  const S *__restrict__ Fin = (const S *)B.Fin;
-  S *__restrict__ Fout = (S *)B.Fout;
+  S *Fout = (S *)B.Fout;
   const long long plane = B.plane;
-  const uint8_t fl = B.flags[c];
   const int type = fl & 3;
   const bool wm = p.write_macros && (p.macro_all || (fl & 8));
 
   if (type == 0) {  // FLUID
     if (fl & 4) {   // block edge: equilibrium at rho0, U0 (stb2 :47-57), collide keeps it
 #pragma unroll
-      for (int k = 0; k < 9; k++) st_f<P>(Fout, k * plane + c, k, (R)p.feqc[k]);
+      for (int k = 0; k < 9; k++) {
+        if constexpr (Prec<P>::shifted) st_ef<EF>(Fout + k * plane + c, from_r<S>((R)p.feqc[k] - wk<P>(k)));
+        else st_ef<EF>(Fout + k * plane + c, (S)p.feqc[k]);
+      }
       if (wm) {
-        ((R *)B.rho)[c] = (R)p.rho0;
-        ((R *)B.ux)[c] = (R)p.u0x;
-        ((R *)B.uy)[c] = (R)p.u0y;
+        st_ef<EF>((R *)B.rho + c, (R)p.rho0);
+        st_ef<EF>((R *)B.ux + c, (R)p.u0x);
+        st_ef<EF>((R *)B.uy + c, (R)p.u0y);
       }
       return;
     }
-    R f[9];
+    R f[9];  // interior FLUID cell: every pull is inside the block
 #pragma unroll
-    for (int k = 0; k < 9; k++) f[k] = to_r(Fin[k * plane + c - ((long long)ey(k) * B.pitch + ex(k))]);
+    for (int k = 0; k < 9; k++) f[k] = to_r(raw[k]);
     R out[9], m[3];
     stb_collide<P>(f, (R)B.rv_tau, out, m);
     if (wm) {
-      ((R *)B.rho)[c] = m[0];
-      ((R *)B.ux)[c] = m[1];
-      ((R *)B.uy)[c] = m[2];
+      st_ef<EF>((R *)B.rho + c, m[0]);
+      st_ef<EF>((R *)B.ux + c, m[1]);
+      st_ef<EF>((R *)B.uy + c, m[2]);
     }
 #pragma unroll
-    for (int k = 0; k < 9; k++) Fout[k * plane + c] = from_r<S>(out[k]);
+    for (int k = 0; k < 9; k++) st_ef<EF>(Fout + k * plane + c, from_r<S>(out[k]));
     return;
   }
   if (type == 1) {  // SOLID_SBB: pull (stale f = feq(rho0,U0) off-block), then on-node bounce-back
@@ -181,36 +232,57 @@ __device__ __forceinline__ void stb_cell(const StbParams &p, const StbBlk &B, in
     for (int k = 0; k < 9; k++) {
       const int id = i - ex(k), jd = j - ey(k);
       if (id >= 0 && id < B.nx && jd >= 0 && jd < B.ny)
-        fr[k] = Fin[k * plane + c - ((long long)ey(k) * B.pitch + ex(k))];
+        fr[k] = raw[k];
       else if constexpr (Prec<P>::shifted)
         fr[k] = from_r<S>((float)(p.feqc[k] - wd(k)));
       else
         fr[k] = (S)p.feqc[k];
     }
 #pragma unroll
-    for (int k = 0; k < 9; k++) Fout[k * plane + c] = fr[opp(k)];  // w_k = w_opp(k): raw move is exact
+    for (int k = 0; k < 9; k++) st_ef<EF>(Fout + k * plane + c, fr[opp(k)]);  // w_k = w_opp(k): raw move is exact
     return;
   }
   // C_BOUNDARY and row padding: untouched by the step, carried to the new buffer
+  const S *Fin = (const S *)B.Fin;
 #pragma unroll
-  for (int k = 0; k < 9; k++) Fout[k * plane + c] = Fin[k * plane + c];
+  for (int k = 0; k < 9; k++) st_ef<EF>(Fout + k * plane + c, ld_ef<EF>(Fin + k * plane + c));
 }
 
+// Pulled values of a cell at least one cell from the block edge: every
+// neighbour is inside the block (constant offsets).
+template <int P, bool EF>
+__device__ __forceinline__ void stb_pull_in(const StbBlk &B, long long c, typename Prec<P>::S *raw) {
+  const typename Prec<P>::S *Fin = (const typename Prec<P>::S *)B.Fin;
+#pragma unroll
+  for (int k = 0; k < 9; k++) raw[k] = ld_ef<EF>(Fin + (k * B.plane + c - ((long long)ey(k) * B.pitch + ex(k))));
+}
+
+template <int P, bool EF>
+__device__ __forceinline__ void stb_cell_h(const StbParams &p, const StbBlk &B, int i, int j) {
+  typename Prec<P>::S raw[9];
+  const long long c = (long long)j * B.pitch + i;
+  if (i > 0 && i < B.nx - 1 && j > 0 && j < B.ny - 1) {
+    stb_pull_in<P, EF>(B, c, raw);  // issued together with the flag load
+    stb_finish<P, EF>(p, B, i, j, raw, B.flags[c]);
+  } else {
+    stb_pull<P, EF>(B, i, j, raw);
+    stb_finish<P, EF>(p, B, i, j, raw, B.flags[c]);
+  }
+}
 
 template <int P>
-__global__ void __launch_bounds__(256, P == MB_PREC_F64 ? 4 : 8) k_block_step(const __grid_constant__ StbParams p) {
-  pdl_trigger();
-  bool waited = false;
-  // grid-stride: a capped grid (bulk interior work) leaves CTA slots on every
-  // SM for kernels that run beside it
-  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < p.total;
-       g += (long long)gridDim.x * blockDim.x) {
-  int t = 0;
+__device__ __forceinline__ void stb_cell(const StbParams &p, const StbBlk &B, int i, int j) {
+  stb_cell_h<P, false>(p, B, i, j);
+}
+
+// Cell g (0 <= g < p.total) of a block-step launch: its block t and its
+// (i, j) in the launch's region.
+__device__ __forceinline__ void stb_locate(const StbParams &p, long long g, int &t, int &i, int &j) {
+  t = 0;
 #pragma unroll 1
   while (t + 1 < p.nblk && g >= p.b[t + 1].cell0) t++;
   const StbBlk &B = p.b[t];
   const int local = int(g - B.cell0);
-  int i, j;
   if (p.region == 1) {  // interior rectangle [2, nx-3] x [2, ny-3]
     const int w = B.nx - 4;
     j = 2 + local / w;
@@ -230,40 +302,153 @@ __global__ void __launch_bounds__(256, P == MB_PREC_F64 ? 4 : 8) k_block_step(co
     j = local / B.nx;
     i = local - j * B.nx;
   }
-  if (!waited) {
-    pdl_wait();
-    waited = true;
+}
+
+// Cell g of a block-step launch.
+template <int P>
+__device__ __forceinline__ void stb_at(const StbParams &p, long long g) {
+  int t, i, j;
+  stb_locate(p, g, t, i, j);
+  if (p.evict_first) stb_cell_h<P, true>(p, p.b[t], i, j);
+  else stb_cell_h<P, false>(p, p.b[t], i, j);
+}
+
+// Cells g0 and g1 of a block-step launch, with the loads of both in flight
+// together.
+template <int P, bool EF>
+__device__ __forceinline__ void stb_at2_h(const StbParams &p, long long g0, long long g1) {
+  using S = typename Prec<P>::S;
+  int t0, i0, j0, t1, i1, j1;
+  stb_locate(p, g0, t0, i0, j0);
+  stb_locate(p, g1, t1, i1, j1);
+  const StbBlk &B0 = p.b[t0], &B1 = p.b[t1];
+  S r0[9], r1[9];
+  const long long c0 = (long long)j0 * B0.pitch + i0, c1 = (long long)j1 * B1.pitch + i1;
+  if (i0 > 0 && i0 < B0.nx - 1 && j0 > 0 && j0 < B0.ny - 1) stb_pull_in<P, EF>(B0, c0, r0);
+  else stb_pull<P, EF>(B0, i0, j0, r0);
+  if (i1 > 0 && i1 < B1.nx - 1 && j1 > 0 && j1 < B1.ny - 1) stb_pull_in<P, EF>(B1, c1, r1);
+  else stb_pull<P, EF>(B1, i1, j1, r1);
+  const uint8_t f0 = B0.flags[(long long)j0 * B0.pitch + i0], f1 = B1.flags[(long long)j1 * B1.pitch + i1];
+  stb_finish<P, EF>(p, B0, i0, j0, r0, f0);
+  stb_finish<P, EF>(p, B1, i1, j1, r1, f1);
+}
+
+// CPT = 1: one cell per thread (grid-stride: a capped grid leaves CTA slots
+// on every SM for kernels that run beside it).  CPT = 2: a CTA owns chunks
+// of 512 cells and a thread cells tid and tid + 256 of a chunk.
+template <int P, int CPT>
+__global__ void __launch_bounds__(256, CPT == 1 ? (P == MB_PREC_F64 ? 4 : 8) : (P == MB_PREC_F64 ? 2 : 4))
+    k_block_step(const __grid_constant__ StbParams p) {
+  pdl_trigger();
+  pdl_wait();
+  if constexpr (CPT == 1) {
+    for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < p.total;
+         g += (long long)gridDim.x * blockDim.x)
+      stb_at<P>(p, g);
+  } else {
+    for (long long base = (long long)blockIdx.x * 512; base < p.total; base += (long long)gridDim.x * 512) {
+      const long long g0 = base + threadIdx.x, g1 = g0 + 256;
+      if (g1 < p.total) {
+        if (p.evict_first) stb_at2_h<P, true>(p, g0, g1);
+        else stb_at2_h<P, false>(p, g0, g1);
+      } else if (g0 < p.total) {
+        stb_at<P>(p, g0);
+      }
+    }
   }
-  stb_cell<P>(p, B, i, j);
+}
+
+// The block step on row tiles: a CTA owns 256 consecutive cells of one row
+// of one block (its block, row and first column are uniform over the CTA),
+// a thread one cell.  Offsets are 32-bit (the host uses this kernel only
+// when 9 planes of every block fit in 2^31 elements).  Interior FLUID cells
+// take a short path; every other cell runs the general stb_finish.
+// cells on the block edge and cells that are not interior FLUID: the general
+// path, out of line so that its registers do not burden the common path
+template <int P, bool EF>
+__device__ __noinline__ void stb_cell_slow(const StbParams &p, const StbBlk &B, int i, int j) {
+  stb_cell_h<P, EF>(p, B, i, j);
+}
+
+template <int P, bool EF, bool INTERIOR>
+__device__ __forceinline__ void stb_cell_rows(const StbParams &p, const StbBlk &B, int i, int j) {
+  using R = typename Prec<P>::R;
+  using S = typename Prec<P>::S;
+  if (INTERIOR || (i > 0 && i < B.nx - 1 && j > 0 && j < B.ny - 1)) {
+    const int c = j * B.pitch + i;
+    const int plane = (int)B.plane;
+    const S *Fin = (const S *)B.Fin;
+    S raw[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) raw[k] = ld_ef<EF>(Fin + (k * plane + c - (ey(k) * B.pitch + ex(k))));
+    const uint8_t fl = B.flags[c];
+    if ((fl & 7) == 0) {  // FLUID away from the block edge
+      R f[9];
+#pragma unroll
+      for (int k = 0; k < 9; k++) f[k] = to_r(raw[k]);
+      R out[9], m[3];
+      stb_collide<P>(f, (R)B.rv_tau, out, m);
+      if (p.write_macros && (p.macro_all || (fl & 8))) {
+        st_ef<EF>((R *)B.rho + c, m[0]);
+        st_ef<EF>((R *)B.ux + c, m[1]);
+        st_ef<EF>((R *)B.uy + c, m[2]);
+      }
+      S *Fout = (S *)B.Fout;
+#pragma unroll
+      for (int k = 0; k < 9; k++) st_ef<EF>(Fout + (k * plane + c), from_r<S>(out[k]));
+      return;
+    }
   }
+  stb_cell_slow<P, EF>(p, B, i, j);
+}
+
+template <int P, bool INTERIOR>
+__global__ void __launch_bounds__(256, P == MB_PREC_F64 ? 4 : 8) k_block_step_r(const __grid_constant__ StbParams p) {
+  pdl_trigger();
+  pdl_wait();
+  const int tile = blockIdx.x;
+  int t = 0;
+#pragma unroll 1
+  while (t + 1 < p.nblk && tile >= p.b[t + 1].rt0) t++;
+  const StbBlk &B = p.b[t];
+  const int lt = tile - B.rt0;
+  const int r = lt / B.rtiles_x;
+  const int j = B.row0 + r;
+  const int i = B.col0 + (lt - r * B.rtiles_x) * 256 + (int)threadIdx.x;
+  if (i > B.col1) return;
+  if (p.evict_first) stb_cell_rows<P, true, INTERIOR>(p, B, i, j);
+  else stb_cell_rows<P, false, INTERIOR>(p, B, i, j);
 }
 
 // Four consecutive cells of a row in the stored form, as arithmetic values
 // (for shifted precisions these are h = f - w); quads start at i % 4 == 0.
-__device__ __forceinline__ void ld_quad(const float *p, float *v) {
-  const float4 x = *(const float4 *)p;
+// EF: evict-first cache hints.
+template <bool EF> __device__ __forceinline__ void ld_quad(const float *p, float *v) {
+  const float4 x = ld_ef<EF>((const float4 *)p);
   v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
 }
-__device__ __forceinline__ void st_quad(float *p, const float *v) { *(float4 *)p = make_float4(v[0], v[1], v[2], v[3]); }
-__device__ __forceinline__ void ld_quad(const double *p, double *v) {
-  const double2 a = *(const double2 *)p, b = *(const double2 *)(p + 2);
+template <bool EF> __device__ __forceinline__ void st_quad(float *p, const float *v) {
+  st_ef<EF>((float4 *)p, make_float4(v[0], v[1], v[2], v[3]));
+}
+template <bool EF> __device__ __forceinline__ void ld_quad(const double *p, double *v) {
+  const double2 a = ld_ef<EF>((const double2 *)p), b = ld_ef<EF>((const double2 *)(p + 2));
   v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
 }
-__device__ __forceinline__ void st_quad(double *p, const double *v) {
-  *(double2 *)p = make_double2(v[0], v[1]);
-  *(double2 *)(p + 2) = make_double2(v[2], v[3]);
+template <bool EF> __device__ __forceinline__ void st_quad(double *p, const double *v) {
+  st_ef<EF>((double2 *)p, make_double2(v[0], v[1]));
+  st_ef<EF>((double2 *)(p + 2), make_double2(v[2], v[3]));
 }
-__device__ __forceinline__ void ld_quad(const __half *p, float *v) {
-  const uint2 u = *(const uint2 *)p;
+template <bool EF> __device__ __forceinline__ void ld_quad(const __half *p, float *v) {
+  const uint2 u = ld_ef<EF>((const uint2 *)p);
   const float2 a = __half22float2(*(const __half2 *)&u.x), b = __half22float2(*(const __half2 *)&u.y);
   v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
 }
-__device__ __forceinline__ void st_quad(__half *p, const float *v) {
+template <bool EF> __device__ __forceinline__ void st_quad(__half *p, const float *v) {
   const __half2 a = __floats2half2_rn(v[0], v[1]), b = __floats2half2_rn(v[2], v[3]);
   uint2 u;
   u.x = *(const uint32_t *)&a;
   u.y = *(const uint32_t *)&b;
-  *(uint2 *)p = u;
+  st_ef<EF>((uint2 *)p, u);
 }
 
 // The block step on quads: a warp owns 128 consecutive cells of one row and
@@ -273,15 +458,10 @@ __device__ __forceinline__ void st_quad(__half *p, const float *v) {
 // load.  Quads that are all FLUID interior cells of the region take this
 // path; any other quad (block-edge rows and columns, solids, region borders,
 // row ends) runs the per-cell stb_cell for its cells.
-template <int P>
-__global__ void __launch_bounds__(256) k_block_step_q(const __grid_constant__ StbParams p) {
+template <int P, bool EF>
+__device__ __forceinline__ void stb_quad_body(const StbParams &p, long long wt, int lane) {
   using R = typename Prec<P>::R;
   using S = typename Prec<P>::S;
-  pdl_trigger();
-  const long long wt = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (wt >= p.total) return;  // warp-uniform
-  pdl_wait();
   int t = 0;
 #pragma unroll 1
   while (t + 1 < p.nblk && wt >= p.b[t + 1].wt0) t++;
@@ -294,7 +474,7 @@ __global__ void __launch_bounds__(256) k_block_step_q(const __grid_constant__ St
   if (j == 0 || j == B.ny - 1) {  // no row on one side: per-cell path for the whole warp
     for (int q = 0; q < 4; q++) {
       const int i = i0 + q;
-      if (i >= clo && i <= chi) stb_cell<P>(p, B, i, j);
+      if (i >= clo && i <= chi) stb_cell_h<P, EF>(p, B, i, j);
     }
     return;
   }
@@ -302,7 +482,7 @@ __global__ void __launch_bounds__(256) k_block_step_q(const __grid_constant__ St
   const long long rowc = (long long)j * B.pitch;
   const uint32_t fl4 = inrow ? *(const uint32_t *)(B.flags + rowc + i0) : 0x03030303u;
   const bool fast = inrow && (fl4 & 0x07070707u) == 0u && i0 >= clo && i0 + 3 <= chi;
-  const S *__restrict__ Fin = (const S *)B.Fin;
+  const S *Fin = (const S *)B.Fin;
   // issue every load before any shuffle consumes one: nine quads and, for the
   // six directions with a column shift, the cell just outside the warp's span
   // (lane 0 for e_x = +1, lane 31 for e_x = -1)
@@ -312,10 +492,10 @@ __global__ void __launch_bounds__(256) k_block_step_q(const __grid_constant__ St
   for (int k = 0; k < 9; k++) {
     const S *rowp = Fin + k * B.plane + (long long)(j - ey(k)) * B.pitch;
     f[k][0] = f[k][1] = f[k][2] = f[k][3] = (R)0;
-    if (inrow) ld_quad(rowp + i0, f[k]);
+    if (inrow) ld_quad<EF>(rowp + i0, f[k]);
     halo[k] = (R)0;
-    if (ex(k) == 1 && lane == 0 && inrow && i0 > 0) halo[k] = to_r(rowp[i0 - 1]);
-    if (ex(k) == -1 && lane == 31 && i0 + 4 < B.pitch) halo[k] = to_r(rowp[i0 + 4]);
+    if (ex(k) == 1 && lane == 0 && inrow && i0 > 0) halo[k] = to_r(ld_ef<EF>(rowp + i0 - 1));
+    if (ex(k) == -1 && lane == 31 && i0 + 4 < B.pitch) halo[k] = to_r(ld_ef<EF>(rowp + i0 + 4));
   }
 #pragma unroll
   for (int k = 0; k < 9; k++) {
@@ -340,20 +520,31 @@ __global__ void __launch_bounds__(256) k_block_step_q(const __grid_constant__ St
 #pragma unroll
       for (int k = 0; k < 9; k++) f[k][q] = o[k];
       if (p.write_macros && (p.macro_all || ((fl4 >> (8 * q)) & 8u))) {
-        ((R *)B.rho)[rowc + i0 + q] = m[0];
-        ((R *)B.ux)[rowc + i0 + q] = m[1];
-        ((R *)B.uy)[rowc + i0 + q] = m[2];
+        st_ef<EF>((R *)B.rho + rowc + i0 + q, m[0]);
+        st_ef<EF>((R *)B.ux + rowc + i0 + q, m[1]);
+        st_ef<EF>((R *)B.uy + rowc + i0 + q, m[2]);
       }
     }
-    S *__restrict__ Fout = (S *)B.Fout;
+    S *Fout = (S *)B.Fout;
 #pragma unroll
-    for (int k = 0; k < 9; k++) st_quad(Fout + k * B.plane + rowc + i0, f[k]);
+    for (int k = 0; k < 9; k++) st_quad<EF>(Fout + k * B.plane + rowc + i0, f[k]);
   } else {
     for (int q = 0; q < 4; q++) {
       const int i = i0 + q;
-      if (i < B.nx && i >= clo && i <= chi) stb_cell<P>(p, B, i, j);
+      if (i < B.nx && i >= clo && i <= chi) stb_cell_h<P, EF>(p, B, i, j);
     }
   }
+}
+
+template <int P>
+__global__ void __launch_bounds__(256) k_block_step_q(const __grid_constant__ StbParams p) {
+  pdl_trigger();
+  const long long wt = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (wt >= p.total) return;  // warp-uniform
+  pdl_wait();
+  if (p.evict_first) stb_quad_body<P, true>(p, wt, lane);
+  else stb_quad_body<P, false>(p, wt, lane);
 }
 
 // ----------------------------------------------------------------------------
@@ -407,13 +598,11 @@ struct RecOpsParams {
 };
 static_assert(sizeof(RecOpsParams) <= 4096, "record launch parameters must fit the 4 KB parameter space");
 
+// Point t (0 <= t < p.total) of a record launch.
 template <int P>
-__global__ void __launch_bounds__(REC_THREADS) k_records(const __grid_constant__ RecOpsParams p) {
+__device__ __forceinline__ void rec_point(const RecOpsParams &p, int t) {
   using R = typename Prec<P>::R;
   using S = typename Prec<P>::S;
-  pdl_trigger();
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= p.total) return;
   int o = 0;
 #pragma unroll 1
   while (o + 1 < p.nops && t >= p.op_start[o + 1]) o++;
@@ -421,37 +610,46 @@ __global__ void __launch_bounds__(REC_THREADS) k_records(const __grid_constant__
   const int ip = t - p.op_start[o];
   const long long dc = (long long)op.dst0 + (long long)ip * op.dstride;
   const long long sc = (long long)op.src0 + (long long)ip * op.sstride;
-  pdl_wait();
-  const uint8_t live = op.has_mask ? p.mask[op.mask_off + ip] : op.bits;
-  const bool wF = live & 4, wM = live & 8;
+  // every source load is issued before the write mask is known: one memory
+  // round trip per point
+  const uint8_t *mp = op.has_mask ? p.mask + op.mask_off + ip : nullptr;
   const RecBlk &D = p.b[op.dst_block];
   S *Fd = (S *)D.F[(op.bits >> 1) & 1];
   if (op.type == 0) {  // same-level copy (assit_multi.h:2-46)
     const RecBlk &A = p.b[op.src_block];
     const S *Fs = (const S *)A.F[op.bits & 1];
-    if (wM) {
-      ((R *)D.rho)[dc] = ((const R *)A.rho)[sc];
-      ((R *)D.ux)[dc] = ((const R *)A.ux)[sc];
-      ((R *)D.uy)[dc] = ((const R *)A.uy)[sc];
-    }
-    if (wF) {
+    const R m0 = ((const R *)A.rho)[sc], m1 = ((const R *)A.ux)[sc], m2 = ((const R *)A.uy)[sc];
+    S f[9];
 #pragma unroll
-      for (int k = 0; k < 9; k++) Fd[k * D.plane + dc] = Fs[k * A.plane + sc];
+    for (int k = 0; k < 9; k++) f[k] = Fs[k * A.plane + sc];
+    const uint8_t live = mp ? *mp : op.bits;
+    if (live & 8) {
+      ((R *)D.rho)[dc] = m0;
+      ((R *)D.ux)[dc] = m1;
+      ((R *)D.uy)[dc] = m2;
+    }
+    if (live & 4) {
+#pragma unroll
+      for (int k = 0; k < 9; k++) Fd[k * D.plane + dc] = f[k];
     }
     return;
   }
   if (op.type == 1 || op.type == 2) {  // temporal interpolation (:213-247) / c_f (:249-271)
-    if (!wF) return;
     const R *s = (const R *)p.slots + sc * 27;
+    R v[9];
     if (op.type == 1) {
       const int wi = (op.bits >> 4) & 3;
       const R a = (R)p.tw[wi][0], b = (R)p.tw[wi][1], cc = (R)p.tw[wi][2];
 #pragma unroll
-      for (int k = 0; k < 9; k++)
-        st_f<P>(Fd, k * D.plane + dc, k, a * s[op.m0 * 9 + k] - b * s[op.m1 * 9 + k] + cc * s[op.m2 * 9 + k]);
+      for (int k = 0; k < 9; k++) v[k] = a * s[op.m0 * 9 + k] - b * s[op.m1 * 9 + k] + cc * s[op.m2 * 9 + k];
     } else {
 #pragma unroll
-      for (int k = 0; k < 9; k++) st_f<P>(Fd, k * D.plane + dc, k, s[op.m2 * 9 + k]);
+      for (int k = 0; k < 9; k++) v[k] = s[op.m2 * 9 + k];
+    }
+    const uint8_t live = mp ? *mp : op.bits;
+    if (live & 4) {
+#pragma unroll
+      for (int k = 0; k < 9; k++) st_f<P>(Fd, k * D.plane + dc, k, v[k]);
     }
     return;
   }
@@ -459,20 +657,32 @@ __global__ void __launch_bounds__(REC_THREADS) k_records(const __grid_constant__
   const RecBlk &Fb = p.b[op.src_block];
   const S *Fs = (const S *)Fb.F[op.bits & 1];
   const R rh = ((const R *)Fb.rho)[sc], ux = ((const R *)Fb.ux)[sc], uy = ((const R *)Fb.uy)[sc];
-  if (wM) {
+  R ft[9];
+#pragma unroll
+  for (int k = 0; k < 9; k++) ft[k] = ld_f<P>(Fs, k * Fb.plane + sc, k);
+  const uint8_t live = mp ? *mp : op.bits;
+  if (live & 8) {
     ((R *)D.rho)[dc] = rh;
     ((R *)D.ux)[dc] = ux;
     ((R *)D.uy)[dc] = uy;
   }
-  if (wF) {
+  if (live & 4) {
     const R para = (R)((double)(Fb.m / D.m) * (D.tau - 1.0) / (Fb.tau - 1.0));
 #pragma unroll
     for (int k = 0; k < 9; k++) {
-      const R ft = ld_f<P>(Fs, k * Fb.plane + sc, k);
       const R fe = feq<R>(k, rh, ux, uy);
-      st_f<P>(Fd, k * D.plane + dc, k, fe + para * (ft - fe));
+      st_f<P>(Fd, k * D.plane + dc, k, fe + para * (ft[k] - fe));
     }
   }
+}
+
+template <int P>
+__global__ void __launch_bounds__(REC_THREADS) k_records(const __grid_constant__ RecOpsParams p) {
+  pdl_trigger();
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= p.total) return;
+  pdl_wait();
+  rec_point<P>(p, t);
 }
 
 // ----------------------------------------------------------------------------
@@ -547,21 +757,20 @@ __device__ __forceinline__ void spl_gather_p(const SplTaskP &T, int ip, typename
   for (int k = 0; k < 9; k++) v[3 + k] = ld_f<P>(F, k * T.cplane + c, k);
 }
 
-template <int P>
-__global__ void __launch_bounds__(32 * SPL_WARPS) k_spline(const __grid_constant__ SplParamsP p) {
+// shared memory of one spline warp: the gathered fields, the forward sweep
+// (then the moments) and the window's c' and 1/den
+template <typename R> __host__ __device__ constexpr size_t spl_warp_smem() { return (size_t)26 * spl_win<R>() * sizeof(R); }
+
+// Segment sid (0 <= sid < p.nseg) of a spline launch, by one warp, with its
+// window arrays at wsm (spl_warp_smem bytes, 16-byte aligned).
+template <int P, bool UNROLL>
+__device__ __forceinline__ void spl_segment(const SplParamsP &p, int sid, int lane, unsigned char *wsm) {
   using R = typename Prec<P>::R;
-  using S = typename Prec<P>::S;
   constexpr int H = SplHalo<R>::v;
   constexpr int W = spl_win<R>();
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  typedef R Win[12][W];
-  Win *sf = (Win *)smem_raw;            // [warp] gathered fields
-  Win *sx = sf + SPL_WARPS;             // [warp] forward sweep, then the moments
-  R(*scf)[2][W] = (R(*)[2][W])(sx + SPL_WARPS);  // [warp] c'_i and 1/den_i of the window
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  pdl_trigger();
-  const int sid = blockIdx.x * SPL_WARPS + warp;
-  if (sid >= p.nseg) return;
+  R(*sfw)[W] = (R(*)[W])wsm;                   // [12][W] gathered fields
+  R(*sxw)[W] = sfw + 12;                        // [12][W] forward sweep, then the moments
+  R(*scw)[W] = sxw + 12;                        // [2][W] c'_i and 1/den_i of the window
   int tk = 0;
 #pragma unroll 1
   while (tk + 1 < p.ntask && sid >= p.t[tk + 1].seg0) tk++;
@@ -575,21 +784,46 @@ __global__ void __launch_bounds__(32 * SPL_WARPS) k_spline(const __grid_constant
   const int Ilo = 1 + seg * SPL_SEG, Ihi = min(N - 1, (seg + 1) * SPL_SEG);
   const int w0 = max(0, Ilo - 1 - H), w1 = min(N - 1, Ihi + H);  // rows solved
   const int g0 = max(0, w0 - 1), g1 = min(N - 1, w1 + 1);        // rows gathered
-  pdl_wait();
-  for (int i = g0 + lane; i <= g1; i += 32) {
-    R v[12];
-    spl_gather_p<P>(T, i, v);
+  if constexpr (UNROLL) {
+    // at most 3 x 32 rows (the window is below 96 rows): every load of the
+    // gather in flight at once
+    static_assert(spl_win<R>() + 2 <= 96, "gather window");
+    R v[3][12], c0[3], c1[3];
 #pragma unroll
-    for (int f = 0; f < 12; f++) sf[warp][f][i - g0] = v[f];
-    scf[warp][0][i - g0] = cpt[i];
-    scf[warp][1][i - g0] = ivd[i];
+    for (int q = 0; q < 3; q++) {
+      const int i = g0 + lane + 32 * q;
+      if (i <= g1) {
+        spl_gather_p<P>(T, i, v[q]);
+        c0[q] = cpt[i];
+        c1[q] = ivd[i];
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      const int i = g0 + lane + 32 * q;
+      if (i <= g1) {
+#pragma unroll
+        for (int f = 0; f < 12; f++) sfw[f][i - g0] = v[q][f];
+        scw[0][i - g0] = c0[q];
+        scw[1][i - g0] = c1[q];
+      }
+    }
+  } else {
+    for (int i = g0 + lane; i <= g1; i += 32) {
+      R v[12];
+      spl_gather_p<P>(T, i, v);
+#pragma unroll
+      for (int f = 0; f < 12; f++) sfw[f][i - g0] = v[f];
+      scw[0][i - g0] = cpt[i];
+      scw[1][i - g0] = ivd[i];
+    }
   }
   __syncwarp();
   if (lane < 12) {
     const int f = lane;
-    const R *x = sf[warp][f] - g0;  // x[i] = field at row i
-    R *y = sx[warp][f] - g0;
-    const R *cp = scf[warp][0] - g0, *iv = scf[warp][1] - g0;
+    const R *x = sfw[f] - g0;  // x[i] = field at row i
+    R *y = sxw[f] - g0;
+    const R *cp = scw[0] - g0, *iv = scw[1] - g0;
     // right-hand sides 6 f_i - 3 f_{i-1} - 3 f_{i+1}, zero at both ends (assit_multi.h:82-107)
     R yv = 0;
 #pragma unroll 4
@@ -620,8 +854,8 @@ __global__ void __launch_bounds__(32 * SPL_WARPS) k_spline(const __grid_constant
     R out[12];
 #pragma unroll
     for (int f = 0; f < 12; f++)
-      out[f] = spline3_s<R>(xx, (R)(I - 1), (R)1.0, sf[warp][f][I - 1 - g0], sf[warp][f][I - g0],
-                            sx[warp][f][I - 1 - g0], sx[warp][f][I - g0]);
+      out[f] = spline3_s<R>(xx, (R)(I - 1), (R)1.0, sfw[f][I - 1 - g0], sfw[f][I - g0],
+                            sxw[f][I - 1 - g0], sxw[f][I - g0]);
     const long long fc = (long long)(T.fj0 + ip * T.fdj) * T.fpitch + (T.fi0 + ip * T.fdi);
     if (T.mask_off < 0 || p.mask[T.mask_off + ip]) {
       ((R *)T.Mf[0])[fc] = out[0];
@@ -634,6 +868,368 @@ __global__ void __launch_bounds__(32 * SPL_WARPS) k_spline(const __grid_constant
       const R fe = feq<R>(k, out[0], out[1], out[2]);
       sl[k] = fe + para * (out[3 + k] - fe);
     }
+  }
+}
+
+template <int P>
+__global__ void __launch_bounds__(32 * SPL_WARPS) k_spline(const __grid_constant__ SplParamsP p) {
+  using R = typename Prec<P>::R;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  pdl_trigger();
+  const int sid = blockIdx.x * (int)(blockDim.x >> 5) + warp;  // blockDim: 1 to SPL_WARPS warps
+  if (sid >= p.nseg) return;
+  pdl_wait();
+  spl_segment<P, true>(p, sid, lane, smem_raw + warp * spl_warp_smem<R>());
+}
+
+// ----------------------------------------------------------------------------
+// Persistent plan executor.  One launch runs every node of a compiled plan
+// (block steps, record ops, spline lines of one or more coarse steps) with the
+// plan's dependencies tracked on the device.  Each node is cut into work
+// items; a node's successors become ready when its last item completes.
+//
+// A CTA is eight worker warps and one scheduler warp.  The scheduler claims
+// items (atomic counter per node), stages the parameter block of the next
+// item in one of two shared buffers while the workers execute the current
+// one, and signals completion of each item after the workers are done with
+// it.  Workers and scheduler hand items over through two named barriers
+// (FULL: an item is staged; EMPTY: the workers finished one).
+//
+// Nodes [0, nurgent) are the latency-bound chain (every node but the
+// interior of split levels), in plan order; nodes [nurgent, nnodes) the bulk
+// interior block steps.  The scheduler takes the first ready urgent node of
+// its scan window, else the first ready bulk node: bulk work fills the time
+// the fine-level chain spends waiting on its own dependencies.  Items never
+// wait, so the executor cannot deadlock; a scheduler that finds no ready
+// work sleeps with backoff and gives up (error word set, all CTAs exit) after
+// timeout_ns without work.
+//
+// Ordering: after the workers pass EMPTY, the scheduler fences and adds one
+// to the node's done count; the scheduler that completes the last item
+// fences, decrements each successor's pending count, fences and increments
+// the generation word.  A scheduler rescans pending counts only after an
+// acquire load shows a new generation (or its window moved), reads them with
+// acquire loads, and publishes the claimed item through FULL before any
+// worker reads the node's inputs.  All loads of distributions are plain
+// (coherent) loads: buffers are written by earlier nodes of the same launch.
+// ----------------------------------------------------------------------------
+constexpr int PRG_WORKERS = 256;
+constexpr int PRG_THREADS = PRG_WORKERS + 32;
+constexpr int PRG_SCHED_WARP = PRG_WORKERS / 32;
+constexpr int PRG_MAX_NODES = 1024;
+constexpr int PRG_WIN = 16;  // scan window per class (urgent, bulk): one lane per node
+constexpr int PRG_BAR_FULL = 1, PRG_BAR_EMPTY = 2;
+enum : int { PK_STB = 0, PK_REC = 1, PK_SPL = 2, PK_NOP = 3 };
+
+struct PrgNode {
+  int kind;
+  int items;       // work items
+  long long units; // cells (STB), points (REC) or segments (SPL)
+  int per_item;    // units per item
+  int param_off;   // byte offset of the node's parameter block in the blob (16-byte aligned)
+  int param_bytes; // multiple of 16
+  int succ0, nsucc;
+  int plan_index;  // index of the node in the compiled plan (for traces)
+};
+static_assert(sizeof(PrgNode) == 40, "PrgNode layout");
+
+// One executed work item, when tracing is on: global-timer stamps of the
+// start of its claim, of its hand-over to the workers and of the workers'
+// completion.
+struct PrgTraceRec {
+  unsigned long long t_pick, t_start, t_end;
+  int plan_node, item;
+  int sm, cta;
+  int launch, pad_;
+};
+static_assert(sizeof(PrgTraceRec) == 48, "PrgTraceRec layout");
+
+struct PrgArgs {
+  const PrgNode *nodes;
+  const int *succ;
+  const unsigned char *blob;
+  unsigned int *claim, *done, *pending;  // per node; reset before every launch
+  unsigned int *gen;                     // nodes completed so far; reset before every launch
+  unsigned int *bulk_active;             // CTAs holding a bulk item; reset before every launch
+  int bulk_limit;                        // claim bulk items only while bulk_active < bulk_limit (0: no limit)
+  unsigned int *err;                     // device error word: nonzero stops every CTA
+  unsigned int *host_err;                // mapped host word mirrored on error (may be null)
+  int nnodes, nurgent;
+  unsigned long long timeout_ns;
+  PrgTraceRec *trace;                    // tracing kernel only
+  unsigned int *trace_n;
+  unsigned int trace_cap;
+  int launch;
+};
+
+// shared memory of the executor: two parameter buffers, then SPL_WARPS
+// spline windows
+__host__ __device__ constexpr size_t prg_cmax(size_t x, size_t y) { return x > y ? x : y; }
+__host__ __device__ constexpr size_t prg_pbuf() {
+  return (prg_cmax(sizeof(StbParams), prg_cmax(sizeof(RecOpsParams), sizeof(SplParamsP))) + 15) / 16 * 16;
+}
+template <typename R> __host__ __device__ constexpr size_t prg_smem() {
+  return 2 * prg_pbuf() + SPL_WARPS * spl_warp_smem<R>();
+}
+
+__device__ __forceinline__ unsigned long long prg_clock() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ unsigned int prg_ld_acquire(const unsigned int *p) {
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ unsigned int prg_ld_relaxed(const unsigned int *p) {
+  unsigned int v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ bool prg_bit(const unsigned int *m, int n) { return (m[n >> 5] >> (n & 31)) & 1u; }
+__device__ __forceinline__ void prg_bar_sync(int id) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "n"(PRG_THREADS) : "memory");
+}
+__device__ __forceinline__ void prg_bar_arrive(int id) {
+  asm volatile("bar.arrive %0, %1;" ::"r"(id), "n"(PRG_THREADS) : "memory");
+}
+
+// Scheduler-warp state (registers of every lane, kept uniform).
+struct PrgSched {
+  int lo_u, lo_b;          // first node of each class not known to be exhausted
+  unsigned int gen_seen;   // generation of the last full readiness scan
+  int scan_u, scan_b;      // window starts of that scan
+};
+
+// Scheduler warp: claim an item.  Returns node >= 0 (and item), -1 when
+// every node is exhausted, -2 on error or timeout, -3 when nothing is ready
+// and block is false.
+__device__ __forceinline__ int prg_claim(const PrgArgs &a, unsigned int *s_exh, unsigned int *s_rdy, PrgSched &st,
+                                         int &item, int lane, bool block) {
+  unsigned long long t0 = 0;
+  unsigned int back = 64;
+#pragma unroll 1
+  for (;;) {
+    // skip the exhausted prefix of each class (one lane; the masks are shared)
+    if (lane == 0) {
+      while (st.lo_u < a.nurgent && prg_bit(s_exh, st.lo_u)) st.lo_u++;
+      while (st.lo_b < a.nnodes && prg_bit(s_exh, st.lo_b)) st.lo_b++;
+    }
+    st.lo_u = __shfl_sync(0xffffffffu, st.lo_u, 0);
+    st.lo_b = __shfl_sync(0xffffffffu, st.lo_b, 0);
+    if (st.lo_u >= a.nurgent && st.lo_b >= a.nnodes) return -1;
+    // pending counts change only when a node completes (new generation)
+    unsigned int g = 0;
+    if (lane == 0) g = prg_ld_acquire(a.gen);
+    g = __shfl_sync(0xffffffffu, g, 0);
+    const bool rescan = g != st.gen_seen || st.lo_u != st.scan_u || st.lo_b != st.scan_b;
+    st.gen_seen = g;
+    st.scan_u = st.lo_u;
+    st.scan_b = st.lo_b;
+    // bulk items only below the concurrency limit: latency-bound chain work
+    // slows several-fold beside saturated memory
+    bool bulk_ok = true;
+    if (a.bulk_limit > 0) {
+      if (lane == 0) bulk_ok = prg_ld_relaxed(a.bulk_active) < (unsigned int)a.bulk_limit;
+      bulk_ok = __shfl_sync(0xffffffffu, bulk_ok, 0);
+    }
+    const int n = lane < PRG_WIN ? st.lo_u + lane : st.lo_b + (lane - PRG_WIN);
+    const bool valid = lane < PRG_WIN ? n < a.nurgent : (bulk_ok && n < a.nnodes);
+    bool cand = false;
+    int items = 0;
+    if (valid && !prg_bit(s_exh, n)) {
+      items = __ldg(&a.nodes[n].items);
+      if (prg_bit(s_rdy, n)) {
+        cand = true;
+      } else if (rescan && prg_ld_acquire(&a.pending[n]) == 0u) {
+        atomicOr(&s_rdy[n >> 5], 1u << (n & 31));
+        cand = true;
+      }
+    }
+    unsigned int m = __ballot_sync(0xffffffffu, cand);
+    while (m) {
+      const int ld = __ffs(m) - 1;
+      int c = 0;
+      if (lane == ld) {
+        c = (int)atomicAdd(&a.claim[n], 1u);
+        if (c >= items) atomicOr(&s_exh[n >> 5], 1u << (n & 31));
+        else if (n >= a.nurgent && a.bulk_limit > 0) atomicAdd(a.bulk_active, 1u);
+      }
+      const int got = __shfl_sync(0xffffffffu, (lane == ld && c < items) ? 1 : 0, ld);
+      if (got) {
+        item = __shfl_sync(0xffffffffu, c, ld);
+        return __shfl_sync(0xffffffffu, n, ld);
+      }
+      m &= m - 1u;
+    }
+    __syncwarp();
+    if (!block) return -3;
+    // nothing to claim: stop on error, else wait (bounded)
+    if (prg_ld_relaxed(a.err)) return -2;
+    const unsigned long long now = prg_clock();
+    if (t0 == 0) {
+      t0 = now;
+    } else if (now - t0 > a.timeout_ns) {
+      if (lane == 0) {
+        atomicCAS(a.err, 0u, 1u);
+        if (a.host_err) *(volatile unsigned int *)a.host_err = 1u;
+      }
+      return -2;
+    }
+    __nanosleep(back);
+    back = back < 2048u ? back * 2u : back;
+  }
+}
+
+// Scheduler warp: one item finished by the workers (after EMPTY).
+__device__ __forceinline__ void prg_complete(const PrgArgs &a, int node, int lane) {
+  if (lane == 0) {
+    if (node >= a.nurgent && a.bulk_limit > 0) atomicSub(a.bulk_active, 1u);
+    __threadfence();
+    const unsigned int old = atomicAdd(&a.done[node], 1u);
+    if (old + 1u == (unsigned int)__ldg(&a.nodes[node].items)) {
+      __threadfence();
+      const int s0 = __ldg(&a.nodes[node].succ0), ns = __ldg(&a.nodes[node].nsucc);
+      for (int q = 0; q < ns; q++) atomicSub(&a.pending[__ldg(&a.succ[s0 + q])], 1u);
+      __threadfence();
+      atomicAdd(a.gen, 1u);
+    }
+  }
+  __syncwarp();
+}
+
+struct PrgSlot {
+  int node, kind;
+  int u0, u1;  // the item's units [u0, u1)
+};
+
+// The scheduler warp's loop (kept out of line: its registers do not count
+// against the worker path).
+template <bool TRACE>
+__device__ __noinline__ void prg_scheduler(const PrgArgs &a, unsigned int *s_exh, unsigned int *s_rdy, PrgSlot *s_slot,
+                                           unsigned char *smem_raw, int lane) {
+  PrgSched st{0, a.nurgent, 0xffffffffu, -1, -1};
+  int pnode0 = -1, pnode1 = -1;  // node whose parameters are in buffer 0 / 1
+  unsigned long long tp0 = 0, tp1 = 0, ts0 = 0, ts1 = 0;  // tracing: claim start, hand-over
+  int titem0 = 0, titem1 = 0;
+  auto stage = [&](int b, int node, int item) {
+    if (lane == 0) {
+      s_slot[b].node = node;
+      if (node >= 0) {
+        const long long per = __ldg(&a.nodes[node].per_item), units = __ldg(&a.nodes[node].units);
+        const long long u0 = (long long)item * per;
+        s_slot[b].kind = __ldg(&a.nodes[node].kind);
+        s_slot[b].u0 = (int)u0;
+        s_slot[b].u1 = (int)(u0 + per < units ? u0 + per : units);
+      }
+    }
+    if (node >= 0 && node != (b ? pnode1 : pnode0)) {
+      const int4 *src = (const int4 *)(a.blob + __ldg(&a.nodes[node].param_off));
+      int4 *dst = (int4 *)(smem_raw + b * prg_pbuf());
+      const int nv = __ldg(&a.nodes[node].param_bytes) >> 4;
+      for (int q = lane; q < nv; q += 32) dst[q] = __ldg(src + q);
+      (b ? pnode1 : pnode0) = node;
+    }
+    if (TRACE) (b ? titem1 : titem0) = item;
+    __syncwarp();
+  };
+  auto publish = [&](int b) {
+    if (TRACE) (b ? ts1 : ts0) = prg_clock();
+    prg_bar_arrive(PRG_BAR_FULL);
+  };
+  auto record = [&](int b, int node) {
+    if (!TRACE || lane != 0) return;
+    const unsigned int r = atomicAdd(a.trace_n, 1u);
+    if (r < a.trace_cap) {
+      unsigned int sm;
+      asm volatile("mov.u32 %0, %%smid;" : "=r"(sm));
+      PrgTraceRec &T = a.trace[r];
+      T.t_pick = b ? tp1 : tp0;
+      T.t_start = b ? ts1 : ts0;
+      T.t_end = prg_clock();
+      T.plan_node = __ldg(&a.nodes[node].plan_index);
+      T.item = b ? titem1 : titem0;
+      T.sm = (int)sm;
+      T.cta = blockIdx.x;
+      T.launch = a.launch;
+      T.pad_ = 0;
+    }
+  };
+  int b = 0, item = 0;
+  if (TRACE) tp0 = prg_clock();
+  int run = prg_claim(a, s_exh, s_rdy, st, item, lane, true);
+  stage(b, run, item);
+  publish(b);
+  if (run < 0) return;
+  b ^= 1;
+#pragma unroll 1
+  for (;;) {
+    // stage the next item while the workers run the current one
+    if (TRACE) (b ? tp1 : tp0) = prg_clock();
+    int nxt = prg_claim(a, s_exh, s_rdy, st, item, lane, false);
+    if (nxt >= 0) stage(b, nxt, item);
+    prg_bar_sync(PRG_BAR_EMPTY);
+    record(b ^ 1, run);
+    if (nxt >= 0) {
+      publish(b);
+      prg_complete(a, run, lane);
+    } else {
+      prg_complete(a, run, lane);
+      if (nxt == -3) {
+        if (TRACE) (b ? tp1 : tp0) = prg_clock();
+        nxt = prg_claim(a, s_exh, s_rdy, st, item, lane, true);
+      }
+      stage(b, nxt < 0 ? -1 : nxt, item);
+      publish(b);
+      if (nxt < 0) return;
+    }
+    run = nxt;
+    b ^= 1;
+  }
+}
+
+template <int P, bool TRACE>
+__global__ void __launch_bounds__(PRG_THREADS, P == MB_PREC_F64 ? 2 : 5) k_program(const __grid_constant__ PrgArgs a) {
+  using R = typename Prec<P>::R;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ unsigned int s_exh[PRG_MAX_NODES / 32], s_rdy[PRG_MAX_NODES / 32];
+  __shared__ PrgSlot s_slot[2];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (int q = tid; q < PRG_MAX_NODES / 32; q += PRG_THREADS) {
+    s_exh[q] = 0u;
+    s_rdy[q] = 0u;
+  }
+  __syncthreads();
+
+  if (warp == PRG_SCHED_WARP) {
+    prg_scheduler<TRACE>(a, s_exh, s_rdy, s_slot, smem_raw, lane);
+    return;
+  }
+
+  // ---------------- worker warps ----------------
+  int b = 0;
+#pragma unroll 1
+  for (;;) {
+    prg_bar_sync(PRG_BAR_FULL);
+    if (s_slot[b].node < 0) break;
+    const int kind = s_slot[b].kind, u0 = s_slot[b].u0, u1 = s_slot[b].u1;
+    const unsigned char *pb = smem_raw + b * prg_pbuf();
+    if (kind == PK_STB) {
+      const StbParams &p = *(const StbParams *)pb;
+      for (int g = u0 + tid; g < u1; g += PRG_WORKERS) stb_at<P>(p, g);
+    } else if (kind == PK_REC) {
+      const RecOpsParams &p = *(const RecOpsParams *)pb;
+      for (int g = u0 + tid; g < u1; g += PRG_WORKERS) rec_point<P>(p, g);
+    } else if (kind == PK_SPL) {
+      const SplParamsP &p = *(const SplParamsP *)pb;
+      const int sid = u0 + warp;
+      if (warp < SPL_WARPS && sid < u1)
+        spl_segment<P, false>(p, sid, lane, smem_raw + 2 * prg_pbuf() + warp * spl_warp_smem<R>());
+    }
+    prg_bar_arrive(PRG_BAR_EMPTY);
+    b ^= 1;
   }
 }
 

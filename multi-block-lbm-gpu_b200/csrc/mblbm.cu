@@ -60,6 +60,14 @@ struct CompiledPlan {
   cudaGraphExec_t exec = nullptr;
   SchedState end;
   long long kernels = 0;
+  // persistent executor (graph mode 3)
+  bool prg_built = false;
+  PrgArgs prg{};
+  unsigned int *prg_state = nullptr;       // claim | done | pending
+  const unsigned int *prg_init = nullptr;  // their values at launch
+  size_t prg_state_bytes = 0;
+  int prg_grid = 0;
+  size_t prg_smem = 0;
   ~CompiledPlan() {
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
@@ -110,9 +118,26 @@ struct mb_ctx {
   int use_graph = 1;
   int period = 1;
   long long split_cells = 1000000;
+  long long stream_cells = 2000000;
+  int bulk_levels = 0;                // 1: whole-level block steps that stream with hints are bulk (low priority) work   // block steps over >= this many cells use evict-first cache hints (0: never)
   int stb_variant[MB_MAX_LEVEL] = {0};  // 0: one cell per thread, 1: quads (k_block_step_q)
   int bulk_ctas_per_sm = 0;             // >0: cap interior (bulk) block-step grids at this many CTAs per SM
   int num_sms = 148;
+  // persistent executor
+  unsigned int *d_prg_err = nullptr;    // device error word of k_program
+  unsigned int *h_prg_err = nullptr;    // mapped pinned mirror, read after any synchronisation
+  unsigned int *d_prg_err_host = nullptr;
+  unsigned long long prg_timeout_ns = 2000000000ull;
+  int prg_bulk_cells = 512;             // cells per item of bulk block-step nodes
+  int prg_urgent_cells = 256;           // cells per item of the other block-step nodes
+  int prg_periods = 2;                  // scheduler periods per executor launch
+  int prg_bulk_limit = 0;               // CTAs allowed on bulk items at once (0: no limit)
+  int rec_points = 32;                  // interface points per record CTA / executor item
+  int spl_segs = 1;                     // spline segments per CTA / executor item
+  PrgTraceRec *d_trace = nullptr;       // executor trace (mb_set_program_trace)
+  unsigned int *d_trace_n = nullptr;
+  unsigned int trace_cap = 0;
+  int prg_launches = 0;
   std::map<std::string, std::unique_ptr<CompiledPlan>> plans;
   long long kernels_last_call = 0;
   long long kernels_per_step = 0;
@@ -162,12 +187,18 @@ void *kfunc(int prec) {
   if (prec == MB_PREC_F32U) return K<MB_PREC_F32U>::ptr();
   return K<MB_PREC_F16S>::ptr();
 }
-template <int P> struct KStb { static void *ptr() { return (void *)k_block_step<P>; } };
+template <int P> struct KStb { static void *ptr() { return (void *)k_block_step<P, 1>; } };
+template <int P> struct KStb2 { static void *ptr() { return (void *)k_block_step<P, 2>; } };
+template <int P> struct KStbR { static void *ptr() { return (void *)k_block_step_r<P, false>; } };
+template <int P> struct KStbRI { static void *ptr() { return (void *)k_block_step_r<P, true>; } };
 template <int P> struct KStbQ { static void *ptr() { return (void *)k_block_step_q<P>; } };
 template <int P> struct KRec { static void *ptr() { return (void *)k_records<P>; } };
 template <int P> struct KSpl { static void *ptr() { return (void *)k_spline<P>; } };
 template <int P> struct KDrag { static void *ptr() { return (void *)k_drag<P>; } };
 template <int P> struct KL2 { static void *ptr() { return (void *)k_error_l2<P>; } };
+template <int P> struct KPrg { static void *ptr() { return (void *)k_program<P, false>; } };
+template <int P> struct KPrgT { static void *ptr() { return (void *)k_program<P, true>; } };
+size_t program_smem(int prec) { return prec == MB_PREC_F64 ? prg_smem<double>() : prg_smem<float>(); }
 
 // dynamic shared memory of k_spline per warp: two 12 x window arrays and the
 // window's c' and 1/den
@@ -199,7 +230,9 @@ StbParams make_stb(mb_ctx *c, int a0, int a1, uint64_t parity, int macro_all, in
   p.rho0 = c->geo.config.rho0;
   p.u0x = c->geo.config.U0[0];
   p.u0y = c->geo.config.U0[1];
-  long long cell = 0, wt = 0;
+  long long cell = 0, wt = 0, rt = 0, level_cells = 0;
+  for (int a = a0; a < a1; a++) level_cells += region_cells(c->blk[a].nx, c->blk[a].ny, region);
+  p.evict_first = c->stream_cells > 0 && level_cells >= c->stream_cells;
   for (int a = a0; a < a1; a++) {
     const IfBlk &B = c->blk[a];
     const int cur = (parity >> a) & 1;
@@ -223,14 +256,55 @@ StbParams make_stb(mb_ctx *c, int a0, int a1, uint64_t parity, int macro_all, in
     const int nrows = region == STB_INTERIOR ? std::max(0, B.ny - 4) : B.ny;
     s.wt0 = wt;
     wt += (long long)s.tiles_x * nrows;
+    // row kernel: tiles of 256 cells over the region's columns
+    s.col0 = region == STB_INTERIOR ? 2 : 0;
+    s.col1 = region == STB_INTERIOR ? B.nx - 3 : B.nx - 1;
+    const int ncols = std::max(0, s.col1 - s.col0 + 1);
+    s.rtiles_x = std::max(1, (ncols + 255) / 256);
+    s.rt0 = (int)rt;
+    rt += ncols > 0 ? (long long)s.rtiles_x * nrows : 0;
   }
+  p.rtiles = rt;
   p.total = quads ? wt : cell;
   return p;
 }
 
 // the rim is always stepped one cell per thread
 bool stb_uses_quads(const mb_ctx *c, int level, int region) {
-  return region != STB_RIM && c->stb_variant[level] == 1;
+  return region != STB_RIM && c->stb_variant[level] == 1 && c->use_graph != 3;
+}
+
+bool background_capped(const mb_ctx *c, bool background) { return background && c->bulk_ctas_per_sm > 0; }
+
+// the row kernel indexes 9 planes of a block with 32-bit offsets
+bool rows_fit(const mb_ctx *c, const StbParams &p) {
+  for (int t = 0; t < p.nblk; t++)
+    if (9 * p.b[t].plane >= (1LL << 31) || (long long)p.b[t].ny * p.b[t].pitch >= (1LL << 31)) return false;
+  (void)c;
+  return p.rtiles < (1LL << 31);
+}
+
+// kernel and grid of a block-step launch (variant 0: one cell per thread,
+// 1: quads, 2: two cells per thread, 3: row tiles); background grids may be
+// capped
+void stb_launch_shape(const mb_ctx *c, int level, int region, bool background, const StbParams &p, void **func,
+                      dim3 *grid) {
+  if (stb_uses_quads(c, level, region)) {
+    *func = kfunc<KStbQ>(c->prec);
+    *grid = dim3((unsigned)((p.total + 7) / 8));  // 8 warp tiles per CTA
+    return;
+  }
+  if (c->stb_variant[level] == 3 && region != STB_RIM && !background_capped(c, background) && rows_fit(c, p)) {
+    *func = region == STB_INTERIOR ? kfunc<KStbRI>(c->prec) : kfunc<KStbR>(c->prec);
+    *grid = dim3((unsigned)p.rtiles);
+    return;
+  }
+  const bool two = c->stb_variant[level] == 2;
+  *func = two ? kfunc<KStb2>(c->prec) : kfunc<KStb>(c->prec);
+  const long long per = two ? 512 : 256;
+  long long ctas = (p.total + per - 1) / per;
+  if (background && c->bulk_ctas_per_sm > 0) ctas = std::min<long long>(ctas, (long long)c->bulk_ctas_per_sm * c->num_sms);
+  *grid = dim3((unsigned)std::max<long long>(ctas, 0));
 }
 
 int lower_plan(mb_ctx *c, CompiledPlan &cp) {
@@ -243,18 +317,11 @@ int lower_plan(mb_ctx *c, CompiledPlan &cp) {
     if (n.kind == NK_STB) {
       const bool quads = stb_uses_quads(c, n.level, n.region);
       d.stb = make_stb(c, n.a0, n.a1, n.parity, n.macro_all, 1, n.region, quads);
-      d.background = (n.region == STB_INTERIOR);
+      // bulk: interiors of split levels, and whole levels streamed with
+      // evict-first hints when bulk_levels is set
+      d.background = (n.region == STB_INTERIOR) || (c->bulk_levels && n.region == STB_ALL && d.stb.evict_first);
       d.block = dim3(256);
-      if (quads) {
-        d.func = kfunc<KStbQ>(c->prec);
-        d.grid = dim3((unsigned)((d.stb.total + 7) / 8));  // 8 warp tiles per CTA
-      } else {
-        d.func = kfunc<KStb>(c->prec);
-        long long ctas = (d.stb.total + 255) / 256;
-        if (d.background && c->bulk_ctas_per_sm > 0)
-          ctas = std::min<long long>(ctas, (long long)c->bulk_ctas_per_sm * c->num_sms);
-        d.grid = dim3((unsigned)ctas);
-      }
+      stb_launch_shape(c, n.level, n.region, d.background, d.stb, &d.func, &d.grid);
       d.args[0] = &d.stb;
     } else if (n.kind == NK_REC) {
       if ((int)n.ops.size() > REC_MAX_OPS) return MB_ERR_UNSUPPORTED;
@@ -310,8 +377,10 @@ int lower_plan(mb_ctx *c, CompiledPlan &cp) {
         d.rec.b[a] = {{B.F[0], B.F[1]}, B.rho, B.ux, B.uy, B.plane, B.tau, B.m, 0};
       }
       d.func = kfunc<KRec>(c->prec);
-      d.block = dim3(REC_THREADS);  // small CTAs spread a launch's scattered accesses over many SMs
-      d.grid = dim3((unsigned)((total + REC_THREADS - 1) / REC_THREADS));
+      // small CTAs spread a launch's scattered accesses (one cache sector
+      // per value on lines across rows) over many SMs' load/store units
+      d.block = dim3(c->rec_points);
+      d.grid = dim3((unsigned)((total + c->rec_points - 1) / c->rec_points));
       d.args[0] = &d.rec;
     } else {
       if ((int)n.spl.size() > SPL_MAX_TASKS) return MB_ERR_UNSUPPORTED;
@@ -347,9 +416,9 @@ int lower_plan(mb_ctx *c, CompiledPlan &cp) {
       d.spl.slots = c->d_slots;
       d.spl.coef = c->d_spl_coef;
       d.func = kfunc<KSpl>(c->prec);
-      d.block = dim3(32 * SPL_WARPS);
-      d.grid = dim3((unsigned)((nseg + SPL_WARPS - 1) / SPL_WARPS));
-      d.smem = spline_smem(c->prec);
+      d.block = dim3(32 * c->spl_segs);
+      d.grid = dim3((unsigned)((nseg + c->spl_segs - 1) / c->spl_segs));
+      d.smem = spline_smem(c->prec) / SPL_WARPS * c->spl_segs;
       d.args[0] = &d.spl;
     }
   }
@@ -420,14 +489,168 @@ int build_graph(CompiledPlan &cp, bool pdl) {
       MB_CUDA(cudaGraphAddDependencies_v2(cp.graph, &from, &gn[q], &ed, 1));
     }
   }
-  MB_CUDA(cudaGraphInstantiate(&cp.exec, cp.graph, 0));
+  // node priorities only take effect when the graph is instantiated with them
+  MB_CUDA(cudaGraphInstantiateWithFlags(&cp.exec, cp.graph, cudaGraphInstantiateFlagUseNodePriority));
   return MB_OK;
 }
 
 int set_smem_limits(int prec) {
   MB_CUDA(cudaFuncSetAttribute(kfunc<KSpl>(prec), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)spline_smem(prec)));
+  MB_CUDA(cudaFuncSetAttribute(kfunc<KPrg>(prec), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)program_smem(prec)));
+  MB_CUDA(cudaFuncSetAttribute(kfunc<KPrgT>(prec), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)program_smem(prec)));
   return MB_OK;
+}
+
+// ---- persistent executor ------------------------------------------------------
+// Lays the lowered nodes out as an executor program: nodes without work are
+// dropped (their successors inherit their dependencies), urgent nodes come
+// first and bulk (interior block-step) nodes after them, each class in plan
+// order, which is a topological order.
+int build_program(mb_ctx *c, CompiledPlan &cp) {
+  const int nd = (int)cp.dn.size();
+  std::vector<long long> units(nd, 0);
+  std::vector<int> per(nd, 1), kind(nd, 0);
+  for (int q = 0; q < nd; q++) {
+    const DevPlanNode &d = cp.dn[q];
+    if (d.kind == NK_STB) {
+      kind[q] = PK_STB;
+      units[q] = d.stb.total;
+      per[q] = d.background ? c->prg_bulk_cells : c->prg_urgent_cells;
+    } else if (d.kind == NK_REC) {
+      kind[q] = PK_REC;
+      units[q] = d.rec.total;
+      per[q] = c->rec_points;
+    } else {
+      kind[q] = PK_SPL;
+      units[q] = d.spl.nseg;
+      per[q] = c->spl_segs;
+    }
+  }
+  // effective dependencies over non-empty nodes
+  std::vector<std::vector<int>> eff(nd);
+  for (int q = 0; q < nd; q++) {
+    std::vector<int> out;
+    for (int p : cp.dn[q].deps) {
+      if (units[p] > 0) out.push_back(p);
+      else out.insert(out.end(), eff[p].begin(), eff[p].end());
+    }
+    std::sort(out.begin(), out.end());
+    out.erase(std::unique(out.begin(), out.end()), out.end());
+    eff[q] = std::move(out);
+  }
+  std::vector<int> order;
+  for (int pass = 0; pass < 2; pass++)
+    for (int q = 0; q < nd; q++)
+      if (units[q] > 0 && cp.dn[q].background == (pass == 1)) order.push_back(q);
+  const int nn = (int)order.size();
+  if (nn > PRG_MAX_NODES) return MB_ERR_UNSUPPORTED;
+  for (int q = 0; q < nd; q++)
+    if (units[q] >= (1LL << 31) - (1LL << 25)) return MB_ERR_UNSUPPORTED;  // item bounds are 32-bit
+  int nurgent = 0;
+  for (int q : order) nurgent += cp.dn[q].background ? 0 : 1;
+  std::vector<int> pos(nd, -1);
+  for (int i = 0; i < nn; i++) pos[order[i]] = i;
+  std::vector<std::vector<int>> succ(nn);
+  std::vector<unsigned int> pending(nn, 0);
+  for (int i = 0; i < nn; i++)
+    for (int p : eff[order[i]]) {
+      succ[pos[p]].push_back(i);
+      pending[i]++;
+    }
+  // node table, successor lists and parameter blob
+  std::vector<PrgNode> nodes(nn);
+  std::vector<int> sl;
+  std::vector<unsigned char> blob;
+  for (int i = 0; i < nn; i++) {
+    const int q = order[i];
+    const DevPlanNode &d = cp.dn[q];
+    PrgNode &N = nodes[i];
+    N = PrgNode{};
+    N.kind = kind[q];
+    N.units = units[q];
+    N.per_item = per[q];
+    N.items = (int)((units[q] + per[q] - 1) / per[q]);
+    const void *src = kind[q] == PK_STB ? (const void *)&d.stb : kind[q] == PK_REC ? (const void *)&d.rec : (const void *)&d.spl;
+    const size_t sz = kind[q] == PK_STB ? sizeof(StbParams) : kind[q] == PK_REC ? sizeof(RecOpsParams) : sizeof(SplParamsP);
+    const size_t padded = (sz + 15) / 16 * 16;
+    N.param_off = (int)blob.size();
+    N.param_bytes = (int)padded;
+    blob.resize(blob.size() + padded, 0);
+    std::memcpy(blob.data() + N.param_off, src, sz);
+    N.succ0 = (int)sl.size();
+    N.nsucc = (int)succ[i].size();
+    N.plan_index = q;
+    sl.insert(sl.end(), succ[i].begin(), succ[i].end());
+  }
+  // one allocation: nodes | succ | blob | init state | state
+  auto al = [](size_t v) { return (v + 255) / 256 * 256; };
+  const size_t o_nodes = 0, o_succ = al(nn * sizeof(PrgNode)), o_blob = o_succ + al(std::max<size_t>(sl.size(), 1) * sizeof(int));
+  const size_t st_bytes = (3 * (size_t)nn + 2) * sizeof(unsigned int);  // claim, done, pending, generation, bulk
+  const size_t o_init = o_blob + al(std::max<size_t>(blob.size(), 16)), o_state = o_init + al(st_bytes);
+  const size_t total = o_state + al(st_bytes);
+  std::vector<unsigned char> host(total, 0);
+  std::memcpy(host.data() + o_nodes, nodes.data(), nn * sizeof(PrgNode));
+  if (!sl.empty()) std::memcpy(host.data() + o_succ, sl.data(), sl.size() * sizeof(int));
+  if (!blob.empty()) std::memcpy(host.data() + o_blob, blob.data(), blob.size());
+  std::memcpy(host.data() + o_init + 2 * nn * sizeof(unsigned int), pending.data(), nn * sizeof(unsigned int));
+  unsigned char *dp = nullptr;
+  if (cudaMalloc(&dp, total) != cudaSuccess) return MB_ERR_NOMEM;
+  cp.dev_allocs.push_back(dp);
+  MB_CUDA(cudaMemcpy(dp, host.data(), total, cudaMemcpyHostToDevice));
+  cp.prg_state = (unsigned int *)(dp + o_state);
+  cp.prg_init = (const unsigned int *)(dp + o_init);
+  cp.prg_state_bytes = st_bytes;
+  PrgArgs &a = cp.prg;
+  a.nodes = (const PrgNode *)(dp + o_nodes);
+  a.succ = (const int *)(dp + o_succ);
+  a.blob = dp + o_blob;
+  a.claim = cp.prg_state;
+  a.done = cp.prg_state + nn;
+  a.pending = cp.prg_state + 2 * nn;
+  a.gen = cp.prg_state + 3 * nn;
+  a.bulk_active = cp.prg_state + 3 * nn + 1;
+  a.bulk_limit = c->prg_bulk_limit;
+  a.err = c->d_prg_err;
+  a.host_err = c->d_prg_err_host;
+  a.nnodes = nn;
+  a.nurgent = nurgent;
+  a.timeout_ns = c->prg_timeout_ns;
+  cp.prg_smem = program_smem(c->prec);
+  int per_sm = 0;
+  MB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfunc<KPrg>(c->prec), PRG_THREADS, cp.prg_smem));
+  if (per_sm < 1) return MB_ERR_UNSUPPORTED;
+  long long items = 0;
+  for (auto &N : nodes) items += N.items;
+  cp.prg_grid = (int)std::max<long long>(1, std::min<long long>((long long)per_sm * c->num_sms, items));
+  cp.prg_built = true;
+  return MB_OK;
+}
+
+int launch_program(mb_ctx *c, CompiledPlan &cp, cudaStream_t s) {
+  if (cp.prg.nnodes == 0) return MB_OK;
+  cp.prg.timeout_ns = c->prg_timeout_ns;
+  cp.prg.trace = c->d_trace;
+  cp.prg.trace_n = c->d_trace_n;
+  cp.prg.trace_cap = c->trace_cap;
+  cp.prg.launch = c->prg_launches++;
+  cp.prg.bulk_limit = c->prg_bulk_limit;
+  MB_CUDA(cudaMemcpyAsync(cp.prg_state, cp.prg_init, cp.prg_state_bytes, cudaMemcpyDeviceToDevice, s));
+  void *args[1] = {&cp.prg};
+  void *fn = c->d_trace ? kfunc<KPrgT>(c->prec) : kfunc<KPrg>(c->prec);
+  MB_CUDA(cudaLaunchKernel(fn, dim3(cp.prg_grid), dim3(PRG_THREADS), args, cp.prg_smem, s));
+  return MB_OK;
+}
+
+// error word of the persistent executor: MB_ERR_TIMEOUT once after a launch
+// gave up waiting (valid after the launch's stream has been synchronised)
+int program_status(mb_ctx *c) {
+  if (!c->h_prg_err || *(volatile unsigned int *)c->h_prg_err == 0u) return MB_OK;
+  *(volatile unsigned int *)c->h_prg_err = 0u;
+  cudaMemset(c->d_prg_err, 0, sizeof(unsigned int));
+  return MB_ERR_TIMEOUT;
 }
 
 CompiledPlan *get_plan(mb_ctx *c, int n, bool final_macros, int *err) {
@@ -449,6 +672,13 @@ CompiledPlan *get_plan(mb_ctx *c, int n, bool final_macros, int *err) {
 
 int exec_plan(mb_ctx *c, CompiledPlan *cp, cudaStream_t s) {
   int e;
+  if (c->use_graph == 3) {
+    if (!cp->prg_built && (e = build_program(c, *cp))) return e;
+    if ((e = launch_program(c, *cp, s))) return e;
+    c->state = cp->end;
+    c->kernels_last_call += 1;
+    return MB_OK;
+  }
   if (c->use_graph) {
     if (!cp->exec) {
       e = build_graph(*cp, c->use_graph == 2);
@@ -709,6 +939,12 @@ extern "C" int mb_create(const mb_geometry *geo, int precision, mb_ctx **out) {
     }
     c->updates_per_step = upd;
   }
+  // error word of the persistent executor, mirrored into mapped host memory
+  if ((e = dalloc(c.get(), &c->d_prg_err, 1))) return e;
+  MB_CUDA(cudaMemset(c->d_prg_err, 0, sizeof(unsigned int)));
+  MB_CUDA(cudaHostAlloc(&c->h_prg_err, sizeof(unsigned int), cudaHostAllocMapped));
+  *c->h_prg_err = 0u;
+  MB_CUDA(cudaHostGetDevicePointer((void **)&c->d_prg_err_host, c->h_prg_err, 0));
   if ((e = set_smem_limits(precision))) return e;
   *out = c.release();
   return MB_OK;
@@ -721,6 +957,9 @@ extern "C" int mb_destroy(mb_ctx *c) {
   for (void *p : c->allocs) cudaFree(p);
   if (c->h_drag_out) cudaFreeHost(c->h_drag_out);
   if (c->h_l2_out) cudaFreeHost(c->h_l2_out);
+  if (c->h_prg_err) cudaFreeHost(c->h_prg_err);
+  if (c->d_trace) cudaFree(c->d_trace);
+  if (c->d_trace_n) cudaFree(c->d_trace_n);
   delete c;
   return MB_OK;
 }
@@ -733,8 +972,27 @@ extern "C" int mb_set_split_cells(mb_ctx *c, long long cells) {
   return MB_OK;
 }
 
+extern "C" int mb_set_interface_shape(mb_ctx *c, int rec_points, int spline_segments) {
+  if (!c || (rec_points != 32 && rec_points != 64) || spline_segments < 1 || spline_segments > SPL_WARPS)
+    return MB_ERR_INVALID;
+  cudaDeviceSynchronize();
+  c->rec_points = rec_points;
+  c->spl_segs = spline_segments;
+  c->plans.clear();
+  return MB_OK;
+}
+
+extern "C" int mb_set_stream_cells(mb_ctx *c, long long cells, int bulk) {
+  if (!c || cells < 0 || bulk < 0 || bulk > 1) return MB_ERR_INVALID;
+  cudaDeviceSynchronize();
+  c->stream_cells = cells;
+  c->bulk_levels = bulk;
+  c->plans.clear();
+  return MB_OK;
+}
+
 extern "C" int mb_set_stb_variant(mb_ctx *c, int level, int variant) {
-  if (!c || level < 0 || level >= c->geo.layout.LEVEL || variant < 0 || variant > 1) return MB_ERR_INVALID;
+  if (!c || level < 0 || level >= c->geo.layout.LEVEL || variant < 0 || variant > 3) return MB_ERR_INVALID;
   cudaDeviceSynchronize();
   c->stb_variant[level] = variant;
   c->plans.clear();
@@ -749,8 +1007,121 @@ extern "C" int mb_set_bulk_occupancy(mb_ctx *c, int ctas_per_sm) {
   return MB_OK;
 }
 
+extern "C" int mb_set_program_timeout(mb_ctx *c, double seconds) {
+  if (!c || !(seconds > 0) || seconds > 600) return MB_ERR_INVALID;
+  c->prg_timeout_ns = (unsigned long long)(seconds * 1e9);
+  return MB_OK;
+}
+
+extern "C" int mb_set_program_shape(mb_ctx *c, int bulk_cells, int urgent_cells, int periods_per_launch,
+                                    int bulk_ctas) {
+  if (!c || bulk_cells < 1 || urgent_cells < 1 || bulk_cells > (1 << 24) || urgent_cells > (1 << 24) ||
+      periods_per_launch < 1 || periods_per_launch > 16 || bulk_ctas < 0)
+    return MB_ERR_INVALID;
+  c->prg_bulk_limit = bulk_ctas;
+  cudaDeviceSynchronize();
+  c->prg_bulk_cells = bulk_cells;
+  c->prg_urgent_cells = urgent_cells;
+  c->prg_periods = periods_per_launch;
+  c->plans.clear();
+  return MB_OK;
+}
+
+extern "C" int mb_set_program_trace(mb_ctx *c, long long capacity) {
+  if (!c || capacity < 0 || capacity > (1LL << 26)) return MB_ERR_INVALID;
+  cudaDeviceSynchronize();
+  if (c->d_trace) cudaFree(c->d_trace);
+  if (c->d_trace_n) cudaFree(c->d_trace_n);
+  c->d_trace = nullptr;
+  c->d_trace_n = nullptr;
+  c->trace_cap = 0;
+  if (capacity == 0) return MB_OK;
+  if (cudaMalloc(&c->d_trace, (size_t)capacity * sizeof(PrgTraceRec)) != cudaSuccess) return MB_ERR_NOMEM;
+  if (cudaMalloc(&c->d_trace_n, sizeof(unsigned int)) != cudaSuccess) return MB_ERR_NOMEM;
+  MB_CUDA(cudaMemset(c->d_trace_n, 0, sizeof(unsigned int)));
+  c->trace_cap = (unsigned int)capacity;
+  return MB_OK;
+}
+
+extern "C" int mb_program_trace(mb_ctx *c, void *records, long long max_records, long long *n_records) {
+  if (!c || !n_records || max_records < 0) return MB_ERR_INVALID;
+  *n_records = 0;
+  if (!c->d_trace) return MB_OK;
+  MB_CUDA(cudaDeviceSynchronize());
+  unsigned int n = 0;
+  MB_CUDA(cudaMemcpy(&n, c->d_trace_n, sizeof(n), cudaMemcpyDeviceToHost));
+  const long long have = std::min<long long>(n, c->trace_cap);
+  const long long m = std::min<long long>(have, max_records);
+  if (m > 0 && records) MB_CUDA(cudaMemcpy(records, c->d_trace, (size_t)m * sizeof(PrgTraceRec), cudaMemcpyDeviceToHost));
+  MB_CUDA(cudaMemset(c->d_trace_n, 0, sizeof(unsigned int)));
+  *n_records = m;
+  return MB_OK;
+}
+
+extern "C" int mb_sync(mb_ctx *c, mb_stream stream) {
+  if (!c) return MB_ERR_INVALID;
+  MB_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+  return program_status(c);
+}
+
+// One executor launch over a single node with no work.  With stall = 1 the
+// node starts with one unmet dependency that no node satisfies: every CTA
+// waits out the executor timeout, sets the error word and exits.
+extern "C" int mb_program_selftest(mb_ctx *c, int stall, mb_stream stream) {
+  if (!c || stall < 0 || stall > 1) return MB_ERR_INVALID;
+  cudaStream_t s = (cudaStream_t)stream;
+  MB_CUDA(cudaStreamSynchronize(s));
+  if (int st = program_status(c)) return st;
+  PrgNode N{};
+  N.kind = PK_NOP;
+  N.items = 1;
+  N.units = 1;
+  N.per_item = 1;
+  unsigned int st0[5] = {0u, 0u, (unsigned int)stall, 0u, 0u};
+  unsigned char *dp = nullptr;
+  if (cudaMalloc(&dp, 512) != cudaSuccess) return MB_ERR_NOMEM;
+  int rc = MB_OK;
+  do {
+    if (cudaMemcpy(dp, &N, sizeof(N), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(dp + 256, st0, sizeof(st0), cudaMemcpyHostToDevice) != cudaSuccess) {
+      rc = MB_ERR_CUDA;
+      break;
+    }
+    PrgArgs a{};
+    a.nodes = (const PrgNode *)dp;
+    a.succ = (const int *)(dp + 128);
+    a.blob = dp + 128;
+    a.claim = (unsigned int *)(dp + 256);
+    a.done = a.claim + 1;
+    a.pending = a.claim + 2;
+    a.gen = a.claim + 3;
+    a.bulk_active = a.claim + 4;
+    a.err = c->d_prg_err;
+    a.host_err = c->d_prg_err_host;
+    a.nnodes = 1;
+    a.nurgent = 1;
+    a.timeout_ns = c->prg_timeout_ns;
+    void *args[1] = {&a};
+    if (cudaLaunchKernel(kfunc<KPrg>(c->prec), dim3(2 * c->num_sms), dim3(PRG_THREADS), args, program_smem(c->prec), s) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+      rc = MB_ERR_CUDA;
+      break;
+    }
+    unsigned int done = 0;
+    if (cudaMemcpy(&done, a.done, sizeof(done), cudaMemcpyDeviceToHost) != cudaSuccess) {
+      rc = MB_ERR_CUDA;
+      break;
+    }
+    rc = program_status(c);
+    if (rc == MB_OK && done != 1u) rc = MB_ERR_STATE;
+  } while (0);
+  cudaFree(dp);
+  return rc;
+}
+
 extern "C" int mb_set_graph_mode(mb_ctx *c, int mode) {
-  if (!c || mode < 0 || mode > 2) return MB_ERR_INVALID;
+  if (!c || mode < 0 || mode > 3) return MB_ERR_INVALID;
   if (mode != c->use_graph) {
     cudaDeviceSynchronize();
     c->plans.clear();
@@ -817,7 +1188,7 @@ extern "C" int mb_step(mb_ctx *c, int n, mb_stream stream) {
   cudaStream_t s = (cudaStream_t)stream;
   c->kernels_last_call = 0;
   int remaining = n;
-  const int G = c->period;
+  const int G = c->use_graph == 3 ? c->period * c->prg_periods : c->period;
   while (remaining > 0) {
     int chunk;
     bool fin;
@@ -848,7 +1219,7 @@ extern "C" int mb_prepare(mb_ctx *c, int n) {
   if (!c->inited) return MB_ERR_STATE;
   const SchedState save = c->state;
   int remaining = n, err = 0;
-  const int G = c->period;
+  const int G = c->use_graph == 3 ? c->period * c->prg_periods : c->period;
   while (remaining > 0) {
     int chunk;
     bool fin;
@@ -857,7 +1228,12 @@ extern "C" int mb_prepare(mb_ctx *c, int n) {
     else { chunk = 1; fin = true; }
     CompiledPlan *cp = get_plan(c, chunk, fin, &err);
     if (!cp) { c->state = save; return err ? err : MB_ERR_INVALID; }
-    if (c->use_graph && !cp->exec && (err = build_graph(*cp, c->use_graph == 2))) { c->state = save; return err; }
+    if (c->use_graph == 3) {
+      if (!cp->prg_built && (err = build_program(c, *cp))) { c->state = save; return err; }
+    } else if (c->use_graph && !cp->exec && (err = build_graph(*cp, c->use_graph == 2))) {
+      c->state = save;
+      return err;
+    }
     c->state = cp->end;
     remaining -= chunk;
   }
@@ -934,6 +1310,7 @@ extern "C" int mb_drag(mb_ctx *c, double force[2], double *cd, double *cl, mb_st
   MB_CUDA(cudaLaunchKernel(kfunc<KDrag>(c->prec), dim3(1), dim3(1024), args, 0, s));
   MB_CUDA(cudaMemcpyAsync(c->h_drag_out, c->d_drag_out, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
   MB_CUDA(cudaStreamSynchronize(s));
+  if (int st = program_status(c)) return st;
   force[0] = c->h_drag_out[0];
   force[1] = c->h_drag_out[1];
   const mb_config &cfg = c->geo.config;
@@ -967,6 +1344,7 @@ extern "C" int mb_error_L2(mb_ctx *c, double *e, mb_stream stream) {
   MB_CUDA(cudaLaunchKernel(kfunc<KL2>(c->prec), dim3(c->l2_grid), dim3(256), args, 0, s));
   MB_CUDA(cudaMemcpyAsync(c->h_l2_out, c->d_l2_out, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
   MB_CUDA(cudaStreamSynchronize(s));
+  if (int st = program_status(c)) return st;
   *e = std::sqrt(c->h_l2_out[0]) / std::sqrt(c->h_l2_out[1]);
   return MB_OK;
 }
@@ -985,6 +1363,7 @@ extern "C" int mb_check_finite(mb_ctx *c, long long *bad, mb_stream stream) {
   unsigned long long h = 0;
   MB_CUDA(cudaMemcpyAsync(&h, c->d_count, sizeof(h), cudaMemcpyDeviceToHost, s));
   MB_CUDA(cudaStreamSynchronize(s));
+  if (int st = program_status(c)) return st;
   *bad = (long long)h;
   return h ? MB_ERR_NUMERIC : MB_OK;
 }
@@ -1003,6 +1382,8 @@ extern "C" int mb_copy_fields(mb_ctx *c, int a, double *rho, double *ux, double 
                               mb_stream stream) {
   if (!c || a < 0 || a >= c->nblk) return MB_ERR_INVALID;
   cudaStream_t s = (cudaStream_t)stream;
+  MB_CUDA(cudaStreamSynchronize(s));
+  if (int st = program_status(c)) return st;
   const IfBlk &B = c->blk[a];
   const long long n = (long long)B.nx * B.ny;
   int e = ensure_stage(c, (size_t)9 * n);
@@ -1231,11 +1612,13 @@ extern "C" int mb_time_block_step(mb_ctx *c, int level, int n, mb_stream stream,
     ps.push_back(make_stb(c, a0, a1, par, 0, 0, STB_ALL, stb_uses_quads(c, level, STB_ALL)));
     for (int a = a0; a < a1; a++) tot += (long long)c->blk[a].nx * c->blk[a].ny;
   }
-  const bool quads = stb_uses_quads(c, level, STB_ALL);
-  void *fn = quads ? kfunc<KStbQ>(c->prec) : kfunc<KStb>(c->prec);
+  void *fn = nullptr;
   auto grid_of = [&](const StbParams &p) {
-    return quads ? dim3((unsigned)((p.total + 7) / 8)) : dim3((unsigned)((p.total + 255) / 256));
+    dim3 gr;
+    stb_launch_shape(c, level, STB_ALL, false, p, &fn, &gr);
+    return gr;
   };
+  { dim3 g0 = grid_of(ps[0]); (void)g0; }
   cudaEvent_t e0, e1;
   MB_CUDA(cudaEventCreate(&e0));
   MB_CUDA(cudaEventCreate(&e1));

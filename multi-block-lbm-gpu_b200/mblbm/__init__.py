@@ -139,6 +139,14 @@ SIGNATURES = {
     "mb_set_split_cells": ([_vp, C.c_longlong], C.c_int),
     "mb_set_stb_variant": ([_vp, C.c_int, C.c_int], C.c_int),
     "mb_set_bulk_occupancy": ([_vp, C.c_int], C.c_int),
+    "mb_set_stream_cells": ([_vp, C.c_longlong, C.c_int], C.c_int),
+    "mb_set_interface_shape": ([_vp, C.c_int, C.c_int], C.c_int),
+    "mb_set_program_timeout": ([_vp, C.c_double], C.c_int),
+    "mb_set_program_shape": ([_vp, C.c_int, C.c_int, C.c_int, C.c_int], C.c_int),
+    "mb_sync": ([_vp, _vp], C.c_int),
+    "mb_set_program_trace": ([_vp, C.c_longlong], C.c_int),
+    "mb_program_trace": ([_vp, _vp, C.c_longlong, C.POINTER(C.c_longlong)], C.c_int),
+    "mb_program_selftest": ([_vp, C.c_int, _vp], C.c_int),
     "mb_prepare": ([_vp, C.c_int], C.c_int),
     "mb_block_step": ([_vp, C.c_int, _vp], C.c_int),
     "mb_c_c_boundary_transfer": ([_vp, C.c_int, _vp], C.c_int),
@@ -289,14 +297,15 @@ class MultiBlockLBM:
 
     def __init__(self, geo, precision="f32", graph=True):
         """graph: False launches kernels one by one, True replays CUDA graphs,
-        "pdl" replays graphs with programmatic kernel-to-kernel edges."""
+        "pdl" replays graphs with programmatic kernel-to-kernel edges,
+        "program" runs each plan as one persistent executor launch."""
         self.lib = load()
         self.geo = geo
         self.precision = precision
         h = C.c_void_p()
         _check(self.lib.mb_create(C.byref(geo), PRECISIONS[precision], C.byref(h)), "mb_create")
         self.h = h
-        mode = 2 if graph == "pdl" else (1 if graph else 0)
+        mode = {"pdl": 2, "program": 3}.get(graph, 1 if graph else 0) if isinstance(graph, str) else (1 if graph else 0)
         if mode != 1:
             _check(self.lib.mb_set_graph_mode(self.h, mode), "mb_set_graph_mode")
         self.n = 0
@@ -329,9 +338,53 @@ class MultiBlockLBM:
         """Block-step kernel of a level: 0 one cell per thread, 1 four cells per thread."""
         _check(self.lib.mb_set_stb_variant(self.h, int(level), int(variant)), "mb_set_stb_variant")
 
+    def set_interface_shape(self, rec_points=32, spline_segments=1):
+        """Points per record CTA/item (32 or 64) and spline segments per CTA/item (1-4)."""
+        _check(self.lib.mb_set_interface_shape(self.h, int(rec_points), int(spline_segments)),
+               "mb_set_interface_shape")
+
+    def set_stream_cells(self, cells, bulk=False):
+        """Block steps over >= cells cells use evict-first cache hints (0: never);
+        bulk=True also runs such whole levels as low-priority bulk work."""
+        _check(self.lib.mb_set_stream_cells(self.h, int(cells), int(bool(bulk))), "mb_set_stream_cells")
+
     def set_bulk_occupancy(self, ctas_per_sm):
         """Cap interior block-step grids at ctas_per_sm CTAs per SM (0: uncapped)."""
         _check(self.lib.mb_set_bulk_occupancy(self.h, int(ctas_per_sm)), "mb_set_bulk_occupancy")
+
+    def set_program_timeout(self, seconds):
+        """Executor (graph="program"): give up after this long without ready work."""
+        _check(self.lib.mb_set_program_timeout(self.h, float(seconds)), "mb_set_program_timeout")
+
+    def set_program_shape(self, bulk_cells=512, urgent_cells=256, periods_per_launch=2, bulk_ctas=0):
+        """Executor: cells per work item of interior and of other block-step
+        nodes, scheduler periods per launch, and the cap on CTAs running bulk
+        items at once (0: none)."""
+        _check(self.lib.mb_set_program_shape(self.h, int(bulk_cells), int(urgent_cells), int(periods_per_launch),
+                                             int(bulk_ctas)), "mb_set_program_shape")
+
+    TRACE_DTYPE = np.dtype([("t_pick", "<u8"), ("t_start", "<u8"), ("t_end", "<u8"), ("plan_node", "<i4"),
+                            ("item", "<i4"), ("sm", "<i4"), ("cta", "<i4"), ("launch", "<i4"), ("pad", "<i4")])
+
+    def set_program_trace(self, capacity):
+        """Executor: record every work item into a device buffer of capacity entries (0: off)."""
+        _check(self.lib.mb_set_program_trace(self.h, int(capacity)), "mb_set_program_trace")
+
+    def program_trace(self, max_records=1 << 22):
+        """Recorded work items (numpy structured array) since the last call."""
+        out = np.zeros(max_records, dtype=self.TRACE_DTYPE)
+        n = C.c_longlong(0)
+        _check(self.lib.mb_program_trace(self.h, out.ctypes.data_as(_vp), int(max_records), C.byref(n)),
+               "mb_program_trace")
+        return out[: n.value]
+
+    def sync(self, stream=None):
+        """Waits for the stream; raises MBError(MB_ERR_TIMEOUT) after an executor timeout."""
+        _check(self.lib.mb_sync(self.h, _stream_ptr(stream)), "mb_sync")
+
+    def program_selftest(self, stall, stream=None):
+        """Raw status of one executor launch over an empty node (stall=1: never ready)."""
+        return self.lib.mb_program_selftest(self.h, int(stall), _stream_ptr(stream))
 
     def prepare(self, n_coarse):
         """Compiles the plans and graphs that evolution(n_coarse) will replay."""

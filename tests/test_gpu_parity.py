@@ -42,7 +42,7 @@ def make_pair(mb, orc, name, prec="f64", graph=True):
     return g, o, m
 
 
-@pytest.mark.parametrize("graph", [True, False])
+@pytest.mark.parametrize("graph", [True, False, "program"])
 @pytest.mark.parametrize("name", make_ref.GOLDEN)
 def test_f64_stepwise(mb, orc, cuda_device, name, graph):
     g, o, m = make_pair(mb, orc, name, "f64", graph)
@@ -285,14 +285,15 @@ def test_interior_rim_split(mb, orc, cuda_device, name):
         assert np.array_equal(a.fields(k)["F"], b.fields(k)["F"])
 
 
+@pytest.mark.parametrize("variant", [1, 2, 3])
 @pytest.mark.parametrize("prec", ["f32", "f16s", "f64"])
-def test_quad_kernel_equals_cell_kernel(mb, cuda_device, prec):
-    """The four-cells-per-thread block step gives bitwise the same state."""
+def test_quad_kernel_equals_cell_kernel(mb, cuda_device, prec, variant):
+    """The four- and two-cells-per-thread block steps give bitwise the same state."""
     g = mb.geo_init(*make_ref.case("n3")[:2])
     a = mb.MultiBlockLBM(g, prec)
     b = mb.MultiBlockLBM(g, prec)
     for lvl in range(g.layout.LEVEL):
-        b.set_stb_variant(lvl, 1)
+        b.set_stb_variant(lvl, variant)
     b.set_split_cells(0)
     for s in (a, b):
         s.init()
