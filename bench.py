@@ -165,8 +165,10 @@ def main():
     ap.add_argument("--precision", default="f32", choices=["f32", "f32u", "f16s", "f64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--roofline-only", type=int, default=0, metavar="N",
-                    help="init, 3 coarse steps, then N timed launches of the level-0 block step alone "
-                         "(the fixed launch order an ncu capture of that kernel needs); prints its roofline")
+                    help="init, then 3 untimed and N timed launches of one level's block step alone (the "
+                         "fixed launch order an ncu capture of that kernel needs: -k regex:k_block_step -s 3); "
+                         "prints its roofline")
+    ap.add_argument("--level", type=int, default=0, help="level of --roofline-only")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -197,11 +199,12 @@ def main():
     sim = mblbm.MultiBlockLBM(geo, args.precision)
     sim.init(stream)
     if args.roofline_only:
-        sim.evolution(3, stream)
-        kms, kbytes, kcells = sim.time_block_step(0, args.roofline_only, stream)
+        kms, kbytes, kcells = sim.time_block_step(args.level, args.roofline_only, stream)
         peak, src = peaks()
-        print(json.dumps({"kernel": "k_block_step level 0", "ms_per_launch": kms, "alg_bytes_per_launch": kbytes,
-                          "cells": kcells, "achieved_gbs": kbytes / kms / 1e6, "frac": kbytes / kms / 1e6 / peak}))
+        print(json.dumps({"kernel": f"k_block_step level {args.level}", "precision": args.precision,
+                          "ms_per_launch": kms, "alg_bytes_per_launch": kbytes, "cells": kcells,
+                          "achieved_gbs": kbytes / kms / 1e6, "frac": kbytes / kms / 1e6 / peak,
+                          "peak_source": src}))
         return 0
     sim.evolution(args.warmup, stream)
     torch.cuda.synchronize()

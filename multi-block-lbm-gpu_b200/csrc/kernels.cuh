@@ -114,54 +114,61 @@ struct StbParams {
   StbBlk b[STB_MAX_BLOCKS];
 };
 
+// BGK relaxation of a cell in FP32 arithmetic with the equilibria of
+// opposite directions paired: for e_k u = +-a,
+//   g_k = w_k (base + rh (3 e_k u + 4.5 (e_k u)^2 - 1.5 u^2))
+//       = w_k (E +- O),  E = base + rh (4.5 a^2 - 1.5 u^2),  O = 3 rh a,
+// with base = rho (plain storage) or rho - 1 (shifted storage, where g_k is
+// feq_k - w_k).  Same scheme as feq (lbm/assit_func.h:2-9), fewer operations.
+template <bool SHIFTED>
+__device__ __forceinline__ void collide_f32(const float *f, float rv, float *out, float *m) {
+  const float sum = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8];
+  const float rh = SHIFTED ? 1.0f + sum : sum;
+  const float base = sum;  // rho - 1 when shifted, rho otherwise
+  const float inv = __frcp_rn(rh);
+  const float ux = (f[1] - f[3] + f[5] - f[6] - f[7] + f[8]) * inv;
+  const float uy = (f[2] - f[4] + f[5] + f[6] - f[7] - f[8]) * inv;
+  m[0] = rh;
+  m[1] = ux;
+  m[2] = uy;
+  const float u15 = 1.5f * (ux * ux + uy * uy);
+  const float rh3 = 3.0f * rh;
+  const float w0 = 4.0f / 9.0f, w1 = 1.0f / 9.0f, w5 = 1.0f / 36.0f;
+  const float g0 = w0 * (base - rh * u15);
+  out[0] = f[0] + rv * (g0 - f[0]);
+  auto pair = [&](float a, float w, int kp, int km) {
+    const float e = w * (base + rh * (4.5f * a * a - u15));
+    const float o = w * (rh3 * a);
+    out[kp] = f[kp] + rv * ((e + o) - f[kp]);
+    out[km] = f[km] + rv * ((e - o) - f[km]);
+  };
+  pair(ux, w1, 1, 3);
+  pair(uy, w1, 2, 4);
+  pair(ux + uy, w5, 5, 7);
+  pair(ux - uy, w5, 8, 6);
+}
+
 // FLUID interior cell: Macros (lbm/assit_func.h:23-31) and BGK (stb3 :103-111,
 // zero forcing term) on pulled values f (f itself, or h = f - w when shifted).
-// Writes the new distributions to out and rho/u to m.
+// Writes the new distributions to out and rho/u to m.  FP64 evaluates the
+// reference's expressions as written; FP32 arithmetic uses collide_f32.
 template <int P>
 __device__ __forceinline__ void stb_collide(const typename Prec<P>::R *f, typename Prec<P>::R rv,
                                             typename Prec<P>::R *out, typename Prec<P>::R *m) {
   using R = typename Prec<P>::R;
-  if constexpr (!Prec<P>::shifted) {
+  if constexpr (sizeof(R) == 4) {
+    collide_f32<Prec<P>::shifted>(f, rv, out, m);
+  } else {
     R rh = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8];
     R ux = f[1] - f[3] + f[5] - f[6] - f[7] + f[8];
     R uy = f[2] - f[4] + f[5] + f[6] - f[7] - f[8];
-    if constexpr (sizeof(R) == 8) {  // FP64: the reference's divisions
-      ux = ux / rh;
-      uy = uy / rh;
-    } else {  // FP32 arithmetic: one correctly rounded reciprocal
-      const R inv = __frcp_rn(rh);
-      ux = ux * inv;
-      uy = uy * inv;
-    }
+    ux = ux / rh;
+    uy = uy / rh;
     m[0] = rh;
     m[1] = ux;
     m[2] = uy;
 #pragma unroll
     for (int k = 0; k < 9; k++) out[k] = f[k] - (f[k] - feq<R>(k, rh, ux, uy)) * rv;
-  } else {
-    // the same scheme in h = f - w: rho = 1 + sum h, j = sum e h, heq = feq - w
-    const R drh = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8];
-    const R rh = (R)1.0 + drh;
-    R ux = f[1] - f[3] + f[5] - f[6] - f[7] + f[8];
-    R uy = f[2] - f[4] + f[5] + f[6] - f[7] - f[8];
-    if constexpr (sizeof(R) == 8) {  // FP64: the reference's divisions
-      ux = ux / rh;
-      uy = uy / rh;
-    } else {  // FP32 arithmetic: one correctly rounded reciprocal
-      const R inv = __frcp_rn(rh);
-      ux = ux * inv;
-      uy = uy * inv;
-    }
-    m[0] = rh;
-    m[1] = ux;
-    m[2] = uy;
-    const R uv = ux * ux + uy * uy;
-#pragma unroll
-    for (int k = 0; k < 9; k++) {
-      const R eu = (R)ex(k) * ux + (R)ey(k) * uy;
-      const R heq = wk<P>(k) * (drh + rh * ((R)3.0 * eu + (R)4.5 * eu * eu - (R)1.5 * uv));
-      out[k] = f[k] - (f[k] - heq) * rv;
-    }
   }
 }
 

@@ -720,6 +720,9 @@ extern "C" int mb_create(const mb_geometry *geo, int precision, mb_ctx **out) {
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return MB_ERR_NODEVICE;
   auto c = std::make_unique<mb_ctx>();
   c->prec = precision;
+  // measured on config 2: FP16 storage gains from overlapping the split
+  // coarse interior with the fine levels, FP32 and FP64 storage do not
+  c->split_cells = precision == MB_PREC_F16S ? 1000000 : (1LL << 62);
   cudaGetDevice(&c->device);
   cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device);
   c->geo = *geo;
