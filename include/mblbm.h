@@ -245,6 +245,13 @@ int mb_drag(mb_ctx *ctx, double force[2], double *cd, double *cl, mb_stream stre
 int mb_drag_link_count(mb_ctx *ctx, int *n_links);
 /* error_L2 (lbm/error_L2.h:57-91) without the file; updates u_prev. */
 int mb_error_L2(mb_ctx *ctx, double *e, mb_stream stream);
+/* The reference's main loop (Multi-block-LBM.cu:144-158): n coarse steps,
+ * each followed by getDrag_block and error_L2 (the same values as calling
+ * mb_step(1), mb_drag and mb_error_L2 in turn), without a host round trip per
+ * step: every step's results are copied to host memory asynchronously and
+ * the call returns once the last one has arrived.  cd, cl and err receive n
+ * values each; any of them may be NULL. */
+int mb_step_diag(mb_ctx *ctx, int n, double *cd, double *cl, double *err, mb_stream stream);
 /* Scans every block for NaN / Inf; *bad = number of bad values. */
 int mb_check_finite(mb_ctx *ctx, long long *bad, mb_stream stream);
 

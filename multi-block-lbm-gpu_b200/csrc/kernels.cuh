@@ -1305,39 +1305,50 @@ struct L2Blk {
   long long cell0;
   int nx, pitch;
   double inv_m;
+  int ny, rt0;    // rows; first row tile (256 cells of one row) of this block
+  int rtiles_x;   // row tiles per row
+  int pad_;
 };
 struct L2Params {
   const L2Blk *blocks;
   const IfBlk *blk;
-  int nblk, pad_;
+  int nblk, ntiles;       // blocks; row tiles over all blocks
   long long total;
   double2 *partial;       // gridDim.x entries
   unsigned int *ticket;   // zero before the first launch; reset by the last CTA
   double *out;            // sum |u-up|^2 / m, sum |u|^2 / m
 };
 
+// A CTA walks row tiles (256 consecutive cells of one row of one block, the
+// block and row uniform over the CTA) with a fixed stride, so every cell is
+// summed by the same thread in the same order on every call.
 template <int P>
 __global__ void __launch_bounds__(256) k_error_l2(const __grid_constant__ L2Params p) {
   using R = typename Prec<P>::R;
+  __shared__ int s_rt0[MB_MAX_AREA];
+  for (int q = threadIdx.x; q < p.nblk; q += blockDim.x) s_rt0[q] = p.blocks[q].rt0;
+  __syncthreads();
   double s1 = 0, s2 = 0;
-  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < p.total;
-       g += (long long)gridDim.x * blockDim.x) {
-    int lo = 0, hi = p.nblk - 1;
+  for (int t = blockIdx.x; t < p.ntiles; t += gridDim.x) {
+    int lo = 0, hi = p.nblk - 1;  // last block whose first tile is <= t
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
-      if (p.blocks[mid].cell0 <= g) lo = mid; else hi = mid - 1;
+      if (s_rt0[mid] <= t) lo = mid; else hi = mid - 1;
     }
     const L2Blk &b = p.blocks[lo];
     const IfBlk &B = p.blk[lo];
-    const int local = int(g - b.cell0);
-    const int j = local / b.nx, i = local - j * b.nx;
-    const long long c = (long long)j * b.pitch + i;
-    const double ux = ((const R *)B.ux)[c], uy = ((const R *)B.uy)[c];
-    const double upx = ((const R *)B.upx)[c], upy = ((const R *)B.upy)[c];
-    s1 += ((ux - upx) * (ux - upx) + (uy - upy) * (uy - upy)) * b.inv_m;
-    s2 += (ux * ux + uy * uy) * b.inv_m;
-    ((R *)B.upx)[c] = (R)ux;
-    ((R *)B.upy)[c] = (R)uy;
+    const int lt = t - s_rt0[lo];
+    const int j = lt / b.rtiles_x;
+    const int i = (lt - j * b.rtiles_x) * 256 + (int)threadIdx.x;
+    if (i < b.nx) {
+      const int c = j * b.pitch + i;
+      const double ux = ((const R *)B.ux)[c], uy = ((const R *)B.uy)[c];
+      const double upx = ((const R *)B.upx)[c], upy = ((const R *)B.upy)[c];
+      s1 += ((ux - upx) * (ux - upx) + (uy - upy) * (uy - upy)) * b.inv_m;
+      s2 += (ux * ux + uy * uy) * b.inv_m;
+      ((R *)B.upx)[c] = (R)ux;
+      ((R *)B.upy)[c] = (R)uy;
+    }
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {

@@ -106,6 +106,11 @@ struct mb_ctx {
   double *d_l2_out = nullptr;
   double *h_l2_out = nullptr;  // pinned
   int l2_grid = 0;
+  int l2_tiles = 0;
+  // mb_step_diag: per-step Fx, Fy and the two L2 sums (device, pinned host)
+  double *d_diag = nullptr;
+  double *h_diag = nullptr;
+  size_t diag_cap = 0;
   long long total_cells = 0;
   // misc scratch
   unsigned long long *d_count = nullptr;
@@ -887,15 +892,26 @@ extern "C" int mb_create(const mb_geometry *geo, int precision, mb_ctx **out) {
   // L2 tables and scratch
   {
     std::vector<L2Blk> lb(c->nblk);
-    long long cell = 0;
+    long long cell = 0, tiles = 0;
     for (int a = 0; a < c->nblk; a++) {
-      lb[a] = {cell, c->bl[a].nx, c->bl[a].pitch, 1.0 / geo->Areas[a].m};
+      L2Blk &b = lb[a];
+      b = L2Blk{};
+      b.cell0 = cell;
+      b.nx = c->bl[a].nx;
+      b.pitch = c->bl[a].pitch;
+      b.inv_m = 1.0 / geo->Areas[a].m;
+      b.ny = c->bl[a].ny;
+      b.rtiles_x = (b.nx + 255) / 256;
+      b.rt0 = (int)tiles;
+      tiles += (long long)b.rtiles_x * b.ny;
       cell += (long long)c->bl[a].nx * c->bl[a].ny;
     }
+    if (tiles >= (1LL << 31)) return MB_ERR_UNSUPPORTED;
     c->total_cells = cell;
+    c->l2_tiles = (int)tiles;
     if ((e = dalloc(c.get(), &c->d_l2blk, c->nblk))) return e;
     MB_CUDA(cudaMemcpy(c->d_l2blk, lb.data(), lb.size() * sizeof(L2Blk), cudaMemcpyHostToDevice));
-    c->l2_grid = (int)std::min<long long>((cell + 255) / 256, 148LL * 8);
+    c->l2_grid = (int)std::min<long long>(tiles, 148LL * 8);
     if ((e = dalloc(c.get(), &c->d_l2_partial, c->l2_grid))) return e;
     if ((e = dalloc(c.get(), &c->d_l2_ticket, 1))) return e;
     MB_CUDA(cudaMemset(c->d_l2_ticket, 0, sizeof(unsigned int)));
@@ -961,6 +977,8 @@ extern "C" int mb_destroy(mb_ctx *c) {
   if (c->h_drag_out) cudaFreeHost(c->h_drag_out);
   if (c->h_l2_out) cudaFreeHost(c->h_l2_out);
   if (c->h_prg_err) cudaFreeHost(c->h_prg_err);
+  if (c->d_diag) cudaFree(c->d_diag);
+  if (c->h_diag) cudaFreeHost(c->h_diag);
   if (c->d_trace) cudaFree(c->d_trace);
   if (c->d_trace_n) cudaFree(c->d_trace_n);
   delete c;
@@ -1296,10 +1314,9 @@ extern "C" int mb_rotate_markers(mb_ctx *c, int line) {
 
 // getDrag_block (lbm/force_block.h:180-216): momentum exchange over the
 // stored links of the drag block, Cd = Fx/(rho0 |U0|^2 m R).
-extern "C" int mb_drag(mb_ctx *c, double force[2], double *cd, double *cl, mb_stream stream) {
-  if (!c || !force) return MB_ERR_INVALID;
-  if (!c->inited) return MB_ERR_STATE;
-  cudaStream_t s = (cudaStream_t)stream;
+namespace {
+// getDrag_block's kernel part: Fx, Fy into out[0..1] (device memory)
+int launch_drag(mb_ctx *c, double *out, cudaStream_t s) {
   const int a = c->drag_area;
   const IfBlk &B = c->blk[a];
   DragParams p{};
@@ -1308,17 +1325,46 @@ extern "C" int mb_drag(mb_ctx *c, double force[2], double *cd, double *cl, mb_st
   p.F = B.F[c->state.parity[a] ^ 1];
   p.plane = B.plane;
   for (int k = 0; k < 9; k++) p.feqc[k] = c->feqc[k];
-  p.out = c->d_drag_out;
+  p.out = out;
   void *args[] = {&p};
   MB_CUDA(cudaLaunchKernel(kfunc<KDrag>(c->prec), dim3(1), dim3(1024), args, 0, s));
+  return MB_OK;
+}
+
+// error_L2's kernel part: the two weighted sums into out[0..1] (device memory)
+int launch_l2(mb_ctx *c, double *out, cudaStream_t s) {
+  L2Params p{};
+  p.blocks = c->d_l2blk;
+  p.blk = c->d_blk;
+  p.nblk = c->nblk;
+  p.ntiles = c->l2_tiles;
+  p.total = c->total_cells;
+  p.partial = c->d_l2_partial;
+  p.ticket = c->d_l2_ticket;
+  p.out = out;
+  void *args[] = {&p};
+  MB_CUDA(cudaLaunchKernel(kfunc<KL2>(c->prec), dim3(c->l2_grid), dim3(256), args, 0, s));
+  return MB_OK;
+}
+
+double drag_norm(const mb_ctx *c) {
+  const mb_config &cfg = c->geo.config;
+  const double u0 = std::sqrt(cfg.U0[0] * cfg.U0[0] + cfg.U0[1] * cfg.U0[1]);
+  return cfg.rho0 * u0 * u0 * c->geo.Areas[c->drag_area].m * cfg.R;
+}
+}  // namespace
+
+extern "C" int mb_drag(mb_ctx *c, double force[2], double *cd, double *cl, mb_stream stream) {
+  if (!c || !force) return MB_ERR_INVALID;
+  if (!c->inited) return MB_ERR_STATE;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (int e = launch_drag(c, c->d_drag_out, s)) return e;
   MB_CUDA(cudaMemcpyAsync(c->h_drag_out, c->d_drag_out, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
   MB_CUDA(cudaStreamSynchronize(s));
   if (int st = program_status(c)) return st;
   force[0] = c->h_drag_out[0];
   force[1] = c->h_drag_out[1];
-  const mb_config &cfg = c->geo.config;
-  const double u0 = std::sqrt(cfg.U0[0] * cfg.U0[0] + cfg.U0[1] * cfg.U0[1]);
-  const double den = cfg.rho0 * u0 * u0 * c->geo.Areas[a].m * cfg.R;
+  const double den = drag_norm(c);
   if (cd) *cd = force[0] / den;
   if (cl) *cl = force[1] / den;
   return MB_OK;
@@ -1335,20 +1381,55 @@ extern "C" int mb_error_L2(mb_ctx *c, double *e, mb_stream stream) {
   if (!c || !e) return MB_ERR_INVALID;
   if (!c->inited) return MB_ERR_STATE;
   cudaStream_t s = (cudaStream_t)stream;
-  L2Params p{};
-  p.blocks = c->d_l2blk;
-  p.blk = c->d_blk;
-  p.nblk = c->nblk;
-  p.total = c->total_cells;
-  p.partial = c->d_l2_partial;
-  p.ticket = c->d_l2_ticket;
-  p.out = c->d_l2_out;
-  void *args[] = {&p};
-  MB_CUDA(cudaLaunchKernel(kfunc<KL2>(c->prec), dim3(c->l2_grid), dim3(256), args, 0, s));
+  if (int r = launch_l2(c, c->d_l2_out, s)) return r;
   MB_CUDA(cudaMemcpyAsync(c->h_l2_out, c->d_l2_out, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
   MB_CUDA(cudaStreamSynchronize(s));
   if (int st = program_status(c)) return st;
   *e = std::sqrt(c->h_l2_out[0]) / std::sqrt(c->h_l2_out[1]);
+  return MB_OK;
+}
+
+// The reference's main loop (Multi-block-LBM.cu:144-158): n coarse steps,
+// each followed by getDrag_block and error_L2, with the per-step results
+// copied to pinned host memory asynchronously; one synchronisation at the end.
+extern "C" int mb_step_diag(mb_ctx *c, int n, double *cd, double *cl, double *err, mb_stream stream) {
+  if (!c || n < 0) return MB_ERR_INVALID;
+  if (!c->inited) return MB_ERR_STATE;
+  if (n == 0) return MB_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  if ((size_t)n > c->diag_cap) {
+    MB_CUDA(cudaStreamSynchronize(s));
+    if (c->d_diag) cudaFree(c->d_diag);
+    if (c->h_diag) cudaFreeHost(c->h_diag);
+    c->d_diag = nullptr;
+    c->h_diag = nullptr;
+    c->diag_cap = 0;
+    const size_t cap = std::max<size_t>((size_t)n, 2 * c->diag_cap);
+    if (cudaMalloc(&c->d_diag, cap * 4 * sizeof(double)) != cudaSuccess) return MB_ERR_NOMEM;
+    if (cudaMallocHost(&c->h_diag, cap * 4 * sizeof(double)) != cudaSuccess) return MB_ERR_NOMEM;
+    c->diag_cap = cap;
+  }
+  c->kernels_last_call = 0;
+  for (int q = 0; q < n; q++) {
+    int e = 0;
+    CompiledPlan *cp = get_plan(c, 1, true, &e);
+    if (!cp) return e ? e : MB_ERR_INVALID;
+    if ((e = exec_plan(c, cp, s))) return e;
+    if ((e = launch_drag(c, c->d_diag + 4 * q, s))) return e;
+    if ((e = launch_l2(c, c->d_diag + 4 * q + 2, s))) return e;
+    MB_CUDA(cudaMemcpyAsync(c->h_diag + 4 * q, c->d_diag + 4 * q, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    c->kernels_last_call += 2;
+  }
+  MB_CUDA(cudaStreamSynchronize(s));
+  if (int st = program_status(c)) return st;
+  const double den = drag_norm(c);
+  for (int q = 0; q < n; q++) {
+    const double *v = c->h_diag + 4 * q;
+    if (cd) cd[q] = v[0] / den;
+    if (cl) cl[q] = v[1] / den;
+    if (err) err[q] = std::sqrt(v[2]) / std::sqrt(v[3]);
+  }
+  MB_CUDA(cudaGetLastError());
   return MB_OK;
 }
 

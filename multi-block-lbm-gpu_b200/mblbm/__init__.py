@@ -144,6 +144,7 @@ SIGNATURES = {
     "mb_set_program_timeout": ([_vp, C.c_double], C.c_int),
     "mb_set_program_shape": ([_vp, C.c_int, C.c_int, C.c_int, C.c_int], C.c_int),
     "mb_sync": ([_vp, _vp], C.c_int),
+    "mb_step_diag": ([_vp, C.c_int, _vp, _vp, _vp, _vp], C.c_int),
     "mb_set_program_trace": ([_vp, C.c_longlong], C.c_int),
     "mb_program_trace": ([_vp, _vp, C.c_longlong, C.POINTER(C.c_longlong)], C.c_int),
     "mb_program_selftest": ([_vp, C.c_int, _vp], C.c_int),
@@ -417,6 +418,16 @@ class MultiBlockLBM:
         cd, cl = C.c_double(), C.c_double()
         _check(self.lib.mb_drag(self.h, f, C.byref(cd), C.byref(cl), _stream_ptr(stream)), "mb_drag")
         return f[0], f[1], cd.value, cl.value
+
+    def evolution_diag(self, n_coarse, stream=None):
+        """n coarse steps, each followed by getDrag_block and error_L2 on the
+        device (mb_step_diag); returns numpy arrays (Cd, Cl, L2 change) of n values."""
+        n = int(n_coarse)
+        cd, cl, err = (np.zeros(n) for _ in range(3))
+        _check(self.lib.mb_step_diag(self.h, n, cd.ctypes.data_as(_vp), cl.ctypes.data_as(_vp),
+                                     err.ctypes.data_as(_vp), _stream_ptr(stream)), "mb_step_diag")
+        self.n += n
+        return cd, cl, err
 
     def drag_links(self):
         n = C.c_int()

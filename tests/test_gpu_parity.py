@@ -343,3 +343,27 @@ def test_checkpoint_restart_bitwise(mb, cuda_device, tmp_path):
     c = mb.MultiBlockLBM(g, "f64")
     with pytest.raises(mb.MBError):
         c.restore((tmp_path / "ck.bin").read_bytes())
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_step_diag_equals_step_by_step(mb, cuda_device, prec):
+    """mb_step_diag gives the values of mb_step(1), mb_drag and mb_error_L2
+    called in turn, bitwise, and the same final state."""
+    g = mb.geo_init(*make_ref.case("n3")[:2])
+    a = mb.MultiBlockLBM(g, prec)
+    b = mb.MultiBlockLBM(g, prec)
+    a.init()
+    b.init()
+    ref = []
+    for _ in range(9):
+        a.evolution(1)
+        _, _, cd, cl = a.getDrag_block()
+        ref.append((cd, cl, a.error_L2()))
+    cd, cl, err = b.evolution_diag(9)
+    assert np.array_equal(cd, [r[0] for r in ref])
+    assert np.array_equal(cl, [r[1] for r in ref])
+    assert np.array_equal(err, [r[2] for r in ref])
+    for k in range(g.layout.number_area):
+        fa, fb = a.fields(k), b.fields(k)
+        for key in ("F", "rho", "ux", "uy"):
+            assert np.array_equal(fa[key], fb[key])
