@@ -131,6 +131,7 @@ typedef struct {
 } mb_geometry;
 
 typedef struct mb_ctx mb_ctx;
+typedef struct mb_batch mb_batch;
 
 /* ---- library ------------------------------------------------------------ */
 int mb_version(void);
@@ -309,6 +310,35 @@ int mb_stats(mb_ctx *ctx, long long *kernels_last_step_call, long long *kernels_
  * on the given stream); returns mean ms per launch and bytes moved per launch. */
 int mb_time_block_step(mb_ctx *ctx, int level, int n, mb_stream stream, double *ms_per_launch,
                        double *alg_bytes_per_launch, long long *cells_per_launch);
+
+/* ---- batches of independent cases (no reference counterpart) ------------- */
+/* Groups n initialised cases of one precision, one number of levels and one
+ * scheduler state (e.g. all freshly initialised) for batched stepping: each
+ * node of their common plan runs as one launch over all cases, and the plan
+ * is replayed as a CUDA graph.  Cases whose plans differ in structure cannot
+ * share a batch (MB_ERR_UNSUPPORTED from the first mb_batch_step).  The
+ * cases stay owned by the caller and usable one by one; they are switched to
+ * graph mode 1 and block-step variant 0. */
+int mb_batch_create(mb_ctx *const *cases, int n, mb_batch **out);
+int mb_batch_destroy(mb_batch *batch);
+/* n coarse steps of every case (the last one leaves all rho/u up to date, as
+ * mb_step).  MB_ERR_STATE if a case was stepped on its own since. */
+int mb_batch_step(mb_batch *batch, int n_coarse, mb_stream stream);
+/* Compiles the plans and graphs mb_batch_step(n) will replay from the
+ * current state (the cases' plans on all host cores). */
+int mb_batch_prepare(mb_batch *batch, int n_coarse);
+/* Cd and Cl of every case (n values each; either may be NULL), one
+ * synchronisation for the whole batch. */
+int mb_batch_drag(mb_batch *batch, double *cd, double *cl, mb_stream stream);
+int mb_batch_stats(mb_batch *batch, long long *cell_updates_per_coarse_step, long long *kernels_last_call);
+/* mb_set_interface_shape on every case of the batch. */
+int mb_batch_set_interface_shape(mb_batch *batch, int rec_points, int spline_segments);
+/* Autotuner: times each candidate interface shape (points per record CTA,
+ * spline segments per CTA) over `steps` coarse steps and keeps the fastest;
+ * reports the choice and its time per coarse step.  The timing steps advance
+ * the cases. */
+int mb_batch_autotune(mb_batch *batch, int steps, mb_stream stream, int *rec_points, int *spline_segments,
+                      double *ms_per_step);
 
 #ifdef __cplusplus
 }

@@ -891,6 +891,64 @@ __global__ void __launch_bounds__(32 * SPL_WARPS) k_spline(const __grid_constant
 }
 
 // ----------------------------------------------------------------------------
+// Batched launches: one launch runs the same plan node of many cases (the
+// cases of a batch share the plan's structure, not their sizes).  Each case
+// has its own parameter block in device memory and a contiguous range of
+// CTAs (cta0[c] .. cta0[c+1]-1); a CTA finds its case, copies the case's
+// parameter block into shared memory and runs the single-case code on its
+// CTA index within that case.
+// ----------------------------------------------------------------------------
+struct BatchArgs {
+  const unsigned char *params;  // ncases parameter blocks, pstride bytes apart (16-byte multiples)
+  const int *cta0;              // first CTA of each case
+  int ncases, pstride;
+};
+
+// the case of this CTA (uniform), and its parameter block copied to smem
+__device__ __forceinline__ int batch_case(const BatchArgs &a, unsigned char *smem, int nbytes) {
+  int lo = 0, hi = a.ncases - 1;
+  const int b = (int)blockIdx.x;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(a.cta0 + mid) <= b) lo = mid; else hi = mid - 1;
+  }
+  const int4 *src = (const int4 *)(a.params + (size_t)lo * a.pstride);
+  for (int q = threadIdx.x; q < nbytes / 16; q += blockDim.x) ((int4 *)smem)[q] = __ldg(src + q);
+  __syncthreads();
+  return lo;
+}
+
+template <int P>
+__global__ void __launch_bounds__(256, P == MB_PREC_F64 ? 4 : 8) kb_block_step(const __grid_constant__ BatchArgs a) {
+  __shared__ __align__(16) unsigned char sp[(sizeof(StbParams) + 15) / 16 * 16];
+  const int c = batch_case(a, sp, (int)sizeof(sp));
+  const StbParams &p = *(const StbParams *)sp;
+  const long long g = (long long)((int)blockIdx.x - __ldg(a.cta0 + c)) * 256 + threadIdx.x;
+  if (g < p.total) stb_at<P>(p, g);
+}
+
+template <int P>
+__global__ void __launch_bounds__(REC_THREADS) kb_records(const __grid_constant__ BatchArgs a) {
+  __shared__ __align__(16) unsigned char sp[(sizeof(RecOpsParams) + 15) / 16 * 16];
+  const int c = batch_case(a, sp, (int)sizeof(sp));
+  const RecOpsParams &p = *(const RecOpsParams *)sp;
+  const int t = ((int)blockIdx.x - __ldg(a.cta0 + c)) * (int)blockDim.x + (int)threadIdx.x;
+  if (t < p.total) rec_point<P>(p, t);
+}
+
+template <int P>
+__global__ void __launch_bounds__(32 * SPL_WARPS) kb_spline(const __grid_constant__ BatchArgs a) {
+  using R = typename Prec<P>::R;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int PB = (sizeof(SplParamsP) + 15) / 16 * 16;
+  const int c = batch_case(a, smem_raw, PB);
+  const SplParamsP &p = *(const SplParamsP *)smem_raw;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int sid = ((int)blockIdx.x - __ldg(a.cta0 + c)) * (int)(blockDim.x >> 5) + warp;
+  if (sid < p.nseg) spl_segment<P, true>(p, sid, lane, smem_raw + PB + warp * spl_warp_smem<R>());
+}
+
+// ----------------------------------------------------------------------------
 // Persistent plan executor.  One launch runs every node of a compiled plan
 // (block steps, record ops, spline lines of one or more coarse steps) with the
 // plan's dependencies tracked on the device.  Each node is cut into work

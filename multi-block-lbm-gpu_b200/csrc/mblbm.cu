@@ -7,7 +7,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <thread>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -202,6 +204,9 @@ template <int P> struct KSpl { static void *ptr() { return (void *)k_spline<P>; 
 template <int P> struct KDrag { static void *ptr() { return (void *)k_drag<P>; } };
 template <int P> struct KL2 { static void *ptr() { return (void *)k_error_l2<P>; } };
 template <int P> struct KPrg { static void *ptr() { return (void *)k_program<P, false>; } };
+template <int P> struct KBStb { static void *ptr() { return (void *)kb_block_step<P>; } };
+template <int P> struct KBRec { static void *ptr() { return (void *)kb_records<P>; } };
+template <int P> struct KBSpl { static void *ptr() { return (void *)kb_spline<P>; } };
 template <int P> struct KPrgT { static void *ptr() { return (void *)k_program<P, true>; } };
 size_t program_smem(int prec) { return prec == MB_PREC_F64 ? prg_smem<double>() : prg_smem<float>(); }
 
@@ -506,6 +511,8 @@ int set_smem_limits(int prec) {
                                (int)program_smem(prec)));
   MB_CUDA(cudaFuncSetAttribute(kfunc<KPrgT>(prec), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)program_smem(prec)));
+  MB_CUDA(cudaFuncSetAttribute(kfunc<KBSpl>(prec), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)((sizeof(SplParamsP) + 15) / 16 * 16 + spline_smem(prec))));
   return MB_OK;
 }
 
@@ -1726,5 +1733,319 @@ extern "C" int mb_time_block_step(mb_ctx *c, int level, int n, mb_stream stream,
   if (ms) *ms = t / n;
   if (bytes) *bytes = (double)tot * 18.0 * (double)prec_bytes(c->prec);
   if (cells) *cells = tot;
+  return MB_OK;
+}
+
+// =============================================================================
+// Batches: many independent cases advanced together.  Cases whose compiled
+// plans have the same structure (node kinds, dependencies and launch shapes;
+// e.g. nested-frame layouts with the same number of levels, whatever their
+// sizes) share one DAG: each plan node becomes one launch over all cases
+// (kb_block_step, kb_records, kb_spline), and the DAG is replayed as a CUDA
+// graph.  Cases keep their own state and remain usable one by one between
+// batch calls.
+// =============================================================================
+namespace {
+struct BatchPlan {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  std::vector<SchedState> end;  // per case
+  std::vector<void *> dev;
+  long long kernels = 0;
+  ~BatchPlan() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    for (void *p : dev) cudaFree(p);
+  }
+};
+}  // namespace
+
+struct mb_batch {
+  std::vector<mb_ctx *> cases;
+  int prec = 0;
+  int period = 1;
+  std::map<std::string, std::unique_ptr<BatchPlan>> plans;
+  long long updates_per_step = 0;
+  long long kernels_last_call = 0;
+  double *d_drag = nullptr;  // 2 per case
+  double *h_drag = nullptr;  // pinned
+};
+
+namespace {
+int batch_plan(mb_batch *b, int n, bool fin, BatchPlan **out) {
+  const std::string key = b->cases[0]->state.key() + "/" + std::to_string(n) + (fin ? "F" : "P");
+  auto it = b->plans.find(key);
+  if (it != b->plans.end()) {
+    *out = it->second.get();
+    return MB_OK;
+  }
+  const int nc = (int)b->cases.size();
+  std::vector<CompiledPlan *> parts(nc, nullptr);
+  std::vector<int> errs(nc, 0);
+  {  // every case compiles its own plan: spread the cases over host threads
+    const int nt = std::max(1, std::min<int>(nc, (int)std::thread::hardware_concurrency()));
+    std::atomic<int> next{0};
+    auto work = [&]() {
+      cudaSetDevice(b->cases[0]->device);
+      for (int c = next++; c < nc; c = next++) parts[c] = get_plan(b->cases[c], n, fin, &errs[c]);
+    };
+    std::vector<std::thread> th;
+    for (int t = 1; t < nt; t++) th.emplace_back(work);
+    work();
+    for (auto &t : th) t.join();
+  }
+  for (int c = 0; c < nc; c++)
+    if (!parts[c]) return errs[c] ? errs[c] : MB_ERR_INVALID;
+  const auto &d0 = parts[0]->dn;
+  for (int c = 1; c < nc; c++) {  // one DAG for all cases
+    const auto &dc = parts[c]->dn;
+    if (dc.size() != d0.size()) return MB_ERR_UNSUPPORTED;
+    for (size_t q = 0; q < d0.size(); q++)
+      if (dc[q].kind != d0[q].kind || dc[q].deps != d0[q].deps || dc[q].block.x != d0[q].block.x ||
+          dc[q].background != d0[q].background)
+        return MB_ERR_UNSUPPORTED;
+  }
+  auto bp = std::make_unique<BatchPlan>();
+  MB_CUDA(cudaGraphCreate(&bp->graph, 0));
+  std::vector<cudaGraphNode_t> gn(d0.size(), nullptr);
+  for (size_t q = 0; q < d0.size(); q++) {
+    const DevPlanNode &n0 = d0[q];
+    size_t psz;
+    void *func;
+    unsigned block = n0.block.x;
+    size_t smem = 0;
+    if (n0.kind == NK_STB) {
+      psz = sizeof(StbParams);
+      func = kfunc<KBStb>(b->prec);
+      block = 256;
+    } else if (n0.kind == NK_REC) {
+      psz = sizeof(RecOpsParams);
+      func = kfunc<KBRec>(b->prec);
+    } else {
+      psz = sizeof(SplParamsP);
+      func = kfunc<KBSpl>(b->prec);
+      smem = (sizeof(SplParamsP) + 15) / 16 * 16 + spline_smem(b->prec) / SPL_WARPS * (n0.block.x / 32);
+    }
+    const size_t stride = (psz + 15) / 16 * 16;
+    std::vector<unsigned char> host(stride * nc + sizeof(int) * (nc + 1), 0);
+    int *cta0 = (int *)(host.data() + stride * nc);
+    long long ctas = 0;
+    for (int c = 0; c < nc; c++) {
+      const DevPlanNode &dn = parts[c]->dn[q];
+      const void *src = n0.kind == NK_STB ? (const void *)&dn.stb : n0.kind == NK_REC ? (const void *)&dn.rec
+                                                                                      : (const void *)&dn.spl;
+      std::memcpy(host.data() + stride * c, src, psz);
+      cta0[c] = (int)ctas;
+      if (n0.kind == NK_STB) ctas += (dn.stb.total + 255) / 256;
+      else ctas += dn.grid.x;
+      if (ctas >= (1LL << 31)) return MB_ERR_UNSUPPORTED;
+    }
+    cta0[nc] = (int)ctas;
+    std::vector<cudaGraphNode_t> deps;
+    for (int p : n0.deps)
+      if (gn[p]) deps.push_back(gn[p]);
+    if (ctas == 0) {
+      MB_CUDA(cudaGraphAddEmptyNode(&gn[q], bp->graph, deps.data(), deps.size()));
+      continue;
+    }
+    void *dp = nullptr;
+    if (cudaMalloc(&dp, host.size()) != cudaSuccess) return MB_ERR_NOMEM;
+    bp->dev.push_back(dp);
+    MB_CUDA(cudaMemcpy(dp, host.data(), host.size(), cudaMemcpyHostToDevice));
+    BatchArgs a{};
+    a.params = (const unsigned char *)dp;
+    a.cta0 = (const int *)((unsigned char *)dp + stride * nc);
+    a.ncases = nc;
+    a.pstride = (int)stride;
+    void *args[1] = {&a};
+    cudaKernelNodeParams kp{};
+    kp.func = func;
+    kp.gridDim = dim3((unsigned)ctas);
+    kp.blockDim = dim3(block);
+    kp.sharedMemBytes = (unsigned)smem;
+    kp.kernelParams = args;
+    MB_CUDA(cudaGraphAddKernelNode(&gn[q], bp->graph, deps.data(), deps.size(), &kp));
+    if (int e = set_priority(gn[q], n0.background)) return e;
+    bp->kernels++;
+  }
+  MB_CUDA(cudaGraphInstantiateWithFlags(&bp->exec, bp->graph, cudaGraphInstantiateFlagUseNodePriority));
+  bp->end.resize(nc);
+  for (int c = 0; c < nc; c++) bp->end[c] = parts[c]->end;
+  *out = bp.get();
+  b->plans[key] = std::move(bp);
+  return MB_OK;
+}
+
+bool batch_in_step(const mb_batch *b) {
+  for (const mb_ctx *c : b->cases)
+    if (!(c->state == b->cases[0]->state)) return false;
+  return true;
+}
+}  // namespace
+
+extern "C" int mb_batch_create(mb_ctx *const *cases, int n, mb_batch **out) {
+  if (!cases || n < 1 || !out) return MB_ERR_INVALID;
+  *out = nullptr;
+  auto b = std::make_unique<mb_batch>();
+  for (int q = 0; q < n; q++) {
+    mb_ctx *c = cases[q];
+    if (!c) return MB_ERR_INVALID;
+    if (!c->inited) return MB_ERR_STATE;
+    if (q > 0 && (c->prec != cases[0]->prec || c->period != cases[0]->period ||
+                  c->geo.layout.LEVEL != cases[0]->geo.layout.LEVEL || c->device != cases[0]->device))
+      return MB_ERR_UNSUPPORTED;
+    b->cases.push_back(c);
+    b->updates_per_step += c->updates_per_step;
+  }
+  if (!batch_in_step(b.get())) return MB_ERR_STATE;
+  b->prec = cases[0]->prec;
+  b->period = cases[0]->period;
+  cudaDeviceSynchronize();
+  for (mb_ctx *c : b->cases) {  // batched launches use one cell per thread and CUDA-graph plans
+    bool clear = c->use_graph != 1;
+    for (int l = 0; l < MB_MAX_LEVEL; l++) clear |= c->stb_variant[l] != 0;
+    if (clear) {
+      c->use_graph = 1;
+      for (int l = 0; l < MB_MAX_LEVEL; l++) c->stb_variant[l] = 0;
+      c->plans.clear();
+    }
+  }
+  if (cudaMalloc(&b->d_drag, 2 * sizeof(double) * n) != cudaSuccess) return MB_ERR_NOMEM;
+  if (cudaMallocHost(&b->h_drag, 2 * sizeof(double) * n) != cudaSuccess) {
+    cudaFree(b->d_drag);
+    return MB_ERR_NOMEM;
+  }
+  *out = b.release();
+  return MB_OK;
+}
+
+extern "C" int mb_batch_destroy(mb_batch *b) {
+  if (!b) return MB_ERR_INVALID;
+  cudaDeviceSynchronize();
+  b->plans.clear();
+  if (b->d_drag) cudaFree(b->d_drag);
+  if (b->h_drag) cudaFreeHost(b->h_drag);
+  delete b;
+  return MB_OK;
+}
+
+extern "C" int mb_batch_step(mb_batch *b, int n, mb_stream stream) {
+  if (!b || n < 0) return MB_ERR_INVALID;
+  if (!batch_in_step(b)) return MB_ERR_STATE;
+  cudaStream_t s = (cudaStream_t)stream;
+  b->kernels_last_call = 0;
+  int remaining = n;
+  const int G = b->period;
+  while (remaining > 0) {
+    int chunk;
+    bool fin;
+    if (remaining - 1 >= G) { chunk = G; fin = false; }
+    else if (remaining > 1) { chunk = 1; fin = false; }
+    else { chunk = 1; fin = true; }
+    BatchPlan *bp = nullptr;
+    if (int e = batch_plan(b, chunk, fin, &bp)) return e;
+    MB_CUDA(cudaGraphLaunch(bp->exec, s));
+    for (size_t c = 0; c < b->cases.size(); c++) b->cases[c]->state = bp->end[c];
+    b->kernels_last_call += bp->kernels;
+    remaining -= chunk;
+  }
+  MB_CUDA(cudaGetLastError());
+  return MB_OK;
+}
+
+// Builds the graphs mb_batch_step(n) will replay from the current state.
+extern "C" int mb_batch_prepare(mb_batch *b, int n) {
+  if (!b || n < 0) return MB_ERR_INVALID;
+  if (!batch_in_step(b)) return MB_ERR_STATE;
+  const int nc = (int)b->cases.size();
+  std::vector<SchedState> save(nc);
+  for (int c = 0; c < nc; c++) save[c] = b->cases[c]->state;
+  int remaining = n, err = MB_OK;
+  const int G = b->period;
+  while (remaining > 0 && !err) {
+    int chunk;
+    bool fin;
+    if (remaining - 1 >= G) { chunk = G; fin = false; }
+    else if (remaining > 1) { chunk = 1; fin = false; }
+    else { chunk = 1; fin = true; }
+    BatchPlan *bp = nullptr;
+    err = batch_plan(b, chunk, fin, &bp);
+    if (!err)
+      for (int c = 0; c < nc; c++) b->cases[c]->state = bp->end[c];
+    remaining -= chunk;
+  }
+  for (int c = 0; c < nc; c++) b->cases[c]->state = save[c];
+  return err;
+}
+
+extern "C" int mb_batch_drag(mb_batch *b, double *cd, double *cl, mb_stream stream) {
+  if (!b) return MB_ERR_INVALID;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int nc = (int)b->cases.size();
+  for (int c = 0; c < nc; c++)
+    if (int e = launch_drag(b->cases[c], b->d_drag + 2 * c, s)) return e;
+  MB_CUDA(cudaMemcpyAsync(b->h_drag, b->d_drag, 2 * sizeof(double) * nc, cudaMemcpyDeviceToHost, s));
+  MB_CUDA(cudaStreamSynchronize(s));
+  for (int c = 0; c < nc; c++) {
+    const double den = drag_norm(b->cases[c]);
+    if (cd) cd[c] = b->h_drag[2 * c] / den;
+    if (cl) cl[c] = b->h_drag[2 * c + 1] / den;
+  }
+  return MB_OK;
+}
+
+extern "C" int mb_batch_stats(mb_batch *b, long long *updates_per_step, long long *kernels_last_call) {
+  if (!b) return MB_ERR_INVALID;
+  if (updates_per_step) *updates_per_step = b->updates_per_step;
+  if (kernels_last_call) *kernels_last_call = b->kernels_last_call;
+  return MB_OK;
+}
+
+// Interface work granularity of every case (mb_set_interface_shape), as
+// the batch autotuner varies it.
+extern "C" int mb_batch_set_interface_shape(mb_batch *b, int rec_points, int spline_segments) {
+  if (!b) return MB_ERR_INVALID;
+  cudaDeviceSynchronize();
+  b->plans.clear();
+  for (mb_ctx *c : b->cases)
+    if (int e = mb_set_interface_shape(c, rec_points, spline_segments)) return e;
+  return MB_OK;
+}
+
+// Times each candidate interface shape over `steps` coarse steps (after one
+// untimed chunk that builds its graphs) and keeps the fastest.  The timing
+// steps advance the cases.
+extern "C" int mb_batch_autotune(mb_batch *b, int steps, mb_stream stream, int *rec_points, int *spline_segments,
+                                 double *ms_per_step) {
+  if (!b || steps < 1) return MB_ERR_INVALID;
+  cudaStream_t s = (cudaStream_t)stream;
+  static const int cand[][2] = {{32, 1}, {64, 1}, {32, 2}, {64, 2}, {64, 4}};
+  double best = 1e30;
+  int br = 32, bs = 1;
+  cudaEvent_t e0, e1;
+  MB_CUDA(cudaEventCreate(&e0));
+  MB_CUDA(cudaEventCreate(&e1));
+  for (const auto &cd : cand) {
+    if (int e = mb_batch_set_interface_shape(b, cd[0], cd[1])) return e;
+    if (int e = mb_batch_step(b, b->period + 1, s)) return e;
+    if (int e = mb_batch_prepare(b, steps)) return e;
+    MB_CUDA(cudaEventRecord(e0, s));
+    if (int e = mb_batch_step(b, steps, s)) return e;
+    MB_CUDA(cudaEventRecord(e1, s));
+    MB_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    MB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    if (ms / steps < best) {
+      best = ms / steps;
+      br = cd[0];
+      bs = cd[1];
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (int e = mb_batch_set_interface_shape(b, br, bs)) return e;
+  if (rec_points) *rec_points = br;
+  if (spline_segments) *spline_segments = bs;
+  if (ms_per_step) *ms_per_step = best;
   return MB_OK;
 }

@@ -145,6 +145,14 @@ SIGNATURES = {
     "mb_set_program_shape": ([_vp, C.c_int, C.c_int, C.c_int, C.c_int], C.c_int),
     "mb_sync": ([_vp, _vp], C.c_int),
     "mb_step_diag": ([_vp, C.c_int, _vp, _vp, _vp, _vp], C.c_int),
+    "mb_batch_create": ([C.POINTER(_vp), C.c_int, C.POINTER(_vp)], C.c_int),
+    "mb_batch_destroy": ([_vp], C.c_int),
+    "mb_batch_step": ([_vp, C.c_int, _vp], C.c_int),
+    "mb_batch_drag": ([_vp, _vp, _vp, _vp], C.c_int),
+    "mb_batch_prepare": ([_vp, C.c_int], C.c_int),
+    "mb_batch_stats": ([_vp, _pll, _pll], C.c_int),
+    "mb_batch_set_interface_shape": ([_vp, C.c_int, C.c_int], C.c_int),
+    "mb_batch_autotune": ([_vp, C.c_int, _vp, _pi, _pi, _pd], C.c_int),
     "mb_set_program_trace": ([_vp, C.c_longlong], C.c_int),
     "mb_program_trace": ([_vp, _vp, C.c_longlong, C.POINTER(C.c_longlong)], C.c_int),
     "mb_program_selftest": ([_vp, C.c_int, _vp], C.c_int),
@@ -261,6 +269,46 @@ def config2_geometry():
     D=32 at (960,512), U0=0.04."""
     L = layout_nested(4096, 1024, [(768, 1280, 384, 640), (896, 1152, 448, 576)])
     return geo_init(L, make_config(4096, 1024, 16, 960, 512, U0=(0.04, 0.0), Re=100.0))
+
+
+def _splitmix64(x):
+    x = (x + 0x9E3779B97F4A7C15) & 0xFFFFFFFFFFFFFFFF
+    z = x
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & 0xFFFFFFFFFFFFFFFF
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & 0xFFFFFFFFFFFFFFFF
+    return x, z ^ (z >> 31)
+
+
+def batch_case(case_id, base_seed=20250, d_range=(10.0, 40.0), levels=None):
+    """One case of the batched workload, drawn with splitmix64 from seed
+    base_seed + case_id: obstacle extent D ~ U[d_range] coarse cells (the
+    ellipse's major axis), aspect ~ U[1,3], angle ~ U[0,pi), Re ~ U[20,200],
+    2 or 3 levels (unless given), domain 20D x 8D, U0 = 0.04.  The obstacle
+    sits at (5D, 4D); level-1 box [CX-2D, CX+6D] x [CY-2D, CY+2D], level-2 box
+    [CX-D, CX+3D] x [CY-D, CY+D].  Returns (geometry, parameters)."""
+    state = (base_seed + case_id) & 0xFFFFFFFFFFFFFFFF
+    u = []
+    for _ in range(5):
+        state, r = _splitmix64(state)
+        u.append((r >> 11) / float(1 << 53))
+    D = d_range[0] + (d_range[1] - d_range[0]) * u[0]
+    aspect = 1.0 + 2.0 * u[1]
+    angle = np.pi * u[2]
+    Re = 20.0 + 180.0 * u[3]
+    nlev = levels if levels is not None else (2 if u[4] < 0.5 else 3)
+    Di = int(round(D))
+    LX, LY = 20 * Di, 8 * Di
+    CX, CY = 5 * Di, 4 * Di
+    boxes = [(CX - 2 * Di, CX + 6 * Di, CY - 2 * Di, CY + 2 * Di)]
+    if nlev == 3:
+        boxes.append((CX - Di, CX + 3 * Di, CY - Di, CY + Di))
+    a = D / 2.0
+    b = a / aspect
+    R = max(1, int(round(D / 2.0)))
+    L = layout_nested(LX, LY, boxes)
+    cfg = make_config(LX, LY, R, CX, CY, U0=(0.04, 0.0), Re=Re, ellipse=(CX, CY, a, b, angle))
+    return geo_init(L, cfg), {"case": case_id, "D": D, "aspect": aspect, "angle": angle, "Re": Re, "levels": nlev,
+                              "LX": LX, "LY": LY}
 
 
 def updates_per_coarse_step(geo):
@@ -488,3 +536,62 @@ class MultiBlockLBM:
         _check(self.lib.mb_time_block_step(self.h, level, n, _stream_ptr(stream), C.byref(ms), C.byref(by), C.byref(cells)),
                "mb_time_block_step")
         return ms.value, by.value, cells.value
+
+
+# ---------------------------------------------------------------------------
+# batches of independent cases
+# ---------------------------------------------------------------------------
+class Batch:
+    """Independent cases of one precision and level count advanced together
+    (mb_batch_*): each plan node is one launch over all cases."""
+
+    def __init__(self, sims):
+        self.lib = load()
+        self.sims = list(sims)
+        arr = (_vp * len(self.sims))(*[s.h.value for s in self.sims])
+        h = _vp()
+        _check(self.lib.mb_batch_create(arr, len(self.sims), C.byref(h)), "mb_batch_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mb_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def evolution(self, n_coarse=1, stream=None):
+        _check(self.lib.mb_batch_step(self.h, int(n_coarse), _stream_ptr(stream)), "mb_batch_step")
+        for s in self.sims:
+            s.n += n_coarse
+
+    def prepare(self, n_coarse):
+        """Compiles the plans and graphs that evolution(n_coarse) will replay."""
+        _check(self.lib.mb_batch_prepare(self.h, int(n_coarse)), "mb_batch_prepare")
+
+    def drag(self, stream=None):
+        """(Cd, Cl) numpy arrays, one value per case."""
+        n = len(self.sims)
+        cd, cl = np.zeros(n), np.zeros(n)
+        _check(self.lib.mb_batch_drag(self.h, cd.ctypes.data_as(_vp), cl.ctypes.data_as(_vp), _stream_ptr(stream)),
+               "mb_batch_drag")
+        return cd, cl
+
+    def stats(self):
+        u, k = C.c_longlong(), C.c_longlong()
+        _check(self.lib.mb_batch_stats(self.h, C.byref(u), C.byref(k)), "mb_batch_stats")
+        return {"updates_per_step": u.value, "kernels_last_call": k.value}
+
+    def set_interface_shape(self, rec_points=32, spline_segments=1):
+        _check(self.lib.mb_batch_set_interface_shape(self.h, int(rec_points), int(spline_segments)),
+               "mb_batch_set_interface_shape")
+
+    def autotune(self, steps=12, stream=None):
+        r, sg, ms = C.c_int(), C.c_int(), C.c_double()
+        _check(self.lib.mb_batch_autotune(self.h, int(steps), _stream_ptr(stream), C.byref(r), C.byref(sg), C.byref(ms)),
+               "mb_batch_autotune")
+        return {"rec_points": r.value, "spline_segments": sg.value, "ms_per_step": ms.value}
