@@ -216,6 +216,48 @@ def run_batch(args):
     return 0
 
 
+def run_timetocd(args):
+    """Convergence of Cd on the 2-level case (400x160 coarse, Re=40, steady):
+    the FP64 value after --steps coarse steps is the converged reference; for
+    FP32 and FP16 storage, the first step after which Cd stays within 0.5 %
+    of it, and the device time to get there (diagnostics every step)."""
+    import torch
+    import mblbm
+
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    geo = mblbm.config1_geometry()
+    upd = mblbm.updates_per_coarse_step(geo)
+    out = {}
+    series = {}
+    for prec in ("f64", "f32", "f16s"):
+        sim = mblbm.MultiBlockLBM(geo, prec)
+        sim.init(stream)
+        sim.evolution_diag(12, stream)  # single-step plans of every scheduler phase
+        sim.init(stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        cd, cl, l2 = sim.evolution_diag(args.steps, stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        series[prec] = (cd, ms)
+        sim.close()
+    ref = float(series["f64"][0][-1])
+    for prec, (cd, ms) in series.items():
+        n = mblbm.settle_step(cd, ref)
+        out[prec] = {"cd_final": round(float(cd[-1]), 6), "rel_to_f64": float(cd[-1] / ref - 1.0),
+                     "steps_to_cd": n, "ms_to_cd": round(ms * n / args.steps, 2),
+                     "ms_per_step_with_diag": round(ms / args.steps, 5)}
+    line = {"metric": "time to Cd within 0.5% of the converged FP64 value", "unit": "ms", "higher_is_better": False,
+            "value": out["f32"]["ms_to_cd"], "n_gpus": 1, "steps": args.steps, "warmup": 12, "data": "synthetic",
+            "config": {"workload": "2-level cylinder Re=40, 400x160 coarse, fine box [60,140]x[40,120], D=20, U0=0.05",
+                       "cell_updates_per_step": upd, "reference": "Cd of FP64 storage after the run"},
+            "dtype": "f32", "by_precision": out}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -229,8 +271,9 @@ def main():
                          "fixed launch order an ncu capture of that kernel needs: -k regex:k_block_step -s 3); "
                          "prints its roofline")
     ap.add_argument("--level", type=int, default=0, help="level of --roofline-only")
-    ap.add_argument("--workload", default="cylinder3", choices=["cylinder3", "batch256"],
-                    help="cylinder3: the single 3-level case (default); batch256: the batched form")
+    ap.add_argument("--workload", default="cylinder3", choices=["cylinder3", "batch256", "timetocd"],
+                    help="cylinder3: the single 3-level case (default); batch256: the batched form; "
+                         "timetocd: Cd convergence of the 2-level case by precision")
     ap.add_argument("--cases", type=int, default=256, help="cases of --workload batch256")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -244,6 +287,8 @@ def main():
         return 0
     if args.workload == "batch256":
         return run_batch(args)
+    if args.workload == "timetocd":
+        return run_timetocd(args)
 
     import torch
 

@@ -595,3 +595,34 @@ class Batch:
         _check(self.lib.mb_batch_autotune(self.h, int(steps), _stream_ptr(stream), C.byref(r), C.byref(sg), C.byref(ms)),
                "mb_batch_autotune")
         return {"rec_points": r.value, "spline_segments": sg.value, "ms_per_step": ms.value}
+
+
+# ---------------------------------------------------------------------------
+# post-processing of the Cd / Cl series
+# ---------------------------------------------------------------------------
+def settle_step(series, target, rel=0.005):
+    """First index from which every later value lies within rel*|target| of
+    target (len(series) when the series never settles)."""
+    x = np.asarray(series, dtype=np.float64)
+    bad = np.nonzero(np.abs(x - target) > rel * abs(target))[0]
+    return 0 if len(bad) == 0 else int(bad[-1]) + 1
+
+
+def strouhal(cl, D, U0, skip=0):
+    """St = f D / U0 from the dominant frequency of the lift series (one value
+    per coarse step, D and U0 in coarse lattice units); None without a clear
+    oscillation.  The frequency comes from mean-crossings of the series after
+    `skip` steps, interpolated between steps."""
+    x = np.asarray(cl[skip:], dtype=np.float64)
+    if len(x) < 8:
+        return None
+    x = x - x.mean()
+    if np.abs(x).max() < 1e-9:
+        return None
+    s = np.signbit(x)
+    idx = np.nonzero(s[1:] != s[:-1])[0]
+    up = [i + x[i] / (x[i] - x[i + 1]) for i in idx if x[i] < 0 <= x[i + 1]]
+    if len(up) < 3:
+        return None
+    period = (up[-1] - up[0]) / (len(up) - 1)
+    return D / (period * U0)

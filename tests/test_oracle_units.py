@@ -65,3 +65,16 @@ def test_oracle_thread_count_does_not_change_results(mb, orc):
         res.append(np.concatenate([o.fields(a)["F"].ravel() for a in range(5)]))
     orc.set_threads(0)
     assert np.array_equal(res[0], res[1])
+
+
+def test_settle_step_and_strouhal():
+    import mblbm
+    x = [1.2, 1.1, 1.004, 0.997, 1.001, 1.0]
+    assert mblbm.settle_step(x, 1.0) == 2
+    assert mblbm.settle_step([1.0] * 4, 1.0) == 0
+    assert mblbm.settle_step([1.0, 1.0, 1.1], 1.0) == 3
+    t = np.arange(4000)
+    cl = 0.3 * np.sin(2 * np.pi * t / 250.0 + 0.3)
+    st = mblbm.strouhal(cl, D=20, U0=0.05)
+    assert abs(st - 20 / (250.0 * 0.05)) < 1e-3
+    assert mblbm.strouhal(np.zeros(100), 20, 0.05) is None
