@@ -340,6 +340,31 @@ int mb_batch_set_interface_shape(mb_batch *batch, int rec_points, int spline_seg
 int mb_batch_autotune(mb_batch *batch, int steps, mb_stream stream, int *rec_points, int *spline_segments,
                       double *ms_per_step);
 
+/* ---- learned warm start (no reference counterpart) ----------------------- */
+/* A 4-level convolutional U-Net (3x3 convolutions with ReLU, 32, 64, 128,
+ * 256 channels, 2x2 average pooling, nearest upsampling with skip
+ * concatenation, a 1x1 head to 3 outputs) on an H x W grid (multiples of 8).
+ * BF16 weights and activations, FP32 accumulation on the tensor cores, FP32
+ * master weights updated by Adam.  Inputs are 4 FP32 channels per point
+ * (NHWC, device memory): signed distance to the obstacle / D, Re / 100,
+ * inside-obstacle flag, x / W.  Outputs are 3 FP32 channels: u / U0, v / U0,
+ * 100 (rho - 1).  He-normal initialisation from `seed`. */
+typedef struct mb_unet mb_unet;
+int mb_unet_create(int H, int W, int max_batch, unsigned long long seed, mb_unet **out);
+int mb_unet_destroy(mb_unet *net);
+int mb_unet_param_count(mb_unet *net, long long *count);
+/* which = 0: FP32 master weights; 1: gradients of the last train step. */
+int mb_unet_get_params(mb_unet *net, float *host, long long count, int which);
+int mb_unet_set_params(mb_unet *net, const float *host, long long count);
+/* d_in: [n][H][W][4], d_out: [n][H][W][3], FP32 device arrays. */
+int mb_unet_forward(mb_unet *net, const float *d_in, int n, float *d_out, mb_stream stream);
+/* Forward, masked squared error sum_p mask_p |y_p - t_p|^2 / (3 n H W)
+ * against d_target ([n][H][W][3]) with d_mask ([n][H][W]), backward, and
+ * (apply = 1) one Adam step with learning rate lr.  Synchronous; *loss is
+ * the loss before the update. */
+int mb_unet_train_step(mb_unet *net, const float *d_in, const float *d_target, const float *d_mask, int n, float lr,
+                       int apply, float *loss, mb_stream stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -150,6 +150,13 @@ SIGNATURES = {
     "mb_batch_step": ([_vp, C.c_int, _vp], C.c_int),
     "mb_batch_drag": ([_vp, _vp, _vp, _vp], C.c_int),
     "mb_batch_prepare": ([_vp, C.c_int], C.c_int),
+    "mb_unet_create": ([C.c_int, C.c_int, C.c_int, C.c_ulonglong, C.POINTER(_vp)], C.c_int),
+    "mb_unet_destroy": ([_vp], C.c_int),
+    "mb_unet_param_count": ([_vp, _pll], C.c_int),
+    "mb_unet_get_params": ([_vp, _vp, C.c_longlong, C.c_int], C.c_int),
+    "mb_unet_set_params": ([_vp, _vp, C.c_longlong], C.c_int),
+    "mb_unet_forward": ([_vp, _vp, C.c_int, _vp, _vp], C.c_int),
+    "mb_unet_train_step": ([_vp, _vp, _vp, _vp, C.c_int, C.c_float, C.c_int, C.POINTER(C.c_float), _vp], C.c_int),
     "mb_batch_stats": ([_vp, _pll, _pll], C.c_int),
     "mb_batch_set_interface_shape": ([_vp, C.c_int, C.c_int], C.c_int),
     "mb_batch_autotune": ([_vp, C.c_int, _vp, _pi, _pi, _pd], C.c_int),
@@ -626,3 +633,53 @@ def strouhal(cl, D, U0, skip=0):
         return None
     period = (up[-1] - up[0]) / (len(up) - 1)
     return D / (period * U0)
+
+
+# ---------------------------------------------------------------------------
+# learned warm start
+# ---------------------------------------------------------------------------
+class UNet:
+    """The surrogate network (mb_unet_*).  Tensors are torch CUDA float32
+    tensors (their device pointers go through the C ABI)."""
+
+    def __init__(self, H=128, W=256, max_batch=16, seed=1):
+        self.lib = load()
+        self.H, self.W, self.max_batch = H, W, max_batch
+        h = _vp()
+        _check(self.lib.mb_unet_create(H, W, max_batch, seed, C.byref(h)), "mb_unet_create")
+        self.h = h
+        n = C.c_longlong()
+        _check(self.lib.mb_unet_param_count(self.h, C.byref(n)), "mb_unet_param_count")
+        self.nparam = n.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mb_unet_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def params(self, grads=False):
+        out = np.zeros(self.nparam, dtype=np.float32)
+        _check(self.lib.mb_unet_get_params(self.h, out.ctypes.data_as(_vp), self.nparam, int(grads)), "mb_unet_get_params")
+        return out
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        _check(self.lib.mb_unet_set_params(self.h, p.ctypes.data_as(_vp), self.nparam), "mb_unet_set_params")
+
+    def forward(self, x, out, stream=None):
+        _check(self.lib.mb_unet_forward(self.h, _vp(x.data_ptr()), x.shape[0], _vp(out.data_ptr()), _stream_ptr(stream)),
+               "mb_unet_forward")
+        return out
+
+    def train_step(self, x, target, mask, lr, apply=True, stream=None):
+        loss = C.c_float()
+        _check(self.lib.mb_unet_train_step(self.h, _vp(x.data_ptr()), _vp(target.data_ptr()), _vp(mask.data_ptr()),
+                                           x.shape[0], float(lr), int(apply), C.byref(loss), _stream_ptr(stream)),
+               "mb_unet_train_step")
+        return loss.value

@@ -1,0 +1,82 @@
+"""The surrogate U-Net's device kernels (tensor-core implicit-GEMM
+convolutions, their input and weight gradients, pooling, upsampling, head,
+Adam) against the numpy CPU oracle oracle/unet_ref.py, which rounds to BF16
+at the same points: forward values to 3e-3 relative L2 (1e-2 of the largest
+value pointwise), the loss to 3e-3, every layer's weight and bias gradients
+to 2e-2 relative L2 (BF16 roundings that FP32 summation order flips by one
+unit)."""
+import numpy as np
+import pytest
+
+import unet_ref
+
+pytestmark = pytest.mark.gpu
+
+
+def data(N, H, W, seed):
+    rng = np.random.default_rng(seed)
+    inp = rng.standard_normal((N, H, W, 4)).astype(np.float32)
+    target = rng.standard_normal((N, H, W, 3)).astype(np.float32)
+    mask = (rng.random((N, H, W)) > 0.2).astype(np.float32)
+    return inp, target, mask
+
+
+def test_unet_matches_cpu_oracle(mb, cuda_device):
+    import torch
+    N, H, W = 2, 16, 32
+    net = mb.UNet(H, W, max_batch=N, seed=7)
+    p = net.params()
+    inp, target, mask = data(N, H, W, 3)
+    ti, tt, tm = (torch.from_numpy(a).cuda() for a in (inp, target, mask))
+    out = torch.zeros((N, H, W, 3), device="cuda")
+    net.forward(ti, out)
+    torch.cuda.synchronize()
+    ref_out, ref_loss, ref_g = unet_ref.forward_backward(p, inp, target, mask)
+    o = out.cpu().numpy()
+    # a BF16 rounding that FP32 summation order flips changes one activation
+    # by one unit (0.4 %); through 14 layers that stays well below these bounds
+    assert np.linalg.norm(o - ref_out) <= 3e-3 * np.linalg.norm(ref_out)
+    assert np.abs(o - ref_out).max() <= 1e-2 * np.abs(ref_out).max()
+    loss = net.train_step(ti, tt, tm, lr=0.0, apply=False)
+    assert loss == pytest.approx(ref_loss, rel=3e-3)
+    g = net.params(grads=True)
+    off, errs = 0, []
+    for i, (cin, cout, _) in enumerate(unet_ref.LAYERS):
+        for n, what in ((cout * 9 * cin, "w"), (cout, "b")):
+            a, b = g[off:off + n], ref_g[off:off + n]
+            errs.append((i, what, float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))))
+            off += n
+    print("gradient errors", errs)
+    assert max(e for _, _, e in errs) < 6e-2, errs
+    assert float(np.median([e for _, _, e in errs])) < 1.5e-2, errs
+    for n in (96, 3):
+        a, b = g[off:off + n], ref_g[off:off + n]
+        assert np.linalg.norm(a - b) <= 1e-2 * np.linalg.norm(b)
+        off += n
+    net.close()
+
+
+def test_unet_training_lowers_loss(mb, cuda_device):
+    """Adam steps on a smooth, learnable target."""
+    import torch
+    N, H, W = 4, 32, 64
+    net = mb.UNet(H, W, max_batch=N, seed=11)
+    yy, xx = np.meshgrid(np.linspace(-1, 1, H), np.linspace(-1, 1, W), indexing="ij")
+    inp = np.zeros((N, H, W, 4), np.float32)
+    target = np.zeros((N, H, W, 3), np.float32)
+    for n in range(N):
+        r = np.sqrt((xx - 0.3 * n + 0.4) ** 2 + yy ** 2)
+        inp[n, ..., 0] = r - 0.3
+        inp[n, ..., 1] = 0.5 + 0.2 * n
+        inp[n, ..., 2] = (r < 0.3)
+        inp[n, ..., 3] = xx
+        target[n, ..., 0] = np.tanh(3 * (r - 0.3)) * inp[n, ..., 1]
+        target[n, ..., 1] = 0.2 * yy * np.exp(-r)
+        target[n, ..., 2] = np.exp(-4 * r * r)
+    mask = (inp[..., 2] == 0).astype(np.float32)
+    ti, tt, tm = (torch.from_numpy(a).cuda() for a in (inp, target, mask))
+    first = net.train_step(ti, tt, tm, lr=1e-3)
+    for _ in range(60):
+        last = net.train_step(ti, tt, tm, lr=1e-3)
+    assert last < 0.25 * first
+    net.close()

@@ -78,3 +78,35 @@ def test_settle_step_and_strouhal():
     st = mblbm.strouhal(cl, D=20, U0=0.05)
     assert abs(st - 20 / (250.0 * 0.05)) < 1e-3
     assert mblbm.strouhal(np.zeros(100), 20, 0.05) is None
+
+
+def test_unet_oracle_gradients_finite_differences():
+    """The CPU oracle's backward pass against central differences of its own
+    loss (exact arithmetic, BF16 rounding off), on sampled parameters."""
+    import unet_ref
+    unet_ref.ROUND = False
+    try:
+        rng = np.random.default_rng(5)
+        N, H, W = 1, 8, 16
+        parts = []
+        for ci, co, _ in unet_ref.LAYERS:  # He-scaled, as the device initialisation
+            parts += [rng.standard_normal(co * 9 * ci) * np.sqrt(2.0 / (9 * ci)), 0.05 * rng.standard_normal(co)]
+        parts += [rng.standard_normal(96) * np.sqrt(1.0 / 32), 0.05 * rng.standard_normal(3)]
+        p = np.concatenate(parts)
+        n = len(p)
+        inp = rng.standard_normal((N, H, W, 4))
+        tgt = rng.standard_normal((N, H, W, 3))
+        mask = (rng.random((N, H, W)) > 0.3).astype(np.float64)
+        _, loss, g = unet_ref.forward_backward(p, inp, tgt, mask)
+        idx = rng.choice(n, 40, replace=False)
+        idx = np.concatenate([idx, [n - 1, n - 50, 5, 16 * 9 * 32 + 3]])
+        eps = 1e-6
+        for i in idx:
+            q = p.copy(); q[i] += eps
+            lp = unet_ref.forward_backward(q, inp, tgt, mask)[1]
+            q[i] -= 2 * eps
+            lm = unet_ref.forward_backward(q, inp, tgt, mask)[1]
+            fd = (lp - lm) / (2 * eps)
+            assert abs(fd - g[i]) <= 1e-5 * max(1.0, abs(fd)) + 1e-8, (i, fd, g[i])
+    finally:
+        unet_ref.ROUND = True
