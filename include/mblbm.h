@@ -158,6 +158,11 @@ int mb_destroy(mb_ctx *ctx);
 /* init_General (lbm/init_block.h:2), init_Fstore / init_tri_A
  * (multi/init_multi.h:3,30), sum_N_drag + fdrag_store (lbm/force_block.h:50,78). */
 int mb_init(mb_ctx *ctx, mb_stream stream);
+/* After mb_set_fields has replaced the fields (a restart from outside data,
+ * the learned warm start): re-derives the state the reference derives from
+ * the initial fields, the ring slots of every coarse-fine line from the fine
+ * edge F (init_Fstore, multi/init_multi.h:3-28) and u_prev from u. */
+int mb_sync_history(mb_ctx *ctx, mb_stream stream);
 /* n coarse steps of evolution(level 0) (evolution.h:2-65).  The last coarse
  * step of every call leaves rho/ux/uy of all cells up to date, as the
  * reference's stb2 does each step; earlier steps keep only the macroscopic

@@ -1441,6 +1441,21 @@ __global__ void __launch_bounds__(256) k_error_l2(const __grid_constant__ L2Para
   }
 }
 
+// Ring slots of one coarse-fine line <- the fine edge F (init_Fstore,
+// multi/init_multi.h:3-28): every slot of fine point ip holds F at that point.
+template <int P>
+__global__ void k_slots_from_edge(const typename Prec<P>::S *F, long long plane, int fi0, int fj0, int fdi, int fdj,
+                                  int pitch, int Nf, typename Prec<P>::R *slots, int slot0) {
+  for (int ip = blockIdx.x * blockDim.x + threadIdx.x; ip < Nf; ip += gridDim.x * blockDim.x) {
+    const long long cell = (long long)(fj0 + ip * fdj) * pitch + (fi0 + ip * fdi);
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+      const typename Prec<P>::R v = ld_f<P>(F, k * plane + cell, k);
+      for (int q = 0; q < 3; q++) slots[((long long)(slot0 + ip) * 3 + q) * 9 + k] = v;
+    }
+  }
+}
+
 // ----------------------------------------------------------------------------
 // Utility kernels: fill, finite check, field conversion.
 // ----------------------------------------------------------------------------

@@ -1210,6 +1210,31 @@ extern "C" int mb_init(mb_ctx *c, mb_stream stream) {
   return MB_OK;
 }
 
+// After fields were set from outside (mb_set_fields), the state that the
+// reference derives from the initial fields in init_Fstore and error_L2:
+// ring slots of every coarse-fine line <- the fine edge F, u_prev <- u.
+extern "C" int mb_sync_history(mb_ctx *c, mb_stream stream) {
+  if (!c) return MB_ERR_INVALID;
+  if (!c->inited) return MB_ERR_STATE;
+  cudaStream_t s = (cudaStream_t)stream;
+  for (const SplLine &L : c->spl_lines) {
+    const IfBlk &B = c->blk[L.fine];
+    const void *F = B.F[c->state.parity[L.fine]];
+    MB_DISPATCH(c->prec, (k_slots_from_edge<P><<<(L.Nf + 127) / 128, 128, 0, s>>>(
+                             (const S *)F, B.plane, L.fi0, L.fj0, L.fdi, L.fdj, B.pitch, L.Nf,
+                             (typename Prec<P>::R *)c->d_slots, L.slot0)));
+  }
+  const size_t rb = real_bytes(c->prec);
+  for (int a = 0; a < c->nblk; a++) {
+    const IfBlk &B = c->blk[a];
+    MB_CUDA(cudaMemcpyAsync(B.upx, B.ux, (size_t)B.plane * rb, cudaMemcpyDeviceToDevice, s));
+    MB_CUDA(cudaMemcpyAsync(B.upy, B.uy, (size_t)B.plane * rb, cudaMemcpyDeviceToDevice, s));
+  }
+  MB_CUDA(cudaStreamSynchronize(s));
+  MB_CUDA(cudaGetLastError());
+  return MB_OK;
+}
+
 extern "C" int mb_step(mb_ctx *c, int n, mb_stream stream) {
   if (!c || n < 0) return MB_ERR_INVALID;
   if (!c->inited) return MB_ERR_STATE;

@@ -27,6 +27,7 @@ PREC_F64, PREC_F32, PREC_F16S, PREC_F32U = 0, 1, 2, 3
 PRECISIONS = {"f64": PREC_F64, "f32": PREC_F32, "f16s": PREC_F16S, "f32u": PREC_F32U}
 FLUID, SOLID_SBB, C_BOUNDARY = 0, 1, 9
 OBST_CIRCLE, OBST_ELLIPSE = 0, 1
+MB_FLUID, MB_SOLID_SBB, MB_C_BOUNDARY = 0, 1, 9  # cell kinds of mb_copy_fields' solid array
 
 
 class P4(C.Structure):
@@ -145,6 +146,7 @@ SIGNATURES = {
     "mb_set_program_shape": ([_vp, C.c_int, C.c_int, C.c_int, C.c_int], C.c_int),
     "mb_sync": ([_vp, _vp], C.c_int),
     "mb_step_diag": ([_vp, C.c_int, _vp, _vp, _vp, _vp], C.c_int),
+    "mb_sync_history": ([_vp, _vp], C.c_int),
     "mb_batch_create": ([C.POINTER(_vp), C.c_int, C.POINTER(_vp)], C.c_int),
     "mb_batch_destroy": ([_vp], C.c_int),
     "mb_batch_step": ([_vp, C.c_int, _vp], C.c_int),
@@ -514,9 +516,23 @@ class MultiBlockLBM:
         )
         return {"rho": rho, "ux": ux, "uy": uy, "F": F, "solid": solid}
 
+    def macros(self, area, stream=None):
+        """Dict of FP64 host arrays rho, ux, uy and solid (ny, nx), without the distributions."""
+        A = self.geo.Areas[area]
+        nx, ny = A.nx, A.ny
+        rho, ux, uy = np.empty((ny, nx)), np.empty((ny, nx)), np.empty((ny, nx))
+        solid = np.empty((ny, nx), dtype=np.int32)
+        _check(self.lib.mb_copy_fields(self.h, area, _dp(rho), _dp(ux), _dp(uy), None, solid.ctypes.data_as(_pi),
+                                       _stream_ptr(stream)), "mb_copy_fields")
+        return {"rho": rho, "ux": ux, "uy": uy, "solid": solid}
+
     def set_fields(self, area, rho=None, ux=None, uy=None, F=None, stream=None):
         arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (rho, ux, uy, F)]
         _check(self.lib.mb_set_fields(self.h, area, *[_dp(a) for a in arrs], _stream_ptr(stream)), "mb_set_fields")
+
+    def sync_history(self, stream=None):
+        """Ring slots <- fine edge F and u_prev <- u, after set_fields (mb_sync_history)."""
+        _check(self.lib.mb_sync_history(self.h, _stream_ptr(stream)), "mb_sync_history")
 
     def checkpoint(self, stream=None):
         """The full device state as bytes (see mb_checkpoint_save)."""
