@@ -135,18 +135,27 @@ def warm_start(sim, geo, pred, stream=None):
     sim.sync_history(stream)
 
 
-def generate(case_ids, steps, precision="f32", h=H, w=W, stream=None, d_range=(10.0, 40.0)):
-    """Snapshots of the batched solver: (inputs, targets, masks, kept ids)
-    after `steps` coarse steps from rest; cases whose fields are not finite
-    are dropped."""
+def _groups(case_ids, steps_per_d, d_range, bin_width=5.0):
+    """Cases grouped by level count and D bin; each group runs
+    steps_per_d * (upper edge of its D bin) coarse steps."""
     groups = {}
     for i in case_ids:
         g, prm = batch_case(i, d_range=d_range)
-        groups.setdefault(prm["levels"], []).append((i, g))
+        hi = d_range[0] + bin_width * (np.floor((prm["D"] - d_range[0]) / bin_width) + 1)
+        steps = int(steps_per_d * min(hi, d_range[1]))
+        groups.setdefault((prm["levels"], steps), []).append((i, g, prm))
+    return groups
+
+
+def generate(case_ids, steps_per_d, precision="f32", h=H, w=W, stream=None, d_range=(10.0, 40.0)):
+    """Snapshots of the batched solver: (inputs, targets, masks, kept ids)
+    after steps_per_d * D coarse steps from rest (D rounded up to its 5-cell
+    bin; the cases of a bin run as one batch); cases whose fields are not
+    finite are dropped."""
     xs, ts, ms, ids = [], [], [], []
-    for items in groups.values():
+    for (_, steps), items in _groups(case_ids, steps_per_d, d_range).items():
         sims = []
-        for i, g in items:
+        for i, g, _ in items:
             s = MultiBlockLBM(g, precision)
             s.init(stream)
             sims.append(s)
@@ -154,7 +163,7 @@ def generate(case_ids, steps, precision="f32", h=H, w=W, stream=None, d_range=(1
         b.prepare(steps)
         b.evolution(steps, stream)
         b.close()
-        for (i, g), s in zip(items, sims):
+        for (i, g, _), s in zip(items, sims):
             if s.check_finite(stream) == 0:
                 x, mk = case_inputs(g, h, w)
                 t = case_targets(s, g, h, w)
@@ -165,6 +174,47 @@ def generate(case_ids, steps, precision="f32", h=H, w=W, stream=None, d_range=(1
                     ids.append(i)
             s.close()
     return np.stack(xs), np.stack(ts), np.stack(ms), ids
+
+
+def drag_series(case_ids, steps_per_d, precision, chunk=50, net=None, d_range=(10.0, 40.0), stream=None):
+    """Cd every `chunk` coarse steps of each case, cold-started (net None) or
+    warm-started from the surrogate, batched by level count and D bin.
+    Returns {id: (series, params)} and the device time per coarse step of
+    each batch {(levels, steps): ms}."""
+    import torch
+
+    out, times = {}, {}
+    for key, items in _groups(case_ids, steps_per_d, d_range).items():
+        steps = key[1]
+        sims = []
+        for i, g, _ in items:
+            s = MultiBlockLBM(g, precision)
+            s.init(stream)
+            sims.append(s)
+        if net is not None:
+            xin = torch.from_numpy(np.stack([case_inputs(g, net.H, net.W)[0] for _, g, _ in items])).cuda()
+            pred = predict(net, xin).cpu().numpy()
+            for (i, g, _), s, p in zip(items, sims, pred):
+                warm_start(s, g, p, stream)
+        b = Batch(sims)
+        b.prepare(chunk)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ms, cds = 0.0, []
+        for _ in range(steps // chunk):
+            e0.record()
+            b.evolution(chunk, stream)
+            e1.record()
+            cd, _ = b.drag(stream)
+            ms += e0.elapsed_time(e1)
+            cds.append(cd)
+        b.close()
+        times[key] = ms / max(1, (steps // chunk) * chunk)
+        cds = np.array(cds)
+        for k, (i, g, prm) in enumerate(items):
+            out[i] = (cds[:, k], prm, key)
+        for s in sims:
+            s.close()
+    return out, times
 
 
 def train(net, x, t, m, epochs, batch=16, lr=1e-3, seed=0, log=None):

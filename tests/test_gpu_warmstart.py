@@ -17,7 +17,7 @@ def test_warm_start_pipeline(mb, cuda_device):
     from mblbm import surrogate as sg
 
     h, w = 64, 128
-    x, t, m, ids = sg.generate(range(16), STEPS, "f32", h, w, d_range=D_RANGE)
+    x, t, m, ids = sg.generate(range(16), STEPS / D_RANGE[1], "f32", h, w, d_range=D_RANGE)
     assert len(ids) >= 12 and np.isfinite(t).all()
     X, T, M = (torch.from_numpy(a).cuda() for a in (x, t, m))
     net = mb.UNet(h, w, max_batch=4, seed=3)
