@@ -351,6 +351,7 @@ def main():
                          "fixed launch order an ncu capture of that kernel needs: -k regex:k_block_step -s 3); "
                          "prints its roofline")
     ap.add_argument("--level", type=int, default=0, help="level of --roofline-only")
+    ap.add_argument("--variant", type=int, default=None, help="block-step variant of every level (mb_set_stb_variant)")
     ap.add_argument("--workload", default="cylinder3", choices=["cylinder3", "batch256", "timetocd", "warmstart"],
                     help="cylinder3: the single 3-level case (default); batch256: the batched form; "
                          "timetocd: Cd convergence of the 2-level case by precision")
@@ -394,6 +395,9 @@ def main():
     upd = mblbm.updates_per_coarse_step(geo)
     stream = torch.cuda.Stream()
     sim = mblbm.MultiBlockLBM(geo, args.precision)
+    if args.variant is not None:
+        for lvl in range(geo.layout.LEVEL):
+            sim.set_stb_variant(lvl, args.variant)
     sim.init(stream)
     if args.roofline_only:
         kms, kbytes, kcells = sim.time_block_step(args.level, args.roofline_only, stream)

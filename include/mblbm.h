@@ -214,6 +214,10 @@ int mb_set_split_cells(mb_ctx *ctx, long long cells);
  * rows touch one cache sector per value, so small units spread a node over
  * many SMs' load/store units.  Results are identical. */
 int mb_set_interface_shape(mb_ctx *ctx, int rec_points, int spline_segments);
+/* Splits exactly the levels whose bit is set in level_mask (bit l = level
+ * l) into interior and rim nodes, overriding mb_set_split_cells; 0 returns
+ * to the cell threshold.  Results are identical. */
+int mb_set_split_levels(mb_ctx *ctx, unsigned level_mask);
 /* Block-step nodes over at least `cells` cells (a whole level, or its
  * interior or rim) load and store with evict-first cache hints, so that the
  * streamed coarse level does not evict the fine levels' buffers from L2.
@@ -223,9 +227,9 @@ int mb_set_interface_shape(mb_ctx *ctx, int rec_points, int spline_segments);
 int mb_set_stream_cells(mb_ctx *ctx, long long cells, int bulk);
 /* Block-step kernel of one level: 0 = one cell per thread (default),
  * 1 = four cells per thread with vector loads, 2 = two cells per thread with
- * the loads of both in flight together, 3 = row tiles of 256 cells per CTA
- * with 32-bit offsets (whole levels and interiors; rims use 0).  Results are
- * identical. */
+ * the loads of both in flight together, 3 = cell ranges: a CTA steps 256
+ * consecutive cells of one block with 32-bit offsets (whole levels and
+ * interiors; rims use 0).  Results are identical. */
 int mb_set_stb_variant(mb_ctx *ctx, int level, int variant);
 /* Caps the grid of interior (bulk) block-step launches at ctas_per_sm CTAs of
  * 256 threads per SM (0 = uncapped), leaving CTA slots on every SM for the

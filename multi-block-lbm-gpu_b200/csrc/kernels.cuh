@@ -97,8 +97,12 @@ struct StbBlk {
   double rv_tau;
   long long wt0;    // first warp tile of this block in the launch (quad kernel)
   int tiles_x, row0;  // quad kernel: tiles of 128 cells per row; first row of the region (quad and row kernels)
-  int rt0, rtiles_x;  // row kernel: first row tile of this block in the launch, tiles of 256 cells per row
-  int col0, col1;     // row kernel: first and last column of the region
+  // range kernel: this block's cells of the region are CTAs cta0.. of the
+  // launch, 256 consecutive cells (row-major over the region) per CTA
+  int cta0, rcells;   // first CTA; cells of the region
+  int rw, rcol0;      // region width and first column (first row: row0)
+  float rinv_w;       // 1 / rw, for the row of a cell index
+  int pad2_;
 };
 
 struct StbParams {
@@ -108,7 +112,7 @@ struct StbParams {
   int region;        // 0: all cells, 1: distance >= 2 from the block edge, 2: distance <= 1
   int evict_first;   // stream the blocks' buffers with evict-first cache hints
   long long total;   // cells in the launch (per-cell kernel) or warp tiles (quad kernel)
-  long long rtiles;  // row tiles in the launch (row kernel)
+  long long rctas;   // CTAs of a range-kernel launch
   double feqc[9];    // feq(rho0, U0): block-edge FLUID cells and stale f of edge solids
   double rho0, u0x, u0y;
   StbBlk b[STB_MAX_BLOCKS];
@@ -409,20 +413,27 @@ __device__ __forceinline__ void stb_cell_rows(const StbParams &p, const StbBlk &
   stb_cell_slow<P, EF>(p, B, i, j);
 }
 
+// The block step on cell ranges: a CTA owns 256 consecutive cells (row-major
+// over the region) of one block, so the block's parameters are uniform over
+// the CTA; the row comes from a float reciprocal of the region width with
+// one integer correction.  Offsets are 32-bit (the host uses this kernel only
+// when 9 planes of every block fit in 2^31 elements).
 template <int P, bool INTERIOR>
-__global__ void __launch_bounds__(256, P == MB_PREC_F64 ? 4 : 8) k_block_step_r(const __grid_constant__ StbParams p) {
+__global__ void __launch_bounds__(256, P == MB_PREC_F64 ? 4 : 6) k_block_step_r(const __grid_constant__ StbParams p) {
   pdl_trigger();
   pdl_wait();
-  const int tile = blockIdx.x;
+  const int cta = blockIdx.x;
   int t = 0;
 #pragma unroll 1
-  while (t + 1 < p.nblk && tile >= p.b[t + 1].rt0) t++;
+  while (t + 1 < p.nblk && cta >= p.b[t + 1].cta0) t++;
   const StbBlk &B = p.b[t];
-  const int lt = tile - B.rt0;
-  const int r = lt / B.rtiles_x;
+  const int local = (cta - B.cta0) * 256 + (int)threadIdx.x;
+  if (local >= B.rcells) return;
+  int r = __float2int_rz((float)local * B.rinv_w);
+  if (r * B.rw > local) r--;
+  else if ((r + 1) * B.rw <= local) r++;
   const int j = B.row0 + r;
-  const int i = B.col0 + (lt - r * B.rtiles_x) * 256 + (int)threadIdx.x;
-  if (i > B.col1) return;
+  const int i = B.rcol0 + (local - r * B.rw);
   if (p.evict_first) stb_cell_rows<P, true, INTERIOR>(p, B, i, j);
   else stb_cell_rows<P, false, INTERIOR>(p, B, i, j);
 }
@@ -1378,8 +1389,12 @@ struct L2Params {
 };
 
 // A CTA walks row tiles (256 consecutive cells of one row of one block, the
-// block and row uniform over the CTA) with a fixed stride, so every cell is
-// summed by the same thread in the same order on every call.
+// block and row uniform over the CTA) with a fixed stride, L2_ILP tiles per
+// iteration with all their loads in flight before any use, so every cell is
+// summed by the same thread in the same order on every call.  The last CTA
+// (ticket counter) adds the per-CTA partials with all its threads in a fixed
+// order and resets the ticket.
+constexpr int L2_ILP = 4;
 template <int P>
 __global__ void __launch_bounds__(256) k_error_l2(const __grid_constant__ L2Params p) {
   using R = typename Prec<P>::R;
@@ -1387,25 +1402,44 @@ __global__ void __launch_bounds__(256) k_error_l2(const __grid_constant__ L2Para
   for (int q = threadIdx.x; q < p.nblk; q += blockDim.x) s_rt0[q] = p.blocks[q].rt0;
   __syncthreads();
   double s1 = 0, s2 = 0;
-  for (int t = blockIdx.x; t < p.ntiles; t += gridDim.x) {
-    int lo = 0, hi = p.nblk - 1;  // last block whose first tile is <= t
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (s_rt0[mid] <= t) lo = mid; else hi = mid - 1;
-    }
-    const L2Blk &b = p.blocks[lo];
-    const IfBlk &B = p.blk[lo];
-    const int lt = t - s_rt0[lo];
-    const int j = lt / b.rtiles_x;
-    const int i = (lt - j * b.rtiles_x) * 256 + (int)threadIdx.x;
-    if (i < b.nx) {
+  const int stride = gridDim.x;
+  for (int t0 = blockIdx.x; t0 < p.ntiles; t0 += L2_ILP * stride) {
+    R ux[L2_ILP], uy[L2_ILP], upx[L2_ILP], upy[L2_ILP];
+    R *px[L2_ILP], *py[L2_ILP];
+    double w[L2_ILP];
+#pragma unroll
+    for (int u = 0; u < L2_ILP; u++) {
+      const int t = t0 + u * stride;
+      px[u] = nullptr;
+      if (t >= p.ntiles) continue;
+      int lo = 0, hi = p.nblk - 1;  // last block whose first tile is <= t
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (s_rt0[mid] <= t) lo = mid; else hi = mid - 1;
+      }
+      const L2Blk &b = p.blocks[lo];
+      const IfBlk &B = p.blk[lo];
+      const int lt = t - s_rt0[lo];
+      const int j = lt / b.rtiles_x;
+      const int i = (lt - j * b.rtiles_x) * 256 + (int)threadIdx.x;
+      if (i >= b.nx) continue;
       const int c = j * b.pitch + i;
-      const double ux = ((const R *)B.ux)[c], uy = ((const R *)B.uy)[c];
-      const double upx = ((const R *)B.upx)[c], upy = ((const R *)B.upy)[c];
-      s1 += ((ux - upx) * (ux - upx) + (uy - upy) * (uy - upy)) * b.inv_m;
-      s2 += (ux * ux + uy * uy) * b.inv_m;
-      ((R *)B.upx)[c] = (R)ux;
-      ((R *)B.upy)[c] = (R)uy;
+      ux[u] = ((const R *)B.ux)[c];
+      uy[u] = ((const R *)B.uy)[c];
+      upx[u] = ((const R *)B.upx)[c];
+      upy[u] = ((const R *)B.upy)[c];
+      px[u] = (R *)B.upx + c;
+      py[u] = (R *)B.upy + c;
+      w[u] = b.inv_m;
+    }
+#pragma unroll
+    for (int u = 0; u < L2_ILP; u++) {
+      if (!px[u]) continue;
+      const double x = ux[u], y = uy[u], xp = upx[u], yp = upy[u];
+      s1 += ((x - xp) * (x - xp) + (y - yp) * (y - yp)) * w[u];
+      s2 += (x * x + y * y) * w[u];
+      *px[u] = ux[u];
+      *py[u] = uy[u];
     }
   }
 #pragma unroll
@@ -1415,8 +1449,8 @@ __global__ void __launch_bounds__(256) k_error_l2(const __grid_constant__ L2Para
   }
   __shared__ double a1[8], a2[8];
   __shared__ bool last;
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  if (l == 0) { a1[w] = s1; a2[w] = s2; }
+  const int w0 = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) { a1[w0] = s1; a2[w0] = s2; }
   __syncthreads();
   if (threadIdx.x == 0) {
     double t1 = 0, t2 = 0;
@@ -1427,16 +1461,29 @@ __global__ void __launch_bounds__(256) k_error_l2(const __grid_constant__ L2Para
     last = (done == gridDim.x - 1);
   }
   __syncthreads();
-  if (last && threadIdx.x == 0) {
-    __threadfence();
-    double t1 = 0, t2 = 0;
-    for (unsigned int q = 0; q < gridDim.x; q++) {
-      const double2 v = __ldcg(&p.partial[q]);
-      t1 += v.x;
-      t2 += v.y;
+  if (!last) return;
+  __threadfence();
+  // thread q adds partials q, q + 256, ... in order; then a fixed tree
+  double t1 = 0, t2 = 0;
+  for (unsigned int q = threadIdx.x; q < gridDim.x; q += blockDim.x) {
+    const double2 v = __ldcg(&p.partial[q]);
+    t1 += v.x;
+    t2 += v.y;
+  }
+  __shared__ double r1[256], r2[256];
+  r1[threadIdx.x] = t1;
+  r2[threadIdx.x] = t2;
+  __syncthreads();
+  for (int sz = blockDim.x / 2; sz > 0; sz >>= 1) {
+    if ((int)threadIdx.x < sz) {
+      r1[threadIdx.x] += r1[threadIdx.x + sz];
+      r2[threadIdx.x] += r2[threadIdx.x + sz];
     }
-    p.out[0] = t1;
-    p.out[1] = t2;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    p.out[0] = r1[0];
+    p.out[1] = r2[0];
     *p.ticket = 0u;
   }
 }

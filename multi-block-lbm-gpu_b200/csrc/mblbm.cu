@@ -126,6 +126,7 @@ struct mb_ctx {
   int period = 1;
   long long split_cells = 1000000;
   long long stream_cells = 2000000;
+  unsigned split_mask = 0;            // nonzero: the levels to split (bit per level), overriding split_cells
   int bulk_levels = 0;                // 1: whole-level block steps that stream with hints are bulk (low priority) work   // block steps over >= this many cells use evict-first cache hints (0: never)
   int stb_variant[MB_MAX_LEVEL] = {0};  // 0: one cell per thread, 1: quads (k_block_step_q)
   int bulk_ctas_per_sm = 0;             // >0: cap interior (bulk) block-step grids at this many CTAs per SM
@@ -266,15 +267,15 @@ StbParams make_stb(mb_ctx *c, int a0, int a1, uint64_t parity, int macro_all, in
     const int nrows = region == STB_INTERIOR ? std::max(0, B.ny - 4) : B.ny;
     s.wt0 = wt;
     wt += (long long)s.tiles_x * nrows;
-    // row kernel: tiles of 256 cells over the region's columns
-    s.col0 = region == STB_INTERIOR ? 2 : 0;
-    s.col1 = region == STB_INTERIOR ? B.nx - 3 : B.nx - 1;
-    const int ncols = std::max(0, s.col1 - s.col0 + 1);
-    s.rtiles_x = std::max(1, (ncols + 255) / 256);
-    s.rt0 = (int)rt;
-    rt += ncols > 0 ? (long long)s.rtiles_x * nrows : 0;
+    // range kernel: CTAs of 256 consecutive cells of the region
+    s.rcol0 = region == STB_INTERIOR ? 2 : 0;
+    s.rw = std::max(0, region == STB_INTERIOR ? B.nx - 4 : B.nx);
+    s.rcells = s.rw > 0 ? (int)std::min<long long>((long long)s.rw * nrows, 1LL << 30) : 0;
+    s.rinv_w = s.rw > 0 ? 1.0f / (float)s.rw : 0.f;
+    s.cta0 = (int)rt;
+    rt += (s.rcells + 255) / 256;
   }
-  p.rtiles = rt;
+  p.rctas = rt;
   p.total = quads ? wt : cell;
   return p;
 }
@@ -286,12 +287,14 @@ bool stb_uses_quads(const mb_ctx *c, int level, int region) {
 
 bool background_capped(const mb_ctx *c, bool background) { return background && c->bulk_ctas_per_sm > 0; }
 
-// the row kernel indexes 9 planes of a block with 32-bit offsets
+// the range kernel indexes 9 planes of a block with 32-bit offsets
 bool rows_fit(const mb_ctx *c, const StbParams &p) {
   for (int t = 0; t < p.nblk; t++)
-    if (9 * p.b[t].plane >= (1LL << 31) || (long long)p.b[t].ny * p.b[t].pitch >= (1LL << 31)) return false;
+    if (9 * p.b[t].plane >= (1LL << 31) || (long long)p.b[t].ny * p.b[t].pitch >= (1LL << 31) ||
+        p.b[t].rcells >= (1 << 24))  // the row of a cell index comes from a float product
+      return false;
   (void)c;
-  return p.rtiles < (1LL << 31);
+  return p.rctas < (1LL << 31);
 }
 
 // kernel and grid of a block-step launch (variant 0: one cell per thread,
@@ -306,7 +309,7 @@ void stb_launch_shape(const mb_ctx *c, int level, int region, bool background, c
   }
   if (c->stb_variant[level] == 3 && region != STB_RIM && !background_capped(c, background) && rows_fit(c, p)) {
     *func = region == STB_INTERIOR ? kfunc<KStbRI>(c->prec) : kfunc<KStbR>(c->prec);
-    *grid = dim3((unsigned)p.rtiles);
+    *grid = dim3((unsigned)p.rctas);
     return;
   }
   const bool two = c->stb_variant[level] == 2;
@@ -672,6 +675,7 @@ CompiledPlan *get_plan(mb_ctx *c, int n, bool final_macros, int *err) {
   auto cp = std::make_unique<CompiledPlan>();
   PlanCompiler pc(c->geo, c->bl, c->hflags, c->spl_lines);
   pc.split_cells = c->split_cells;
+  pc.split_mask = c->split_mask;
   SchedState s = c->state;
   cp->nodes = pc.compile(s, n, final_macros);
   cp->end = s;
@@ -918,7 +922,7 @@ extern "C" int mb_create(const mb_geometry *geo, int precision, mb_ctx **out) {
     c->l2_tiles = (int)tiles;
     if ((e = dalloc(c.get(), &c->d_l2blk, c->nblk))) return e;
     MB_CUDA(cudaMemcpy(c->d_l2blk, lb.data(), lb.size() * sizeof(L2Blk), cudaMemcpyHostToDevice));
-    c->l2_grid = (int)std::min<long long>(tiles, 148LL * 8);
+    c->l2_grid = (int)std::min<long long>(tiles, 148LL * 16);
     if ((e = dalloc(c.get(), &c->d_l2_partial, c->l2_grid))) return e;
     if ((e = dalloc(c.get(), &c->d_l2_ticket, 1))) return e;
     MB_CUDA(cudaMemset(c->d_l2_ticket, 0, sizeof(unsigned int)));
@@ -1006,6 +1010,14 @@ extern "C" int mb_set_interface_shape(mb_ctx *c, int rec_points, int spline_segm
   cudaDeviceSynchronize();
   c->rec_points = rec_points;
   c->spl_segs = spline_segments;
+  c->plans.clear();
+  return MB_OK;
+}
+
+extern "C" int mb_set_split_levels(mb_ctx *c, unsigned level_mask) {
+  if (!c || level_mask >= (1u << MB_MAX_LEVEL)) return MB_ERR_INVALID;
+  cudaDeviceSynchronize();
+  c->split_mask = level_mask;
   c->plans.clear();
   return MB_OK;
 }

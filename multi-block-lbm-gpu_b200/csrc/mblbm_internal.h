@@ -121,6 +121,8 @@ struct PlanCompiler {
   const std::vector<SplLine> &spl_lines;
   // levels with at least this many cells step their interior and rim as two nodes
   long long split_cells = 1000000;
+  // nonzero: level l splits exactly when bit l is set (overrides split_cells)
+  unsigned split_mask = 0;
   PlanCompiler(const mb_geometry &g_, const std::vector<BlockLayout> &bl_,
                const std::vector<std::vector<uint8_t>> &fl, const std::vector<SplLine> &sl)
       : g(g_), bl(bl_), flags(fl), spl_lines(sl) {}

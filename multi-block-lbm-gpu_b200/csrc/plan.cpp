@@ -271,7 +271,7 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
       I.parity = o.parity;
       long long level_cells = 0;
       for (int a = L.ASP[o.level]; a < L.ASP[o.level + 1]; a++) level_cells += (long long)bl[a].nx * bl[a].ny;
-      const bool split = level_cells >= split_cells;
+      const bool split = split_mask ? ((split_mask >> o.level) & 1u) != 0 : level_cells >= split_cells;
       for (int a0 = L.ASP[o.level]; a0 < L.ASP[o.level + 1]; a0 += 16) {
         const int a1 = std::min(L.ASP[o.level + 1], a0 + 16);
         for (int region : split ? std::vector<int>{STB_RIM, STB_INTERIOR} : std::vector<int>{STB_ALL}) {

@@ -142,6 +142,7 @@ SIGNATURES = {
     "mb_set_bulk_occupancy": ([_vp, C.c_int], C.c_int),
     "mb_set_stream_cells": ([_vp, C.c_longlong, C.c_int], C.c_int),
     "mb_set_interface_shape": ([_vp, C.c_int, C.c_int], C.c_int),
+    "mb_set_split_levels": ([_vp, C.c_uint], C.c_int),
     "mb_set_program_timeout": ([_vp, C.c_double], C.c_int),
     "mb_set_program_shape": ([_vp, C.c_int, C.c_int, C.c_int, C.c_int], C.c_int),
     "mb_sync": ([_vp, _vp], C.c_int),
@@ -396,6 +397,10 @@ class MultiBlockLBM:
         """Block-step kernel of a level: 0 one cell per thread, 1 four cells per thread."""
         _check(self.lib.mb_set_stb_variant(self.h, int(level), int(variant)), "mb_set_stb_variant")
 
+    def set_split_levels(self, level_mask):
+        """Split exactly the levels of level_mask (bit per level) into interior and rim nodes (0: threshold)."""
+        _check(self.lib.mb_set_split_levels(self.h, int(level_mask)), "mb_set_split_levels")
+
     def set_interface_shape(self, rec_points=32, spline_segments=1):
         """Points per record CTA/item (32 or 64) and spline segments per CTA/item (1-4)."""
         _check(self.lib.mb_set_interface_shape(self.h, int(rec_points), int(spline_segments)),
@@ -608,6 +613,10 @@ class Batch:
         u, k = C.c_longlong(), C.c_longlong()
         _check(self.lib.mb_batch_stats(self.h, C.byref(u), C.byref(k)), "mb_batch_stats")
         return {"updates_per_step": u.value, "kernels_last_call": k.value}
+
+    def set_split_levels(self, level_mask):
+        """Split exactly the levels of level_mask (bit per level) into interior and rim nodes (0: threshold)."""
+        _check(self.lib.mb_set_split_levels(self.h, int(level_mask)), "mb_set_split_levels")
 
     def set_interface_shape(self, rec_points=32, spline_segments=1):
         _check(self.lib.mb_batch_set_interface_shape(self.h, int(rec_points), int(spline_segments)),
