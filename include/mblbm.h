@@ -229,7 +229,8 @@ int mb_set_stream_cells(mb_ctx *ctx, long long cells, int bulk);
  * 1 = four cells per thread with vector loads, 2 = two cells per thread with
  * the loads of both in flight together, 3 = cell ranges: a CTA steps 256
  * consecutive cells of one block with 32-bit offsets (whole levels and
- * interiors; rims use 0).  Results are identical. */
+ * interiors; rims use 0).  Default 0, and 3 for level 0 in MB_PREC_F16S.
+ * Results are identical. */
 int mb_set_stb_variant(mb_ctx *ctx, int level, int variant);
 /* Caps the grid of interior (bulk) block-step launches at ctas_per_sm CTAs of
  * 256 threads per SM (0 = uncapped), leaving CTA slots on every SM for the

@@ -731,7 +731,7 @@ __device__ __forceinline__ R spline3_s(R xx, R x_1, R h, R fi_1, R fi, R mi_1, R
 // the data (1e-16 in FP64, 1e-9 in FP32), i.e. they equal the whole-line solve
 // to rounding.  Every segment is independent, so a line's gathers and solves
 // spread over many SMs.
-constexpr int SPL_SEG = 32;
+constexpr int SPL_SEG = 16;
 constexpr int SPL_WARPS = 4;
 template <typename R> struct SplHalo { static constexpr int v = 16; };
 template <> struct SplHalo<double> { static constexpr int v = 28; };
