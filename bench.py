@@ -381,15 +381,10 @@ def main():
     import torch
 
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-
     import mblbm
+    from mblbm import ranks
+
+    dist = ranks.init("nccl") if world > 1 else None
 
     geo = mblbm.config2_geometry()
     upd = mblbm.updates_per_coarse_step(geo)
@@ -471,10 +466,7 @@ def main():
     wall_e2e = time.perf_counter() - t0
     sim2.close()
 
-    if dist:
-        t = torch.tensor([ms, ms_e2e], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, ms_e2e = float(t[0]), float(t[1])
+    ms, ms_e2e = ranks.reduce([ms, ms_e2e], "max", dist, device="cuda")  # the slowest rank's device time
 
     if rank == 0:
         peak, src = peaks()
