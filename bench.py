@@ -331,6 +331,47 @@ def run_warmstart(args):
     return 0
 
 
+def run_forces(args):
+    """Config 2's flow outputs: the 3-level cylinder at Re=100 run for --steps
+    coarse steps from rest with Cd and Cl recorded every step (mb_step_diag);
+    mean Cd, rms Cl and the Strouhal number over the second half of the run."""
+    import numpy as np
+    import torch
+    import mblbm
+
+    torch.cuda.set_device(0)
+    geo = mblbm.config2_geometry()
+    sim = mblbm.MultiBlockLBM(geo, args.precision)
+    sim.init()
+    cd, cl = [], []
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    chunk = 5000
+    for q in range(0, args.steps, chunk):
+        a, b, _ = sim.evolution_diag(min(chunk, args.steps - q))
+        cd.append(a)
+        cl.append(b)
+    e1.record()
+    torch.cuda.synchronize()
+    cd, cl = np.concatenate(cd), np.concatenate(cl)
+    half = len(cd) // 2
+    c = geo.config
+    D, U0 = 2.0 * c.R, c.U0[0]
+    st = mblbm.strouhal(cl, D, U0, skip=half)
+    line = {"metric": "mean Cd, rms Cl, Strouhal number", "unit": "dimensionless", "n_gpus": 1, "steps": args.steps,
+            "data": "synthetic", "dtype": args.precision,
+            "config": {"workload": WORKLOAD, "statistics_over": f"coarse steps {half}..{len(cd) - 1}"},
+            "mean_cd": round(float(cd[half:].mean()), 5), "rms_cl": round(float(np.sqrt(np.mean(cl[half:] ** 2))), 5),
+            "strouhal": None if st is None else round(float(st), 5),
+            "cd_last": round(float(cd[-1]), 5), "cl_last": round(float(cl[-1]), 5),
+            "max_abs_cl": round(float(np.abs(cl[half:]).max()), 5), "device_s": round(e0.elapsed_time(e1) / 1e3, 2)}
+    print(json.dumps(line), flush=True)
+    np.save(os.path.join(REPO, "gpurun_out", f"forces_{args.precision}.npy"), np.stack([cd, cl])) if os.path.isdir(
+        os.path.join(REPO, "gpurun_out")) else None
+    sim.close()
+    return 0
+
+
 def unet_gflop(H, W):
     """Forward GFLOP of the surrogate for one sample (3x3 convolutions)."""
     layers = [(16, 32, 0), (32, 32, 0), (32, 64, 1), (64, 64, 1), (64, 128, 2), (128, 128, 2), (128, 256, 3),
@@ -352,7 +393,7 @@ def main():
                          "prints its roofline")
     ap.add_argument("--level", type=int, default=0, help="level of --roofline-only")
     ap.add_argument("--variant", type=int, default=None, help="block-step variant of every level (mb_set_stb_variant)")
-    ap.add_argument("--workload", default="cylinder3", choices=["cylinder3", "batch256", "timetocd", "warmstart"],
+    ap.add_argument("--workload", default="cylinder3", choices=["cylinder3", "batch256", "timetocd", "warmstart", "forces"],
                     help="cylinder3: the single 3-level case (default); batch256: the batched form; "
                          "timetocd: Cd convergence of the 2-level case by precision")
     ap.add_argument("--cases", type=int, default=256, help="cases of --workload batch256 / training cases of warmstart")
@@ -377,6 +418,8 @@ def main():
         return run_timetocd(args)
     if args.workload == "warmstart":
         return run_warmstart(args)
+    if args.workload == "forces":
+        return run_forces(args)
 
     import torch
 

@@ -643,21 +643,24 @@ def settle_step(series, target, rel=0.005):
 def strouhal(cl, D, U0, skip=0):
     """St = f D / U0 from the dominant frequency of the lift series (one value
     per coarse step, D and U0 in coarse lattice units); None without a clear
-    oscillation.  The frequency comes from mean-crossings of the series after
-    `skip` steps, interpolated between steps."""
+    oscillation.  f is the peak of the Hann-windowed spectrum of the series
+    after `skip` steps, refined by a parabola through the peak and its
+    neighbours (robust to the high-frequency noise of FP16 storage)."""
     x = np.asarray(cl[skip:], dtype=np.float64)
-    if len(x) < 8:
+    if len(x) < 16:
         return None
     x = x - x.mean()
     if np.abs(x).max() < 1e-9:
         return None
-    s = np.signbit(x)
-    idx = np.nonzero(s[1:] != s[:-1])[0]
-    up = [i + x[i] / (x[i] - x[i + 1]) for i in idx if x[i] < 0 <= x[i + 1]]
-    if len(up) < 3:
+    sp = np.abs(np.fft.rfft(x * np.hanning(len(x))))
+    k = int(np.argmax(sp[1:])) + 1
+    if k >= len(sp) - 1:
         return None
-    period = (up[-1] - up[0]) / (len(up) - 1)
-    return D / (period * U0)
+    a, b, c = np.log(sp[k - 1] + 1e-300), np.log(sp[k] + 1e-300), np.log(sp[k + 1] + 1e-300)
+    den = a - 2 * b + c
+    dk = 0.5 * (a - c) / den if den != 0 else 0.0
+    f = (k + dk) / len(x)
+    return f * D / U0
 
 
 # ---------------------------------------------------------------------------
