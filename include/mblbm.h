@@ -53,7 +53,13 @@ extern "C" {
 /* ---- cell type codes, values as in lbm/lbm.h:26-32 -------------------- */
 #define MB_FLUID 0
 #define MB_SOLID_SBB 1
+#define MB_SOLID_SLIP 2 /* free-slip on-node wall, slip_gpu (lbm/lbm.h:51); no code in the reference */
+#define MB_SOLID_HBB 3  /* half-way bounce-back, SOLID_HBB (lbm/lbm.h:28); declared, unused there */
 #define MB_C_BOUNDARY 9
+
+/* ---- collision operators -------------------------------------------------- */
+#define MB_COLL_BGK 0 /* evolution_block.h:99-111 */
+#define MB_COLL_MRT 1 /* M_gpu/InvM_gpu (lbm/lbm.h:53-75), Meq (lbm/assit_func.h:10-22) */
 
 /* ---- obstacle kinds ---------------------------------------------------- */
 #define MB_OBST_CIRCLE 0  /* (x-CX)^2+(y-CY)^2 < R^2, lbm/init_block.h:28    */
@@ -236,6 +242,27 @@ int mb_set_stb_variant(mb_ctx *ctx, int level, int variant);
  * 256 threads per SM (0 = uncapped), leaving CTA slots on every SM for the
  * fine-level kernels that run beside them. */
 int mb_set_bulk_occupancy(mb_ctx *ctx, int ctas_per_sm);
+
+/* ---- collision and boundary options ----------------------------------------
+ * The reference declares these but never uses them: MRT (M_gpu, InvM_gpu,
+ * lbm/lbm.h:53-75; Meq, lbm/assit_func.h:10-22), the body-force term of stb3
+ * (multi/FH/evolution_block.h:97-108, forcex/forcey), free slip (slip_gpu,
+ * lbm/lbm.h:51) and half-way bounce-back (SOLID_HBB, lbm/lbm.h:28).  While any
+ * is on, every block step runs one general kernel; the persistent executor
+ * (graph mode 3) and batches return MB_ERR_UNSUPPORTED. */
+/* MB_COLL_BGK, or MB_COLL_MRT with S = diag(0, s_e, s_eps, 0, s_q, 0, s_q,
+ * 1/tau, 1/tau); a rate <= 0 stands for the block's 1/tau (all three <= 0:
+ * the BGK result up to rounding).  Rates must be below 2. */
+int mb_set_collision(mb_ctx *ctx, int kind, double s_e, double s_eps, double s_q);
+/* forcex, forcey of every cell (coarse lattice units), added as
+ * dt (1 - 1/(2 tau)) w_k (v_k . F) on every FLUID cell, dt = 1/m. */
+int mb_set_body_force(mb_ctx *ctx, double fx, double fy);
+/* Cell types of one block, nx*ny codes (i + j*nx): MB_FLUID, MB_SOLID_SBB,
+ * MB_SOLID_SLIP or MB_SOLID_HBB on cells that are FLUID or solid; C_BOUNDARY
+ * cells must be passed unchanged.  A FLUID cell whose upstream neighbour
+ * x - e_k is HBB takes f_k = F_opp(k) of itself; a slip cell returns
+ * F_k = f_slip(k).  The drag sums SBB and HBB links.  Kept across mb_init. */
+int mb_set_cell_types(mb_ctx *ctx, int area, const int *types);
 /* Compiles the plans (and CUDA graphs) that mb_step(ctx, n) will replay from
  * the current state, so the step call itself spends no host time on them. */
 int mb_prepare(mb_ctx *ctx, int n_coarse);

@@ -22,6 +22,7 @@ namespace dev {
 __host__ __device__ constexpr int ex(int k) { return k == 1 || k == 5 || k == 8 ? 1 : (k == 3 || k == 6 || k == 7 ? -1 : 0); }
 __host__ __device__ constexpr int ey(int k) { return k == 2 || k == 5 || k == 6 ? 1 : (k == 4 || k == 7 || k == 8 ? -1 : 0); }
 __host__ __device__ constexpr int opp(int k) { return k == 0 ? 0 : (k <= 4 ? ((k + 1) & 3) + 1 : ((k - 3) & 3) + 5); }
+__host__ __device__ constexpr int slip(int k) { return k == 2 ? 4 : k == 4 ? 2 : k == 5 ? 8 : k == 8 ? 5 : k == 6 ? 7 : k == 7 ? 6 : k; }
 __host__ __device__ constexpr double wd(int k) { return k == 0 ? 4. / 9 : (k <= 4 ? 1. / 9 : 1. / 36); }
 
 template <int P> struct Prec;
@@ -103,6 +104,15 @@ struct StbBlk {
   int rw, rcol0;      // region width and first column (first row: row0)
   float rinv_w;       // 1 / rw, for the row of a cell index
   int pad2_;
+  double dt;          // 1 / m: time step of the block in coarse units (body-force term)
+};
+
+// Collision and boundary options (the options kernel k_block_step_x only).
+struct StbOptions {
+  int coll;         // MB_COLL_BGK or MB_COLL_MRT
+  int has_force;    // body force non-zero
+  double mrt_s[3];  // s_e, s_eps, s_q; <= 0: the block's 1/tau
+  double force[2];  // forcex, forcey of every cell
 };
 
 struct StbParams {
@@ -115,6 +125,7 @@ struct StbParams {
   long long rctas;   // CTAs of a range-kernel launch
   double feqc[9];    // feq(rho0, U0): block-edge FLUID cells and stale f of edge solids
   double rho0, u0x, u0y;
+  StbOptions opt;
   StbBlk b[STB_MAX_BLOCKS];
 };
 
@@ -366,6 +377,206 @@ __global__ void __launch_bounds__(256, CPT == 1 ? (P == MB_PREC_F64 ? 4 : 8) : (
         stb_at<P>(p, g0);
       }
     }
+  }
+}
+
+// ----------------------------------------------------------------------------
+// Options kernel: the block step with the collision and boundary options the
+// reference declares but never uses.  Used for every block step of a context
+// once any option is on; the other block-step kernels assume BGK, no force
+// and only SOLID_SBB walls.
+//  - body force: the term of stb3 (multi/FH/evolution_block.h:99-108) with
+//    forcex/forcey one value everywhere, on every FLUID cell (block-edge
+//    cells too, where stb3 collides the imposed equilibrium);
+//  - MRT: F = f - M^-1 S (M f - meq) + dt Force_k with M_gpu (lbm/lbm.h:53-63),
+//    M^-1 = M^T diag(1/|row|^2) (InvM_gpu, lbm/lbm.h:64-75, exactly), meq of
+//    Meq (lbm/assit_func.h:10-22, A = 1, B = -3), S = diag(0, s_e, s_eps, 0,
+//    s_q, 0, s_q, 1/tau, 1/tau);
+//  - MB_SOLID_SLIP: on-node wall returning F_k = f_slip(k) (slip_gpu,
+//    lbm/lbm.h:51) where SOLID_SBB returns f_opp(k);
+//  - MB_SOLID_HBB: a FLUID cell whose upstream neighbour x - e_k is an HBB
+//    cell takes f_k(x) = F_opp(k)(x), its own value of the previous step; HBB
+//    cells keep their distributions.
+// ----------------------------------------------------------------------------
+constexpr uint8_t FL_HBB = 16, FL_SLIP = 32;
+
+// M_gpu entries (lbm/lbm.h:53-63) and squared row norms
+__host__ __device__ constexpr int mrt_m(int q, int k) {
+  return q == 0 ? 1
+       : q == 1 ? (k == 0 ? -4 : k <= 4 ? -1 : 2)
+       : q == 2 ? (k == 0 ? 4 : k <= 4 ? -2 : 1)
+       : q == 3 ? ex(k)
+       : q == 4 ? (k == 0 ? 0 : k <= 4 ? -2 * ex(k) : ex(k))
+       : q == 5 ? ey(k)
+       : q == 6 ? (k == 0 ? 0 : k <= 4 ? -2 * ey(k) : ey(k))
+       : q == 7 ? (k == 0 ? 0 : k <= 4 ? ex(k) * ex(k) - ey(k) * ey(k) : 0)
+       : (k <= 4 ? 0 : ex(k) * ey(k));
+}
+__host__ __device__ constexpr double mrt_norm(int q) {
+  return q == 0 ? 9 : q == 1 || q == 2 ? 36 : q == 3 || q == 5 ? 6 : q == 4 || q == 6 ? 12 : 4;
+}
+
+// MRT relaxation of a FLUID cell.  f holds f (or h = f - w when shifted);
+// writes the post-collision values (same variable) and rho/u to m.
+template <int P>
+__device__ __forceinline__ void mrt_collide(const typename Prec<P>::R *f, typename Prec<P>::R rv,
+                                            const StbOptions &o, typename Prec<P>::R *out,
+                                            typename Prec<P>::R *m) {
+  using R = typename Prec<P>::R;
+  // Macros (lbm/assit_func.h:23-31)
+  R rh = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8];
+  const R base = rh;  // rho - 1 when shifted
+  if constexpr (Prec<P>::shifted) rh = (R)1 + rh;
+  R ux = f[1] - f[3] + f[5] - f[6] - f[7] + f[8];
+  R uy = f[2] - f[4] + f[5] + f[6] - f[7] - f[8];
+  ux = ux / rh;
+  uy = uy / rh;
+  m[0] = rh;
+  m[1] = ux;
+  m[2] = uy;
+  R mo[9];
+#pragma unroll
+  for (int q = 0; q < 9; q++) {
+    R a = (R)0;
+#pragma unroll
+    for (int k = 0; k < 9; k++)
+      if (mrt_m(q, k) != 0) a += (R)mrt_m(q, k) * f[k];
+    mo[q] = a;
+  }
+  const R uv = ux * ux + uy * uy;
+  R meq[9];
+  if constexpr (Prec<P>::shifted) {  // Meq minus the moments of w: (1, -2, 1, 0, ...)
+    meq[0] = base;
+    meq[1] = (R)-2 * base + (R)3 * rh * uv;
+    meq[2] = base - (R)3 * rh * uv;
+  } else {
+    meq[0] = rh;
+    meq[1] = rh * ((R)-2.0 + (R)3.0 * uv);
+    meq[2] = rh * ((R)1.0 - (R)3.0 * uv);
+  }
+  meq[3] = rh * ux;
+  meq[4] = -meq[3];
+  meq[5] = rh * uy;
+  meq[6] = -meq[5];
+  meq[7] = rh * (ux * ux - uy * uy);
+  meq[8] = rh * (ux * uy);
+  const R se = o.mrt_s[0] > 0 ? (R)o.mrt_s[0] : rv;
+  const R sp = o.mrt_s[1] > 0 ? (R)o.mrt_s[1] : rv;
+  const R sq = o.mrt_s[2] > 0 ? (R)o.mrt_s[2] : rv;
+  R dm[9];
+  dm[0] = dm[3] = dm[5] = (R)0;
+  dm[1] = se * (mo[1] - meq[1]) / (R)mrt_norm(1);
+  dm[2] = sp * (mo[2] - meq[2]) / (R)mrt_norm(2);
+  dm[4] = sq * (mo[4] - meq[4]) / (R)mrt_norm(4);
+  dm[6] = sq * (mo[6] - meq[6]) / (R)mrt_norm(6);
+  dm[7] = rv * (mo[7] - meq[7]) / (R)mrt_norm(7);
+  dm[8] = rv * (mo[8] - meq[8]) / (R)mrt_norm(8);
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    R r = (R)0;
+#pragma unroll
+    for (int q = 0; q < 9; q++)
+      if (mrt_m(q, k) != 0 && q != 0 && q != 3 && q != 5) r += (R)mrt_m(q, k) * dm[q];
+    out[k] = f[k] - r;
+  }
+}
+
+// body-force term of stb3 (evolution_block.h:102-107) for direction k
+template <typename R>
+__device__ __forceinline__ R force_k(int k, R ux, R uy, R fx, R fy, R rv) {
+  const R eu = (R)ex(k) * ux + (R)ey(k) * uy;
+  const R vx = (R)3.0 * ((R)ex(k) - ux) + (R)9.0 * eu * (R)ex(k);
+  const R vy = (R)3.0 * ((R)ey(k) - uy) + (R)9.0 * eu * (R)ey(k);
+  return ((R)1.0 - (R)0.5 * rv) * (R)wd(k) * (vx * fx + vy * fy);
+}
+
+template <int P>
+__device__ __forceinline__ void stbx_cell(const StbParams &p, const StbBlk &B, int i, int j) {
+  using R = typename Prec<P>::R;
+  using S = typename Prec<P>::S;
+  const long long c = (long long)j * B.pitch + i;
+  const uint8_t fl = B.flags[c];
+  const int type = fl & 3;
+  const S *Fin = (const S *)B.Fin;
+  S *Fout = (S *)B.Fout;
+  const long long plane = B.plane;
+  const R rv = (R)B.rv_tau, dt = (R)B.dt;
+  const R fx = (R)p.opt.force[0], fy = (R)p.opt.force[1];
+  if (type == 0) {
+    const bool wm = p.write_macros && (p.macro_all || (fl & 8));
+    if (fl & 4) {  // block edge: the imposed equilibrium, collided (identity) plus the force term
+#pragma unroll
+      for (int k = 0; k < 9; k++) {
+        R v = (R)p.feqc[k];
+        if (p.opt.has_force) v += dt * force_k<R>(k, (R)p.u0x, (R)p.u0y, fx, fy, rv);
+        if constexpr (Prec<P>::shifted) v -= wk<P>(k);
+        Fout[k * plane + c] = from_r<S>(v);
+      }
+      if (wm) {
+        ((R *)B.rho)[c] = (R)p.rho0;
+        ((R *)B.ux)[c] = (R)p.u0x;
+        ((R *)B.uy)[c] = (R)p.u0y;
+      }
+      return;
+    }
+    R f[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+      const long long n = c - ((long long)ey(k) * B.pitch + ex(k));
+      const bool hbb = (B.flags[n] & (3 | FL_HBB)) == (1 | FL_HBB);
+      f[k] = to_r(hbb ? Fin[opp(k) * plane + c] : Fin[k * plane + n]);
+    }
+    R out[9], m[3];
+    if (p.opt.coll == MB_COLL_MRT) mrt_collide<P>(f, rv, p.opt, out, m);
+    else stb_collide<P>(f, rv, out, m);
+    if (p.opt.has_force) {
+#pragma unroll
+      for (int k = 0; k < 9; k++) out[k] += dt * force_k<R>(k, m[1], m[2], fx, fy, rv);
+    }
+    if (wm) {
+      ((R *)B.rho)[c] = m[0];
+      ((R *)B.ux)[c] = m[1];
+      ((R *)B.uy)[c] = m[2];
+    }
+#pragma unroll
+    for (int k = 0; k < 9; k++) Fout[k * plane + c] = from_r<S>(out[k]);
+    return;
+  }
+  if (type == 1 && (fl & FL_SLIP)) {  // pull as SOLID_SBB, return the slip partner
+    S raw[9];
+    stb_pull<P, false>(B, i, j, raw);
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+      const int id = i - ex(k), jd = j - ey(k);
+      if (!(id >= 0 && id < B.nx && jd >= 0 && jd < B.ny)) {
+        if constexpr (Prec<P>::shifted) raw[k] = from_r<S>((float)(p.feqc[k] - wd(k)));
+        else raw[k] = (S)p.feqc[k];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 9; k++) Fout[k * plane + c] = raw[slip(k)];  // w_k = w_slip(k)
+    return;
+  }
+  if (type == 1 && !(fl & FL_HBB)) {  // SOLID_SBB
+    S raw[9];
+    stb_pull<P, false>(B, i, j, raw);
+    stb_finish<P, false>(p, B, i, j, raw, fl);
+    return;
+  }
+  // HBB walls, C_BOUNDARY and row padding keep their distributions
+#pragma unroll
+  for (int k = 0; k < 9; k++) Fout[k * plane + c] = Fin[k * plane + c];
+}
+
+template <int P>
+__global__ void __launch_bounds__(256) k_block_step_x(const __grid_constant__ StbParams p) {
+  pdl_trigger();
+  pdl_wait();
+  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < p.total;
+       g += (long long)gridDim.x * blockDim.x) {
+    int t, i, j;
+    stb_locate(p, g, t, i, j);
+    stbx_cell<P>(p, p.b[t], i, j);
   }
 }
 
@@ -1318,7 +1529,7 @@ __global__ void __launch_bounds__(PRG_THREADS, P == MB_PREC_F64 ? 2 : 5) k_progr
 // ----------------------------------------------------------------------------
 struct DragLink {
   int32_t cell_s, cell_f;
-  int32_t k, fluid_edge;
+  int32_t k, fluid_edge;  // bit 0: cell_f on the block edge; bit 1: cell_s is a half-way wall
 };
 struct DragParams {
   const DragLink *links;
@@ -1343,7 +1554,12 @@ __global__ void __launch_bounds__(1024) k_drag(const __grid_constant__ DragParam
     for (int q = 0; q < 9; q++)
       if (q == k) { kd = opp(q); ek = ex(q); eky = ey(q); ekd = ex(opp(q)); ekdy = ey(opp(q)); }
     const double fs = (double)ld_f<P>(F, (long long)k * p.plane + L.cell_f, k);
-    const double ff = L.fluid_edge ? p.feqc[kd] : (double)ld_f<P>(F, (long long)kd * p.plane + L.cell_s, kd);
+    // returning value: feq(rho0, U0) at a block-edge FLUID cell (bit 0), the
+    // outgoing value itself at a half-way wall (bit 1), else the on-node
+    // wall's F_opp
+    const double ff = (L.fluid_edge & 1) ? p.feqc[kd]
+                      : (L.fluid_edge & 2) ? fs
+                                           : (double)ld_f<P>(F, (long long)kd * p.plane + L.cell_s, kd);
     fx += fs * ek - ff * ekd;
     fy += fs * eky - ff * ekdy;
   }

@@ -119,6 +119,9 @@ struct mb_ctx {
   double *d_stage = nullptr;
   size_t stage_elems = 0;
   double feqc[9]{};
+  // collision and boundary options (k_block_step_x)
+  StbOptions opt{};
+  long long n_alt_walls = 0;  // HBB and slip cells over all blocks
   // scheduler
   SchedState state;
   bool inited = false;
@@ -185,6 +188,49 @@ int dalloc(mb_ctx *c, T **p, size_t n) {
   return MB_OK;
 }
 
+// Links of the drag sum (fdrag_store, force_block.h:78-127), i-outer,
+// j-inner, k: SOLID_SBB and SOLID_HBB cells of the drag block with a FLUID
+// upstream neighbour (slip walls are left out).  Replaces any earlier list.
+int upload_drag_links(mb_ctx *c) {
+  const int a = c->drag_area;
+  const BlockLayout &b = c->bl[a];
+  const auto &fl = c->hflags[a];
+  std::vector<DragLink> links;
+  for (int i = 0; i < b.nx; i++)
+    for (int j = 0; j < b.ny; j++) {
+      const long long cs = (long long)j * b.pitch + i;
+      if ((fl[cs] & 3) != CT_SOLID || (fl[cs] & CF_SLIP)) continue;
+      for (int k = 0; k < 9; k++) {
+        const int id = i - ex(k), jd = j - ey(k);
+        if (id < 0 || id > b.nx - 1 || jd < 0 || jd > b.ny - 1) continue;
+        const long long cf = (long long)jd * b.pitch + id;
+        if ((fl[cf] & 3) != CT_FLUID) continue;
+        const int32_t kind = ((fl[cf] & CF_EDGE) ? 1 : 0) | ((fl[cs] & CF_HBB) ? 2 : 0);
+        links.push_back({(int32_t)cs, (int32_t)cf, k, kind});
+      }
+    }
+  if (c->d_links) {
+    auto it = std::find(c->allocs.begin(), c->allocs.end(), (void *)c->d_links);
+    if (it != c->allocs.end()) c->allocs.erase(it);
+    cudaFree(c->d_links);
+    c->d_links = nullptr;
+  }
+  c->n_drag = (int)links.size();
+  int e;
+  if ((e = dalloc(c, &c->d_links, links.size()))) return e;
+  if (!links.empty())
+    MB_CUDA(cudaMemcpy(c->d_links, links.data(), links.size() * sizeof(DragLink), cudaMemcpyHostToDevice));
+  return MB_OK;
+}
+
+// MB_* cell type code of a flag byte
+int flag_code(uint8_t f) {
+  const int t = f & 3;
+  if (t == CT_FLUID) return MB_FLUID;
+  if (t == CT_SOLID) return (f & CF_HBB) ? MB_SOLID_HBB : (f & CF_SLIP) ? MB_SOLID_SLIP : MB_SOLID_SBB;
+  return MB_C_BOUNDARY;
+}
+
 int launch_grid(long long n, int threads) { return (int)std::min<long long>((n + threads - 1) / threads, 148LL * 64); }
 
 // ---- templated dispatch over precision -------------------------------------
@@ -200,6 +246,7 @@ template <int P> struct KStb2 { static void *ptr() { return (void *)k_block_step
 template <int P> struct KStbR { static void *ptr() { return (void *)k_block_step_r<P, false>; } };
 template <int P> struct KStbRI { static void *ptr() { return (void *)k_block_step_r<P, true>; } };
 template <int P> struct KStbQ { static void *ptr() { return (void *)k_block_step_q<P>; } };
+template <int P> struct KStbX { static void *ptr() { return (void *)k_block_step_x<P>; } };
 template <int P> struct KRec { static void *ptr() { return (void *)k_records<P>; } };
 template <int P> struct KSpl { static void *ptr() { return (void *)k_spline<P>; } };
 template <int P> struct KDrag { static void *ptr() { return (void *)k_drag<P>; } };
@@ -228,6 +275,9 @@ long long region_cells(int nx, int ny, int region) {
 
 bool stb_uses_quads(const mb_ctx *c, int level, int region);
 
+// any collision or boundary option on: every block step runs k_block_step_x
+bool options_on(const mb_ctx *c) { return c->opt.coll != MB_COLL_BGK || c->opt.has_force || c->n_alt_walls > 0; }
+
 // Launch parameters of a block-step node.  total counts cells for the
 // one-cell-per-thread kernel and warp tiles for the quad kernel (quads).
 StbParams make_stb(mb_ctx *c, int a0, int a1, uint64_t parity, int macro_all, int write_macros, int region,
@@ -241,6 +291,7 @@ StbParams make_stb(mb_ctx *c, int a0, int a1, uint64_t parity, int macro_all, in
   p.rho0 = c->geo.config.rho0;
   p.u0x = c->geo.config.U0[0];
   p.u0y = c->geo.config.U0[1];
+  p.opt = c->opt;
   long long cell = 0, wt = 0, rt = 0, level_cells = 0;
   for (int a = a0; a < a1; a++) level_cells += region_cells(c->blk[a].nx, c->blk[a].ny, region);
   p.evict_first = c->stream_cells > 0 && level_cells >= c->stream_cells;
@@ -260,6 +311,7 @@ StbParams make_stb(mb_ctx *c, int a0, int a1, uint64_t parity, int macro_all, in
     s.plane = B.plane;
     s.cell0 = cell;
     s.rv_tau = c->geo.Areas[a].rv_tau;
+    s.dt = 1.0 / c->geo.Areas[a].m;
     cell += region_cells(B.nx, B.ny, region);
     // quad kernel: rows of the region in tiles of 128 cells
     s.tiles_x = (B.nx + 127) / 128;
@@ -282,7 +334,7 @@ StbParams make_stb(mb_ctx *c, int a0, int a1, uint64_t parity, int macro_all, in
 
 // the rim is always stepped one cell per thread
 bool stb_uses_quads(const mb_ctx *c, int level, int region) {
-  return region != STB_RIM && c->stb_variant[level] == 1 && c->use_graph != 3;
+  return region != STB_RIM && c->stb_variant[level] == 1 && c->use_graph != 3 && !options_on(c);
 }
 
 bool background_capped(const mb_ctx *c, bool background) { return background && c->bulk_ctas_per_sm > 0; }
@@ -302,6 +354,11 @@ bool rows_fit(const mb_ctx *c, const StbParams &p) {
 // capped
 void stb_launch_shape(const mb_ctx *c, int level, int region, bool background, const StbParams &p, void **func,
                       dim3 *grid) {
+  if (options_on(c)) {
+    *func = kfunc<KStbX>(c->prec);
+    *grid = dim3((unsigned)std::max<long long>((p.total + 255) / 256, 0));
+    return;
+  }
   if (stb_uses_quads(c, level, region)) {
     *func = kfunc<KStbQ>(c->prec);
     *grid = dim3((unsigned)((p.total + 7) / 8));  // 8 warp tiles per CTA
@@ -689,6 +746,7 @@ CompiledPlan *get_plan(mb_ctx *c, int n, bool final_macros, int *err) {
 int exec_plan(mb_ctx *c, CompiledPlan *cp, cudaStream_t s) {
   int e;
   if (c->use_graph == 3) {
+    if (options_on(c)) return MB_ERR_UNSUPPORTED;  // the executor runs the BGK/SBB step only
     if (!cp->prg_built && (e = build_program(c, *cp))) return e;
     if ((e = launch_program(c, *cp, s))) return e;
     c->state = cp->end;
@@ -878,30 +936,9 @@ extern "C" int mb_create(const mb_geometry *geo, int precision, mb_ctx **out) {
   // drag links (fdrag_store, force_block.h:78-127): i-outer, j-inner, k
   c->drag_area = cfg.drag_area < 0 ? c->nblk - 1 : cfg.drag_area;
   if (c->drag_area >= c->nblk) return MB_ERR_INVALID;
-  {
-    const int a = c->drag_area;
-    const BlockLayout &b = c->bl[a];
-    const auto &fl = c->hflags[a];
-    std::vector<DragLink> links;
-    for (int i = 0; i < b.nx; i++)
-      for (int j = 0; j < b.ny; j++) {
-        const long long cs = (long long)j * b.pitch + i;
-        if ((fl[cs] & 3) != CT_SOLID) continue;
-        for (int k = 0; k < 9; k++) {
-          const int id = i - ex(k), jd = j - ey(k);
-          if (id < 0 || id > b.nx - 1 || jd < 0 || jd > b.ny - 1) continue;
-          const long long cf = (long long)jd * b.pitch + id;
-          if ((fl[cf] & 3) != CT_FLUID) continue;
-          links.push_back({(int32_t)cs, (int32_t)cf, k, (fl[cf] & CF_EDGE) ? 1 : 0});
-        }
-      }
-    c->n_drag = (int)links.size();
-    if ((e = dalloc(c.get(), &c->d_links, links.size()))) return e;
-    if (!links.empty())
-      MB_CUDA(cudaMemcpy(c->d_links, links.data(), links.size() * sizeof(DragLink), cudaMemcpyHostToDevice));
-    if ((e = dalloc(c.get(), &c->d_drag_out, 2))) return e;
-    MB_CUDA(cudaMallocHost(&c->h_drag_out, 2 * sizeof(double)));
-  }
+  if ((e = upload_drag_links(c.get()))) return e;
+  if ((e = dalloc(c.get(), &c->d_drag_out, 2))) return e;
+  MB_CUDA(cudaMallocHost(&c->h_drag_out, 2 * sizeof(double)));
 
   // L2 tables and scratch
   {
@@ -1038,6 +1075,56 @@ extern "C" int mb_set_stb_variant(mb_ctx *c, int level, int variant) {
   if (!c || level < 0 || level >= c->geo.layout.LEVEL || variant < 0 || variant > 3) return MB_ERR_INVALID;
   cudaDeviceSynchronize();
   c->stb_variant[level] = variant;
+  c->plans.clear();
+  return MB_OK;
+}
+
+extern "C" int mb_set_collision(mb_ctx *c, int kind, double s_e, double s_eps, double s_q) {
+  if (!c || (kind != MB_COLL_BGK && kind != MB_COLL_MRT) || !std::isfinite(s_e) || !std::isfinite(s_eps) ||
+      !std::isfinite(s_q) || s_e >= 2.0 || s_eps >= 2.0 || s_q >= 2.0)
+    return MB_ERR_INVALID;
+  cudaDeviceSynchronize();
+  c->opt.coll = kind;
+  c->opt.mrt_s[0] = s_e;
+  c->opt.mrt_s[1] = s_eps;
+  c->opt.mrt_s[2] = s_q;
+  c->plans.clear();
+  return MB_OK;
+}
+
+extern "C" int mb_set_body_force(mb_ctx *c, double fx, double fy) {
+  if (!c || !std::isfinite(fx) || !std::isfinite(fy)) return MB_ERR_INVALID;
+  cudaDeviceSynchronize();
+  c->opt.force[0] = fx;
+  c->opt.force[1] = fy;
+  c->opt.has_force = fx != 0.0 || fy != 0.0;
+  c->plans.clear();
+  return MB_OK;
+}
+
+extern "C" int mb_set_cell_types(mb_ctx *c, int a, const int *types) {
+  if (!c || a < 0 || a >= c->nblk || !types) return MB_ERR_INVALID;
+  const BlockLayout &b = c->bl[a];
+  auto movable = [](int t) { return t == MB_FLUID || t == MB_SOLID_SBB || t == MB_SOLID_SLIP || t == MB_SOLID_HBB; };
+  std::vector<uint8_t> fl = c->hflags[a];
+  long long alt_before = 0, alt_after = 0;
+  for (int j = 0; j < b.ny; j++)
+    for (int i = 0; i < b.nx; i++) {
+      uint8_t &f = fl[(size_t)j * b.pitch + i];
+      const int was = flag_code(f), t = types[(size_t)j * b.nx + i];
+      if (movable(was) != movable(t) || (!movable(was) && t != was)) return MB_ERR_INVALID;
+      if (f & (CF_HBB | CF_SLIP)) alt_before++;
+      if (!movable(t)) continue;
+      f = uint8_t((f & ~(3 | CF_HBB | CF_SLIP)) | (t == MB_FLUID ? CT_FLUID : CT_SOLID) |
+                  (t == MB_SOLID_HBB ? CF_HBB : 0) | (t == MB_SOLID_SLIP ? CF_SLIP : 0));
+      if (f & (CF_HBB | CF_SLIP)) alt_after++;
+    }
+  cudaDeviceSynchronize();
+  c->hflags[a] = fl;
+  MB_CUDA(cudaMemcpy((void *)c->blk[a].flags, fl.data(), fl.size(), cudaMemcpyHostToDevice));
+  c->n_alt_walls += alt_after - alt_before;
+  int e;
+  if (a == c->drag_area && (e = upload_drag_links(c))) return e;
   c->plans.clear();
   return MB_OK;
 }
@@ -1539,8 +1626,7 @@ extern "C" int mb_copy_fields(mb_ctx *c, int a, double *rho, double *ux, double 
     const auto &fl = c->hflags[a];
     for (int j = 0; j < B.ny; j++)
       for (int i = 0; i < B.nx; i++) {
-        const int t = fl[(size_t)j * B.pitch + i] & 3;
-        solid[(size_t)j * B.nx + i] = t == CT_FLUID ? MB_FLUID : (t == CT_SOLID ? MB_SOLID_SBB : MB_C_BOUNDARY);
+        solid[(size_t)j * B.nx + i] = flag_code(fl[(size_t)j * B.pitch + i]);
       }
   }
   MB_CUDA(cudaGetLastError());
@@ -1931,6 +2017,7 @@ extern "C" int mb_batch_create(mb_ctx *const *cases, int n, mb_batch **out) {
     mb_ctx *c = cases[q];
     if (!c) return MB_ERR_INVALID;
     if (!c->inited) return MB_ERR_STATE;
+    if (options_on(c)) return MB_ERR_UNSUPPORTED;  // batched kernels run the BGK/SBB step only
     if (q > 0 && (c->prec != cases[0]->prec || c->period != cases[0]->period ||
                   c->geo.layout.LEVEL != cases[0]->geo.layout.LEVEL || c->device != cases[0]->device))
       return MB_ERR_UNSUPPORTED;
@@ -1972,6 +2059,8 @@ extern "C" int mb_batch_destroy(mb_batch *b) {
 extern "C" int mb_batch_step(mb_batch *b, int n, mb_stream stream) {
   if (!b || n < 0) return MB_ERR_INVALID;
   if (!batch_in_step(b)) return MB_ERR_STATE;
+  for (mb_ctx *c : b->cases)
+    if (options_on(c)) return MB_ERR_UNSUPPORTED;
   cudaStream_t s = (cudaStream_t)stream;
   b->kernels_last_call = 0;
   int remaining = n;

@@ -18,6 +18,8 @@ enum : uint8_t {
   CT_PAD = 3,   // row padding beyond nx
   CF_EDGE = 4,  // i==0 || j==0 || i==nx-1 || j==ny-1
   CF_MACRO = 8, // rho/ux/uy of this FLUID cell are read by an interface op
+  CF_HBB = 16,  // CT_SOLID cell that is a half-way bounce-back wall (MB_SOLID_HBB)
+  CF_SLIP = 32, // CT_SOLID cell that is an on-node free-slip wall (MB_SOLID_SLIP)
 };
 
 bool obstacle_contains(const mb_config &c, double x, double y);

@@ -27,7 +27,8 @@ PREC_F64, PREC_F32, PREC_F16S, PREC_F32U = 0, 1, 2, 3
 PRECISIONS = {"f64": PREC_F64, "f32": PREC_F32, "f16s": PREC_F16S, "f32u": PREC_F32U}
 FLUID, SOLID_SBB, C_BOUNDARY = 0, 1, 9
 OBST_CIRCLE, OBST_ELLIPSE = 0, 1
-MB_FLUID, MB_SOLID_SBB, MB_C_BOUNDARY = 0, 1, 9  # cell kinds of mb_copy_fields' solid array
+MB_FLUID, MB_SOLID_SBB, MB_SOLID_SLIP, MB_SOLID_HBB, MB_C_BOUNDARY = 0, 1, 2, 3, 9
+MB_COLL_BGK, MB_COLL_MRT = 0, 1  # cell kinds of mb_copy_fields' solid array
 
 
 class P4(C.Structure):
@@ -140,6 +141,9 @@ SIGNATURES = {
     "mb_set_split_cells": ([_vp, C.c_longlong], C.c_int),
     "mb_set_stb_variant": ([_vp, C.c_int, C.c_int], C.c_int),
     "mb_set_bulk_occupancy": ([_vp, C.c_int], C.c_int),
+    "mb_set_collision": ([_vp, C.c_int, C.c_double, C.c_double, C.c_double], C.c_int),
+    "mb_set_body_force": ([_vp, C.c_double, C.c_double], C.c_int),
+    "mb_set_cell_types": ([_vp, C.c_int, _pi], C.c_int),
     "mb_set_stream_cells": ([_vp, C.c_longlong, C.c_int], C.c_int),
     "mb_set_interface_shape": ([_vp, C.c_int, C.c_int], C.c_int),
     "mb_set_split_levels": ([_vp, C.c_uint], C.c_int),
@@ -414,6 +418,23 @@ class MultiBlockLBM:
     def set_bulk_occupancy(self, ctas_per_sm):
         """Cap interior block-step grids at ctas_per_sm CTAs per SM (0: uncapped)."""
         _check(self.lib.mb_set_bulk_occupancy(self.h, int(ctas_per_sm)), "mb_set_bulk_occupancy")
+
+    def set_collision(self, kind, s_e=0.0, s_eps=0.0, s_q=0.0):
+        """MB_COLL_BGK, or MB_COLL_MRT with rates s_e, s_eps, s_q (<= 0: the block's 1/tau)."""
+        _check(self.lib.mb_set_collision(self.h, int(kind), float(s_e), float(s_eps), float(s_q)), "mb_set_collision")
+
+    def set_body_force(self, fx, fy):
+        """Uniform body force (forcex, forcey of every cell, coarse lattice units)."""
+        _check(self.lib.mb_set_body_force(self.h, float(fx), float(fy)), "mb_set_body_force")
+
+    def set_cell_types(self, area, types):
+        """Cell types of one block, an (ny, nx) array of MB_FLUID / MB_SOLID_SBB /
+        MB_SOLID_SLIP / MB_SOLID_HBB codes (C_BOUNDARY cells unchanged)."""
+        t = np.ascontiguousarray(types, dtype=np.int32)
+        A = self.geo.Areas[area]
+        if t.size != A.nx * A.ny:
+            raise ValueError("types must have nx*ny entries")
+        _check(self.lib.mb_set_cell_types(self.h, int(area), t.ctypes.data_as(_pi)), "mb_set_cell_types")
 
     def set_program_timeout(self, seconds):
         """Executor (graph="program"): give up after this long without ready work."""

@@ -31,6 +31,16 @@
 static const double Wt[Q] = {4. / 9, 1. / 9, 1. / 9, 1. / 9, 1. / 9, 1. / 36, 1. / 36, 1. / 36, 1. / 36};
 static const int Ev[2 * Q] = {0, 1, 0, -1, 0, 1, -1, -1, 1, 0, 0, 1, 0, -1, 1, 1, -1, -1};
 static const int Opp[Q] = {0, 3, 4, 1, 2, 7, 8, 5, 6};
+static const int Slip[Q] = {0, 1, 4, 3, 2, 8, 7, 6, 5}; /* slip_gpu, lbm/lbm.h:51 */
+/* MRT moment matrix M_gpu (lbm/lbm.h:53-63); its rows are orthogonal with
+ * squared norms Mn, so M^-1 = M^T diag(1/Mn) (the exact form of InvM_gpu,
+ * lbm/lbm.h:64-75) */
+static const int Mm[Q][Q] = {{1, 1, 1, 1, 1, 1, 1, 1, 1},   {-4, -1, -1, -1, -1, 2, 2, 2, 2},
+                             {4, -2, -2, -2, -2, 1, 1, 1, 1}, {0, 1, 0, -1, 0, 1, -1, -1, 1},
+                             {0, -2, 0, 2, 0, 1, -1, -1, 1},  {0, 0, 1, 0, -1, 1, 1, -1, -1},
+                             {0, 0, -2, 0, 2, 1, 1, -1, -1},  {0, 1, -1, 1, -1, 0, 0, 0, 0},
+                             {0, 0, 0, 0, 0, 1, -1, 1, -1}};
+static const double Mn[Q] = {9, 36, 36, 6, 12, 6, 12, 4, 4};
 
 typedef struct {
   int *solid;
@@ -62,6 +72,12 @@ struct orc_sim {
   int n_drag;
   int *drag; /* 3 * n_drag: i, j, k */
   double U0_2;
+  /* collision options: 0 BGK, 1 MRT with rates s_e, s_eps, s_q (<= 0: the
+   * block's 1/tau); shear rates are always the block's 1/tau */
+  int coll;
+  double s_e, s_eps, s_q;
+  double fx, fy;                /* uniform body force on every cell's forcex/forcey */
+  int *types[MB_MAX_AREA];      /* cell-type overrides, applied after init_General */
 };
 
 void orc_set_threads(int n) {
@@ -254,6 +270,7 @@ void orc_destroy(orc_sim *s) {
     for (int k = 0; k < Q; k++) free(sp->F[k]);
   }
   free(s->drag);
+  for (int a = 0; a < MB_MAX_AREA; a++) free(s->types[a]);
   free(s);
 }
 
@@ -353,6 +370,8 @@ static void init_tri_a(orc_sim *s, int b) {
  * (lbm/force_block.h:2-127).  Enumeration is i-outer, j-inner, k.
  * ------------------------------------------------------------------------- */
 static void drag_setup(orc_sim *s) {
+  free(s->drag);
+  s->drag = NULL;
   const int a = s->drag_area;
   const mb_area *ar = &s->geo.Areas[a];
   const int *solid = s->pp[a].solid;
@@ -362,7 +381,7 @@ static void drag_setup(orc_sim *s) {
     for (int i = 0; i < ar->nx; i++)
       for (int j = 0; j < ar->ny; j++) {
         int ixy = i + j * ar->nx;
-        if (solid[ixy] != MB_SOLID_SBB) continue;
+        if (solid[ixy] != MB_SOLID_SBB && solid[ixy] != MB_SOLID_HBB) continue;
         for (int k = 0; k < Q; k++) {
           int id = i - Ev[k], jd = j - Ev[k + Q];
           if (id < 0 || id > ar->nx - 1 || jd < 0 || jd > ar->ny - 1) continue;
@@ -376,9 +395,78 @@ static void drag_setup(orc_sim *s) {
   }
 }
 
+/* ---------------------------------------------------------------------------
+ * Collision and boundary options the reference declares but never uses:
+ * MRT (M_gpu, InvM_gpu, lbm/lbm.h:53-75; Meq, lbm/assit_func.h:10-22), the
+ * body-force term of stb3 (evolution_block.h:97-108, forcex/forcey set to one
+ * value everywhere), free slip (slip_gpu, lbm/lbm.h:51) and half-way
+ * bounce-back (SOLID_HBB, lbm/lbm.h:28).  The reference gives no kernel for
+ * the last three; their semantics here:
+ *  - SOLID_SLIP (code 2, unused by the reference): an on-node wall like
+ *    SOLID_SBB that returns F_k = f_slip(k) instead of f_opp(k);
+ *  - SOLID_HBB: a FLUID cell whose upstream neighbour x - e_k is an HBB cell
+ *    takes f_k(x) = F_opp(k)(x), its own post-collision value of the previous
+ *    step; HBB cells are pulled (for the drag sum) but never collide;
+ *  - MRT: F = f - M^-1 S (M f - meq) + dt Force_k, S = diag(0, s_e, s_eps, 0,
+ *    s_q, 0, s_q, 1/tau, 1/tau), meq = Meq with A = 1, B = -3.
+ * ------------------------------------------------------------------------- */
+int orc_set_collision(orc_sim *s, int kind, double s_e, double s_eps, double s_q) {
+  if (kind != MB_COLL_BGK && kind != MB_COLL_MRT) return MB_ERR_INVALID;
+  s->coll = kind;
+  s->s_e = s_e;
+  s->s_eps = s_eps;
+  s->s_q = s_q;
+  return MB_OK;
+}
+
+void orc_set_body_force(orc_sim *s, double fx, double fy) {
+  s->fx = fx;
+  s->fy = fy;
+  for (int a = 0; a < s->geo.layout.number_area; a++) {
+    const size_t N = (size_t)s->geo.Areas[a].nx * s->geo.Areas[a].ny;
+    for (size_t c = 0; c < N; c++) {
+      s->pp[a].forcex[c] = fx;
+      s->pp[a].forcey[c] = fy;
+    }
+  }
+}
+
+/* Cell types of block a (nx*ny, ixy = i + j*nx): FLUID, SOLID_SBB,
+ * SOLID_SLIP or SOLID_HBB where init_General put FLUID or SOLID_SBB;
+ * C_BOUNDARY cells must stay C_BOUNDARY. */
+int orc_set_cell_types(orc_sim *s, int a, const int *types) {
+  if (a < 0 || a >= s->geo.layout.number_area) return MB_ERR_INVALID;
+  const size_t N = (size_t)s->geo.Areas[a].nx * s->geo.Areas[a].ny;
+  int *solid = s->pp[a].solid;
+  for (size_t c = 0; c < N; c++) {
+    const int t = types[c], was = solid[c];
+    const int movable = was == MB_FLUID || was == MB_SOLID_SBB || was == MB_SOLID_SLIP || was == MB_SOLID_HBB;
+    if (movable != (t == MB_FLUID || t == MB_SOLID_SBB || t == MB_SOLID_SLIP || t == MB_SOLID_HBB)) return MB_ERR_INVALID;
+    if (!movable && t != was) return MB_ERR_INVALID;
+  }
+  if (!s->types[a]) s->types[a] = (int *)malloc(N * sizeof(int));
+  memcpy(s->types[a], types, N * sizeof(int));
+  memcpy(solid, types, N * sizeof(int));
+  if (a == s->drag_area) drag_setup(s);
+  return MB_OK;
+}
+
+static void apply_options(orc_sim *s, int a) {
+  const size_t N = (size_t)s->geo.Areas[a].nx * s->geo.Areas[a].ny;
+  o_d2q9 *pp = &s->pp[a];
+  if (s->types[a]) memcpy(pp->solid, s->types[a], N * sizeof(int));
+  for (size_t c = 0; c < N; c++) {
+    pp->forcex[c] = s->fx;
+    pp->forcey[c] = s->fy;
+  }
+}
+
 int orc_init(orc_sim *s) {
   const mb_layout *L = &s->geo.layout;
-  for (int a = 0; a < L->number_area; a++) init_general(s, a);
+  for (int a = 0; a < L->number_area; a++) {
+    init_general(s, a);
+    apply_options(s, a);
+  }
   drag_setup(s);
   for (int b = 0; b < L->number_line; b++) { init_fstore(s, b); init_tri_a(s, b); }
   return MB_OK;
@@ -397,11 +485,15 @@ void orc_block_step(orc_sim *s, int a) {
   for (int j = 0; j < ny; j++)
     for (int i = 0; i < nx; i++) {
       int ixy = i + j * nx;
-      if (pp->solid[ixy] == MB_FLUID || pp->solid[ixy] == MB_SOLID_SBB) {
+      const int t = pp->solid[ixy];
+      if (t == MB_FLUID || t == MB_SOLID_SBB || t == MB_SOLID_SLIP || t == MB_SOLID_HBB) {
         for (int k = 0; k < Q; k++) {
           int id = i - Ev[k], jd = j - Ev[k + Q];
           if (id < 0 || id > nx - 1 || jd < 0 || jd > ny - 1) continue;
-          pp->f[k][ixy] = pp->F[k][id + jd * nx];
+          if (t == MB_FLUID && pp->solid[id + jd * nx] == MB_SOLID_HBB)
+            pp->f[k][ixy] = pp->F[Opp[k]][ixy]; /* half-way bounce-back */
+          else
+            pp->f[k][ixy] = pp->F[k][id + jd * nx];
         }
       }
     }
@@ -436,14 +528,46 @@ void orc_block_step(orc_sim *s, int a) {
       if (pp->solid[ixy] == MB_FLUID) {
         double rh = pp->rho[ixy], ux = pp->ux[ixy], uy = pp->uy[ixy];
         double fx = pp->forcex[ixy], fy = pp->forcey[ixy];
+        double dm[Q]; /* MRT: M^-1 S (M f - meq) as S_i (m_i - meq_i) / Mn_i */
+        if (s->coll == MB_COLL_MRT) {
+          double m[Q], meq[Q], sr[Q];
+          for (int q = 0; q < Q; q++) {
+            m[q] = 0.0;
+            for (int k = 0; k < Q; k++) m[q] += Mm[q][k] * ft[k];
+          }
+          const double uv = ux * ux + uy * uy; /* Meq, assit_func.h:10-22, A = 1, B = -3 */
+          meq[0] = rh;
+          meq[1] = rh * (-2.0 + 3.0 * uv);
+          meq[2] = rh * (1.0 - 3.0 * uv);
+          meq[3] = rh * ux;
+          meq[4] = -meq[3];
+          meq[5] = rh * uy;
+          meq[6] = -meq[5];
+          meq[7] = rh * (ux * ux - uy * uy);
+          meq[8] = rh * (ux * uy);
+          sr[0] = 0.0; sr[3] = 0.0; sr[5] = 0.0;
+          sr[1] = s->s_e > 0 ? s->s_e : area.rv_tau;
+          sr[2] = s->s_eps > 0 ? s->s_eps : area.rv_tau;
+          sr[4] = sr[6] = s->s_q > 0 ? s->s_q : area.rv_tau;
+          sr[7] = sr[8] = area.rv_tau;
+          for (int q = 0; q < Q; q++) dm[q] = sr[q] * (m[q] - meq[q]) / Mn[q];
+        }
         for (int k = 0; k < Q; k++) {
           double vx = 3.0 * (Ev[k] - ux) + 9.0 * (Ev[k] * ux + Ev[k + Q] * uy) * Ev[k];
           double vy = 3.0 * (Ev[k + Q] - uy) + 9.0 * (Ev[k] * ux + Ev[k + Q] * uy) * Ev[k + Q];
           double Fk = (1.0 - 0.5 * area.rv_tau) * Wt[k] * (vx * fx + vy * fy);
-          pp->F[k][ixy] = ft[k] - (ft[k] - orc_feq(k, rh, ux, uy)) * area.rv_tau + dt * Fk;
+          if (s->coll == MB_COLL_MRT) {
+            double r = 0.0;
+            for (int q = 0; q < Q; q++) r += Mm[q][k] * dm[q];
+            pp->F[k][ixy] = ft[k] - r + dt * Fk;
+          } else {
+            pp->F[k][ixy] = ft[k] - (ft[k] - orc_feq(k, rh, ux, uy)) * area.rv_tau + dt * Fk;
+          }
         }
       } else if (pp->solid[ixy] == MB_SOLID_SBB) {
         for (int k = 0; k < Q; k++) pp->F[k][ixy] = ft[Opp[k]];
+      } else if (pp->solid[ixy] == MB_SOLID_SLIP) {
+        for (int k = 0; k < Q; k++) pp->F[k][ixy] = ft[Slip[k]];
       }
     }
 }

@@ -54,6 +54,12 @@ void orc_gtsv(int n, int nrhs, const double *l, const double *m, const double *u
 double orc_spline3_s(double xx, double x_1, double h, double fi_1, double fi, double mi_1, double mi);
 double orc_feq(int k, double rh, double ux, double uy);
 
+/* options the reference declares but never uses (MRT, body force, free slip,
+ * half-way bounce-back); semantics at their definitions in oracle.c */
+int orc_set_collision(orc_sim *s, int kind, double s_e, double s_eps, double s_q);
+void orc_set_body_force(orc_sim *s, double fx, double fy);
+int orc_set_cell_types(orc_sim *s, int area, const int *types);
+
 /* field access (FP64, ixy = i + j*nx; F and f are 9*nx*ny, plane-major) */
 void orc_get_fields(orc_sim *s, int area, double *rho, double *ux, double *uy, double *F,
                     double *f, int *solid);

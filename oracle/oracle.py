@@ -48,6 +48,9 @@ _SIG = {
     "orc_get_slots": ([_vp, C.c_int, _pd], None),
     "orc_get_markers": ([_vp, C.c_int, _pi], None),
     "orc_write_tecplot": ([_vp, C.c_char_p], C.c_int),
+    "orc_set_collision": ([_vp, C.c_int, C.c_double, C.c_double, C.c_double], C.c_int),
+    "orc_set_body_force": ([_vp, C.c_double, C.c_double], None),
+    "orc_set_cell_types": ([_vp, C.c_int, _pi], C.c_int),
 }
 _lib = None
 
@@ -124,6 +127,20 @@ class Oracle:
         out = np.zeros((max(n, 1), 3), dtype=np.int32)
         self.lib.orc_drag_links(self.s, out.ctypes.data_as(_pi))
         return out[:n]
+
+    def set_collision(self, kind, s_e=0.0, s_eps=0.0, s_q=0.0):
+        rc = self.lib.orc_set_collision(self.s, int(kind), float(s_e), float(s_eps), float(s_q))
+        if rc:
+            raise ValueError(f"orc_set_collision failed ({rc})")
+
+    def set_body_force(self, fx, fy):
+        self.lib.orc_set_body_force(self.s, float(fx), float(fy))
+
+    def set_cell_types(self, a, types):
+        t = np.ascontiguousarray(types, dtype=np.int32)
+        rc = self.lib.orc_set_cell_types(self.s, int(a), t.ctypes.data_as(_pi))
+        if rc:
+            raise ValueError(f"orc_set_cell_types failed ({rc})")
 
     def block_step(self, a):
         self.lib.orc_block_step(self.s, a)
