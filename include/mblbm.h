@@ -220,6 +220,13 @@ int mb_set_split_cells(mb_ctx *ctx, long long cells);
  * rows touch one cache sector per value, so small units spread a node over
  * many SMs' load/store units.  Results are identical. */
 int mb_set_interface_shape(mb_ctx *ctx, int rec_points, int spline_segments);
+/* Minimum dynamic shared memory (KB, at most 200) per CTA of the spline and
+ * the record kernels, which caps how many of their CTAs share one SM: a
+ * latency-bound launch that starts while a block step still holds most SMs
+ * then spreads over the SMs that free up instead of piling onto the first
+ * ones.  Defaults 96 (spline: at most 2 CTAs per SM) and 0.  Results are
+ * identical. */
+int mb_set_cta_spread(mb_ctx *ctx, int spline_kb, int records_kb);
 /* Splits exactly the levels whose bit is set in level_mask (bit l = level
  * l) into interior and rim nodes, overriding mb_set_split_cells; 0 returns
  * to the cell threshold.  Results are identical. */
@@ -235,13 +242,19 @@ int mb_set_stream_cells(mb_ctx *ctx, long long cells, int bulk);
  * 1 = four cells per thread with vector loads, 2 = two cells per thread with
  * the loads of both in flight together, 3 = cell ranges: a CTA steps 256
  * consecutive cells of one block with 32-bit offsets (whole levels and
- * interiors; rims use 0).  Default 0, and 3 for level 0 in MB_PREC_F16S.
- * Results are identical. */
+ * interiors; rims use 0), 4 = cell pairs: a thread steps cells i, i+1 with
+ * shared addresses and vector accesses, 256 pairs per CTA (same coverage as 3).
+ * Default 0, and 3 for level 0 in MB_PREC_F16S.  Results are identical. */
 int mb_set_stb_variant(mb_ctx *ctx, int level, int variant);
 /* Caps the grid of interior (bulk) block-step launches at ctas_per_sm CTAs of
  * 256 threads per SM (0 = uncapped), leaving CTA slots on every SM for the
  * fine-level kernels that run beside them. */
 int mb_set_bulk_occupancy(mb_ctx *ctx, int ctas_per_sm);
+/* Kernel fusions of the plan (bit mask; default 1).  Bit 0: the same-level
+ * copies (c_c_boundary_transfer, multi/FH/assit_multi.h:2-46) of a level run
+ * inside its block-step launch: each target cell computes its source's new
+ * values itself.  Results are identical. */
+int mb_set_fusion(mb_ctx *ctx, int flags);
 
 /* ---- collision and boundary options ----------------------------------------
  * The reference declares these but never uses them: MRT (M_gpu, InvM_gpu,
@@ -343,8 +356,10 @@ int mb_error_L2_noalloc(const mb_l2_segment *segs, int nseg, double *d_out, mb_s
 /* Number of kernels launched by the last mb_step call, and in one coarse step. */
 int mb_stats(mb_ctx *ctx, long long *kernels_last_step_call, long long *kernels_per_coarse_step,
              long long *cell_updates_per_coarse_step);
-/* Times the fused block-step kernel of one level alone (n launches, CUDA events
- * on the given stream); returns mean ms per launch and bytes moved per launch. */
+/* Times the fused block-step kernel of one level alone: n launches captured as
+ * one CUDA graph, replayed once to warm up and once between CUDA events on a
+ * private stream (after the given stream drains); returns mean ms per launch
+ * and algorithmic bytes per launch. */
 int mb_time_block_step(mb_ctx *ctx, int level, int n, mb_stream stream, double *ms_per_launch,
                        double *alg_bytes_per_launch, long long *cells_per_launch);
 

@@ -86,6 +86,7 @@ __device__ __forceinline__ R feq(int k, R rh, R uxx, R uyy) {
 // into one pull collide-stream pass from buffer Fin into Fout.
 // ----------------------------------------------------------------------------
 constexpr int STB_MAX_BLOCKS = 16;
+constexpr uint8_t FL_CCPULL = 64;  // C_BOUNDARY target of a same-level copy run beside the block step
 
 struct StbBlk {
   const void *Fin;
@@ -103,8 +104,21 @@ struct StbBlk {
   int cta0, rcells;   // first CTA; cells of the region
   int rw, rcol0;      // region width and first column (first row: row0)
   float rinv_w;       // 1 / rw, for the row of a cell index
+  // pair kernel: pairs of cells (i, i + 1), i - rcol0 even; ppr pairs per
+  // row, CTAs pcta0.. of 256 consecutive pairs
+  int pcta0, npairs;
+  int ppr;
+  float pinv;         // 1 / ppr
   int pad2_;
   double dt;          // 1 / m: time step of the block in coarse units (body-force term)
+};
+
+// One same-level copy run beside the block step (k_cc_pull).
+struct CcEntry {
+  int tblk, sblk;  // global block ids
+  int tcell;       // target cell, j * pitch + i
+  int si, sj;      // source cell
+  int pad_;
 };
 
 // Collision and boundary options (the options kernel k_block_step_x only).
@@ -121,8 +135,13 @@ struct StbParams {
   int write_macros;  // 0: never write rho/u (kernel timing only)
   int region;        // 0: all cells, 1: distance >= 2 from the block edge, 2: distance <= 1
   int evict_first;   // stream the blocks' buffers with evict-first cache hints
+  int ccpull;        // skip cells flagged FL_CCPULL: k_cc_pull writes them
+  int a0;            // global index of b[0]
+  const CcEntry *cc_list;  // k_cc_pull: the copies of the launch
+  int cc_n, pad_cc;
   long long total;   // cells in the launch (per-cell kernel) or warp tiles (quad kernel)
   long long rctas;   // CTAs of a range-kernel launch
+  long long pctas;   // CTAs of a pair-kernel launch
   double feqc[9];    // feq(rho0, U0): block-edge FLUID cells and stale f of edge solids
   double rho0, u0x, u0y;
   StbOptions opt;
@@ -207,6 +226,77 @@ __device__ __forceinline__ void stb_pull(const StbBlk &B, int i, int j, typename
   }
 }
 
+// The block step of cell (i, j) of block B (stb_finish below) with its new
+// values stored at cell cd of block D: a same-level copy target's values.
+// cc: the values are a c_c_boundary_transfer copy (multi/FH/assit_multi.h:38-44),
+// which also carries rho/u whatever the source's type.
+template <int P, bool EF>
+__device__ __forceinline__ void stb_finish_at(const StbParams &p, const StbBlk &B, int i, int j,
+                                              const typename Prec<P>::S *raw, uint8_t fl, const StbBlk &D,
+                                              long long cd, bool cc) {
+  using R = typename Prec<P>::R;
+  using S = typename Prec<P>::S;
+  const long long c = (long long)j * B.pitch + i;
+  S *Fout = (S *)D.Fout;
+  const long long plane = D.plane;
+  const int type = fl & 3;
+  const bool wm = cc || (p.write_macros && (p.macro_all || (fl & 8)));
+
+  if (type == 0) {  // FLUID
+    if (fl & 4) {   // block edge: equilibrium at rho0, U0 (stb2 :47-57), collide keeps it
+#pragma unroll
+      for (int k = 0; k < 9; k++) {
+        if constexpr (Prec<P>::shifted) st_ef<EF>(Fout + k * plane + cd, from_r<S>((R)p.feqc[k] - wk<P>(k)));
+        else st_ef<EF>(Fout + k * plane + cd, (S)p.feqc[k]);
+      }
+      if (wm) {
+        st_ef<EF>((R *)D.rho + cd, (R)p.rho0);
+        st_ef<EF>((R *)D.ux + cd, (R)p.u0x);
+        st_ef<EF>((R *)D.uy + cd, (R)p.u0y);
+      }
+      return;
+    }
+    R f[9];  // interior FLUID cell: every pull is inside the block
+#pragma unroll
+    for (int k = 0; k < 9; k++) f[k] = to_r(raw[k]);
+    R out[9], m[3];
+    stb_collide<P>(f, (R)B.rv_tau, out, m);
+    if (wm) {
+      st_ef<EF>((R *)D.rho + cd, m[0]);
+      st_ef<EF>((R *)D.ux + cd, m[1]);
+      st_ef<EF>((R *)D.uy + cd, m[2]);
+    }
+#pragma unroll
+    for (int k = 0; k < 9; k++) st_ef<EF>(Fout + k * plane + cd, from_r<S>(out[k]));
+    return;
+  }
+  if (cc) {  // rho/u of a solid or C_BOUNDARY source: its current values
+    st_ef<EF>((R *)D.rho + cd, ((const R *)B.rho)[c]);
+    st_ef<EF>((R *)D.ux + cd, ((const R *)B.ux)[c]);
+    st_ef<EF>((R *)D.uy + cd, ((const R *)B.uy)[c]);
+  }
+  if (type == 1) {  // SOLID_SBB: pull (stale f = feq(rho0,U0) off-block), then on-node bounce-back
+    S fr[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+      const int id = i - ex(k), jd = j - ey(k);
+      if (id >= 0 && id < B.nx && jd >= 0 && jd < B.ny)
+        fr[k] = raw[k];
+      else if constexpr (Prec<P>::shifted)
+        fr[k] = from_r<S>((float)(p.feqc[k] - wd(k)));
+      else
+        fr[k] = (S)p.feqc[k];
+    }
+#pragma unroll
+    for (int k = 0; k < 9; k++) st_ef<EF>(Fout + k * plane + cd, fr[opp(k)]);  // w_k = w_opp(k): raw move is exact
+    return;
+  }
+  // C_BOUNDARY and row padding: untouched by the step, carried to the new buffer
+  const S *Fin = (const S *)B.Fin;
+#pragma unroll
+  for (int k = 0; k < 9; k++) st_ef<EF>(Fout + k * plane + cd, ld_ef<EF>(Fin + k * B.plane + c));
+}
+
 // One cell of the block step, evolution_area_stb1/2/3
 // (multi/FH/evolution_block.h:3-119), from its pulled values and flag byte.
 template <int P, bool EF>
@@ -264,10 +354,32 @@ __device__ __forceinline__ void stb_finish(const StbParams &p, const StbBlk &B, 
     for (int k = 0; k < 9; k++) st_ef<EF>(Fout + k * plane + c, fr[opp(k)]);  // w_k = w_opp(k): raw move is exact
     return;
   }
-  // C_BOUNDARY and row padding: untouched by the step, carried to the new buffer
+  // C_BOUNDARY and row padding: untouched by the step, carried to the new
+  // buffer; a same-level copy target (FL_CCPULL) is k_cc_pull's
+  if (p.ccpull && (fl & FL_CCPULL)) return;
   const S *Fin = (const S *)B.Fin;
 #pragma unroll
   for (int k = 0; k < 9; k++) st_ef<EF>(Fout + k * plane + c, ld_ef<EF>(Fin + k * plane + c));
+}
+
+
+// Same-level copies (c_c_boundary_transfer, multi/FH/assit_multi.h:2-46) of a
+// level whose sources are FLUID cells, run beside the level's block step
+// instead of after it: each thread computes what its source cell gets in this
+// step from the source block's input buffer (the block step's own code) and
+// stores it, rho/u included, at the target.  The block step skips the
+// targets (FL_CCPULL).  Chains of copies are resolved on the host.
+template <int P>
+__global__ void __launch_bounds__(128) k_cc_pull(const __grid_constant__ StbParams p) {
+  pdl_trigger();
+  pdl_wait();
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= p.cc_n) return;
+  const CcEntry e = p.cc_list[t];
+  const StbBlk &B = p.b[e.sblk - p.a0], &D = p.b[e.tblk - p.a0];
+  typename Prec<P>::S raw[9];
+  stb_pull<P, false>(B, e.si, e.sj, raw);
+  stb_finish_at<P, false>(p, B, e.si, e.sj, raw, B.flags[(long long)e.sj * B.pitch + e.si], D, e.tcell, true);
 }
 
 // Pulled values of a cell at least one cell from the block edge: every
@@ -398,7 +510,7 @@ __global__ void __launch_bounds__(256, CPT == 1 ? (P == MB_PREC_F64 ? 4 : 8) : (
 //    cell takes f_k(x) = F_opp(k)(x), its own value of the previous step; HBB
 //    cells keep their distributions.
 // ----------------------------------------------------------------------------
-constexpr uint8_t FL_HBB = 16, FL_SLIP = 32;
+constexpr uint8_t FL_HBB = 16, FL_SLIP = 32;  // FL_CCPULL = 64 is defined with the block step
 
 // M_gpu entries (lbm/lbm.h:53-63) and squared row norms
 __host__ __device__ constexpr int mrt_m(int q, int k) {
@@ -647,6 +759,98 @@ __global__ void __launch_bounds__(256, P == MB_PREC_F64 ? 4 : 6) k_block_step_r(
   const int i = B.rcol0 + (local - r * B.rw);
   if (p.evict_first) stb_cell_rows<P, true, INTERIOR>(p, B, i, j);
   else stb_cell_rows<P, false, INTERIOR>(p, B, i, j);
+}
+
+// ----------------------------------------------------------------------------
+// The block step on cell pairs: a thread steps cells (i, j) and (i + 1, j),
+// i even, so one address serves both cells of a plane: the three planes with
+// e_x = 0 and all nine stores move both values in one aligned vector access,
+// the six others in two scalar loads at neighbouring addresses.  A CTA owns
+// 256 consecutive pairs (row-major over the region) of one block.  Offsets
+// are 32-bit (the host uses this kernel only when 9 planes of every block fit
+// in 2^31 elements).  Pairs of interior FLUID cells take the short path;
+// every other cell runs the general stb_finish.
+// ----------------------------------------------------------------------------
+template <typename S> struct Vec2;
+template <> struct Vec2<float> { using T = float2; };
+template <> struct Vec2<double> { using T = double2; };
+template <> struct Vec2<__half> { using T = __half2; };
+__device__ __forceinline__ void unpack2(float2 v, float &a, float &b) { a = v.x; b = v.y; }
+__device__ __forceinline__ void unpack2(double2 v, double &a, double &b) { a = v.x; b = v.y; }
+__device__ __forceinline__ void unpack2(__half2 v, __half &a, __half &b) { a = __low2half(v); b = __high2half(v); }
+__device__ __forceinline__ float2 pack2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ double2 pack2(double a, double b) { return make_double2(a, b); }
+__device__ __forceinline__ __half2 pack2(__half a, __half b) { return __halves2half2(a, b); }
+
+template <int P, bool EF, bool INTERIOR>
+__device__ __forceinline__ void stb_pair(const StbParams &p, const StbBlk &B, int i, int j, bool two) {
+  using R = typename Prec<P>::R;
+  using S = typename Prec<P>::S;
+  using V = typename Vec2<S>::T;
+  if (two && (INTERIOR || (i > 0 && i + 1 < B.nx - 1 && j > 0 && j < B.ny - 1))) {
+    const int c = j * B.pitch + i;  // even: pitch and i are even
+    const int plane = (int)B.plane;
+    const S *Fin = (const S *)B.Fin;
+    S a[9], b[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+      const int o = k * plane + c - (ey(k) * B.pitch + ex(k));
+      if (ex(k) == 0) unpack2(ld_ef<EF>((const V *)(Fin + o)), a[k], b[k]);
+      else { a[k] = ld_ef<EF>(Fin + o); b[k] = ld_ef<EF>(Fin + o + 1); }
+    }
+    const unsigned short fl2 = *(const unsigned short *)(B.flags + c);
+    const uint8_t fa = uint8_t(fl2 & 0xff), fb = uint8_t(fl2 >> 8);
+    if (((fa | fb) & 7) == 0) {  // both FLUID away from the block edge
+      R f[9], oa[9], ob[9], ma[3], mb[3];
+#pragma unroll
+      for (int k = 0; k < 9; k++) f[k] = to_r(a[k]);
+      stb_collide<P>(f, (R)B.rv_tau, oa, ma);
+#pragma unroll
+      for (int k = 0; k < 9; k++) f[k] = to_r(b[k]);
+      stb_collide<P>(f, (R)B.rv_tau, ob, mb);
+      if (p.write_macros) {
+        const bool wa = p.macro_all || (fa & 8), wb = p.macro_all || (fb & 8);
+        R *rho = (R *)B.rho + c, *ux = (R *)B.ux + c, *uy = (R *)B.uy + c;
+        if (wa && wb) {
+          using VR = typename Vec2<R>::T;
+          st_ef<EF>((VR *)rho, pack2(ma[0], mb[0]));
+          st_ef<EF>((VR *)ux, pack2(ma[1], mb[1]));
+          st_ef<EF>((VR *)uy, pack2(ma[2], mb[2]));
+        } else {
+          if (wa) { st_ef<EF>(rho, ma[0]); st_ef<EF>(ux, ma[1]); st_ef<EF>(uy, ma[2]); }
+          if (wb) { st_ef<EF>(rho + 1, mb[0]); st_ef<EF>(ux + 1, mb[1]); st_ef<EF>(uy + 1, mb[2]); }
+        }
+      }
+      S *Fout = (S *)B.Fout;
+#pragma unroll
+      for (int k = 0; k < 9; k++) st_ef<EF>((V *)(Fout + (k * plane + c)), pack2(from_r<S>(oa[k]), from_r<S>(ob[k])));
+      return;
+    }
+  }
+  stb_cell_slow<P, EF>(p, B, i, j);
+  if (two) stb_cell_slow<P, EF>(p, B, i + 1, j);
+}
+
+template <int P, bool INTERIOR>
+__global__ void __launch_bounds__(256, P == MB_PREC_F64 ? 2 : 4) k_block_step_p(const __grid_constant__ StbParams p) {
+  pdl_trigger();
+  pdl_wait();
+  const int cta = blockIdx.x;
+  int t = 0;
+#pragma unroll 1
+  while (t + 1 < p.nblk && cta >= p.b[t + 1].pcta0) t++;
+  const StbBlk &B = p.b[t];
+  const int local = (cta - B.pcta0) * 256 + (int)threadIdx.x;
+  if (local >= B.npairs) return;
+  int r = __float2int_rz((float)local * B.pinv);
+  if (r * B.ppr > local) r--;
+  else if ((r + 1) * B.ppr <= local) r++;
+  const int q = local - r * B.ppr;
+  const int j = B.row0 + r;
+  const int i = B.rcol0 + 2 * q;
+  const bool two = 2 * q + 1 < B.rw;
+  if (p.evict_first) stb_pair<P, true, INTERIOR>(p, B, i, j, two);
+  else stb_pair<P, false, INTERIOR>(p, B, i, j, two);
 }
 
 // Four consecutive cells of a row in the stored form, as arithmetic values

@@ -122,6 +122,10 @@ struct mb_ctx {
   // collision and boundary options (k_block_step_x)
   StbOptions opt{};
   long long n_alt_walls = 0;  // HBB and slip cells over all blocks
+  // same-level copies fused into block steps
+  std::vector<CcLevel> cc;
+  std::vector<CcEntry *> d_cclist;  // per level: the copies of fusable levels (k_cc_pull)
+  int fuse_cc = 1;
   // scheduler
   SchedState state;
   bool inited = false;
@@ -145,6 +149,12 @@ struct mb_ctx {
   int prg_bulk_limit = 0;               // CTAs allowed on bulk items at once (0: no limit)
   int rec_points = 32;                  // interface points per record CTA / executor item
   int spl_segs = 1;                     // spline segments per CTA / executor item
+  // minimum dynamic shared memory per spline / record CTA: caps how many CTAs
+  // of these latency-bound launches one SM takes, so that a launch that
+  // starts while a block step still holds most SMs spreads over the SMs that
+  // free up instead of piling onto the first ones
+  int spl_cta_smem = 96 * 1024;
+  int rec_cta_smem = 0;
   PrgTraceRec *d_trace = nullptr;       // executor trace (mb_set_program_trace)
   unsigned int *d_trace_n = nullptr;
   unsigned int trace_cap = 0;
@@ -245,8 +255,11 @@ template <int P> struct KStb { static void *ptr() { return (void *)k_block_step<
 template <int P> struct KStb2 { static void *ptr() { return (void *)k_block_step<P, 2>; } };
 template <int P> struct KStbR { static void *ptr() { return (void *)k_block_step_r<P, false>; } };
 template <int P> struct KStbRI { static void *ptr() { return (void *)k_block_step_r<P, true>; } };
+template <int P> struct KStbP { static void *ptr() { return (void *)k_block_step_p<P, false>; } };
+template <int P> struct KStbPI { static void *ptr() { return (void *)k_block_step_p<P, true>; } };
 template <int P> struct KStbQ { static void *ptr() { return (void *)k_block_step_q<P>; } };
 template <int P> struct KStbX { static void *ptr() { return (void *)k_block_step_x<P>; } };
+template <int P> struct KCcp { static void *ptr() { return (void *)k_cc_pull<P>; } };
 template <int P> struct KRec { static void *ptr() { return (void *)k_records<P>; } };
 template <int P> struct KSpl { static void *ptr() { return (void *)k_spline<P>; } };
 template <int P> struct KDrag { static void *ptr() { return (void *)k_drag<P>; } };
@@ -260,6 +273,8 @@ size_t program_smem(int prec) { return prec == MB_PREC_F64 ? prg_smem<double>() 
 
 // dynamic shared memory of k_spline per warp: two 12 x window arrays and the
 // window's c' and 1/den
+constexpr int MB_CTA_SMEM_MAX = 200 * 1024;  // largest spread request (B200: 227 KB per CTA)
+
 size_t spline_smem(int prec) {
   return prec == MB_PREC_F64 ? (size_t)26 * SPL_WARPS * spl_win<double>() * sizeof(double)
                              : (size_t)26 * SPL_WARPS * spl_win<float>() * sizeof(float);
@@ -281,9 +296,11 @@ bool options_on(const mb_ctx *c) { return c->opt.coll != MB_COLL_BGK || c->opt.h
 // Launch parameters of a block-step node.  total counts cells for the
 // one-cell-per-thread kernel and warp tiles for the quad kernel (quads).
 StbParams make_stb(mb_ctx *c, int a0, int a1, uint64_t parity, int macro_all, int write_macros, int region,
-                   bool quads) {
+                   bool quads, int ccpull) {
   StbParams p{};
   p.nblk = a1 - a0;
+  p.a0 = a0;
+  p.ccpull = ccpull;
   p.macro_all = macro_all;
   p.write_macros = write_macros;
   p.region = region;
@@ -292,7 +309,7 @@ StbParams make_stb(mb_ctx *c, int a0, int a1, uint64_t parity, int macro_all, in
   p.u0x = c->geo.config.U0[0];
   p.u0y = c->geo.config.U0[1];
   p.opt = c->opt;
-  long long cell = 0, wt = 0, rt = 0, level_cells = 0;
+  long long cell = 0, wt = 0, rt = 0, pt = 0, level_cells = 0;
   for (int a = a0; a < a1; a++) level_cells += region_cells(c->blk[a].nx, c->blk[a].ny, region);
   p.evict_first = c->stream_cells > 0 && level_cells >= c->stream_cells;
   for (int a = a0; a < a1; a++) {
@@ -326,8 +343,15 @@ StbParams make_stb(mb_ctx *c, int a0, int a1, uint64_t parity, int macro_all, in
     s.rinv_w = s.rw > 0 ? 1.0f / (float)s.rw : 0.f;
     s.cta0 = (int)rt;
     rt += (s.rcells + 255) / 256;
+    // pair kernel: CTAs of 256 consecutive pairs of the region
+    s.ppr = (s.rw + 1) / 2;
+    s.npairs = s.ppr > 0 ? (int)std::min<long long>((long long)s.ppr * nrows, 1LL << 30) : 0;
+    s.pinv = s.ppr > 0 ? 1.0f / (float)s.ppr : 0.f;
+    s.pcta0 = (int)pt;
+    pt += (s.npairs + 255) / 256;
   }
   p.rctas = rt;
+  p.pctas = pt;
   p.total = quads ? wt : cell;
   return p;
 }
@@ -343,10 +367,10 @@ bool background_capped(const mb_ctx *c, bool background) { return background && 
 bool rows_fit(const mb_ctx *c, const StbParams &p) {
   for (int t = 0; t < p.nblk; t++)
     if (9 * p.b[t].plane >= (1LL << 31) || (long long)p.b[t].ny * p.b[t].pitch >= (1LL << 31) ||
-        p.b[t].rcells >= (1 << 24))  // the row of a cell index comes from a float product
+        p.b[t].rcells >= (1 << 24) || p.b[t].npairs >= (1 << 24))  // rows come from float products
       return false;
   (void)c;
-  return p.rctas < (1LL << 31);
+  return p.rctas < (1LL << 31) && p.pctas < (1LL << 31);
 }
 
 // kernel and grid of a block-step launch (variant 0: one cell per thread,
@@ -362,6 +386,11 @@ void stb_launch_shape(const mb_ctx *c, int level, int region, bool background, c
   if (stb_uses_quads(c, level, region)) {
     *func = kfunc<KStbQ>(c->prec);
     *grid = dim3((unsigned)((p.total + 7) / 8));  // 8 warp tiles per CTA
+    return;
+  }
+  if (c->stb_variant[level] == 4 && region != STB_RIM && !background_capped(c, background) && rows_fit(c, p)) {
+    *func = region == STB_INTERIOR ? kfunc<KStbPI>(c->prec) : kfunc<KStbP>(c->prec);
+    *grid = dim3((unsigned)p.pctas);
     return;
   }
   if (c->stb_variant[level] == 3 && region != STB_RIM && !background_capped(c, background) && rows_fit(c, p)) {
@@ -386,12 +415,20 @@ int lower_plan(mb_ctx *c, CompiledPlan &cp) {
     d.deps = n.deps;
     if (n.kind == NK_STB) {
       const bool quads = stb_uses_quads(c, n.level, n.region);
-      d.stb = make_stb(c, n.a0, n.a1, n.parity, n.macro_all, 1, n.region, quads);
+      d.stb = make_stb(c, n.a0, n.a1, n.parity, n.macro_all, 1, n.region, quads, n.ccpull);
       // bulk: interiors of split levels, and whole levels streamed with
       // evict-first hints when bulk_levels is set
       d.background = (n.region == STB_INTERIOR) || (c->bulk_levels && n.region == STB_ALL && d.stb.evict_first);
       d.block = dim3(256);
       stb_launch_shape(c, n.level, n.region, d.background, d.stb, &d.func, &d.grid);
+      d.args[0] = &d.stb;
+    } else if (n.kind == NK_CCP) {
+      d.stb = make_stb(c, n.a0, n.a1, n.parity, 0, 1, STB_ALL, false, 0);
+      d.stb.cc_list = c->d_cclist[n.level];
+      d.stb.cc_n = (int)c->cc[n.level].links.size();
+      d.func = kfunc<KCcp>(c->prec);
+      d.block = dim3(128);
+      d.grid = dim3((unsigned)((d.stb.cc_n + 127) / 128));
       d.args[0] = &d.stb;
     } else if (n.kind == NK_REC) {
       if ((int)n.ops.size() > REC_MAX_OPS) return MB_ERR_UNSUPPORTED;
@@ -451,6 +488,7 @@ int lower_plan(mb_ctx *c, CompiledPlan &cp) {
       // per value on lines across rows) over many SMs' load/store units
       d.block = dim3(c->rec_points);
       d.grid = dim3((unsigned)((total + c->rec_points - 1) / c->rec_points));
+      d.smem = (size_t)c->rec_cta_smem;
       d.args[0] = &d.rec;
     } else {
       if ((int)n.spl.size() > SPL_MAX_TASKS) return MB_ERR_UNSUPPORTED;
@@ -488,7 +526,7 @@ int lower_plan(mb_ctx *c, CompiledPlan &cp) {
       d.func = kfunc<KSpl>(c->prec);
       d.block = dim3(32 * c->spl_segs);
       d.grid = dim3((unsigned)((nseg + c->spl_segs - 1) / c->spl_segs));
-      d.smem = spline_smem(c->prec) / SPL_WARPS * c->spl_segs;
+      d.smem = std::max(spline_smem(c->prec) / SPL_WARPS * c->spl_segs, (size_t)c->spl_cta_smem);
       d.args[0] = &d.spl;
     }
   }
@@ -566,7 +604,8 @@ int build_graph(CompiledPlan &cp, bool pdl) {
 
 int set_smem_limits(int prec) {
   MB_CUDA(cudaFuncSetAttribute(kfunc<KSpl>(prec), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)spline_smem(prec)));
+                               (int)std::max(spline_smem(prec), (size_t)MB_CTA_SMEM_MAX)));
+  MB_CUDA(cudaFuncSetAttribute(kfunc<KRec>(prec), cudaFuncAttributeMaxDynamicSharedMemorySize, MB_CTA_SMEM_MAX));
   MB_CUDA(cudaFuncSetAttribute(kfunc<KPrg>(prec), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)program_smem(prec)));
   MB_CUDA(cudaFuncSetAttribute(kfunc<KPrgT>(prec), cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -725,14 +764,17 @@ int program_status(mb_ctx *c) {
   return MB_ERR_TIMEOUT;
 }
 
-CompiledPlan *get_plan(mb_ctx *c, int n, bool final_macros, int *err) {
-  std::string key = c->state.key() + "/" + std::to_string(n) + (final_macros ? "F" : "P");
+CompiledPlan *get_plan(mb_ctx *c, int n, bool final_macros, int *err, bool batch = false) {
+  // batches and the persistent executor run the plain node kinds only
+  const bool fuse = c->fuse_cc && !options_on(c) && !batch && c->use_graph != 3;
+  std::string key = c->state.key() + "/" + std::to_string(n) + (final_macros ? "F" : "P") + (fuse ? "c" : "");
   auto it = c->plans.find(key);
   if (it != c->plans.end()) return it->second.get();
   auto cp = std::make_unique<CompiledPlan>();
   PlanCompiler pc(c->geo, c->bl, c->hflags, c->spl_lines);
   pc.split_cells = c->split_cells;
   pc.split_mask = c->split_mask;
+  if (fuse) pc.cc = &c->cc;
   SchedState s = c->state;
   cp->nodes = pc.compile(s, n, final_macros);
   cp->end = s;
@@ -841,6 +883,16 @@ extern "C" int mb_create(const mb_geometry *geo, int precision, mb_ctx **out) {
       }
   }
   mark_macro_sources(*geo, c->bl, c->hflags);
+  // same-level copies the block step of their level can perform: flag the
+  // targets and keep, per target cell, where its source is
+  c->cc = cc_levels(*geo, c->bl, c->hflags);
+  for (CcLevel &cl : c->cc) {
+    if (!cl.fusable) continue;
+    for (const CcLink &lk : cl.links)
+      if (lk.tcell >= (1LL << 31) || lk.scell >= (1LL << 31)) cl.fusable = false;  // 32-bit cells in CcEntry
+    if (!cl.fusable) continue;
+    for (const CcLink &lk : cl.links) c->hflags[lk.tblk][(size_t)lk.tcell] |= CF_CCPULL;
+  }
 
   // coarse-fine line table for the spline kernel; slots: 3 x 9 values per fine point
   c->spl_lines.resize(L.number_line);
@@ -893,6 +945,18 @@ extern "C" int mb_create(const mb_geometry *geo, int precision, mb_ctx **out) {
   }
   if ((e = dalloc(c.get(), &c->d_blk, c->nblk))) return e;
   MB_CUDA(cudaMemcpy(c->d_blk, c->blk.data(), c->nblk * sizeof(IfBlk), cudaMemcpyHostToDevice));
+  c->d_cclist.assign(L.LEVEL, nullptr);
+  for (int l = 0; l < L.LEVEL; l++) {
+    const CcLevel &cl = c->cc[l];
+    if (!cl.fusable) continue;
+    std::vector<CcEntry> ents;
+    for (const CcLink &lk : cl.links) {
+      const int sp = c->bl[lk.sblk].pitch;
+      ents.push_back({lk.tblk, lk.sblk, (int)lk.tcell, (int)(lk.scell % sp), (int)(lk.scell / sp), 0});
+    }
+    if ((e = dalloc(c.get(), &c->d_cclist[l], ents.size()))) return e;
+    MB_CUDA(cudaMemcpy(c->d_cclist[l], ents.data(), ents.size() * sizeof(CcEntry), cudaMemcpyHostToDevice));
+  }
   {
     void *p;
     if (cudaMalloc(&p, std::max<long long>(slot_pts, 1) * 27 * rb) != cudaSuccess) return MB_ERR_NOMEM;
@@ -1044,6 +1108,16 @@ extern "C" int mb_set_split_cells(mb_ctx *c, long long cells) {
   return MB_OK;
 }
 
+extern "C" int mb_set_cta_spread(mb_ctx *c, int spline_kb, int records_kb) {
+  if (!c || spline_kb < 0 || records_kb < 0 || spline_kb * 1024 > MB_CTA_SMEM_MAX || records_kb * 1024 > MB_CTA_SMEM_MAX)
+    return MB_ERR_INVALID;
+  cudaDeviceSynchronize();
+  c->spl_cta_smem = spline_kb * 1024;
+  c->rec_cta_smem = records_kb * 1024;
+  c->plans.clear();
+  return MB_OK;
+}
+
 extern "C" int mb_set_interface_shape(mb_ctx *c, int rec_points, int spline_segments) {
   if (!c || (rec_points != 32 && rec_points != 64) || spline_segments < 1 || spline_segments > SPL_WARPS)
     return MB_ERR_INVALID;
@@ -1072,7 +1146,7 @@ extern "C" int mb_set_stream_cells(mb_ctx *c, long long cells, int bulk) {
 }
 
 extern "C" int mb_set_stb_variant(mb_ctx *c, int level, int variant) {
-  if (!c || level < 0 || level >= c->geo.layout.LEVEL || variant < 0 || variant > 3) return MB_ERR_INVALID;
+  if (!c || level < 0 || level >= c->geo.layout.LEVEL || variant < 0 || variant > 4) return MB_ERR_INVALID;
   cudaDeviceSynchronize();
   c->stb_variant[level] = variant;
   c->plans.clear();
@@ -1125,6 +1199,14 @@ extern "C" int mb_set_cell_types(mb_ctx *c, int a, const int *types) {
   c->n_alt_walls += alt_after - alt_before;
   int e;
   if (a == c->drag_area && (e = upload_drag_links(c))) return e;
+  c->plans.clear();
+  return MB_OK;
+}
+
+extern "C" int mb_set_fusion(mb_ctx *c, int flags) {
+  if (!c || flags < 0 || flags > 1) return MB_ERR_INVALID;
+  cudaDeviceSynchronize();
+  c->fuse_cc = flags & 1;
   c->plans.clear();
   return MB_OK;
 }
@@ -1826,7 +1908,7 @@ extern "C" int mb_time_block_step(mb_ctx *c, int level, int n, mb_stream stream,
   long long tot = 0;
   for (int a0 = L.ASP[level]; a0 < L.ASP[level + 1]; a0 += STB_MAX_BLOCKS) {
     const int a1 = std::min(L.ASP[level + 1], a0 + STB_MAX_BLOCKS);
-    ps.push_back(make_stb(c, a0, a1, par, 0, 0, STB_ALL, stb_uses_quads(c, level, STB_ALL)));
+    ps.push_back(make_stb(c, a0, a1, par, 0, 0, STB_ALL, stb_uses_quads(c, level, STB_ALL), 0));
     for (int a = a0; a < a1; a++) tot += (long long)c->blk[a].nx * c->blk[a].ny;
   }
   void *fn = nullptr;
@@ -1836,26 +1918,40 @@ extern "C" int mb_time_block_step(mb_ctx *c, int level, int n, mb_stream stream,
     return gr;
   };
   { dim3 g0 = grid_of(ps[0]); (void)g0; }
-  cudaEvent_t e0, e1;
-  MB_CUDA(cudaEventCreate(&e0));
-  MB_CUDA(cudaEventCreate(&e1));
-  for (int w = 0; w < 3; w++)
-    for (auto &p : ps) {
-      void *args[] = {&p};
-      MB_CUDA(cudaLaunchKernel(fn, grid_of(p), dim3(256), args, 0, s));
-    }
-  MB_CUDA(cudaEventRecord(e0, s));
+  // the n launches replay as one CUDA graph on a private stream, so that
+  // the host's launch rate does not bound launches of a few microseconds
+  MB_CUDA(cudaStreamSynchronize(s));
+  cudaStream_t cs;
+  MB_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  cudaGraph_t gr = nullptr;
+  cudaGraphExec_t ge = nullptr;
+  MB_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
   for (int it = 0; it < n; it++)
     for (auto &p : ps) {
       void *args[] = {&p};
-      MB_CUDA(cudaLaunchKernel(fn, grid_of(p), dim3(256), args, 0, s));
+      if (cudaLaunchKernel(fn, grid_of(p), dim3(256), args, 0, cs) != cudaSuccess) break;
     }
-  MB_CUDA(cudaEventRecord(e1, s));
+  const cudaError_t ce = cudaStreamEndCapture(cs, &gr);
+  if (ce != cudaSuccess || cudaGraphInstantiate(&ge, gr, 0) != cudaSuccess) {
+    if (gr) cudaGraphDestroy(gr);
+    cudaStreamDestroy(cs);
+    return MB_ERR_CUDA;
+  }
+  cudaEvent_t e0, e1;
+  MB_CUDA(cudaEventCreate(&e0));
+  MB_CUDA(cudaEventCreate(&e1));
+  MB_CUDA(cudaGraphLaunch(ge, cs));  // warm-up
+  MB_CUDA(cudaEventRecord(e0, cs));
+  MB_CUDA(cudaGraphLaunch(ge, cs));
+  MB_CUDA(cudaEventRecord(e1, cs));
   MB_CUDA(cudaEventSynchronize(e1));
   float t = 0;
   MB_CUDA(cudaEventElapsedTime(&t, e0, e1));
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  cudaGraphExecDestroy(ge);
+  cudaGraphDestroy(gr);
+  cudaStreamDestroy(cs);
   if (ms) *ms = t / n;
   if (bytes) *bytes = (double)tot * 18.0 * (double)prec_bytes(c->prec);
   if (cells) *cells = tot;
@@ -1913,7 +2009,7 @@ int batch_plan(mb_batch *b, int n, bool fin, BatchPlan **out) {
     std::atomic<int> next{0};
     auto work = [&]() {
       cudaSetDevice(b->cases[0]->device);
-      for (int c = next++; c < nc; c = next++) parts[c] = get_plan(b->cases[c], n, fin, &errs[c]);
+      for (int c = next++; c < nc; c = next++) parts[c] = get_plan(b->cases[c], n, fin, &errs[c], true);
     };
     std::vector<std::thread> th;
     for (int t = 1; t < nt; t++) th.emplace_back(work);

@@ -20,6 +20,7 @@ enum : uint8_t {
   CF_MACRO = 8, // rho/ux/uy of this FLUID cell are read by an interface op
   CF_HBB = 16,  // CT_SOLID cell that is a half-way bounce-back wall (MB_SOLID_HBB)
   CF_SLIP = 32, // CT_SOLID cell that is an on-node free-slip wall (MB_SOLID_SLIP)
+  CF_CCPULL = 64, // C_BOUNDARY target of a same-level copy run beside its level's block step (NK_CCP)
 };
 
 bool obstacle_contains(const mb_config &c, double x, double y);
@@ -68,7 +69,7 @@ struct SplTask {
   int mask_off;   // offset into the node's M-write mask (-1: write all points)
 };
 
-enum NodeKind { NK_STB = 0, NK_REC = 1, NK_SPL = 2 };
+enum NodeKind { NK_STB = 0, NK_REC = 1, NK_SPL = 2, NK_CCP = 3 };  // NK_CCP: same-level copies beside a block step
 // cells a block-step node updates: all, those at distance >= 2 from the block
 // edge (they read nothing an interface op writes), or the distance <= 1 rim
 enum StbRegion { STB_ALL = 0, STB_INTERIOR = 1, STB_RIM = 2 };
@@ -80,6 +81,7 @@ struct PlanNode {
   int region = STB_ALL;       // STB: StbRegion
   uint64_t parity = 0;        // STB: current buffer of each block before the step
   int macro_all = 0;          // STB: write rho/u of every FLUID cell
+  int ccpull = 0;             // STB: skips CF_CCPULL cells (an NK_CCP node of the same level writes them)
   std::vector<Rec> recs;      // REC
   std::vector<std::pair<int, int>> ops;  // REC: (first record, count) of each reference line op
   double tw[4][3] = {};       // REC: temporal weight triples (a, b, c)
@@ -113,6 +115,23 @@ struct Op {
   std::array<int, 3> mk{};  // ring markers of the line at the call
 };
 
+// Same-level copies (c_c_boundary_transfer) of one level with chains
+// resolved: after the copies of the level run in order, target cell
+// (tblk, tcell) holds what source cell (sblk, scell) has after the level's
+// block step.  Cells are pitched (j * pitch + i).
+struct CcLink {
+  int tblk, sblk;
+  long long tcell, scell;
+};
+struct CcLevel {
+  bool fusable = false;           // `links` can run beside the level's block step
+  std::vector<CcLink> links;      // FLUID source, C_BOUNDARY target: run beside the block step (CF_CCPULL)
+  std::vector<CcLink> rec_links;  // other sources (their rho/u may come from later ops): point copies after the step
+};
+// One CcLevel per level, from the line tables (Line_Inf_CC, LCCP).
+std::vector<CcLevel> cc_levels(const mb_geometry &g, const std::vector<BlockLayout> &bl,
+                               const std::vector<std::vector<uint8_t>> &flags);
+
 // Compiles n coarse steps of evolution() (evolution.h:2-65) starting from
 // state s into plan nodes with dependency edges; advances s.  final_macros:
 // the last sub-step of every level writes rho/u of all FLUID cells.
@@ -125,6 +144,8 @@ struct PlanCompiler {
   long long split_cells = 1000000;
   // nonzero: level l splits exactly when bit l is set (overrides split_cells)
   unsigned split_mask = 0;
+  // non-null: same-level copies of fusable levels run inside the block step
+  const std::vector<CcLevel> *cc = nullptr;
   PlanCompiler(const mb_geometry &g_, const std::vector<BlockLayout> &bl_,
                const std::vector<std::vector<uint8_t>> &fl, const std::vector<SplLine> &sl)
       : g(g_), bl(bl_), flags(fl), spl_lines(sl) {}

@@ -51,6 +51,7 @@ struct Whole {
   uint32_t s;       // kind<<8 | block
   bool fluid_only;
   uint8_t dlo, dhi;
+  bool skip_cc = false;  // CF_CCPULL cells excluded (written by an NK_CCP node instead)
 };
 constexpr uint8_t DMAX = 255;
 
@@ -61,8 +62,8 @@ struct Access {
   void read(uint64_t k) { r.insert(k); rs.insert(summ(k)); }
   void write(uint64_t k) { w.insert(k); ws.insert(summ(k)); }
   void read_whole(uint32_t s, uint8_t dlo = 0, uint8_t dhi = DMAX) { wr.push_back({s, false, dlo, dhi}); rs.insert(s); }
-  void write_whole(uint32_t s, bool fo, uint8_t dlo = 0, uint8_t dhi = DMAX) {
-    ww.push_back({s, fo, dlo, dhi});
+  void write_whole(uint32_t s, bool fo, uint8_t dlo = 0, uint8_t dhi = DMAX, bool skip_cc = false) {
+    ww.push_back({s, fo, dlo, dhi, skip_cc});
     ws.insert(s);
   }
   void merge(const Access &o) {
@@ -124,6 +125,69 @@ void mark_macro_sources(const mb_geometry &g, const std::vector<BlockLayout> &bl
     const int r = g.Areas[lf.areaf_n].m / g.Areas[lf.areac_n].m;
     mark_line(g, bl, flags, lf.areaf_n, lf.line_F, lf.Nc, r);
   }
+}
+
+// ---------------------------------------------------------------------------
+// Same-level copies of each level with chains resolved (a copy whose source
+// an earlier copy of the level wrote passes that copy's source on).  Copies
+// from a FLUID source to a C_BOUNDARY target can run beside the block step
+// (the target computes the source's new values; the step leaves C_BOUNDARY
+// targets alone); the others stay point copies after the step: the rho/u a
+// non-FLUID source carries may be written by an interface op between the
+// step and the copy, and a FLUID target is the block step's own work.  A level is fusable when every copy stays within
+// the level's first block-step launch (its first 16 blocks), no line reads a
+// cell it writes, and no point copy reads a copy target.
+// ---------------------------------------------------------------------------
+std::vector<CcLevel> cc_levels(const mb_geometry &g, const std::vector<BlockLayout> &bl,
+                               const std::vector<std::vector<uint8_t>> &flags) {
+  const mb_layout &L = g.layout;
+  std::vector<CcLevel> out(L.LEVEL);
+  if (L.number_line2 == 0) return out;
+  for (int level = 0; level < L.LEVEL; level++) {
+    CcLevel &cl = out[level];
+    std::map<std::pair<int, long long>, std::pair<int, long long>> src;  // target -> final source
+    std::vector<std::pair<int, long long>> order;
+    bool ok = true;
+    for (int c = L.LCCP[level]; c < L.LCCP[level + 1]; c++) {
+      const mb_line &l = g.Line_Inf_CC[c];
+      const int A = l.areac_n, B = l.areaf_n;
+      const int a0 = L.ASP[level], a1 = L.ASP[level + 1];
+      // every copy of the level within the first launch chunk of 16 blocks
+      if (A < a0 || A >= a1 || B < a0 || B >= a1 || A - a0 >= 16 || B - a0 >= 16 || A > 255 || B > 255) ok = false;
+      std::set<std::pair<int, long long>> reads, writes;
+      for (int ip = 0; ip < l.Nc && ok; ip++) {
+        int i1 = 0, j1 = 0, i2 = 0, j2 = 0;  // c_c_boundary_transfer :20-33
+        if (l.line_C.xstart == l.line_C.xend) { i1 = l.line_C.xstart; j1 = l.line_C.ystart + ip; i2 = l.line_F.xstart; j2 = l.line_F.ystart + ip; }
+        if (l.line_C.ystart == l.line_C.yend) { i1 = l.line_C.xstart + ip; j1 = l.line_C.ystart; i2 = l.line_F.xstart + ip; j2 = l.line_F.ystart; }
+        if (i1 < 0 || j1 < 0 || i1 >= bl[A].nx || j1 >= bl[A].ny || i2 < 0 || j2 < 0 || i2 >= bl[B].nx ||
+            j2 >= bl[B].ny || i1 >= (1 << 28) || j1 >= (1 << 28)) {
+          ok = false;
+          break;
+        }
+        const std::pair<int, long long> sc{A, (long long)j1 * bl[A].pitch + i1}, tc{B, (long long)j2 * bl[B].pitch + i2};
+        reads.insert(sc);
+        writes.insert(tc);
+        auto it = src.find(sc);
+        const std::pair<int, long long> fin = it != src.end() ? it->second : sc;
+        if (!src.count(tc)) order.push_back(tc);
+        src[tc] = fin;
+      }
+      for (auto &w : writes)
+        if (reads.count(w)) ok = false;  // the reference's threads would race
+    }
+    for (auto &t : order) {
+      const CcLink lk{t.first, src[t].first, t.second, src[t].second};
+      if ((flags[lk.sblk][(size_t)lk.scell] & 3) == CT_FLUID && (flags[lk.tblk][(size_t)lk.tcell] & 3) == CT_COPY)
+        cl.links.push_back(lk);
+      else
+        cl.rec_links.push_back(lk);
+    }
+    for (const CcLink &lk : cl.rec_links)
+      if (src.count({lk.sblk, lk.scell})) ok = false;
+    if ((int)cl.rec_links.size() > PLAN_MAX_REC_OPS) ok = false;
+    cl.fusable = ok && !cl.links.empty();
+  }
+  return out;
 }
 
 // ---------------------------------------------------------------------------
@@ -235,6 +299,7 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
     const long long cell = (long long)(k & 0xffffffffffffull);
     const int d = edge_dist(blk, cell);
     if (d < wh.dlo || d > wh.dhi) return false;
+    if (wh.skip_cc && (flags[blk][cell] & CF_CCPULL)) return false;
     return !wh.fluid_only || is_fluid(blk, cell);
   };
 
@@ -249,6 +314,9 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
   };
   struct OpInfo {
     bool stb = false;
+    bool cc_fused = false;      // STB: its level's same-level copies run beside it (cc_nodes)
+    std::vector<int> stb_nodes; // STB: its nodes
+    std::vector<int> cc_nodes;  // STB: NK_CCP nodes, one per launch chunk with copies
     int level = -1;
     std::vector<int> parity;
     std::vector<Part> parts;
@@ -259,6 +327,7 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
   std::vector<PlanNode> nodes;
   std::vector<Access> acc;  // forward (unpruned) sets: used only to decide batching
   int open = -1;
+  int last_stb = -1;  // latest STB op; same-level copies right after it can fuse into it
 
   // ---- forward: expand ops into records and batch them ---------------------
   for (size_t oi = 0; oi < ops.size(); oi++) {
@@ -266,6 +335,7 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
     OpInfo &I = info[oi];
     if (o.kind == Op::STB) {
       open = -1;
+      last_stb = int(oi);
       I.stb = true;
       I.level = o.level;
       I.parity = o.parity;
@@ -288,11 +358,47 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
           nd.label = lab;
           nd.a0 = a0;
           nd.a1 = a1;
+          I.stb_nodes.push_back(int(nodes.size()));
           nodes.push_back(nd);
           acc.push_back(Access());
         }
       }
       continue;
+    }
+    bool cc_points = false;  // this op carries the point copies of a fused level
+    if (o.kind == Op::CC && cc && (*cc)[o.level].fusable && last_stb >= 0 && ops[last_stb].level == o.level) {
+      bool adjacent = true;  // only same-level copies of this level since the block step
+      for (size_t q = size_t(last_stb) + 1; q < oi; q++)
+        if (ops[q].kind != Op::CC || ops[q].level != o.level) adjacent = false;
+      const bool first = !info[last_stb].cc_fused;
+      if (adjacent && first) {
+        OpInfo &S = info[last_stb];
+        S.cc_fused = true;
+        for (int q : S.stb_nodes) {
+          nodes[q].ccpull = 1;
+          bool any = false;
+          for (const CcLink &lk : (*cc)[o.level].links) any |= lk.tblk >= nodes[q].a0 && lk.tblk < nodes[q].a1;
+          if (!any || nodes[q].region == STB_INTERIOR) continue;  // one copy node per chunk
+          bool have = false;
+          for (int c2 : S.cc_nodes) have |= nodes[c2].a0 == nodes[q].a0;
+          if (have) continue;
+          PlanNode nd;
+          nd.kind = NK_CCP;
+          nd.level = o.level;
+          nd.a0 = nodes[q].a0;
+          nd.a1 = nodes[q].a1;
+          nd.parity = nodes[q].parity;
+          nd.label = "ccp L" + std::to_string(o.level);
+          S.cc_nodes.push_back(int(nodes.size()));
+          nodes.push_back(nd);
+          acc.push_back(Access());
+        }
+      }
+      if (adjacent) {
+        if (!first || (*cc)[o.level].rec_links.empty())
+          continue;  // I.node stays -1: the copies have no node of their own
+        cc_points = true;
+      }
     }
     Access ac;
     std::vector<Rec> recs;
@@ -303,7 +409,22 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
     const bool is_spl = (o.kind == Op::SPL);
     double tw[3] = {0, 0, 0};
 
-    if (o.kind == Op::CC) {
+    if (cc_points) {
+      // the level's copies from non-FLUID sources, each its own one-point op
+      for (const CcLink &lk : (*cc)[o.level].rec_links) {
+        const int pA = o.parity[lk.sblk], pB = o.parity[lk.tblk];
+        Rec r{};
+        r.type = REC_CC;
+        r.bits = uint8_t((pA ? RB_SRC_BUF : 0) | (pB ? RB_DST_BUF : 0) | RB_WRITE_F | RB_WRITE_M);
+        r.dst_block = uint8_t(lk.tblk);
+        r.src_block = uint8_t(lk.sblk);
+        r.dst_cell = int32_t(lk.tcell);
+        r.src = int32_t(lk.scell);
+        recs.push_back(r);
+        rparts.push_back({fkey(pB, lk.tblk, lk.tcell), key(RK_M, lk.tblk, lk.tcell), {fkey(pA, lk.sblk, lk.scell)},
+                          {key(RK_M, lk.sblk, lk.scell)}});
+      }
+    } else if (o.kind == Op::CC) {
       const mb_line &l = g.Line_Inf_CC[o.line];
       const int A = l.areac_n, B = l.areaf_n;
       const int pA = o.parity[A], pB = o.parity[B];
@@ -406,7 +527,8 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
 
     const NodeKind want = is_spl ? NK_SPL : NK_REC;
     bool join = (open >= 0 && nodes[open].kind == want);
-    if (join && want == NK_REC && int(nodes[open].ops.size()) >= PLAN_MAX_REC_OPS) join = false;
+    if (join && want == NK_REC && int(nodes[open].ops.size() + (cc_points ? recs.size() : 1)) > PLAN_MAX_REC_OPS)
+      join = false;
     if (join && want == NK_SPL && int(nodes[open].spl.size()) >= PLAN_MAX_SPL_TASKS) join = false;
     if (join && want == NK_REC && o.kind == Op::TEMPORAL) {
       const PlanNode &nd = nodes[open];
@@ -447,7 +569,11 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
           nd.tw[widx][2] = tw[2];
         }
       }
-      nd.ops.push_back({int(nd.recs.size()), int(recs.size())});
+      if (cc_points) {
+        for (size_t q = 0; q < recs.size(); q++) nd.ops.push_back({int(nd.recs.size() + q), 1});
+      } else {
+        nd.ops.push_back({int(nd.recs.size()), int(recs.size())});
+      }
       for (size_t q = 0; q < recs.size(); q++) {
         Rec r = recs[q];
         r.bits |= uint8_t(widx << RB_WIDX_SHIFT);
@@ -507,10 +633,15 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
       // cells and read F of buffer p, over the whole block
       for (int a = L.ASP[I.level]; a < L.ASP[I.level + 1]; a++) {
         const int p = I.parity[a];
-        apply_layer({uint32_t(((p ? RK_F0 : RK_F1) << 8) | a), false, 0, DMAX}, true);
-        apply_layer({uint32_t((RK_M << 8) | a), true, 0, DMAX}, true);
+        apply_layer({uint32_t(((p ? RK_F0 : RK_F1) << 8) | a), false, 0, DMAX, I.cc_fused}, true);
+        apply_layer({uint32_t((RK_M << 8) | a), true, 0, DMAX, I.cc_fused}, true);
         apply_layer({uint32_t(((p ? RK_F1 : RK_F0) << 8) | a), false, 0, DMAX}, false);
       }
+      if (I.cc_fused)  // the copies beside the step write F and rho/u of their targets
+        for (const CcLink &lk : (*cc)[I.level].links) {
+          set_state(fkey(I.parity[lk.tblk] ^ 1, lk.tblk, lk.tcell), true);
+          set_state(key(RK_M, lk.tblk, lk.tcell), true);
+        }
       continue;
     }
     for (Part &pt : I.parts) pt.live = !state_of(pt.wkey);
@@ -538,12 +669,34 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
     for (int a = nodes[q].a0; a < nodes[q].a1; a++) {
       const int p = int((nodes[q].parity >> a) & 1);
       fin[q].read_whole(uint32_t(((p ? RK_F1 : RK_F0) << 8) | a), rlo, rhi);
-      fin[q].write_whole(uint32_t(((p ? RK_F0 : RK_F1) << 8) | a), false, wlo, whi);
-      fin[q].write_whole(uint32_t((RK_M << 8) | a), true, wlo, whi);
+      fin[q].write_whole(uint32_t(((p ? RK_F0 : RK_F1) << 8) | a), false, wlo, whi, nodes[q].ccpull != 0);
+      fin[q].write_whole(uint32_t((RK_M << 8) | a), true, wlo, whi, nodes[q].ccpull != 0);
     }
   }
   for (auto &I : info) {
-    if (I.stb) continue;
+    if (!I.stb || !I.cc_fused) continue;
+    for (const CcLink &lk : (*cc)[I.level].links) {
+      int q = -1;  // the copy node of the target's launch chunk
+      for (int c2 : I.cc_nodes)
+        if (lk.tblk >= nodes[c2].a0 && lk.tblk < nodes[c2].a1) q = c2;
+      if (q < 0) continue;  // cannot happen: fusable levels keep each copy within one chunk
+      Access &A = fin[q];
+      A.write(fkey(I.parity[lk.tblk] ^ 1, lk.tblk, lk.tcell));
+      A.write(key(RK_M, lk.tblk, lk.tcell));
+      const int ps = I.parity[lk.sblk];  // buffer the step reads
+      const BlockLayout &sb = bl[lk.sblk];
+      const int si = int(lk.scell % sb.pitch), sj = int(lk.scell / sb.pitch);
+      for (int k = 0; k < 9; k++) {
+        static const int EX[9] = {0, 1, 0, -1, 0, 1, -1, -1, 1}, EY[9] = {0, 0, 1, 0, -1, 1, 1, -1, -1};
+        const int ii = si - EX[k], jj = sj - EY[k];
+        if (ii < 0 || jj < 0 || ii >= sb.nx || jj >= sb.ny) continue;
+        A.read(fkey(ps, lk.sblk, (long long)jj * sb.pitch + ii));
+      }
+      A.read(fkey(ps, lk.sblk, lk.scell));  // sources are FLUID: their rho/u come from the pulled values
+    }
+  }
+  for (auto &I : info) {
+    if (I.stb || I.node < 0) continue;
     Access &A = fin[I.node];
     for (auto &pt : I.parts) {
       if (!pt.live) continue;

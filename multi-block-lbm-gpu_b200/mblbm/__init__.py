@@ -142,6 +142,8 @@ SIGNATURES = {
     "mb_set_stb_variant": ([_vp, C.c_int, C.c_int], C.c_int),
     "mb_set_bulk_occupancy": ([_vp, C.c_int], C.c_int),
     "mb_set_collision": ([_vp, C.c_int, C.c_double, C.c_double, C.c_double], C.c_int),
+    "mb_set_fusion": ([_vp, C.c_int], C.c_int),
+    "mb_set_cta_spread": ([_vp, C.c_int, C.c_int], C.c_int),
     "mb_set_body_force": ([_vp, C.c_double, C.c_double], C.c_int),
     "mb_set_cell_types": ([_vp, C.c_int, _pi], C.c_int),
     "mb_set_stream_cells": ([_vp, C.c_longlong, C.c_int], C.c_int),
@@ -418,6 +420,14 @@ class MultiBlockLBM:
     def set_bulk_occupancy(self, ctas_per_sm):
         """Cap interior block-step grids at ctas_per_sm CTAs per SM (0: uncapped)."""
         _check(self.lib.mb_set_bulk_occupancy(self.h, int(ctas_per_sm)), "mb_set_bulk_occupancy")
+
+    def set_cta_spread(self, spline_kb, records_kb):
+        """Minimum shared memory per spline / record CTA (KB): caps their CTAs per SM."""
+        _check(self.lib.mb_set_cta_spread(self.h, int(spline_kb), int(records_kb)), "mb_set_cta_spread")
+
+    def set_fusion(self, flags):
+        """Plan fusions (bit 0: same-level copies inside the block step); results are identical."""
+        _check(self.lib.mb_set_fusion(self.h, int(flags)), "mb_set_fusion")
 
     def set_collision(self, kind, s_e=0.0, s_eps=0.0, s_q=0.0):
         """MB_COLL_BGK, or MB_COLL_MRT with rates s_e, s_eps, s_q (<= 0: the block's 1/tau)."""

@@ -285,16 +285,19 @@ def test_interior_rim_split(mb, orc, cuda_device, name):
         assert np.array_equal(a.fields(k)["F"], b.fields(k)["F"])
 
 
-@pytest.mark.parametrize("variant", [1, 2, 3])
+@pytest.mark.parametrize("split", [0, 10**12])
+@pytest.mark.parametrize("variant", [1, 2, 3, 4])
 @pytest.mark.parametrize("prec", ["f32", "f16s", "f64"])
-def test_quad_kernel_equals_cell_kernel(mb, cuda_device, prec, variant):
-    """The four- and two-cells-per-thread block steps give bitwise the same state."""
+def test_quad_kernel_equals_cell_kernel(mb, cuda_device, prec, variant, split):
+    """Every block-step variant gives bitwise the same state, on whole levels
+    and on split (interior + rim) levels."""
     g = mb.geo_init(*make_ref.case("n3")[:2])
     a = mb.MultiBlockLBM(g, prec)
     b = mb.MultiBlockLBM(g, prec)
     for lvl in range(g.layout.LEVEL):
+        a.set_stb_variant(lvl, 0)
         b.set_stb_variant(lvl, variant)
-    b.set_split_cells(0)
+    b.set_split_cells(split)
     for s in (a, b):
         s.init()
         s.evolution(9)
@@ -367,3 +370,28 @@ def test_step_diag_equals_step_by_step(mb, cuda_device, prec):
         fa, fb = a.fields(k), b.fields(k)
         for key in ("F", "rho", "ux", "uy"):
             assert np.array_equal(fa[key], fb[key])
+
+
+@pytest.mark.parametrize("graph", [True, False, "program"])
+@pytest.mark.parametrize("split,variant", [(10**12, 0), (0, 0), (10**12, 4), (0, 3)])
+@pytest.mark.parametrize("name,prec", [("n3", "f32"), ("g49", "f64"), ("g25", "f16s")])
+def test_fused_copies_bitwise(mb, cuda_device, name, prec, split, variant, graph):
+    """Same-level copies done inside the block step (mb_set_fusion bit 0, the
+    default) give bitwise the state of separate copy launches."""
+    g = mb.geo_init(*make_ref.case(name)[:2])
+    sims = []
+    for fuse in (0, 1):
+        s = mb.MultiBlockLBM(g, prec, graph=graph)
+        s.set_fusion(fuse)
+        s.set_split_cells(split)
+        for lvl in range(g.layout.LEVEL):
+            s.set_stb_variant(lvl, variant)
+        s.init()
+        s.evolution(13)
+        sims.append(s)
+    for k in range(g.layout.number_area):
+        fa, fb = sims[0].fields(k), sims[1].fields(k)
+        for key in ("F", "rho", "ux", "uy"):
+            assert np.array_equal(fa[key], fb[key]), (k, key)
+    assert sims[0].getDrag_block()[2] == sims[1].getDrag_block()[2]
+    assert sims[0].error_L2() == sims[1].error_L2()
