@@ -211,8 +211,8 @@ int mb_sync(mb_ctx *ctx, mb_stream stream);
 int mb_program_selftest(mb_ctx *ctx, int stall, mb_stream stream);
 /* Levels with at least `cells` cells update their interior (cells two or more
  * from a block edge) and their rim as separate DAG nodes, so that the interior
- * of the next coarse step overlaps the fine levels of this one.  Default 1e6
- * for MB_PREC_F16S, no split for the other precisions; 0 splits every level. */
+ * of the next coarse step overlaps the fine levels of this one.  Default 1e6,
+ * no split for MB_PREC_F64; 0 splits every level. */
 int mb_set_split_cells(mb_ctx *ctx, long long cells);
 /* Work granularity of interface nodes: points per record CTA (graph modes)
  * or work item (mode 3), 32 (default) or 64; spline segments of 32 coarse

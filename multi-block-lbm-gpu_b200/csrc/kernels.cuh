@@ -1091,8 +1091,17 @@ __device__ __forceinline__ void rec_point(const RecOpsParams &p, int t) {
   const S *Fs = (const S *)Fb.F[op.bits & 1];
   const R rh = ((const R *)Fb.rho)[sc], ux = ((const R *)Fb.ux)[sc], uy = ((const R *)Fb.uy)[sc];
   R ft[9];
+  if (op.type == 4) {  // the fine cell holds what a c_f stored from slot point sstride
+    const R *sv = (const R *)p.slots + (long long)op.sstride * 27 + op.m2 * 9;
 #pragma unroll
-  for (int k = 0; k < 9; k++) ft[k] = ld_f<P>(Fs, k * Fb.plane + sc, k);
+    for (int k = 0; k < 9; k++) {  // the stored form's rounding, as st_f then ld_f
+      if constexpr (Prec<P>::shifted) ft[k] = to_r(from_r<S>(sv[k] - wk<P>(k))) + wk<P>(k);
+      else ft[k] = to_r(from_r<S>(sv[k]));
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < 9; k++) ft[k] = ld_f<P>(Fs, k * Fb.plane + sc, k);
+  }
   const uint8_t live = mp ? *mp : op.bits;
   if (live & 8) {
     ((R *)D.rho)[dc] = rh;

@@ -450,6 +450,10 @@ int lower_plan(mb_ctx *c, CompiledPlan &cp) {
         op.src0 = a.src;
         op.dstride = cnt > 1 ? n.recs[r0 + 1].dst_cell - a.dst_cell : 0;
         op.sstride = cnt > 1 ? n.recs[r0 + 1].src - a.src : 0;
+        if (a.type == REC_FC_SLOT) {  // single point: sstride carries its slot point
+          if (cnt != 1) return MB_ERR_INVALID;
+          op.sstride = int32_t(a.m0 | (a.m1 << 8) | (a.pad << 16));
+        }
         uint8_t full = 0, all_same = 1;
         const uint8_t buf_bits = uint8_t(a.bits & ~(RB_WRITE_F | RB_WRITE_M));
         for (int q = 0; q < cnt; q++) {
@@ -836,9 +840,10 @@ extern "C" int mb_create(const mb_geometry *geo, int precision, mb_ctx **out) {
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return MB_ERR_NODEVICE;
   auto c = std::make_unique<mb_ctx>();
   c->prec = precision;
-  // measured on config 2: FP16 storage gains from overlapping the split
-  // coarse interior with the fine levels, FP32 and FP64 storage do not
-  c->split_cells = precision == MB_PREC_F16S ? 1000000 : (1LL << 62);
+  // measured on config 2: overlapping the split coarse interior with the
+  // fine levels gains 5% (FP32) and 13% (FP16 storage) per step once the
+  // spline launches spread over the SMs (mb_set_cta_spread); FP64 unmeasured
+  c->split_cells = precision == MB_PREC_F64 ? (1LL << 62) : 1000000;
   // FP16 storage: the level-0 step is issue-bound; the cell-range kernel
   // issues a quarter fewer instructions (106 against 109 us per step)
   if (precision == MB_PREC_F16S) c->stb_variant[0] = 3;

@@ -27,7 +27,10 @@ bool obstacle_contains(const mb_config &c, double x, double y);
 int cell_type(const mb_geometry &g, int a, int i, int j);
 
 // One interface point operation (16 bytes, the unit of the record kernel).
-enum : uint8_t { REC_CC = 0, REC_TEMPORAL = 1, REC_CF = 2, REC_FC = 3 };
+// REC_FC_SLOT: an f_c point whose fine cell's F was last written by a c_f
+// record; it reads that value from the c_f's slot (slot point in
+// m0 | m1 << 8 | pad << 16, marker m2), so the two can share a launch.
+enum : uint8_t { REC_CC = 0, REC_TEMPORAL = 1, REC_CF = 2, REC_FC = 3, REC_FC_SLOT = 4 };
 enum : uint8_t {
   RB_SRC_BUF = 1,   // current F buffer of the source block
   RB_DST_BUF = 2,   // current F buffer of the target block

@@ -43,6 +43,8 @@ enum : uint64_t { RK_F0 = 0, RK_F1 = 1, RK_M = 2, RK_SLOT = 3 };
 inline uint64_t key(uint64_t kind, uint64_t owner, uint64_t idx) { return (kind << 56) | (owner << 48) | idx; }
 inline uint32_t summ(uint64_t k) { return uint32_t(k >> 48); }  // kind<<8 | owner
 inline uint64_t fkey(int buf, int block, long long cell) { return key(buf ? RK_F1 : RK_F0, block, cell); }
+// records of one op share their type and buffer bits
+inline int run_key(const Rec &r) { return (r.type << 8) | (r.bits & (RB_SRC_BUF | RB_DST_BUF)); }
 
 // A whole-block access of a block step: every cell of block `s & 0xff` whose
 // distance to the block edge lies in [dlo, dhi] (FLUID cells only if
@@ -328,6 +330,24 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
   std::vector<Access> acc;  // forward (unpruned) sets: used only to decide batching
   int open = -1;
   int last_stb = -1;  // latest STB op; same-level copies right after it can fuse into it
+  // Reads of a C_BOUNDARY cell's F that no op has written since its block's
+  // last step may read the step's input buffer instead: the step copies
+  // C_BOUNDARY cells unchanged, so both buffers hold the same value there,
+  // and the read no longer conflicts with a later write of the cell.  An f_c
+  // read of a cell whose latest write is a c_f record takes the value from
+  // that record's slot instead (REC_FC_SLOT), for the same reason.
+  std::vector<int> stb_op(L.number_area, -1);  // op index of each block's latest step
+  struct LastWrite {
+    int op;
+    int line = -1, slot = 0, marker = 0;  // c_f writes: where the value comes from
+  };
+  std::unordered_map<uint64_t, LastWrite> lastw;  // F key -> its latest point write
+  auto src_buf = [&](int b, int p, long long cell) -> int {
+    const uint8_t f = flags[b][(size_t)cell];
+    if ((f & 3) != CT_COPY || (f & CF_CCPULL) || stb_op[b] < 0) return p;
+    auto it = lastw.find(fkey(p, b, cell));
+    return (it == lastw.end() || it->second.op < stb_op[b]) ? p ^ 1 : p;
+  };
 
   // ---- forward: expand ops into records and batch them ---------------------
   for (size_t oi = 0; oi < ops.size(); oi++) {
@@ -336,6 +356,7 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
     if (o.kind == Op::STB) {
       open = -1;
       last_stb = int(oi);
+      for (int a = L.ASP[o.level]; a < L.ASP[o.level + 1]; a++) stb_op[a] = int(oi);
       I.stb = true;
       I.level = o.level;
       I.parity = o.parity;
@@ -412,7 +433,7 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
     if (cc_points) {
       // the level's copies from non-FLUID sources, each its own one-point op
       for (const CcLink &lk : (*cc)[o.level].rec_links) {
-        const int pA = o.parity[lk.sblk], pB = o.parity[lk.tblk];
+        const int pA = src_buf(lk.sblk, o.parity[lk.sblk], lk.scell), pB = o.parity[lk.tblk];
         Rec r{};
         r.type = REC_CC;
         r.bits = uint8_t((pA ? RB_SRC_BUF : 0) | (pB ? RB_DST_BUF : 0) | RB_WRITE_F | RB_WRITE_M);
@@ -427,12 +448,13 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
     } else if (o.kind == Op::CC) {
       const mb_line &l = g.Line_Inf_CC[o.line];
       const int A = l.areac_n, B = l.areaf_n;
-      const int pA = o.parity[A], pB = o.parity[B];
+      const int pB = o.parity[B];
       for (int ip = 0; ip < l.Nc; ip++) {
         int i1 = 0, j1 = 0, i2 = 0, j2 = 0;
         if (l.line_C.xstart == l.line_C.xend) { i1 = l.line_C.xstart; j1 = l.line_C.ystart + ip; i2 = l.line_F.xstart; j2 = l.line_F.ystart + ip; }
         if (l.line_C.ystart == l.line_C.yend) { i1 = l.line_C.xstart + ip; j1 = l.line_C.ystart; i2 = l.line_F.xstart + ip; j2 = l.line_F.ystart; }
         const long long c1 = pitch_cell(A, i1, j1), c2 = pitch_cell(B, i2, j2);
+        const int pA = src_buf(A, o.parity[A], c1);
         Rec r{};
         r.type = REC_CC;
         r.bits = uint8_t((pA ? RB_SRC_BUF : 0) | (pB ? RB_DST_BUF : 0) | RB_WRITE_F | RB_WRITE_M);
@@ -477,13 +499,14 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
     } else if (o.kind == Op::FC) {
       const mb_line &l = g.Line_Inf_F[o.line];
       const int Cb = l.areac_n, Fb = l.areaf_n;
-      const int pC = o.parity[Cb], pF = o.parity[Fb];
+      const int pC = o.parity[Cb];
       const int r = g.Areas[Fb].m / g.Areas[Cb].m;
       for (int ip = 0; ip < l.Nc; ip++) {
         int ic, jc, i_f, j_f;
         if (l.line_C.xstart == l.line_C.xend) { ic = l.line_C.xstart; jc = l.line_C.ystart + ip; i_f = l.line_F.xstart; j_f = l.line_F.ystart + r * ip; }
         else { ic = l.line_C.xstart + ip; jc = l.line_C.ystart; i_f = l.line_F.xstart + r * ip; j_f = l.line_F.ystart; }
         const long long cc = pitch_cell(Cb, ic, jc), cf = pitch_cell(Fb, i_f, j_f);
+        const int pF = src_buf(Fb, o.parity[Fb], cf);
         Rec rr{};
         rr.type = REC_FC;
         rr.bits = uint8_t((pF ? RB_SRC_BUF : 0) | (pC ? RB_DST_BUF : 0) | RB_WRITE_F | RB_WRITE_M);
@@ -491,8 +514,18 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
         rr.src_block = uint8_t(Fb);
         rr.dst_cell = int32_t(cc);
         rr.src = int32_t(cf);
+        uint64_t rF = fkey(pF, Fb, cf);
+        auto lw = lastw.find(fkey(o.parity[Fb], Fb, cf));
+        if (lw != lastw.end() && lw->second.line >= 0 && lw->second.op > stb_op[Fb] && lw->second.slot < (1 << 24)) {
+          rr.type = REC_FC_SLOT;
+          rr.m0 = uint8_t(lw->second.slot & 0xff);
+          rr.m1 = uint8_t((lw->second.slot >> 8) & 0xff);
+          rr.pad = uint8_t((lw->second.slot >> 16) & 0xff);
+          rr.m2 = uint8_t(lw->second.marker);
+          rF = key(RK_SLOT, lw->second.line, lw->second.marker);
+        }
         recs.push_back(rr);
-        rparts.push_back({fkey(pC, Cb, cc), key(RK_M, Cb, cc), {fkey(pF, Fb, cf), key(RK_M, Fb, cf)}, {key(RK_M, Fb, cf)}});
+        rparts.push_back({fkey(pC, Cb, cc), key(RK_M, Cb, cc), {rF, key(RK_M, Fb, cf)}, {key(RK_M, Fb, cf)}});
       }
     } else if (is_spl) {
       const mb_line &l = g.Line_Inf_C[o.line];
@@ -515,6 +548,16 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
       task.m0 = o.mk[0];
       task.mask_off = -1;
     }
+    for (size_t q = 0; q < rparts.size(); q++) {
+      if (rparts[q].wF == ~0ull) continue;
+      LastWrite w{int(oi)};
+      if (recs[q].type == REC_CF) {
+        w.line = o.line;
+        w.slot = recs[q].src;
+        w.marker = o.mk[2];
+      }
+      lastw[rparts[q].wF] = w;
+    }
     for (auto &rp : rparts) {
       for (auto k : rp.rF) ac.read(k);
       for (auto k : rp.rM) ac.read(k);
@@ -527,8 +570,14 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
 
     const NodeKind want = is_spl ? NK_SPL : NK_REC;
     bool join = (open >= 0 && nodes[open].kind == want);
-    if (join && want == NK_REC && int(nodes[open].ops.size() + (cc_points ? recs.size() : 1)) > PLAN_MAX_REC_OPS)
-      join = false;
+    int nruns = 0;
+    if (want == NK_REC) {
+      nruns = recs.empty() ? 0 : 1;
+      for (size_t q = 1; q < recs.size(); q++)
+        nruns += cc_points || run_key(recs[q]) != run_key(recs[q - 1]) || recs[q].type == REC_FC_SLOT ||
+                 recs[q - 1].type == REC_FC_SLOT;
+    }
+    if (join && want == NK_REC && int(nodes[open].ops.size()) + nruns > PLAN_MAX_REC_OPS) join = false;
     if (join && want == NK_SPL && int(nodes[open].spl.size()) >= PLAN_MAX_SPL_TASKS) join = false;
     if (join && want == NK_REC && o.kind == Op::TEMPORAL) {
       const PlanNode &nd = nodes[open];
@@ -571,8 +620,14 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
       }
       if (cc_points) {
         for (size_t q = 0; q < recs.size(); q++) nd.ops.push_back({int(nd.recs.size() + q), 1});
-      } else {
-        nd.ops.push_back({int(nd.recs.size()), int(recs.size())});
+      } else {  // runs of records with the same type and buffer bits (each run is affine)
+        size_t q0 = 0;
+        for (size_t q = 1; q <= recs.size(); q++)
+          if (q == recs.size() || run_key(recs[q]) != run_key(recs[q0]) || recs[q].type == REC_FC_SLOT ||
+              recs[q0].type == REC_FC_SLOT) {
+            nd.ops.push_back({int(nd.recs.size() + q0), int(q - q0)});
+            q0 = q;
+          }
       }
       for (size_t q = 0; q < recs.size(); q++) {
         Rec r = recs[q];
