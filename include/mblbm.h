@@ -244,7 +244,8 @@ int mb_set_stream_cells(mb_ctx *ctx, long long cells, int bulk);
  * consecutive cells of one block with 32-bit offsets (whole levels and
  * interiors; rims use 0), 4 = cell pairs: a thread steps cells i, i+1 with
  * shared addresses and vector accesses, 256 pairs per CTA (same coverage as 3).
- * Default 0, and 3 for level 0 in MB_PREC_F16S.  Results are identical. */
+ * Default 0; level 0 uses 3 in MB_PREC_F16S and 1 in MB_PREC_F32 and
+ * MB_PREC_F32U.  Results are identical. */
 int mb_set_stb_variant(mb_ctx *ctx, int level, int variant);
 /* Caps the grid of interior (bulk) block-step launches at ctas_per_sm CTAs of
  * 256 threads per SM (0 = uncapped), leaving CTA slots on every SM for the

@@ -844,9 +844,12 @@ extern "C" int mb_create(const mb_geometry *geo, int precision, mb_ctx **out) {
   // fine levels gains 5% (FP32) and 13% (FP16 storage) per step once the
   // spline launches spread over the SMs (mb_set_cta_spread); FP64 unmeasured
   c->split_cells = precision == MB_PREC_F64 ? (1LL << 62) : 1000000;
-  // FP16 storage: the level-0 step is issue-bound; the cell-range kernel
-  // issues a quarter fewer instructions (106 against 109 us per step)
+  // level 0 of config 2, measured per coarse step: FP16 storage is
+  // issue-bound and the cell-range kernel issues a quarter fewer
+  // instructions (106 against 109 us); FP32 storage gains from the quads'
+  // vector accesses (112 against 117 us with the split level 0)
   if (precision == MB_PREC_F16S) c->stb_variant[0] = 3;
+  if (precision == MB_PREC_F32 || precision == MB_PREC_F32U) c->stb_variant[0] = 1;
   cudaGetDevice(&c->device);
   cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device);
   c->geo = *geo;
@@ -1691,31 +1694,33 @@ extern "C" int mb_copy_fields(mb_ctx *c, int a, double *rho, double *ux, double 
   if (int st = program_status(c)) return st;
   const IfBlk &B = c->blk[a];
   const long long n = (long long)B.nx * B.ny;
-  int e = ensure_stage(c, (size_t)9 * n);
+  // one staging area for every requested field: all conversions and copies
+  // are queued together and the call waits once
+  int e = ensure_stage(c, (size_t)12 * n);
   if (e) return e;
   const int gr = launch_grid(9 * n, 256);
   if (F) {
     const void *Fs = B.F[c->state.parity[a]];
     MB_DISPATCH(c->prec, (k_planes_to_f64<P><<<gr, 256, 0, s>>>((const S *)Fs, B.plane, B.nx, B.ny, B.pitch, c->d_stage)));
     MB_CUDA(cudaMemcpyAsync(F, c->d_stage, 9 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
-    MB_CUDA(cudaStreamSynchronize(s));
   }
   void *M[3] = {B.rho, B.ux, B.uy};
   double *H[3] = {rho, ux, uy};
   for (int q = 0; q < 3; q++) {
     if (!H[q]) continue;
-    if (c->prec == MB_PREC_F64) k_field_to_f64<double><<<gr, 256, 0, s>>>((const double *)M[q], B.nx, B.ny, B.pitch, c->d_stage);
-    else k_field_to_f64<float><<<gr, 256, 0, s>>>((const float *)M[q], B.nx, B.ny, B.pitch, c->d_stage);
-    MB_CUDA(cudaMemcpyAsync(H[q], c->d_stage, n * sizeof(double), cudaMemcpyDeviceToHost, s));
-    MB_CUDA(cudaStreamSynchronize(s));
+    double *st = c->d_stage + (9 + q) * n;
+    if (c->prec == MB_PREC_F64) k_field_to_f64<double><<<gr, 256, 0, s>>>((const double *)M[q], B.nx, B.ny, B.pitch, st);
+    else k_field_to_f64<float><<<gr, 256, 0, s>>>((const float *)M[q], B.nx, B.ny, B.pitch, st);
+    MB_CUDA(cudaMemcpyAsync(H[q], st, n * sizeof(double), cudaMemcpyDeviceToHost, s));
   }
-  if (solid) {
+  if (solid) {  // host work while the copies run
     const auto &fl = c->hflags[a];
     for (int j = 0; j < B.ny; j++)
       for (int i = 0; i < B.nx; i++) {
         solid[(size_t)j * B.nx + i] = flag_code(fl[(size_t)j * B.pitch + i]);
       }
   }
+  MB_CUDA(cudaStreamSynchronize(s));
   MB_CUDA(cudaGetLastError());
   return MB_OK;
 }
@@ -1726,24 +1731,24 @@ extern "C" int mb_set_fields(mb_ctx *c, int a, const double *rho, const double *
   cudaStream_t s = (cudaStream_t)stream;
   const IfBlk &B = c->blk[a];
   const long long n = (long long)B.nx * B.ny;
-  int e = ensure_stage(c, (size_t)9 * n);
+  int e = ensure_stage(c, (size_t)12 * n);
   if (e) return e;
   const int gr = launch_grid(9 * n, 256);
   if (F) {
     MB_CUDA(cudaMemcpyAsync(c->d_stage, F, 9 * n * sizeof(double), cudaMemcpyHostToDevice, s));
     void *Fd = B.F[c->state.parity[a]];
     MB_DISPATCH(c->prec, (k_f64_to_planes<P><<<gr, 256, 0, s>>>((S *)Fd, B.plane, B.nx, B.ny, B.pitch, c->d_stage)));
-    MB_CUDA(cudaStreamSynchronize(s));
   }
   void *M[3] = {B.rho, B.ux, B.uy};
   const double *H[3] = {rho, ux, uy};
   for (int q = 0; q < 3; q++) {
     if (!H[q]) continue;
-    MB_CUDA(cudaMemcpyAsync(c->d_stage, H[q], n * sizeof(double), cudaMemcpyHostToDevice, s));
-    if (c->prec == MB_PREC_F64) k_f64_to_field<double><<<gr, 256, 0, s>>>((double *)M[q], B.nx, B.ny, B.pitch, c->d_stage);
-    else k_f64_to_field<float><<<gr, 256, 0, s>>>((float *)M[q], B.nx, B.ny, B.pitch, c->d_stage);
-    MB_CUDA(cudaStreamSynchronize(s));
+    double *st = c->d_stage + (9 + q) * n;
+    MB_CUDA(cudaMemcpyAsync(st, H[q], n * sizeof(double), cudaMemcpyHostToDevice, s));
+    if (c->prec == MB_PREC_F64) k_f64_to_field<double><<<gr, 256, 0, s>>>((double *)M[q], B.nx, B.ny, B.pitch, st);
+    else k_f64_to_field<float><<<gr, 256, 0, s>>>((float *)M[q], B.nx, B.ny, B.pitch, st);
   }
+  MB_CUDA(cudaStreamSynchronize(s));  // the host arrays may be reused on return
   MB_CUDA(cudaGetLastError());
   return MB_OK;
 }

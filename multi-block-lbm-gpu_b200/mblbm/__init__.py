@@ -537,15 +537,25 @@ class MultiBlockLBM:
         self.lib.mb_check_finite(self.h, C.byref(bad), _stream_ptr(stream))
         return bad.value
 
-    def fields(self, area, stream=None):
-        """Dict of FP64 host arrays rho, ux, uy (ny, nx), F (9, ny, nx), solid (ny, nx)."""
+    def fields(self, area, stream=None, out=None):
+        """Dict of FP64 host arrays rho, ux, uy (ny, nx), F (9, ny, nx), solid (ny, nx).
+        out: a dict of preallocated C-contiguous arrays of those shapes (pinned
+        host memory makes the copies direct) to fill instead."""
         A = self.geo.Areas[area]
         nx, ny = A.nx, A.ny
-        rho = np.empty((ny, nx))
-        ux = np.empty((ny, nx))
-        uy = np.empty((ny, nx))
-        F = np.empty((9, ny, nx))
-        solid = np.empty((ny, nx), dtype=np.int32)
+        if out is not None:
+            rho, ux, uy, F, solid = (out[k] for k in ("rho", "ux", "uy", "F", "solid"))
+            for k, shp, dt in (("rho", (ny, nx), np.float64), ("ux", (ny, nx), np.float64), ("uy", (ny, nx), np.float64),
+                               ("F", (9, ny, nx), np.float64), ("solid", (ny, nx), np.int32)):
+                a = out[k]
+                if a.size != int(np.prod(shp)) or a.dtype != dt or not a.flags.c_contiguous:
+                    raise ValueError(f"out[{k!r}] must be a C-contiguous {dt.__name__} array of {shp}")
+        else:
+            rho = np.empty((ny, nx))
+            ux = np.empty((ny, nx))
+            uy = np.empty((ny, nx))
+            F = np.empty((9, ny, nx))
+            solid = np.empty((ny, nx), dtype=np.int32)
         _check(
             self.lib.mb_copy_fields(self.h, area, _dp(rho), _dp(ux), _dp(uy), _dp(F), solid.ctypes.data_as(_pi), _stream_ptr(stream)),
             "mb_copy_fields",
