@@ -1799,18 +1799,22 @@ __global__ void __launch_bounds__(1024) k_drag(const __grid_constant__ DragParam
 // pair to scratch; the last CTA to finish (ticket counter) sums the partials
 // in CTA order and resets the ticket, so the result is deterministic.
 // ----------------------------------------------------------------------------
+// One rectangle of cells of the L2 change: columns i0.., rows j0.. of block
+// blk.  error_L2 runs in two parts (the interiors of split levels, and every
+// other cell), each over its own list of boxes.
+constexpr int L2_MAX_BOXES = 4 * MB_MAX_AREA;
 struct L2Blk {
-  long long cell0;
-  int nx, pitch;
+  int blk, i0, j0;
+  int nx, pitch;  // box width; the block's pitch
   double inv_m;
-  int ny, rt0;    // rows; first row tile (256 cells of one row) of this block
-  int rtiles_x;   // row tiles per row
+  int ny, rt0;    // box rows; first row tile (256 cells of one box row) of this box
+  int rtiles_x;   // row tiles per box row
   int pad_;
 };
 struct L2Params {
   const L2Blk *blocks;
   const IfBlk *blk;
-  int nblk, ntiles;       // blocks; row tiles over all blocks
+  int nblk, ntiles;       // boxes; row tiles over all boxes
   long long total;
   double2 *partial;       // gridDim.x entries
   unsigned int *ticket;   // zero before the first launch; reset by the last CTA
@@ -1827,7 +1831,7 @@ constexpr int L2_ILP = 4;
 template <int P>
 __global__ void __launch_bounds__(256) k_error_l2(const __grid_constant__ L2Params p) {
   using R = typename Prec<P>::R;
-  __shared__ int s_rt0[MB_MAX_AREA];
+  __shared__ int s_rt0[L2_MAX_BOXES];
   for (int q = threadIdx.x; q < p.nblk; q += blockDim.x) s_rt0[q] = p.blocks[q].rt0;
   __syncthreads();
   double s1 = 0, s2 = 0;
@@ -1841,18 +1845,18 @@ __global__ void __launch_bounds__(256) k_error_l2(const __grid_constant__ L2Para
       const int t = t0 + u * stride;
       px[u] = nullptr;
       if (t >= p.ntiles) continue;
-      int lo = 0, hi = p.nblk - 1;  // last block whose first tile is <= t
+      int lo = 0, hi = p.nblk - 1;  // last box whose first tile is <= t
       while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
         if (s_rt0[mid] <= t) lo = mid; else hi = mid - 1;
       }
       const L2Blk &b = p.blocks[lo];
-      const IfBlk &B = p.blk[lo];
+      const IfBlk &B = p.blk[b.blk];
       const int lt = t - s_rt0[lo];
       const int j = lt / b.rtiles_x;
       const int i = (lt - j * b.rtiles_x) * 256 + (int)threadIdx.x;
       if (i >= b.nx) continue;
-      const int c = j * b.pitch + i;
+      const int c = (b.j0 + j) * b.pitch + b.i0 + i;
       ux[u] = ((const R *)B.ux)[c];
       uy[u] = ((const R *)B.uy)[c];
       upx[u] = ((const R *)B.upx)[c];

@@ -39,6 +39,13 @@ namespace {
 size_t prec_bytes(int prec) { return prec == MB_PREC_F64 ? 8 : (prec == MB_PREC_F16S ? 2 : 4); }
 size_t real_bytes(int prec) { return prec == MB_PREC_F64 ? 8 : 4; }
 
+// One part of error_L2 (interiors of split levels, or every other cell) as
+// boxes in device memory.
+struct L2Part {
+  L2Blk *d = nullptr;
+  int nbox = 0, ntiles = 0, grid = 0;
+};
+
 struct DevPlanNode {
   NodeKind kind;
   bool background = false;  // bandwidth-bound bulk work: lowest scheduling priority
@@ -50,6 +57,8 @@ struct DevPlanNode {
   StbParams stb;
   RecOpsParams rec;
   SplParamsP spl;
+  L2Params l2;
+  DragParams drag;
   void *args[1];
   std::vector<int> deps;
 };
@@ -62,6 +71,8 @@ struct CompiledPlan {
   cudaGraphExec_t exec = nullptr;
   SchedState end;
   long long kernels = 0;
+  double *d_diag_res = nullptr;  // diagnostic plans: Fx, Fy and the two L2 sums of both parts, per coarse step
+  int diag_steps = 0;
   // persistent executor (graph mode 3)
   bool prg_built = false;
   PrgArgs prg{};
@@ -102,9 +113,10 @@ struct mb_ctx {
   double *d_drag_out = nullptr;
   double *h_drag_out = nullptr;  // pinned
   // L2
-  L2Blk *d_l2blk = nullptr;
-  double2 *d_l2_partial = nullptr;
-  unsigned int *d_l2_ticket = nullptr;
+  // error_L2 in two parts (interiors of split levels, the rest), per split mask
+  std::map<unsigned, std::array<L2Part, 2>> l2parts;
+  double2 *d_l2_partial[2] = {nullptr, nullptr};  // per part: parts may run concurrently
+  unsigned int *d_l2_ticket[2] = {nullptr, nullptr};
   double *d_l2_out = nullptr;
   double *h_l2_out = nullptr;  // pinned
   int l2_grid = 0;
@@ -406,8 +418,102 @@ void stb_launch_shape(const mb_ctx *c, int level, int region, bool background, c
   *grid = dim3((unsigned)std::max<long long>(ctas, 0));
 }
 
+// The boxes of both error_L2 parts for a split mask (bit per level): part 0
+// the interiors (distance >= 2 from the block edge) of split levels, part 1
+// their rims and every cell of the other levels, blocks in order.
+int l2_parts(mb_ctx *c, unsigned mask, const L2Part **out) {
+  auto it = c->l2parts.find(mask);
+  if (it == c->l2parts.end()) {
+    std::array<L2Part, 2> parts;
+    const mb_layout &L = c->geo.layout;
+    for (int q = 0; q < 2; q++) {
+      std::vector<L2Blk> bx;
+      long long tiles = 0;
+      auto add = [&](int a, int i0, int j0, int w, int h) {
+        if (w <= 0 || h <= 0) return;
+        L2Blk b{};
+        b.blk = a;
+        b.i0 = i0;
+        b.j0 = j0;
+        b.nx = w;
+        b.ny = h;
+        b.pitch = c->bl[a].pitch;
+        b.inv_m = 1.0 / c->geo.Areas[a].m;
+        b.rtiles_x = (w + 255) / 256;
+        b.rt0 = (int)tiles;
+        tiles += (long long)b.rtiles_x * h;
+        bx.push_back(b);
+      };
+      for (int l = 0; l < L.LEVEL; l++) {
+        const bool sp = (mask >> l) & 1;
+        for (int a = L.ASP[l]; a < L.ASP[l + 1]; a++) {
+          const int nx = c->bl[a].nx, ny = c->bl[a].ny;
+          const bool inner = sp && nx > 4 && ny > 4;
+          if (q == 0) {
+            if (inner) add(a, 2, 2, nx - 4, ny - 4);
+          } else if (inner) {
+            add(a, 0, 0, nx, 2);
+            add(a, 0, ny - 2, nx, 2);
+            add(a, 0, 2, 2, ny - 4);
+            add(a, nx - 2, 2, 2, ny - 4);
+          } else {
+            add(a, 0, 0, nx, ny);
+          }
+        }
+      }
+      if ((int)bx.size() > L2_MAX_BOXES || tiles > c->l2_tiles) return MB_ERR_UNSUPPORTED;
+      L2Part &pt = parts[q];
+      pt.nbox = (int)bx.size();
+      pt.ntiles = (int)tiles;
+      pt.grid = (int)std::min<long long>(tiles, c->l2_grid);
+      if (!bx.empty()) {
+        if (int e = dalloc(c, &pt.d, bx.size())) return e;
+        MB_CUDA(cudaMemcpy(pt.d, bx.data(), bx.size() * sizeof(L2Blk), cudaMemcpyHostToDevice));
+      }
+    }
+    it = c->l2parts.emplace(mask, parts).first;
+  }
+  *out = it->second.data();
+  return MB_OK;
+}
+
+// CTAs of a part's launch: the interiors' part runs beside the fine levels'
+// chain with two CTAs per SM, so that the chain's launches find free slots
+// (the same grid everywhere: the sums' order follows the grid)
+int l2_grid_of(const mb_ctx *c, const L2Part *pt, int q) {
+  return q == 0 ? std::min(pt[q].grid, 2 * c->num_sms) : pt[q].grid;
+}
+
+L2Params l2_params(mb_ctx *c, const L2Part *pt, int q, double *out) {
+  L2Params p{};
+  p.blocks = pt[q].d;
+  p.blk = c->d_blk;
+  p.nblk = pt[q].nbox;
+  p.ntiles = pt[q].ntiles;
+  p.total = c->total_cells;
+  p.partial = c->d_l2_partial[q];
+  p.ticket = c->d_l2_ticket[q];
+  p.out = out;
+  return p;
+}
+
+// the levels the plans split into interior and rim nodes
+unsigned current_split_levels(const mb_ctx *c) {
+  PlanCompiler pc(c->geo, c->bl, c->hflags, c->spl_lines);
+  pc.split_cells = c->split_cells;
+  pc.split_mask = c->split_mask;
+  return pc.split_levels();
+}
+
 int lower_plan(mb_ctx *c, CompiledPlan &cp) {
   cp.dn.resize(cp.nodes.size());
+  for (const PlanNode &n : cp.nodes)
+    if (n.kind == NK_DRAG || n.kind == NK_L2) cp.diag_steps = std::max(cp.diag_steps, n.level + 1);
+  if (cp.diag_steps > 0) {  // zero: a part without cells adds nothing
+    if (cudaMalloc(&cp.d_diag_res, (size_t)cp.diag_steps * 6 * sizeof(double)) != cudaSuccess) return MB_ERR_NOMEM;
+    cp.dev_allocs.push_back(cp.d_diag_res);
+    MB_CUDA(cudaMemset(cp.d_diag_res, 0, (size_t)cp.diag_steps * 6 * sizeof(double)));
+  }
   for (size_t q = 0; q < cp.nodes.size(); q++) {
     const PlanNode &n = cp.nodes[q];
     DevPlanNode &d = cp.dn[q];
@@ -422,6 +528,30 @@ int lower_plan(mb_ctx *c, CompiledPlan &cp) {
       d.block = dim3(256);
       stb_launch_shape(c, n.level, n.region, d.background, d.stb, &d.func, &d.grid);
       d.args[0] = &d.stb;
+    } else if (n.kind == NK_L2) {
+      const int part = n.region == STB_INTERIOR ? 0 : 1;
+      const L2Part *pt = nullptr;
+      if (int e = l2_parts(c, (unsigned)n.a0, &pt)) return e;
+      d.l2 = l2_params(c, pt, part, cp.d_diag_res + 6 * n.level + 2 + 2 * part);
+      d.func = kfunc<KL2>(c->prec);
+      d.block = dim3(256);
+      d.grid = dim3((unsigned)l2_grid_of(c, pt, part));
+      d.background = part == 0;  // beside the fine levels' chain: bulk work
+      d.args[0] = &d.l2;
+    } else if (n.kind == NK_DRAG) {
+      const int a = c->drag_area;
+      const IfBlk &B = c->blk[a];
+      d.drag = DragParams{};
+      d.drag.links = c->d_links;
+      d.drag.n = c->n_drag;
+      d.drag.F = B.F[((n.parity >> a) & 1) ^ 1];  // the buffer the block's last step read
+      d.drag.plane = B.plane;
+      for (int k = 0; k < 9; k++) d.drag.feqc[k] = c->feqc[k];
+      d.drag.out = cp.d_diag_res + 6 * n.level;
+      d.func = kfunc<KDrag>(c->prec);
+      d.block = dim3(1024);
+      d.grid = dim3(1);
+      d.args[0] = &d.drag;
     } else if (n.kind == NK_CCP) {
       d.stb = make_stb(c, n.a0, n.a1, n.parity, 0, 1, STB_ALL, false, 0);
       d.stb.cc_list = c->d_cclist[n.level];
@@ -789,6 +919,30 @@ CompiledPlan *get_plan(mb_ctx *c, int n, bool final_macros, int *err, bool batch
   return raw;
 }
 
+// n coarse steps of the reference's main loop (a step, getDrag_block and
+// error_L2 each step) as one plan: the drag and the L2 change of a step run
+// beside the rest of the plan where their reads and writes allow.
+CompiledPlan *get_diag_plan(mb_ctx *c, int n, int *err) {
+  const bool fuse = c->fuse_cc && !options_on(c);
+  const std::string key = c->state.key() + "/" + std::to_string(n) + "D" + (fuse ? "c" : "");
+  auto it = c->plans.find(key);
+  if (it != c->plans.end()) return it->second.get();
+  auto cp = std::make_unique<CompiledPlan>();
+  PlanCompiler pc(c->geo, c->bl, c->hflags, c->spl_lines);
+  pc.split_cells = c->split_cells;
+  pc.split_mask = c->split_mask;
+  pc.drag_area = c->drag_area;
+  if (fuse) pc.cc = &c->cc;
+  SchedState s = c->state;
+  cp->nodes = pc.compile_diag(s, n);
+  cp->end = s;
+  *err = lower_plan(c, *cp);
+  if (*err) return nullptr;
+  CompiledPlan *raw = cp.get();
+  c->plans[key] = std::move(cp);
+  return raw;
+}
+
 int exec_plan(mb_ctx *c, CompiledPlan *cp, cudaStream_t s) {
   int e;
   if (c->use_graph == 3) {
@@ -1013,33 +1167,23 @@ extern "C" int mb_create(const mb_geometry *geo, int precision, mb_ctx **out) {
   MB_CUDA(cudaMallocHost(&c->h_drag_out, 2 * sizeof(double)));
 
   // L2 tables and scratch
-  {
-    std::vector<L2Blk> lb(c->nblk);
+  {  // tiles of 256 cells of one row: at most ceil(nx / 256) + 2 per row over both parts
     long long cell = 0, tiles = 0;
     for (int a = 0; a < c->nblk; a++) {
-      L2Blk &b = lb[a];
-      b = L2Blk{};
-      b.cell0 = cell;
-      b.nx = c->bl[a].nx;
-      b.pitch = c->bl[a].pitch;
-      b.inv_m = 1.0 / geo->Areas[a].m;
-      b.ny = c->bl[a].ny;
-      b.rtiles_x = (b.nx + 255) / 256;
-      b.rt0 = (int)tiles;
-      tiles += (long long)b.rtiles_x * b.ny;
+      tiles += (long long)((c->bl[a].nx + 255) / 256 + 2) * c->bl[a].ny;
       cell += (long long)c->bl[a].nx * c->bl[a].ny;
     }
     if (tiles >= (1LL << 31)) return MB_ERR_UNSUPPORTED;
     c->total_cells = cell;
     c->l2_tiles = (int)tiles;
-    if ((e = dalloc(c.get(), &c->d_l2blk, c->nblk))) return e;
-    MB_CUDA(cudaMemcpy(c->d_l2blk, lb.data(), lb.size() * sizeof(L2Blk), cudaMemcpyHostToDevice));
     c->l2_grid = (int)std::min<long long>(tiles, 148LL * 8);
-    if ((e = dalloc(c.get(), &c->d_l2_partial, c->l2_grid))) return e;
-    if ((e = dalloc(c.get(), &c->d_l2_ticket, 1))) return e;
-    MB_CUDA(cudaMemset(c->d_l2_ticket, 0, sizeof(unsigned int)));
-    if ((e = dalloc(c.get(), &c->d_l2_out, 2))) return e;
-    MB_CUDA(cudaMallocHost(&c->h_l2_out, 2 * sizeof(double)));
+    for (int q = 0; q < 2; q++) {
+      if ((e = dalloc(c.get(), &c->d_l2_partial[q], c->l2_grid))) return e;
+      if ((e = dalloc(c.get(), &c->d_l2_ticket[q], 1))) return e;
+      MB_CUDA(cudaMemset(c->d_l2_ticket[q], 0, sizeof(unsigned int)));
+    }
+    if ((e = dalloc(c.get(), &c->d_l2_out, 4))) return e;
+    MB_CUDA(cudaMallocHost(&c->h_l2_out, 4 * sizeof(double)));
   }
   if ((e = dalloc(c.get(), &c->d_count, 1))) return e;
 
@@ -1555,21 +1699,23 @@ int launch_drag(mb_ctx *c, double *out, cudaStream_t s) {
   return MB_OK;
 }
 
-// error_L2's kernel part: the two weighted sums into out[0..1] (device memory)
+// error_L2's kernel part: the two weighted sums of the interiors of the
+// split levels into out[0..1] (zero when there are none) and of every other
+// cell into out[2..3] (device memory); the host adds the parts in that order
 int launch_l2(mb_ctx *c, double *out, cudaStream_t s) {
-  L2Params p{};
-  p.blocks = c->d_l2blk;
-  p.blk = c->d_blk;
-  p.nblk = c->nblk;
-  p.ntiles = c->l2_tiles;
-  p.total = c->total_cells;
-  p.partial = c->d_l2_partial;
-  p.ticket = c->d_l2_ticket;
-  p.out = out;
-  void *args[] = {&p};
-  MB_CUDA(cudaLaunchKernel(kfunc<KL2>(c->prec), dim3(c->l2_grid), dim3(256), args, 0, s));
+  const L2Part *pt = nullptr;
+  if (int e = l2_parts(c, current_split_levels(c), &pt)) return e;
+  if (pt[0].grid == 0) MB_CUDA(cudaMemsetAsync(out, 0, 2 * sizeof(double), s));
+  for (int q = 0; q < 2; q++) {
+    if (pt[q].grid == 0) continue;
+    L2Params p = l2_params(c, pt, q, out + 2 * q);
+    void *args[] = {&p};
+    MB_CUDA(cudaLaunchKernel(kfunc<KL2>(c->prec), dim3(l2_grid_of(c, pt, q)), dim3(256), args, 0, s));
+  }
   return MB_OK;
 }
+
+double l2_value(const double *v) { return std::sqrt(v[0] + v[2]) / std::sqrt(v[1] + v[3]); }
 
 double drag_norm(const mb_ctx *c) {
   const mb_config &cfg = c->geo.config;
@@ -1606,10 +1752,10 @@ extern "C" int mb_error_L2(mb_ctx *c, double *e, mb_stream stream) {
   if (!c->inited) return MB_ERR_STATE;
   cudaStream_t s = (cudaStream_t)stream;
   if (int r = launch_l2(c, c->d_l2_out, s)) return r;
-  MB_CUDA(cudaMemcpyAsync(c->h_l2_out, c->d_l2_out, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  MB_CUDA(cudaMemcpyAsync(c->h_l2_out, c->d_l2_out, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
   MB_CUDA(cudaStreamSynchronize(s));
   if (int st = program_status(c)) return st;
-  *e = std::sqrt(c->h_l2_out[0]) / std::sqrt(c->h_l2_out[1]);
+  *e = l2_value(c->h_l2_out);
   return MB_OK;
 }
 
@@ -1629,29 +1775,44 @@ extern "C" int mb_step_diag(mb_ctx *c, int n, double *cd, double *cl, double *er
     c->h_diag = nullptr;
     c->diag_cap = 0;
     const size_t cap = std::max<size_t>((size_t)n, 2 * c->diag_cap);
-    if (cudaMalloc(&c->d_diag, cap * 4 * sizeof(double)) != cudaSuccess) return MB_ERR_NOMEM;
-    if (cudaMallocHost(&c->h_diag, cap * 4 * sizeof(double)) != cudaSuccess) return MB_ERR_NOMEM;
+    if (cudaMalloc(&c->d_diag, cap * 6 * sizeof(double)) != cudaSuccess) return MB_ERR_NOMEM;
+    if (cudaMallocHost(&c->h_diag, cap * 6 * sizeof(double)) != cudaSuccess) return MB_ERR_NOMEM;
     c->diag_cap = cap;
   }
   c->kernels_last_call = 0;
-  for (int q = 0; q < n; q++) {
-    int e = 0;
-    CompiledPlan *cp = get_plan(c, 1, true, &e);
-    if (!cp) return e ? e : MB_ERR_INVALID;
-    if ((e = exec_plan(c, cp, s))) return e;
-    if ((e = launch_drag(c, c->d_diag + 4 * q, s))) return e;
-    if ((e = launch_l2(c, c->d_diag + 4 * q + 2, s))) return e;
-    MB_CUDA(cudaMemcpyAsync(c->h_diag + 4 * q, c->d_diag + 4 * q, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
-    c->kernels_last_call += 2;
+  if (c->use_graph != 3) {
+    // plans of `period` steps with their diagnostics; each plan's results go
+    // to the host with one copy
+    for (int q = 0; q < n;) {
+      const int chunk = (n - q >= c->period) ? c->period : 1;
+      int e = 0;
+      CompiledPlan *cp = get_diag_plan(c, chunk, &e);
+      if (!cp) return e ? e : MB_ERR_INVALID;
+      if ((e = exec_plan(c, cp, s))) return e;
+      MB_CUDA(cudaMemcpyAsync(c->h_diag + 6 * q, cp->d_diag_res, (size_t)chunk * 6 * sizeof(double),
+                              cudaMemcpyDeviceToHost, s));
+      q += chunk;
+    }
+  } else {
+    for (int q = 0; q < n; q++) {
+      int e = 0;
+      CompiledPlan *cp = get_plan(c, 1, true, &e);
+      if (!cp) return e ? e : MB_ERR_INVALID;
+      if ((e = exec_plan(c, cp, s))) return e;
+      if ((e = launch_drag(c, c->d_diag + 6 * q, s))) return e;
+      if ((e = launch_l2(c, c->d_diag + 6 * q + 2, s))) return e;
+      MB_CUDA(cudaMemcpyAsync(c->h_diag + 6 * q, c->d_diag + 6 * q, 6 * sizeof(double), cudaMemcpyDeviceToHost, s));
+      c->kernels_last_call += 2;
+    }
   }
   MB_CUDA(cudaStreamSynchronize(s));
   if (int st = program_status(c)) return st;
   const double den = drag_norm(c);
   for (int q = 0; q < n; q++) {
-    const double *v = c->h_diag + 4 * q;
+    const double *v = c->h_diag + 6 * q;
     if (cd) cd[q] = v[0] / den;
     if (cl) cl[q] = v[1] / den;
-    if (err) err[q] = std::sqrt(v[2]) / std::sqrt(v[3]);
+    if (err) err[q] = l2_value(v + 2);
   }
   MB_CUDA(cudaGetLastError());
   return MB_OK;

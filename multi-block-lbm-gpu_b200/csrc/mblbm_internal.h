@@ -72,7 +72,11 @@ struct SplTask {
   int mask_off;   // offset into the node's M-write mask (-1: write all points)
 };
 
-enum NodeKind { NK_STB = 0, NK_REC = 1, NK_SPL = 2, NK_CCP = 3 };  // NK_CCP: same-level copies beside a block step
+// NK_CCP: same-level copies beside a block step.  NK_DRAG: getDrag_block of
+// a coarse step; NK_L2: one part of its error_L2 (region STB_INTERIOR: the
+// interiors of the split levels in a0's bit mask, else every other cell);
+// `level` holds the step's index within the plan for both.
+enum NodeKind { NK_STB = 0, NK_REC = 1, NK_SPL = 2, NK_CCP = 3, NK_DRAG = 5, NK_L2 = 6 };
 // cells a block-step node updates: all, those at distance >= 2 from the block
 // edge (they read nothing an interface op writes), or the distance <= 1 rim
 enum StbRegion { STB_ALL = 0, STB_INTERIOR = 1, STB_RIM = 2 };
@@ -110,7 +114,9 @@ struct BlockLayout {
 
 // One call of the reference scheduler: a block step of a level or one line op.
 struct Op {
-  enum Kind { STB = 0, CC = 1, TEMPORAL = 2, CF = 3, FC = 4, SPL = 5 } kind;
+  // DRAG, L2: the per-step diagnostics of a diagnostic plan (line = the coarse
+  // step's index within the plan; level = the part of an L2 op)
+  enum Kind { STB = 0, CC = 1, TEMPORAL = 2, CF = 3, FC = 4, SPL = 5, DRAG = 7, L2 = 8 } kind;
   int level = -1, line = -1;
   double xm = 0;
   int macro_all = 0;
@@ -153,6 +159,12 @@ struct PlanCompiler {
                const std::vector<std::vector<uint8_t>> &fl, const std::vector<SplLine> &sl)
       : g(g_), bl(bl_), flags(fl), spl_lines(sl) {}
   std::vector<PlanNode> compile(SchedState &s, int n_coarse, bool final_macros) const;
+  // n coarse steps, each with rho/u of every FLUID cell written and followed
+  // by its drag and relative L2 change (the reference's main loop,
+  // Multi-block-LBM.cu:148-158)
+  std::vector<PlanNode> compile_diag(SchedState &s, int n_coarse) const;
+  int drag_area = -1;  // block of getDrag_block (compile_diag)
+  unsigned split_levels() const;  // levels stepped as interior and rim nodes (bit per level)
   // one reference call (Op::Kind, level or line index) at state s, state unchanged
   std::vector<PlanNode> compile_single(int kind, int index, double xm, const SchedState &s) const;
   // line ops expanded into launches (REC / SPL batches, STB nodes) with DAG edges

@@ -38,7 +38,8 @@ std::string SchedState::key() const {
 namespace {
 
 // resource kinds of an access key
-enum : uint64_t { RK_F0 = 0, RK_F1 = 1, RK_M = 2, RK_SLOT = 3 };
+// RK_UP: u_prev of error_L2; RK_DIAG: the per-step diagnostic results
+enum : uint64_t { RK_F0 = 0, RK_F1 = 1, RK_M = 2, RK_SLOT = 3, RK_UP = 5, RK_DIAG = 6 };
 
 inline uint64_t key(uint64_t kind, uint64_t owner, uint64_t idx) { return (kind << 56) | (owner << 48) | idx; }
 inline uint32_t summ(uint64_t k) { return uint32_t(k >> 48); }  // kind<<8 | owner
@@ -271,6 +272,42 @@ std::vector<PlanNode> PlanCompiler::compile(SchedState &s, int n_coarse, bool fi
   return build(ops);
 }
 
+unsigned PlanCompiler::split_levels() const {
+  const mb_layout &L = g.layout;
+  unsigned m = 0;
+  for (int l = 0; l < L.LEVEL; l++) {
+    long long cells = 0;
+    for (int a = L.ASP[l]; a < L.ASP[l + 1]; a++) cells += (long long)bl[a].nx * bl[a].ny;
+    if (split_mask ? ((split_mask >> l) & 1u) != 0 : cells >= split_cells) m |= 1u << l;
+  }
+  return m;
+}
+
+// error_L2 runs in two parts: the interiors of split levels (which only
+// their block step writes, so the part runs beside the rest of the step and
+// the next step's interior waits for nothing else) and every other cell.
+std::vector<PlanNode> PlanCompiler::compile_diag(SchedState &s, int n_coarse) const {
+  std::vector<Op> ops;
+  const bool any_split = split_levels() != 0;
+  for (int n = 0; n < n_coarse; n++) {
+    emit(g, 0, s, ops, true);
+    for (int part = any_split ? 0 : 1; part < 2; part++) {
+      Op o;
+      o.kind = Op::L2;
+      o.level = part;  // 0: interiors of split levels, 1: the rest
+      o.line = n;
+      o.parity = s.parity;
+      ops.push_back(o);
+    }
+    Op o;
+    o.kind = Op::DRAG;
+    o.line = n;
+    o.parity = s.parity;
+    ops.push_back(o);
+  }
+  return build(ops);
+}
+
 std::vector<PlanNode> PlanCompiler::compile_single(int kind, int index, double xm, const SchedState &s) const {
   Op o;
   o.kind = Op::Kind(kind);
@@ -319,6 +356,7 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
     bool cc_fused = false;      // STB: its level's same-level copies run beside it (cc_nodes)
     std::vector<int> stb_nodes; // STB: its nodes
     std::vector<int> cc_nodes;  // STB: NK_CCP nodes, one per launch chunk with copies
+    int diag = -1;              // SNAP / DRAG / L2 op: its Op::Kind
     int level = -1;
     std::vector<int> parity;
     std::vector<Part> parts;
@@ -353,6 +391,25 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
   for (size_t oi = 0; oi < ops.size(); oi++) {
     const Op &o = ops[oi];
     OpInfo &I = info[oi];
+    if (o.kind == Op::DRAG || o.kind == Op::L2) {
+      open = -1;
+      I.diag = int(o.kind);
+      I.parity = o.parity;
+      PlanNode nd;
+      nd.kind = o.kind == Op::DRAG ? NK_DRAG : NK_L2;
+      nd.level = o.line;
+      if (o.kind == Op::L2) {
+        nd.region = o.level == 0 ? STB_INTERIOR : STB_RIM;  // the part
+        nd.a0 = int(split_levels());
+      }
+      for (int a = 0; a < L.number_area; a++)
+        if (o.parity[a]) nd.parity |= (1ull << a);
+      nd.label = o.kind == Op::DRAG ? "drag" : (o.level == 0 ? "l2 int" : "l2");
+      I.node = int(nodes.size());
+      nodes.push_back(nd);
+      acc.push_back(Access());
+      continue;
+    }
     if (o.kind == Op::STB) {
       open = -1;
       last_stb = int(oi);
@@ -360,9 +417,7 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
       I.stb = true;
       I.level = o.level;
       I.parity = o.parity;
-      long long level_cells = 0;
-      for (int a = L.ASP[o.level]; a < L.ASP[o.level + 1]; a++) level_cells += (long long)bl[a].nx * bl[a].ny;
-      const bool split = split_mask ? ((split_mask >> o.level) & 1u) != 0 : level_cells >= split_cells;
+      const bool split = ((split_levels() >> o.level) & 1u) != 0;
       for (int a0 = L.ASP[o.level]; a0 < L.ASP[o.level + 1]; a0 += 16) {
         const int a1 = std::min(L.ASP[o.level + 1], a0 + 16);
         for (int region : split ? std::vector<int>{STB_RIM, STB_INTERIOR} : std::vector<int>{STB_ALL}) {
@@ -683,6 +738,21 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
   };
   for (int oi = int(ops.size()) - 1; oi >= 0; oi--) {
     OpInfo &I = info[oi];
+    if (I.diag == Op::L2) {  // reads rho/u of the cells of its part
+      const PlanNode &nd = nodes[I.node];
+      for (int l = 0; l < L.LEVEL; l++) {
+        const bool sp = (nd.a0 >> l) & 1;
+        if (nd.region == STB_INTERIOR && !sp) continue;
+        const uint8_t lo = nd.region == STB_INTERIOR ? 2 : 0, hi = (nd.region == STB_RIM && sp) ? 1 : DMAX;
+        for (int a = L.ASP[l]; a < L.ASP[l + 1]; a++) apply_layer({uint32_t((RK_M << 8) | a), false, lo, hi}, false);
+      }
+      continue;
+    }
+    if (I.diag == Op::DRAG) {  // reads the buffer the drag block's last step read
+      const int a = drag_area, p = I.parity[a] ^ 1;
+      apply_layer({uint32_t(((p ? RK_F1 : RK_F0) << 8) | a), false, 0, DMAX}, false);
+      continue;
+    }
     if (I.stb) {
       // the op's nodes together write F of buffer 1-p and rho/u of FLUID
       // cells and read F of buffer p, over the whole block
@@ -751,7 +821,29 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
     }
   }
   for (auto &I : info) {
-    if (I.stb || I.node < 0) continue;
+    if (I.diag < 0) continue;
+    Access &A = fin[I.node];
+    if (I.diag == Op::L2) {
+      const PlanNode &nd = nodes[I.node];
+      for (int l = 0; l < L.LEVEL; l++) {
+        const bool sp = (nd.a0 >> l) & 1;
+        if (nd.region == STB_INTERIOR && !sp) continue;
+        const uint8_t lo = nd.region == STB_INTERIOR ? 2 : 0, hi = (nd.region == STB_RIM && sp) ? 1 : DMAX;
+        for (int a = L.ASP[l]; a < L.ASP[l + 1]; a++) {
+          A.read_whole(uint32_t((RK_M << 8) | a), lo, hi);
+          A.read_whole(uint32_t((RK_UP << 8) | a), lo, hi);
+          A.write_whole(uint32_t((RK_UP << 8) | a), false, lo, hi);
+        }
+      }
+      A.write(key(RK_DIAG, 0, 3 * nd.level + 1 + (nd.region == STB_INTERIOR ? 0 : 1)));
+    } else {
+      const int a = drag_area, p = I.parity[a] ^ 1;
+      A.read_whole(uint32_t(((p ? RK_F1 : RK_F0) << 8) | a));
+      A.write(key(RK_DIAG, 0, 3 * nodes[I.node].level));
+    }
+  }
+  for (auto &I : info) {
+    if (I.stb || I.node < 0 || I.diag >= 0) continue;
     Access &A = fin[I.node];
     for (auto &pt : I.parts) {
       if (!pt.live) continue;

@@ -348,21 +348,28 @@ def test_checkpoint_restart_bitwise(mb, cuda_device, tmp_path):
         c.restore((tmp_path / "ck.bin").read_bytes())
 
 
-@pytest.mark.parametrize("prec", ["f32", "f64"])
-def test_step_diag_equals_step_by_step(mb, cuda_device, prec):
-    """mb_step_diag gives the values of mb_step(1), mb_drag and mb_error_L2
-    called in turn, bitwise, and the same final state."""
+@pytest.mark.parametrize("graph", [True, False])
+@pytest.mark.parametrize("split", [10**12, 0])
+@pytest.mark.parametrize("prec", ["f32", "f64", "f16s"])
+def test_step_diag_equals_step_by_step(mb, cuda_device, prec, split, graph):
+    """mb_step_diag (plans of several steps with the drag and the L2 change of
+    each step beside the next) gives the values of mb_step(1), mb_drag and
+    mb_error_L2 called in turn, bitwise, and the same final state, over two
+    calls in a row."""
     g = mb.geo_init(*make_ref.case("n3")[:2])
-    a = mb.MultiBlockLBM(g, prec)
-    b = mb.MultiBlockLBM(g, prec)
-    a.init()
-    b.init()
+    a = mb.MultiBlockLBM(g, prec, graph=graph)
+    b = mb.MultiBlockLBM(g, prec, graph=graph)
+    for s in (a, b):
+        s.set_split_cells(split)
+        s.init()
     ref = []
-    for _ in range(9):
+    for _ in range(17):
         a.evolution(1)
         _, _, cd, cl = a.getDrag_block()
         ref.append((cd, cl, a.error_L2()))
-    cd, cl, err = b.evolution_diag(9)
+    cd1, cl1, err1 = b.evolution_diag(13)
+    cd2, cl2, err2 = b.evolution_diag(4)
+    cd, cl, err = np.concatenate([cd1, cd2]), np.concatenate([cl1, cl2]), np.concatenate([err1, err2])
     assert np.array_equal(cd, [r[0] for r in ref])
     assert np.array_equal(cl, [r[1] for r in ref])
     assert np.array_equal(err, [r[2] for r in ref])
