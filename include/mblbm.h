@@ -243,7 +243,10 @@ int mb_set_stream_cells(mb_ctx *ctx, long long cells, int bulk);
  * the loads of both in flight together, 3 = cell ranges: a CTA steps 256
  * consecutive cells of one block with 32-bit offsets (whole levels and
  * interiors; rims use 0), 4 = cell pairs: a thread steps cells i, i+1 with
- * shared addresses and vector accesses, 256 pairs per CTA (same coverage as 3).
+ * shared addresses and vector accesses, 256 pairs per CTA (same coverage as 3),
+ * 5 = bulk asynchronous copies: persistent CTAs stage the nine input row
+ * segments of 256 cells in shared memory with cp.async.bulk and mbarriers
+ * (interiors of split levels; the other regions use 0).
  * Default 0; level 0 uses 3 in MB_PREC_F16S and 1 in MB_PREC_F32 and
  * MB_PREC_F32U.  Results are identical. */
 int mb_set_stb_variant(mb_ctx *ctx, int level, int variant);

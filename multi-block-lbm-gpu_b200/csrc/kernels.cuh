@@ -109,6 +109,10 @@ struct StbBlk {
   int pcta0, npairs;
   int ppr;
   float pinv;         // 1 / ppr
+  // bulk-copy kernel (interior region): items tb0.. of 256 cells of one row,
+  // tb_tiles per row (tiles start at column 0, multiples of 256)
+  long long tb0;
+  int tb_tiles, pad3_;
   int pad2_;
   double dt;          // 1 / m: time step of the block in coarse units (body-force term)
 };
@@ -139,6 +143,8 @@ struct StbParams {
   int a0;            // global index of b[0]
   const CcEntry *cc_list;  // k_cc_pull: the copies of the launch
   int cc_n, pad_cc;
+  long long tb_items;      // bulk-copy kernel: items of the launch
+  unsigned int *err_host;  // error word (mapped host memory) of bounded waits
   long long total;   // cells in the launch (per-cell kernel) or warp tiles (quad kernel)
   long long rctas;   // CTAs of a range-kernel launch
   long long pctas;   // CTAs of a pair-kernel launch
@@ -851,6 +857,179 @@ __global__ void __launch_bounds__(256, P == MB_PREC_F64 ? 2 : 4) k_block_step_p(
   const bool two = 2 * q + 1 < B.rw;
   if (p.evict_first) stb_pair<P, true, INTERIOR>(p, B, i, j, two);
   else stb_pair<P, false, INTERIOR>(p, B, i, j, two);
+}
+
+// ----------------------------------------------------------------------------
+// The block step of split levels' interiors with bulk asynchronous copies:
+// a persistent CTA (8 consumer warps and one producer warp) walks items of
+// 256 output cells of one row (row-major over the interiors of its blocks,
+// items round-robin over the CTAs).  For an item the producer's elected lane
+// brings the nine input row segments (plane k at row j - e_y(k), columns
+// x0 - A .. x0 + 256 + A, A = 16 bytes of stored words, clamped to the row)
+// and the row's flag bytes into a shared-memory stage with cp.async.bulk
+// (TMA without a tensor map) completing on the stage's mbarrier; consumers
+// pull their cell's values from the stage, collide and store to global
+// memory, then release the stage.  STAGES stages keep that many items' loads
+// in flight per CTA without holding registers.  Cells that are not interior
+// FLUID cells take the general per-cell path from global memory.
+// Every mbarrier wait is bounded: a wait that runs out sets the error word
+// (mb_sync and the other synchronising calls then return MB_ERR_TIMEOUT) and
+// the CTA stops after waiting, again bounded, for the copies it issued.
+// ----------------------------------------------------------------------------
+constexpr int TB_TW = 256;                   // output cells per item
+constexpr int TB_THREADS = 288;              // 8 consumer warps + the producer warp
+constexpr unsigned TB_SPIN_LIMIT = 1u << 22; // bounded waits: about a second with the sleeps
+template <typename S> struct TbCfg {
+  static constexpr int A = 16 / (int)sizeof(S);      // halo, rounded up to 16 bytes
+  static constexpr int SEG = TB_TW + 2 * A;          // stored words per row segment
+  static constexpr int SEG_BYTES = SEG * (int)sizeof(S);
+  static constexpr int FLAG_BYTES = TB_TW + 32;      // flag bytes x0 - 16 .. x0 + 256 + 16
+  static constexpr int STAGE_BYTES = 9 * SEG_BYTES + FLAG_BYTES;
+  // two CTAs per SM leave room for a spline CTA's 96 KB (mb_set_cta_spread)
+  static constexpr int STAGES = sizeof(S) == 2 ? 12 : (sizeof(S) == 4 ? 6 : 4);
+  static constexpr int SMEM = STAGES * STAGE_BYTES + 2 * STAGES * 8;
+};
+static_assert(TbCfg<__half>::SEG_BYTES % 16 == 0 && TbCfg<float>::SEG_BYTES % 16 == 0 &&
+                  TbCfg<double>::SEG_BYTES % 16 == 0 && TbCfg<float>::FLAG_BYTES % 16 == 0,
+              "bulk copies need 16-byte sizes and offsets");
+
+__device__ __forceinline__ void tb_mbar_init(uint64_t *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"((unsigned)__cvta_generic_to_shared(bar)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void tb_mbar_expect_tx(uint64_t *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
+                   (unsigned)__cvta_generic_to_shared(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void tb_mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"((unsigned)__cvta_generic_to_shared(bar)) : "memory");
+}
+// bounded wait for the phase of the given parity to complete; false when it ran out
+__device__ __forceinline__ bool tb_mbar_wait(uint64_t *bar, unsigned parity) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+  for (unsigned n = 0; n < TB_SPIN_LIMIT; n++) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (n > 4096) __nanosleep(128);
+  }
+  return false;
+}
+__device__ __forceinline__ void tb_bulk_load(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          (unsigned)__cvta_generic_to_shared(dst)),
+      "l"(src), "r"(bytes), "r"((unsigned)__cvta_generic_to_shared(bar))
+      : "memory");
+}
+
+// item n of a launch: block t, row j, first column x0 of the tile
+__device__ __forceinline__ void tb_locate(const StbParams &p, long long it, int &t, int &j, int &x0) {
+  t = 0;
+#pragma unroll 1
+  while (t + 1 < p.nblk && it >= p.b[t + 1].tb0) t++;
+  const StbBlk &B = p.b[t];
+  const int local = int(it - B.tb0);
+  const int r = local / B.tb_tiles;
+  j = 2 + r;
+  x0 = (local - r * B.tb_tiles) * TB_TW;
+}
+
+template <int P>
+__global__ void __launch_bounds__(TB_THREADS, 1) k_block_step_tb(const __grid_constant__ StbParams p) {
+  using R = typename Prec<P>::R;
+  using S = typename Prec<P>::S;
+  using C = TbCfg<S>;
+  extern __shared__ __align__(128) unsigned char tb_smem[];
+  uint64_t *full = (uint64_t *)(tb_smem + C::STAGES * C::STAGE_BYTES);
+  uint64_t *empty = full + C::STAGES;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (tid == 0) {
+    for (int s = 0; s < C::STAGES; s++) {
+      tb_mbar_init(&full[s], 1);   // the producer's expect_tx arrival (+ the bytes)
+      tb_mbar_init(&empty[s], 8);  // one arrival per consumer warp
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  pdl_trigger();
+  pdl_wait();
+  const long long items = p.tb_items;
+  if (warp == 8) {  // producer
+    if (lane != 0) return;
+    long long n = 0;
+    bool ok = true;
+    for (long long it = blockIdx.x; it < items; it += gridDim.x, n++) {
+      const int s = int(n % C::STAGES);
+      const unsigned ph = unsigned((n / C::STAGES) & 1);
+      if (n >= C::STAGES && !tb_mbar_wait(&empty[s], ph ^ 1u)) { ok = false; break; }
+      int t, j, x0;
+      tb_locate(p, it, t, j, x0);
+      const StbBlk &B = p.b[t];
+      unsigned char *st = tb_smem + (size_t)s * C::STAGE_BYTES;
+      const S *Fin = (const S *)B.Fin;
+      const int lo = max(x0 - C::A, 0), hi = min(x0 + TB_TW + C::A, B.pitch);
+      const int flo = max(x0 - 16, 0), fhi = min(x0 + TB_TW + 16, B.pitch);
+      const unsigned seg = unsigned(hi - lo) * (unsigned)sizeof(S), fseg = unsigned(fhi - flo);
+      tb_mbar_expect_tx(&full[s], 9u * seg + fseg);
+#pragma unroll
+      for (int k = 0; k < 9; k++) {
+        const S *src = Fin + (long long)k * B.plane + (long long)(j - ey(k)) * B.pitch + lo;
+        tb_bulk_load(st + k * C::SEG_BYTES + (lo - (x0 - C::A)) * (int)sizeof(S), src, seg, &full[s]);
+      }
+      tb_bulk_load(st + 9 * C::SEG_BYTES + (flo - (x0 - 16)), B.flags + (long long)j * B.pitch + flo, fseg, &full[s]);
+    }
+    // every issued stage completes before the CTA may end
+    const long long issued = n;
+    for (long long q = (issued > C::STAGES ? issued - C::STAGES : 0); q < issued; q++)
+      if (!tb_mbar_wait(&full[q % C::STAGES], unsigned((q / C::STAGES) & 1))) ok = false;
+    if (!ok && p.err_host) atomicOr(p.err_host, 2u);
+    return;
+  }
+  // consumers
+  long long n = 0;
+  for (long long it = blockIdx.x; it < items; it += gridDim.x, n++) {
+    const int s = int(n % C::STAGES);
+    const unsigned ph = unsigned((n / C::STAGES) & 1);
+    if (!tb_mbar_wait(&full[s], ph)) {
+      if (lane == 0 && p.err_host) atomicOr(p.err_host, 2u);
+      break;
+    }
+    int t, j, x0;
+    tb_locate(p, it, t, j, x0);
+    const StbBlk &B = p.b[t];
+    const unsigned char *st = tb_smem + (size_t)s * C::STAGE_BYTES;
+    const int i = x0 + tid;
+    if (i >= 2 && i <= B.nx - 3) {
+      const uint8_t fl = st[9 * C::SEG_BYTES + 16 + tid];
+      if ((fl & 7) == 0) {
+        R f[9];
+#pragma unroll
+        for (int k = 0; k < 9; k++) f[k] = to_r(((const S *)(st + k * C::SEG_BYTES))[tid + C::A - ex(k)]);
+        R out[9], m[3];
+        stb_collide<P>(f, (R)B.rv_tau, out, m);
+        const long long c = (long long)j * B.pitch + i;
+        if (p.write_macros && (p.macro_all || (fl & 8))) {
+          ((R *)B.rho)[c] = m[0];
+          ((R *)B.ux)[c] = m[1];
+          ((R *)B.uy)[c] = m[2];
+        }
+        S *Fout = (S *)B.Fout;
+#pragma unroll
+        for (int k = 0; k < 9; k++) Fout[k * B.plane + c] = from_r<S>(out[k]);
+      } else {
+        stb_cell_slow<P, false>(p, B, i, j);
+      }
+    }
+    __syncwarp();
+    if (lane == 0) tb_mbar_arrive(&empty[s]);
+  }
 }
 
 // Four consecutive cells of a row in the stored form, as arithmetic values

@@ -149,6 +149,7 @@ struct mb_ctx {
   int bulk_levels = 0;                // 1: whole-level block steps that stream with hints are bulk (low priority) work   // block steps over >= this many cells use evict-first cache hints (0: never)
   int stb_variant[MB_MAX_LEVEL] = {0};  // 0: one cell per thread, 1: quads (k_block_step_q)
   int bulk_ctas_per_sm = 0;             // >0: cap interior (bulk) block-step grids at this many CTAs per SM
+  int tb_ctas_per_sm = 2;               // persistent CTAs per SM of the bulk-copy block step (variant 5)
   int num_sms = 148;
   // persistent executor
   unsigned int *d_prg_err = nullptr;    // device error word of k_program
@@ -272,6 +273,14 @@ template <int P> struct KStbPI { static void *ptr() { return (void *)k_block_ste
 template <int P> struct KStbQ { static void *ptr() { return (void *)k_block_step_q<P>; } };
 template <int P> struct KStbX { static void *ptr() { return (void *)k_block_step_x<P>; } };
 template <int P> struct KCcp { static void *ptr() { return (void *)k_cc_pull<P>; } };
+template <int P> struct KStbTb { static void *ptr() { return (void *)k_block_step_tb<P>; } };
+int tb_smem(int prec) {
+  switch (prec) {
+    case MB_PREC_F64: return TbCfg<double>::SMEM;
+    case MB_PREC_F16S: return TbCfg<__half>::SMEM;
+    default: return TbCfg<float>::SMEM;
+  }
+}
 template <int P> struct KRec { static void *ptr() { return (void *)k_records<P>; } };
 template <int P> struct KSpl { static void *ptr() { return (void *)k_spline<P>; } };
 template <int P> struct KDrag { static void *ptr() { return (void *)k_drag<P>; } };
@@ -313,6 +322,7 @@ StbParams make_stb(mb_ctx *c, int a0, int a1, uint64_t parity, int macro_all, in
   p.nblk = a1 - a0;
   p.a0 = a0;
   p.ccpull = ccpull;
+  p.err_host = c->d_prg_err_host;
   p.macro_all = macro_all;
   p.write_macros = write_macros;
   p.region = region;
@@ -321,7 +331,7 @@ StbParams make_stb(mb_ctx *c, int a0, int a1, uint64_t parity, int macro_all, in
   p.u0x = c->geo.config.U0[0];
   p.u0y = c->geo.config.U0[1];
   p.opt = c->opt;
-  long long cell = 0, wt = 0, rt = 0, pt = 0, level_cells = 0;
+  long long cell = 0, wt = 0, rt = 0, pt = 0, tb = 0, level_cells = 0;
   for (int a = a0; a < a1; a++) level_cells += region_cells(c->blk[a].nx, c->blk[a].ny, region);
   p.evict_first = c->stream_cells > 0 && level_cells >= c->stream_cells;
   for (int a = a0; a < a1; a++) {
@@ -361,7 +371,12 @@ StbParams make_stb(mb_ctx *c, int a0, int a1, uint64_t parity, int macro_all, in
     s.pinv = s.ppr > 0 ? 1.0f / (float)s.ppr : 0.f;
     s.pcta0 = (int)pt;
     pt += (s.npairs + 255) / 256;
+    // bulk-copy kernel: interior rows 2..ny-3 in tiles of 256 columns from column 0
+    s.tb0 = tb;
+    s.tb_tiles = (B.nx > 4 && B.ny > 4) ? (B.nx - 2 + TB_TW - 1) / TB_TW : 0;
+    tb += (long long)s.tb_tiles * std::max(0, B.ny - 4);
   }
+  p.tb_items = tb;
   p.rctas = rt;
   p.pctas = pt;
   p.total = quads ? wt : cell;
@@ -398,6 +413,12 @@ void stb_launch_shape(const mb_ctx *c, int level, int region, bool background, c
   if (stb_uses_quads(c, level, region)) {
     *func = kfunc<KStbQ>(c->prec);
     *grid = dim3((unsigned)((p.total + 7) / 8));  // 8 warp tiles per CTA
+    return;
+  }
+  if (c->stb_variant[level] == 5 && region == STB_INTERIOR && p.tb_items > 0) {
+    *func = kfunc<KStbTb>(c->prec);
+    const int per_sm = c->bulk_ctas_per_sm > 0 ? c->bulk_ctas_per_sm : c->tb_ctas_per_sm;
+    *grid = dim3((unsigned)std::min<long long>(p.tb_items, (long long)c->num_sms * per_sm));
     return;
   }
   if (c->stb_variant[level] == 4 && region != STB_RIM && !background_capped(c, background) && rows_fit(c, p)) {
@@ -527,6 +548,10 @@ int lower_plan(mb_ctx *c, CompiledPlan &cp) {
       d.background = (n.region == STB_INTERIOR) || (c->bulk_levels && n.region == STB_ALL && d.stb.evict_first);
       d.block = dim3(256);
       stb_launch_shape(c, n.level, n.region, d.background, d.stb, &d.func, &d.grid);
+      if (d.func == kfunc<KStbTb>(c->prec)) {
+        d.block = dim3(TB_THREADS);
+        d.smem = (size_t)tb_smem(c->prec);
+      }
       d.args[0] = &d.stb;
     } else if (n.kind == NK_L2) {
       const int part = n.region == STB_INTERIOR ? 0 : 1;
@@ -740,6 +765,7 @@ int set_smem_limits(int prec) {
   MB_CUDA(cudaFuncSetAttribute(kfunc<KSpl>(prec), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)std::max(spline_smem(prec), (size_t)MB_CTA_SMEM_MAX)));
   MB_CUDA(cudaFuncSetAttribute(kfunc<KRec>(prec), cudaFuncAttributeMaxDynamicSharedMemorySize, MB_CTA_SMEM_MAX));
+  MB_CUDA(cudaFuncSetAttribute(kfunc<KStbTb>(prec), cudaFuncAttributeMaxDynamicSharedMemorySize, tb_smem(prec)));
   MB_CUDA(cudaFuncSetAttribute(kfunc<KPrg>(prec), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)program_smem(prec)));
   MB_CUDA(cudaFuncSetAttribute(kfunc<KPrgT>(prec), cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1298,7 +1324,7 @@ extern "C" int mb_set_stream_cells(mb_ctx *c, long long cells, int bulk) {
 }
 
 extern "C" int mb_set_stb_variant(mb_ctx *c, int level, int variant) {
-  if (!c || level < 0 || level >= c->geo.layout.LEVEL || variant < 0 || variant > 4) return MB_ERR_INVALID;
+  if (!c || level < 0 || level >= c->geo.layout.LEVEL || variant < 0 || variant > 5) return MB_ERR_INVALID;
   cudaDeviceSynchronize();
   c->stb_variant[level] = variant;
   c->plans.clear();

@@ -286,7 +286,7 @@ def test_interior_rim_split(mb, orc, cuda_device, name):
 
 
 @pytest.mark.parametrize("split", [0, 10**12])
-@pytest.mark.parametrize("variant", [1, 2, 3, 4])
+@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5])
 @pytest.mark.parametrize("prec", ["f32", "f16s", "f64"])
 def test_quad_kernel_equals_cell_kernel(mb, cuda_device, prec, variant, split):
     """Every block-step variant gives bitwise the same state, on whole levels
