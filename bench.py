@@ -233,6 +233,8 @@ def run_timetocd(args):
     for prec in ("f64", "f32", "f16s"):
         sim = mblbm.MultiBlockLBM(geo, prec)
         sim.init(stream)
+        if args.bc == "survey":  # free-slip top and bottom, half-way bounce-back on the cylinder
+            mblbm.channel_walls(sim, geo)
         sim.evolution_diag(12, stream)  # single-step plans of every scheduler phase
         sim.init(stream)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -252,6 +254,8 @@ def run_timetocd(args):
     line = {"metric": "time to Cd within 0.5% of the converged FP64 value", "unit": "ms", "higher_is_better": False,
             "value": out["f32"]["ms_to_cd"], "n_gpus": 1, "steps": args.steps, "warmup": 12, "data": "synthetic",
             "config": {"workload": "2-level cylinder Re=40, 400x160 coarse, fine box [60,140]x[40,120], D=20, U0=0.05",
+                       "boundaries": ("free-slip top and bottom, half-way bounce-back cylinder" if args.bc == "survey"
+                                      else "the reference's: equilibrium domain edges, on-node bounce-back cylinder"),
                        "cell_updates_per_step": upd, "reference": "Cd of FP64 storage after the run"},
             "dtype": "f32", "by_precision": out}
     print(json.dumps(line), flush=True)
@@ -402,6 +406,9 @@ def main():
     ap.add_argument("--eval-per-d", type=float, default=900.0, help="coarse steps per unit D of a warm-start evaluation run")
     ap.add_argument("--warm-precision", default="f16s", choices=["f16s", "f32"], help="solver storage of warm starts")
     ap.add_argument("--epochs", type=int, default=40, help="training epochs of --workload warmstart")
+    ap.add_argument("--bc", default="reference", choices=["reference", "survey"],
+                    help="boundaries of --workload timetocd: the reference's, or free-slip top and bottom with a "
+                         "half-way bounce-back cylinder")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 

@@ -280,6 +280,28 @@ def config1_geometry():
     return geo_init(L, make_config(400, 160, 10, 100, 80, U0=(0.05, 0.0), Re=40.0))
 
 
+def channel_walls(sim, geo, slip_walls=True, halfway_obstacle=True):
+    """The boundaries config 1 of the survey names instead of the reference's
+    equilibrium edges and on-node walls: free-slip walls on the domain's
+    bottom and top rows (MB_SOLID_SLIP, the reference's slip_gpu table) and
+    half-way bounce-back on the obstacle (MB_SOLID_HBB).  The inlet and outlet
+    columns keep their equilibrium."""
+    cfg = geo.config
+    for a in range(geo.layout.number_area):
+        A = geo.Areas[a]
+        t = sim.fields(a)["solid"].copy()
+        x = A.base_x + np.arange(A.nx) / A.m
+        y = A.base_y + np.arange(A.ny) / A.m
+        if halfway_obstacle:
+            t[t == MB_SOLID_SBB] = MB_SOLID_HBB
+        if slip_walls:
+            inner = (x != 0.0) & (x != cfg.LX - 1.0)
+            for j in np.nonzero((y == 0.0) | (y == cfg.LY - 1.0))[0]:
+                row = t[j]
+                row[inner & (row == MB_FLUID)] = MB_SOLID_SLIP
+        sim.set_cell_types(a, t)
+
+
 def config2_geometry():
     """3-level cylinder, Re=100: 4096x1024 coarse, level-1 box 512x256, level-2 box 256x128,
     D=32 at (960,512), U0=0.04."""

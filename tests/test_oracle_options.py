@@ -166,3 +166,28 @@ def test_cell_types_reject_interface_cells(mb, orc):
     bad[t == FLUID] = 5
     with pytest.raises(ValueError):
         o.set_cell_types(1, bad)
+
+
+def test_channel_walls_of_config1(mb, orc):
+    """mblbm.channel_walls marks the domain's bottom and top rows (inlet and
+    outlet columns excepted) free-slip and the cylinder half-way bounce-back;
+    the oracle then runs the config-1 case with those boundaries."""
+    g = mb.config1_geometry()
+    o = orc.Oracle(g)
+    o.init()
+    mb.channel_walls(o, g)
+    cfg = g.config
+    for a in range(g.layout.number_area):
+        A = g.Areas[a]
+        t = o.fields(a)["solid"]
+        y = A.base_y + np.arange(A.ny) / A.m
+        x = A.base_x + np.arange(A.nx) / A.m
+        for j in range(A.ny):
+            wall = y[j] in (0.0, cfg.LY - 1.0)
+            for i in (1, A.nx // 2):
+                if wall and x[i] not in (0.0, cfg.LX - 1.0):
+                    assert t[j, i] == SLIP
+        assert not (t == SBB).any()
+    assert (o.fields(g.layout.number_area - 1)["solid"] == HBB).sum() > 0
+    o.evolution(20)
+    assert np.isfinite(o.getDrag_block()[2])
