@@ -233,7 +233,7 @@ def run_timetocd(args):
     for prec in ("f64", "f32", "f16s"):
         sim = mblbm.MultiBlockLBM(geo, prec)
         sim.init(stream)
-        if args.bc == "survey":  # free-slip top and bottom, half-way bounce-back on the cylinder
+        if args.bc == "channel":  # free-slip top and bottom, half-way bounce-back on the cylinder
             mblbm.channel_walls(sim, geo)
         sim.evolution_diag(12, stream)  # single-step plans of every scheduler phase
         sim.init(stream)
@@ -254,7 +254,7 @@ def run_timetocd(args):
     line = {"metric": "time to Cd within 0.5% of the converged FP64 value", "unit": "ms", "higher_is_better": False,
             "value": out["f32"]["ms_to_cd"], "n_gpus": 1, "steps": args.steps, "warmup": 12, "data": "synthetic",
             "config": {"workload": "2-level cylinder Re=40, 400x160 coarse, fine box [60,140]x[40,120], D=20, U0=0.05",
-                       "boundaries": ("free-slip top and bottom, half-way bounce-back cylinder" if args.bc == "survey"
+                       "boundaries": ("free-slip top and bottom, half-way bounce-back cylinder" if args.bc == "channel"
                                       else "the reference's: equilibrium domain edges, on-node bounce-back cylinder"),
                        "cell_updates_per_step": upd, "reference": "Cd of FP64 storage after the run"},
             "dtype": "f32", "by_precision": out}
@@ -376,6 +376,55 @@ def run_forces(args):
     return 0
 
 
+def run_tgv(args):
+    """The 2-level periodic Taylor-Green vortex: 1024^2 coarse cells with a
+    centred 256^2-cell refined patch (512^2 fine cells), u0 = 0.01, tau = 0.6
+    on level 0, --steps coarse steps (5000) in FP64, FP32 and FP16-shifted
+    storage: device time, MLUPS, and the vortex amplitude against the exact
+    decay u0 exp(-2 nu k^2 t) and against the FP64 run."""
+    import numpy as np
+    import torch
+    import mblbm
+
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    geo = mblbm.tgv_geometry(n=1024, patch=256, u0=0.01, tau=0.6, levels=2)
+    upd = mblbm.updates_per_coarse_step(geo)
+    nu = (geo.Areas[0].tau - 0.5) / 3.0
+    k = 2.0 * np.pi / (geo.config.LX - 2)
+    out = {}
+    for prec in ("f64", "f32", "f16s"):
+        sim = mblbm.MultiBlockLBM(geo, prec)
+        sim.init(stream)
+        sim.evolution(args.warmup, stream)  # plans and graphs built before the timed run
+        sim.init(stream)
+        mblbm.tgv_init(sim, geo)
+        a0 = mblbm.tgv_amplitude(sim, geo)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sim.evolution(args.steps, stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        amp = mblbm.tgv_amplitude(sim, geo)
+        exact = a0 * np.exp(-2.0 * nu * k * k * args.steps)
+        out[prec] = {"amplitude": amp, "rel_to_exact": amp / exact - 1.0, "ms": round(ms, 2),
+                     "mlups": round(upd * args.steps / ms / 1e3, 1)}
+        sim.close()
+    for prec in ("f32", "f16s"):
+        out[prec]["rel_to_f64"] = out[prec]["amplitude"] / out["f64"]["amplitude"] - 1.0
+    line = {"metric": "periodic Taylor-Green vortex: MLUPS and amplitude error after the run", "unit": "MLUPS",
+            "value": out["f16s"]["mlups"], "higher_is_better": True, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "data": "synthetic", "dtype": "f16s",
+            "config": {"workload": "2-level periodic Taylor-Green vortex, 1024x1024 coarse, 256x256-cell refined "
+                                   "patch (512x512 fine cells), u0=0.01, tau=0.6",
+                       "cell_updates_per_step": upd, "exact": "u0 exp(-2 nu k^2 t), nu = (tau - 1/2)/3"},
+            "by_precision": out}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def unet_gflop(H, W):
     """Forward GFLOP of the surrogate for one sample (3x3 convolutions)."""
     layers = [(16, 32, 0), (32, 32, 0), (32, 64, 1), (64, 64, 1), (64, 128, 2), (128, 128, 2), (128, 256, 3),
@@ -397,16 +446,18 @@ def main():
                          "-s 3 with N >= 2); prints its roofline")
     ap.add_argument("--level", type=int, default=0, help="level of --roofline-only")
     ap.add_argument("--variant", type=int, default=None, help="block-step variant of every level (mb_set_stb_variant)")
-    ap.add_argument("--workload", default="cylinder3", choices=["cylinder3", "batch256", "timetocd", "warmstart", "forces"],
+    ap.add_argument("--workload", default="cylinder3",
+                    choices=["cylinder3", "batch256", "timetocd", "warmstart", "forces", "tgv"],
                     help="cylinder3: the single 3-level case (default); batch256: the batched form; "
-                         "timetocd: Cd convergence of the 2-level case by precision")
+                         "timetocd: Cd convergence of the 2-level case by precision; tgv: the 2-level periodic "
+                         "Taylor-Green vortex by precision")
     ap.add_argument("--cases", type=int, default=256, help="cases of --workload batch256 / training cases of warmstart")
     ap.add_argument("--eval", type=int, default=64, help="held-out cases of --workload warmstart")
     ap.add_argument("--snap-per-d", type=float, default=300.0, help="coarse steps per unit D before a training snapshot")
     ap.add_argument("--eval-per-d", type=float, default=900.0, help="coarse steps per unit D of a warm-start evaluation run")
     ap.add_argument("--warm-precision", default="f16s", choices=["f16s", "f32"], help="solver storage of warm starts")
     ap.add_argument("--epochs", type=int, default=40, help="training epochs of --workload warmstart")
-    ap.add_argument("--bc", default="reference", choices=["reference", "survey"],
+    ap.add_argument("--bc", default="reference", choices=["reference", "channel"],
                     help="boundaries of --workload timetocd: the reference's, or free-slip top and bottom with a "
                          "half-way bounce-back cylinder")
     args = ap.parse_args()
@@ -427,6 +478,8 @@ def main():
         return run_warmstart(args)
     if args.workload == "forces":
         return run_forces(args)
+    if args.workload == "tgv":
+        return run_tgv(args)
 
     import torch
 

@@ -64,6 +64,19 @@ extern "C" {
 /* ---- obstacle kinds ---------------------------------------------------- */
 #define MB_OBST_CIRCLE 0  /* (x-CX)^2+(y-CY)^2 < R^2, lbm/init_block.h:28    */
 #define MB_OBST_ELLIPSE 1 /* rotated ellipse (batched cases; no reference)  */
+#define MB_OBST_NONE 2    /* no obstacle (periodic flows; no reference)     */
+
+/* ---- periodic level-0 domain (mb_config.periodic; no reference counterpart)
+ * With MB_PERIODIC_X the level-0 nodes x = 0 and x = LX-1 become ghost cells
+ * (MB_C_BOUNDARY) of x = LX-2 and x = 1: the period is LX-2 nodes.  Likewise
+ * MB_PERIODIC_Y in y.  mb_geo_init adds same-level copy lines, direction code
+ * MB_DIR_PERIODIC in NeborCC, that give every ghost the state of the level-0
+ * cell computing its image node after each level-0 step, and drops the ghost
+ * cells from the ends of the layout's own level-0 lines.  Blocks of finer
+ * levels must not touch a periodic edge. */
+#define MB_PERIODIC_X 1
+#define MB_PERIODIC_Y 2
+#define MB_DIR_PERIODIC 8
 
 typedef void *mb_stream; /* cudaStream_t */
 
@@ -109,6 +122,7 @@ typedef struct {
   int obstacle;     /* MB_OBST_* */
   double ell_cx, ell_cy, ell_a, ell_b, ell_angle; /* MB_OBST_ELLIPSE only */
   int drag_area;    /* block used for drag; -1 = last block (Multi-block-LBM.cu:127) */
+  int periodic;     /* MB_PERIODIC_* bits; 0 = the reference's equilibrium edges */
 } mb_config;
 
 /* AREA (lbm/data_type_lbm.h:43-51) */
@@ -152,7 +166,10 @@ int mb_layout_builtin(const char *name, mb_layout *out);
  * blocks (top, bottom, left, right) that overlap their neighbours by one
  * coarse cell, the pattern of geo/geometry.h:55-100 (_GEO_2_5). */
 int mb_layout_nested(int LX, int LY, int nlevels, const int *boxes, mb_layout *out);
-/* geo_init() + Line_init() (geo/init_geo.h:17-165). */
+/* geo_init() + Line_init() (geo/init_geo.h:17-165); with mb_config.periodic
+ * also the periodic ghost lines (MB_PERIODIC_X above).  Entries of the
+ * layout's NeborCC with direction MB_DIR_PERIODIC are dropped first, so the
+ * layout of a geometry may be passed in again. */
 int mb_geo_init(const mb_layout *layout, const mb_config *cfg, mb_geometry *geo);
 /* Checks that every C_BOUNDARY cell is the target of some transfer line. */
 int mb_geo_check_coverage(const mb_geometry *geo, int *n_uncovered);

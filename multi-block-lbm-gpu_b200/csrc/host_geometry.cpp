@@ -276,11 +276,160 @@ void make_line_pair(int d, const mb_p4 &DC, const mb_area &C, const mb_p4 &DF, c
   lf.Nf = lc.Nf;
 }
 
+// Drops the periodic ghost lines (MB_DIR_PERIODIC) of a layout that an
+// earlier mb_geo_init produced, with the level ranges of LCCP.
+void strip_periodic(mb_layout &L) {
+  int lccp[MB_MAX_LEVEL + 1];
+  std::memcpy(lccp, L.LCCP, sizeof(lccp));
+  int n = 0;
+  for (int c = 0; c < L.number_line2; c++) {
+    if (L.NeborCC[c].direction == MB_DIR_PERIODIC) {
+      for (int l = 0; l <= L.LEVEL; l++)
+        if (lccp[l] > c) L.LCCP[l]--;
+      continue;
+    }
+    L.NeborCC[n++] = L.NeborCC[c];
+  }
+  L.number_line2 = n;
+}
+
+// Point ip of a same-level line in the orientation c_c_boundary_transfer
+// gives it (multi/FH/assit_multi.h:20-33): along y when the source segment
+// is vertical, along x when it is horizontal (a single point is both).
+void cc_point(const mb_line &l, int ip, int &i1, int &j1, int &i2, int &j2) {
+  i1 = j1 = i2 = j2 = 0;
+  if (l.line_C.xstart == l.line_C.xend) { i1 = l.line_C.xstart; j1 = l.line_C.ystart + ip; i2 = l.line_F.xstart; j2 = l.line_F.ystart + ip; }
+  if (l.line_C.ystart == l.line_C.yend) { i1 = l.line_C.xstart + ip; j1 = l.line_C.ystart; i2 = l.line_F.xstart + ip; j2 = l.line_F.ystart; }
+}
+
+// Periodic ghost lines (no reference counterpart).  Every level-0 cell on a
+// wrapped domain edge is a ghost of its image node one period (LX-2 or LY-2
+// nodes) away; the cell that computes the image is the one level-0 cell at
+// that node that is not C_BOUNDARY (the first block in index order where
+// several are, as for equilibrium edge cells shared by two blocks).  Runs of
+// ghosts along one block edge whose image cells are consecutive in one block
+// become one copy line.  The layout's own level-0 lines lose the ghost cells
+// at their ends, so that each ghost has one writer and no line reads a ghost.
+// The new lines follow the level-0 lines of LCCP, entries MB_DIR_PERIODIC.
+int periodic_lines(mb_geometry &g) {
+  mb_layout &L = g.layout;
+  const mb_config &c = g.config;
+  const bool px = c.periodic & MB_PERIODIC_X, py = c.periodic & MB_PERIODIC_Y;
+  if (L.mi[0] != 1 || (px && c.LX < 4) || (py && c.LY < 4)) return MB_ERR_GEOMETRY;
+  for (int a = L.ASP[1]; a < L.number_area; a++) {  // finer blocks stay off wrapped edges
+    const mb_p4 &D = g.AreaDefine[a];
+    if ((px && (D.xstart <= 0 || D.xend >= c.LX - 1)) || (py && (D.ystart <= 0 || D.yend >= c.LY - 1)))
+      return MB_ERR_GEOMETRY;
+  }
+  auto ghost = [&](int a, int i, int j) {
+    const mb_area &A = g.Areas[a];
+    return mblbm::periodic_ghost(c, i + A.base_x, j + A.base_y);
+  };
+  // the layout's level-0 lines without ghost targets
+  for (int ln = L.LCCP[0]; ln < L.LCCP[1]; ln++) {
+    mb_line &l = g.Line_Inf_CC[ln];
+    auto tg = [&](int ip) {
+      int i1, j1, i2, j2;
+      cc_point(l, ip, i1, j1, i2, j2);
+      return ghost(l.areaf_n, i2, j2);
+    };
+    int lo = 0, hi = l.Nc;
+    while (lo < hi && tg(lo)) lo++;
+    while (hi > lo && tg(hi - 1)) hi--;
+    for (int ip = lo; ip < hi; ip++)
+      if (tg(ip)) return MB_ERR_GEOMETRY;
+    if (lo == 0 && hi == l.Nc) continue;
+    if (hi - lo < 2) return MB_ERR_GEOMETRY;  // keeps the line's orientation
+    int i1, j1, i2, j2;
+    cc_point(l, lo, i1, j1, i2, j2);
+    const bool vert = l.line_C.xstart == l.line_C.xend;
+    const int n = hi - lo;
+    l.line_C = vert ? mb_p4{i1, i1, j1, j1 + n - 1} : mb_p4{i1, i1 + n - 1, j1, j1};
+    l.line_F = vert ? mb_p4{i2, i2, j2, j2 + n - 1} : mb_p4{i2, i2 + n - 1, j2, j2};
+    l.Nc = l.Nf = n;
+  }
+  // ghost runs: rows j = 0 and ny-1, then columns i = 0 and nx-1 without the corners
+  std::vector<mb_line> extra;
+  for (int a = L.ASP[0]; a < L.ASP[1]; a++) {
+    const mb_area &A = g.Areas[a];
+    for (int e = 0; e < 4; e++) {
+      const bool vert = e >= 2;
+      const int n = vert ? A.ny - 2 : A.nx;
+      bool open = false;
+      mb_line cur{};
+      int last_ip = 0;
+      for (int ip = 0; ip < n; ip++) {
+        const int i = vert ? (e == 2 ? 0 : A.nx - 1) : ip;
+        const int j = vert ? ip + 1 : (e == 0 ? 0 : A.ny - 1);
+        if (!ghost(a, i, j)) {
+          if (open) extra.push_back(cur);
+          open = false;
+          continue;
+        }
+        if (mblbm::cell_type(g, a, i, j) != MB_C_BOUNDARY) return MB_ERR_GEOMETRY;
+        const int X = i + (int)A.base_x, Y = j + (int)A.base_y;
+        const int Xi = !px ? X : X == 0 ? c.LX - 2 : X == c.LX - 1 ? 1 : X;
+        const int Yi = !py ? Y : Y == 0 ? c.LY - 2 : Y == c.LY - 1 ? 1 : Y;
+        int owner = -1, oi = 0, oj = 0;
+        for (int b = L.ASP[0]; b < L.ASP[1] && owner < 0; b++) {
+          const mb_area &B = g.Areas[b];
+          const int ii = Xi - (int)B.base_x, jj = Yi - (int)B.base_y;
+          if (ii < 0 || jj < 0 || ii >= B.nx || jj >= B.ny) continue;
+          if (mblbm::cell_type(g, b, ii, jj) == MB_C_BOUNDARY) continue;
+          owner = b;
+          oi = ii;
+          oj = jj;
+        }
+        if (owner < 0) return MB_ERR_GEOMETRY;
+        const bool extends = open && cur.areac_n == owner && ip == last_ip + 1 &&
+                             (vert ? (oi == cur.line_C.xend && oj == cur.line_C.yend + 1)
+                                   : (oj == cur.line_C.yend && oi == cur.line_C.xend + 1));
+        if (extends) {
+          cur.Nc++;
+          cur.Nf++;
+          cur.line_C.xend = oi;
+          cur.line_C.yend = oj;
+          cur.line_F.xend = i;
+          cur.line_F.yend = j;
+        } else {
+          if (open) extra.push_back(cur);
+          cur = mb_line{};
+          cur.areac_n = owner;
+          cur.areaf_n = a;
+          cur.Nc = cur.Nf = 1;
+          cur.line_C = {oi, oi, oj, oj};
+          cur.line_F = {i, i, j, j};
+          open = true;
+        }
+        last_ip = ip;
+      }
+      if (open) extra.push_back(cur);
+    }
+  }
+  const int P = (int)extra.size(), at = L.LCCP[1];
+  if (L.number_line2 + P > MB_MAX_LINE2) return MB_ERR_UNSUPPORTED;
+  for (int q = L.number_line2 - 1; q >= at; q--) {
+    g.Line_Inf_CC[q + P] = g.Line_Inf_CC[q];
+    L.NeborCC[q + P] = L.NeborCC[q];
+  }
+  for (int p = 0; p < P; p++) {
+    g.Line_Inf_CC[at + p] = extra[p];
+    L.NeborCC[at + p] = {extra[p].areac_n, extra[p].areaf_n, MB_DIR_PERIODIC};
+  }
+  for (int l = 1; l <= L.LEVEL; l++) L.LCCP[l] += P;
+  L.number_line2 += P;
+  return MB_OK;
+}
+
 }  // namespace
 
 extern "C" int mb_geo_init(const mb_layout *layout, const mb_config *cfg, mb_geometry *geo) {
   if (!layout || !cfg || !geo) return MB_ERR_INVALID;
-  const mb_layout &L = *layout;
+  if (layout->LEVEL < 1 || layout->LEVEL > MB_MAX_LEVEL || layout->number_line2 < 0 ||
+      layout->number_line2 > MB_MAX_LINE2)
+    return MB_ERR_INVALID;
+  mb_layout L = *layout;
+  strip_periodic(L);
   if (L.LEVEL < 1 || L.LEVEL > MB_MAX_LEVEL || L.number_area < 1 || L.number_area > MB_MAX_AREA ||
       L.number_line < 0 || L.number_line > MB_MAX_LINE || L.number_line2 < 0 || L.number_line2 > MB_MAX_LINE2 ||
       (L.number_line2 & 1))
@@ -301,6 +450,7 @@ extern "C" int mb_geo_init(const mb_layout *layout, const mb_config *cfg, mb_geo
         L.NeborCC[c].nf >= L.number_area)
       return MB_ERR_INVALID;
   if (cfg->Re <= 0 || cfg->LX < 2 || cfg->LY < 2) return MB_ERR_INVALID;
+  if (cfg->periodic & ~(MB_PERIODIC_X | MB_PERIODIC_Y)) return MB_ERR_INVALID;
 
   mb_geometry &g = *geo;
   std::memset(&g, 0, sizeof(g));
@@ -354,6 +504,7 @@ extern "C" int mb_geo_init(const mb_layout *layout, const mb_config *cfg, mb_geo
     l1.areaf_n = L.NeborCC[i + 1].nf;
     std::swap(l1.line_C, l1.line_F);
   }
+  if (cfg->periodic) return periodic_lines(g);
   return MB_OK;
 }
 
@@ -363,6 +514,7 @@ extern "C" int mb_geo_init(const mb_layout *layout, const mb_config *cfg, mb_geo
 namespace mblbm {
 
 bool obstacle_contains(const mb_config &c, double x, double y) {
+  if (c.obstacle == MB_OBST_NONE) return false;
   if (c.obstacle == MB_OBST_ELLIPSE) {
     const double dx = x - c.ell_cx, dy = y - c.ell_cy;
     const double ca = std::cos(c.ell_angle), sa = std::sin(c.ell_angle);
@@ -373,15 +525,24 @@ bool obstacle_contains(const mb_config &c, double x, double y) {
   return (x - c.CX) * (x - c.CX) + (y - c.CY) * (y - c.CY) < c.R * c.R;
 }
 
+// A node on an edge of the domain that mb_config.periodic wraps: a ghost of
+// the node one period away (no reference counterpart).
+bool periodic_ghost(const mb_config &c, double x, double y) {
+  return ((c.periodic & MB_PERIODIC_X) && (x == 0.0 || x == c.LX - 1.0)) ||
+         ((c.periodic & MB_PERIODIC_Y) && (y == 0.0 || y == c.LY - 1.0));
+}
+
 // Cell type of init_General (lbm/init_block.h:28-42): solid inside the
 // obstacle, FLUID on the physical domain edge (FP64 coordinate equality),
-// C_BOUNDARY on any other block edge, FLUID inside.
+// C_BOUNDARY on any other block edge, FLUID inside.  Periodic domain edges
+// are C_BOUNDARY: their cells are ghosts filled by copy lines.
 int cell_type(const mb_geometry &g, int a, int i, int j) {
   const mb_area &A = g.Areas[a];
   const double dx = 1.0 / A.m;
   const double x = i * dx + A.base_x, y = j * dx + A.base_y;
   const mb_config &c = g.config;
   if (obstacle_contains(c, x, y)) return MB_SOLID_SBB;
+  if (periodic_ghost(c, x, y)) return MB_C_BOUNDARY;
   if (y == 0.0 || y == c.LY - 1.0 || x == 0.0 || x == c.LX - 1.0) return MB_FLUID;
   if (i == 0 || j == 0 || i == A.nx - 1 || j == A.ny - 1) return MB_C_BOUNDARY;
   return MB_FLUID;

@@ -24,6 +24,7 @@ enum : uint8_t {
 };
 
 bool obstacle_contains(const mb_config &c, double x, double y);
+bool periodic_ghost(const mb_config &c, double x, double y);
 int cell_type(const mb_geometry &g, int a, int i, int j);
 
 // One interface point operation (16 bytes, the unit of the record kernel).

@@ -26,7 +26,8 @@ PREC_F64, PREC_F32, PREC_F16S, PREC_F32U = 0, 1, 2, 3
 # f32: FP32 storage of f - w (the product FP32 form); f32u: FP32 storage of f
 PRECISIONS = {"f64": PREC_F64, "f32": PREC_F32, "f16s": PREC_F16S, "f32u": PREC_F32U}
 FLUID, SOLID_SBB, C_BOUNDARY = 0, 1, 9
-OBST_CIRCLE, OBST_ELLIPSE = 0, 1
+OBST_CIRCLE, OBST_ELLIPSE, OBST_NONE = 0, 1, 2
+PERIODIC_X, PERIODIC_Y, DIR_PERIODIC = 1, 2, 8  # mb_config.periodic bits, NeborCC code of ghost lines
 MB_FLUID, MB_SOLID_SBB, MB_SOLID_SLIP, MB_SOLID_HBB, MB_C_BOUNDARY = 0, 1, 2, 3, 9
 MB_COLL_BGK, MB_COLL_MRT = 0, 1  # cell kinds of mb_copy_fields' solid array
 
@@ -81,6 +82,7 @@ class Config(C.Structure):
         ("ell_b", C.c_double),
         ("ell_angle", C.c_double),
         ("drag_area", C.c_int),
+        ("periodic", C.c_int),
     ]
 
 
@@ -248,12 +250,14 @@ def layout_nested(LX, LY, boxes):
     return L
 
 
-def make_config(LX, LY, R, CX, CY, U0=(0.1, 0.0), Re=10.0, rho0=1.0, drag_area=-1, ellipse=None):
+def make_config(LX, LY, R, CX, CY, U0=(0.1, 0.0), Re=10.0, rho0=1.0, drag_area=-1, ellipse=None,
+                periodic=0, obstacle=True):
     c = Config()
     c.Re, c.rho0, c.LX, c.LY, c.R, c.CX, c.CY = float(Re), float(rho0), LX, LY, R, CX, CY
     c.U0[0], c.U0[1] = float(U0[0]), float(U0[1])
-    c.obstacle = OBST_CIRCLE
+    c.obstacle = OBST_CIRCLE if obstacle else OBST_NONE
     c.drag_area = drag_area
+    c.periodic = periodic
     if ellipse is not None:
         c.obstacle = OBST_ELLIPSE
         c.ell_cx, c.ell_cy, c.ell_a, c.ell_b, c.ell_angle = [float(v) for v in ellipse]
@@ -281,8 +285,8 @@ def config1_geometry():
 
 
 def channel_walls(sim, geo, slip_walls=True, halfway_obstacle=True):
-    """The boundaries config 1 of the survey names instead of the reference's
-    equilibrium edges and on-node walls: free-slip walls on the domain's
+    """Channel boundaries for the 2-level cylinder at Re=40 in place of the
+    reference's equilibrium edges and on-node walls: free-slip walls on the domain's
     bottom and top rows (MB_SOLID_SLIP, the reference's slip_gpu table) and
     half-way bounce-back on the obstacle (MB_SOLID_HBB).  The inlet and outlet
     columns keep their equilibrium."""
@@ -300,6 +304,79 @@ def channel_walls(sim, geo, slip_walls=True, halfway_obstacle=True):
                 row = t[j]
                 row[inner & (row == MB_FLUID)] = MB_SOLID_SLIP
         sim.set_cell_types(a, t)
+
+
+def tgv_geometry(n=1024, patch=256, u0=0.01, tau=0.6, levels=2):
+    """Taylor-Green vortex on a doubly periodic n x n coarse domain (nodes
+    0..n+1, the outer ring being ghosts of the opposite side) with a centred
+    refined patch of patch x patch coarse cells per finer level (each level
+    halving the previous patch), no obstacle, relaxation time tau on level 0.
+    The reference has no periodic boundary; this is the decay check of the
+    multi-block step.  U0 = (u0, 0) is the vortex amplitude; R = 1 and Re
+    are chosen so that geo_init's nu = |U0| 2R / Re gives tau."""
+    nu = (tau - 0.5) / 3.0
+    N = n + 2
+    boxes = []
+    w = patch
+    for _ in range(levels - 1):
+        lo = (N - 1 - w) // 2
+        boxes.append((lo, lo + w, lo, lo + w))
+        w //= 2
+    L = layout_nested(N, N, boxes)
+    cfg = make_config(N, N, 1, N // 2, N // 2, U0=(u0, 0.0), Re=u0 * 2.0 / nu, obstacle=False,
+                      periodic=PERIODIC_X | PERIODIC_Y)
+    return geo_init(L, cfg)
+
+
+_EX = np.array([0, 1, 0, -1, 0, 1, -1, -1, 1], dtype=np.float64)
+_EY = np.array([0, 0, 1, 0, -1, 1, 1, -1, -1], dtype=np.float64)
+_WD = np.array([4 / 9] + [1 / 9] * 4 + [1 / 36] * 4)
+
+
+def feq(rho, ux, uy):
+    """feq of every direction (lbm/assit_func.h:2-9), arrays (9, ...)."""
+    rho, ux, uy = np.asarray(rho, np.float64), np.asarray(ux, np.float64), np.asarray(uy, np.float64)
+    eu = _EX.reshape((9,) + (1,) * ux.ndim) * ux + _EY.reshape((9,) + (1,) * uy.ndim) * uy
+    uv = ux * ux + uy * uy
+    return _WD.reshape((9,) + (1,) * rho.ndim) * rho * (1.0 + 3.0 * eu + 4.5 * eu * eu - 1.5 * uv)
+
+
+def tgv_mode(geo, a):
+    """Phases of block a's nodes in the periodic frame: (s, c) with
+    ux = u0 s, uy = u0 c for the initial vortex, k = 2 pi / (LX - 2)."""
+    A, cfg = geo.Areas[a], geo.config
+    kx, ky = 2.0 * np.pi / (cfg.LX - 2), 2.0 * np.pi / (cfg.LY - 2)
+    X = (A.base_x + np.arange(A.nx) / A.m - 1.0) * kx
+    Y = (A.base_y + np.arange(A.ny) / A.m - 1.0) * ky
+    X, Y = np.meshgrid(X, Y)
+    return np.sin(X) * np.cos(Y), -np.cos(X) * np.sin(Y), X, Y
+
+
+def tgv_init(sim, geo, u0=None):
+    """Sets every block to the equilibrium of the initial vortex,
+    u = u0 (sin kx cos ky, -cos kx sin ky), rho = rho0 (1 - 3 u0^2/4 (cos 2kx
+    + cos 2ky)), and re-derives the interface history (sync_history)."""
+    cfg = geo.config
+    u0 = cfg.U0[0] if u0 is None else u0
+    for a in range(geo.layout.number_area):
+        s, c, X, Y = tgv_mode(geo, a)
+        ux, uy = u0 * s, u0 * c
+        rho = cfg.rho0 * (1.0 - 0.75 * u0 * u0 * (np.cos(2 * X) + np.cos(2 * Y)))
+        sim.set_fields(a, rho=rho, ux=ux, uy=uy, F=feq(rho, ux, uy))
+    sim.sync_history()
+
+
+def tgv_amplitude(sim, geo, fields=None):
+    """Least-squares amplitude of the vortex mode in u over the FLUID cells
+    of all blocks; u0 exp(-2 nu k^2 t) for the exact decay."""
+    num = den = 0.0
+    for a in range(geo.layout.number_area):
+        f = fields[a] if fields is not None else sim.fields(a)
+        s, c, _, _ = tgv_mode(geo, a)
+        m = f["solid"] == MB_FLUID
+        num += float((f["ux"][m] * s[m]).sum() + (f["uy"][m] * c[m]).sum())
+        den += float((s[m] * s[m]).sum() + (c[m] * c[m]).sum())
+    return num / den
 
 
 def config2_geometry():

@@ -78,6 +78,8 @@ struct orc_sim {
   double s_e, s_eps, s_q;
   double fx, fy;                /* uniform body force on every cell's forcex/forcey */
   int *types[MB_MAX_AREA];      /* cell-type overrides, applied after init_General */
+  int n_pfill;                  /* periodic ghosts: 4 ints each, ghost block/cell, image block/cell */
+  int *pfill;
 };
 
 void orc_set_threads(int n) {
@@ -270,6 +272,7 @@ void orc_destroy(orc_sim *s) {
     for (int k = 0; k < Q; k++) free(sp->F[k]);
   }
   free(s->drag);
+  free(s->pfill);
   for (int a = 0; a < MB_MAX_AREA; a++) free(s->types[a]);
   free(s);
 }
@@ -279,6 +282,7 @@ void orc_destroy(orc_sim *s) {
  * counterpart (batched cases only).
  * ------------------------------------------------------------------------- */
 static int is_solid(const mb_config *c, double x, double y) {
+  if (c->obstacle == MB_OBST_NONE) return 0;
   if (c->obstacle == MB_OBST_ELLIPSE) {
     double dx = x - c->ell_cx, dy = y - c->ell_cy;
     double ca = cos(c->ell_angle), sa = sin(c->ell_angle);
@@ -286,6 +290,13 @@ static int is_solid(const mb_config *c, double x, double y) {
     return (xr * xr) / (c->ell_a * c->ell_a) + (yr * yr) / (c->ell_b * c->ell_b) < 1.0;
   }
   return (x - c->CX) * (x - c->CX) + (y - c->CY) * (y - c->CY) < c->R * c->R;
+}
+
+/* Periodic domain (mb_config.periodic; no reference counterpart): the level-0
+ * nodes on a wrapped edge are ghosts of the node LX-2 (LY-2) nodes away. */
+static int is_periodic_ghost(const mb_config *c, double x, double y) {
+  return ((c->periodic & MB_PERIODIC_X) && (x == 0.0 || x == c->LX - 1.0)) ||
+         ((c->periodic & MB_PERIODIC_Y) && (y == 0.0 || y == c->LY - 1.0));
 }
 
 static void init_general(orc_sim *s, int a) {
@@ -309,6 +320,7 @@ static void init_general(orc_sim *s, int a) {
       pp->forcey[ixy] = 0.0;
       double X = pp->x[ixy], Y = pp->y[ixy];
       if (is_solid(c, X, Y)) pp->solid[ixy] = MB_SOLID_SBB;
+      else if (is_periodic_ghost(c, X, Y)) pp->solid[ixy] = MB_C_BOUNDARY;
       else if (Y == 0.0) pp->solid[ixy] = MB_FLUID;
       else if (Y == c->LY - 1.0) pp->solid[ixy] = MB_FLUID;
       else if (X == 0.0) pp->solid[ixy] = MB_FLUID;
@@ -461,12 +473,79 @@ static void apply_options(orc_sim *s, int a) {
   }
 }
 
+/* Periodic ghost map: for every level-0 ghost cell, the level-0 cell at its
+ * image node that the block step computes (the first block in index order
+ * whose cell there is not C_BOUNDARY).  Built from the cell types alone,
+ * without the copy lines of the geometry. */
+static int build_pfill(orc_sim *s) {
+  const mb_layout *L = &s->geo.layout;
+  const mb_config *c = &s->geo.config;
+  free(s->pfill);
+  s->pfill = NULL;
+  s->n_pfill = 0;
+  if (!c->periodic) return MB_OK;
+  size_t cap = 0;
+  for (int a = L->ASP[0]; a < L->ASP[1]; a++) cap += 2 * (size_t)(s->geo.Areas[a].nx + s->geo.Areas[a].ny);
+  s->pfill = (int *)malloc(4 * sizeof(int) * (cap ? cap : 1));
+  if (!s->pfill) return MB_ERR_NOMEM;
+  for (int a = L->ASP[0]; a < L->ASP[1]; a++) {
+    const mb_area *A = &s->geo.Areas[a];
+    for (int j = 0; j < A->ny; j++)
+      for (int i = 0; i < A->nx; i++) {
+        const double X = i + A->base_x, Y = j + A->base_y;
+        if (!is_periodic_ghost(c, X, Y)) continue;
+        double Xi = X, Yi = Y;
+        if (c->periodic & MB_PERIODIC_X) Xi = X == 0.0 ? c->LX - 2.0 : (X == c->LX - 1.0 ? 1.0 : X);
+        if (c->periodic & MB_PERIODIC_Y) Yi = Y == 0.0 ? c->LY - 2.0 : (Y == c->LY - 1.0 ? 1.0 : Y);
+        int owner = -1, cell = 0;
+        for (int b = L->ASP[0]; b < L->ASP[1] && owner < 0; b++) {
+          const mb_area *B = &s->geo.Areas[b];
+          const int ii = (int)(Xi - B->base_x), jj = (int)(Yi - B->base_y);
+          if (ii < 0 || jj < 0 || ii >= B->nx || jj >= B->ny) continue;
+          if (s->pp[b].solid[ii + jj * B->nx] == MB_C_BOUNDARY) continue;
+          owner = b;
+          cell = ii + jj * B->nx;
+        }
+        if (owner < 0) return MB_ERR_GEOMETRY;
+        int *e = s->pfill + 4 * s->n_pfill++;
+        e[0] = a; e[1] = i + j * A->nx; e[2] = owner; e[3] = cell;
+      }
+  }
+  return MB_OK;
+}
+
+/* after the level-0 copies: every ghost takes its image cell's state */
+static void periodic_fill(orc_sim *s) {
+  for (int q = 0; q < s->n_pfill; q++) {
+    const int *e = s->pfill + 4 * q;
+    o_d2q9 *g = &s->pp[e[0]], *o = &s->pp[e[2]];
+    g->rho[e[1]] = o->rho[e[3]];
+    g->ux[e[1]] = o->ux[e[3]];
+    g->uy[e[1]] = o->uy[e[3]];
+    for (int k = 0; k < Q; k++) g->F[k][e[1]] = o->F[k][e[3]];
+  }
+}
+
+/* The state the reference derives from the initial fields, after
+ * orc_set_fields replaced them: ring slots from the fine edge F (init_Fstore,
+ * multi/init_multi.h:3-28) and u_prev from u. */
+void orc_sync_history(orc_sim *s) {
+  const mb_layout *L = &s->geo.layout;
+  for (int b = 0; b < L->number_line; b++) init_fstore(s, b);
+  for (int a = 0; a < L->number_area; a++) {
+    const size_t N = (size_t)s->geo.Areas[a].nx * s->geo.Areas[a].ny;
+    memcpy(s->upx[a], s->pp[a].ux, N * sizeof(double));
+    memcpy(s->upy[a], s->pp[a].uy, N * sizeof(double));
+  }
+}
+
 int orc_init(orc_sim *s) {
   const mb_layout *L = &s->geo.layout;
   for (int a = 0; a < L->number_area; a++) {
     init_general(s, a);
     apply_options(s, a);
   }
+  if (build_pfill(s)) return MB_ERR_GEOMETRY;
   drag_setup(s);
   for (int b = 0; b < L->number_line; b++) { init_fstore(s, b); init_tri_a(s, b); }
   return MB_OK;
@@ -785,7 +864,9 @@ static void evolution(orc_sim *s, int level) {
     }
     for (int a = L->ASP[level]; a < L->ASP[level + 1]; a++) orc_block_step(s, a);
     if (L->number_line2 != 0)
-      for (int c = L->LCCP[level]; c < L->LCCP[level + 1]; c++) orc_c_c(s, c);
+      for (int c = L->LCCP[level]; c < L->LCCP[level + 1]; c++)
+        if (L->NeborCC[c].direction != MB_DIR_PERIODIC) orc_c_c(s, c);
+    if (level == 0) periodic_fill(s);
     if (level != L->LEVEL - 1) {
       for (int b = L->LS3CFFCP[level]; b < L->LS3CFFCP[level + 1]; b++) {
         orc_space_interpolation(s, b);

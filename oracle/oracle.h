@@ -30,6 +30,7 @@ void orc_set_threads(int n);
 /* init_General + init_Fstore + init_tri_A + sum_N_drag + fdrag_store
  * (Multi-block-LBM.cu:116-140) */
 int orc_init(orc_sim *s);
+void orc_sync_history(orc_sim *s);
 /* evolution(level 0) (evolution.h:2-65), one coarse step */
 void orc_evolution(orc_sim *s, int n);
 /* error_L2 (lbm/error_L2.h:57-91); returns the value written to error_L2.dat */

@@ -28,6 +28,7 @@ _SIG = {
     "orc_destroy": ([_vp], None),
     "orc_set_threads": ([C.c_int], None),
     "orc_init": ([_vp], C.c_int),
+    "orc_sync_history": ([_vp], None),
     "orc_evolution": ([_vp, C.c_int], None),
     "orc_error_L2": ([_vp], C.c_double),
     "orc_drag": ([_vp, _pd, _pd, _pd], None),
@@ -107,7 +108,13 @@ class Oracle:
             pass
 
     def init(self):
-        self.lib.orc_init(self.s)
+        rc = self.lib.orc_init(self.s)
+        if rc != 0:
+            raise ValueError(f"orc_init failed ({rc})")
+
+    def sync_history(self):
+        """Ring slots <- fine edge F and u_prev <- u, after set_fields."""
+        self.lib.orc_sync_history(self.s)
 
     def evolution(self, n=1):
         for _ in range(n):

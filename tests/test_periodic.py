@@ -1,0 +1,197 @@
+"""Periodic level-0 domain (mb_config.periodic), which the reference does not
+have: geometry of the ghost lines and the oracle's own ghost fill, checked
+against invariants and the exact Taylor-Green decay.
+
+The product geometry gives each ghost cell (a level-0 cell on a wrapped
+domain edge) a copy line from the cell computing its image node; the oracle
+ignores those lines and fills the ghosts from the cell types alone.  The
+checks here pin both to the definition: image node = node +- (L - 2), source
+= the one non-C_BOUNDARY level-0 cell at the image.
+"""
+import numpy as np
+import pytest
+
+FLUID, CB, PERIODIC = 0, 9, 8
+
+
+def geo_lines(g):
+    L = g.layout
+    out = []
+    for c in range(L.number_line2):
+        ln, d = g.Line_Inf_CC[c], L.NeborCC[c]
+        pts = []
+        for ip in range(ln.Nc):
+            i1 = j1 = i2 = j2 = 0
+            if ln.line_C.xstart == ln.line_C.xend:
+                i1, j1, i2, j2 = ln.line_C.xstart, ln.line_C.ystart + ip, ln.line_F.xstart, ln.line_F.ystart + ip
+            if ln.line_C.ystart == ln.line_C.yend:
+                i1, j1, i2, j2 = ln.line_C.xstart + ip, ln.line_C.ystart, ln.line_F.xstart + ip, ln.line_F.ystart
+            pts.append((ln.areac_n, i1, j1, ln.areaf_n, i2, j2))
+        out.append((d.direction, pts))
+    return out
+
+
+def node(g, a, i, j):
+    A = g.Areas[a]
+    return A.base_x + i / A.m, A.base_y + j / A.m
+
+
+def is_ghost(g, x, y):
+    c = g.config
+    return ((c.periodic & 1) and x in (0.0, c.LX - 1.0)) or ((c.periodic & 2) and y in (0.0, c.LY - 1.0))
+
+
+def image(g, x, y):
+    c = g.config
+    if c.periodic & 1:
+        x = c.LX - 2.0 if x == 0.0 else (1.0 if x == c.LX - 1.0 else x)
+    if c.periodic & 2:
+        y = c.LY - 2.0 if y == 0.0 else (1.0 if y == c.LY - 1.0 else y)
+    return x, y
+
+
+def channel_x(mb):
+    """Cylinder channel periodic in x only: equilibrium rows top and bottom."""
+    L = mb.layout_nested(66, 34, [(20, 40, 9, 25)])
+    return mb.geo_init(L, mb.make_config(66, 34, 4, 30, 17, U0=(0.05, 0.0), Re=20.0, periodic=mb.PERIODIC_X))
+
+
+CASES = {
+    "tgv2": lambda mb: mb.tgv_geometry(n=64, patch=32, levels=2),
+    "tgv3": lambda mb: mb.tgv_geometry(n=64, patch=32, levels=3),
+    "tgv1": lambda mb: mb.tgv_geometry(n=48, levels=1),
+    "channel_x": channel_x,
+}
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_ghost_lines_copy_each_ghost_from_its_image(mb, orc, name):
+    g = CASES[name](mb)
+    assert mb.coverage(g) == 0
+    o = orc.Oracle(g)
+    o.init()
+    types = [o.fields(a)["solid"] for a in range(g.layout.number_area)]
+    L = g.layout
+    lvl0 = range(L.ASP[0], L.ASP[1])
+    writers = {}
+    for c, (d, pts) in enumerate(geo_lines(g)):
+        for (sa, si, sj, ta, ti, tj) in pts:
+            tx, ty = node(g, ta, ti, tj)
+            if d != PERIODIC:
+                # the layout's own lines no longer reach a ghost, as source or target
+                assert not is_ghost(g, tx, ty) and not is_ghost(g, *node(g, sa, si, sj))
+                continue
+            assert c < L.LCCP[1] and ta in lvl0 and sa in lvl0
+            assert is_ghost(g, tx, ty) and types[ta][tj, ti] == CB
+            assert node(g, sa, si, sj) == image(g, tx, ty)
+            assert types[sa][sj, si] != CB
+            # the first level-0 block computing the image node is the source
+            ix, iy = image(g, tx, ty)
+            first = next(b for b in lvl0 if 0 <= ix - g.Areas[b].base_x < g.Areas[b].nx
+                         and 0 <= iy - g.Areas[b].base_y < g.Areas[b].ny
+                         and types[b][int(iy - g.Areas[b].base_y), int(ix - g.Areas[b].base_x)] != CB)
+            assert first == sa
+            writers[(ta, ti, tj)] = writers.get((ta, ti, tj), 0) + 1
+    ghosts = {(a, i, j) for a in lvl0 for j in range(g.Areas[a].ny) for i in range(g.Areas[a].nx)
+              if is_ghost(g, *node(g, a, i, j))}
+    assert set(writers) == ghosts
+    assert set(writers.values()) == {1}
+
+
+def test_geo_init_takes_its_own_layout_again(mb):
+    g = mb.tgv_geometry(n=64, patch=32, levels=3)
+    g2 = mb.geo_init(g.layout, g.config)
+    assert bytes(g2) == bytes(g)
+    # without the periodic bit the ghost lines go and the ends come back
+    cfg = g.config
+    cfg.periodic = 0
+    plain = mb.geo_init(g.layout, cfg)
+    assert plain.layout.number_line2 == 16
+    assert all(plain.layout.NeborCC[c].direction != PERIODIC for c in range(16))
+
+
+def test_periodic_refuses_fine_blocks_on_a_wrapped_edge(mb):
+    cfg = mb.make_config(64, 64, 4, 30, 20, Re=20.0, periodic=mb.PERIODIC_Y)
+    with pytest.raises(mb.MBError):
+        mb.geo_init(mb.layout_builtin("2_2"), cfg)  # the fine half reaches y = LY-1
+    cfg.periodic = 4
+    with pytest.raises(mb.MBError):
+        mb.geo_init(mb.layout_builtin("1_1"), cfg)
+
+
+@pytest.mark.parametrize("name", ["tgv2", "channel_x"])
+def test_oracle_uniform_stream_stays_uniform(mb, orc, name):
+    """A uniform equilibrium is a fixed point of the step with periodic ghosts,
+    across the refinement interfaces too."""
+    g = CASES[name](mb)
+    if name == "channel_x":
+        cfg = g.config
+        cfg.obstacle = mb.OBST_NONE
+        g = mb.geo_init(g.layout, cfg)
+    o = orc.Oracle(g)
+    o.init()
+    o.evolution(30)
+    U = g.config.U0
+    for a in range(g.layout.number_area):
+        f = o.fields(a)
+        m = f["solid"] == FLUID
+        assert np.abs(f["ux"][m] - U[0]).max() < 1e-14
+        assert np.abs(f["uy"][m] - U[1]).max() < 1e-14
+        assert np.abs(f["rho"][m] - 1.0).max() < 1e-13
+
+
+def test_oracle_tgv_single_level_decays_at_the_exact_rate(mb, orc):
+    """u0 exp(-2 nu k^2 t) with nu = (tau - 1/2)/3: after the initial
+    adjustment the measured rate is within 0.5% of the exact one."""
+    g = CASES["tgv1"](mb)
+    o = orc.Oracle(g)
+    o.init()
+    mb.tgv_init(o, g)
+    nu = (g.Areas[0].tau - 0.5) / 3.0
+    k = 2 * np.pi / (g.config.LX - 2)
+    o.evolution(50)
+    a1 = mb.tgv_amplitude(o, g)
+    for _ in range(250):
+        o.evolution(1)
+    a2 = mb.tgv_amplitude(o, g)
+    rate = -np.log(a2 / a1) / 250
+    assert rate == pytest.approx(2 * nu * k * k, rel=5e-3)
+
+
+def test_oracle_tgv_two_levels_stays_close_to_the_exact_decay(mb, orc):
+    """With the refined patch the interface interpolation adds dissipation;
+    at 64 coarse cells and a 32-cell patch the amplitude stays within 1.5% of
+    the exact decay over 200 steps, and decays monotonically."""
+    g = CASES["tgv2"](mb)
+    o = orc.Oracle(g)
+    o.init()
+    mb.tgv_init(o, g)
+    a0 = mb.tgv_amplitude(o, g)
+    assert a0 == pytest.approx(0.01, rel=1e-12)
+    nu = (g.Areas[0].tau - 0.5) / 3.0
+    k = 2 * np.pi / (g.config.LX - 2)
+    prev = a0
+    for t in range(1, 201):
+        o.evolution(1)
+        if t % 50 == 0:
+            a = mb.tgv_amplitude(o, g)
+            assert a < prev
+            assert a == pytest.approx(a0 * np.exp(-2 * nu * k * k * t), rel=1.5e-2)
+            prev = a
+
+
+def test_tgv_golden_amplitudes_follow_the_exact_decay(mb):
+    """The oracle's full-size amplitudes (tests/golden/tgv_1024.json) lie
+    within 0.1% of u0 exp(-2 nu k^2 t)."""
+    import json
+    import os
+
+    from conftest import GOLDEN
+
+    with open(os.path.join(GOLDEN, "tgv_1024.json")) as f:
+        gold = json.load(f)
+    nu = (gold["tau"] - 0.5) / 3.0
+    k = 2 * np.pi / gold["n"]
+    assert gold["a0"] == pytest.approx(gold["u0"], rel=1e-12)
+    for t, a in gold["amplitude"].items():
+        assert a == pytest.approx(gold["a0"] * np.exp(-2 * nu * k * k * int(t)), rel=1e-3)
