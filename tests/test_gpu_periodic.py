@@ -22,7 +22,7 @@ import pytest
 
 from conftest import GOLDEN
 from test_gpu_parity import all_fields, rel_l2
-from test_periodic import CASES
+from test_periodic import CASES, poiseuille, poiseuille_profile_error, poiseuille_walls
 
 pytestmark = pytest.mark.gpu
 
@@ -129,3 +129,26 @@ def test_tgv_1024_two_levels_decay(mb, cuda_device):
     assert amp["f64"] == pytest.approx(exact, rel=1e-3)
     assert amp["f32"] == pytest.approx(amp["f64"], rel=5e-4)
     assert amp["f16s"] == pytest.approx(amp["f64"], rel=2e-3)
+
+
+@pytest.mark.parametrize("levels", [1, 2])
+def test_poiseuille_matches_oracle(mb, orc, cuda_device, levels):
+    """Body force, on-node walls and x-periodic ghosts together (the options
+    kernel with ghost copies), to the steady state: FP64 fields within 1e-12
+    of the oracle, FP32's profile error within 1e-4 of the oracle's."""
+    g, fx = poiseuille(mb, levels)
+    o = orc.Oracle(g)
+    o.init()
+    poiseuille_walls(o, g, fx)
+    o.evolution(12000)
+    for prec in ("f64", "f32"):
+        m = mb.MultiBlockLBM(g, prec)
+        m.init()
+        poiseuille_walls(m, g, fx)
+        m.evolution(12000)
+        if prec == "f64":
+            for fo, fm in zip(all_fields(o, g), all_fields(m, g)):
+                for k in ("rho", "ux", "uy", "F"):
+                    np.testing.assert_allclose(fm[k], fo[k], rtol=0, atol=1e-12, err_msg=k)
+        assert poiseuille_profile_error(m, g, fx) == pytest.approx(poiseuille_profile_error(o, g, fx), abs=1e-4)
+        m.close()

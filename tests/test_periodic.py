@@ -195,3 +195,76 @@ def test_tgv_golden_amplitudes_follow_the_exact_decay(mb):
     assert gold["a0"] == pytest.approx(gold["u0"], rel=1e-12)
     for t, a in gold["amplitude"].items():
         assert a == pytest.approx(gold["a0"] * np.exp(-2 * nu * k * k * int(t)), rel=1e-3)
+
+
+def poiseuille(mb, levels):
+    """Channel periodic in x with on-node bounce-back rows at y = 0 and
+    y = LY-1 (fluid rows 1..16), tau = 0.6, driven by a uniform body force;
+    2 levels: a refined patch [20,40] x [4,13] inside the channel."""
+    tau, fx = 0.6, 1e-6
+    nu = (tau - 0.5) / 3.0
+    LX, LY = (34, 18) if levels == 1 else (66, 18)
+    L = mb.layout_builtin("1_1") if levels == 1 else mb.layout_nested(LX, LY, [(20, 40, 4, 13)])
+    u_mean = (2.0 / 3.0) * fx * (1.0 - 0.5 / tau) * (LY - 2) ** 2 / (8.0 * nu)
+    cfg = mb.make_config(LX, LY, 1, 0, 0, U0=(u_mean, 0.0), Re=u_mean * 2.0 / nu, obstacle=False,
+                         periodic=mb.PERIODIC_X)
+    return mb.geo_init(L, cfg), fx
+
+
+def poiseuille_walls(sim, g, fx):
+    sim.set_body_force(fx, 0.0)
+    LY = g.config.LY
+    for a in range(g.layout.ASP[1]):
+        A = g.Areas[a]
+        t = sim.fields(a)["solid"].copy()
+        y = A.base_y + np.arange(A.ny)
+        for j in np.nonzero((y == 0.0) | (y == LY - 1.0))[0]:
+            t[j][t[j] == FLUID] = 1  # MB_SOLID_SBB
+        sim.set_cell_types(a, t)
+
+
+def poiseuille_profile_error(sim, g, fx):
+    """Largest deviation of ux on the middle column of the finest block from
+    F'/(2 nu) (y - 1/2)(LY - 3/2 - y), relative to its maximum.  The walls of
+    on-node bounce-back sit half-way to the first fluid row; F' = (1 - 1/(2
+    tau)) F is the momentum the reference's force term adds per step, its
+    velocity being sum(e f)/rho without a half-force shift."""
+    a = g.layout.number_area - 1
+    A, LY = g.Areas[a], g.config.LY
+    tau = g.Areas[0].tau
+    nu = (tau - 0.5) / 3.0
+    f = sim.fields(a)
+    i = A.nx // 2
+    y = A.base_y + np.arange(A.ny) / A.m
+    exact = fx * (1.0 - 0.5 / tau) / (2.0 * nu) * (y - 0.5) * (LY - 1.5 - y)
+    umax = fx * (1.0 - 0.5 / tau) * (LY - 2) ** 2 / (8.0 * nu)
+    m = f["solid"][:, i] == FLUID
+    return float(np.abs(f["ux"][m, i] - exact[m]).max() / umax)
+
+
+def test_oracle_poiseuille_single_level_matches_the_parabola(mb, orc):
+    g, fx = poiseuille(mb, 1)
+    o = orc.Oracle(g)
+    o.init()
+    poiseuille_walls(o, g, fx)
+    o.evolution(11000)
+    o.error_L2()
+    o.evolution(1000)
+    assert o.error_L2() < 2e-5  # change of u over the last 1000 steps: steady
+    assert poiseuille_profile_error(o, g, fx) < 6e-3  # measured 4.2e-3: the walls' slip
+
+
+def test_oracle_poiseuille_two_levels_stays_near_the_parabola(mb, orc):
+    """The refined patch has tau = 0.7, so the force term adds (1 - 1/1.4) F
+    there against (1 - 1/1.2) F on level 0: the patch is driven 1.7 times
+    harder and pulls the whole periodic channel along, 10% faster on level 0
+    and 14% of u_max above the single-level parabola in the patch."""
+    g, fx = poiseuille(mb, 2)
+    o = orc.Oracle(g)
+    o.init()
+    poiseuille_walls(o, g, fx)
+    o.evolution(11000)
+    o.error_L2()
+    o.evolution(1000)
+    assert o.error_L2() < 2e-5  # change of u over the last 1000 steps: steady
+    assert 0.1 < poiseuille_profile_error(o, g, fx) < 0.18  # measured 0.140
