@@ -274,7 +274,13 @@ int mb_set_bulk_occupancy(mb_ctx *ctx, int ctas_per_sm);
 /* Kernel fusions of the plan (bit mask; default 1).  Bit 0: the same-level
  * copies (c_c_boundary_transfer, multi/FH/assit_multi.h:2-46) of a level run
  * inside its block-step launch: each target cell computes its source's new
- * values itself.  Results are identical. */
+ * values itself.  Bit 1: the spline of a coarse-fine line
+ * (calculate_Spline3_gpu, assit_multi.h:136-185) also does the line's
+ * temporal interpolation (assit_multi.h:213-247) of the fine level's next
+ * substep, in place of a launch before that substep's block step; the spline
+ * then waits for the fine level's current substep, which on the 3-level
+ * cylinder costs more than the launch saves, so it is off by default.
+ * Results are identical. */
 int mb_set_fusion(mb_ctx *ctx, int flags);
 
 /* ---- collision and boundary options ----------------------------------------

@@ -73,6 +73,14 @@ template <bool EF, typename T> __device__ __forceinline__ void st_ef(T *p, T v) 
 __device__ __forceinline__ void pdl_trigger() { cudaTriggerProgrammaticLaunchCompletion(); }
 __device__ __forceinline__ void pdl_wait() { cudaGridDependencySynchronize(); }
 
+// temporal_interpolation (multi/FH/assit_multi.h:213-247) of one direction
+// from the three ring slots s0, s1, s2 of a fine point: one expression for
+// the record kernel and the spline's fused form, so both round alike
+template <typename R>
+__device__ __forceinline__ R temporal3(R a, R b, R c, R s0, R s1, R s2) {
+  return a * s0 - b * s1 + c * s2;
+}
+
 // feq, lbm/assit_func.h:2-9
 template <typename R>
 __device__ __forceinline__ R feq(int k, R rh, R uxx, R uyy) {
@@ -751,20 +759,23 @@ template <int P, bool INTERIOR>
 __global__ void __launch_bounds__(256, P == MB_PREC_F64 ? 4 : 6) k_block_step_r(const __grid_constant__ StbParams p) {
   pdl_trigger();
   pdl_wait();
-  const int cta = blockIdx.x;
-  int t = 0;
+  // a capped grid (bulk occupancy) walks the range tiles with a stride
 #pragma unroll 1
-  while (t + 1 < p.nblk && cta >= p.b[t + 1].cta0) t++;
-  const StbBlk &B = p.b[t];
-  const int local = (cta - B.cta0) * 256 + (int)threadIdx.x;
-  if (local >= B.rcells) return;
-  int r = __float2int_rz((float)local * B.rinv_w);
-  if (r * B.rw > local) r--;
-  else if ((r + 1) * B.rw <= local) r++;
-  const int j = B.row0 + r;
-  const int i = B.rcol0 + (local - r * B.rw);
-  if (p.evict_first) stb_cell_rows<P, true, INTERIOR>(p, B, i, j);
-  else stb_cell_rows<P, false, INTERIOR>(p, B, i, j);
+  for (long long cta = blockIdx.x; cta < p.rctas; cta += gridDim.x) {
+    int t = 0;
+#pragma unroll 1
+    while (t + 1 < p.nblk && cta >= p.b[t + 1].cta0) t++;
+    const StbBlk &B = p.b[t];
+    const int local = int(cta - B.cta0) * 256 + (int)threadIdx.x;
+    if (local >= B.rcells) continue;
+    int r = __float2int_rz((float)local * B.rinv_w);
+    if (r * B.rw > local) r--;
+    else if ((r + 1) * B.rw <= local) r++;
+    const int j = B.row0 + r;
+    const int i = B.rcol0 + (local - r * B.rw);
+    if (p.evict_first) stb_cell_rows<P, true, INTERIOR>(p, B, i, j);
+    else stb_cell_rows<P, false, INTERIOR>(p, B, i, j);
+  }
 }
 
 // ----------------------------------------------------------------------------
@@ -1151,12 +1162,17 @@ __device__ __forceinline__ void stb_quad_body(const StbParams &p, long long wt, 
 template <int P>
 __global__ void __launch_bounds__(256) k_block_step_q(const __grid_constant__ StbParams p) {
   pdl_trigger();
-  const long long wt = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long w0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
-  if (wt >= p.total) return;  // warp-uniform
+  if (w0 >= p.total) return;  // warp-uniform
   pdl_wait();
-  if (p.evict_first) stb_quad_body<P, true>(p, wt, lane);
-  else stb_quad_body<P, false>(p, wt, lane);
+  // a capped grid (bulk occupancy) walks the warp tiles with a stride
+  const long long stride = (long long)gridDim.x * (blockDim.x >> 5);
+#pragma unroll 1
+  for (long long wt = w0; wt < p.total; wt += stride) {
+    if (p.evict_first) stb_quad_body<P, true>(p, wt, lane);
+    else stb_quad_body<P, false>(p, wt, lane);
+  }
 }
 
 // ----------------------------------------------------------------------------
@@ -1253,7 +1269,7 @@ __device__ __forceinline__ void rec_point(const RecOpsParams &p, int t) {
       const int wi = (op.bits >> 4) & 3;
       const R a = (R)p.tw[wi][0], b = (R)p.tw[wi][1], cc = (R)p.tw[wi][2];
 #pragma unroll
-      for (int k = 0; k < 9; k++) v[k] = a * s[op.m0 * 9 + k] - b * s[op.m1 * 9 + k] + cc * s[op.m2 * 9 + k];
+      for (int k = 0; k < 9; k++) v[k] = temporal3<R>(a, b, cc, s[op.m0 * 9 + k], s[op.m1 * 9 + k], s[op.m2 * 9 + k]);
     } else {
 #pragma unroll
       for (int k = 0; k < 9; k++) v[k] = s[op.m2 * 9 + k];
@@ -1354,6 +1370,14 @@ struct SplTaskP {
   void *Mf[3];             // fine rho, ux, uy
   long long cplane;
   int cpitch, fpitch;
+  // fused temporal interpolation (tmp != 0): F of each fine edge point in
+  // buffer Ft <- tw0 s[tm0] - tw1 s[tm1] + tw2 s[tm2] of its slots, where
+  // mask[tmask_off + ip] is set
+  int tmp, tmask_off;
+  int tm[3];
+  double tw[3];
+  void *Ft;
+  long long fplane;
 };
 struct SplParamsP {
   int ntask, nseg;
@@ -1488,6 +1512,14 @@ __device__ __forceinline__ void spl_segment(const SplParamsP &p, int sid, int la
     for (int k = 0; k < 9; k++) {
       const R fe = feq<R>(k, out[0], out[1], out[2]);
       sl[k] = fe + para * (out[3 + k] - fe);
+    }
+    if (T.tmp && p.mask[T.tmask_off + ip]) {  // the fused temporal interpolation, from the slots just written
+      const R *s3 = slots + (long long)(T.slot0 + ip) * 27;
+      const R a = (R)T.tw[0], b = (R)T.tw[1], cc = (R)T.tw[2];
+      typename Prec<P>::S *Fd = (typename Prec<P>::S *)T.Ft;
+#pragma unroll
+      for (int k = 0; k < 9; k++)
+        st_f<P>(Fd, k * T.fplane + fc, k, temporal3<R>(a, b, cc, s3[T.tm[0] * 9 + k], s3[T.tm[1] * 9 + k], s3[T.tm[2] * 9 + k]));
     }
   }
 }

@@ -138,6 +138,7 @@ struct mb_ctx {
   std::vector<CcLevel> cc;
   std::vector<CcEntry *> d_cclist;  // per level: the copies of fusable levels (k_cc_pull)
   int fuse_cc = 1;
+  int fuse_tmp = 0;  // splines do the next temporal interpolation of their line (mb_set_fusion bit 1)
   // scheduler
   SchedState state;
   bool inited = false;
@@ -410,9 +411,10 @@ void stb_launch_shape(const mb_ctx *c, int level, int region, bool background, c
     *grid = dim3((unsigned)std::max<long long>((p.total + 255) / 256, 0));
     return;
   }
+  const long long cap = background_capped(c, background) ? (long long)c->bulk_ctas_per_sm * c->num_sms : (1LL << 31) - 1;
   if (stb_uses_quads(c, level, region)) {
     *func = kfunc<KStbQ>(c->prec);
-    *grid = dim3((unsigned)((p.total + 7) / 8));  // 8 warp tiles per CTA
+    *grid = dim3((unsigned)std::min<long long>((p.total + 7) / 8, cap));  // 8 warp tiles per CTA
     return;
   }
   if (c->stb_variant[level] == 5 && region == STB_INTERIOR && p.tb_items > 0) {
@@ -426,9 +428,9 @@ void stb_launch_shape(const mb_ctx *c, int level, int region, bool background, c
     *grid = dim3((unsigned)p.pctas);
     return;
   }
-  if (c->stb_variant[level] == 3 && region != STB_RIM && !background_capped(c, background) && rows_fit(c, p)) {
+  if (c->stb_variant[level] == 3 && region != STB_RIM && rows_fit(c, p)) {
     *func = region == STB_INTERIOR ? kfunc<KStbRI>(c->prec) : kfunc<KStbR>(c->prec);
-    *grid = dim3((unsigned)p.rctas);
+    *grid = dim3((unsigned)std::min<long long>(p.rctas, cap));
     return;
   }
   const bool two = c->stb_variant[level] == 2;
@@ -671,6 +673,14 @@ int lower_plan(mb_ctx *c, CompiledPlan &cp) {
         T.cplane = Cb.plane;
         T.cpitch = Cb.pitch;
         T.fpitch = Fb.pitch;
+        T.tmp = n.spl[t].tmp;
+        T.tmask_off = n.spl[t].tmask_off;
+        for (int q = 0; q < 3; q++) {
+          T.tm[q] = n.spl[t].tm[q];
+          T.tw[q] = n.spl[t].tw[q];
+        }
+        T.Ft = n.spl[t].tmp ? Fb.F[n.spl[t].tbuf] : nullptr;
+        T.fplane = Fb.plane;
         nseg += (L.Nc - 1 + SPL_SEG - 1) / SPL_SEG;
       }
       d.spl.ntask = (int)n.spl.size();
@@ -738,13 +748,16 @@ int build_graph(CompiledPlan &cp, bool pdl) {
       if (int e = set_priority(gn[q], d.background)) return e;
       continue;
     }
-    // programmatic edges from kernel producers: this kernel is scheduled once
-    // every producer CTA has started and waits in-kernel for their completion
+    // programmatic edges between kernels of the fine-level chain: this kernel
+    // is scheduled once every producer CTA has started and waits in-kernel
+    // for their completion.  Edges from or into background (bulk interior)
+    // nodes stay plain: early CTAs of a consumer would hold SM slots while
+    // waiting, slots the chain or the bulk work needs.
     std::vector<cudaGraphNode_t> plain;
     std::vector<cudaGraphNode_t> prog;
     for (int p : d.deps) {
       if (!gn[p]) continue;
-      (cp.dn[p].grid.x ? prog : plain).push_back(gn[p]);
+      (cp.dn[p].grid.x && !cp.dn[p].background && !d.background ? prog : plain).push_back(gn[p]);
     }
     MB_CUDA(cudaGraphAddKernelNode(&gn[q], cp.graph, plain.data(), plain.size(), &kp));
     if (int e = set_priority(gn[q], d.background)) return e;
@@ -927,7 +940,8 @@ int program_status(mb_ctx *c) {
 CompiledPlan *get_plan(mb_ctx *c, int n, bool final_macros, int *err, bool batch = false) {
   // batches and the persistent executor run the plain node kinds only
   const bool fuse = c->fuse_cc && !options_on(c) && !batch && c->use_graph != 3;
-  std::string key = c->state.key() + "/" + std::to_string(n) + (final_macros ? "F" : "P") + (fuse ? "c" : "");
+  std::string key = c->state.key() + "/" + std::to_string(n) + (final_macros ? "F" : "P") + (fuse ? "c" : "") +
+                    (c->fuse_tmp ? "t" : "");
   auto it = c->plans.find(key);
   if (it != c->plans.end()) return it->second.get();
   auto cp = std::make_unique<CompiledPlan>();
@@ -935,6 +949,7 @@ CompiledPlan *get_plan(mb_ctx *c, int n, bool final_macros, int *err, bool batch
   pc.split_cells = c->split_cells;
   pc.split_mask = c->split_mask;
   if (fuse) pc.cc = &c->cc;
+  pc.fuse_tmp = c->fuse_tmp != 0;
   SchedState s = c->state;
   cp->nodes = pc.compile(s, n, final_macros);
   cp->end = s;
@@ -950,7 +965,7 @@ CompiledPlan *get_plan(mb_ctx *c, int n, bool final_macros, int *err, bool batch
 // beside the rest of the plan where their reads and writes allow.
 CompiledPlan *get_diag_plan(mb_ctx *c, int n, int *err) {
   const bool fuse = c->fuse_cc && !options_on(c);
-  const std::string key = c->state.key() + "/" + std::to_string(n) + "D" + (fuse ? "c" : "");
+  const std::string key = c->state.key() + "/" + std::to_string(n) + "D" + (fuse ? "c" : "") + (c->fuse_tmp ? "t" : "");
   auto it = c->plans.find(key);
   if (it != c->plans.end()) return it->second.get();
   auto cp = std::make_unique<CompiledPlan>();
@@ -959,6 +974,7 @@ CompiledPlan *get_diag_plan(mb_ctx *c, int n, int *err) {
   pc.split_mask = c->split_mask;
   pc.drag_area = c->drag_area;
   if (fuse) pc.cc = &c->cc;
+  pc.fuse_tmp = c->fuse_tmp != 0;
   SchedState s = c->state;
   cp->nodes = pc.compile_diag(s, n);
   cp->end = s;
@@ -1382,9 +1398,10 @@ extern "C" int mb_set_cell_types(mb_ctx *c, int a, const int *types) {
 }
 
 extern "C" int mb_set_fusion(mb_ctx *c, int flags) {
-  if (!c || flags < 0 || flags > 1) return MB_ERR_INVALID;
+  if (!c || flags < 0 || flags > 3) return MB_ERR_INVALID;
   cudaDeviceSynchronize();
   c->fuse_cc = flags & 1;
+  c->fuse_tmp = (flags >> 1) & 1;
   c->plans.clear();
   return MB_OK;
 }

@@ -71,6 +71,11 @@ struct SplTask {
   int src_buf;    // current F buffer of the coarse block
   int m0;         // slot written (marker[0] at the time of the call)
   int mask_off;   // offset into the node's M-write mask (-1: write all points)
+  // the temporal interpolation of the line that follows, fused (tmp = 1): F
+  // of each fine edge point, buffer tbuf, <- tw0 s[tm0] - tw1 s[tm1] + tw2 s[tm2]
+  int tmp = 0, tbuf = 0, tmask_off = -1;
+  int tm[3] = {0, 0, 0};
+  double tw[3] = {0, 0, 0};
 };
 
 // NK_CCP: same-level copies beside a block step.  NK_DRAG: getDrag_block of
@@ -123,6 +128,12 @@ struct Op {
   int macro_all = 0;
   std::vector<int> parity;  // current buffer of every block at the call
   std::array<int, 3> mk{};  // ring markers of the line at the call
+  // SPL with the line's next temporal interpolation fused (fuse_temporal):
+  // the temporal op's xm, markers and block buffers
+  int tmp = 0;
+  double txm = 0;
+  std::array<int, 3> tmk{};
+  std::vector<int> tparity;
 };
 
 // Same-level copies (c_c_boundary_transfer) of one level with chains
@@ -156,6 +167,9 @@ struct PlanCompiler {
   unsigned split_mask = 0;
   // non-null: same-level copies of fusable levels run inside the block step
   const std::vector<CcLevel> *cc = nullptr;
+  // a spline of a coarse-fine line also does the line's temporal
+  // interpolation of the fine level's next substep (fuse_temporal)
+  bool fuse_tmp = false;
   PlanCompiler(const mb_geometry &g_, const std::vector<BlockLayout> &bl_,
                const std::vector<std::vector<uint8_t>> &fl, const std::vector<SplLine> &sl)
       : g(g_), bl(bl_), flags(fl), spl_lines(sl) {}

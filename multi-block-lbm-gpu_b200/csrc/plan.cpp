@@ -266,10 +266,52 @@ static inline void line_pt(const mb_p4 &p, int ip, int stride, int &i, int &j) {
   else { i = p.xstart + ip * stride; j = p.ystart; }
 }
 
+// A spline of line b runs at the place of b's next temporal interpolation
+// and does it too, when only ops of the fine level (its block steps and
+// same-level copies, splines and other lines' temporal interpolations) lie
+// between them.  None of those reads what the spline writes (slots of b,
+// rho/u of b's fine edge points, C_BOUNDARY cells the fine step leaves
+// alone) or writes what it reads (F and rho/u of coarse line cells), so the
+// spline may move there; the temporal interpolation itself stays in place.
+// The temporal launch before the fine step then leaves the fine chain.
+static std::vector<Op> fuse_temporal(const std::vector<Op> &ops) {
+  const int n = int(ops.size());
+  std::vector<int> with(n, -1);
+  std::vector<char> moved(n, 0);
+  for (int ti = 0; ti < n; ti++) {
+    const Op &t = ops[ti];
+    if (t.kind != Op::TEMPORAL) continue;
+    int si = ti - 1;
+    for (; si >= 0; si--) {
+      const Op &q = ops[si];
+      if (q.kind == Op::SPL && q.line == t.line) break;
+      const bool ok = q.kind == Op::SPL || ((q.kind == Op::STB || q.kind == Op::CC) && q.level == t.level) ||
+                      (q.kind == Op::TEMPORAL && q.level == t.level && q.line != t.line);
+      if (!ok) { si = -1; break; }
+    }
+    if (si < 0 || moved[si]) continue;
+    with[ti] = si;
+    moved[si] = 1;
+  }
+  std::vector<Op> out;
+  out.reserve(n);
+  for (int i = 0; i < n; i++) {
+    if (moved[i]) continue;
+    if (with[i] < 0) { out.push_back(ops[i]); continue; }
+    Op f = ops[with[i]];
+    f.tmp = 1;
+    f.txm = ops[i].xm;
+    f.tmk = ops[i].mk;
+    f.tparity = ops[i].parity;
+    out.push_back(f);
+  }
+  return out;
+}
+
 std::vector<PlanNode> PlanCompiler::compile(SchedState &s, int n_coarse, bool final_macros) const {
   std::vector<Op> ops;
   for (int n = 0; n < n_coarse; n++) emit(g, 0, s, ops, final_macros && n == n_coarse - 1);
-  return build(ops);
+  return build(fuse_tmp ? fuse_temporal(ops) : ops);
 }
 
 unsigned PlanCompiler::split_levels() const {
@@ -290,7 +332,13 @@ std::vector<PlanNode> PlanCompiler::compile_diag(SchedState &s, int n_coarse) co
   std::vector<Op> ops;
   const bool any_split = split_levels() != 0;
   for (int n = 0; n < n_coarse; n++) {
+    const size_t first = ops.size();
     emit(g, 0, s, ops, true);
+    if (fuse_tmp) {
+      std::vector<Op> step(ops.begin() + first, ops.end());
+      ops.resize(first);
+      for (Op &o : fuse_temporal(step)) ops.push_back(std::move(o));
+    }
     for (int part = any_split ? 0 : 1; part < 2; part++) {
       Op o;
       o.kind = Op::L2;
@@ -481,6 +529,7 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
     struct RP { uint64_t wF, wM; std::vector<uint64_t> rF, rM; };
     std::vector<RP> rparts;
     std::vector<uint64_t> spl_wM;
+    std::vector<uint64_t> tmp_w, tmp_r;  // fused temporal: F writes of the fine edge, slot reads
     SplTask task{};
     const bool is_spl = (o.kind == Op::SPL);
     double tw[3] = {0, 0, 0};
@@ -602,6 +651,25 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
       task.src_buf = pC;
       task.m0 = o.mk[0];
       task.mask_off = -1;
+      if (o.tmp) {  // the fused temporal interpolation: F of every fine edge point
+        const double xm = o.txm;
+        task.tmp = 1;
+        task.tbuf = o.tparity[Fb];
+        task.tw[0] = 0.5 * (xm - 1.0) * xm;
+        task.tw[1] = (xm - 1.0) * (xm + 1.0);
+        task.tw[2] = 0.5 * xm * (xm + 1.0);
+        std::vector<uint64_t> sr;
+        for (int q = 0; q < 3; q++) {
+          task.tm[q] = o.tmk[q];
+          sr.push_back(key(RK_SLOT, o.line, o.tmk[q]));
+        }
+        for (int ip = 0; ip < l.Nf; ip++) {
+          int i, j;
+          line_pt(l.line_F, ip, 1, i, j);
+          tmp_w.push_back(fkey(task.tbuf, Fb, pitch_cell(Fb, i, j)));
+        }
+        tmp_r = sr;
+      }
     }
     for (size_t q = 0; q < rparts.size(); q++) {
       if (rparts[q].wF == ~0ull) continue;
@@ -613,6 +681,7 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
       }
       lastw[rparts[q].wF] = w;
     }
+    for (auto k : tmp_w) lastw[k] = LastWrite{int(oi)};
     for (auto &rp : rparts) {
       for (auto k : rp.rF) ac.read(k);
       for (auto k : rp.rM) ac.read(k);
@@ -622,6 +691,8 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
     for (auto k : I.always_r) ac.read(k);
     for (auto k : I.always_w) ac.write(k);
     for (auto k : spl_wM) ac.write(k);
+    for (auto k : tmp_w) ac.write(k);
+    for (auto k : tmp_r) ac.read(k);
 
     const NodeKind want = is_spl ? NK_SPL : NK_REC;
     bool join = (open >= 0 && nodes[open].kind == want);
@@ -698,6 +769,13 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
       for (size_t q = 0; q < spl_wM.size(); q++) {
         I.parts.push_back({open, task.mask_off + int(q), 0, spl_wM[q], {}});
         nd.spl_mask.push_back(1);
+      }
+      if (task.tmp) {
+        task.tmask_off = int(nd.spl_mask.size());
+        for (size_t q = 0; q < tmp_w.size(); q++) {
+          I.parts.push_back({open, task.tmask_off + int(q), 0, tmp_w[q], tmp_r});
+          nd.spl_mask.push_back(1);
+        }
       }
       nd.spl.push_back(task);
     }

@@ -525,7 +525,8 @@ class MultiBlockLBM:
         _check(self.lib.mb_set_cta_spread(self.h, int(spline_kb), int(records_kb)), "mb_set_cta_spread")
 
     def set_fusion(self, flags):
-        """Plan fusions (bit 0: same-level copies inside the block step); results are identical."""
+        """Plan fusions (bit 0: same-level copies inside the block step; bit 1: temporal
+        interpolations inside the splines); results are identical."""
         _check(self.lib.mb_set_fusion(self.h, int(flags)), "mb_set_fusion")
 
     def set_collision(self, kind, s_e=0.0, s_eps=0.0, s_q=0.0):

@@ -383,11 +383,12 @@ def test_step_diag_equals_step_by_step(mb, cuda_device, prec, split, graph):
 @pytest.mark.parametrize("split,variant", [(10**12, 0), (0, 0), (10**12, 4), (0, 3)])
 @pytest.mark.parametrize("name,prec", [("n3", "f32"), ("g49", "f64"), ("g25", "f16s")])
 def test_fused_copies_bitwise(mb, cuda_device, name, prec, split, variant, graph):
-    """Same-level copies done inside the block step (mb_set_fusion bit 0, the
-    default) give bitwise the state of separate copy launches."""
+    """Same-level copies done inside the block step (mb_set_fusion bit 0) and
+    temporal interpolations done by the splines (bit 1), alone and together
+    (the default), give bitwise the state of separate launches."""
     g = mb.geo_init(*make_ref.case(name)[:2])
     sims = []
-    for fuse in (0, 1):
+    for fuse in (0, 1, 2, 3):
         s = mb.MultiBlockLBM(g, prec, graph=graph)
         s.set_fusion(fuse)
         s.set_split_cells(split)
@@ -396,9 +397,11 @@ def test_fused_copies_bitwise(mb, cuda_device, name, prec, split, variant, graph
         s.init()
         s.evolution(13)
         sims.append(s)
-    for k in range(g.layout.number_area):
-        fa, fb = sims[0].fields(k), sims[1].fields(k)
-        for key in ("F", "rho", "ux", "uy"):
-            assert np.array_equal(fa[key], fb[key]), (k, key)
-    assert sims[0].getDrag_block()[2] == sims[1].getDrag_block()[2]
-    assert sims[0].error_L2() == sims[1].error_L2()
+    cd0, l20 = sims[0].getDrag_block()[2], sims[0].error_L2()
+    for other in sims[1:]:
+        for k in range(g.layout.number_area):
+            fa, fb = sims[0].fields(k), other.fields(k)
+            for key in ("F", "rho", "ux", "uy"):
+                assert np.array_equal(fa[key], fb[key]), (k, key)
+        assert cd0 == other.getDrag_block()[2]
+        assert l20 == other.error_L2()
