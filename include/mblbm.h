@@ -264,8 +264,8 @@ int mb_set_stream_cells(mb_ctx *ctx, long long cells, int bulk);
  * 5 = bulk asynchronous copies: persistent CTAs stage the nine input row
  * segments of 256 cells in shared memory with cp.async.bulk and mbarriers
  * (interiors of split levels; the other regions use 0).
- * Default 0; level 0 uses 3 in MB_PREC_F16S and 1 in MB_PREC_F32 and
- * MB_PREC_F32U.  Results are identical. */
+ * Default 0; every level uses 4 in MB_PREC_F16S, level 0 uses 1 in
+ * MB_PREC_F32 and MB_PREC_F32U.  Results are identical. */
 int mb_set_stb_variant(mb_ctx *ctx, int level, int variant);
 /* Caps the grid of interior (bulk) block-step launches at ctas_per_sm CTAs of
  * 256 threads per SM (0 = uncapped), leaving CTA slots on every SM for the

@@ -759,23 +759,20 @@ template <int P, bool INTERIOR>
 __global__ void __launch_bounds__(256, P == MB_PREC_F64 ? 4 : 6) k_block_step_r(const __grid_constant__ StbParams p) {
   pdl_trigger();
   pdl_wait();
-  // a capped grid (bulk occupancy) walks the range tiles with a stride
+  const int cta = blockIdx.x;
+  int t = 0;
 #pragma unroll 1
-  for (long long cta = blockIdx.x; cta < p.rctas; cta += gridDim.x) {
-    int t = 0;
-#pragma unroll 1
-    while (t + 1 < p.nblk && cta >= p.b[t + 1].cta0) t++;
-    const StbBlk &B = p.b[t];
-    const int local = int(cta - B.cta0) * 256 + (int)threadIdx.x;
-    if (local >= B.rcells) continue;
-    int r = __float2int_rz((float)local * B.rinv_w);
-    if (r * B.rw > local) r--;
-    else if ((r + 1) * B.rw <= local) r++;
-    const int j = B.row0 + r;
-    const int i = B.rcol0 + (local - r * B.rw);
-    if (p.evict_first) stb_cell_rows<P, true, INTERIOR>(p, B, i, j);
-    else stb_cell_rows<P, false, INTERIOR>(p, B, i, j);
-  }
+  while (t + 1 < p.nblk && cta >= p.b[t + 1].cta0) t++;
+  const StbBlk &B = p.b[t];
+  const int local = (cta - B.cta0) * 256 + (int)threadIdx.x;
+  if (local >= B.rcells) return;
+  int r = __float2int_rz((float)local * B.rinv_w);
+  if (r * B.rw > local) r--;
+  else if ((r + 1) * B.rw <= local) r++;
+  const int j = B.row0 + r;
+  const int i = B.rcol0 + (local - r * B.rw);
+  if (p.evict_first) stb_cell_rows<P, true, INTERIOR>(p, B, i, j);
+  else stb_cell_rows<P, false, INTERIOR>(p, B, i, j);
 }
 
 // ----------------------------------------------------------------------------
@@ -1162,17 +1159,12 @@ __device__ __forceinline__ void stb_quad_body(const StbParams &p, long long wt, 
 template <int P>
 __global__ void __launch_bounds__(256) k_block_step_q(const __grid_constant__ StbParams p) {
   pdl_trigger();
-  const long long w0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long wt = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
-  if (w0 >= p.total) return;  // warp-uniform
+  if (wt >= p.total) return;  // warp-uniform
   pdl_wait();
-  // a capped grid (bulk occupancy) walks the warp tiles with a stride
-  const long long stride = (long long)gridDim.x * (blockDim.x >> 5);
-#pragma unroll 1
-  for (long long wt = w0; wt < p.total; wt += stride) {
-    if (p.evict_first) stb_quad_body<P, true>(p, wt, lane);
-    else stb_quad_body<P, false>(p, wt, lane);
-  }
+  if (p.evict_first) stb_quad_body<P, true>(p, wt, lane);
+  else stb_quad_body<P, false>(p, wt, lane);
 }
 
 // ----------------------------------------------------------------------------

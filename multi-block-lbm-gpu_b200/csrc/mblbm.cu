@@ -49,6 +49,7 @@ struct L2Part {
 struct DevPlanNode {
   NodeKind kind;
   bool background = false;  // bandwidth-bound bulk work: lowest scheduling priority
+  bool slack = false;       // off the estimated critical path: one priority step below the chain
   // launch
   void *func = nullptr;
   dim3 grid, block;
@@ -411,10 +412,9 @@ void stb_launch_shape(const mb_ctx *c, int level, int region, bool background, c
     *grid = dim3((unsigned)std::max<long long>((p.total + 255) / 256, 0));
     return;
   }
-  const long long cap = background_capped(c, background) ? (long long)c->bulk_ctas_per_sm * c->num_sms : (1LL << 31) - 1;
-  if (stb_uses_quads(c, level, region)) {
+  if (stb_uses_quads(c, level, region)) {  // the quad grid is never capped
     *func = kfunc<KStbQ>(c->prec);
-    *grid = dim3((unsigned)std::min<long long>((p.total + 7) / 8, cap));  // 8 warp tiles per CTA
+    *grid = dim3((unsigned)((p.total + 7) / 8));  // 8 warp tiles per CTA
     return;
   }
   if (c->stb_variant[level] == 5 && region == STB_INTERIOR && p.tb_items > 0) {
@@ -428,9 +428,9 @@ void stb_launch_shape(const mb_ctx *c, int level, int region, bool background, c
     *grid = dim3((unsigned)p.pctas);
     return;
   }
-  if (c->stb_variant[level] == 3 && region != STB_RIM && rows_fit(c, p)) {
+  if (c->stb_variant[level] == 3 && region != STB_RIM && !background_capped(c, background) && rows_fit(c, p)) {
     *func = region == STB_INTERIOR ? kfunc<KStbRI>(c->prec) : kfunc<KStbR>(c->prec);
-    *grid = dim3((unsigned)std::min<long long>(p.rctas, cap));
+    *grid = dim3((unsigned)p.rctas);
     return;
   }
   const bool two = c->stb_variant[level] == 2;
@@ -713,18 +713,47 @@ int run_direct(CompiledPlan &cp, cudaStream_t s) {
 }
 
 // Interior nodes of split levels get the lowest priority and every other
-// kernel the highest: pending CTAs of the latency-bound fine-level chain are
-// then dispatched ahead of the queued bulk CTAs as SMs free up.
-int set_priority(cudaGraphNode_t node, bool background) {
+// kernel the highest, one step less for nodes with slack: pending CTAs of the
+// latency-bound fine-level chain are then dispatched ahead of the queued bulk
+// CTAs as SMs free up, and a fine-level step that can wait (the first
+// substep of a level, beside the coarser level's step) yields to the chain.
+int set_priority(cudaGraphNode_t node, bool background, bool slack = false) {
   int least = 0, greatest = 0;
   MB_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
   cudaKernelNodeAttrValue v{};
-  v.priority = background ? least : greatest;
+  v.priority = background ? least : (slack && greatest < least ? greatest + 1 : greatest);
   MB_CUDA(cudaGraphKernelNodeSetAttribute(node, cudaKernelNodeAttributePriority, &v));
   return MB_OK;
 }
 
+// Marks the nodes whose start may slip by more than SLACK_US without
+// lengthening the plan, by longest paths over a rough cost model of each
+// launch (a fixed latency plus a term in its CTAs; bulk nodes cost nothing
+// here, as they run beside the chain).
+constexpr double SLACK_US = 3.0;
+void mark_slack(CompiledPlan &cp) {
+  const int nd = (int)cp.dn.size();
+  std::vector<double> cost(nd, 0), head(nd, 0), tail(nd, 0);
+  for (int q = 0; q < nd; q++) {
+    const DevPlanNode &d = cp.dn[q];
+    if (d.grid.x == 0 || d.background) continue;
+    if (d.kind == NK_STB) cost[q] = 2.0 + d.grid.x / 200.0;
+    else if (d.kind == NK_SPL) cost[q] = 4.0 + d.grid.x / 20.0;
+    else if (d.kind == NK_REC) cost[q] = 3.0 + d.grid.x / 100.0;
+    else cost[q] = 2.0;
+  }
+  for (int q = 0; q < nd; q++)  // nodes are in topological order
+    for (int p : cp.dn[q].deps) head[q] = std::max(head[q], head[p] + cost[p]);
+  for (int q = nd - 1; q >= 0; q--) tail[q] = std::max(tail[q], cost[q]);
+  for (int q = nd - 1; q >= 0; q--)
+    for (int p : cp.dn[q].deps) tail[p] = std::max(tail[p], cost[p] + tail[q]);
+  double T = 0;
+  for (int q = 0; q < nd; q++) T = std::max(T, head[q] + tail[q]);
+  for (int q = 0; q < nd; q++) cp.dn[q].slack = T - (head[q] + tail[q]) > SLACK_US;
+}
+
 int build_graph(CompiledPlan &cp, bool pdl) {
+  mark_slack(cp);
   MB_CUDA(cudaGraphCreate(&cp.graph, 0));
   std::vector<cudaGraphNode_t> gn(cp.dn.size(), nullptr);
   for (size_t q = 0; q < cp.dn.size(); q++) {
@@ -745,7 +774,7 @@ int build_graph(CompiledPlan &cp, bool pdl) {
     kp.extra = nullptr;
     if (!pdl) {
       MB_CUDA(cudaGraphAddKernelNode(&gn[q], cp.graph, deps.data(), deps.size(), &kp));
-      if (int e = set_priority(gn[q], d.background)) return e;
+      if (int e = set_priority(gn[q], d.background, d.slack)) return e;
       continue;
     }
     // programmatic edges between kernels of the fine-level chain: this kernel
@@ -760,7 +789,7 @@ int build_graph(CompiledPlan &cp, bool pdl) {
       (cp.dn[p].grid.x && !cp.dn[p].background && !d.background ? prog : plain).push_back(gn[p]);
     }
     MB_CUDA(cudaGraphAddKernelNode(&gn[q], cp.graph, plain.data(), plain.size(), &kp));
-    if (int e = set_priority(gn[q], d.background)) return e;
+    if (int e = set_priority(gn[q], d.background, d.slack)) return e;
     for (cudaGraphNode_t from : prog) {
       cudaGraphEdgeData ed{};
       ed.from_port = cudaGraphKernelNodePortProgrammatic;
@@ -1040,11 +1069,14 @@ extern "C" int mb_create(const mb_geometry *geo, int precision, mb_ctx **out) {
   // fine levels gains 5% (FP32) and 13% (FP16 storage) per step once the
   // spline launches spread over the SMs (mb_set_cta_spread); FP64 unmeasured
   c->split_cells = precision == MB_PREC_F64 ? (1LL << 62) : 1000000;
-  // level 0 of config 2, measured per coarse step: FP16 storage is
-  // issue-bound and the cell-range kernel issues a quarter fewer
-  // instructions (106 against 109 us); FP32 storage gains from the quads'
-  // vector accesses (112 against 117 us with the split level 0)
-  if (precision == MB_PREC_F16S) c->stb_variant[0] = 3;
+  // measured per coarse step of the 3-level cylinder: FP16 storage steps
+  // cell pairs on every level, whose shared addresses and paired accesses
+  // cut its issue-bound instruction count (85.4 against 86.7 us with cell
+  // ranges on level 0 and one cell per thread elsewhere; level 0 alone 39.7
+  // against 46.0 us); FP32 storage gains from the quads' vector accesses on
+  // level 0 (112 against 117 us with the split level 0)
+  if (precision == MB_PREC_F16S)
+    for (int l = 0; l < MB_MAX_LEVEL; l++) c->stb_variant[l] = 4;
   if (precision == MB_PREC_F32 || precision == MB_PREC_F32U) c->stb_variant[0] = 1;
   cudaGetDevice(&c->device);
   cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device);
