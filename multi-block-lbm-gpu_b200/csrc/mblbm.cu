@@ -72,7 +72,7 @@ struct CompiledPlan {
   cudaGraphExec_t exec = nullptr;
   SchedState end;
   long long kernels = 0;
-  double *d_diag_res = nullptr;  // diagnostic plans: Fx, Fy and the two L2 sums of both parts, per coarse step
+  double *d_diag_res = nullptr;  // diagnostic plans: Fx, Fy and the two L2 sums of every part, per coarse step
   int diag_steps = 0;
   // persistent executor (graph mode 3)
   bool prg_built = false;
@@ -115,9 +115,9 @@ struct mb_ctx {
   double *h_drag_out = nullptr;  // pinned
   // L2
   // error_L2 in two parts (interiors of split levels, the rest), per split mask
-  std::map<unsigned, std::array<L2Part, 2>> l2parts;
-  double2 *d_l2_partial[2] = {nullptr, nullptr};  // per part: parts may run concurrently
-  unsigned int *d_l2_ticket[2] = {nullptr, nullptr};
+  std::map<unsigned, std::array<L2Part, L2_NPARTS>> l2parts;
+  double2 *d_l2_partial[L2_NPARTS] = {};  // per part: parts may run concurrently
+  unsigned int *d_l2_ticket[L2_NPARTS] = {};
   double *d_l2_out = nullptr;
   double *h_l2_out = nullptr;  // pinned
   int l2_grid = 0;
@@ -447,9 +447,9 @@ void stb_launch_shape(const mb_ctx *c, int level, int region, bool background, c
 int l2_parts(mb_ctx *c, unsigned mask, const L2Part **out) {
   auto it = c->l2parts.find(mask);
   if (it == c->l2parts.end()) {
-    std::array<L2Part, 2> parts;
+    std::array<L2Part, L2_NPARTS> parts;
     const mb_layout &L = c->geo.layout;
-    for (int q = 0; q < 2; q++) {
+    for (int q = 0; q < L2_NPARTS; q++) {
       std::vector<L2Blk> bx;
       long long tiles = 0;
       auto add = [&](int a, int i0, int j0, int w, int h) {
@@ -469,6 +469,7 @@ int l2_parts(mb_ctx *c, unsigned mask, const L2Part **out) {
       };
       for (int l = 0; l < L.LEVEL; l++) {
         const bool sp = (mask >> l) & 1;
+        if (q != 0 && q != 1 + l) continue;
         for (int a = L.ASP[l]; a < L.ASP[l + 1]; a++) {
           const int nx = c->bl[a].nx, ny = c->bl[a].ny;
           const bool inner = sp && nx > 4 && ny > 4;
@@ -500,11 +501,13 @@ int l2_parts(mb_ctx *c, unsigned mask, const L2Part **out) {
   return MB_OK;
 }
 
-// CTAs of a part's launch: the interiors' part runs beside the fine levels'
-// chain with two CTAs per SM, so that the chain's launches find free slots
-// (the same grid everywhere: the sums' order follows the grid)
+// CTAs of a part's launch: two per SM at most, so that the parts running
+// beside the fine levels' chain (the interiors, and each level's part at the
+// turn of a step) leave the chain's launches free slots (the same grid
+// everywhere: the sums' order follows the grid)
 int l2_grid_of(const mb_ctx *c, const L2Part *pt, int q) {
-  return q == 0 ? std::min(pt[q].grid, 2 * c->num_sms) : pt[q].grid;
+  (void)q;
+  return std::min(pt[q].grid, 2 * c->num_sms);
 }
 
 L2Params l2_params(mb_ctx *c, const L2Part *pt, int q, double *out) {
@@ -533,9 +536,10 @@ int lower_plan(mb_ctx *c, CompiledPlan &cp) {
   for (const PlanNode &n : cp.nodes)
     if (n.kind == NK_DRAG || n.kind == NK_L2) cp.diag_steps = std::max(cp.diag_steps, n.level + 1);
   if (cp.diag_steps > 0) {  // zero: a part without cells adds nothing
-    if (cudaMalloc(&cp.d_diag_res, (size_t)cp.diag_steps * 6 * sizeof(double)) != cudaSuccess) return MB_ERR_NOMEM;
+    const size_t bytes = (size_t)cp.diag_steps * DIAG_STRIDE * sizeof(double);
+    if (cudaMalloc(&cp.d_diag_res, bytes) != cudaSuccess) return MB_ERR_NOMEM;
     cp.dev_allocs.push_back(cp.d_diag_res);
-    MB_CUDA(cudaMemset(cp.d_diag_res, 0, (size_t)cp.diag_steps * 6 * sizeof(double)));
+    MB_CUDA(cudaMemset(cp.d_diag_res, 0, bytes));
   }
   for (size_t q = 0; q < cp.nodes.size(); q++) {
     const PlanNode &n = cp.nodes[q];
@@ -556,10 +560,10 @@ int lower_plan(mb_ctx *c, CompiledPlan &cp) {
       }
       d.args[0] = &d.stb;
     } else if (n.kind == NK_L2) {
-      const int part = n.region == STB_INTERIOR ? 0 : 1;
+      const int part = n.part;
       const L2Part *pt = nullptr;
       if (int e = l2_parts(c, (unsigned)n.a0, &pt)) return e;
-      d.l2 = l2_params(c, pt, part, cp.d_diag_res + 6 * n.level + 2 + 2 * part);
+      d.l2 = l2_params(c, pt, part, cp.d_diag_res + DIAG_STRIDE * n.level + 2 + 2 * part);
       d.func = kfunc<KL2>(c->prec);
       d.block = dim3(256);
       d.grid = dim3((unsigned)l2_grid_of(c, pt, part));
@@ -574,7 +578,7 @@ int lower_plan(mb_ctx *c, CompiledPlan &cp) {
       d.drag.F = B.F[((n.parity >> a) & 1) ^ 1];  // the buffer the block's last step read
       d.drag.plane = B.plane;
       for (int k = 0; k < 9; k++) d.drag.feqc[k] = c->feqc[k];
-      d.drag.out = cp.d_diag_res + 6 * n.level;
+      d.drag.out = cp.d_diag_res + DIAG_STRIDE * n.level;
       d.func = kfunc<KDrag>(c->prec);
       d.block = dim3(1024);
       d.grid = dim3(1);
@@ -1251,13 +1255,13 @@ extern "C" int mb_create(const mb_geometry *geo, int precision, mb_ctx **out) {
     c->total_cells = cell;
     c->l2_tiles = (int)tiles;
     c->l2_grid = (int)std::min<long long>(tiles, 148LL * 8);
-    for (int q = 0; q < 2; q++) {
+    for (int q = 0; q < L2_NPARTS; q++) {
       if ((e = dalloc(c.get(), &c->d_l2_partial[q], c->l2_grid))) return e;
       if ((e = dalloc(c.get(), &c->d_l2_ticket[q], 1))) return e;
       MB_CUDA(cudaMemset(c->d_l2_ticket[q], 0, sizeof(unsigned int)));
     }
-    if ((e = dalloc(c.get(), &c->d_l2_out, 4))) return e;
-    MB_CUDA(cudaMallocHost(&c->h_l2_out, 4 * sizeof(double)));
+    if ((e = dalloc(c.get(), &c->d_l2_out, 2 * L2_NPARTS))) return e;
+    MB_CUDA(cudaMallocHost(&c->h_l2_out, 2 * L2_NPARTS * sizeof(double)));
   }
   if ((e = dalloc(c.get(), &c->d_count, 1))) return e;
 
@@ -1774,14 +1778,15 @@ int launch_drag(mb_ctx *c, double *out, cudaStream_t s) {
   return MB_OK;
 }
 
-// error_L2's kernel part: the two weighted sums of the interiors of the
-// split levels into out[0..1] (zero when there are none) and of every other
-// cell into out[2..3] (device memory); the host adds the parts in that order
+// error_L2's kernel part: the two weighted sums of each part (the interiors
+// of the split levels, then each level's other cells) into out[2q..2q+1]
+// (device memory; zero for a part without cells); the host adds the parts
+// in that order
 int launch_l2(mb_ctx *c, double *out, cudaStream_t s) {
   const L2Part *pt = nullptr;
   if (int e = l2_parts(c, current_split_levels(c), &pt)) return e;
-  if (pt[0].grid == 0) MB_CUDA(cudaMemsetAsync(out, 0, 2 * sizeof(double), s));
-  for (int q = 0; q < 2; q++) {
+  MB_CUDA(cudaMemsetAsync(out, 0, 2 * L2_NPARTS * sizeof(double), s));
+  for (int q = 0; q < L2_NPARTS; q++) {
     if (pt[q].grid == 0) continue;
     L2Params p = l2_params(c, pt, q, out + 2 * q);
     void *args[] = {&p};
@@ -1790,7 +1795,14 @@ int launch_l2(mb_ctx *c, double *out, cudaStream_t s) {
   return MB_OK;
 }
 
-double l2_value(const double *v) { return std::sqrt(v[0] + v[2]) / std::sqrt(v[1] + v[3]); }
+double l2_value(const double *v) {
+  double num = v[0], den = v[1];
+  for (int q = 1; q < L2_NPARTS; q++) {
+    num += v[2 * q];
+    den += v[2 * q + 1];
+  }
+  return std::sqrt(num) / std::sqrt(den);
+}
 
 double drag_norm(const mb_ctx *c) {
   const mb_config &cfg = c->geo.config;
@@ -1827,7 +1839,7 @@ extern "C" int mb_error_L2(mb_ctx *c, double *e, mb_stream stream) {
   if (!c->inited) return MB_ERR_STATE;
   cudaStream_t s = (cudaStream_t)stream;
   if (int r = launch_l2(c, c->d_l2_out, s)) return r;
-  MB_CUDA(cudaMemcpyAsync(c->h_l2_out, c->d_l2_out, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  MB_CUDA(cudaMemcpyAsync(c->h_l2_out, c->d_l2_out, 2 * L2_NPARTS * sizeof(double), cudaMemcpyDeviceToHost, s));
   MB_CUDA(cudaStreamSynchronize(s));
   if (int st = program_status(c)) return st;
   *e = l2_value(c->h_l2_out);
@@ -1850,8 +1862,8 @@ extern "C" int mb_step_diag(mb_ctx *c, int n, double *cd, double *cl, double *er
     c->h_diag = nullptr;
     c->diag_cap = 0;
     const size_t cap = std::max<size_t>((size_t)n, 2 * c->diag_cap);
-    if (cudaMalloc(&c->d_diag, cap * 6 * sizeof(double)) != cudaSuccess) return MB_ERR_NOMEM;
-    if (cudaMallocHost(&c->h_diag, cap * 6 * sizeof(double)) != cudaSuccess) return MB_ERR_NOMEM;
+    if (cudaMalloc(&c->d_diag, cap * DIAG_STRIDE * sizeof(double)) != cudaSuccess) return MB_ERR_NOMEM;
+    if (cudaMallocHost(&c->h_diag, cap * DIAG_STRIDE * sizeof(double)) != cudaSuccess) return MB_ERR_NOMEM;
     c->diag_cap = cap;
   }
   c->kernels_last_call = 0;
@@ -1864,7 +1876,7 @@ extern "C" int mb_step_diag(mb_ctx *c, int n, double *cd, double *cl, double *er
       CompiledPlan *cp = get_diag_plan(c, chunk, &e);
       if (!cp) return e ? e : MB_ERR_INVALID;
       if ((e = exec_plan(c, cp, s))) return e;
-      MB_CUDA(cudaMemcpyAsync(c->h_diag + 6 * q, cp->d_diag_res, (size_t)chunk * 6 * sizeof(double),
+      MB_CUDA(cudaMemcpyAsync(c->h_diag + DIAG_STRIDE * q, cp->d_diag_res, (size_t)chunk * DIAG_STRIDE * sizeof(double),
                               cudaMemcpyDeviceToHost, s));
       q += chunk;
     }
@@ -1874,9 +1886,10 @@ extern "C" int mb_step_diag(mb_ctx *c, int n, double *cd, double *cl, double *er
       CompiledPlan *cp = get_plan(c, 1, true, &e);
       if (!cp) return e ? e : MB_ERR_INVALID;
       if ((e = exec_plan(c, cp, s))) return e;
-      if ((e = launch_drag(c, c->d_diag + 6 * q, s))) return e;
-      if ((e = launch_l2(c, c->d_diag + 6 * q + 2, s))) return e;
-      MB_CUDA(cudaMemcpyAsync(c->h_diag + 6 * q, c->d_diag + 6 * q, 6 * sizeof(double), cudaMemcpyDeviceToHost, s));
+      if ((e = launch_drag(c, c->d_diag + DIAG_STRIDE * q, s))) return e;
+      if ((e = launch_l2(c, c->d_diag + DIAG_STRIDE * q + 2, s))) return e;
+      MB_CUDA(cudaMemcpyAsync(c->h_diag + DIAG_STRIDE * q, c->d_diag + DIAG_STRIDE * q, DIAG_STRIDE * sizeof(double),
+                              cudaMemcpyDeviceToHost, s));
       c->kernels_last_call += 2;
     }
   }
@@ -1884,7 +1897,7 @@ extern "C" int mb_step_diag(mb_ctx *c, int n, double *cd, double *cl, double *er
   if (int st = program_status(c)) return st;
   const double den = drag_norm(c);
   for (int q = 0; q < n; q++) {
-    const double *v = c->h_diag + 6 * q;
+    const double *v = c->h_diag + DIAG_STRIDE * q;
     if (cd) cd[q] = v[0] / den;
     if (cl) cl[q] = v[1] / den;
     if (err) err[q] = l2_value(v + 2);

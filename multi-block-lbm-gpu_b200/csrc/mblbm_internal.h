@@ -64,6 +64,11 @@ struct SplLine {
 // every op, line and block descriptor, see kernels.cuh).
 constexpr int PLAN_MAX_REC_OPS = 24;
 constexpr int PLAN_MAX_SPL_TASKS = 16;
+// error_L2 parts: 0 the interiors of split levels, 1 + l level l (its rim
+// when split, every cell otherwise); per coarse step a diagnostic plan
+// stores Fx, Fy and the two sums of every part
+constexpr int L2_NPARTS = 1 + MB_MAX_LEVEL;
+constexpr int DIAG_STRIDE = 2 + 2 * L2_NPARTS;
 
 // One line of a spline node.
 struct SplTask {
@@ -95,6 +100,7 @@ struct PlanNode {
   uint64_t parity = 0;        // STB: current buffer of each block before the step
   int macro_all = 0;          // STB: write rho/u of every FLUID cell
   int ccpull = 0;             // STB: skips CF_CCPULL cells (an NK_CCP node of the same level writes them)
+  int part = 0;               // L2: the error_L2 part (L2_NPARTS)
   std::vector<Rec> recs;      // REC
   std::vector<std::pair<int, int>> ops;  // REC: (first record, count) of each reference line op
   double tw[4][3] = {};       // REC: temporal weight triples (a, b, c)

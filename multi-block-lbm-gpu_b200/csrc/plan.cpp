@@ -325,9 +325,11 @@ unsigned PlanCompiler::split_levels() const {
   return m;
 }
 
-// error_L2 runs in two parts: the interiors of split levels (which only
-// their block step writes, so the part runs beside the rest of the step and
-// the next step's interior waits for nothing else) and every other cell.
+// error_L2 runs in parts: the interiors of split levels (which only their
+// block step writes, so the part runs beside the rest of the step and the
+// next step's interior waits for nothing else), then one part per level (its
+// rim when split, all its cells otherwise), so that each level's next step
+// waits only for the part that reads its own cells.
 std::vector<PlanNode> PlanCompiler::compile_diag(SchedState &s, int n_coarse) const {
   std::vector<Op> ops;
   const bool any_split = split_levels() != 0;
@@ -339,10 +341,10 @@ std::vector<PlanNode> PlanCompiler::compile_diag(SchedState &s, int n_coarse) co
       ops.resize(first);
       for (Op &o : fuse_temporal(step)) ops.push_back(std::move(o));
     }
-    for (int part = any_split ? 0 : 1; part < 2; part++) {
+    for (int part = any_split ? 0 : 1; part <= g.layout.LEVEL; part++) {
       Op o;
       o.kind = Op::L2;
-      o.level = part;  // 0: interiors of split levels, 1: the rest
+      o.level = part;  // 0: interiors of split levels, 1 + l: the rest of level l
       o.line = n;
       o.parity = s.parity;
       ops.push_back(o);
@@ -447,7 +449,8 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
       nd.kind = o.kind == Op::DRAG ? NK_DRAG : NK_L2;
       nd.level = o.line;
       if (o.kind == Op::L2) {
-        nd.region = o.level == 0 ? STB_INTERIOR : STB_RIM;  // the part
+        nd.region = o.level == 0 ? STB_INTERIOR : STB_RIM;
+        nd.part = o.level;
         nd.a0 = int(split_levels());
       }
       for (int a = 0; a < L.number_area; a++)
@@ -820,8 +823,8 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
       const PlanNode &nd = nodes[I.node];
       for (int l = 0; l < L.LEVEL; l++) {
         const bool sp = (nd.a0 >> l) & 1;
-        if (nd.region == STB_INTERIOR && !sp) continue;
-        const uint8_t lo = nd.region == STB_INTERIOR ? 2 : 0, hi = (nd.region == STB_RIM && sp) ? 1 : DMAX;
+        if (nd.part == 0 ? !sp : l != nd.part - 1) continue;
+        const uint8_t lo = nd.part == 0 ? 2 : 0, hi = (nd.part != 0 && sp) ? 1 : DMAX;
         for (int a = L.ASP[l]; a < L.ASP[l + 1]; a++) apply_layer({uint32_t((RK_M << 8) | a), false, lo, hi}, false);
       }
       continue;
@@ -905,19 +908,19 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
       const PlanNode &nd = nodes[I.node];
       for (int l = 0; l < L.LEVEL; l++) {
         const bool sp = (nd.a0 >> l) & 1;
-        if (nd.region == STB_INTERIOR && !sp) continue;
-        const uint8_t lo = nd.region == STB_INTERIOR ? 2 : 0, hi = (nd.region == STB_RIM && sp) ? 1 : DMAX;
+        if (nd.part == 0 ? !sp : l != nd.part - 1) continue;
+        const uint8_t lo = nd.part == 0 ? 2 : 0, hi = (nd.part != 0 && sp) ? 1 : DMAX;
         for (int a = L.ASP[l]; a < L.ASP[l + 1]; a++) {
           A.read_whole(uint32_t((RK_M << 8) | a), lo, hi);
           A.read_whole(uint32_t((RK_UP << 8) | a), lo, hi);
           A.write_whole(uint32_t((RK_UP << 8) | a), false, lo, hi);
         }
       }
-      A.write(key(RK_DIAG, 0, 3 * nd.level + 1 + (nd.region == STB_INTERIOR ? 0 : 1)));
+      A.write(key(RK_DIAG, 0, (1 + L2_NPARTS) * nd.level + 1 + nd.part));
     } else {
       const int a = drag_area, p = I.parity[a] ^ 1;
       A.read_whole(uint32_t(((p ? RK_F1 : RK_F0) << 8) | a));
-      A.write(key(RK_DIAG, 0, 3 * nodes[I.node].level));
+      A.write(key(RK_DIAG, 0, (1 + L2_NPARTS) * nodes[I.node].level));
     }
   }
   for (auto &I : info) {
