@@ -370,8 +370,8 @@ def run_forces(args):
             "cd_last": round(float(cd[-1]), 5), "cl_last": round(float(cl[-1]), 5),
             "max_abs_cl": round(float(np.abs(cl[half:]).max()), 5), "device_s": round(e0.elapsed_time(e1) / 1e3, 2)}
     print(json.dumps(line), flush=True)
-    np.save(os.path.join(REPO, "gpurun_out", f"forces_{args.precision}.npy"), np.stack([cd, cl])) if os.path.isdir(
-        os.path.join(REPO, "gpurun_out")) else None
+    if args.save:
+        np.save(os.path.join(args.save, f"forces_{args.precision}.npy"), np.stack([cd, cl]))
     sim.close()
     return 0
 
@@ -457,6 +457,7 @@ def main():
     ap.add_argument("--eval-per-d", type=float, default=900.0, help="coarse steps per unit D of a warm-start evaluation run")
     ap.add_argument("--warm-precision", default="f16s", choices=["f16s", "f32"], help="solver storage of warm starts")
     ap.add_argument("--epochs", type=int, default=40, help="training epochs of --workload warmstart")
+    ap.add_argument("--save", default=None, metavar="DIR", help="--workload forces: write Cd and Cl per step to DIR")
     ap.add_argument("--bc", default="reference", choices=["reference", "channel"],
                     help="boundaries of --workload timetocd: the reference's, or free-slip top and bottom with a "
                          "half-way bounce-back cylinder")

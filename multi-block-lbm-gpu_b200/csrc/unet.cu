@@ -9,7 +9,7 @@
 // weights; the weight gradient is a GEMM over pixels (M = output channels,
 // N = input channels of one tap, K = pixels) split over pixel chunks with
 // FP32 atomics.  Parameters are FP32 masters updated by Adam; BF16 copies
-// feed the tensor cores.  No reference counterpart (north-star extension).
+// feed the tensor cores.  No reference counterpart.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 

@@ -87,7 +87,9 @@ def header(L, cfg):
 
 
 def race_notes(L, cfg):
-    """Lines where the reference's own launches race."""
+    """Lines where the reference's own launches race: init_Spline3 reads
+    neighbour points other CTAs write when Nc > 256, and init_tri_A's
+    conditional stores collide when Nc - 1 is a multiple of 32."""
     g = mblbm.geo_init(L, cfg)
     notes = []
     for b in range(L.number_line):
