@@ -846,7 +846,7 @@ __device__ __forceinline__ void stb_pair(const StbParams &p, const StbBlk &B, in
 }
 
 template <int P, bool INTERIOR>
-__global__ void __launch_bounds__(256, P == MB_PREC_F64 ? 2 : 4) k_block_step_p(const __grid_constant__ StbParams p) {
+__global__ void __launch_bounds__(256, P == MB_PREC_F64 ? 2 : 5) k_block_step_p(const __grid_constant__ StbParams p) {
   pdl_trigger();
   pdl_wait();
   const int cta = blockIdx.x;
