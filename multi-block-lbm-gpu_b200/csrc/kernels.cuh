@@ -1956,8 +1956,11 @@ struct DragParams {
   double *out;  // Fx, Fy
 };
 
+// one CTA of 256 threads: it finds a free slot among the bulk work's CTAs as
+// soon as one of them retires (a 1024-thread CTA waits for four)
+constexpr int DRAG_THREADS = 256;
 template <int P>
-__global__ void __launch_bounds__(1024) k_drag(const __grid_constant__ DragParams p) {
+__global__ void __launch_bounds__(DRAG_THREADS) k_drag(const __grid_constant__ DragParams p) {
   using S = typename Prec<P>::S;
   const S *F = (const S *)p.F;
   double fx = 0, fy = 0;

@@ -580,7 +580,7 @@ int lower_plan(mb_ctx *c, CompiledPlan &cp) {
       for (int k = 0; k < 9; k++) d.drag.feqc[k] = c->feqc[k];
       d.drag.out = cp.d_diag_res + DIAG_STRIDE * n.level;
       d.func = kfunc<KDrag>(c->prec);
-      d.block = dim3(1024);
+      d.block = dim3(DRAG_THREADS);
       d.grid = dim3(1);
       d.args[0] = &d.drag;
     } else if (n.kind == NK_CCP) {
@@ -1774,7 +1774,7 @@ int launch_drag(mb_ctx *c, double *out, cudaStream_t s) {
   for (int k = 0; k < 9; k++) p.feqc[k] = c->feqc[k];
   p.out = out;
   void *args[] = {&p};
-  MB_CUDA(cudaLaunchKernel(kfunc<KDrag>(c->prec), dim3(1), dim3(1024), args, 0, s));
+  MB_CUDA(cudaLaunchKernel(kfunc<KDrag>(c->prec), dim3(1), dim3(DRAG_THREADS), args, 0, s));
   return MB_OK;
 }
 
