@@ -280,7 +280,14 @@ int mb_set_bulk_occupancy(mb_ctx *ctx, int ctas_per_sm);
  * substep, in place of a launch before that substep's block step; the spline
  * then waits for the fine level's current substep, which on the 3-level
  * cylinder costs more than the launch saves, so it is off by default.
- * Results are identical. */
+ * Bit 2: the same at the spline's own place, on fine levels without
+ * same-level copies: the spline writes the interpolated values into the
+ * buffer the level's next block step reads, and the level's block step in
+ * between leaves those edge cells alone; the spline then runs beside that
+ * block step.  Bit 2 takes the lines it applies to before bit 1.  On the
+ * 3-level cylinder bit 2 measured the same step time as without it (the
+ * spline's longer tail takes what the dropped launch saved), so it is off by
+ * default.  Results are identical. */
 int mb_set_fusion(mb_ctx *ctx, int flags);
 
 /* ---- collision and boundary options ----------------------------------------

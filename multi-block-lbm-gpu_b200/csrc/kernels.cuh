@@ -95,6 +95,7 @@ __device__ __forceinline__ R feq(int k, R rh, R uxx, R uyy) {
 // ----------------------------------------------------------------------------
 constexpr int STB_MAX_BLOCKS = 16;
 constexpr uint8_t FL_CCPULL = 64;  // C_BOUNDARY target of a same-level copy run beside the block step
+constexpr uint8_t FL_TSKIP = 128;  // fine edge cell a spline writes for the next substep (StbParams::tskip)
 
 struct StbBlk {
   const void *Fin;
@@ -159,6 +160,8 @@ struct StbParams {
   double feqc[9];    // feq(rho0, U0): block-edge FLUID cells and stale f of edge solids
   double rho0, u0x, u0y;
   StbOptions opt;
+  int tskip;         // leave cells flagged FL_TSKIP alone: a spline writes their next values
+  int pad_t;
   StbBlk b[STB_MAX_BLOCKS];
 };
 
@@ -371,6 +374,7 @@ __device__ __forceinline__ void stb_finish(const StbParams &p, const StbBlk &B, 
   // C_BOUNDARY and row padding: untouched by the step, carried to the new
   // buffer; a same-level copy target (FL_CCPULL) is k_cc_pull's
   if (p.ccpull && (fl & FL_CCPULL)) return;
+  if (p.tskip && (fl & FL_TSKIP)) return;
   const S *Fin = (const S *)B.Fin;
 #pragma unroll
   for (int k = 0; k < 9; k++) st_ef<EF>(Fout + k * plane + c, ld_ef<EF>(Fin + k * plane + c));

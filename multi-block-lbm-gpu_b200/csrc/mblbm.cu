@@ -140,6 +140,8 @@ struct mb_ctx {
   std::vector<CcEntry *> d_cclist;  // per level: the copies of fusable levels (k_cc_pull)
   int fuse_cc = 1;
   int fuse_tmp = 0;  // splines do the next temporal interpolation of their line (mb_set_fusion bit 1)
+  int fuse_early = 0;  // ... in place, beside the fine level's substep (mb_set_fusion bit 2)
+  unsigned early_levels = 0;  // levels whose temporal edge cells carry CF_TSKIP
   // scheduler
   SchedState state;
   bool inited = false;
@@ -549,6 +551,7 @@ int lower_plan(mb_ctx *c, CompiledPlan &cp) {
     if (n.kind == NK_STB) {
       const bool quads = stb_uses_quads(c, n.level, n.region);
       d.stb = make_stb(c, n.a0, n.a1, n.parity, n.macro_all, 1, n.region, quads, n.ccpull);
+      d.stb.tskip = n.tskip;
       // bulk: interiors of split levels, and whole levels streamed with
       // evict-first hints when bulk_levels is set
       d.background = (n.region == STB_INTERIOR) || (c->bulk_levels && n.region == STB_ALL && d.stb.evict_first);
@@ -973,8 +976,9 @@ int program_status(mb_ctx *c) {
 CompiledPlan *get_plan(mb_ctx *c, int n, bool final_macros, int *err, bool batch = false) {
   // batches and the persistent executor run the plain node kinds only
   const bool fuse = c->fuse_cc && !options_on(c) && !batch && c->use_graph != 3;
+  const bool early = c->fuse_early && !options_on(c) && !batch && c->use_graph != 3;
   std::string key = c->state.key() + "/" + std::to_string(n) + (final_macros ? "F" : "P") + (fuse ? "c" : "") +
-                    (c->fuse_tmp ? "t" : "");
+                    (c->fuse_tmp ? "t" : "") + (early ? "e" : "");
   auto it = c->plans.find(key);
   if (it != c->plans.end()) return it->second.get();
   auto cp = std::make_unique<CompiledPlan>();
@@ -983,6 +987,7 @@ CompiledPlan *get_plan(mb_ctx *c, int n, bool final_macros, int *err, bool batch
   pc.split_mask = c->split_mask;
   if (fuse) pc.cc = &c->cc;
   pc.fuse_tmp = c->fuse_tmp != 0;
+  if (early) pc.early_levels = c->early_levels;
   SchedState s = c->state;
   cp->nodes = pc.compile(s, n, final_macros);
   cp->end = s;
@@ -998,7 +1003,9 @@ CompiledPlan *get_plan(mb_ctx *c, int n, bool final_macros, int *err, bool batch
 // beside the rest of the plan where their reads and writes allow.
 CompiledPlan *get_diag_plan(mb_ctx *c, int n, int *err) {
   const bool fuse = c->fuse_cc && !options_on(c);
-  const std::string key = c->state.key() + "/" + std::to_string(n) + "D" + (fuse ? "c" : "") + (c->fuse_tmp ? "t" : "");
+  const bool early = c->fuse_early && !options_on(c) && c->use_graph != 3;
+  const std::string key =
+      c->state.key() + "/" + std::to_string(n) + "D" + (fuse ? "c" : "") + (c->fuse_tmp ? "t" : "") + (early ? "e" : "");
   auto it = c->plans.find(key);
   if (it != c->plans.end()) return it->second.get();
   auto cp = std::make_unique<CompiledPlan>();
@@ -1008,6 +1015,7 @@ CompiledPlan *get_diag_plan(mb_ctx *c, int n, int *err) {
   pc.drag_area = c->drag_area;
   if (fuse) pc.cc = &c->cc;
   pc.fuse_tmp = c->fuse_tmp != 0;
+  if (early) pc.early_levels = c->early_levels;
   SchedState s = c->state;
   cp->nodes = pc.compile_diag(s, n);
   cp->end = s;
@@ -1156,6 +1164,30 @@ extern "C" int mb_create(const mb_geometry *geo, int precision, mb_ctx **out) {
     slot_pts += l.Nf;
   }
   c->n_slot_points = slot_pts;
+
+  // fine levels without same-level copies, whose splines can do the next
+  // temporal interpolation in place: CF_TSKIP on the edge cells it writes
+  for (int l = 1; l < L.LEVEL; l++) {
+    if (L.LCCP[l] != L.LCCP[l + 1] || L.LTCFFCP[l] == L.LTCFFCP[l + 1]) continue;
+    bool ok = true;
+    for (int b = L.LTCFFCP[l]; b < L.LTCFFCP[l + 1] && ok; b++) {
+      const int a = geo->Line_Inf_C[b].areaf_n;
+      ok = a >= L.ASP[l] && a < L.ASP[l + 1];
+      const SplLine &sl = c->spl_lines[b];
+      for (int ip = 0; ok && ip < sl.Nf; ip++) {
+        const int i = sl.fi0 + ip * sl.fdi, j = sl.fj0 + ip * sl.fdj;
+        ok = (c->hflags[a][(size_t)j * c->bl[a].pitch + i] & 3) == CT_COPY;
+      }
+    }
+    if (!ok) continue;
+    c->early_levels |= 1u << l;
+    for (int b = L.LTCFFCP[l]; b < L.LTCFFCP[l + 1]; b++) {
+      const int a = geo->Line_Inf_C[b].areaf_n;
+      const SplLine &sl = c->spl_lines[b];
+      for (int ip = 0; ip < sl.Nf; ip++)
+        c->hflags[a][(size_t)(sl.fj0 + ip * sl.fdj) * c->bl[a].pitch + (sl.fi0 + ip * sl.fdi)] |= CF_TSKIP;
+    }
+  }
 
   // device allocations (Multi-block-LBM.cu:26-113, without x/y/force/f arrays)
   int e;
@@ -1434,10 +1466,11 @@ extern "C" int mb_set_cell_types(mb_ctx *c, int a, const int *types) {
 }
 
 extern "C" int mb_set_fusion(mb_ctx *c, int flags) {
-  if (!c || flags < 0 || flags > 3) return MB_ERR_INVALID;
+  if (!c || flags < 0 || flags > 7) return MB_ERR_INVALID;
   cudaDeviceSynchronize();
   c->fuse_cc = flags & 1;
   c->fuse_tmp = (flags >> 1) & 1;
+  c->fuse_early = (flags >> 2) & 1;
   c->plans.clear();
   return MB_OK;
 }

@@ -21,6 +21,8 @@ enum : uint8_t {
   CF_HBB = 16,  // CT_SOLID cell that is a half-way bounce-back wall (MB_SOLID_HBB)
   CF_SLIP = 32, // CT_SOLID cell that is an on-node free-slip wall (MB_SOLID_SLIP)
   CF_CCPULL = 64, // C_BOUNDARY target of a same-level copy run beside its level's block step (NK_CCP)
+  CF_TSKIP = 128, // fine edge cell of a temporal interpolation that a spline may do early: a block step
+                  // flagged tskip leaves it alone (the spline writes its next value there)
 };
 
 bool obstacle_contains(const mb_config &c, double x, double y);
@@ -101,6 +103,7 @@ struct PlanNode {
   int macro_all = 0;          // STB: write rho/u of every FLUID cell
   int ccpull = 0;             // STB: skips CF_CCPULL cells (an NK_CCP node of the same level writes them)
   int part = 0;               // L2: the error_L2 part (L2_NPARTS)
+  int tskip = 0;              // STB: leaves CF_TSKIP cells alone (a spline writes them)
   std::vector<Rec> recs;      // REC
   std::vector<std::pair<int, int>> ops;  // REC: (first record, count) of each reference line op
   double tw[4][3] = {};       // REC: temporal weight triples (a, b, c)
@@ -140,6 +143,7 @@ struct Op {
   double txm = 0;
   std::array<int, 3> tmk{};
   std::vector<int> tparity;
+  int tskip = 0;  // STB: leaves CF_TSKIP cells alone (fuse_early)
 };
 
 // Same-level copies (c_c_boundary_transfer) of one level with chains
@@ -176,6 +180,10 @@ struct PlanCompiler {
   // a spline of a coarse-fine line also does the line's temporal
   // interpolation of the fine level's next substep (fuse_temporal)
   bool fuse_tmp = false;
+  // levels (bit per level) whose splines do that interpolation in place, the
+  // level's substep between them leaving the edge cells alone (fuse_early);
+  // their edge cells carry CF_TSKIP
+  unsigned early_levels = 0;
   PlanCompiler(const mb_geometry &g_, const std::vector<BlockLayout> &bl_,
                const std::vector<std::vector<uint8_t>> &fl, const std::vector<SplLine> &sl)
       : g(g_), bl(bl_), flags(fl), spl_lines(sl) {}
@@ -190,6 +198,8 @@ struct PlanCompiler {
   std::vector<PlanNode> compile_single(int kind, int index, double xm, const SchedState &s) const;
   // line ops expanded into launches (REC / SPL batches, STB nodes) with DAG edges
   std::vector<PlanNode> build(const std::vector<Op> &ops) const;
+  // ops with the fusions switched on (fuse_early, fuse_tmp) applied
+  std::vector<Op> fused(const std::vector<Op> &ops) const;
 };
 
 // Cells whose rho/ux/uy an interface op reads (the CF_MACRO attribute).

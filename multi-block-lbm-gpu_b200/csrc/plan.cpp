@@ -55,6 +55,7 @@ struct Whole {
   bool fluid_only;
   uint8_t dlo, dhi;
   bool skip_cc = false;  // CF_CCPULL cells excluded (written by an NK_CCP node instead)
+  bool skip_t = false;   // CF_TSKIP cells excluded (written by a spline instead)
 };
 constexpr uint8_t DMAX = 255;
 
@@ -65,8 +66,9 @@ struct Access {
   void read(uint64_t k) { r.insert(k); rs.insert(summ(k)); }
   void write(uint64_t k) { w.insert(k); ws.insert(summ(k)); }
   void read_whole(uint32_t s, uint8_t dlo = 0, uint8_t dhi = DMAX) { wr.push_back({s, false, dlo, dhi}); rs.insert(s); }
-  void write_whole(uint32_t s, bool fo, uint8_t dlo = 0, uint8_t dhi = DMAX, bool skip_cc = false) {
-    ww.push_back({s, fo, dlo, dhi, skip_cc});
+  void write_whole(uint32_t s, bool fo, uint8_t dlo = 0, uint8_t dhi = DMAX, bool skip_cc = false,
+                   bool skip_t = false) {
+    ww.push_back({s, fo, dlo, dhi, skip_cc, skip_t});
     ws.insert(s);
   }
   void merge(const Access &o) {
@@ -308,10 +310,87 @@ static std::vector<Op> fuse_temporal(const std::vector<Op> &ops) {
   return out;
 }
 
+// The same fusion without moving the spline, for levels in early_levels
+// (no same-level copies): the spline writes the interpolated values at its
+// own place into the buffer the level's next block step will read, and the
+// one block step of the level between them (the substep without an
+// interpolation) leaves those edge cells alone (tskip) instead of copying
+// its input there.  The spline then runs beside that block step.
+static std::vector<Op> fuse_early(const std::vector<Op> &ops, unsigned levels) {
+  const int n = int(ops.size());
+  std::vector<int> with(n, -1), stb_of(n, -1);
+  std::vector<char> used(n, 0);
+  for (int ti = 0; ti < n; ti++) {
+    const Op &t = ops[ti];
+    if (t.kind != Op::TEMPORAL || !((levels >> t.level) & 1u)) continue;
+    int si = ti - 1, stb = -1, nstb = 0;
+    for (; si >= 0; si--) {
+      const Op &q = ops[si];
+      if (q.kind == Op::SPL && q.line == t.line) break;
+      if (q.kind == Op::STB && q.level == t.level) { stb = si; nstb++; continue; }
+      const bool ok = q.kind == Op::SPL || (q.kind == Op::TEMPORAL && q.level == t.level && q.line != t.line);
+      if (!ok) { si = -1; break; }
+    }
+    if (si < 0 || used[si] || nstb != 1) continue;
+    with[si] = ti;
+    used[si] = 1;
+    stb_of[ti] = stb;
+  }
+  // all or none of a run of interpolations (lines may share corner cells,
+  // whose last writer must stay the last line of the run), with the splines
+  // in the order of the interpolations
+  std::vector<int> from(n, -1);
+  for (int i = 0; i < n; i++)
+    if (with[i] >= 0) from[with[i]] = i;
+  for (int t0 = 0; t0 < n;) {
+    if (ops[t0].kind != Op::TEMPORAL) { t0++; continue; }
+    int t1 = t0;
+    while (t1 < n && ops[t1].kind == Op::TEMPORAL && ops[t1].level == ops[t0].level) t1++;
+    bool all = true;
+    for (int t = t0; t < t1; t++) all = all && from[t] >= 0 && (t == t0 || from[t] > from[t - 1]);
+    if (!all)
+      for (int t = t0; t < t1; t++)
+        if (from[t] >= 0) {
+          with[from[t]] = -1;
+          used[from[t]] = 0;
+          stb_of[t] = -1;
+          from[t] = -1;
+        }
+    t0 = t1;
+  }
+  std::vector<char> drop(n, 0), skip(n, 0);
+  for (int i = 0; i < n; i++)
+    if (with[i] >= 0) {
+      drop[with[i]] = 1;
+      skip[stb_of[with[i]]] = 1;
+    }
+  std::vector<Op> out;
+  out.reserve(n);
+  for (int i = 0; i < n; i++) {
+    if (drop[i]) continue;
+    Op o = ops[i];
+    if (with[i] >= 0) {
+      const Op &t = ops[with[i]];
+      o.tmp = 1;
+      o.txm = t.xm;
+      o.tmk = t.mk;
+      o.tparity = t.parity;
+    }
+    if (skip[i]) o.tskip = 1;
+    out.push_back(std::move(o));
+  }
+  return out;
+}
+
+std::vector<Op> PlanCompiler::fused(const std::vector<Op> &ops) const {
+  std::vector<Op> o = early_levels ? fuse_early(ops, early_levels) : ops;
+  return fuse_tmp ? fuse_temporal(o) : o;
+}
+
 std::vector<PlanNode> PlanCompiler::compile(SchedState &s, int n_coarse, bool final_macros) const {
   std::vector<Op> ops;
   for (int n = 0; n < n_coarse; n++) emit(g, 0, s, ops, final_macros && n == n_coarse - 1);
-  return build(fuse_tmp ? fuse_temporal(ops) : ops);
+  return build(fused(ops));
 }
 
 unsigned PlanCompiler::split_levels() const {
@@ -336,10 +415,10 @@ std::vector<PlanNode> PlanCompiler::compile_diag(SchedState &s, int n_coarse) co
   for (int n = 0; n < n_coarse; n++) {
     const size_t first = ops.size();
     emit(g, 0, s, ops, true);
-    if (fuse_tmp) {
+    if (fuse_tmp || early_levels) {
       std::vector<Op> step(ops.begin() + first, ops.end());
       ops.resize(first);
-      for (Op &o : fuse_temporal(step)) ops.push_back(std::move(o));
+      for (Op &o : fused(step)) ops.push_back(std::move(o));
     }
     for (int part = any_split ? 0 : 1; part <= g.layout.LEVEL; part++) {
       Op o;
@@ -389,6 +468,7 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
     const int d = edge_dist(blk, cell);
     if (d < wh.dlo || d > wh.dhi) return false;
     if (wh.skip_cc && (flags[blk][cell] & CF_CCPULL)) return false;
+    if (wh.skip_t && (flags[blk][cell] & CF_TSKIP)) return false;
     return !wh.fluid_only || is_fluid(blk, cell);
   };
 
@@ -404,6 +484,7 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
   struct OpInfo {
     bool stb = false;
     bool cc_fused = false;      // STB: its level's same-level copies run beside it (cc_nodes)
+    bool tskip = false;         // STB: leaves CF_TSKIP cells alone
     std::vector<int> stb_nodes; // STB: its nodes
     std::vector<int> cc_nodes;  // STB: NK_CCP nodes, one per launch chunk with copies
     int diag = -1;              // SNAP / DRAG / L2 op: its Op::Kind
@@ -465,6 +546,15 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
       open = -1;
       last_stb = int(oi);
       for (int a = L.ASP[o.level]; a < L.ASP[o.level + 1]; a++) stb_op[a] = int(oi);
+      if (o.tskip) {  // cells it leaves alone: no read may take them from its input buffer
+        I.tskip = true;
+        for (int a = L.ASP[o.level]; a < L.ASP[o.level + 1]; a++)
+          for (int j = 0; j < bl[a].ny; j++)
+            for (int i = 0; i < bl[a].nx; i++) {
+              const long long cell = pitch_cell(a, i, j);
+              if (flags[a][(size_t)cell] & CF_TSKIP) lastw[fkey(o.parity[a] ^ 1, a, cell)] = LastWrite{int(oi)};
+            }
+      }
       I.stb = true;
       I.level = o.level;
       I.parity = o.parity;
@@ -485,6 +575,7 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
           nd.label = lab;
           nd.a0 = a0;
           nd.a1 = a1;
+          nd.tskip = o.tskip;
           I.stb_nodes.push_back(int(nodes.size()));
           nodes.push_back(nd);
           acc.push_back(Access());
@@ -839,7 +930,7 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
       // cells and read F of buffer p, over the whole block
       for (int a = L.ASP[I.level]; a < L.ASP[I.level + 1]; a++) {
         const int p = I.parity[a];
-        apply_layer({uint32_t(((p ? RK_F0 : RK_F1) << 8) | a), false, 0, DMAX, I.cc_fused}, true);
+        apply_layer({uint32_t(((p ? RK_F0 : RK_F1) << 8) | a), false, 0, DMAX, I.cc_fused, I.tskip}, true);
         apply_layer({uint32_t((RK_M << 8) | a), true, 0, DMAX, I.cc_fused}, true);
         apply_layer({uint32_t(((p ? RK_F1 : RK_F0) << 8) | a), false, 0, DMAX}, false);
       }
@@ -875,7 +966,8 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
     for (int a = nodes[q].a0; a < nodes[q].a1; a++) {
       const int p = int((nodes[q].parity >> a) & 1);
       fin[q].read_whole(uint32_t(((p ? RK_F1 : RK_F0) << 8) | a), rlo, rhi);
-      fin[q].write_whole(uint32_t(((p ? RK_F0 : RK_F1) << 8) | a), false, wlo, whi, nodes[q].ccpull != 0);
+      fin[q].write_whole(uint32_t(((p ? RK_F0 : RK_F1) << 8) | a), false, wlo, whi, nodes[q].ccpull != 0,
+                         nodes[q].tskip != 0);
       fin[q].write_whole(uint32_t((RK_M << 8) | a), true, wlo, whi, nodes[q].ccpull != 0);
     }
   }

@@ -384,11 +384,11 @@ def test_step_diag_equals_step_by_step(mb, cuda_device, prec, split, graph):
 @pytest.mark.parametrize("name,prec", [("n3", "f32"), ("g49", "f64"), ("g25", "f16s")])
 def test_fused_copies_bitwise(mb, cuda_device, name, prec, split, variant, graph):
     """Same-level copies done inside the block step (mb_set_fusion bit 0) and
-    temporal interpolations done by the splines (bit 1), alone and together
-    (the default), give bitwise the state of separate launches."""
+    temporal interpolations done by the splines (bits 1 and 2), alone and
+    together, give bitwise the state of separate launches."""
     g = mb.geo_init(*make_ref.case(name)[:2])
     sims = []
-    for fuse in (0, 1, 2, 3):
+    for fuse in (0, 1, 2, 3, 4, 5, 7):
         s = mb.MultiBlockLBM(g, prec, graph=graph)
         s.set_fusion(fuse)
         s.set_split_cells(split)
