@@ -71,20 +71,22 @@ def test_f64_periodic_kernel_variants(mb, orc, cuda_device, split, variant):
 
 
 def test_fused_ghost_copies_bitwise(mb, cuda_device):
-    """Ghost copies done beside the block step (the default) equal separate
-    copy launches bitwise."""
+    """Ghost copies done beside the block step (the default), and temporal
+    interpolations done by the splines (fusion bits 1 and 2), equal separate
+    launches bitwise."""
     g = CASES["tgv2"](mb)
     out = []
-    for fuse in (0, 1):
+    for fuse in (0, 1, 2, 4, 5):
         s = mb.MultiBlockLBM(g, "f32")
         s.set_fusion(fuse)
         s.init()
         mb.tgv_init(s, g)
         s.evolution(13)
         out.append([s.fields(a) for a in range(g.layout.number_area)])
-    for fa, fb in zip(*out):
-        for key in ("F", "rho", "ux", "uy"):
-            assert np.array_equal(fa[key], fb[key])
+    for other in out[1:]:
+        for fa, fb in zip(out[0], other):
+            for key in ("F", "rho", "ux", "uy"):
+                assert np.array_equal(fa[key], fb[key])
 
 
 @pytest.mark.parametrize("prec,tol", [("f32", 1e-5), ("f32u", 5e-5), ("f16s", 5e-3)])
