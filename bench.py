@@ -28,7 +28,7 @@ sys.path.insert(0, os.path.join(REPO, "multi-block-lbm-gpu_b200"))
 
 METRIC = "multi-block D2Q9 MLUPS & % HBM roofline; time-to-Cd (±0.5%) vs plain FP32"
 WORKLOAD = "3-level cylinder Re=100, 4096x1024 coarse, L1 box 512x256, L2 box 256x128 coarse, D=32"
-BYTES_PER_UPDATE = {"f32": 72, "f32u": 72, "f16s": 36, "f64": 144}
+BYTES_PER_UPDATE = {"f32": 72, "f32u": 72, "f16s": 36, "f16c": 36, "f64": 144}
 
 
 def peaks():
@@ -128,19 +128,37 @@ def cpu_baseline(budget_s=12.0):
             "sample": f"{n} coarse steps of the same workload after 1 warm-up step ({dt:.1f} s), FP64 C oracle, OpenMP"}
 
 
-def run_reference(args):
-    exe = os.path.join(REPO, "oracle", "_ref", "ref_c2")
-    import mblbm
+# Cell updates of one coarse step of WORKLOAD: level 0 has 4,079,875 cells in
+# 4 blocks (1 sub-step), level 1 401,676 cells in 4 blocks (2 sub-steps),
+# level 2 525,825 cells in 1 block (4 sub-steps).  The product arm counts it
+# from its geometry (mblbm.updates_per_coarse_step); the reference binary
+# prints it from its own AREA table (sum over blocks of nx*ny*m).
+UPDATES_PER_STEP = 6986527
+L2_NOTE = "working set larger than L2 (5.1M cells: 370 MB of FP32 state buffers, 740 MB in FP64); no flush"
 
-    upd = mblbm.updates_per_coarse_step(mblbm.config2_geometry())
+
+def bench_config(world):
+    """The `config` object of both arms (the compute precision is `dtype`)."""
+    return {"workload": WORKLOAD, "cell_updates_per_step": UPDATES_PER_STEP, "l2": L2_NOTE,
+            "parallelism": f"{world} independent cases, one per GPU"}
+
+
+def run_reference(args):
+    """The reference's own CUDA build (oracle/_ref/ref_c2) on WORKLOAD.  Loads
+    nothing of this repository's library: the update count comes from the
+    reference binary itself."""
+    exe = os.path.join(REPO, "oracle", "_ref", "ref_c2")
     base = {"metric": METRIC, "unit": "MLUPS", "impl": "reference", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "data": "synthetic",
-            "config": {"workload": WORKLOAD, "l2": "working set larger than L2"}}
+            "config": bench_config(1)}
     if os.path.exists(exe):
         wd = tempfile.mkdtemp()
         r = subprocess.run([exe, "bench", str(args.steps), str(args.warmup)], cwd=wd, capture_output=True, text=True,
                            timeout=1800)
         js = json.loads(r.stdout.strip().splitlines()[-1])
+        upd = int(js["cell_updates_per_step"])
+        if upd != UPDATES_PER_STEP:
+            raise RuntimeError(f"reference build counts {upd} cell updates per step, expected {UPDATES_PER_STEP}")
         v = upd / js["ms_per_step"] / 1e3
         ve = upd / js["ms_per_step_diag"] / 1e3
         base.update(value=round(v, 2), ms_per_step=js["ms_per_step"], dtype="f64",
@@ -151,7 +169,8 @@ def run_reference(args):
                                             f"on cuda:0, {args.steps} timed coarse steps after {args.warmup}"})
     else:
         cb = cpu_baseline()
-        base.update(value=cb["value"], ms_per_step=round(upd / cb["value"] / 1e3, 4), dtype="f64", cpu_baseline=cb,
+        base.update(value=cb["value"], ms_per_step=round(UPDATES_PER_STEP / cb["value"] / 1e3, 4), dtype="f64",
+                    cpu_baseline=cb,
                     e2e={"value": cb["value"], "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
     print(json.dumps(base), flush=True)
 
@@ -159,18 +178,25 @@ def run_reference(args):
 def run_batch(args):
     """The batched workload: 256 independent cases drawn by mblbm.batch_case
     (seeded per case), grouped by level count into two batches, each
-    autotuned, then K coarse steps of both timed together with CUDA events."""
+    autotuned, then K coarse steps of both timed together with CUDA events.
+    Under torchrun the cases are sharded over the ranks by cost (cell updates
+    per coarse step, mblbm.ranks.balance); ranks exchange nothing while they
+    step, only the slowest rank's time and the total updates."""
     import torch
     import mblbm
+    from mblbm import ranks
 
-    torch.cuda.set_device(0)
+    rank, world, local = ranks.env()
+    torch.cuda.set_device(local)
+    dist = ranks.init("nccl") if world > 1 else None
     stream = torch.cuda.Stream()
     t_setup = time.perf_counter()
+    drawn = [mblbm.batch_case(i) for i in range(args.cases)]
+    costs = [mblbm.updates_per_coarse_step(g) for g, _ in drawn]
+    mine = ranks.balance(costs, rank, world)
     groups = {2: [], 3: []}
-    params = []
-    for i in range(args.cases):
-        g, prm = mblbm.batch_case(i)
-        params.append(prm)
+    for i in mine:
+        g, prm = drawn[i]
         sim = mblbm.MultiBlockLBM(g, args.precision)
         sim.init(stream)
         groups[prm["levels"]].append(sim)
@@ -182,37 +208,52 @@ def run_batch(args):
         b.prepare(args.steps)  # plans and graphs of the timed call, compiled outside the timed region
     torch.cuda.synchronize()
     t_setup = time.perf_counter() - t_setup
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with Clocks(0) as clk:
+
+    def barrier():
+        if dist:
+            dist.barrier()
         torch.cuda.synchronize()
+
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        barrier()
         e0.record(stream)
         for b in batches:
             b.evolution(args.steps, stream)
         e1.record(stream)
-        torch.cuda.synchronize()
+        barrier()
     ms = e0.elapsed_time(e1)
     kernels = sum(b.stats()["kernels_last_call"] for b in batches)
     cds = [b.drag(stream)[0] for b in batches]
-    peak, src = peaks()
-    bpu = BYTES_PER_UPDATE[args.precision]
-    achieved = upd * args.steps * bpu / (ms * 1e-3) / 1e9
-    line = {"metric": METRIC, "value": round(upd * args.steps / (ms * 1e-3) / 1e6, 1), "unit": "MLUPS", "n_gpus": 1,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 5),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": args.precision,
-            "data": "synthetic",
-            "config": {"workload": f"batched: {args.cases} cases, D~U[10,40], aspect~U[1,3], angle~U[0,pi), "
-                                   "Re~U[20,200], domain 20Dx8D, U0=0.04, 2 or 3 levels, splitmix64 seed 20250+case",
-                       "batches": {f"{len(v)} cases of {lv} levels": t for (lv, v), t in
-                                   zip([(lv, v) for lv, v in groups.items() if v], tune)},
-                       "cell_updates_per_step": upd, "setup_s": round(t_setup, 1)},
-            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                         "frac": round(achieved / peak, 4), "traffic": None, "peak_source": src,
-                         "kernel": "whole batched step (all launches)", "bytes_per_update": bpu},
-            "gpu_launches": kernels, "clocks": clk.summary(),
-            "cd_range": [round(float(min(c.min() for c in cds)), 4), round(float(max(c.max() for c in cds)), 4)]}
-    print(json.dumps(line), flush=True)
+    cd_lo = min(float(c.min()) for c in cds) if cds else float("inf")
+    cd_hi = max(float(c.max()) for c in cds) if cds else float("-inf")
+    ms, = ranks.reduce([ms], "max", dist, device="cuda")
+    tot_upd, tot_kernels = ranks.reduce([upd, kernels], "sum", dist, device="cuda")
+    if rank == 0:
+        peak, src = peaks()
+        bpu = BYTES_PER_UPDATE[args.precision]
+        achieved = tot_upd * args.steps * bpu / (ms * 1e-3) / 1e9
+        line = {"metric": METRIC, "value": round(tot_upd * args.steps / (ms * 1e-3) / 1e6, 1), "unit": "MLUPS",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 5),
+                "higher_is_better": True, "scaling": "strong" if world > 1 else "weak", "vs_baseline": None,
+                "dtype": args.precision, "data": "synthetic",
+                "config": {"workload": f"batched: {args.cases} cases, D~U[10,40], aspect~U[1,3], angle~U[0,pi), "
+                                       "Re~U[20,200], domain 20Dx8D, U0=0.04, 2 or 3 levels, splitmix64 seed 20250+case",
+                           "batches_rank0": {f"{len(v)} cases of {lv} levels": t for (lv, v), t in
+                                             zip([(lv, v) for lv, v in groups.items() if v], tune)},
+                           "cell_updates_per_step": int(tot_upd), "setup_s": round(t_setup, 1),
+                           "parallelism": f"{args.cases} cases sharded by cost over {world} GPU(s)"},
+                "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                             "frac": round(achieved / peak, 4), "traffic": None, "peak_source": src,
+                             "kernel": "whole batched step (all launches)", "bytes_per_update": bpu},
+                "gpu_launches": int(tot_kernels), "clocks": clk.summary(),
+                "cd_range_rank0": [round(cd_lo, 4), round(cd_hi, 4)]}
+        print(json.dumps(line), flush=True)
     for b in batches:
         b.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
     return 0
 
 
@@ -230,13 +271,13 @@ def run_timetocd(args):
     upd = mblbm.updates_per_coarse_step(geo)
     out = {}
     series = {}
-    for prec in ("f64", "f32", "f16s"):
+    for prec in ("f64", "f32", "f16s", "f16c"):
         sim = mblbm.MultiBlockLBM(geo, prec)
         sim.init(stream)
         if args.bc == "channel":  # free-slip top and bottom, half-way bounce-back on the cylinder
             mblbm.channel_walls(sim, geo)
-        sim.evolution_diag(12, stream)  # single-step plans of every scheduler phase
         sim.init(stream)
+        sim.prepare_diag(args.steps)  # plans, graphs and result buffers of the timed call
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         cd, cl, l2 = sim.evolution_diag(args.steps, stream)
@@ -393,7 +434,7 @@ def run_tgv(args):
     nu = (geo.Areas[0].tau - 0.5) / 3.0
     k = 2.0 * np.pi / (geo.config.LX - 2)
     out = {}
-    for prec in ("f64", "f32", "f16s"):
+    for prec in ("f64", "f32", "f16s", "f16c"):
         sim = mblbm.MultiBlockLBM(geo, prec)
         sim.init(stream)
         sim.evolution(args.warmup, stream)  # plans and graphs built before the timed run
@@ -412,7 +453,7 @@ def run_tgv(args):
         out[prec] = {"amplitude": amp, "rel_to_exact": amp / exact - 1.0, "ms": round(ms, 2),
                      "mlups": round(upd * args.steps / ms / 1e3, 1)}
         sim.close()
-    for prec in ("f32", "f16s"):
+    for prec in ("f32", "f16s", "f16c"):
         out[prec]["rel_to_f64"] = out[prec]["amplitude"] / out["f64"]["amplitude"] - 1.0
     line = {"metric": "periodic Taylor-Green vortex: MLUPS and amplitude error after the run", "unit": "MLUPS",
             "value": out["f16s"]["mlups"], "higher_is_better": True, "n_gpus": 1, "steps": args.steps,
@@ -438,7 +479,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5000)
     ap.add_argument("--warmup", type=int, default=12)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="f32", choices=["f32", "f32u", "f16s", "f64"])
+    ap.add_argument("--precision", default="f32", choices=["f32", "f32u", "f16s", "f16c", "f64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--roofline-only", type=int, default=0, metavar="N",
                     help="init, then N launches of one level's block step alone, replayed twice as one CUDA "
@@ -455,7 +496,7 @@ def main():
     ap.add_argument("--eval", type=int, default=64, help="held-out cases of --workload warmstart")
     ap.add_argument("--snap-per-d", type=float, default=300.0, help="coarse steps per unit D before a training snapshot")
     ap.add_argument("--eval-per-d", type=float, default=900.0, help="coarse steps per unit D of a warm-start evaluation run")
-    ap.add_argument("--warm-precision", default="f16s", choices=["f16s", "f32"], help="solver storage of warm starts")
+    ap.add_argument("--warm-precision", default="f16s", choices=["f16s", "f16c", "f32"], help="solver storage of warm starts")
     ap.add_argument("--epochs", type=int, default=40, help="training epochs of --workload warmstart")
     ap.add_argument("--save", default=None, metavar="DIR", help="--workload forces: write Cd and Cl per step to DIR")
     ap.add_argument("--bc", default="reference", choices=["reference", "channel"],
@@ -492,6 +533,7 @@ def main():
 
     geo = mblbm.config2_geometry()
     upd = mblbm.updates_per_coarse_step(geo)
+    assert upd == UPDATES_PER_STEP, upd
     stream = torch.cuda.Stream()
     sim = mblbm.MultiBlockLBM(geo, args.precision)
     if args.variant is not None:
@@ -544,19 +586,19 @@ def main():
         for k in h:
             h[k][:] = f[k].ravel()
     ref.close()
-    # the final state comes back into pinned host buffers as well
+    # the result fields (rho, ux, uy and the cell types: what the reference's
+    # output() writes) come back into pinned host buffers
     host_out = []
     for a in A:
         pin = lambda shp, dt: torch.empty(shp, dtype=dt).pin_memory().numpy()
         host_out.append({"rho": pin((a.ny, a.nx), torch.float64), "ux": pin((a.ny, a.nx), torch.float64),
-                         "uy": pin((a.ny, a.nx), torch.float64), "F": pin((9, a.ny, a.nx), torch.float64),
-                         "solid": pin((a.ny, a.nx), torch.int32)})
+                         "uy": pin((a.ny, a.nx), torch.float64), "solid": pin((a.ny, a.nx), torch.int32)})
     sim2 = mblbm.MultiBlockLBM(geo, args.precision)
     sim2.init(stream)
     for i, h in enumerate(host):  # sizes the library's staging buffer outside the timed region
         sim2.set_fields(i, h["rho"], h["ux"], h["uy"], h["F"], stream)
-    sim2.evolution_diag(12, stream)  # compiles the single-step plans of every scheduler phase
     sim2.init(stream)
+    sim2.prepare_diag(args.steps)  # plans, graphs and result buffers of the timed call
     torch.cuda.synchronize()
     h2d = sum(h[k].nbytes for h in host for k in h)
     d2h = 0
@@ -598,9 +640,7 @@ def main():
             "vs_baseline": None,
             "dtype": args.precision,
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "precision": args.precision, "cell_updates_per_step": upd,
-                       "l2": "working set larger than L2 (two FP32 state buffers of 5.1M cells = 370 MB); no flush",
-                       "parallelism": f"{world} independent cases, one per GPU"},
+            "config": bench_config(world),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": src,
                          "kernel": "k_block_step level 0", "alg_bytes_per_launch": kbytes, "cells_per_launch": kcells,
@@ -608,9 +648,9 @@ def main():
             "e2e": {"value": round(world * upd * args.steps / (ms_e2e * 1e-3) / 1e6, 1), "unit": "MLUPS",
                     "h2d_bytes_per_step": round(h2d / args.steps), "d2h_bytes_per_step": round(d2h / args.steps),
                     "wall_s": round(wall_e2e, 3),
-                    "what": "C ABI with host buffers: state upload from pinned memory, mb_step_diag (per step: "
-                            "coarse step, drag and L2 change as the reference loop, 32 B of results copied to the "
-                            "host), final field download"},
+                    "what": "C ABI with host buffers: upload of the FP64 D2Q9 state (rho, ux, uy, F) from pinned "
+                            "memory, mb_step_diag (per step: coarse step, drag and L2 change as the reference loop, "
+                            "32 B of results copied to the host), download of the final rho, ux, uy (FP64)"},
             "gpu_launches": kernels,
             "clocks": clk.summary(),
         }

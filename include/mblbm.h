@@ -49,6 +49,10 @@ extern "C" {
 #define MB_PREC_F32 1  /* FP32 storage of f - w (shifted), FP32 arithmetic      */
 #define MB_PREC_F16S 2 /* FP16 storage of f - w (shifted), FP32 arithmetic      */
 #define MB_PREC_F32U 3 /* FP32 storage of f (unshifted), FP32 arithmetic        */
+/* 16-bit storage of f - w (shifted) with a 3-bit exponent and 12-bit
+ * fraction: |f - w| below 1/4, a quarter of FP16's spacing there; FP32
+ * arithmetic.  Out-of-range values saturate and mb_check_finite counts them. */
+#define MB_PREC_F16C 4
 
 /* ---- cell type codes, values as in lbm/lbm.h:26-32 -------------------- */
 #define MB_FLUID 0
@@ -310,9 +314,13 @@ int mb_set_body_force(mb_ctx *ctx, double fx, double fy);
  * x - e_k is HBB takes f_k = F_opp(k) of itself; a slip cell returns
  * F_k = f_slip(k).  The drag sums SBB and HBB links.  Kept across mb_init. */
 int mb_set_cell_types(mb_ctx *ctx, int area, const int *types);
-/* Compiles the plans (and CUDA graphs) that mb_step(ctx, n) will replay from
- * the current state, so the step call itself spends no host time on them. */
+/* Compiles the plans (and CUDA graphs, instantiated and uploaded) that
+ * mb_step(ctx, n) will replay from the current state, so the step call itself
+ * spends no host time on them.  Synchronous; the scheduler state is unchanged. */
 int mb_prepare(mb_ctx *ctx, int n_coarse);
+/* The same for mb_step_diag(ctx, n), whose per-step result buffers it also
+ * sizes, so that the diagnostic call allocates nothing either. */
+int mb_prepare_diag(mb_ctx *ctx, int n_coarse);
 /* evolution_area_stb (multi/FH/evolution_block.h:121) on one block. */
 int mb_block_step(mb_ctx *ctx, int area, mb_stream stream);
 /* Single interface operations, for per-kernel checks. */
@@ -369,8 +377,9 @@ int mb_checkpoint_load(mb_ctx *ctx, const void *host, long long bytes, mb_stream
  * dense) per segment and a device output of 3 doubles:
  *   out[0] = sum over segments of weight * sum |u - u_prev|^2,
  *   out[1] = sum of weight * sum |u|^2,   out[2] = sqrt(out[0]) / sqrt(out[1]),
- * and u_prev <- u, the sums of error_L2 (lbm/error_L2.h:57-91) with weight
- * 1/m per block.  Scratch is a fixed array inside the library (one copy per
+ * and u_prev <- u: with weight 1/m per block these are the two sums of the
+ * relative L2 change that mb_error_L2 reports.  With no cells at all (every
+ * n zero) out[0] = out[1] = 0 and out[2] is 0/0, a NaN.  Scratch is a fixed array inside the library (one copy per
  * device, kept until exit); the first call on a device looks up its address
  * and should come before any stream capture.  Calls share that array, so
  * calls that overlap on the GPU race.  Returns MB_ERR_UNSUPPORTED beyond the

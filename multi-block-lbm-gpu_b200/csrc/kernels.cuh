@@ -6,12 +6,16 @@
 //                  shifted variables (rho = 1 + sum h)
 //   MB_PREC_F16S : half storage of h = f - w_k, float arithmetic as above
 //   MB_PREC_F32U : float storage of f itself, float arithmetic
+//   MB_PREC_F16C : 16-bit storage of h = f - w_k in the format h16c below
+//                  (3 exponent and 12 fraction bits), float arithmetic
 // Distributions live in structure-of-arrays planes: element (k, cell) of a
 // block is F[k*plane + j*pitch + i] with pitch a multiple of 128 bytes.
 #pragma once
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include <type_traits>
 
 #include "../../include/mblbm.h"
 
@@ -25,11 +29,23 @@ __host__ __device__ constexpr int opp(int k) { return k == 0 ? 0 : (k <= 4 ? ((k
 __host__ __device__ constexpr int slip(int k) { return k == 2 ? 4 : k == 4 ? 2 : k == 5 ? 8 : k == 8 ? 5 : k == 6 ? 7 : k == 7 ? 6 : k; }
 __host__ __device__ constexpr double wd(int k) { return k == 0 ? 4. / 9 : (k <= 4 ? 1. / 9 : 1. / 36); }
 
+// Stored word of MB_PREC_F16C: sign, a 3-bit exponent E and a 12-bit fraction
+// M.  E = 1..7 holds +-2^(E-10) (1 + M/4096), magnitudes in [2^-9, 2^-2);
+// E = 0 holds +-2^-9 M/4096 (spacing 2^-21).  Against IEEE binary16 the
+// shifted distributions |h| < 1/4 keep two more fraction bits: the spacing
+// is 1/4 of binary16's at every |h| >= 2^-9 and at most 1/2 of it below.
+// Conversion rounds to nearest (ties to even); magnitudes of 1/4 and above,
+// Inf and NaN saturate to the largest code 0x7fff (with their sign), which
+// mb_check_finite counts as bad.
+struct __align__(2) h16c { unsigned short x; };
+struct __align__(4) h16c2 { unsigned int x; };  // two codes, the lower one first in memory
+
 template <int P> struct Prec;
 template <> struct Prec<MB_PREC_F64> { using S = double; using R = double; static constexpr bool shifted = false; };
 template <> struct Prec<MB_PREC_F32> { using S = float; using R = float; static constexpr bool shifted = true; };
 template <> struct Prec<MB_PREC_F16S> { using S = __half; using R = float; static constexpr bool shifted = true; };
 template <> struct Prec<MB_PREC_F32U> { using S = float; using R = float; static constexpr bool shifted = false; };
+template <> struct Prec<MB_PREC_F16C> { using S = h16c; using R = float; static constexpr bool shifted = true; };
 
 template <int P> __device__ __forceinline__ typename Prec<P>::R wk(int k) { return (typename Prec<P>::R)wd(k); }
 
@@ -41,6 +57,30 @@ template <typename S> __device__ __forceinline__ S from_r(float v);
 template <> __device__ __forceinline__ __half from_r<__half>(float v) { return __float2half_rn(v); }
 template <> __device__ __forceinline__ float from_r<float>(float v) { return v; }
 template <typename S> __device__ __forceinline__ S from_r(double v) { return (S)v; }
+
+// h16c codec.  Decode: the code shifted into an FP32 bit pattern (E into the
+// exponent field, M into the top fraction bits; E = 0 lands on FP32
+// subnormals, which keep the same linear spacing), scaled by 2^117.
+__device__ __forceinline__ float h16c_decode(unsigned int u) {
+  const unsigned int bits = ((u & 0x7fffu) << 11) | ((u & 0x8000u) << 16);
+  return __uint_as_float(bits) * 0x1p117f;
+}
+// Encode: scale by 2^-117 (exact for |v| >= 2^-9; below, the product is
+// rounded to the FP32 subnormal grid 2^-149, 2^-11 of the code's spacing
+// there, so the result is the nearest code up to that much), then round the
+// 11 dropped fraction bits to nearest even with an integer add (the carry
+// moves into the exponent across binade and subnormal boundaries alike),
+// saturating.
+__device__ __forceinline__ unsigned int h16c_encode(float v) {
+  const unsigned int b = __float_as_uint(v * 0x1p-117f);
+  const unsigned int mag = b & 0x7fffffffu;
+  unsigned int r = mag >= 0x7f800000u ? 0x7fffu : (mag + 0x3ffu + ((mag >> 11) & 1u)) >> 11;
+  r = r < 0x7fffu ? r : 0x7fffu;
+  return r | ((b >> 16) & 0x8000u);
+}
+__device__ __forceinline__ float to_r(h16c h) { return h16c_decode(h.x); }
+template <> __device__ __forceinline__ h16c from_r<h16c>(float v) { return h16c{(unsigned short)h16c_encode(v)}; }
+template <> __device__ __forceinline__ h16c from_r<h16c>(double v) { return from_r<h16c>((float)v); }
 
 // value of distribution k from its stored form (shifted forms store f - w_k)
 template <int P>
@@ -58,12 +98,26 @@ __device__ __forceinline__ void st_f(typename Prec<P>::S *p, long long idx, int 
 // the coarse level streams several hundred MB per step and, hinted, leaves
 // the fine levels' buffers resident in L2.
 template <bool EF, typename T> __device__ __forceinline__ T ld_ef(const T *p) {
-  if constexpr (EF) return __ldcs(p);
-  else return *p;
+  if constexpr (EF) {
+    if constexpr (std::is_same<T, h16c>::value) {
+      return h16c{__ldcs((const unsigned short *)p)};
+    } else if constexpr (std::is_same<T, h16c2>::value) {
+      return h16c2{__ldcs((const unsigned int *)p)};
+    } else {
+      return __ldcs(p);
+    }
+  } else {
+    return *p;
+  }
 }
 template <bool EF, typename T> __device__ __forceinline__ void st_ef(T *p, T v) {
-  if constexpr (EF) __stcs(p, v);
-  else *p = v;
+  if constexpr (EF) {
+    if constexpr (std::is_same<T, h16c>::value) __stcs((unsigned short *)p, v.x);
+    else if constexpr (std::is_same<T, h16c2>::value) __stcs((unsigned int *)p, v.x);
+    else __stcs(p, v);
+  } else {
+    *p = v;
+  }
 }
 
 // Programmatic dependent launch: a kernel lets the next one in the graph be
@@ -793,12 +847,18 @@ template <typename S> struct Vec2;
 template <> struct Vec2<float> { using T = float2; };
 template <> struct Vec2<double> { using T = double2; };
 template <> struct Vec2<__half> { using T = __half2; };
+template <> struct Vec2<h16c> { using T = h16c2; };
 __device__ __forceinline__ void unpack2(float2 v, float &a, float &b) { a = v.x; b = v.y; }
 __device__ __forceinline__ void unpack2(double2 v, double &a, double &b) { a = v.x; b = v.y; }
 __device__ __forceinline__ void unpack2(__half2 v, __half &a, __half &b) { a = __low2half(v); b = __high2half(v); }
 __device__ __forceinline__ float2 pack2(float a, float b) { return make_float2(a, b); }
 __device__ __forceinline__ double2 pack2(double a, double b) { return make_double2(a, b); }
 __device__ __forceinline__ __half2 pack2(__half a, __half b) { return __halves2half2(a, b); }
+__device__ __forceinline__ void unpack2(h16c2 v, h16c &a, h16c &b) {
+  a.x = (unsigned short)(v.x & 0xffffu);
+  b.x = (unsigned short)(v.x >> 16);
+}
+__device__ __forceinline__ h16c2 pack2(h16c a, h16c b) { return h16c2{(unsigned int)a.x | ((unsigned int)b.x << 16)}; }
 
 template <int P, bool EF, bool INTERIOR>
 __device__ __forceinline__ void stb_pair(const StbParams &p, const StbBlk &B, int i, int j, bool two) {
@@ -1066,6 +1126,17 @@ template <bool EF> __device__ __forceinline__ void ld_quad(const __half *p, floa
   const uint2 u = ld_ef<EF>((const uint2 *)p);
   const float2 a = __half22float2(*(const __half2 *)&u.x), b = __half22float2(*(const __half2 *)&u.y);
   v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+template <bool EF> __device__ __forceinline__ void ld_quad(const h16c *p, float *v) {
+  const uint2 u = ld_ef<EF>((const uint2 *)p);
+  v[0] = h16c_decode(u.x & 0xffffu); v[1] = h16c_decode(u.x >> 16);
+  v[2] = h16c_decode(u.y & 0xffffu); v[3] = h16c_decode(u.y >> 16);
+}
+template <bool EF> __device__ __forceinline__ void st_quad(h16c *p, const float *v) {
+  uint2 u;
+  u.x = h16c_encode(v[0]) | (h16c_encode(v[1]) << 16);
+  u.y = h16c_encode(v[2]) | (h16c_encode(v[3]) << 16);
+  st_ef<EF>((uint2 *)p, u);
 }
 template <bool EF> __device__ __forceinline__ void st_quad(__half *p, const float *v) {
   const __half2 a = __floats2half2_rn(v[0], v[1]), b = __floats2half2_rn(v[2], v[3]);
@@ -2176,8 +2247,12 @@ __global__ void k_count_nonfinite(const typename Prec<P>::S *F, long long plane,
     const long long c = (long long)j * pitch + i;
 #pragma unroll
     for (int k = 0; k < 9; k++) {
-      const double v = (double)ld_f<P>(F, k * plane + c, k);
-      if (!isfinite(v)) bad++;
+      if constexpr (std::is_same<typename Prec<P>::S, h16c>::value) {
+        if ((F[k * plane + c].x & 0x7fffu) == 0x7fffu) bad++;  // saturated: out of range, Inf or NaN
+      } else {
+        const double v = (double)ld_f<P>(F, k * plane + c, k);
+        if (!isfinite(v)) bad++;
+      }
     }
   }
   if (bad) atomicAdd(count, bad);

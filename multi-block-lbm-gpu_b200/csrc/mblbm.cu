@@ -36,7 +36,9 @@ using namespace mblbm::dev;
 
 namespace {
 
-size_t prec_bytes(int prec) { return prec == MB_PREC_F64 ? 8 : (prec == MB_PREC_F16S ? 2 : 4); }
+size_t prec_bytes(int prec) {
+  return prec == MB_PREC_F64 ? 8 : ((prec == MB_PREC_F16S || prec == MB_PREC_F16C) ? 2 : 4);
+}
 size_t real_bytes(int prec) { return prec == MB_PREC_F64 ? 8 : 4; }
 
 // One part of error_L2 (interiors of split levels, or every other cell) as
@@ -178,7 +180,6 @@ struct mb_ctx {
   int prg_launches = 0;
   std::map<std::string, std::unique_ptr<CompiledPlan>> plans;
   long long kernels_last_call = 0;
-  long long kernels_per_step = 0;
   long long updates_per_step = 0;
 };
 
@@ -198,6 +199,10 @@ namespace {
     } else if ((prec) == MB_PREC_F32U) {                            \
       constexpr int P = MB_PREC_F32U;                               \
       using S = float;                                              \
+      STMT;                                                         \
+    } else if ((prec) == MB_PREC_F16C) {                            \
+      constexpr int P = MB_PREC_F16C;                               \
+      using S = h16c;                                               \
       STMT;                                                         \
     } else {                                                        \
       constexpr int P = MB_PREC_F16S;                               \
@@ -266,6 +271,7 @@ void *kfunc(int prec) {
   if (prec == MB_PREC_F64) return K<MB_PREC_F64>::ptr();
   if (prec == MB_PREC_F32) return K<MB_PREC_F32>::ptr();
   if (prec == MB_PREC_F32U) return K<MB_PREC_F32U>::ptr();
+  if (prec == MB_PREC_F16C) return K<MB_PREC_F16C>::ptr();
   return K<MB_PREC_F16S>::ptr();
 }
 template <int P> struct KStb { static void *ptr() { return (void *)k_block_step<P, 1>; } };
@@ -282,6 +288,7 @@ int tb_smem(int prec) {
   switch (prec) {
     case MB_PREC_F64: return TbCfg<double>::SMEM;
     case MB_PREC_F16S: return TbCfg<__half>::SMEM;
+    case MB_PREC_F16C: return TbCfg<h16c>::SMEM;
     default: return TbCfg<float>::SMEM;
   }
 }
@@ -1071,7 +1078,8 @@ int exec_nodes_once(mb_ctx *c, std::vector<PlanNode> nodes, cudaStream_t s) {
 extern "C" int mb_create(const mb_geometry *geo, int precision, mb_ctx **out) {
   if (!geo || !out) return MB_ERR_INVALID;
   *out = nullptr;
-  if (precision != MB_PREC_F64 && precision != MB_PREC_F32 && precision != MB_PREC_F16S && precision != MB_PREC_F32U)
+  if (precision != MB_PREC_F64 && precision != MB_PREC_F32 && precision != MB_PREC_F16S && precision != MB_PREC_F32U &&
+      precision != MB_PREC_F16C)
     return MB_ERR_INVALID;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return MB_ERR_NODEVICE;
@@ -1087,7 +1095,7 @@ extern "C" int mb_create(const mb_geometry *geo, int precision, mb_ctx **out) {
   // ranges on level 0 and one cell per thread elsewhere; level 0 alone 39.7
   // against 46.0 us); FP32 storage gains from the quads' vector accesses on
   // level 0 (112 against 117 us with the split level 0)
-  if (precision == MB_PREC_F16S)
+  if (precision == MB_PREC_F16S || precision == MB_PREC_F16C)
     for (int l = 0; l < MB_MAX_LEVEL; l++) c->stb_variant[l] = 4;
   if (precision == MB_PREC_F32 || precision == MB_PREC_F32U) c->stb_variant[0] = 1;
   cudaGetDevice(&c->device);
@@ -1702,44 +1710,91 @@ extern "C" int mb_step(mb_ctx *c, int n, mb_stream stream) {
     if ((err = exec_plan(c, cp, s))) return err;
     remaining -= chunk;
   }
-  {
-    int err = 0;
-    SchedState save = c->state;
-    CompiledPlan *cp = get_plan(c, 1, true, &err);
-    if (cp) c->kernels_per_step = cp->kernels;
-    c->state = save;
-  }
   MB_CUDA(cudaGetLastError());
   return MB_OK;
 }
 
-// Compiles (and instantiates as graphs) every plan mb_step(n) will replay from
-// the current state, so that a later mb_step spends no host time on it.
-extern "C" int mb_prepare(mb_ctx *c, int n) {
-  if (!c || n < 0) return MB_ERR_INVALID;
-  if (!c->inited) return MB_ERR_STATE;
+namespace {
+// Makes a compiled plan ready to replay: the executor program (mode 3) or the
+// instantiated CUDA graph, uploaded on `up` so that its first launch pays no
+// upload.  Direct launches (mode 0) need nothing.
+int ready_plan(mb_ctx *c, CompiledPlan *cp, cudaStream_t up) {
+  if (c->use_graph == 3) return cp->prg_built ? MB_OK : build_program(c, *cp);
+  if (!c->use_graph || cp->exec) return MB_OK;
+  if (int e = build_graph(*cp, c->use_graph == 2)) return e;
+  MB_CUDA(cudaGraphUpload(cp->exec, up));
+  return MB_OK;
+}
+
+// Host side of mb_prepare / mb_prepare_diag: walks the chunks the step call
+// will take from the current state (the scheduler state is restored after).
+int prepare_chunks(mb_ctx *c, int n, bool diag) {
+  cudaStream_t up = nullptr;
+  MB_CUDA(cudaStreamCreateWithFlags(&up, cudaStreamNonBlocking));
   const SchedState save = c->state;
-  int remaining = n, err = 0;
+  int remaining = n, err = MB_OK;
   const int G = c->use_graph == 3 ? c->period * c->prg_periods : c->period;
-  while (remaining > 0) {
+  while (remaining > 0 && err == MB_OK) {
+    CompiledPlan *cp = nullptr;
     int chunk;
-    bool fin;
-    if (remaining - 1 >= G) { chunk = G; fin = false; }
-    else if (remaining > 1) { chunk = 1; fin = false; }
-    else { chunk = 1; fin = true; }
-    CompiledPlan *cp = get_plan(c, chunk, fin, &err);
-    if (!cp) { c->state = save; return err ? err : MB_ERR_INVALID; }
-    if (c->use_graph == 3) {
-      if (!cp->prg_built && (err = build_program(c, *cp))) { c->state = save; return err; }
-    } else if (c->use_graph && !cp->exec && (err = build_graph(*cp, c->use_graph == 2))) {
-      c->state = save;
-      return err;
+    if (diag && c->use_graph != 3) {  // mb_step_diag: plans of `period` steps, else single steps
+      chunk = remaining >= c->period ? c->period : 1;
+      cp = get_diag_plan(c, chunk, &err);
+    } else if (diag) {  // executor: one final-state step per plan, drag and L2 launched apart
+      chunk = 1;
+      cp = get_plan(c, 1, true, &err);
+    } else {
+      bool fin;
+      if (remaining - 1 >= G) { chunk = G; fin = false; }
+      else if (remaining > 1) { chunk = 1; fin = false; }
+      else { chunk = 1; fin = true; }
+      cp = get_plan(c, chunk, fin, &err);
     }
+    if (!cp) { err = err ? err : MB_ERR_INVALID; break; }
+    if ((err = ready_plan(c, cp, up))) break;
     c->state = cp->end;
     remaining -= chunk;
   }
   c->state = save;
+  const cudaError_t se = cudaStreamSynchronize(up);
+  cudaStreamDestroy(up);
+  if (err) return err;
+  return se == cudaSuccess ? MB_OK : MB_ERR_CUDA;
+}
+
+// Grows the per-step result buffers of mb_step_diag to n steps (device and
+// pinned host memory); the stream drains first when they are replaced.
+int ensure_diag(mb_ctx *c, size_t n, cudaStream_t s) {
+  if (n <= c->diag_cap) return MB_OK;
+  MB_CUDA(cudaStreamSynchronize(s));
+  const size_t cap = std::max(n, 2 * c->diag_cap);
+  if (c->d_diag) cudaFree(c->d_diag);
+  if (c->h_diag) cudaFreeHost(c->h_diag);
+  c->d_diag = nullptr;
+  c->h_diag = nullptr;
+  c->diag_cap = 0;
+  if (cudaMalloc(&c->d_diag, cap * DIAG_STRIDE * sizeof(double)) != cudaSuccess) return MB_ERR_NOMEM;
+  if (cudaMallocHost(&c->h_diag, cap * DIAG_STRIDE * sizeof(double)) != cudaSuccess) return MB_ERR_NOMEM;
+  c->diag_cap = cap;
   return MB_OK;
+}
+}  // namespace
+
+// Compiles (and instantiates and uploads as graphs) every plan mb_step(n) will
+// replay from the current state, so that a later mb_step spends no host time
+// on it.
+extern "C" int mb_prepare(mb_ctx *c, int n) {
+  if (!c || n < 0) return MB_ERR_INVALID;
+  if (!c->inited) return MB_ERR_STATE;
+  return prepare_chunks(c, n, false);
+}
+
+// The same for mb_step_diag(n), which also gets its result buffers sized.
+extern "C" int mb_prepare_diag(mb_ctx *c, int n) {
+  if (!c || n < 0) return MB_ERR_INVALID;
+  if (!c->inited) return MB_ERR_STATE;
+  if (int e = ensure_diag(c, (size_t)n, nullptr)) return e;
+  return prepare_chunks(c, n, true);
 }
 
 extern "C" int mb_block_step(mb_ctx *c, int area, mb_stream stream) {
@@ -1887,18 +1942,7 @@ extern "C" int mb_step_diag(mb_ctx *c, int n, double *cd, double *cl, double *er
   if (!c->inited) return MB_ERR_STATE;
   if (n == 0) return MB_OK;
   cudaStream_t s = (cudaStream_t)stream;
-  if ((size_t)n > c->diag_cap) {
-    MB_CUDA(cudaStreamSynchronize(s));
-    if (c->d_diag) cudaFree(c->d_diag);
-    if (c->h_diag) cudaFreeHost(c->h_diag);
-    c->d_diag = nullptr;
-    c->h_diag = nullptr;
-    c->diag_cap = 0;
-    const size_t cap = std::max<size_t>((size_t)n, 2 * c->diag_cap);
-    if (cudaMalloc(&c->d_diag, cap * DIAG_STRIDE * sizeof(double)) != cudaSuccess) return MB_ERR_NOMEM;
-    if (cudaMallocHost(&c->h_diag, cap * DIAG_STRIDE * sizeof(double)) != cudaSuccess) return MB_ERR_NOMEM;
-    c->diag_cap = cap;
-  }
+  if (int e = ensure_diag(c, (size_t)n, s)) return e;
   c->kernels_last_call = 0;
   if (c->use_graph != 3) {
     // plans of `period` steps with their diagnostics; each plan's results go
@@ -2182,7 +2226,19 @@ extern "C" int mb_write_tecplot(mb_ctx *c, const char *path) {
 extern "C" int mb_stats(mb_ctx *c, long long *kl, long long *kps, long long *ups) {
   if (!c) return MB_ERR_INVALID;
   if (kl) *kl = c->kernels_last_call;
-  if (kps) *kps = c->kernels_per_step;
+  if (kps) {
+    // launches of one final-state coarse step from the current scheduler
+    // state (its plan is compiled here if no step call has needed it yet)
+    *kps = 0;
+    if (c->inited) {
+      int err = 0;
+      const SchedState save = c->state;
+      CompiledPlan *cp = get_plan(c, 1, true, &err);
+      c->state = save;
+      if (!cp) return err ? err : MB_ERR_INVALID;
+      *kps = cp->kernels;
+    }
+  }
   if (ups) *ups = c->updates_per_step;
   return MB_OK;
 }

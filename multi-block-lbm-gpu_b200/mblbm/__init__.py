@@ -22,9 +22,11 @@ MB_MAX_LINE = 128
 MB_MAX_LINE2 = 128
 
 MB_OK = 0
-PREC_F64, PREC_F32, PREC_F16S, PREC_F32U = 0, 1, 2, 3
-# f32: FP32 storage of f - w (the product FP32 form); f32u: FP32 storage of f
-PRECISIONS = {"f64": PREC_F64, "f32": PREC_F32, "f16s": PREC_F16S, "f32u": PREC_F32U}
+PREC_F64, PREC_F32, PREC_F16S, PREC_F32U, PREC_F16C = 0, 1, 2, 3, 4
+# f32: FP32 storage of f - w (the product FP32 form); f32u: FP32 storage of f;
+# f16s: IEEE FP16 storage of f - w; f16c: 16-bit storage of f - w with a
+# 3-bit exponent and 12-bit fraction (a quarter of FP16's spacing for |f - w| < 1/4)
+PRECISIONS = {"f64": PREC_F64, "f32": PREC_F32, "f16s": PREC_F16S, "f32u": PREC_F32U, "f16c": PREC_F16C}
 FLUID, SOLID_SBB, C_BOUNDARY = 0, 1, 9
 OBST_CIRCLE, OBST_ELLIPSE, OBST_NONE = 0, 1, 2
 PERIODIC_X, PERIODIC_Y, DIR_PERIODIC = 1, 2, 8  # mb_config.periodic bits, NeborCC code of ghost lines
@@ -175,6 +177,7 @@ SIGNATURES = {
     "mb_program_trace": ([_vp, _vp, C.c_longlong, C.POINTER(C.c_longlong)], C.c_int),
     "mb_program_selftest": ([_vp, C.c_int, _vp], C.c_int),
     "mb_prepare": ([_vp, C.c_int], C.c_int),
+    "mb_prepare_diag": ([_vp, C.c_int], C.c_int),
     "mb_block_step": ([_vp, C.c_int, _vp], C.c_int),
     "mb_c_c_boundary_transfer": ([_vp, C.c_int, _vp], C.c_int),
     "mb_space_interpolation": ([_vp, C.c_int, _vp], C.c_int),
@@ -586,6 +589,11 @@ class MultiBlockLBM:
         """Compiles the plans and graphs that evolution(n_coarse) will replay."""
         _check(self.lib.mb_prepare(self.h, int(n_coarse)), "mb_prepare")
 
+    def prepare_diag(self, n_coarse):
+        """Compiles the plans and graphs that evolution_diag(n_coarse) will replay
+        and sizes its result buffers."""
+        _check(self.lib.mb_prepare_diag(self.h, int(n_coarse)), "mb_prepare_diag")
+
     def block_step(self, area, stream=None):
         _check(self.lib.mb_block_step(self.h, area, _stream_ptr(stream)), "mb_block_step")
 
@@ -642,14 +650,17 @@ class MultiBlockLBM:
     def fields(self, area, stream=None, out=None):
         """Dict of FP64 host arrays rho, ux, uy (ny, nx), F (9, ny, nx), solid (ny, nx).
         out: a dict of preallocated C-contiguous arrays of those shapes (pinned
-        host memory makes the copies direct) to fill instead."""
+        host memory makes the copies direct) to fill instead; without an "F"
+        entry the distributions are not copied."""
         A = self.geo.Areas[area]
         nx, ny = A.nx, A.ny
         if out is not None:
-            rho, ux, uy, F, solid = (out[k] for k in ("rho", "ux", "uy", "F", "solid"))
+            rho, ux, uy, F, solid = (out.get(k) for k in ("rho", "ux", "uy", "F", "solid"))
             for k, shp, dt in (("rho", (ny, nx), np.float64), ("ux", (ny, nx), np.float64), ("uy", (ny, nx), np.float64),
                                ("F", (9, ny, nx), np.float64), ("solid", (ny, nx), np.int32)):
-                a = out[k]
+                a = out.get(k)
+                if a is None and k == "F":
+                    continue
                 if a.size != int(np.prod(shp)) or a.dtype != dt or not a.flags.c_contiguous:
                     raise ValueError(f"out[{k!r}] must be a C-contiguous {dt.__name__} array of {shp}")
         else:
@@ -659,10 +670,12 @@ class MultiBlockLBM:
             F = np.empty((9, ny, nx))
             solid = np.empty((ny, nx), dtype=np.int32)
         _check(
-            self.lib.mb_copy_fields(self.h, area, _dp(rho), _dp(ux), _dp(uy), _dp(F), solid.ctypes.data_as(_pi), _stream_ptr(stream)),
+            self.lib.mb_copy_fields(self.h, area, _dp(rho), _dp(ux), _dp(uy), None if F is None else _dp(F),
+                                    solid.ctypes.data_as(_pi), _stream_ptr(stream)),
             "mb_copy_fields",
         )
-        return {"rho": rho, "ux": ux, "uy": uy, "F": F, "solid": solid}
+        res = {"rho": rho, "ux": ux, "uy": uy, "F": F, "solid": solid}
+        return res if F is not None else {k: v for k, v in res.items() if k != "F"}
 
     def macros(self, area, stream=None):
         """Dict of FP64 host arrays rho, ux, uy and solid (ny, nx), without the distributions."""

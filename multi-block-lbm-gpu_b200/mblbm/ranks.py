@@ -31,6 +31,23 @@ def shard(case_ids, rank, world):
     return list(case_ids)[rank::world]
 
 
+def balance(costs, rank, world):
+    """The cases of one rank when cases differ in cost (cell updates per
+    coarse step): longest-processing-time-first assignment, every case to the
+    rank with the least total so far (ties to the lowest rank).  Every rank
+    computes the same assignment from the same costs; the shards are disjoint,
+    cover every case, and no rank's total exceeds the mean by more than the
+    largest single cost.  Returns the case indices of `rank`, ascending."""
+    order = sorted(range(len(costs)), key=lambda i: (-costs[i], i))
+    load = [0] * world
+    owner = [0] * len(costs)
+    for i in order:
+        r = min(range(world), key=lambda q: (load[q], q))
+        owner[i] = r
+        load[r] += costs[i]
+    return [i for i in range(len(costs)) if owner[i] == rank]
+
+
 def reduce(values, op, dist=None, device="cpu"):
     """Element-wise MAX or SUM of a list of floats over all ranks (identity
     without a process group); every rank gets the result."""

@@ -11,6 +11,10 @@ runs `ref_<case> golden <steps>` in a scratch directory and writes
   solid_<a>, Fsum_<a>, fsum_<a>       cell types and per-direction sums
   markers, slotsum                    ring markers and per-slot sums per line
   tecplot                             steady_<steps>.dat text (case g11 only)
+With --long CASE STEPS it runs one benchmark case (c1: the 400x160 2-level
+cylinder at Re=40) for STEPS coarse steps and writes <out>/<CASE>_<STEPS>.npz
+with the final rho/ux/uy of every block and the drag and error_L2 series
+sampled every --every steps (pack_long).
 The committed fixtures in tests/golden/ were produced by
     python oracle/ref_harness/make_ref.py && python oracle/ref_harness/make_golden.py --out <dir>
 on a B200 and copied from <dir>.
@@ -72,12 +76,55 @@ def pack(name, wd, geo, steps):
     return out
 
 
+def pack_long(wd, geo, steps, every):
+    """A long run of a benchmark case, kept small: the final rho, ux, uy of
+    every block (FP64), the cell types, and the drag and error_L2 series
+    sampled every `every` steps plus the last step."""
+    L = geo.layout
+    out = {}
+    drag = np.fromfile(os.path.join(wd, "drag.bin"), dtype=np.float64).reshape(steps, 2)
+    l2 = np.array([float(line.split()[1]) for line in open(os.path.join(wd, "error_L2.dat")) if line.strip()])
+    idx = np.unique(np.r_[np.arange(every - 1, steps, every), steps - 1])
+    out["sample_steps"] = idx + 1
+    out["drag"] = drag[idx]
+    out["l2"] = l2[idx]
+    buf = open(os.path.join(wd, "fields.bin"), "rb").read()
+    off = 0
+    for a in range(L.number_area):
+        nx, ny = geo.Areas[a].nx, geo.Areas[a].ny
+        N = nx * ny
+        out[f"solid_{a}"] = np.frombuffer(buf, dtype=np.int32, count=N, offset=off).reshape(ny, nx).astype(np.int8)
+        off += 4 * N
+        arr = np.frombuffer(buf, dtype=np.float64, count=25 * N, offset=off).reshape(25, ny, nx)
+        off += 8 * 27 * N
+        out[f"rho_{a}"] = arr[2].copy()
+        out[f"ux_{a}"] = arr[3].copy()
+        out[f"uy_{a}"] = arr[4].copy()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", required=True)
+    ap.add_argument("--long", nargs=2, metavar=("CASE", "STEPS"),
+                    help="one long run of a benchmark case (e.g. c1 20000), packed as <out>/<CASE>_<STEPS>.npz")
+    ap.add_argument("--every", type=int, default=20, help="--long: drag and L2 sample interval")
     ap.add_argument("names", nargs="*")
     a = ap.parse_args()
     os.makedirs(a.out, exist_ok=True)
+    if a.long:
+        name, steps = a.long[0], int(a.long[1])
+        L, cfg, _ = make_ref.case(name)
+        geo = mblbm.geo_init(L, cfg)
+        exe = os.path.join(make_ref.OUT, f"ref_{name}")
+        wd = tempfile.mkdtemp(prefix=f"ref_{name}_")
+        r = subprocess.run([exe, "golden", str(steps)], cwd=wd, capture_output=True, text=True, timeout=3000)
+        print(name, steps, r.returncode, r.stdout.strip(), r.stderr.strip()[-500:], flush=True)
+        if r.returncode != 0:
+            return 1
+        np.savez_compressed(os.path.join(a.out, f"{name}_{steps}.npz"), steps=steps,
+                            **pack_long(wd, geo, steps, a.every))
+        return 0
     for name in a.names or make_ref.GOLDEN:
         L, cfg, steps = make_ref.case(name)
         geo = mblbm.geo_init(L, cfg)

@@ -10,7 +10,8 @@ types as those files) into oracle/_ref/cfg_<name>.h and compiles
 so every kernel, geo_init, evolution, error_L2 and getDrag_block come from the
 unmodified reference sources where they lie; nothing is copied into the
 repository.  The binaries run on a GPU box only (oracle/_ref travels with the
-snapshot).  Usage: python make_ref.py [--ref /root/reference] [names...]
+snapshot).  Usage: python make_ref.py [--ref DIR] [names...]; the reference
+tree is DIR, else $MBLBM_REFERENCE_DIR, else reference_dir()'s default.
 """
 import argparse
 import os
@@ -101,6 +102,12 @@ def race_notes(L, cfg):
     return notes
 
 
+def reference_dir():
+    """Where the reference sources lie: $MBLBM_REFERENCE_DIR, else the
+    read-only checkout of the build machine."""
+    return os.environ.get("MBLBM_REFERENCE_DIR", "/root/reference")
+
+
 def build(name, ref):
     L, cfg, _ = case(name)
     os.makedirs(OUT, exist_ok=True)
@@ -119,9 +126,10 @@ def build(name, ref):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=None, help="reference source tree (default: reference_dir())")
     ap.add_argument("names", nargs="*")
     a = ap.parse_args()
+    a.ref = a.ref or reference_dir()
     if not os.path.isdir(a.ref):
         print(f"reference tree {a.ref} absent; nothing built")
         return 0

@@ -183,9 +183,13 @@ int main(int argc, char **argv) {
     float t1 = 0, t2 = 0;
     cudaEventElapsedTime(&t1, e0, e1);
     cudaEventElapsedTime(&t2, e1, e2);
+    // cell updates of one coarse step from the reference's own block table:
+    // a block of cumulative ratio m takes m sub-steps per coarse step
+    long long updates = 0;
+    for (int a = 0; a < number_area; a++) updates += (long long)Areas[a].nx * Areas[a].ny * Areas[a].m;
     printf("{\"ms_per_step\": %.6f, \"ms_per_step_diag\": %.6f, \"steps\": %d, \"warmup\": %d, \"Fx\": %.17g, "
-           "\"status\": \"%s\"}\n",
-           t1 / nsteps, t2 / nsteps, nsteps, warm, Force[0], cudaGetErrorString(cudaGetLastError()));
+           "\"cell_updates_per_step\": %lld, \"status\": \"%s\"}\n",
+           t1 / nsteps, t2 / nsteps, nsteps, warm, Force[0], updates, cudaGetErrorString(cudaGetLastError()));
   }
   cusparseDestroy(handle);
   return 0;

@@ -148,7 +148,7 @@ def test_interface_ops_random_state(mb, orc, cuda_device, name):
     check(1e-13)
 
 
-@pytest.mark.parametrize("prec,tol_u,tol_cd", [("f32", 1e-5, 1e-4), ("f16s", 5e-3, 5e-3)])
+@pytest.mark.parametrize("prec,tol_u,tol_cd", [("f32", 1e-5, 1e-4), ("f16s", 5e-3, 5e-3), ("f16c", 2e-3, 2e-3)])
 def test_reduced_precision_error(mb, orc, cuda_device, prec, tol_u, tol_cd):
     """Config-1 layout (400x160, Re=40) for 2000 coarse steps against the oracle."""
     g = mb.config1_geometry()
@@ -287,7 +287,7 @@ def test_interior_rim_split(mb, orc, cuda_device, name):
 
 @pytest.mark.parametrize("split", [0, 10**12])
 @pytest.mark.parametrize("variant", [1, 2, 3, 4, 5])
-@pytest.mark.parametrize("prec", ["f32", "f16s", "f64"])
+@pytest.mark.parametrize("prec", ["f32", "f16s", "f64", "f16c"])
 def test_quad_kernel_equals_cell_kernel(mb, cuda_device, prec, variant, split):
     """Every block-step variant gives bitwise the same state, on whole levels
     and on split (interior + rim) levels."""
@@ -350,7 +350,7 @@ def test_checkpoint_restart_bitwise(mb, cuda_device, tmp_path):
 
 @pytest.mark.parametrize("graph", [True, False])
 @pytest.mark.parametrize("split", [10**12, 0])
-@pytest.mark.parametrize("prec", ["f32", "f64", "f16s"])
+@pytest.mark.parametrize("prec", ["f32", "f64", "f16s", "f16c"])
 def test_step_diag_equals_step_by_step(mb, cuda_device, prec, split, graph):
     """mb_step_diag (plans of several steps with the drag and the L2 change of
     each step beside the next) gives the values of mb_step(1), mb_drag and
@@ -380,8 +380,8 @@ def test_step_diag_equals_step_by_step(mb, cuda_device, prec, split, graph):
 
 
 @pytest.mark.parametrize("graph", [True, False, "program"])
-@pytest.mark.parametrize("split,variant", [(10**12, 0), (0, 0), (10**12, 4), (0, 3)])
-@pytest.mark.parametrize("name,prec", [("n3", "f32"), ("g49", "f64"), ("g25", "f16s")])
+@pytest.mark.parametrize("split,variant", [(10**12, 0), (0, 0), (10**12, 4), (0, 4), (0, 3), (0, 5)])
+@pytest.mark.parametrize("name,prec", [("n3", "f32"), ("g49", "f64"), ("g25", "f16s"), ("n3", "f16c")])
 def test_fused_copies_bitwise(mb, cuda_device, name, prec, split, variant, graph):
     """Same-level copies done inside the block step (mb_set_fusion bit 0) and
     temporal interpolations done by the splines (bits 1 and 2), alone and
@@ -405,3 +405,27 @@ def test_fused_copies_bitwise(mb, cuda_device, name, prec, split, variant, graph
                 assert np.array_equal(fa[key], fb[key]), (k, key)
         assert cd0 == other.getDrag_block()[2]
         assert l20 == other.error_L2()
+
+
+@pytest.mark.parametrize("graph", [True, False])
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_fused_tskip_options_kernel_bitwise(mb, cuda_device, prec, graph):
+    """With a collision option on, every block step runs the options kernel
+    (k_block_step_x); the splines' next temporal interpolation (fusion bit 2,
+    with the fine substep in between leaving those edge cells alone) still
+    gives bitwise the state of separate launches."""
+    g = mb.geo_init(*make_ref.case("n3")[:2])
+    sims = []
+    for fuse in (0, 4, 5, 7):
+        s = mb.MultiBlockLBM(g, prec, graph=graph)
+        s.set_fusion(fuse)
+        s.set_body_force(1e-6, 0.0)
+        s.init()
+        s.evolution(13)
+        sims.append(s)
+    for other in sims[1:]:
+        for k in range(g.layout.number_area):
+            fa, fb = sims[0].fields(k), other.fields(k)
+            for key in ("F", "rho", "ux", "uy"):
+                assert np.array_equal(fa[key], fb[key]), (k, key)
+        assert sims[0].getDrag_block()[2] == other.getDrag_block()[2]

@@ -89,7 +89,7 @@ def test_fused_ghost_copies_bitwise(mb, cuda_device):
                 assert np.array_equal(fa[key], fb[key])
 
 
-@pytest.mark.parametrize("prec,tol", [("f32", 1e-5), ("f32u", 5e-5), ("f16s", 5e-3)])
+@pytest.mark.parametrize("prec,tol", [("f32", 1e-5), ("f32u", 5e-5), ("f16s", 5e-3), ("f16c", 2e-3)])
 def test_reduced_precision_periodic(mb, orc, cuda_device, prec, tol):
     g, o, m = pair(mb, orc, "tgv2", prec)
     o.evolution(200)
@@ -111,7 +111,7 @@ def test_tgv_1024_two_levels_decay(mb, cuda_device):
     nu = (g.Areas[0].tau - 0.5) / 3.0
     k = 2 * np.pi / 1024
     amp = {}
-    for prec in ("f64", "f32", "f16s"):
+    for prec in ("f64", "f32", "f16s", "f16c"):
         s = mb.MultiBlockLBM(g, prec)
         s.init()
         mb.tgv_init(s, g)
@@ -131,6 +131,7 @@ def test_tgv_1024_two_levels_decay(mb, cuda_device):
     assert amp["f64"] == pytest.approx(exact, rel=1e-3)
     assert amp["f32"] == pytest.approx(amp["f64"], rel=5e-4)
     assert amp["f16s"] == pytest.approx(amp["f64"], rel=2e-3)
+    assert amp["f16c"] == pytest.approx(amp["f64"], rel=1e-3)
 
 
 @pytest.mark.parametrize("levels", [1, 2])

@@ -38,7 +38,7 @@ def assert_same_state(g, a, b):
     assert a.getDrag_block() == b.getDrag_block()
 
 
-@pytest.mark.parametrize("prec", ["f32", "f16s", "f64", "f32u"])
+@pytest.mark.parametrize("prec", ["f32", "f16s", "f64", "f32u", "f16c"])
 @pytest.mark.parametrize("name", ["n3", "g49", "c1"])
 def test_program_equals_graph_bitwise(mb, cuda_device, name, prec):
     g = mb.geo_init(*make_ref.case(name)[:2])

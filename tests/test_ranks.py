@@ -28,9 +28,13 @@ def _worker(rank, world, port, q):
     mine = ranks.shard(range(10), r, w)
     mx = ranks.reduce([1.0 + r, 10.0 - r], "max", dist)
     sm = ranks.reduce([len(mine)], "sum", dist)
+    # the batched workload's shards: cases of uneven cost, balanced by cost
+    costs = [(7 * i * i + 3) % 41 + 1 for i in range(37)]
+    bal = ranks.balance(costs, r, w)
+    load = ranks.reduce([sum(costs[i] for i in bal), len(bal)], "sum", dist)
     dist.barrier()
     dist.destroy_process_group()
-    q.put((r, w, lr, mine, mx, sm))
+    q.put((r, w, lr, mine, mx, sm, bal, load))
 
 
 def test_two_gloo_ranks():
@@ -46,11 +50,16 @@ def test_two_gloo_ranks():
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
-    (r0, w0, l0, s0, mx0, sm0), (r1, w1, l1, s1, mx1, sm1) = out
+    (r0, w0, l0, s0, mx0, sm0, b0, ld0), (r1, w1, l1, s1, mx1, sm1, b1, ld1) = out
     assert (r0, r1, w0, w1, l0, l1) == (0, 1, 2, 2, 0, 1)
     assert sorted(s0 + s1) == list(range(10)) and not set(s0) & set(s1)
     assert mx0 == mx1 == [2.0, 10.0]
     assert sm0 == sm1 == [10.0]
+    costs = [(7 * i * i + 3) % 41 + 1 for i in range(37)]
+    assert sorted(b0 + b1) == list(range(37)) and not set(b0) & set(b1)
+    assert ld0 == ld1 == [float(sum(costs)), 37.0]
+    t0, t1 = sum(costs[i] for i in b0), sum(costs[i] for i in b1)
+    assert abs(t0 - t1) <= max(costs)
 
 
 def test_single_rank_is_identity():
@@ -60,3 +69,18 @@ def test_single_rank_is_identity():
     from mblbm import ranks
     assert ranks.reduce([3.0, 4.0], "max") == [3.0, 4.0]
     assert ranks.shard(range(5), 0, 1) == [0, 1, 2, 3, 4]
+    assert ranks.balance([5, 1, 9], 0, 1) == [0, 1, 2]
+
+
+def test_balance_bound():
+    """Greedy longest-first: disjoint, complete, within one largest cost of the mean."""
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                                    "multi-block-lbm-gpu_b200"))
+    from mblbm import ranks
+    costs = [((i * 2654435761) % 1000) + 100 for i in range(256)]
+    for world in (2, 3, 4, 8):
+        shards = [ranks.balance(costs, r, world) for r in range(world)]
+        assert sorted(sum(shards, [])) == list(range(256))
+        loads = [sum(costs[i] for i in s) for s in shards]
+        assert max(loads) - sum(costs) / world <= max(costs)
