@@ -225,6 +225,19 @@ def run_batch(args):
     ms = e0.elapsed_time(e1)
     kernels = sum(b.stats()["kernels_last_call"] for b in batches)
     cds = [b.drag(stream)[0] for b in batches]
+    # per-case Cd against the single-case solver: a few cases of each batch
+    # stepped alone from rest for as many coarse steps as the batch took
+    check = []
+    for b, sims in zip(batches, [v for v in groups.values() if v]):
+        done = b.stats()["steps_done"]
+        cd_b = b.drag(stream)[0]
+        for q in sorted({0, len(sims) // 2, len(sims) - 1})[: args.cd_check]:
+            one = mblbm.MultiBlockLBM(sims[q].geo, args.precision)
+            one.init(stream)
+            one.evolution(done, stream)
+            cd1 = one.getDrag_block(stream)[2]
+            check.append(abs(float(cd_b[q]) / cd1 - 1.0) if cd1 != 0 else abs(float(cd_b[q])))
+            one.close()
     cd_lo = min(float(c.min()) for c in cds) if cds else float("inf")
     cd_hi = max(float(c.max()) for c in cds) if cds else float("-inf")
     ms, = ranks.reduce([ms], "max", dist, device="cuda")
@@ -247,7 +260,8 @@ def run_batch(args):
                              "frac": round(achieved / peak, 4), "traffic": None, "peak_source": src,
                              "kernel": "whole batched step (all launches)", "bytes_per_update": bpu},
                 "gpu_launches": int(tot_kernels), "clocks": clk.summary(),
-                "cd_range_rank0": [round(cd_lo, 4), round(cd_hi, 4)]}
+                "cd_range_rank0": [round(cd_lo, 4), round(cd_hi, 4)],
+                "cd_vs_single_case_rank0": {"cases": len(check), "max_rel_diff": max(check) if check else None}}
         print(json.dumps(line), flush=True)
     for b in batches:
         b.close()
@@ -313,8 +327,10 @@ def run_warmstart(args):
     sampled every 50 steps; its running mean (500 steps for steady cases,
     Re < 47; 150 D steps, at least one shedding period, otherwise) must
     settle within 0.5 % of the cold run's final running mean.  A warm start
-    whose final running mean differs from the cold one by more than 0.5 % is
-    rejected and its case counted at the cold start's time (fallback)."""
+    whose final running mean differs from the cold one by more than 0.5 %, or
+    (shedding cases) whose Strouhal number over the second half of the run
+    differs from the cold one's by more than 1 %, is rejected and its case
+    counted at the cold start's time (fallback)."""
     import numpy as np
     import torch
     import mblbm
@@ -341,16 +357,27 @@ def run_warmstart(args):
     t_warm_total = time.perf_counter() - t2
     res = []
     for i in eval_ids:
-        sc, prm, key = cold[i]
-        sw = warm[i][0]
+        sc, prm, key, lc = cold[i]
+        sw, lw = warm[i][0], warm[i][3]
         win = 10 if prm["Re"] < 47 else max(10, int(np.ceil(150 * prm["D"] / chunk)))
         kern = np.ones(win) / win
         rc, rw = np.convolve(sc, kern, "valid"), np.convolve(sw, kern, "valid")
         ref = rc[-1]
         nc, nw = mblbm.settle_step(rc, ref), mblbm.settle_step(rw, ref)
         ok = abs(rw[-1] / ref - 1.0) <= 0.005
+        # shedding cases: the Strouhal number of the second half of the run
+        # (lift sampled every `chunk` steps) must also agree within 1 %
+        st_c = st_w = None
+        if prm["Re"] >= 47:
+            half = len(lc) // 2
+            st_c = mblbm.strouhal(lc, prm["D"], 0.04 * chunk, skip=half)
+            st_w = mblbm.strouhal(lw, prm["D"], 0.04 * chunk, skip=half)
+            if st_c is not None and (st_w is None or abs(st_w / st_c - 1.0) > 0.01):
+                ok = False
         steps_c, steps_w = (nc + win) * chunk, (nw + win) * chunk
         res.append({"case": i, "Re": round(prm["Re"], 1), "D": round(prm["D"], 1), "cd": round(float(ref), 4),
+                    "st_cold": None if st_c is None else round(st_c, 4),
+                    "st_warm": None if st_w is None else round(st_w, 4),
                     "cold_steps": steps_c, "warm_steps": steps_w, "accepted": bool(ok),
                     "ms_cold": steps_c * tc[key], "ms_warm": steps_w * tw[key] if ok else steps_c * tc[key]})
     acc = [r for r in res if r["accepted"]]
@@ -493,6 +520,8 @@ def main():
                          "timetocd: Cd convergence of the 2-level case by precision; tgv: the 2-level periodic "
                          "Taylor-Green vortex by precision")
     ap.add_argument("--cases", type=int, default=256, help="cases of --workload batch256 / training cases of warmstart")
+    ap.add_argument("--cd-check", type=int, default=3,
+                    help="--workload batch256: cases per batch re-run alone to compare Cd with the batch")
     ap.add_argument("--eval", type=int, default=64, help="held-out cases of --workload warmstart")
     ap.add_argument("--snap-per-d", type=float, default=300.0, help="coarse steps per unit D before a training snapshot")
     ap.add_argument("--eval-per-d", type=float, default=900.0, help="coarse steps per unit D of a warm-start evaluation run")

@@ -425,15 +425,25 @@ int mb_batch_prepare(mb_batch *batch, int n_coarse);
 /* Cd and Cl of every case (n values each; either may be NULL), one
  * synchronisation for the whole batch. */
 int mb_batch_drag(mb_batch *batch, double *cd, double *cl, mb_stream stream);
-int mb_batch_stats(mb_batch *batch, long long *cell_updates_per_coarse_step, long long *kernels_last_call);
+/* Cell updates of one coarse step of all cases, launches of the last step
+ * call, and coarse steps taken through the batch so far (the autotuner's
+ * timing steps included). */
+int mb_batch_stats(mb_batch *batch, long long *cell_updates_per_coarse_step, long long *kernels_last_call,
+                   long long *coarse_steps_done);
 /* mb_set_interface_shape on every case of the batch. */
 int mb_batch_set_interface_shape(mb_batch *batch, int rec_points, int spline_segments);
-/* Autotuner: times each candidate interface shape (points per record CTA,
- * spline segments per CTA) over `steps` coarse steps and keeps the fastest;
- * reports the choice and its time per coarse step.  The timing steps advance
- * the cases. */
+/* Block-step schedule of the batch: 0 launches one CTA per tile of 256
+ * cells (cases in order); k = 1..8 (1..4 in FP64) launches a persistent grid
+ * of k CTAs per SM, each CTA taking an equal share of the tiles, in order.
+ * Results are identical. */
+int mb_batch_set_schedule(mb_batch *batch, int stb_ctas_per_sm);
+/* Autotuner: times the block-step schedules (0, 2, 4, 8 CTAs per SM), then
+ * with the fastest the interface shapes (points per record CTA, spline
+ * segments per CTA), each over `steps` coarse steps, and keeps the fastest;
+ * reports the choice and its time per coarse step (any pointer may be NULL).
+ * The timing steps advance the cases. */
 int mb_batch_autotune(mb_batch *batch, int steps, mb_stream stream, int *rec_points, int *spline_segments,
-                      double *ms_per_step);
+                      int *stb_ctas_per_sm, double *ms_per_step);
 
 /* ---- learned warm start (no reference counterpart) ----------------------- */
 /* A 4-level convolutional U-Net (3x3 convolutions with ReLU, 32, 64, 128,
@@ -451,6 +461,13 @@ int mb_unet_param_count(mb_unet *net, long long *count);
 /* which = 0: FP32 master weights; 1: gradients of the last train step. */
 int mb_unet_get_params(mb_unet *net, float *host, long long count, int which);
 int mb_unet_set_params(mb_unet *net, const float *host, long long count);
+/* 3x3 convolutions (forward and input gradient) on the tcgen05 tensor cores
+ * (kind 1, the default; layers whose shape does not fit fall back per layer)
+ * or on mma.sync (kind 0). */
+int mb_unet_set_gemm(mb_unet *net, int kind);
+/* MB_ERR_TIMEOUT (once) when a tcgen05 kernel's bounded wait ran out since
+ * the last call; synchronises the stream. */
+int mb_unet_status(mb_unet *net, mb_stream stream);
 /* d_in: [n][H][W][4], d_out: [n][H][W][3], FP32 device arrays. */
 int mb_unet_forward(mb_unet *net, const float *d_in, int n, float *d_out, mb_stream stream);
 /* Forward, masked squared error sum_p mask_p |y_p - t_p|^2 / (3 n H W)

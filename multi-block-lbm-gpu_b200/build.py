@@ -56,7 +56,9 @@ def build_lib(force=False, verbose_ptxas=False):
             cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-I/usr/local/cuda/include", "-c", s, "-o", o]
         _run(cmd)
         objs.append(o)
-    _run([NVCC, "-shared", "-o", LIB] + objs + ARCH + ["-lcudart"])
+    tmp = LIB + ".tmp"
+    _run([NVCC, "-shared", "-o", tmp] + objs + ARCH + ["-lcudart"])
+    os.replace(tmp, LIB)  # a reader never sees a half-written library
     return LIB
 
 

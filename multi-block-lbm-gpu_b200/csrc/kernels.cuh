@@ -1640,6 +1640,38 @@ __global__ void __launch_bounds__(256, P == MB_PREC_F64 ? 4 : 8) kb_block_step(c
   if (g < p.total) stb_at<P>(p, g);
 }
 
+// Persistent form of kb_block_step: a grid of G CTAs (a few per SM, all
+// resident), CTA b takes the tiles [T b / G, T (b + 1) / G) of the launch's
+// T tiles of 256 cells (cases in order, cta0 holding each case's first
+// tile), so the work is split evenly by cells and a CTA copies a case's
+// parameter block only when its range enters that case.
+template <int P>
+__global__ void __launch_bounds__(256, P == MB_PREC_F64 ? 4 : 8) kb_block_step_ps(const __grid_constant__ BatchArgs a) {
+  __shared__ __align__(16) unsigned char sp[(sizeof(StbParams) + 15) / 16 * 16];
+  const StbParams &p = *(const StbParams *)sp;
+  const long long T = __ldg(a.cta0 + a.ncases), G = gridDim.x;
+  const int t0 = (int)(T * blockIdx.x / G), t1 = (int)(T * (blockIdx.x + 1) / G);
+  int lo = 0, hi = a.ncases - 1;  // case of the first tile
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(a.cta0 + mid) <= t0) lo = mid; else hi = mid - 1;
+  }
+  int cur = -1;
+#pragma unroll 1
+  for (int t = t0; t < t1; t++) {
+    while (lo + 1 < a.ncases && __ldg(a.cta0 + lo + 1) <= t) lo++;
+    if (lo != cur) {
+      __syncthreads();  // every thread is done with the previous case's parameters
+      const int4 *src = (const int4 *)(a.params + (size_t)lo * a.pstride);
+      for (int q = threadIdx.x; q < (int)sizeof(sp) / 16; q += blockDim.x) ((int4 *)sp)[q] = __ldg(src + q);
+      __syncthreads();
+      cur = lo;
+    }
+    const long long g = (long long)(t - __ldg(a.cta0 + lo)) * 256 + threadIdx.x;
+    if (g < p.total) stb_at<P>(p, g);
+  }
+}
+
 template <int P>
 __global__ void __launch_bounds__(REC_THREADS) kb_records(const __grid_constant__ BatchArgs a) {
   __shared__ __align__(16) unsigned char sp[(sizeof(RecOpsParams) + 15) / 16 * 16];

@@ -298,6 +298,7 @@ template <int P> struct KDrag { static void *ptr() { return (void *)k_drag<P>; }
 template <int P> struct KL2 { static void *ptr() { return (void *)k_error_l2<P>; } };
 template <int P> struct KPrg { static void *ptr() { return (void *)k_program<P, false>; } };
 template <int P> struct KBStb { static void *ptr() { return (void *)kb_block_step<P>; } };
+template <int P> struct KBStbPs { static void *ptr() { return (void *)kb_block_step_ps<P>; } };
 template <int P> struct KBRec { static void *ptr() { return (void *)kb_records<P>; } };
 template <int P> struct KBSpl { static void *ptr() { return (void *)kb_spline<P>; } };
 template <int P> struct KPrgT { static void *ptr() { return (void *)k_program<P, true>; } };
@@ -2322,6 +2323,7 @@ struct BatchPlan {
   std::vector<SchedState> end;  // per case
   std::vector<void *> dev;
   long long kernels = 0;
+  bool uploaded = false;
   ~BatchPlan() {
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
@@ -2339,6 +2341,12 @@ struct mb_batch {
   long long kernels_last_call = 0;
   double *d_drag = nullptr;  // 2 per case
   double *h_drag = nullptr;  // pinned
+  // block-step schedule: 0 one CTA per tile of 256 cells (kb_block_step);
+  // k > 0 a persistent grid of k CTAs per SM over equal shares of the
+  // tiles (kb_block_step_ps)
+  int stb_ctas_per_sm = 0;
+  int num_sms = 148;
+  long long steps_done = 0;  // coarse steps of mb_batch_step calls (the autotuner's included)
 };
 
 namespace {
@@ -2386,7 +2394,7 @@ int batch_plan(mb_batch *b, int n, bool fin, BatchPlan **out) {
     size_t smem = 0;
     if (n0.kind == NK_STB) {
       psz = sizeof(StbParams);
-      func = kfunc<KBStb>(b->prec);
+      func = b->stb_ctas_per_sm > 0 ? kfunc<KBStbPs>(b->prec) : kfunc<KBStb>(b->prec);
       block = 256;
     } else if (n0.kind == NK_REC) {
       psz = sizeof(RecOpsParams);
@@ -2431,6 +2439,8 @@ int batch_plan(mb_batch *b, int n, bool fin, BatchPlan **out) {
     cudaKernelNodeParams kp{};
     kp.func = func;
     kp.gridDim = dim3((unsigned)ctas);
+    if (n0.kind == NK_STB && b->stb_ctas_per_sm > 0)
+      kp.gridDim = dim3((unsigned)std::min<long long>(ctas, (long long)b->num_sms * b->stb_ctas_per_sm));
     kp.blockDim = dim3(block);
     kp.sharedMemBytes = (unsigned)smem;
     kp.kernelParams = args;
@@ -2471,6 +2481,7 @@ extern "C" int mb_batch_create(mb_ctx *const *cases, int n, mb_batch **out) {
   if (!batch_in_step(b.get())) return MB_ERR_STATE;
   b->prec = cases[0]->prec;
   b->period = cases[0]->period;
+  b->num_sms = cases[0]->num_sms > 0 ? cases[0]->num_sms : 148;
   cudaDeviceSynchronize();
   for (mb_ctx *c : b->cases) {  // batched launches use one cell per thread and CUDA-graph plans
     bool clear = c->use_graph != 1;
@@ -2522,6 +2533,7 @@ extern "C" int mb_batch_step(mb_batch *b, int n, mb_stream stream) {
     b->kernels_last_call += bp->kernels;
     remaining -= chunk;
   }
+  b->steps_done += n;
   MB_CUDA(cudaGetLastError());
   return MB_OK;
 }
@@ -2535,6 +2547,8 @@ extern "C" int mb_batch_prepare(mb_batch *b, int n) {
   for (int c = 0; c < nc; c++) save[c] = b->cases[c]->state;
   int remaining = n, err = MB_OK;
   const int G = b->period;
+  cudaStream_t up = nullptr;
+  MB_CUDA(cudaStreamCreateWithFlags(&up, cudaStreamNonBlocking));
   while (remaining > 0 && !err) {
     int chunk;
     bool fin;
@@ -2543,11 +2557,17 @@ extern "C" int mb_batch_prepare(mb_batch *b, int n) {
     else { chunk = 1; fin = true; }
     BatchPlan *bp = nullptr;
     err = batch_plan(b, chunk, fin, &bp);
+    if (!err && !bp->uploaded) {  // the first replay then pays no upload
+      err = cudaGraphUpload(bp->exec, up) == cudaSuccess ? MB_OK : MB_ERR_CUDA;
+      bp->uploaded = true;
+    }
     if (!err)
       for (int c = 0; c < nc; c++) b->cases[c]->state = bp->end[c];
     remaining -= chunk;
   }
   for (int c = 0; c < nc; c++) b->cases[c]->state = save[c];
+  if (cudaStreamSynchronize(up) != cudaSuccess && !err) err = MB_ERR_CUDA;
+  cudaStreamDestroy(up);
   return err;
 }
 
@@ -2567,10 +2587,12 @@ extern "C" int mb_batch_drag(mb_batch *b, double *cd, double *cl, mb_stream stre
   return MB_OK;
 }
 
-extern "C" int mb_batch_stats(mb_batch *b, long long *updates_per_step, long long *kernels_last_call) {
+extern "C" int mb_batch_stats(mb_batch *b, long long *updates_per_step, long long *kernels_last_call,
+                              long long *coarse_steps_done) {
   if (!b) return MB_ERR_INVALID;
   if (updates_per_step) *updates_per_step = b->updates_per_step;
   if (kernels_last_call) *kernels_last_call = b->kernels_last_call;
+  if (coarse_steps_done) *coarse_steps_done = b->steps_done;
   return MB_OK;
 }
 
@@ -2585,40 +2607,69 @@ extern "C" int mb_batch_set_interface_shape(mb_batch *b, int rec_points, int spl
   return MB_OK;
 }
 
-// Times each candidate interface shape over `steps` coarse steps (after one
-// untimed chunk that builds its graphs) and keeps the fastest.  The timing
-// steps advance the cases.
+extern "C" int mb_batch_set_schedule(mb_batch *b, int stb_ctas_per_sm) {
+  if (!b || stb_ctas_per_sm < 0 || stb_ctas_per_sm > 8) return MB_ERR_INVALID;
+  if (b->prec == MB_PREC_F64 && stb_ctas_per_sm > 4) return MB_ERR_INVALID;  // launch bounds: 4 CTAs per SM
+  cudaDeviceSynchronize();
+  b->plans.clear();
+  b->stb_ctas_per_sm = stb_ctas_per_sm;
+  return MB_OK;
+}
+
+namespace {
+// Mean device time of one coarse step of the batch with its current shapes:
+// one untimed chunk (period + 1 steps) builds the graphs, then `steps` timed
+// steps.  Both advance the cases.
+int batch_time(mb_batch *b, int steps, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1, double *ms) {
+  if (int e = mb_batch_step(b, b->period + 1, s)) return e;
+  if (int e = mb_batch_prepare(b, steps)) return e;
+  MB_CUDA(cudaEventRecord(e0, s));
+  if (int e = mb_batch_step(b, steps, s)) return e;
+  MB_CUDA(cudaEventRecord(e1, s));
+  MB_CUDA(cudaEventSynchronize(e1));
+  float t = 0;
+  MB_CUDA(cudaEventElapsedTime(&t, e0, e1));
+  *ms = t / steps;
+  return MB_OK;
+}
+}  // namespace
+
+// Coordinate search: first the block-step schedule (one CTA per tile, or a
+// persistent grid of 2, 4 or 8 CTAs per SM over equal shares of the tiles)
+// with the default interface shape, then, with the best schedule, the
+// interface shapes (points per record CTA, spline segments per CTA).  Each
+// candidate is timed over `steps` coarse steps after one untimed chunk that
+// builds its graphs; the fastest is kept.  The timing steps advance the cases.
 extern "C" int mb_batch_autotune(mb_batch *b, int steps, mb_stream stream, int *rec_points, int *spline_segments,
-                                 double *ms_per_step) {
+                                 int *stb_ctas_per_sm, double *ms_per_step) {
   if (!b || steps < 1) return MB_ERR_INVALID;
   cudaStream_t s = (cudaStream_t)stream;
-  static const int cand[][2] = {{32, 1}, {64, 1}, {32, 2}, {64, 2}, {64, 4}};
-  double best = 1e30;
-  int br = 32, bs = 1;
+  static const int sched[] = {0, 2, 4, 8};
+  static const int cand[][2] = {{64, 1}, {32, 2}, {64, 2}, {64, 4}};
   cudaEvent_t e0, e1;
   MB_CUDA(cudaEventCreate(&e0));
   MB_CUDA(cudaEventCreate(&e1));
-  for (const auto &cd : cand) {
-    if (int e = mb_batch_set_interface_shape(b, cd[0], cd[1])) return e;
-    if (int e = mb_batch_step(b, b->period + 1, s)) return e;
-    if (int e = mb_batch_prepare(b, steps)) return e;
-    MB_CUDA(cudaEventRecord(e0, s));
-    if (int e = mb_batch_step(b, steps, s)) return e;
-    MB_CUDA(cudaEventRecord(e1, s));
-    MB_CUDA(cudaEventSynchronize(e1));
-    float ms = 0;
-    MB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    if (ms / steps < best) {
-      best = ms / steps;
-      br = cd[0];
-      bs = cd[1];
-    }
+  double best = 1e30, ms = 0;
+  int bk = 0, br = 32, bs = 1, err = MB_OK;
+  if ((err = mb_batch_set_interface_shape(b, 32, 1))) return err;
+  for (int k : sched) {
+    if (b->prec == MB_PREC_F64 && k > 4) continue;
+    if ((err = mb_batch_set_schedule(b, k)) || (err = batch_time(b, steps, s, e0, e1, &ms))) break;
+    if (ms < best) { best = ms; bk = k; }
+  }
+  if (!err) err = mb_batch_set_schedule(b, bk);
+  for (int q = 0; q < 4 && !err; q++) {
+    if ((err = mb_batch_set_interface_shape(b, cand[q][0], cand[q][1])) || (err = batch_time(b, steps, s, e0, e1, &ms)))
+      break;
+    if (ms < best) { best = ms; br = cand[q][0]; bs = cand[q][1]; }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  if (err) return err;
   if (int e = mb_batch_set_interface_shape(b, br, bs)) return e;
   if (rec_points) *rec_points = br;
   if (spline_segments) *spline_segments = bs;
+  if (stb_ctas_per_sm) *stb_ctas_per_sm = bk;
   if (ms_per_step) *ms_per_step = best;
   return MB_OK;
 }

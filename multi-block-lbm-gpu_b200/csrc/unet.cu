@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "../../include/mblbm.h"
+#include "unet_umma.cuh"
 
 #define UN_CUDA(call)                                                                          \
   do {                                                                                         \
@@ -475,6 +476,8 @@ struct ConvLayer {
 
 struct mb_unet {
   int H, W, maxN, C0;
+  int gemm = 0;                  // 3x3 convolutions: 1 tcgen05 (where the layer's shape fits), 0 mma.sync
+  unsigned int *d_err = nullptr; // error word of the tcgen05 kernels' bounded waits
   std::vector<ConvLayer> conv;  // 14 layers, in forward order
   long long head_w = 0, head_b = 0, nparam = 0;
   float *P = nullptr, *M = nullptr, *V = nullptr, *G = nullptr;  // params, Adam moments, gradients
@@ -517,10 +520,109 @@ uint64_t sm64(uint64_t &s) {
 
 long long npix(const mb_unet *n, int N, int level) { return (long long)N * (n->H >> level) * (n->W >> level); }
 
+// ---- tcgen05 path: tensor maps and launch --------------------------------
+using EncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                 const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiled encode_fn() {
+  static EncodeTiled fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (EncodeTiled)p;
+  }
+  return fn;
+}
+
+// Pixel tile, channel step and channel tile of a layer on the tcgen05 path;
+// false when the layer's shape does not fit it (the mma.sync kernel runs).
+struct UmmaShape {
+  int Cw, R, CH, NT;
+};
+bool umma_shape(int H, int W, int Cin, int Cout, UmmaShape *u) {
+  u->Cw = W >= umma::TM ? umma::TM : W;
+  if (u->Cw < 8 || umma::TM % u->Cw || W % u->Cw) return false;
+  u->R = umma::TM / u->Cw;
+  if (H % u->R) return false;
+  u->CH = Cin % 64 == 0 ? 64 : (Cin % 32 == 0 ? 32 : (Cin % 16 == 0 ? 16 : 0));
+  if (!u->CH) return false;
+  u->NT = Cout <= 256 ? Cout : (Cout % 2 == 0 && Cout / 2 <= 256 ? Cout / 2 : 0);
+  return u->NT >= 32 && u->NT % 16 == 0 && Cout % u->NT == 0;
+}
+
+// 3x3 convolution of X (view, Cin channels, N images of H x W) with weights
+// wt [Cout][9][Cin] on the tensor cores: BF16 output with bias and ReLU, or
+// FP32 output (accumulated when asked).  Returns MB_ERR_UNSUPPORTED when the
+// shape or the driver's tensor-map entry point rules it out.
+int conv_umma(mb_unet *n, View X, const bf16 *wt, const float *bias, View Y, int N, int H, int W, int Cin, int Cout,
+              bool out_f32, bool accumulate, cudaStream_t s) {
+  UmmaShape u;
+  EncodeTiled enc = encode_fn();
+  if (!enc || !umma_shape(H, W, Cin, Cout, &u)) return MB_ERR_UNSUPPORTED;
+  if ((X.co % 8) || (X.cs % 8) || (Y.co % 8) || (Y.cs % 8)) return MB_ERR_UNSUPPORTED;  // 16-byte alignment
+  const CUtensorMapSwizzle sw = u.CH == 64 ? CU_TENSOR_MAP_SWIZZLE_128B
+                                           : (u.CH == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B);
+  CUtensorMap xmap, wmap;
+  {
+    const cuuint64_t dims[4] = {(cuuint64_t)Cin, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)N};
+    const cuuint64_t strides[3] = {(cuuint64_t)X.cs * 2, (cuuint64_t)X.cs * 2 * W, (cuuint64_t)X.cs * 2 * W * H};
+    const cuuint32_t box[4] = {(cuuint32_t)u.CH, (cuuint32_t)u.Cw, (cuuint32_t)u.R, 1};
+    const cuuint32_t es[4] = {1, 1, 1, 1};
+    if (enc(&xmap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, (bf16 *)X.ptr + X.co, dims, strides, box, es,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return MB_ERR_CUDA;
+  }
+  {
+    const cuuint64_t dims[2] = {(cuuint64_t)9 * Cin, (cuuint64_t)Cout};
+    const cuuint64_t strides[1] = {(cuuint64_t)9 * Cin * 2};
+    const cuuint32_t box[2] = {(cuuint32_t)u.CH, (cuuint32_t)u.NT};
+    const cuuint32_t es[2] = {1, 1};
+    if (enc(&wmap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void *)wt, dims, strides, box, es,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return MB_ERR_CUDA;
+  }
+  umma::ConvArgs a{};
+  a.H = H;
+  a.W = W;
+  a.Cw = u.Cw;
+  a.R = u.R;
+  a.tiles_x = W / u.Cw;
+  a.tiles_y = H / u.R;
+  a.Cin = Cin;
+  a.NT = u.NT;
+  a.relu = out_f32 ? 0 : 1;
+  a.out_f32 = out_f32;
+  a.accumulate = accumulate;
+  a.bias = bias;
+  a.Y = Y.ptr;
+  a.ycs = Y.cs;
+  a.yco = Y.co;
+  a.Cout = Cout;
+  a.err = n->d_err;
+  const dim3 grid((unsigned)(a.tiles_x * a.tiles_y * N), (unsigned)(Cout / u.NT));
+  void *args[3] = {&xmap, &wmap, &a};
+  const void *fn = u.CH == 64 ? (const void *)umma::k_conv3x3_umma<64>
+                              : (u.CH == 32 ? (const void *)umma::k_conv3x3_umma<32> : (const void *)umma::k_conv3x3_umma<16>);
+  const size_t smem = u.CH == 64 ? umma::Cfg<64>::smem(u.NT) : (u.CH == 32 ? umma::Cfg<32>::smem(u.NT) : umma::Cfg<16>::smem(u.NT));
+  UN_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  UN_CUDA(cudaLaunchKernel(fn, grid, dim3(umma::THREADS), args, smem, s));
+  return MB_OK;
+}
+
 int conv_fwd(mb_unet *n, int li, View X, View Y, int N, cudaStream_t s) {
   const ConvLayer &L = n->conv[li];
   const int H = n->H >> L.level, W = n->W >> L.level;
   const long long NP = (long long)N * H * W;
+  if (n->gemm == 1) {
+    const int e = conv_umma(n, X, L.wb, n->P + L.b_off, Y, N, H, W, L.cin, L.cout, false, false, s);
+    if (e != MB_ERR_UNSUPPORTED) return e;
+  }
   dim3 grid((unsigned)((NP + 63) / 64), (unsigned)((L.cout + 63) / 64));
   k_conv3x3<false><<<grid, 128, 0, s>>>(X, L.wb, n->P + L.b_off, Y, (int)NP, H, W, L.cin, L.cout, 1, 0);
   UN_CUDA(cudaGetLastError());
@@ -539,9 +641,15 @@ int conv_bwd(mb_unet *n, int li, View X, const float *g, View gX, bool need_gx, 
   const int bt = 256 / L.cout * L.cout;
   k_bias_grad<<<grid_for(NP, 256), bt > 0 ? bt : L.cout, 0, s>>>(n->gbf, n->G + L.b_off, (int)NP, L.cout);
   if (need_gx) {
-    dim3 grid((unsigned)((NP + 63) / 64), (unsigned)((L.cin + 63) / 64));
     View gy{n->gbf, L.cout, 0};
-    k_conv3x3<true><<<grid, 128, 0, s>>>(gy, L.wt, nullptr, gX, (int)NP, H, W, L.cout, L.cin, 0, 1);
+    int e = MB_ERR_UNSUPPORTED;
+    if (n->gemm == 1) e = conv_umma(n, gy, L.wt, nullptr, gX, N, H, W, L.cout, L.cin, true, true, s);
+    if (e == MB_ERR_UNSUPPORTED) {
+      dim3 grid((unsigned)((NP + 63) / 64), (unsigned)((L.cin + 63) / 64));
+      k_conv3x3<true><<<grid, 128, 0, s>>>(gy, L.wt, nullptr, gX, (int)NP, H, W, L.cout, L.cin, 0, 1);
+    } else if (e) {
+      return e;
+    }
   }
   UN_CUDA(cudaGetLastError());
   return MB_OK;
@@ -724,6 +832,8 @@ extern "C" int mb_unet_create(int H, int W, int max_batch, unsigned long long se
   }
   if ((e = ualloc(n.get(), &n->gbf, maxg))) return e;
   if ((e = ualloc(n.get(), &n->d_loss, 1))) return e;
+  if ((e = ualloc(n.get(), &n->d_err, 1))) return e;
+  UN_CUDA(cudaMemset(n->d_err, 0, sizeof(unsigned int)));
   UN_CUDA(cudaMallocHost(&n->h_loss, sizeof(float)));
   if ((e = refresh_weights(n.get(), 0))) return e;
   UN_CUDA(cudaDeviceSynchronize());
@@ -758,6 +868,23 @@ extern "C" int mb_unet_set_params(mb_unet *n, const float *host, long long count
   if (int e = refresh_weights(n, 0)) return e;
   UN_CUDA(cudaDeviceSynchronize());
   return MB_OK;
+}
+
+extern "C" int mb_unet_set_gemm(mb_unet *n, int kind) {
+  if (!n || kind < 0 || kind > 1) return MB_ERR_INVALID;
+  n->gemm = kind;
+  return MB_OK;
+}
+
+extern "C" int mb_unet_status(mb_unet *n, mb_stream stream) {
+  if (!n) return MB_ERR_INVALID;
+  unsigned int h = 0;
+  cudaStream_t s = (cudaStream_t)stream;
+  UN_CUDA(cudaMemcpyAsync(&h, n->d_err, sizeof(h), cudaMemcpyDeviceToHost, s));
+  UN_CUDA(cudaStreamSynchronize(s));
+  if (!h) return MB_OK;
+  UN_CUDA(cudaMemset(n->d_err, 0, sizeof(unsigned int)));
+  return MB_ERR_TIMEOUT;
 }
 
 extern "C" int mb_unet_forward(mb_unet *n, const float *d_in, int N, float *d_out, mb_stream stream) {

@@ -169,10 +169,13 @@ SIGNATURES = {
     "mb_unet_get_params": ([_vp, _vp, C.c_longlong, C.c_int], C.c_int),
     "mb_unet_set_params": ([_vp, _vp, C.c_longlong], C.c_int),
     "mb_unet_forward": ([_vp, _vp, C.c_int, _vp, _vp], C.c_int),
+    "mb_unet_set_gemm": ([_vp, C.c_int], C.c_int),
+    "mb_unet_status": ([_vp, _vp], C.c_int),
     "mb_unet_train_step": ([_vp, _vp, _vp, _vp, C.c_int, C.c_float, C.c_int, C.POINTER(C.c_float), _vp], C.c_int),
-    "mb_batch_stats": ([_vp, _pll, _pll], C.c_int),
+    "mb_batch_stats": ([_vp, _pll, _pll, _pll], C.c_int),
     "mb_batch_set_interface_shape": ([_vp, C.c_int, C.c_int], C.c_int),
-    "mb_batch_autotune": ([_vp, C.c_int, _vp, _pi, _pi, _pd], C.c_int),
+    "mb_batch_autotune": ([_vp, C.c_int, _vp, _pi, _pi, _pi, _pd], C.c_int),
+    "mb_batch_set_schedule": ([_vp, C.c_int], C.c_int),
     "mb_set_program_trace": ([_vp, C.c_longlong], C.c_int),
     "mb_program_trace": ([_vp, _vp, C.c_longlong, C.POINTER(C.c_longlong)], C.c_int),
     "mb_program_selftest": ([_vp, C.c_int, _vp], C.c_int),
@@ -766,9 +769,9 @@ class Batch:
         return cd, cl
 
     def stats(self):
-        u, k = C.c_longlong(), C.c_longlong()
-        _check(self.lib.mb_batch_stats(self.h, C.byref(u), C.byref(k)), "mb_batch_stats")
-        return {"updates_per_step": u.value, "kernels_last_call": k.value}
+        u, k, n = C.c_longlong(), C.c_longlong(), C.c_longlong()
+        _check(self.lib.mb_batch_stats(self.h, C.byref(u), C.byref(k), C.byref(n)), "mb_batch_stats")
+        return {"updates_per_step": u.value, "kernels_last_call": k.value, "steps_done": n.value}
 
     def set_split_levels(self, level_mask):
         """Split exactly the levels of level_mask (bit per level) into interior and rim nodes (0: threshold)."""
@@ -778,11 +781,18 @@ class Batch:
         _check(self.lib.mb_batch_set_interface_shape(self.h, int(rec_points), int(spline_segments)),
                "mb_batch_set_interface_shape")
 
+    def set_schedule(self, stb_ctas_per_sm):
+        """Block-step schedule: 0 one CTA per 256-cell tile; k > 0 a persistent
+        grid of k CTAs per SM over equal shares of the tiles."""
+        _check(self.lib.mb_batch_set_schedule(self.h, int(stb_ctas_per_sm)), "mb_batch_set_schedule")
+
     def autotune(self, steps=12, stream=None):
-        r, sg, ms = C.c_int(), C.c_int(), C.c_double()
-        _check(self.lib.mb_batch_autotune(self.h, int(steps), _stream_ptr(stream), C.byref(r), C.byref(sg), C.byref(ms)),
-               "mb_batch_autotune")
-        return {"rec_points": r.value, "spline_segments": sg.value, "ms_per_step": ms.value}
+        """Times the block-step schedules, then the interface shapes; keeps the fastest."""
+        r, sg, k, ms = C.c_int(), C.c_int(), C.c_int(), C.c_double()
+        _check(self.lib.mb_batch_autotune(self.h, int(steps), _stream_ptr(stream), C.byref(r), C.byref(sg), C.byref(k),
+                                          C.byref(ms)), "mb_batch_autotune")
+        return {"rec_points": r.value, "spline_segments": sg.value, "stb_ctas_per_sm": k.value,
+                "ms_per_step": ms.value}
 
 
 # ---------------------------------------------------------------------------
@@ -855,6 +865,14 @@ class UNet:
     def set_params(self, p):
         p = np.ascontiguousarray(p, dtype=np.float32)
         _check(self.lib.mb_unet_set_params(self.h, p.ctypes.data_as(_vp), self.nparam), "mb_unet_set_params")
+
+    def set_gemm(self, kind):
+        """3x3 convolutions on the tcgen05 tensor cores (1, default) or on mma.sync (0)."""
+        _check(self.lib.mb_unet_set_gemm(self.h, int(kind)), "mb_unet_set_gemm")
+
+    def status(self, stream=None):
+        """Raises MBError(MB_ERR_TIMEOUT) if a tcgen05 kernel's bounded wait ran out."""
+        _check(self.lib.mb_unet_status(self.h, _stream_ptr(stream)), "mb_unet_status")
 
     def forward(self, x, out, stream=None):
         _check(self.lib.mb_unet_forward(self.h, _vp(x.data_ptr()), x.shape[0], _vp(out.data_ptr()), _stream_ptr(stream)),

@@ -177,10 +177,10 @@ def generate(case_ids, steps_per_d, precision="f32", h=H, w=W, stream=None, d_ra
 
 
 def drag_series(case_ids, steps_per_d, precision, chunk=50, net=None, d_range=(10.0, 40.0), stream=None):
-    """Cd every `chunk` coarse steps of each case, cold-started (net None) or
-    warm-started from the surrogate, batched by level count and D bin.
-    Returns {id: (series, params)} and the device time per coarse step of
-    each batch {(levels, steps): ms}."""
+    """Cd and Cl every `chunk` coarse steps of each case, cold-started (net
+    None) or warm-started from the surrogate, batched by level count and D
+    bin.  Returns {id: (cd series, params, batch key, cl series)} and the
+    device time per coarse step of each batch {(levels, steps): ms}."""
     import torch
 
     out, times = {}, {}
@@ -199,19 +199,20 @@ def drag_series(case_ids, steps_per_d, precision, chunk=50, net=None, d_range=(1
         b = Batch(sims)
         b.prepare(chunk)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        ms, cds = 0.0, []
+        ms, cds, cls = 0.0, [], []
         for _ in range(steps // chunk):
             e0.record()
             b.evolution(chunk, stream)
             e1.record()
-            cd, _ = b.drag(stream)
+            cd, cl = b.drag(stream)
             ms += e0.elapsed_time(e1)
             cds.append(cd)
+            cls.append(cl)
         b.close()
         times[key] = ms / max(1, (steps // chunk) * chunk)
-        cds = np.array(cds)
+        cds, cls = np.array(cds), np.array(cls)
         for k, (i, g, prm) in enumerate(items):
-            out[i] = (cds[:, k], prm, key)
+            out[i] = (cds[:, k], prm, key, cls[:, k])
         for s in sims:
             s.close()
     return out, times

@@ -47,9 +47,10 @@ def test_batch_autotune_keeps_results(mb, cuda_device):
     batch = mb.Batch(sims)
     choice = batch.autotune(steps=3)
     assert choice["rec_points"] in (32, 64) and 1 <= choice["spline_segments"] <= 4 and choice["ms_per_step"] > 0
+    assert choice["stb_ctas_per_sm"] in (0, 2, 4, 8)
     batch.evolution(5)
-    # 5 candidates x (one untimed chunk of period + 1 = 7 steps, then 3 timed), then 5 more
-    steps_done = 5 * (7 + 3) + 5
+    # 4 schedules + 4 interface shapes, each (one untimed chunk of period + 1 = 7 steps, then 3 timed), then 5 more
+    steps_done = 8 * (7 + 3) + 5
     for g, a, s in zip(geos, alone, sims):
         a.evolution(steps_done)
         assert_same(g, s, a)
@@ -65,4 +66,58 @@ def test_batch_rejects_diverged_state(mb, cuda_device):
     sims[0].evolution(1)
     with pytest.raises(mb.MBError):
         batch.evolution(1)
+    batch.close()
+
+
+@pytest.mark.parametrize("sched", [1, 2, 4, 8])
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_batch_persistent_schedule_bitwise(mb, cuda_device, prec, sched):
+    """The persistent block-step schedule (k CTAs per SM over equal shares of
+    the 256-cell tiles of all cases) gives the state of one CTA per tile."""
+    if prec == "f64" and sched > 4:
+        pytest.skip("FP64 block steps run at most 4 CTAs per SM")
+    geos = cases(mb, range(6), 3, d_range=(10.0, 30.0))
+    a = [mb.MultiBlockLBM(g, prec) for g in geos]
+    b = [mb.MultiBlockLBM(g, prec) for g in geos]
+    for s in a + b:
+        s.init()
+    ba, bb = mb.Batch(a), mb.Batch(b)
+    bb.set_schedule(sched)
+    ba.evolution(9)
+    bb.evolution(9)
+    for g, x, y in zip(geos, a, b):
+        assert_same(g, x, y)
+    ba.close()
+    bb.close()
+
+
+@pytest.mark.parametrize("levels", [2, 3])
+def test_batch_f64_matches_oracle_full_ranges(mb, orc, cuda_device, levels):
+    """FP64 batches of the batched workload's cases over its full ranges
+    (D in [10, 40], Re in [20, 200], ellipses of aspect 1-3 at any angle)
+    against the FP64 C oracle, every field after 12 coarse steps and the
+    drag."""
+    ids = [3, 17, 42] if levels == 2 else [5, 23]
+    drawn = [mb.batch_case(i, levels=levels) for i in ids]
+    geos = [g for g, _ in drawn]
+    assert max(p["D"] for _, p in drawn) > 25 and min(p["Re"] for _, p in drawn) < 150
+    sims = [mb.MultiBlockLBM(g, "f64") for g in geos]
+    for s in sims:
+        s.init()
+    batch = mb.Batch(sims)
+    batch.set_schedule(4)
+    batch.set_interface_shape(64, 2)
+    n = 0
+    batch.evolution(12)
+    cd, _ = batch.drag()
+    for g, s, c in zip(geos, sims, cd):
+        o = orc.Oracle(g)
+        o.init()
+        o.evolution(n + 12)
+        for k in range(g.layout.number_area):
+            fo, fm = o.fields(k), s.fields(k)
+            for key in ("rho", "ux", "uy", "F"):
+                np.testing.assert_allclose(fm[key], fo[key], rtol=0, atol=1e-12, err_msg=f"block {k} {key}")
+        assert c == pytest.approx(o.getDrag_block()[2], rel=1e-10)
+        o.close()
     batch.close()

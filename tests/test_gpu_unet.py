@@ -84,3 +84,36 @@ def test_unet_training_lowers_loss(mb, cuda_device):
         last = net.train_step(ti, tt, tm, lr=1e-3)
     assert last < 0.25 * first
     net.close()
+
+
+def test_tcgen05_convolutions_match_mma_sync(mb, cuda_device):
+    """At 64 x 128 every 3x3 layer (forward and input gradient) fits the
+    tcgen05 kernel (128-pixel tiles down to 8 x 16 at the deepest level):
+    its forward output, loss and every layer's gradients equal the mma.sync
+    kernels' up to the BF16 roundings that FP32 summation order flips."""
+    import torch
+    N, H, W = 2, 64, 128
+    inp, target, mask = data(N, H, W, 5)
+    ti, tt, tm = (torch.from_numpy(a).cuda() for a in (inp, target, mask))
+    res = {}
+    for kind in (0, 1):
+        net = mb.UNet(H, W, max_batch=N, seed=11)
+        net.set_gemm(kind)
+        out = torch.zeros((N, H, W, 3), device="cuda")
+        net.forward(ti, out)
+        loss = net.train_step(ti, tt, tm, lr=0.0, apply=False)
+        net.status()
+        res[kind] = (out.cpu().numpy(), loss, net.params(grads=True))
+        net.close()
+    (o0, l0, g0), (o1, l1, g1) = res[0], res[1]
+    assert np.isfinite(o1).all() and np.isfinite(g1).all()
+    assert np.linalg.norm(o1 - o0) <= 3e-3 * np.linalg.norm(o0)
+    assert l1 == pytest.approx(l0, rel=3e-3)
+    off, errs = 0, []
+    for i, (cin, cout, _) in enumerate(unet_ref.LAYERS):
+        n = cout * 9 * cin
+        a, b = g1[off:off + n], g0[off:off + n]
+        errs.append(float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)))
+        off += n + cout
+    print("tcgen05 vs mma.sync weight-gradient differences", errs)
+    assert max(errs) < 5e-2, errs
