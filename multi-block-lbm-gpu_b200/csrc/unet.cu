@@ -16,6 +16,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
+#include <algorithm>
 #include <cstring>
 #include <memory>
 #include <vector>
@@ -554,6 +555,64 @@ bool umma_shape(int H, int W, int Cin, int Cout, UmmaShape *u) {
   return u->NT >= 32 && u->NT % 16 == 0 && Cout % u->NT == 0;
 }
 
+// Weight gradient of a 3x3 layer on the tensor cores (umma::k_wgrad_umma):
+// dW [Cout][9][Cin] += sum_p dY[p][co] X[p + off_t][ci].  MB_ERR_UNSUPPORTED
+// when the shape does not fit (fewer than 64 channels on either side, or
+// images that do not split into 64-pixel boxes).
+int wgrad_umma(mb_unet *n, View X, const bf16 *dY, float *dW, int N, int H, int W, int Cin, int Cout,
+               cudaStream_t s) {
+  EncodeTiled enc = encode_fn();
+  if (!enc || Cin < 64 || Cin % 64 || Cout < 64 || (X.co % 8) || (X.cs % 8)) return MB_ERR_UNSUPPORTED;
+  const int Cw = W >= umma::WG_KP ? umma::WG_KP : W;
+  if (Cw < 8 || umma::WG_KP % Cw || W % Cw) return MB_ERR_UNSUPPORTED;
+  const int R = umma::WG_KP / Cw;
+  if (H % R) return MB_ERR_UNSUPPORTED;
+  const int NT = Cin <= 256 ? Cin : (Cin % 128 == 0 && Cin / 2 <= 256 ? Cin / 2 : 0);
+  if (!NT || NT % 64) return MB_ERR_UNSUPPORTED;
+  CUtensorMap gmap, xmap;
+  const cuuint32_t box[4] = {64, (cuuint32_t)Cw, (cuuint32_t)R, 1};
+  const cuuint32_t es[4] = {1, 1, 1, 1};
+  {
+    const cuuint64_t dims[4] = {(cuuint64_t)Cout, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)N};
+    const cuuint64_t st[3] = {(cuuint64_t)Cout * 2, (cuuint64_t)Cout * 2 * W, (cuuint64_t)Cout * 2 * W * H};
+    if (enc(&gmap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, (void *)dY, dims, st, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return MB_ERR_CUDA;
+  }
+  {
+    const cuuint64_t dims[4] = {(cuuint64_t)Cin, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)N};
+    const cuuint64_t st[3] = {(cuuint64_t)X.cs * 2, (cuuint64_t)X.cs * 2 * W, (cuuint64_t)X.cs * 2 * W * H};
+    if (enc(&xmap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, (bf16 *)X.ptr + X.co, dims, st, box, es,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return MB_ERR_CUDA;
+  }
+  umma::WgradArgs a{};
+  a.H = H;
+  a.W = W;
+  a.Cw = Cw;
+  a.R = R;
+  a.bx = W / Cw;
+  a.by = H / R;
+  a.nboxes = a.bx * a.by * N;
+  const int mt = (Cout + umma::TM - 1) / umma::TM, nt = Cin / NT;
+  // split-K: about two CTAs per SM over (pixel runs x channel tiles x taps)
+  const long long want = std::max<long long>(1, (long long)a.nboxes * 9 * mt * nt / (148 * 2));
+  a.boxes_per_cta = (int)std::min<long long>(128, std::max<long long>(4, want));
+  a.Cin = Cin;
+  a.Cout = Cout;
+  a.NT = NT;
+  a.dW = dW;
+  a.err = n->d_err;
+  const dim3 grid((unsigned)((a.nboxes + a.boxes_per_cta - 1) / a.boxes_per_cta), (unsigned)mt, (unsigned)(9 * nt));
+  const size_t smem = umma::wgrad_smem(NT);
+  UN_CUDA(cudaFuncSetAttribute((const void *)umma::k_wgrad_umma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  void *args[3] = {&gmap, &xmap, &a};
+  UN_CUDA(cudaLaunchKernel((const void *)umma::k_wgrad_umma, grid, dim3(umma::THREADS), args, smem, s));
+  return MB_OK;
+}
+
 // 3x3 convolution of X (view, Cin channels, N images of H x W) with weights
 // wt [Cout][9][Cin] on the tensor cores: BF16 output with bias and ReLU, or
 // FP32 output (accumulated when asked).  Returns MB_ERR_UNSUPPORTED when the
@@ -636,8 +695,15 @@ int conv_bwd(mb_unet *n, int li, View X, const float *g, View gX, bool need_gx, 
   const int H = n->H >> L.level, W = n->W >> L.level;
   const long long NP = (long long)N * H * W;
   k_relu_grad<<<grid_for(NP * L.cout), 256, 0, s>>>(g, n->act[li], n->gbf, NP * L.cout);
-  dim3 wg((unsigned)((NP + WG_CHUNK - 1) / WG_CHUNK), (unsigned)(9 * ((L.cin + 63) / 64)), (unsigned)((L.cout + 63) / 64));
-  k_conv3x3_wgrad<<<wg, 128, 0, s>>>(X, n->gbf, n->G + L.w_off, (int)NP, H, W, L.cin, L.cout);
+  int ew = MB_ERR_UNSUPPORTED;
+  if (n->gemm == 1) ew = wgrad_umma(n, X, n->gbf, n->G + L.w_off, N, H, W, L.cin, L.cout, s);
+  if (ew == MB_ERR_UNSUPPORTED) {
+    dim3 wg((unsigned)((NP + WG_CHUNK - 1) / WG_CHUNK), (unsigned)(9 * ((L.cin + 63) / 64)),
+            (unsigned)((L.cout + 63) / 64));
+    k_conv3x3_wgrad<<<wg, 128, 0, s>>>(X, n->gbf, n->G + L.w_off, (int)NP, H, W, L.cin, L.cout);
+  } else if (ew) {
+    return ew;
+  }
   const int bt = 256 / L.cout * L.cout;
   k_bias_grad<<<grid_for(NP, 256), bt > 0 ? bt : L.cout, 0, s>>>(n->gbf, n->G + L.b_off, (int)NP, L.cout);
   if (need_gx) {

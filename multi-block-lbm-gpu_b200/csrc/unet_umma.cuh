@@ -295,4 +295,137 @@ __global__ void __launch_bounds__(THREADS, 1)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Weight gradient: dW[co][t][ci] += sum over pixels p of dY[p][co] * X[p + off_t][ci]
+// as a GEMM with M = 128 output channels (co), N = NT input channels (ci),
+// K = pixels.  Both operands keep the channels contiguous in memory, so both
+// are MN-major tiles: a stage holds 64 pixels (a box of R rows x Cw columns
+// of one image) of 64-channel chunks, each chunk 64 rows (pixels) of 128
+// bytes with the 128-byte swizzle, chunks 8 KB apart (the descriptor's
+// leading byte offset), 8-row groups 1 KB apart (its stride byte offset).
+// A CTA reduces one tap over a contiguous run of pixel boxes and adds its
+// 128 x NT partial sums to dW with FP32 atomics.  Channels beyond Cout read
+// as zeros (the TMA fills them) and are not written.
+// ---------------------------------------------------------------------------
+constexpr int WG_KP = 64;  // pixels per stage
+struct WgradArgs {
+  int H, W, Cw, R;       // image size; pixel box Cw columns x R rows (64 pixels)
+  int bx, by;            // boxes per row block, per image
+  int nboxes;            // boxes of the whole batch
+  int boxes_per_cta;     // split-K: boxes of one CTA
+  int Cin, Cout, NT;     // NT: input channels of this launch's tiles (a multiple of 64)
+  float *dW;             // [Cout][9][Cin]
+  unsigned int *err;
+};
+
+__host__ __device__ constexpr uint32_t instr_desc_mn(int n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) | ((uint32_t)(n >> 3) << 17) |
+         ((uint32_t)(TM >> 4) << 24);
+}
+__device__ __forceinline__ uint64_t smem_desc_mn(unsigned saddr) {
+  uint64_t d = (uint64_t)((saddr & 0x3FFFFu) >> 4);
+  d |= (uint64_t)(8192u >> 4) << 16;  // leading byte offset: next 64-channel chunk
+  d |= (uint64_t)(1024u >> 4) << 32;  // stride byte offset: next 8 pixels
+  d |= (uint64_t)1u << 46;
+  d |= (uint64_t)2u << 61;            // 128-byte swizzle
+  return d;
+}
+inline size_t wgrad_smem(int nt) { return 1024 + (size_t)STAGES * (2 * 8192 + (size_t)(nt / 64) * 8192) + 256; }
+
+__global__ void __launch_bounds__(THREADS, 1)
+    k_wgrad_umma(const __grid_constant__ CUtensorMap gmap, const __grid_constant__ CUtensorMap xmap,
+                 const __grid_constant__ WgradArgs a) {
+  extern __shared__ __align__(1024) unsigned char dyn[];
+  unsigned char *base = (unsigned char *)(((uintptr_t)dyn + 1023) & ~(uintptr_t)1023);
+  const int nch = a.NT / 64;
+  const int ABYTES = 2 * 8192, BBYTES = nch * 8192;
+  unsigned char *sA = base;
+  unsigned char *sB = base + STAGES * ABYTES;
+  uint64_t *full = (uint64_t *)(sB + STAGES * BBYTES);
+  uint64_t *empty = full + STAGES;
+  uint64_t *done = empty + STAGES;
+  uint32_t *tslot = (uint32_t *)(done + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int ncols = a.NT <= 64 ? 64 : (a.NT <= 128 ? 128 : 256);
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                 "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 32) {
+    for (int s = 0; s < STAGES; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(done, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tslot;
+
+  const int co0 = blockIdx.y * TM;
+  const int tap = blockIdx.z % 9, ci0 = (blockIdx.z / 9) * a.NT;
+  const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+  const int b0 = blockIdx.x * a.boxes_per_cta;
+  const int b1 = min(a.nboxes, b0 + a.boxes_per_cta);
+  const int KIT = b1 - b0;
+  bool ok = true;
+  if (warp == 0 && lane == 0) {  // TMA producer
+    const unsigned bytes = (unsigned)(ABYTES + BBYTES);
+    for (int it = 0; it < KIT && ok; it++) {
+      const int s = it % STAGES;
+      if (it >= STAGES && !mbar_wait(&empty[s], ((it / STAGES) - 1) & 1)) { ok = false; break; }
+      int b = b0 + it;
+      const int bxi = b % a.bx;
+      b /= a.bx;
+      const int byi = b % a.by, img = b / a.by;
+      const int x0 = bxi * a.Cw, y0 = byi * a.R;
+      mbar_expect_tx(&full[s], bytes);
+      tma_load_4d(sA + s * ABYTES, &gmap, co0, x0, y0, img, &full[s]);
+      tma_load_4d(sA + s * ABYTES + 8192, &gmap, co0 + 64, x0, y0, img, &full[s]);
+      for (int c = 0; c < nch; c++)
+        tma_load_4d(sB + s * BBYTES + c * 8192, &xmap, ci0 + 64 * c, x0 + dx, y0 + dy, img, &full[s]);
+    }
+  } else if (warp == 1 && lane == 0) {  // MMA issuer
+    const uint32_t idesc = instr_desc_mn(a.NT);
+    for (int it = 0; it < KIT && ok; it++) {
+      const int s = it % STAGES;
+      if (!mbar_wait(&full[s], (it / STAGES) & 1)) { ok = false; break; }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const unsigned aa = smem_u32(sA + s * ABYTES), ba = smem_u32(sB + s * BBYTES);
+#pragma unroll
+      for (int k = 0; k < WG_KP / 16; k++)  // 16 pixels per MMA: 16 rows of 128 bytes further
+        mma_f16(tmem, smem_desc_mn(aa + k * 2048), smem_desc_mn(ba + k * 2048), idesc, (it > 0 || k > 0) ? 1u : 0u);
+      mma_commit(&empty[s]);
+    }
+    mma_commit(done);
+  }
+  if (!ok) atomicExch(a.err, 1u);
+  __syncwarp();
+  const bool acc_ready = KIT > 0 && mbar_wait(done, 0);
+  if (KIT > 0 && !acc_ready) atomicExch(a.err, 1u);
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (acc_ready) {
+    const int co = co0 + warp * 32 + lane;  // row of this thread
+    for (int c = 0; c < a.NT; c += 16) {
+      float v[16];
+      tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
+      if (co >= a.Cout) continue;
+      float *d = a.dW + ((long long)co * 9 + tap) * a.Cin + ci0 + c;
+#pragma unroll
+      for (int q = 0; q < 16; q++)
+        if (ci0 + c + q < a.Cin) atomicAdd(d + q, v[q]);
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
+  }
+}
+
 }  // namespace umma
