@@ -1,0 +1,124 @@
+"""The product path against the reference's own CUDA build at the stated step
+count of the 2-level cylinder (400 x 160 coarse, fine box [60,140]x[40,120],
+D = 20, Re = 40, U0 = 0.05): 20,000 coarse steps from rest.
+
+tests/golden/c1_20000.npz holds the reference's output of that run on a
+B200 (oracle/ref_harness/make_golden.py --long c1 20000: its kernels,
+geo_init, evolution, error_L2 and getDrag_block compiled unmodified): the
+final rho, ux, uy of every block and the drag and error_L2 series every 20
+steps.  Every C-F line of this layout has Nc = 81, so none of the
+reference's own launch races applies and its result is well defined.
+
+Bounds (relative L2 over all blocks, weight 1/m per block, as error_L2):
+  FP64 storage            u, rho <= 1e-9,  Cd <= 1e-9
+  FP32 storage of f - w   u, rho <= 1e-5,  Cd <= 1e-4  (and the same against FP64)
+  16-bit storage          Cd within 0.5 %  (u, rho reported)
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+import make_ref
+
+pytestmark = pytest.mark.gpu
+
+STEPS = 20000
+FIXTURE = os.path.join(GOLDEN, f"c1_{STEPS}.npz")
+
+
+def _rel_l2(geo, ref, got, key):
+    num = den = 0.0
+    for a in range(geo.layout.number_area):
+        m = geo.Areas[a].m
+        if key == "u":
+            for k in ("ux", "uy"):
+                num += np.sum((ref[f"{k}_{a}"] - got[a][k]) ** 2) / m
+                den += np.sum(ref[f"{k}_{a}"] ** 2) / m
+        else:
+            num += np.sum((ref[f"{key}_{a}"] - got[a][key]) ** 2) / m
+            den += np.sum(ref[f"{key}_{a}"] ** 2) / m
+    return float(np.sqrt(num / den))
+
+
+@pytest.fixture(scope="module")
+def runs(mb, cuda_device):
+    z = np.load(FIXTURE)
+    L, cfg, _ = make_ref.case("c1")
+    g = mb.geo_init(L, cfg)
+    out = {}
+    for prec in ("f64", "f32", "f16c", "f16s"):
+        s = mb.MultiBlockLBM(g, prec)
+        s.init()
+        cd, cl, err = s.evolution_diag(STEPS)
+        fields = [s.macros(a) for a in range(g.layout.number_area)]
+        out[prec] = (cd, cl, err, fields)
+        s.close()
+    return g, z, out
+
+
+def _ref_cd(g, z):
+    c = g.config
+    norm = c.rho0 * (c.U0[0] ** 2 + c.U0[1] ** 2) * g.Areas[c.drag_area if c.drag_area >= 0 else
+                                                             g.layout.number_area - 1].m * c.R
+    return z["drag"][:, 0] / norm, z["drag"][:, 1] / norm
+
+
+def test_fixture_is_the_stated_run(runs):
+    g, z, _ = runs
+    assert int(z["steps"]) == STEPS
+    assert int(z["sample_steps"][-1]) == STEPS
+    for a in range(g.layout.number_area):
+        assert z[f"rho_{a}"].shape == (g.Areas[a].ny, g.Areas[a].nx)
+
+
+def test_cell_types_equal_the_reference(runs):
+    g, z, out = runs
+    for a in range(g.layout.number_area):
+        assert np.array_equal(out["f64"][3][a]["solid"], z[f"solid_{a}"].astype(np.int32)), a
+
+
+@pytest.mark.parametrize("prec,tol_f,tol_cd", [("f64", 1e-9, 1e-9), ("f32", 1e-5, 1e-4)])
+def test_fields_and_drag_match_reference(runs, prec, tol_f, tol_cd):
+    g, z, out = runs
+    cd, cl, _, fields = out[prec]
+    eu, er = _rel_l2(g, z, fields, "u"), _rel_l2(g, z, fields, "rho")
+    cd_ref, cl_ref = _ref_cd(g, z)
+    idx = z["sample_steps"] - 1
+    dcd = float(np.max(np.abs(cd[idx] / cd_ref - 1.0)))
+    print(f"{prec} after {STEPS} steps: relL2 u {eu:.3e} rho {er:.3e}; max rel Cd diff over the series {dcd:.3e}; "
+          f"Cd {cd[-1]:.8f} (reference {cd_ref[-1]:.8f})")
+    assert eu <= tol_f and er <= tol_f
+    assert abs(cd[-1] / cd_ref[-1] - 1.0) <= tol_cd
+    assert dcd <= 10 * tol_cd  # the transient, too
+    assert np.max(np.abs(cl[idx] - cl_ref)) <= tol_cd * abs(cd_ref[-1]) * 10
+
+
+def test_f64_error_l2_series_matches_reference(runs):
+    """error_L2.dat holds %g values (6 significant digits)."""
+    g, z, out = runs
+    err = out["f64"][2]
+    idx = z["sample_steps"] - 1
+    np.testing.assert_allclose(err[idx], z["l2"], rtol=1e-4, atol=0)
+
+
+def test_f32_matches_f64(runs):
+    g, z, out = runs
+    ref = {f"{k}_{a}": out["f64"][3][a][k] for a in range(g.layout.number_area) for k in ("rho", "ux", "uy")}
+    eu, er = _rel_l2(g, ref, out["f32"][3], "u"), _rel_l2(g, ref, out["f32"][3], "rho")
+    assert eu <= 1e-5 and er <= 1e-5
+    assert abs(out["f32"][0][-1] / out["f64"][0][-1] - 1.0) <= 1e-4
+
+
+@pytest.mark.parametrize("prec", ["f16c", "f16s"])
+def test_16bit_storage_cd_within_half_percent(runs, prec):
+    g, z, out = runs
+    cd, _, _, fields = out[prec]
+    cd_ref, _ = _ref_cd(g, z)
+    eu, er = _rel_l2(g, z, fields, "u"), _rel_l2(g, z, fields, "rho")
+    print(f"{prec}: Cd {cd[-1]:.6f} vs reference {cd_ref[-1]:.6f} ({cd[-1] / cd_ref[-1] - 1:+.3e}); "
+          f"relL2 u {eu:.3e} rho {er:.3e}")
+    assert np.all(np.isfinite(cd))
+    assert abs(cd[-1] / cd_ref[-1] - 1.0) <= 5e-3
