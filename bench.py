@@ -413,6 +413,8 @@ def run_forces(args):
 
     torch.cuda.set_device(0)
     geo = mblbm.config2_geometry()
+    if args.spinup > 0:
+        return run_forces_developed(args, geo)
     sim = mblbm.MultiBlockLBM(geo, args.precision)
     sim.init()
     cd, cl = [], []
@@ -441,6 +443,55 @@ def run_forces(args):
     if args.save:
         np.save(os.path.join(args.save, f"forces_{args.precision}.npy"), np.stack([cd, cl]))
     sim.close()
+    return 0
+
+
+def run_forces_developed(args, geo):
+    """The storage precisions on developed shedding: FP64 storage runs
+    --spinup coarse steps from rest (past the onset of shedding, which the
+    symmetric start delays by tens of thousands of steps), then its fields
+    (rho, u, F of every block) seed one context per precision, whose ring
+    slots and u_prev are rebuilt from them (mb_sync_history); each runs
+    --steps more coarse steps with Cd and Cl every step.  Mean Cd, rms Cl and
+    St over those steps, and their relative differences to FP64's."""
+    import numpy as np
+    import mblbm
+
+    base = mblbm.MultiBlockLBM(geo, "f64")
+    base.init()
+    for q in range(0, args.spinup, 5000):
+        base.evolution_diag(min(5000, args.spinup - q))
+    state = [base.fields(a) for a in range(geo.layout.number_area)]
+    base.close()
+    c = geo.config
+    D, U0 = 2.0 * c.R, c.U0[0]
+    out = {}
+    for prec in ("f64", "f32", "f16s", "f16c"):
+        sim = mblbm.MultiBlockLBM(geo, prec)
+        sim.init()
+        for a, f in enumerate(state):
+            sim.set_fields(a, f["rho"], f["ux"], f["uy"], f["F"])
+        sim.sync_history()
+        cd, cl = [], []
+        for q in range(0, args.steps, 5000):
+            x, y, _ = sim.evolution_diag(min(5000, args.steps - q))
+            cd.append(x)
+            cl.append(y)
+        sim.close()
+        cd, cl = np.concatenate(cd), np.concatenate(cl)
+        st = mblbm.strouhal(cl, D, U0)
+        out[prec] = {"mean_cd": float(cd.mean()), "rms_cl": float(np.sqrt(np.mean(cl ** 2))),
+                     "strouhal": None if st is None else float(st)}
+        if args.save:
+            np.save(os.path.join(args.save, f"forces_dev_{prec}.npy"), np.stack([cd, cl]))
+    for prec in ("f32", "f16s", "f16c"):
+        for k in ("mean_cd", "rms_cl", "strouhal"):
+            a, b = out[prec][k], out["f64"][k]
+            out[prec][k + "_rel_f64"] = None if a is None or b is None else a / b - 1.0
+    line = {"metric": "mean Cd, rms Cl, Strouhal number on developed shedding, by storage precision",
+            "unit": "dimensionless", "n_gpus": 1, "steps": args.steps, "spinup_f64": args.spinup,
+            "data": "synthetic", "config": {"workload": WORKLOAD}, "by_precision": out}
+    print(json.dumps(line), flush=True)
     return 0
 
 
@@ -528,6 +579,9 @@ def main():
     ap.add_argument("--warm-precision", default="f16s", choices=["f16s", "f16c", "f32"], help="solver storage of warm starts")
     ap.add_argument("--epochs", type=int, default=40, help="training epochs of --workload warmstart")
     ap.add_argument("--save", default=None, metavar="DIR", help="--workload forces: write Cd and Cl per step to DIR")
+    ap.add_argument("--spinup", type=int, default=0,
+                    help="--workload forces: FP64 coarse steps from rest before every precision continues from "
+                         "that state for --steps steps")
     ap.add_argument("--bc", default="reference", choices=["reference", "channel"],
                     help="boundaries of --workload timetocd: the reference's, or free-slip top and bottom with a "
                          "half-way bounce-back cylinder")

@@ -396,6 +396,13 @@ typedef struct {
 int mb_error_L2_noalloc(const mb_l2_segment *segs, int nseg, double *d_out, mb_stream stream);
 
 /* ---- introspection ------------------------------------------------------- */
+/* Text description of the plan that mb_step(ctx, n) starts with from the
+ * current state (n >= period + 1: the plan of `period` coarse steps; else a
+ * single step): one line per launch with its kind, level, region, grid,
+ * scheduling class, label and the launches it waits for.  Writes at most
+ * cap - 1 characters and a terminating zero; *len receives the full length.
+ * No counterpart in the reference (whose order is the call order). */
+int mb_plan_describe(mb_ctx *ctx, int n_coarse, char *buf, long long cap, long long *len);
 /* Number of kernels launched by the last mb_step call, and in one coarse step. */
 int mb_stats(mb_ctx *ctx, long long *kernels_last_step_call, long long *kernels_per_coarse_step,
              long long *cell_updates_per_coarse_step);

@@ -1798,6 +1798,42 @@ extern "C" int mb_prepare_diag(mb_ctx *c, int n) {
   return prepare_chunks(c, n, true);
 }
 
+// Text description of the plan mb_step(n) starts with from the current
+// state: one line per lowered node (index, kind, level, region, grid, graph
+// priority class, label, dependencies).  The plan is compiled if needed; the
+// scheduler state is unchanged.
+extern "C" int mb_plan_describe(mb_ctx *c, int n, char *buf, long long cap, long long *len) {
+  if (!c || n < 1 || (!buf && cap > 0)) return MB_ERR_INVALID;
+  if (!c->inited) return MB_ERR_STATE;
+  const int G = c->use_graph == 3 ? c->period * c->prg_periods : c->period;
+  int err = 0;
+  const SchedState save = c->state;
+  CompiledPlan *cp = get_plan(c, n - 1 >= G ? G : 1, n == 1, &err);
+  c->state = save;
+  if (!cp) return err ? err : MB_ERR_INVALID;
+  if (c->use_graph && c->use_graph != 3) mark_slack(*cp);
+  std::string out;
+  static const char *kinds[] = {"stb", "rec", "spl", "ccp", "?", "drag", "l2"};
+  for (size_t q = 0; q < cp->dn.size(); q++) {
+    const DevPlanNode &d = cp->dn[q];
+    const PlanNode &nd = cp->nodes[q];
+    char line[256];
+    std::snprintf(line, sizeof line, "%zu %s L%d r%d grid %u %s %s deps", q,
+                  (int)d.kind >= 0 && (int)d.kind < 7 ? kinds[(int)d.kind] : "?", nd.level, nd.region, d.grid.x,
+                  d.background ? "bulk" : (d.slack ? "slack" : "chain"), nd.label.c_str());
+    out += line;
+    for (int p : d.deps) out += " " + std::to_string(p);
+    out += "\n";
+  }
+  if (len) *len = (long long)out.size();
+  if (cap > 0) {
+    const size_t m = std::min<size_t>(out.size(), (size_t)cap - 1);
+    std::memcpy(buf, out.data(), m);
+    buf[m] = 0;
+  }
+  return MB_OK;
+}
+
 extern "C" int mb_block_step(mb_ctx *c, int area, mb_stream stream) {
   if (!c || area < 0 || area >= c->nblk) return MB_ERR_INVALID;
   if (!c->inited) return MB_ERR_STATE;

@@ -181,6 +181,7 @@ SIGNATURES = {
     "mb_program_selftest": ([_vp, C.c_int, _vp], C.c_int),
     "mb_prepare": ([_vp, C.c_int], C.c_int),
     "mb_prepare_diag": ([_vp, C.c_int], C.c_int),
+    "mb_plan_describe": ([_vp, C.c_int, C.c_char_p, C.c_longlong, _pll], C.c_int),
     "mb_block_step": ([_vp, C.c_int, _vp], C.c_int),
     "mb_c_c_boundary_transfer": ([_vp, C.c_int, _vp], C.c_int),
     "mb_space_interpolation": ([_vp, C.c_int, _vp], C.c_int),
@@ -596,6 +597,15 @@ class MultiBlockLBM:
         """Compiles the plans and graphs that evolution_diag(n_coarse) will replay
         and sizes its result buffers."""
         _check(self.lib.mb_prepare_diag(self.h, int(n_coarse)), "mb_prepare_diag")
+
+    def plan_description(self, n_coarse):
+        """Text listing of the plan mb_step(n_coarse) starts with: one line per
+        launch with its dependencies."""
+        need = C.c_longlong()
+        _check(self.lib.mb_plan_describe(self.h, int(n_coarse), None, 0, C.byref(need)), "mb_plan_describe")
+        buf = C.create_string_buffer(need.value + 1)
+        _check(self.lib.mb_plan_describe(self.h, int(n_coarse), buf, need.value + 1, C.byref(need)), "mb_plan_describe")
+        return buf.value.decode()
 
     def block_step(self, area, stream=None):
         _check(self.lib.mb_block_step(self.h, area, _stream_ptr(stream)), "mb_block_step")
