@@ -143,6 +143,36 @@ def bench_config(world):
             "parallelism": f"{world} independent cases, one per GPU"}
 
 
+def level0_in_step(sim, stream):
+    """(kernel, mean ms, algorithmic bytes) of level 0's interior block-step
+    launches inside one replayed plan of `period` coarse steps, from the
+    CUPTI kernel records of torch.profiler (outside any timed region); None
+    when the profiler records no such kernel."""
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+
+    n = 13  # one plan of 6 steps twice, then single steps
+    sim.prepare(n)
+    torch.cuda.synchronize()
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        sim.evolution(n, stream)
+        torch.cuda.synchronize()
+    durs = {}
+    for e in prof.events():
+        nm = e.name
+        interior = "block_step_q<" in nm or ("block_step_p<" in nm and ", true>" in nm) or \
+            ("block_step_r<" in nm and ", true>" in nm) or "block_step_tb<" in nm
+        if e.device_type == torch.autograd.DeviceType.CUDA and interior:
+            durs.setdefault(e.name.split("(")[0], []).append((e.time_range.end - e.time_range.start) / 1e3)
+    if not durs:
+        return None
+    name, d = max(durs.items(), key=lambda kv: len(kv[1]))
+    geo = sim.geo
+    # the interior (distance >= 2 from the block edges) of the level-0 blocks
+    cells = sum((geo.Areas[a].nx - 4) * (geo.Areas[a].ny - 4) for a in range(geo.layout.ASP[0], geo.layout.ASP[1]))
+    return name, float(sum(d) / len(d)), float(BYTES_PER_UPDATE[sim.precision]) * cells
+
+
 def run_reference(args):
     """The reference's own CUDA build (oracle/_ref/ref_c2) on WORKLOAD.  Loads
     nothing of this repository's library: the update count comes from the
@@ -653,6 +683,8 @@ def main():
 
     # ---- dominant kernel alone: level-0 block step, CUDA events on its stream
     kms, kbytes, kcells = sim.time_block_step(0, 50, stream)
+    # ---- the same kernel inside the step: CUPTI kernel records of one plan
+    in_step = level0_in_step(sim, stream)
     # ---- end to end through the C ABI with host buffers ----------------------
     import numpy as np
 
@@ -727,7 +759,14 @@ def main():
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": src,
                          "kernel": "k_block_step level 0", "alg_bytes_per_launch": kbytes, "cells_per_launch": kcells,
-                         "ms_per_launch": round(kms, 5), "bytes_per_update": BYTES_PER_UPDATE[args.precision]},
+                         "ms_per_launch": round(kms, 5), "bytes_per_update": BYTES_PER_UPDATE[args.precision],
+                         "in_step": None if in_step is None else {
+                             "kernel": in_step[0], "ms_per_launch": round(in_step[1], 5),
+                             "achieved": round(in_step[2] / (in_step[1] * 1e-3) / 1e9, 1),
+                             "frac": round(in_step[2] / (in_step[1] * 1e-3) / 1e9 / peak, 4),
+                             "what": "mean duration of the level-0 interior launch inside the CUDA graph of "
+                                     "6 coarse steps (CUPTI kernel records via torch.profiler), beside the "
+                                     "fine levels' chain; bytes per update x its cells"}},
             "e2e": {"value": round(world * upd * args.steps / (ms_e2e * 1e-3) / 1e6, 1), "unit": "MLUPS",
                     "h2d_bytes_per_step": round(h2d / args.steps), "d2h_bytes_per_step": round(d2h / args.steps),
                     "wall_s": round(wall_e2e, 3),

@@ -241,6 +241,11 @@ int mb_set_split_cells(mb_ctx *ctx, long long cells);
  * rows touch one cache sector per value, so small units spread a node over
  * many SMs' load/store units.  Results are identical. */
 int mb_set_interface_shape(mb_ctx *ctx, int rec_points, int spline_segments);
+/* Unused shared memory (KB) reserved by every CTA of the bulk block-step
+ * launches (the interiors of split levels): an SM then holds fewer of them at
+ * once and keeps room for the latency-bound chain launches beside them
+ * (0, the default: no reservation).  Results are identical. */
+int mb_set_bulk_spread(mb_ctx *ctx, int kb);
 /* Minimum dynamic shared memory (KB, at most 200) per CTA of the spline and
  * the record kernels, which caps how many of their CTAs share one SM: a
  * latency-bound launch that starts while a block step still holds most SMs

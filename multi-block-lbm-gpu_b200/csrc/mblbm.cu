@@ -174,6 +174,7 @@ struct mb_ctx {
   // free up instead of piling onto the first ones
   int spl_cta_smem = 96 * 1024;
   int rec_cta_smem = 0;
+  int bulk_cta_smem = 0;  // unused shared memory reserved by each bulk (interior) block-step CTA
   PrgTraceRec *d_trace = nullptr;       // executor trace (mb_set_program_trace)
   unsigned int *d_trace_n = nullptr;
   unsigned int trace_cap = 0;
@@ -568,6 +569,10 @@ int lower_plan(mb_ctx *c, CompiledPlan &cp) {
       if (d.func == kfunc<KStbTb>(c->prec)) {
         d.block = dim3(TB_THREADS);
         d.smem = (size_t)tb_smem(c->prec);
+      } else if (d.background && c->bulk_cta_smem > 0) {
+        // shared memory the kernel does not use, reserved so that an SM holds
+        // fewer bulk CTAs and keeps room for the chain's (mb_set_bulk_spread)
+        d.smem = (size_t)c->bulk_cta_smem;
       }
       d.args[0] = &d.stb;
     } else if (n.kind == NK_L2) {
@@ -1376,6 +1381,19 @@ extern "C" int mb_set_split_cells(mb_ctx *c, long long cells) {
   cudaDeviceSynchronize();
   c->split_cells = cells;
   c->plans.clear();
+  return MB_OK;
+}
+
+extern "C" int mb_set_bulk_spread(mb_ctx *c, int kb) {
+  if (!c || kb < 0 || kb * 1024 > MB_CTA_SMEM_MAX) return MB_ERR_INVALID;
+  cudaDeviceSynchronize();
+  c->plans.clear();
+  c->bulk_cta_smem = kb * 1024;
+  if (kb > 0) {  // every kernel a bulk node may run, allowed that much dynamic shared memory
+    void *fns[] = {kfunc<KStb>(c->prec), kfunc<KStb2>(c->prec), kfunc<KStbQ>(c->prec), kfunc<KStbPI>(c->prec),
+                   kfunc<KStbP>(c->prec), kfunc<KStbRI>(c->prec), kfunc<KStbR>(c->prec)};
+    for (void *f : fns) MB_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, kb * 1024));
+  }
   return MB_OK;
 }
 

@@ -477,7 +477,7 @@ struct ConvLayer {
 
 struct mb_unet {
   int H, W, maxN, C0;
-  int gemm = 0;                  // 3x3 convolutions: 1 tcgen05 (where the layer's shape fits), 0 mma.sync
+  int gemm = 1;                  // 3x3 convolutions: 1 tcgen05 (where the layer's shape fits), 0 mma.sync
   unsigned int *d_err = nullptr; // error word of the tcgen05 kernels' bounded waits
   std::vector<ConvLayer> conv;  // 14 layers, in forward order
   long long head_w = 0, head_b = 0, nparam = 0;

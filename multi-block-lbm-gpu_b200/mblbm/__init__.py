@@ -181,6 +181,7 @@ SIGNATURES = {
     "mb_program_selftest": ([_vp, C.c_int, _vp], C.c_int),
     "mb_prepare": ([_vp, C.c_int], C.c_int),
     "mb_prepare_diag": ([_vp, C.c_int], C.c_int),
+    "mb_set_bulk_spread": ([_vp, C.c_int], C.c_int),
     "mb_plan_describe": ([_vp, C.c_int, C.c_char_p, C.c_longlong, _pll], C.c_int),
     "mb_block_step": ([_vp, C.c_int, _vp], C.c_int),
     "mb_c_c_boundary_transfer": ([_vp, C.c_int, _vp], C.c_int),
@@ -530,6 +531,10 @@ class MultiBlockLBM:
     def set_cta_spread(self, spline_kb, records_kb):
         """Minimum shared memory per spline / record CTA (KB): caps their CTAs per SM."""
         _check(self.lib.mb_set_cta_spread(self.h, int(spline_kb), int(records_kb)), "mb_set_cta_spread")
+
+    def set_bulk_spread(self, kb):
+        """Unused shared memory (KB) reserved by each bulk (interior) block-step CTA (0: none)."""
+        _check(self.lib.mb_set_bulk_spread(self.h, int(kb)), "mb_set_bulk_spread")
 
     def set_fusion(self, flags):
         """Plan fusions (bit 0: same-level copies inside the block step; bit 1: temporal
