@@ -496,8 +496,11 @@ def run_forces_developed(args, geo):
     c = geo.config
     D, U0 = 2.0 * c.R, c.U0[0]
     out = {}
-    for prec in ("f64", "f32", "f16s", "f16c"):
-        sim = mblbm.MultiBlockLBM(geo, prec)
+    runs = [("f64", None), ("f32", None), ("f32", "w"), ("f16s", None), ("f16s", "feq0"), ("f16c", None),
+            ("f16c", "feq0")]
+    for prec, shift in runs:
+        name = prec if shift is None else f"{prec}_{shift}"
+        sim = mblbm.MultiBlockLBM(geo, prec, shift=shift)
         sim.init()
         for a, f in enumerate(state):
             sim.set_fields(a, f["rho"], f["ux"], f["uy"], f["F"])
@@ -510,14 +513,16 @@ def run_forces_developed(args, geo):
         sim.close()
         cd, cl = np.concatenate(cd), np.concatenate(cl)
         st = mblbm.strouhal(cl, D, U0)
-        out[prec] = {"mean_cd": float(cd.mean()), "rms_cl": float(np.sqrt(np.mean(cl ** 2))),
+        out[name] = {"mean_cd": float(cd.mean()), "rms_cl": float(np.sqrt(np.mean(cl ** 2))),
                      "strouhal": None if st is None else float(st)}
         if args.save:
-            np.save(os.path.join(args.save, f"forces_dev_{prec}.npy"), np.stack([cd, cl]))
-    for prec in ("f32", "f16s", "f16c"):
+            np.save(os.path.join(args.save, f"forces_dev_{name}.npy"), np.stack([cd, cl]))
+    for name in out:
+        if name == "f64":
+            continue
         for k in ("mean_cd", "rms_cl", "strouhal"):
-            a, b = out[prec][k], out["f64"][k]
-            out[prec][k + "_rel_f64"] = None if a is None or b is None else a / b - 1.0
+            a, b = out[name][k], out["f64"][k]
+            out[name][k + "_rel_f64"] = None if a is None or b is None else a / b - 1.0
     line = {"metric": "mean Cd, rms Cl, Strouhal number on developed shedding, by storage precision",
             "unit": "dimensionless", "n_gpus": 1, "steps": args.steps, "spinup_f64": args.spinup,
             "data": "synthetic", "config": {"workload": WORKLOAD}, "by_precision": out}

@@ -54,6 +54,15 @@ extern "C" {
  * arithmetic.  Out-of-range values saturate and mb_check_finite counts them. */
 #define MB_PREC_F16C 4
 
+/* ---- shift of the stored distributions (shifted precisions) ------------- */
+/* The shifted precisions store h = f - s with a constant vector s: the lattice
+ * weights w (MB_SHIFT_W, the 16-bit forms' default), or the equilibrium of
+ * the free stream feq(rho0, U0) (MB_SHIFT_FEQ0, FP32's default: the stored
+ * words are then small wherever the flow is close to the free stream, and so
+ * are their rounding errors). */
+#define MB_SHIFT_W 0
+#define MB_SHIFT_FEQ0 1
+
 /* ---- cell type codes, values as in lbm/lbm.h:26-32 -------------------- */
 #define MB_FLUID 0
 #define MB_SOLID_SBB 1
@@ -246,6 +255,11 @@ int mb_set_interface_shape(mb_ctx *ctx, int rec_points, int spline_segments);
  * once and keeps room for the latency-bound chain launches beside them
  * (0, the default: no reservation).  Results are identical. */
 int mb_set_bulk_spread(mb_ctx *ctx, int kb);
+/* MB_SHIFT_W or MB_SHIFT_FEQ0 for the stored distributions (no effect on
+ * MB_PREC_F64 and MB_PREC_F32U, which store f).  Changing it discards the
+ * state: mb_init, mb_set_fields or a checkpoint of the same shift must come
+ * next (mb_step returns MB_ERR_STATE until then). */
+int mb_set_shift(mb_ctx *ctx, int mode);
 /* Minimum dynamic shared memory (KB, at most 200) per CTA of the spline and
  * the record kernels, which caps how many of their CTAs share one SM: a
  * latency-bound launch that starts while a block step still holds most SMs

@@ -49,6 +49,23 @@ template <> struct Prec<MB_PREC_F16C> { using S = h16c; using R = float; static 
 
 template <int P> __device__ __forceinline__ typename Prec<P>::R wk(int k) { return (typename Prec<P>::R)wd(k); }
 
+// The shift of the shifted precisions: the stored word of direction k is
+// h_k = f_k - s_k, with s = feq(rho_s, U_s) for constants rho_s, U_s (s = w:
+// rho_s = 1, U_s = 0; s = feq(rho0, U0): the free stream).  The collision
+// works on h directly: rho = rho_s + sum h, rho u = J_s + sum e h (J_s =
+// rho_s U_s), and feq_k - s_k = w_k (d + 3 e.J_h + rho (4.5 (e.u)^2 - 1.5 u^2))
+// + c_k with d = sum h, J_h = sum e h and c_k = w_k (rho_s + 3 e_k.J_s) - s_k,
+// which depends on the direction pair only (zero for s = w).
+struct Sh9 { float s[9]; };
+struct Shift {
+  Sh9 v;              // s_k
+  float c[5];         // c_k for k = 0, the pairs (1,3), (2,4), (5,7) and (8,6)
+  float rhos, jx, jy; // rho_s, J_s
+  float q2, qd, qx;   // rho_s |U_s|^2, rho_s (Usx^2 - Usy^2), rho_s Usx Usy (MRT)
+  int sym;            // s_k = s_opp(k) = s_slip(k): walls move stored words unchanged
+  int pad_;
+};
+
 // stored word <-> arithmetic type
 __device__ __forceinline__ float to_r(__half h) { return __half2float(h); }
 __device__ __forceinline__ float to_r(float v) { return v; }
@@ -84,14 +101,32 @@ template <> __device__ __forceinline__ h16c from_r<h16c>(double v) { return from
 
 // value of distribution k from its stored form (shifted forms store f - w_k)
 template <int P>
-__device__ __forceinline__ typename Prec<P>::R ld_f(const typename Prec<P>::S *p, long long idx, int k) {
-  if constexpr (Prec<P>::shifted) return to_r(p[idx]) + wk<P>(k);
+__device__ __forceinline__ typename Prec<P>::R ld_f(const typename Prec<P>::S *p, long long idx, int k, const Sh9 &sh) {
+  if constexpr (Prec<P>::shifted) return to_r(p[idx]) + sh.s[k];
   else return p[idx];
 }
 template <int P>
-__device__ __forceinline__ void st_f(typename Prec<P>::S *p, long long idx, int k, typename Prec<P>::R v) {
-  if constexpr (Prec<P>::shifted) p[idx] = from_r<typename Prec<P>::S>(v - wk<P>(k));
+__device__ __forceinline__ void st_f(typename Prec<P>::S *p, long long idx, int k, typename Prec<P>::R v,
+                                     const Sh9 &sh) {
+  if constexpr (Prec<P>::shifted) p[idx] = from_r<typename Prec<P>::S>(v - sh.s[k]);
   else p[idx] = v;
+}
+// the stored word of f_k = x given in FP64 (an equilibrium, a stale value)
+template <int P>
+__device__ __forceinline__ typename Prec<P>::S stored_of(double x, int k, const Sh9 &sh) {
+  if constexpr (Prec<P>::shifted) return from_r<typename Prec<P>::S>((float)(x - (double)sh.s[k]));
+  else return (typename Prec<P>::S)x;
+}
+// the stored word of f_k when f_k equals f_j of a stored word v (a wall
+// returning another direction's value): v itself when s_k = s_j
+template <int P>
+__device__ __forceinline__ typename Prec<P>::S moved(typename Prec<P>::S v, int j, int k, const Shift &sh) {
+  if constexpr (Prec<P>::shifted) {
+    if (sh.sym) return v;
+    return from_r<typename Prec<P>::S>(to_r(v) + (sh.v.s[j] - sh.v.s[k]));
+  } else {
+    return v;
+  }
 }
 
 // Global loads and stores with an optional evict-first cache hint (.cs):
@@ -216,6 +251,7 @@ struct StbParams {
   StbOptions opt;
   int tskip;         // leave cells flagged FL_TSKIP alone: a spline writes their next values
   int pad_t;
+  Shift sh;          // shift of the stored words (shifted precisions)
   StbBlk b[STB_MAX_BLOCKS];
 };
 
@@ -226,31 +262,40 @@ struct StbParams {
 // with base = rho (plain storage) or rho - 1 (shifted storage, where g_k is
 // feq_k - w_k).  Same scheme as feq (lbm/assit_func.h:2-9), fewer operations.
 template <bool SHIFTED>
-__device__ __forceinline__ void collide_f32(const float *f, float rv, float *out, float *m) {
+__device__ __forceinline__ void collide_f32(const float *f, float rv, float *out, float *m, const Shift &sh) {
   const float sum = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8];
-  const float rh = SHIFTED ? 1.0f + sum : sum;
-  const float base = sum;  // rho - 1 when shifted, rho otherwise
+  const float rh = SHIFTED ? sh.rhos + sum : sum;
+  const float base = sum;  // rho - rho_s when shifted, rho otherwise
   const float inv = __frcp_rn(rh);
-  const float ux = (f[1] - f[3] + f[5] - f[6] - f[7] + f[8]) * inv;
-  const float uy = (f[2] - f[4] + f[5] + f[6] - f[7] - f[8]) * inv;
+  const float jx = f[1] - f[3] + f[5] - f[6] - f[7] + f[8], jy = f[2] - f[4] + f[5] + f[6] - f[7] - f[8];
+  const float ux = (SHIFTED ? jx + sh.jx : jx) * inv;
+  const float uy = (SHIFTED ? jy + sh.jy : jy) * inv;
   m[0] = rh;
   m[1] = ux;
   m[2] = uy;
   const float u15 = 1.5f * (ux * ux + uy * uy);
-  const float rh3 = 3.0f * rh;
   const float w0 = 4.0f / 9.0f, w1 = 1.0f / 9.0f, w5 = 1.0f / 36.0f;
-  const float g0 = w0 * (base - rh * u15);
+  const float g0 = w0 * (base - rh * u15) + (SHIFTED ? sh.c[0] : 0.0f);
   out[0] = f[0] + rv * (g0 - f[0]);
-  auto pair = [&](float a, float w, int kp, int km) {
-    const float e = w * (base + rh * (4.5f * a * a - u15));
-    const float o = w * (rh3 * a);
+  // the odd part 3 w e.(rho u) of a pair, from J_h when shifted (J_s cancels
+  // against the shift's own odd part)
+  auto pair = [&](float a, float jo, float w, float cq, int kp, int km) {
+    const float e = w * (base + rh * (4.5f * a * a - u15)) + cq;
+    const float o = w * (3.0f * jo);
     out[kp] = f[kp] + rv * ((e + o) - f[kp]);
     out[km] = f[km] + rv * ((e - o) - f[km]);
   };
-  pair(ux, w1, 1, 3);
-  pair(uy, w1, 2, 4);
-  pair(ux + uy, w5, 5, 7);
-  pair(ux - uy, w5, 8, 6);
+  if (SHIFTED) {
+    pair(ux, jx, w1, sh.c[1], 1, 3);
+    pair(uy, jy, w1, sh.c[2], 2, 4);
+    pair(ux + uy, jx + jy, w5, sh.c[3], 5, 7);
+    pair(ux - uy, jx - jy, w5, sh.c[4], 8, 6);
+  } else {
+    pair(ux, rh * ux, w1, 0.0f, 1, 3);
+    pair(uy, rh * uy, w1, 0.0f, 2, 4);
+    pair(ux + uy, rh * (ux + uy), w5, 0.0f, 5, 7);
+    pair(ux - uy, rh * (ux - uy), w5, 0.0f, 8, 6);
+  }
 }
 
 // FLUID interior cell: Macros (lbm/assit_func.h:23-31) and BGK (stb3 :103-111,
@@ -259,10 +304,10 @@ __device__ __forceinline__ void collide_f32(const float *f, float rv, float *out
 // reference's expressions as written; FP32 arithmetic uses collide_f32.
 template <int P>
 __device__ __forceinline__ void stb_collide(const typename Prec<P>::R *f, typename Prec<P>::R rv,
-                                            typename Prec<P>::R *out, typename Prec<P>::R *m) {
+                                            typename Prec<P>::R *out, typename Prec<P>::R *m, const Shift &sh) {
   using R = typename Prec<P>::R;
   if constexpr (sizeof(R) == 4) {
-    collide_f32<Prec<P>::shifted>(f, rv, out, m);
+    collide_f32<Prec<P>::shifted>(f, rv, out, m, sh);
   } else {
     R rh = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8];
     R ux = f[1] - f[3] + f[5] - f[6] - f[7] + f[8];
@@ -317,7 +362,7 @@ __device__ __forceinline__ void stb_finish_at(const StbParams &p, const StbBlk &
     if (fl & 4) {   // block edge: equilibrium at rho0, U0 (stb2 :47-57), collide keeps it
 #pragma unroll
       for (int k = 0; k < 9; k++) {
-        if constexpr (Prec<P>::shifted) st_ef<EF>(Fout + k * plane + cd, from_r<S>((R)p.feqc[k] - wk<P>(k)));
+        if constexpr (Prec<P>::shifted) st_ef<EF>(Fout + k * plane + cd, from_r<S>((R)p.feqc[k] - p.sh.v.s[k]));
         else st_ef<EF>(Fout + k * plane + cd, (S)p.feqc[k]);
       }
       if (wm) {
@@ -331,7 +376,7 @@ __device__ __forceinline__ void stb_finish_at(const StbParams &p, const StbBlk &
 #pragma unroll
     for (int k = 0; k < 9; k++) f[k] = to_r(raw[k]);
     R out[9], m[3];
-    stb_collide<P>(f, (R)B.rv_tau, out, m);
+    stb_collide<P>(f, (R)B.rv_tau, out, m, p.sh);
     if (wm) {
       st_ef<EF>((R *)D.rho + cd, m[0]);
       st_ef<EF>((R *)D.ux + cd, m[1]);
@@ -351,15 +396,10 @@ __device__ __forceinline__ void stb_finish_at(const StbParams &p, const StbBlk &
 #pragma unroll
     for (int k = 0; k < 9; k++) {
       const int id = i - ex(k), jd = j - ey(k);
-      if (id >= 0 && id < B.nx && jd >= 0 && jd < B.ny)
-        fr[k] = raw[k];
-      else if constexpr (Prec<P>::shifted)
-        fr[k] = from_r<S>((float)(p.feqc[k] - wd(k)));
-      else
-        fr[k] = (S)p.feqc[k];
+      fr[k] = (id >= 0 && id < B.nx && jd >= 0 && jd < B.ny) ? raw[k] : stored_of<P>(p.feqc[k], k, p.sh.v);
     }
 #pragma unroll
-    for (int k = 0; k < 9; k++) st_ef<EF>(Fout + k * plane + cd, fr[opp(k)]);  // w_k = w_opp(k): raw move is exact
+    for (int k = 0; k < 9; k++) st_ef<EF>(Fout + k * plane + cd, moved<P>(fr[opp(k)], opp(k), k, p.sh));
     return;
   }
   // C_BOUNDARY and row padding: untouched by the step, carried to the new buffer
@@ -385,7 +425,7 @@ __device__ __forceinline__ void stb_finish(const StbParams &p, const StbBlk &B, 
     if (fl & 4) {   // block edge: equilibrium at rho0, U0 (stb2 :47-57), collide keeps it
 #pragma unroll
       for (int k = 0; k < 9; k++) {
-        if constexpr (Prec<P>::shifted) st_ef<EF>(Fout + k * plane + c, from_r<S>((R)p.feqc[k] - wk<P>(k)));
+        if constexpr (Prec<P>::shifted) st_ef<EF>(Fout + k * plane + c, from_r<S>((R)p.feqc[k] - p.sh.v.s[k]));
         else st_ef<EF>(Fout + k * plane + c, (S)p.feqc[k]);
       }
       if (wm) {
@@ -399,7 +439,7 @@ __device__ __forceinline__ void stb_finish(const StbParams &p, const StbBlk &B, 
 #pragma unroll
     for (int k = 0; k < 9; k++) f[k] = to_r(raw[k]);
     R out[9], m[3];
-    stb_collide<P>(f, (R)B.rv_tau, out, m);
+    stb_collide<P>(f, (R)B.rv_tau, out, m, p.sh);
     if (wm) {
       st_ef<EF>((R *)B.rho + c, m[0]);
       st_ef<EF>((R *)B.ux + c, m[1]);
@@ -414,15 +454,10 @@ __device__ __forceinline__ void stb_finish(const StbParams &p, const StbBlk &B, 
 #pragma unroll
     for (int k = 0; k < 9; k++) {
       const int id = i - ex(k), jd = j - ey(k);
-      if (id >= 0 && id < B.nx && jd >= 0 && jd < B.ny)
-        fr[k] = raw[k];
-      else if constexpr (Prec<P>::shifted)
-        fr[k] = from_r<S>((float)(p.feqc[k] - wd(k)));
-      else
-        fr[k] = (S)p.feqc[k];
+      fr[k] = (id >= 0 && id < B.nx && jd >= 0 && jd < B.ny) ? raw[k] : stored_of<P>(p.feqc[k], k, p.sh.v);
     }
 #pragma unroll
-    for (int k = 0; k < 9; k++) st_ef<EF>(Fout + k * plane + c, fr[opp(k)]);  // w_k = w_opp(k): raw move is exact
+    for (int k = 0; k < 9; k++) st_ef<EF>(Fout + k * plane + c, moved<P>(fr[opp(k)], opp(k), k, p.sh));
     return;
   }
   // C_BOUNDARY and row padding: untouched by the step, carried to the new
@@ -605,14 +640,18 @@ __host__ __device__ constexpr double mrt_norm(int q) {
 template <int P>
 __device__ __forceinline__ void mrt_collide(const typename Prec<P>::R *f, typename Prec<P>::R rv,
                                             const StbOptions &o, typename Prec<P>::R *out,
-                                            typename Prec<P>::R *m) {
+                                            typename Prec<P>::R *m, const Shift &sh) {
   using R = typename Prec<P>::R;
   // Macros (lbm/assit_func.h:23-31)
   R rh = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8];
-  const R base = rh;  // rho - 1 when shifted
-  if constexpr (Prec<P>::shifted) rh = (R)1 + rh;
+  const R base = rh;  // rho - rho_s when shifted
+  if constexpr (Prec<P>::shifted) rh = (R)sh.rhos + rh;
   R ux = f[1] - f[3] + f[5] - f[6] - f[7] + f[8];
   R uy = f[2] - f[4] + f[5] + f[6] - f[7] - f[8];
+  if constexpr (Prec<P>::shifted) {
+    ux += (R)sh.jx;
+    uy += (R)sh.jy;
+  }
   ux = ux / rh;
   uy = uy / rh;
   m[0] = rh;
@@ -629,21 +668,25 @@ __device__ __forceinline__ void mrt_collide(const typename Prec<P>::R *f, typena
   }
   const R uv = ux * ux + uy * uy;
   R meq[9];
-  if constexpr (Prec<P>::shifted) {  // Meq minus the moments of w: (1, -2, 1, 0, ...)
+  if constexpr (Prec<P>::shifted) {  // Meq minus the moments of s = feq(rho_s, U_s)
     meq[0] = base;
-    meq[1] = (R)-2 * base + (R)3 * rh * uv;
-    meq[2] = base - (R)3 * rh * uv;
+    meq[1] = (R)-2 * base + (R)3 * (rh * uv - (R)sh.q2);
+    meq[2] = base - (R)3 * (rh * uv - (R)sh.q2);
+    meq[3] = rh * ux - (R)sh.jx;
+    meq[5] = rh * uy - (R)sh.jy;
+    meq[7] = rh * (ux * ux - uy * uy) - (R)sh.qd;
+    meq[8] = rh * (ux * uy) - (R)sh.qx;
   } else {
     meq[0] = rh;
     meq[1] = rh * ((R)-2.0 + (R)3.0 * uv);
     meq[2] = rh * ((R)1.0 - (R)3.0 * uv);
+    meq[3] = rh * ux;
+    meq[5] = rh * uy;
+    meq[7] = rh * (ux * ux - uy * uy);
+    meq[8] = rh * (ux * uy);
   }
-  meq[3] = rh * ux;
   meq[4] = -meq[3];
-  meq[5] = rh * uy;
   meq[6] = -meq[5];
-  meq[7] = rh * (ux * ux - uy * uy);
-  meq[8] = rh * (ux * uy);
   const R se = o.mrt_s[0] > 0 ? (R)o.mrt_s[0] : rv;
   const R sp = o.mrt_s[1] > 0 ? (R)o.mrt_s[1] : rv;
   const R sq = o.mrt_s[2] > 0 ? (R)o.mrt_s[2] : rv;
@@ -693,7 +736,7 @@ __device__ __forceinline__ void stbx_cell(const StbParams &p, const StbBlk &B, i
       for (int k = 0; k < 9; k++) {
         R v = (R)p.feqc[k];
         if (p.opt.has_force) v += dt * force_k<R>(k, (R)p.u0x, (R)p.u0y, fx, fy, rv);
-        if constexpr (Prec<P>::shifted) v -= wk<P>(k);
+        if constexpr (Prec<P>::shifted) v -= (R)p.sh.v.s[k];
         Fout[k * plane + c] = from_r<S>(v);
       }
       if (wm) {
@@ -708,11 +751,11 @@ __device__ __forceinline__ void stbx_cell(const StbParams &p, const StbBlk &B, i
     for (int k = 0; k < 9; k++) {
       const long long n = c - ((long long)ey(k) * B.pitch + ex(k));
       const bool hbb = (B.flags[n] & (3 | FL_HBB)) == (1 | FL_HBB);
-      f[k] = to_r(hbb ? Fin[opp(k) * plane + c] : Fin[k * plane + n]);
+      f[k] = to_r(hbb ? moved<P>(Fin[opp(k) * plane + c], opp(k), k, p.sh) : Fin[k * plane + n]);
     }
     R out[9], m[3];
-    if (p.opt.coll == MB_COLL_MRT) mrt_collide<P>(f, rv, p.opt, out, m);
-    else stb_collide<P>(f, rv, out, m);
+    if (p.opt.coll == MB_COLL_MRT) mrt_collide<P>(f, rv, p.opt, out, m, p.sh);
+    else stb_collide<P>(f, rv, out, m, p.sh);
     if (p.opt.has_force) {
 #pragma unroll
       for (int k = 0; k < 9; k++) out[k] += dt * force_k<R>(k, m[1], m[2], fx, fy, rv);
@@ -732,13 +775,10 @@ __device__ __forceinline__ void stbx_cell(const StbParams &p, const StbBlk &B, i
 #pragma unroll
     for (int k = 0; k < 9; k++) {
       const int id = i - ex(k), jd = j - ey(k);
-      if (!(id >= 0 && id < B.nx && jd >= 0 && jd < B.ny)) {
-        if constexpr (Prec<P>::shifted) raw[k] = from_r<S>((float)(p.feqc[k] - wd(k)));
-        else raw[k] = (S)p.feqc[k];
-      }
+      if (!(id >= 0 && id < B.nx && jd >= 0 && jd < B.ny)) raw[k] = stored_of<P>(p.feqc[k], k, p.sh.v);
     }
 #pragma unroll
-    for (int k = 0; k < 9; k++) Fout[k * plane + c] = raw[slip(k)];  // w_k = w_slip(k)
+    for (int k = 0; k < 9; k++) Fout[k * plane + c] = moved<P>(raw[slip(k)], slip(k), k, p.sh);
     return;
   }
   if (type == 1 && !(fl & FL_HBB)) {  // SOLID_SBB
@@ -793,7 +833,7 @@ __device__ __forceinline__ void stb_cell_rows(const StbParams &p, const StbBlk &
 #pragma unroll
       for (int k = 0; k < 9; k++) f[k] = to_r(raw[k]);
       R out[9], m[3];
-      stb_collide<P>(f, (R)B.rv_tau, out, m);
+      stb_collide<P>(f, (R)B.rv_tau, out, m, p.sh);
       if (p.write_macros && (p.macro_all || (fl & 8))) {
         st_ef<EF>((R *)B.rho + c, m[0]);
         st_ef<EF>((R *)B.ux + c, m[1]);
@@ -882,10 +922,10 @@ __device__ __forceinline__ void stb_pair(const StbParams &p, const StbBlk &B, in
       R f[9], oa[9], ob[9], ma[3], mb[3];
 #pragma unroll
       for (int k = 0; k < 9; k++) f[k] = to_r(a[k]);
-      stb_collide<P>(f, (R)B.rv_tau, oa, ma);
+      stb_collide<P>(f, (R)B.rv_tau, oa, ma, p.sh);
 #pragma unroll
       for (int k = 0; k < 9; k++) f[k] = to_r(b[k]);
-      stb_collide<P>(f, (R)B.rv_tau, ob, mb);
+      stb_collide<P>(f, (R)B.rv_tau, ob, mb, p.sh);
       if (p.write_macros) {
         const bool wa = p.macro_all || (fa & 8), wb = p.macro_all || (fb & 8);
         R *rho = (R *)B.rho + c, *ux = (R *)B.ux + c, *uy = (R *)B.uy + c;
@@ -1085,7 +1125,7 @@ __global__ void __launch_bounds__(TB_THREADS, 1) k_block_step_tb(const __grid_co
 #pragma unroll
         for (int k = 0; k < 9; k++) f[k] = to_r(((const S *)(st + k * C::SEG_BYTES))[tid + C::A - ex(k)]);
         R out[9], m[3];
-        stb_collide<P>(f, (R)B.rv_tau, out, m);
+        stb_collide<P>(f, (R)B.rv_tau, out, m, p.sh);
         const long long c = (long long)j * B.pitch + i;
         if (p.write_macros && (p.macro_all || (fl & 8))) {
           ((R *)B.rho)[c] = m[0];
@@ -1211,7 +1251,7 @@ __device__ __forceinline__ void stb_quad_body(const StbParams &p, long long wt, 
       R fc[9], o[9], m[3];
 #pragma unroll
       for (int k = 0; k < 9; k++) fc[k] = f[k][q];
-      stb_collide<P>(fc, rv, o, m);
+      stb_collide<P>(fc, rv, o, m, p.sh);
 #pragma unroll
       for (int k = 0; k < 9; k++) f[k][q] = o[k];
       if (p.write_macros && (p.macro_all || ((fl4 >> (8 * q)) & 8u))) {
@@ -1290,6 +1330,7 @@ struct RecOpsParams {
   void *slots;
   const uint8_t *mask;
   double tw[4][3];
+  Sh9 sh;  // shift of the stored words
 };
 static_assert(sizeof(RecOpsParams) <= 4096, "record launch parameters must fit the 4 KB parameter space");
 
@@ -1344,7 +1385,7 @@ __device__ __forceinline__ void rec_point(const RecOpsParams &p, int t) {
     const uint8_t live = mp ? *mp : op.bits;
     if (live & 4) {
 #pragma unroll
-      for (int k = 0; k < 9; k++) st_f<P>(Fd, k * D.plane + dc, k, v[k]);
+      for (int k = 0; k < 9; k++) st_f<P>(Fd, k * D.plane + dc, k, v[k], p.sh);
     }
     return;
   }
@@ -1357,12 +1398,12 @@ __device__ __forceinline__ void rec_point(const RecOpsParams &p, int t) {
     const R *sv = (const R *)p.slots + (long long)op.sstride * 27 + op.m2 * 9;
 #pragma unroll
     for (int k = 0; k < 9; k++) {  // the stored form's rounding, as st_f then ld_f
-      if constexpr (Prec<P>::shifted) ft[k] = to_r(from_r<S>(sv[k] - wk<P>(k))) + wk<P>(k);
+      if constexpr (Prec<P>::shifted) ft[k] = to_r(from_r<S>(sv[k] - p.sh.s[k])) + p.sh.s[k];
       else ft[k] = to_r(from_r<S>(sv[k]));
     }
   } else {
 #pragma unroll
-    for (int k = 0; k < 9; k++) ft[k] = ld_f<P>(Fs, k * Fb.plane + sc, k);
+    for (int k = 0; k < 9; k++) ft[k] = ld_f<P>(Fs, k * Fb.plane + sc, k, p.sh);
   }
   const uint8_t live = mp ? *mp : op.bits;
   if (live & 8) {
@@ -1375,7 +1416,7 @@ __device__ __forceinline__ void rec_point(const RecOpsParams &p, int t) {
 #pragma unroll
     for (int k = 0; k < 9; k++) {
       const R fe = feq<R>(k, rh, ux, uy);
-      st_f<P>(Fd, k * D.plane + dc, k, fe + para * (ft[k] - fe));
+      st_f<P>(Fd, k * D.plane + dc, k, fe + para * (ft[k] - fe), p.sh);
     }
   }
 }
@@ -1452,12 +1493,13 @@ struct SplParamsP {
   void *slots;
   const uint8_t *mask;
   const void *coef;  // per line: c'_i (Nc values) then 1/den_i (Nc values), at 2 * coef0
+  Sh9 sh;            // shift of the stored words
 };
 static_assert(sizeof(SplParamsP) <= 4096, "spline launch parameters must fit the 4 KB parameter space");
 
 // the 12 fields (rho, ux, uy, F0..F8) of coarse point ip
 template <int P>
-__device__ __forceinline__ void spl_gather_p(const SplTaskP &T, int ip, typename Prec<P>::R *v) {
+__device__ __forceinline__ void spl_gather_p(const SplTaskP &T, int ip, typename Prec<P>::R *v, const Sh9 &sh) {
   using R = typename Prec<P>::R;
   using S = typename Prec<P>::S;
   const long long c = (long long)(T.cj0 + ip * T.cdj) * T.cpitch + (T.ci0 + ip * T.cdi);
@@ -1466,7 +1508,7 @@ __device__ __forceinline__ void spl_gather_p(const SplTaskP &T, int ip, typename
   v[2] = ((const R *)T.Mc[2])[c];
   const S *F = (const S *)T.Fc;
 #pragma unroll
-  for (int k = 0; k < 9; k++) v[3 + k] = ld_f<P>(F, k * T.cplane + c, k);
+  for (int k = 0; k < 9; k++) v[3 + k] = ld_f<P>(F, k * T.cplane + c, k, sh);
 }
 
 // shared memory of one spline warp: the gathered fields, the forward sweep
@@ -1505,7 +1547,7 @@ __device__ __forceinline__ void spl_segment(const SplParamsP &p, int sid, int la
     for (int q = 0; q < 3; q++) {
       const int i = g0 + lane + 32 * q;
       if (i <= g1) {
-        spl_gather_p<P>(T, i, v[q]);
+        spl_gather_p<P>(T, i, v[q], p.sh);
         c0[q] = cpt[i];
         c1[q] = ivd[i];
       }
@@ -1523,7 +1565,7 @@ __device__ __forceinline__ void spl_segment(const SplParamsP &p, int sid, int la
   } else {
     for (int i = g0 + lane; i <= g1; i += 32) {
       R v[12];
-      spl_gather_p<P>(T, i, v);
+      spl_gather_p<P>(T, i, v, p.sh);
 #pragma unroll
       for (int f = 0; f < 12; f++) sfw[f][i - g0] = v[f];
       scw[0][i - g0] = cpt[i];
@@ -1586,7 +1628,8 @@ __device__ __forceinline__ void spl_segment(const SplParamsP &p, int sid, int la
       typename Prec<P>::S *Fd = (typename Prec<P>::S *)T.Ft;
 #pragma unroll
       for (int k = 0; k < 9; k++)
-        st_f<P>(Fd, k * T.fplane + fc, k, temporal3<R>(a, b, cc, s3[T.tm[0] * 9 + k], s3[T.tm[1] * 9 + k], s3[T.tm[2] * 9 + k]));
+        st_f<P>(Fd, k * T.fplane + fc, k, temporal3<R>(a, b, cc, s3[T.tm[0] * 9 + k], s3[T.tm[1] * 9 + k], s3[T.tm[2] * 9 + k]),
+                p.sh);
     }
   }
 }
@@ -2061,6 +2104,7 @@ struct DragParams {
   long long plane;
   double feqc[9];
   double *out;  // Fx, Fy
+  Sh9 sh;       // shift of the stored words
 };
 
 // one CTA of 256 threads: it finds a free slot among the bulk work's CTAs as
@@ -2079,13 +2123,13 @@ __global__ void __launch_bounds__(DRAG_THREADS) k_drag(const __grid_constant__ D
 #pragma unroll
     for (int q = 0; q < 9; q++)
       if (q == k) { kd = opp(q); ek = ex(q); eky = ey(q); ekd = ex(opp(q)); ekdy = ey(opp(q)); }
-    const double fs = (double)ld_f<P>(F, (long long)k * p.plane + L.cell_f, k);
+    const double fs = (double)ld_f<P>(F, (long long)k * p.plane + L.cell_f, k, p.sh);
     // returning value: feq(rho0, U0) at a block-edge FLUID cell (bit 0), the
     // outgoing value itself at a half-way wall (bit 1), else the on-node
     // wall's F_opp
     const double ff = (L.fluid_edge & 1) ? p.feqc[kd]
                       : (L.fluid_edge & 2) ? fs
-                                           : (double)ld_f<P>(F, (long long)kd * p.plane + L.cell_s, kd);
+                                           : (double)ld_f<P>(F, (long long)kd * p.plane + L.cell_s, kd, p.sh);
     fx += fs * ek - ff * ekd;
     fy += fs * eky - ff * ekdy;
   }
@@ -2238,12 +2282,12 @@ __global__ void __launch_bounds__(256) k_error_l2(const __grid_constant__ L2Para
 // multi/init_multi.h:3-28): every slot of fine point ip holds F at that point.
 template <int P>
 __global__ void k_slots_from_edge(const typename Prec<P>::S *F, long long plane, int fi0, int fj0, int fdi, int fdj,
-                                  int pitch, int Nf, typename Prec<P>::R *slots, int slot0) {
+                                  int pitch, int Nf, typename Prec<P>::R *slots, int slot0, const Sh9 sh) {
   for (int ip = blockIdx.x * blockDim.x + threadIdx.x; ip < Nf; ip += gridDim.x * blockDim.x) {
     const long long cell = (long long)(fj0 + ip * fdj) * pitch + (fi0 + ip * fdi);
 #pragma unroll
     for (int k = 0; k < 9; k++) {
-      const typename Prec<P>::R v = ld_f<P>(F, k * plane + cell, k);
+      const typename Prec<P>::R v = ld_f<P>(F, k * plane + cell, k, sh);
       for (int q = 0; q < 3; q++) slots[((long long)(slot0 + ip) * 3 + q) * 9 + k] = v;
     }
   }
@@ -2260,18 +2304,18 @@ __global__ void k_fill(T *p, long long n, T v) {
 
 template <int P>
 __global__ void k_fill_planes(typename Prec<P>::S *F, long long plane, double f0, double f1, double f2, double f3,
-                              double f4, double f5, double f6, double f7, double f8) {
+                              double f4, double f5, double f6, double f7, double f8, const Sh9 sh) {
   const double fv[9] = {f0, f1, f2, f3, f4, f5, f6, f7, f8};
   for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < 9 * plane;
        g += (long long)gridDim.x * blockDim.x) {
     const int k = int(g / plane);
-    st_f<P>(F, g, k, (typename Prec<P>::R)fv[k]);
+    st_f<P>(F, g, k, (typename Prec<P>::R)fv[k], sh);
   }
 }
 
 template <int P>
 __global__ void k_count_nonfinite(const typename Prec<P>::S *F, long long plane, const uint8_t *flags, int nx,
-                                  int ny, int pitch, unsigned long long *count) {
+                                  int ny, int pitch, unsigned long long *count, const Sh9 sh) {
   unsigned long long bad = 0;
   const long long n = (long long)nx * ny;
   for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += (long long)gridDim.x * blockDim.x) {
@@ -2282,7 +2326,7 @@ __global__ void k_count_nonfinite(const typename Prec<P>::S *F, long long plane,
       if constexpr (std::is_same<typename Prec<P>::S, h16c>::value) {
         if ((F[k * plane + c].x & 0x7fffu) == 0x7fffu) bad++;  // saturated: out of range, Inf or NaN
       } else {
-        const double v = (double)ld_f<P>(F, k * plane + c, k);
+        const double v = (double)ld_f<P>(F, k * plane + c, k, sh);
         if (!isfinite(v)) bad++;
       }
     }
@@ -2292,23 +2336,25 @@ __global__ void k_count_nonfinite(const typename Prec<P>::S *F, long long plane,
 
 // pitched device planes <-> dense FP64 staging buffer
 template <int P>
-__global__ void k_planes_to_f64(const typename Prec<P>::S *F, long long plane, int nx, int ny, int pitch, double *out) {
+__global__ void k_planes_to_f64(const typename Prec<P>::S *F, long long plane, int nx, int ny, int pitch, double *out,
+                                const Sh9 sh) {
   const long long n = (long long)nx * ny;
   for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < 9 * n; g += (long long)gridDim.x * blockDim.x) {
     const int k = int(g / n);
     const long long r = g - k * n;
     const int j = int(r / nx), i = int(r - (long long)j * nx);
-    out[g] = (double)ld_f<P>(F, k * plane + (long long)j * pitch + i, k);
+    out[g] = (double)ld_f<P>(F, k * plane + (long long)j * pitch + i, k, sh);
   }
 }
 template <int P>
-__global__ void k_f64_to_planes(typename Prec<P>::S *F, long long plane, int nx, int ny, int pitch, const double *in) {
+__global__ void k_f64_to_planes(typename Prec<P>::S *F, long long plane, int nx, int ny, int pitch, const double *in,
+                                const Sh9 sh) {
   const long long n = (long long)nx * ny;
   for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < 9 * n; g += (long long)gridDim.x * blockDim.x) {
     const int k = int(g / n);
     const long long r = g - k * n;
     const int j = int(r / nx), i = int(r - (long long)j * nx);
-    st_f<P>(F, k * plane + (long long)j * pitch + i, k, (typename Prec<P>::R)in[g]);
+    st_f<P>(F, k * plane + (long long)j * pitch + i, k, (typename Prec<P>::R)in[g], sh);
   }
 }
 template <typename R>

@@ -40,6 +40,11 @@ size_t prec_bytes(int prec) {
   return prec == MB_PREC_F64 ? 8 : ((prec == MB_PREC_F16S || prec == MB_PREC_F16C) ? 2 : 4);
 }
 size_t real_bytes(int prec) { return prec == MB_PREC_F64 ? 8 : 4; }
+bool prec_shifted(int prec) { return prec == MB_PREC_F32 || prec == MB_PREC_F16S || prec == MB_PREC_F16C; }
+// FP32 storage subtracts the free stream's equilibrium (its stored words are
+// then small wherever the flow is near the free stream); the 16-bit forms
+// keep f - w
+int default_shift(int prec) { return prec == MB_PREC_F32 ? MB_SHIFT_FEQ0 : MB_SHIFT_W; }
 
 // One part of error_L2 (interiors of split levels, or every other cell) as
 // boxes in device memory.
@@ -175,6 +180,8 @@ struct mb_ctx {
   int spl_cta_smem = 96 * 1024;
   int rec_cta_smem = 0;
   int bulk_cta_smem = 0;  // unused shared memory reserved by each bulk (interior) block-step CTA
+  int shift_mode = MB_SHIFT_W;  // stored words h = f - s: s = w, or feq(rho0, U0)
+  Shift shift{};
   PrgTraceRec *d_trace = nullptr;       // executor trace (mb_set_program_trace)
   unsigned int *d_trace_n = nullptr;
   unsigned int trace_cap = 0;
@@ -185,6 +192,44 @@ struct mb_ctx {
 };
 
 namespace {
+
+// The shift of a context's stored words and the collision's constants for it
+// (kernels.cuh, Shift): s = w (rho_s = 1, U_s = 0) or s = feq(rho0, U0) of
+// the configuration.  Precisions that store f itself get s = 0.
+Shift make_shift(const mb_ctx *c, int mode) {
+  Shift sh{};
+  if (!prec_shifted(c->prec)) {
+    sh.sym = 1;
+    return sh;
+  }
+  const mb_config &cfg = c->geo.config;
+  const double rs = mode == MB_SHIFT_FEQ0 ? cfg.rho0 : 1.0;
+  const double ux = mode == MB_SHIFT_FEQ0 ? cfg.U0[0] : 0.0, uy = mode == MB_SHIFT_FEQ0 ? cfg.U0[1] : 0.0;
+  const double uv = ux * ux + uy * uy;
+  double sd[9];
+  for (int k = 0; k < 9; k++) {
+    const double eu = ex(k) * ux + ey(k) * uy;
+    sd[k] = wd(k) * rs * (1.0 + 3.0 * eu + 4.5 * eu * eu - 1.5 * uv);
+    sh.v.s[k] = (float)sd[k];
+  }
+  // c_k = w_k (rho_s + 3 e_k.J_s) - s_k = -w_k rho_s (4.5 (e_k.U_s)^2 - 1.5 |U_s|^2), per pair
+  const int rep[5] = {0, 1, 2, 5, 8};
+  for (int q = 0; q < 5; q++) {
+    const int k = rep[q];
+    const double eu = ex(k) * ux + ey(k) * uy;
+    sh.c[q] = (float)(-wd(k) * rs * (4.5 * eu * eu - 1.5 * uv));
+  }
+  sh.rhos = (float)rs;
+  sh.jx = (float)(rs * ux);
+  sh.jy = (float)(rs * uy);
+  sh.q2 = (float)(rs * uv);
+  sh.qd = (float)(rs * (ux * ux - uy * uy));
+  sh.qx = (float)(rs * ux * uy);
+  sh.sym = 1;
+  for (int k = 0; k < 9; k++)
+    if (sh.v.s[k] != sh.v.s[opp(k)] || sh.v.s[k] != sh.v.s[slip(k)]) sh.sym = 0;
+  return sh;
+}
 
 // Runs STMT with P bound to the runtime precision and S to its storage type.
 #define MB_DISPATCH(prec, STMT)                                     \
@@ -340,6 +385,7 @@ StbParams make_stb(mb_ctx *c, int a0, int a1, uint64_t parity, int macro_all, in
   p.write_macros = write_macros;
   p.region = region;
   for (int k = 0; k < 9; k++) p.feqc[k] = c->feqc[k];
+  p.sh = c->shift;
   p.rho0 = c->geo.config.rho0;
   p.u0x = c->geo.config.U0[0];
   p.u0y = c->geo.config.U0[1];
@@ -594,6 +640,7 @@ int lower_plan(mb_ctx *c, CompiledPlan &cp) {
       d.drag.F = B.F[((n.parity >> a) & 1) ^ 1];  // the buffer the block's last step read
       d.drag.plane = B.plane;
       for (int k = 0; k < 9; k++) d.drag.feqc[k] = c->feqc[k];
+      d.drag.sh = c->shift.v;
       d.drag.out = cp.d_diag_res + DIAG_STRIDE * n.level;
       d.func = kfunc<KDrag>(c->prec);
       d.block = dim3(DRAG_THREADS);
@@ -659,6 +706,7 @@ int lower_plan(mb_ctx *c, CompiledPlan &cp) {
       if (!mask.empty()) MB_CUDA(cudaMemcpy(dm, mask.data(), mask.size(), cudaMemcpyHostToDevice));
       d.rec.mask = dm;
       d.rec.slots = c->d_slots;
+      d.rec.sh = c->shift.v;
       std::memcpy(d.rec.tw, n.tw, sizeof(n.tw));
       for (int a = 0; a < c->nblk; a++) {
         const IfBlk &B = c->blk[a];
@@ -712,6 +760,7 @@ int lower_plan(mb_ctx *c, CompiledPlan &cp) {
       d.spl.mask = dm;
       d.spl.slots = c->d_slots;
       d.spl.coef = c->d_spl_coef;
+      d.spl.sh = c->shift.v;
       d.func = kfunc<KSpl>(c->prec);
       d.block = dim3(32 * c->spl_segs);
       d.grid = dim3((unsigned)((nseg + c->spl_segs - 1) / c->spl_segs));
@@ -1121,6 +1170,8 @@ extern "C" int mb_create(const mb_geometry *geo, int precision, mb_ctx **out) {
     const double uv = cfg.U0[0] * cfg.U0[0] + cfg.U0[1] * cfg.U0[1];
     c->feqc[k] = wd(k) * cfg.rho0 * (1.0 + 3.0 * eu + 4.5 * eu * eu - 1.5 * uv);
   }
+  c->shift_mode = default_shift(precision);
+  c->shift = make_shift(c.get(), c->shift_mode);
 
   // block layouts and flags
   c->bl.resize(c->nblk);
@@ -1381,6 +1432,17 @@ extern "C" int mb_set_split_cells(mb_ctx *c, long long cells) {
   cudaDeviceSynchronize();
   c->split_cells = cells;
   c->plans.clear();
+  return MB_OK;
+}
+
+extern "C" int mb_set_shift(mb_ctx *c, int mode) {
+  if (!c || (mode != MB_SHIFT_W && mode != MB_SHIFT_FEQ0)) return MB_ERR_INVALID;
+  if (mode == c->shift_mode) return MB_OK;
+  cudaDeviceSynchronize();
+  c->plans.clear();
+  c->shift_mode = mode;
+  c->shift = make_shift(c, mode);
+  c->inited = false;  // the stored words mean something else now: mb_init (or a restore) comes next
   return MB_OK;
 }
 
@@ -1648,7 +1710,7 @@ extern "C" int mb_init(mb_ctx *c, mb_stream stream) {
       const int gr = launch_grid(9 * n, th);
       const double *f = c->feqc;
       MB_DISPATCH(c->prec, (k_fill_planes<P><<<gr, th, 0, s>>>((S *)B.F[q], n, f[0], f[1], f[2], f[3], f[4], f[5],
-                                                               f[6], f[7], f[8])));
+                                                               f[6], f[7], f[8], c->shift.v)));
     }
     const int gr = launch_grid(n, th);
     if (c->prec == MB_PREC_F64) {
@@ -1697,7 +1759,7 @@ extern "C" int mb_sync_history(mb_ctx *c, mb_stream stream) {
     const void *F = B.F[c->state.parity[L.fine]];
     MB_DISPATCH(c->prec, (k_slots_from_edge<P><<<(L.Nf + 127) / 128, 128, 0, s>>>(
                              (const S *)F, B.plane, L.fi0, L.fj0, L.fdi, L.fdj, B.pitch, L.Nf,
-                             (typename Prec<P>::R *)c->d_slots, L.slot0)));
+                             (typename Prec<P>::R *)c->d_slots, L.slot0, c->shift.v)));
   }
   const size_t rb = real_bytes(c->prec);
   for (int a = 0; a < c->nblk; a++) {
@@ -1915,6 +1977,7 @@ int launch_drag(mb_ctx *c, double *out, cudaStream_t s) {
   p.F = B.F[c->state.parity[a] ^ 1];
   p.plane = B.plane;
   for (int k = 0; k < 9; k++) p.feqc[k] = c->feqc[k];
+  p.sh = c->shift.v;
   p.out = out;
   void *args[] = {&p};
   MB_CUDA(cudaLaunchKernel(kfunc<KDrag>(c->prec), dim3(1), dim3(DRAG_THREADS), args, 0, s));
@@ -2047,7 +2110,7 @@ extern "C" int mb_check_finite(mb_ctx *c, long long *bad, mb_stream stream) {
     const void *F = B.F[c->state.parity[a]];
     const int gr = launch_grid((long long)B.nx * B.ny, 256);
     MB_DISPATCH(c->prec, (k_count_nonfinite<P><<<gr, 256, 0, s>>>((const S *)F, B.plane, B.flags, B.nx, B.ny, B.pitch,
-                                                                    c->d_count)));
+                                                                    c->d_count, c->shift.v)));
   }
   unsigned long long h = 0;
   MB_CUDA(cudaMemcpyAsync(&h, c->d_count, sizeof(h), cudaMemcpyDeviceToHost, s));
@@ -2082,7 +2145,8 @@ extern "C" int mb_copy_fields(mb_ctx *c, int a, double *rho, double *ux, double 
   const int gr = launch_grid(9 * n, 256);
   if (F) {
     const void *Fs = B.F[c->state.parity[a]];
-    MB_DISPATCH(c->prec, (k_planes_to_f64<P><<<gr, 256, 0, s>>>((const S *)Fs, B.plane, B.nx, B.ny, B.pitch, c->d_stage)));
+    MB_DISPATCH(c->prec,
+                (k_planes_to_f64<P><<<gr, 256, 0, s>>>((const S *)Fs, B.plane, B.nx, B.ny, B.pitch, c->d_stage, c->shift.v)));
     MB_CUDA(cudaMemcpyAsync(F, c->d_stage, 9 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
   }
   void *M[3] = {B.rho, B.ux, B.uy};
@@ -2118,7 +2182,8 @@ extern "C" int mb_set_fields(mb_ctx *c, int a, const double *rho, const double *
   if (F) {
     MB_CUDA(cudaMemcpyAsync(c->d_stage, F, 9 * n * sizeof(double), cudaMemcpyHostToDevice, s));
     void *Fd = B.F[c->state.parity[a]];
-    MB_DISPATCH(c->prec, (k_f64_to_planes<P><<<gr, 256, 0, s>>>((S *)Fd, B.plane, B.nx, B.ny, B.pitch, c->d_stage)));
+    MB_DISPATCH(c->prec,
+                (k_f64_to_planes<P><<<gr, 256, 0, s>>>((S *)Fd, B.plane, B.nx, B.ny, B.pitch, c->d_stage, c->shift.v)));
   }
   void *M[3] = {B.rho, B.ux, B.uy};
   const double *H[3] = {rho, ux, uy};
@@ -2181,7 +2246,7 @@ extern "C" int mb_checkpoint_save(mb_ctx *c, void *host, long long bytes, mb_str
   CkptHeader h{};
   std::memcpy(h.magic, "MBLBMCK1", 8);
   h.version = 1;
-  h.precision = c->prec;
+  h.precision = c->prec | (c->shift_mode << 8);  // the stored words depend on both
   h.nblk = c->nblk;
   h.nline = c->geo.layout.number_line;
   h.slot_points = c->n_slot_points;
@@ -2219,7 +2284,7 @@ extern "C" int mb_checkpoint_load(mb_ctx *c, const void *host, long long bytes, 
   const unsigned char *o = (const unsigned char *)host;
   CkptHeader h;
   std::memcpy(&h, o, sizeof h);
-  if (std::memcmp(h.magic, "MBLBMCK1", 8) || h.version != 1 || h.precision != c->prec || h.nblk != c->nblk ||
+  if (std::memcmp(h.magic, "MBLBMCK1", 8) || h.version != 1 || h.precision != (c->prec | (c->shift_mode << 8)) || h.nblk != c->nblk ||
       h.nline != c->geo.layout.number_line || h.slot_points != c->n_slot_points ||
       h.geo_hash != fnv1a(&c->geo, sizeof(c->geo)) || bytes < (long long)ckpt_bytes(c))
     return MB_ERR_INVALID;

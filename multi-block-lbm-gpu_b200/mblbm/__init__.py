@@ -27,6 +27,7 @@ PREC_F64, PREC_F32, PREC_F16S, PREC_F32U, PREC_F16C = 0, 1, 2, 3, 4
 # f16s: IEEE FP16 storage of f - w; f16c: 16-bit storage of f - w with a
 # 3-bit exponent and 12-bit fraction (a quarter of FP16's spacing for |f - w| < 1/4)
 PRECISIONS = {"f64": PREC_F64, "f32": PREC_F32, "f16s": PREC_F16S, "f32u": PREC_F32U, "f16c": PREC_F16C}
+SHIFT_W, SHIFT_FEQ0 = 0, 1  # mb_set_shift modes
 FLUID, SOLID_SBB, C_BOUNDARY = 0, 1, 9
 OBST_CIRCLE, OBST_ELLIPSE, OBST_NONE = 0, 1, 2
 PERIODIC_X, PERIODIC_Y, DIR_PERIODIC = 1, 2, 8  # mb_config.periodic bits, NeborCC code of ghost lines
@@ -182,6 +183,7 @@ SIGNATURES = {
     "mb_prepare": ([_vp, C.c_int], C.c_int),
     "mb_prepare_diag": ([_vp, C.c_int], C.c_int),
     "mb_set_bulk_spread": ([_vp, C.c_int], C.c_int),
+    "mb_set_shift": ([_vp, C.c_int], C.c_int),
     "mb_plan_describe": ([_vp, C.c_int, C.c_char_p, C.c_longlong, _pll], C.c_int),
     "mb_block_step": ([_vp, C.c_int, _vp], C.c_int),
     "mb_c_c_boundary_transfer": ([_vp, C.c_int, _vp], C.c_int),
@@ -467,10 +469,12 @@ def _stream_ptr(stream):
 class MultiBlockLBM:
     """One multi-block simulation on the current CUDA device."""
 
-    def __init__(self, geo, precision="f32", graph=True):
+    def __init__(self, geo, precision="f32", graph=True, shift=None):
         """graph: False launches kernels one by one, True replays CUDA graphs,
         "pdl" replays graphs with programmatic kernel-to-kernel edges,
-        "program" runs each plan as one persistent executor launch."""
+        "program" runs each plan as one persistent executor launch.
+        shift: "w" or "feq0" for the stored distributions of the shifted
+        precisions (None: the precision's default, feq0 for f32, w otherwise)."""
         self.lib = load()
         self.geo = geo
         self.precision = precision
@@ -480,6 +484,8 @@ class MultiBlockLBM:
         mode = {"pdl": 2, "program": 3}.get(graph, 1 if graph else 0) if isinstance(graph, str) else (1 if graph else 0)
         if mode != 1:
             _check(self.lib.mb_set_graph_mode(self.h, mode), "mb_set_graph_mode")
+        if shift is not None:
+            _check(self.lib.mb_set_shift(self.h, {"w": SHIFT_W, "feq0": SHIFT_FEQ0}[shift]), "mb_set_shift")
         self.n = 0
 
     def close(self):

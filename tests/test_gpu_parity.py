@@ -429,3 +429,33 @@ def test_fused_tskip_options_kernel_bitwise(mb, cuda_device, prec, graph):
             for key in ("F", "rho", "ux", "uy"):
                 assert np.array_equal(fa[key], fb[key]), (k, key)
         assert sims[0].getDrag_block()[2] == other.getDrag_block()[2]
+
+
+@pytest.mark.parametrize("prec", ["f32", "f16c"])
+def test_shift_modes(mb, orc, cuda_device, prec):
+    """Both shifts of the stored words (f - w and f - feq(rho0, U0)) give the
+    scheme: every field within the precision's bound of the FP64 oracle after
+    300 steps of the 3-level nested layout; a checkpoint of one shift does not
+    load into a context of the other."""
+    g = mb.geo_init(*make_ref.case("n3")[:2])
+    o = orc.Oracle(g)
+    o.init()
+    o.evolution(300)
+    fo = all_fields(o, g)
+    tol = 2e-5 if prec == "f32" else 2e-3
+    ck = {}
+    for shift in ("w", "feq0"):
+        m = mb.MultiBlockLBM(g, prec, shift=shift)
+        m.init()
+        m.evolution(300)
+        fm = all_fields(m, g)
+        eu, er = rel_l2(g, fo, fm, "u"), rel_l2(g, fo, fm, "rho")
+        print(f"{prec} shift {shift}: relL2 u {eu:.3e} rho {er:.3e}")
+        assert eu <= tol and er <= tol
+        ck[shift] = m.checkpoint()
+        m.close()
+    other = mb.MultiBlockLBM(g, prec, shift="w")
+    with pytest.raises(mb.MBError):
+        other.restore(ck["feq0"])
+    other.restore(ck["w"])
+    other.close()
