@@ -252,8 +252,9 @@ int mb_set_split_cells(mb_ctx *ctx, long long cells);
 int mb_set_interface_shape(mb_ctx *ctx, int rec_points, int spline_segments);
 /* Unused shared memory (KB) reserved by every CTA of the bulk block-step
  * launches (the interiors of split levels): an SM then holds fewer of them at
- * once and keeps room for the latency-bound chain launches beside them
- * (0, the default: no reservation).  Results are identical. */
+ * once and keeps room for the latency-bound chain launches beside them.
+ * Defaults: 80 KB in FP32 storage (two CTAs of the level-0 interior per SM),
+ * 60 KB in the 16-bit forms (three), 0 in FP64.  Results are identical. */
 int mb_set_bulk_spread(mb_ctx *ctx, int kb);
 /* MB_SHIFT_W or MB_SHIFT_FEQ0 for the stored distributions (no effect on
  * MB_PREC_F64 and MB_PREC_F32U, which store f).  Changing it discards the
@@ -264,8 +265,8 @@ int mb_set_shift(mb_ctx *ctx, int mode);
  * the record kernels, which caps how many of their CTAs share one SM: a
  * latency-bound launch that starts while a block step still holds most SMs
  * then spreads over the SMs that free up instead of piling onto the first
- * ones.  Defaults 96 (spline: at most 2 CTAs per SM) and 0.  Results are
- * identical. */
+ * ones.  Defaults: spline 48 KB in FP32 storage, 64 KB in the 16-bit forms,
+ * 96 KB otherwise (at most 2 CTAs per SM); records 0.  Results are identical. */
 int mb_set_cta_spread(mb_ctx *ctx, int spline_kb, int records_kb);
 /* Splits exactly the levels whose bit is set in level_mask (bit l = level
  * l) into interior and rim nodes, overriding mb_set_split_cells; 0 returns
