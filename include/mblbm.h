@@ -46,20 +46,21 @@ extern "C" {
 
 /* ---- storage precisions of the distributions -------------------------- */
 #define MB_PREC_F64 0  /* FP64 storage and arithmetic (reference precision)     */
-#define MB_PREC_F32 1  /* FP32 storage of f - w (shifted), FP32 arithmetic      */
+#define MB_PREC_F32 1  /* FP32 storage of f - s (shifted, mb_set_shift), FP32 arithmetic */
 #define MB_PREC_F16S 2 /* FP16 storage of f - w (shifted), FP32 arithmetic      */
 #define MB_PREC_F32U 3 /* FP32 storage of f (unshifted), FP32 arithmetic        */
-/* 16-bit storage of f - w (shifted) with a 3-bit exponent and 12-bit
- * fraction: |f - w| below 1/4, a quarter of FP16's spacing there; FP32
- * arithmetic.  Out-of-range values saturate and mb_check_finite counts them. */
+/* 16-bit storage of the shifted distributions (default f - feq(rho0, U0))
+ * with a 3-bit exponent and 12-bit fraction: magnitudes below 1/4, a quarter
+ * of FP16's spacing there; FP32 arithmetic.  Out-of-range values saturate
+ * and mb_check_finite counts them. */
 #define MB_PREC_F16C 4
 
 /* ---- shift of the stored distributions (shifted precisions) ------------- */
 /* The shifted precisions store h = f - s with a constant vector s: the lattice
- * weights w (MB_SHIFT_W, the 16-bit forms' default), or the equilibrium of
- * the free stream feq(rho0, U0) (MB_SHIFT_FEQ0, FP32's default: the stored
- * words are then small wherever the flow is close to the free stream, and so
- * are their rounding errors). */
+ * weights w (MB_SHIFT_W, MB_PREC_F16S's default), or the equilibrium of the
+ * free stream feq(rho0, U0) (MB_SHIFT_FEQ0, the default of MB_PREC_F32 and
+ * MB_PREC_F16C: the stored words are then small wherever the flow is close
+ * to the free stream, and so are their rounding errors). */
 #define MB_SHIFT_W 0
 #define MB_SHIFT_FEQ0 1
 

@@ -279,22 +279,22 @@ __device__ __forceinline__ void collide_f32(const float *f, float rv, float *out
   out[0] = f[0] + rv * (g0 - f[0]);
   // the odd part 3 w e.(rho u) of a pair, from J_h when shifted (J_s cancels
   // against the shift's own odd part)
-  auto pair = [&](float a, float jo, float w, float cq, int kp, int km) {
+  auto pair = [&](float a, float o, float w, float cq, int kp, int km) {
     const float e = w * (base + rh * (4.5f * a * a - u15)) + cq;
-    const float o = w * (3.0f * jo);
     out[kp] = f[kp] + rv * ((e + o) - f[kp]);
     out[km] = f[km] + rv * ((e - o) - f[km]);
   };
   if (SHIFTED) {
-    pair(ux, jx, w1, sh.c[1], 1, 3);
-    pair(uy, jy, w1, sh.c[2], 2, 4);
-    pair(ux + uy, jx + jy, w5, sh.c[3], 5, 7);
-    pair(ux - uy, jx - jy, w5, sh.c[4], 8, 6);
+    pair(ux, w1 * (3.0f * jx), w1, sh.c[1], 1, 3);
+    pair(uy, w1 * (3.0f * jy), w1, sh.c[2], 2, 4);
+    pair(ux + uy, w5 * (3.0f * (jx + jy)), w5, sh.c[3], 5, 7);
+    pair(ux - uy, w5 * (3.0f * (jx - jy)), w5, sh.c[4], 8, 6);
   } else {
-    pair(ux, rh * ux, w1, 0.0f, 1, 3);
-    pair(uy, rh * uy, w1, 0.0f, 2, 4);
-    pair(ux + uy, rh * (ux + uy), w5, 0.0f, 5, 7);
-    pair(ux - uy, rh * (ux - uy), w5, 0.0f, 8, 6);
+    const float rh3 = 3.0f * rh;
+    pair(ux, w1 * (rh3 * ux), w1, 0.0f, 1, 3);
+    pair(uy, w1 * (rh3 * uy), w1, 0.0f, 2, 4);
+    pair(ux + uy, w5 * (rh3 * (ux + uy)), w5, 0.0f, 5, 7);
+    pair(ux - uy, w5 * (rh3 * (ux - uy)), w5, 0.0f, 8, 6);
   }
 }
 
