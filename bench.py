@@ -496,11 +496,12 @@ def run_forces_developed(args, geo):
     c = geo.config
     D, U0 = 2.0 * c.R, c.U0[0]
     out = {}
-    runs = [("f64", None), ("f32", None), ("f32", "w"), ("f16s", None), ("f16s", "feq0"), ("f16c", None),
-            ("f16c", "feq0")]
-    for prec, shift in runs:
-        name = prec if shift is None else f"{prec}_{shift}"
-        sim = mblbm.MultiBlockLBM(geo, prec, shift=shift)
+    runs = [("f64", None, None), ("f32", None, None), ("f32", "w", None), ("f16s", None, None),
+            ("f16s", "feq0", None), ("f16s", None, "nearest"), ("f16c", None, None), ("f16c", "w", None),
+            ("f16c", None, "nearest")]
+    for prec, shift, rounding in runs:
+        name = prec + ("" if shift is None else f"_{shift}") + {None: "", "nearest": "_rn", "stochastic": "_sr"}[rounding]
+        sim = mblbm.MultiBlockLBM(geo, prec, shift=shift, rounding=rounding)
         sim.init()
         for a, f in enumerate(state):
             sim.set_fields(a, f["rho"], f["ux"], f["uy"], f["F"])

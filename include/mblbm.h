@@ -64,6 +64,19 @@ extern "C" {
 #define MB_SHIFT_W 0
 #define MB_SHIFT_FEQ0 1
 
+/* ---- rounding of the stored words (mb_set_rounding) -------------------- */
+/* MB_ROUND_NEAREST: round to nearest even (every precision; the default of
+ * the FP64 and FP32 forms).
+ * MB_ROUND_STOCHASTIC (the 16-bit forms, their default): the
+ * collision rounds each output to one of its two neighbouring values of the
+ * stored type, the upper one with probability equal to the distance from the
+ * lower one over their spacing, so rounding errors have zero mean (FP16: the
+ * hardware's stochastic-rounding conversion).  The random bits are a hash of
+ * the cell and three of its inputs: every kernel variant and execution mode
+ * gives the same words. */
+#define MB_ROUND_NEAREST 0
+#define MB_ROUND_STOCHASTIC 1
+
 /* ---- cell type codes, values as in lbm/lbm.h:26-32 -------------------- */
 #define MB_FLUID 0
 #define MB_SOLID_SBB 1
@@ -257,11 +270,31 @@ int mb_set_interface_shape(mb_ctx *ctx, int rec_points, int spline_segments);
  * Defaults: 80 KB in FP32 storage (two CTAs of the level-0 interior per SM),
  * 60 KB in the 16-bit forms (three), 0 in FP64.  Results are identical. */
 int mb_set_bulk_spread(mb_ctx *ctx, int kb);
+/* Sets aside up to mb MB of L2 (capped by the device's persisting maximum and
+ * by the size of the fine levels' state) for persisting lines, and gives
+ * every graph kernel except the bulk interiors an access-policy window over
+ * one allocation that holds F and rho/u of the blocks with m > 1 and the
+ * interface slots: the fine levels' chain then finds its lines in L2 while
+ * the level-0 interior streams beside it.  0 (the default) releases it.  The
+ * set-aside is a limit of the calling process's CUDA context, restored to 0
+ * by mb_destroy.  Results are identical. */
+int mb_set_l2_persist(mb_ctx *ctx, int mb);
+/* Coarse steps per replayed CUDA graph (default 24, rounded up to a whole
+ * number of scheduler periods; 1 to 4096): a call of n steps replays plans of
+ * that length and one plan of the remaining steps.  Longer plans have fewer
+ * graph boundaries, across which the next step's level-0 interior cannot
+ * start beside the fine levels' chain, and cost more host time to compile
+ * once (mb_prepare).  Results are identical. */
+int mb_set_plan_steps(mb_ctx *ctx, int n);
 /* MB_SHIFT_W or MB_SHIFT_FEQ0 for the stored distributions (no effect on
  * MB_PREC_F64 and MB_PREC_F32U, which store f).  Changing it discards the
  * state: mb_init, mb_set_fields or a checkpoint of the same shift must come
  * next (mb_step returns MB_ERR_STATE until then). */
 int mb_set_shift(mb_ctx *ctx, int mode);
+/* MB_ROUND_NEAREST or MB_ROUND_STOCHASTIC (MB_PREC_F16C and MB_PREC_F16S,
+ * else MB_ERR_INVALID) for the words the collision stores.  The state is
+ * kept. */
+int mb_set_rounding(mb_ctx *ctx, int mode);
 /* Minimum dynamic shared memory (KB, at most 200) per CTA of the spline and
  * the record kernels, which caps how many of their CTAs share one SM: a
  * latency-bound launch that starts while a block step still holds most SMs

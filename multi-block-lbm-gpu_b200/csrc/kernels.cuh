@@ -63,7 +63,7 @@ struct Shift {
   float rhos, jx, jy; // rho_s, J_s
   float q2, qd, qx;   // rho_s |U_s|^2, rho_s (Usx^2 - Usy^2), rho_s Usx Usy (MRT)
   int sym;            // s_k = s_opp(k) = s_slip(k): walls move stored words unchanged
-  int pad_;
+  int sr;             // h16c: the collision rounds its outputs to the stored grid stochastically
 };
 
 // stored word <-> arithmetic type
@@ -96,6 +96,33 @@ __device__ __forceinline__ unsigned int h16c_encode(float v) {
   return r | ((b >> 16) & 0x8000u);
 }
 __device__ __forceinline__ float to_r(h16c h) { return h16c_decode(h.x); }
+// Random word of a cell for stochastic rounding: a hash of the cell's
+// identity (block index and position) and of three of its inputs, whose low
+// bits change whenever the state of the cell or its neighbours does; so the
+// dither is the same in every kernel variant and execution mode.  Two
+// multiply-xorshift rounds mix it.
+__device__ __forceinline__ unsigned int sr_seed(unsigned int key, const float *f) {
+  unsigned int h = key * 0x9E3779B1u + __float_as_uint(f[0]);
+  h = (h ^ (h >> 15)) * 0x2C1B3C6Du;
+  h += __float_as_uint(f[5]) ^ __float_as_uint(f[7]);
+  h = (h ^ (h >> 12)) * 0x297A2D39u;
+  return h ^ (h >> 15);
+}
+// odd multipliers that spread a cell's random word over its outputs
+__host__ __device__ constexpr unsigned int sr_mul(int q) {
+  return q == 0 ? 0x9E3779B1u : q == 1 ? 0x85EBCA77u : q == 2 ? 0xC2B2AE3Du : q == 3 ? 0x27D4EB2Fu
+       : q == 4 ? 0x165667B1u : q == 5 ? 0xD3A2646Du : q == 6 ? 0xFD7046C5u : q == 7 ? 0xB55A4F09u : 0x2C1B3C6Du;
+}
+// v rounded to one of its two neighbouring h16c values, the upper one with
+// probability (v - lower) / (upper - lower): the 11 dropped fraction bits get
+// the 11 low bits of r added before truncation.  Returns the code's value.
+__device__ __forceinline__ float h16c_round_sr(float v, unsigned int r) {
+  const unsigned int b = __float_as_uint(v * 0x1p-117f);
+  const unsigned int mag = b & 0x7fffffffu;
+  unsigned int c = mag >= 0x7f800000u ? 0x7fffu : (mag + (r & 0x7ffu)) >> 11;
+  c = c < 0x7fffu ? c : 0x7fffu;
+  return h16c_decode(c | ((b >> 16) & 0x8000u));
+}
 template <> __device__ __forceinline__ h16c from_r<h16c>(float v) { return h16c{(unsigned short)h16c_encode(v)}; }
 template <> __device__ __forceinline__ h16c from_r<h16c>(double v) { return from_r<h16c>((float)v); }
 
@@ -191,7 +218,7 @@ struct StbBlk {
   void *Fout;
   void *rho, *ux, *uy;
   const uint8_t *flags;
-  int nx, ny, pitch, pad_;
+  int nx, ny, pitch, gid;  // gid: the block's index in its context
   long long plane;
   long long cell0;  // first linear cell index of this block in the launch (per-cell kernel)
   double rv_tau;
@@ -214,6 +241,10 @@ struct StbBlk {
   int pad2_;
   double dt;          // 1 / m: time step of the block in coarse units (body-force term)
 };
+// a cell's identity for the stochastic rounding of h16c: block index and cell
+__device__ __forceinline__ unsigned int cell_key(const StbBlk &B, int i, int j) {
+  return (unsigned int)B.gid * 0x01000193u + (unsigned int)(j * B.nx + i);
+}
 
 // One same-level copy run beside the block step (k_cc_pull).
 struct CcEntry {
@@ -304,10 +335,34 @@ __device__ __forceinline__ void collide_f32(const float *f, float rv, float *out
 // reference's expressions as written; FP32 arithmetic uses collide_f32.
 template <int P>
 __device__ __forceinline__ void stb_collide(const typename Prec<P>::R *f, typename Prec<P>::R rv,
-                                            typename Prec<P>::R *out, typename Prec<P>::R *m, const Shift &sh) {
+                                            typename Prec<P>::R *out, typename Prec<P>::R *m, const Shift &sh,
+                                            unsigned int key = 0u) {
   using R = typename Prec<P>::R;
   if constexpr (sizeof(R) == 4) {
     collide_f32<Prec<P>::shifted>(f, rv, out, m, sh);
+    // stochastic rounding: each output is rounded here to a value of the
+    // stored type, which the store then encodes exactly
+    if constexpr (P == MB_PREC_F16C) {
+      if (sh.sr) {
+        const unsigned int h = sr_seed(key, f);
+#pragma unroll
+        for (int k = 0; k < 9; k++) out[k] = h16c_round_sr(out[k], (h * sr_mul(k)) >> 21);
+      }
+    }
+    if constexpr (P == MB_PREC_F16S) {
+      if (sh.sr) {  // the hardware's stochastic rounding to FP16, two values per instruction
+        const unsigned int h = sr_seed(key, f);
+#pragma unroll
+        for (int q = 0; q < 5; q++) {
+          unsigned int r = h * sr_mul(q);
+          r ^= r >> 16;
+          unsigned int d;
+          asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(out[2 * q]), "f"(q < 4 ? out[2 * q + 1] : 0.0f), "r"(r));
+          out[2 * q] = __half2float(__ushort_as_half((unsigned short)(d >> 16)));
+          if (q < 4) out[2 * q + 1] = __half2float(__ushort_as_half((unsigned short)(d & 0xffffu)));
+        }
+      }
+    }
   } else {
     R rh = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8];
     R ux = f[1] - f[3] + f[5] - f[6] - f[7] + f[8];
@@ -376,7 +431,7 @@ __device__ __forceinline__ void stb_finish_at(const StbParams &p, const StbBlk &
 #pragma unroll
     for (int k = 0; k < 9; k++) f[k] = to_r(raw[k]);
     R out[9], m[3];
-    stb_collide<P>(f, (R)B.rv_tau, out, m, p.sh);
+    stb_collide<P>(f, (R)B.rv_tau, out, m, p.sh, cell_key(B, i, j));
     if (wm) {
       st_ef<EF>((R *)D.rho + cd, m[0]);
       st_ef<EF>((R *)D.ux + cd, m[1]);
@@ -439,7 +494,7 @@ __device__ __forceinline__ void stb_finish(const StbParams &p, const StbBlk &B, 
 #pragma unroll
     for (int k = 0; k < 9; k++) f[k] = to_r(raw[k]);
     R out[9], m[3];
-    stb_collide<P>(f, (R)B.rv_tau, out, m, p.sh);
+    stb_collide<P>(f, (R)B.rv_tau, out, m, p.sh, cell_key(B, i, j));
     if (wm) {
       st_ef<EF>((R *)B.rho + c, m[0]);
       st_ef<EF>((R *)B.ux + c, m[1]);
@@ -755,7 +810,7 @@ __device__ __forceinline__ void stbx_cell(const StbParams &p, const StbBlk &B, i
     }
     R out[9], m[3];
     if (p.opt.coll == MB_COLL_MRT) mrt_collide<P>(f, rv, p.opt, out, m, p.sh);
-    else stb_collide<P>(f, rv, out, m, p.sh);
+    else stb_collide<P>(f, rv, out, m, p.sh, cell_key(B, i, j));
     if (p.opt.has_force) {
 #pragma unroll
       for (int k = 0; k < 9; k++) out[k] += dt * force_k<R>(k, m[1], m[2], fx, fy, rv);
@@ -833,7 +888,7 @@ __device__ __forceinline__ void stb_cell_rows(const StbParams &p, const StbBlk &
 #pragma unroll
       for (int k = 0; k < 9; k++) f[k] = to_r(raw[k]);
       R out[9], m[3];
-      stb_collide<P>(f, (R)B.rv_tau, out, m, p.sh);
+      stb_collide<P>(f, (R)B.rv_tau, out, m, p.sh, cell_key(B, i, j));
       if (p.write_macros && (p.macro_all || (fl & 8))) {
         st_ef<EF>((R *)B.rho + c, m[0]);
         st_ef<EF>((R *)B.ux + c, m[1]);
@@ -922,10 +977,10 @@ __device__ __forceinline__ void stb_pair(const StbParams &p, const StbBlk &B, in
       R f[9], oa[9], ob[9], ma[3], mb[3];
 #pragma unroll
       for (int k = 0; k < 9; k++) f[k] = to_r(a[k]);
-      stb_collide<P>(f, (R)B.rv_tau, oa, ma, p.sh);
+      stb_collide<P>(f, (R)B.rv_tau, oa, ma, p.sh, cell_key(B, i, j));
 #pragma unroll
       for (int k = 0; k < 9; k++) f[k] = to_r(b[k]);
-      stb_collide<P>(f, (R)B.rv_tau, ob, mb, p.sh);
+      stb_collide<P>(f, (R)B.rv_tau, ob, mb, p.sh, cell_key(B, i + 1, j));
       if (p.write_macros) {
         const bool wa = p.macro_all || (fa & 8), wb = p.macro_all || (fb & 8);
         R *rho = (R *)B.rho + c, *ux = (R *)B.ux + c, *uy = (R *)B.uy + c;
@@ -1125,7 +1180,7 @@ __global__ void __launch_bounds__(TB_THREADS, 1) k_block_step_tb(const __grid_co
 #pragma unroll
         for (int k = 0; k < 9; k++) f[k] = to_r(((const S *)(st + k * C::SEG_BYTES))[tid + C::A - ex(k)]);
         R out[9], m[3];
-        stb_collide<P>(f, (R)B.rv_tau, out, m, p.sh);
+        stb_collide<P>(f, (R)B.rv_tau, out, m, p.sh, cell_key(B, i, j));
         const long long c = (long long)j * B.pitch + i;
         if (p.write_macros && (p.macro_all || (fl & 8))) {
           ((R *)B.rho)[c] = m[0];
@@ -1251,7 +1306,7 @@ __device__ __forceinline__ void stb_quad_body(const StbParams &p, long long wt, 
       R fc[9], o[9], m[3];
 #pragma unroll
       for (int k = 0; k < 9; k++) fc[k] = f[k][q];
-      stb_collide<P>(fc, rv, o, m, p.sh);
+      stb_collide<P>(fc, rv, o, m, p.sh, cell_key(B, i0 + q, j));
 #pragma unroll
       for (int k = 0; k < 9; k++) f[k][q] = o[k];
       if (p.write_macros && (p.macro_all || ((fl4 >> (8 * q)) & 8u))) {

@@ -174,6 +174,7 @@ struct mb_ctx {
   int prg_bulk_cells = 512;             // cells per item of bulk block-step nodes
   int prg_urgent_cells = 256;           // cells per item of the other block-step nodes
   int prg_periods = 2;                  // scheduler periods per executor launch
+  int plan_steps = 24;                  // coarse steps per replayed graph (rounded up to periods)
   int prg_bulk_limit = 0;               // CTAs allowed on bulk items at once (0: no limit)
   int rec_points = 32;                  // interface points per record CTA / executor item
   int spl_segs = 1;                     // spline segments per CTA / executor item
@@ -184,6 +185,11 @@ struct mb_ctx {
   int spl_cta_smem = 96 * 1024;
   int rec_cta_smem = 0;
   int bulk_cta_smem = 0;  // unused shared memory reserved by each bulk (interior) block-step CTA
+  // the fine levels' F and rho/u and the interface slots, one allocation
+  // (the range of the L2 access-policy window, mb_set_l2_persist)
+  void *fine_arena = nullptr;
+  size_t fine_bytes = 0;
+  size_t l2_persist = 0;  // bytes of L2 set aside for it (0: none)
   int shift_mode = MB_SHIFT_W;  // stored words h = f - s: s = w, or feq(rho0, U0)
   Shift shift{};
   PrgTraceRec *d_trace = nullptr;       // executor trace (mb_set_program_trace)
@@ -410,6 +416,7 @@ StbParams make_stb(mb_ctx *c, int a0, int a1, uint64_t parity, int macro_all, in
     s.nx = B.nx;
     s.ny = B.ny;
     s.pitch = B.pitch;
+    s.gid = a;
     s.plane = B.plane;
     s.cell0 = cell;
     s.rv_tau = c->geo.Areas[a].rv_tau;
@@ -799,6 +806,22 @@ int set_priority(cudaGraphNode_t node, bool background, bool slack = false) {
   return MB_OK;
 }
 
+// The access-policy window of the chain kernels: the fine levels' arena,
+// hits persisting in the set-aside part of L2, in proportion to its size.
+bool l2_window(const mb_ctx *c, cudaAccessPolicyWindow *w) {
+  if (!c->l2_persist || !c->fine_arena) return false;
+  int dev = 0, maxw = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&maxw, cudaDevAttrMaxAccessPolicyWindowSize, dev) != cudaSuccess || maxw <= 0)
+    return false;
+  w->base_ptr = c->fine_arena;
+  w->num_bytes = std::min(c->fine_bytes, (size_t)maxw);
+  w->hitRatio = (float)std::min(1.0, (double)c->l2_persist / (double)w->num_bytes);
+  w->hitProp = cudaAccessPropertyPersisting;
+  w->missProp = cudaAccessPropertyStreaming;
+  return true;
+}
+
 // Marks the nodes whose start may slip by more than SLACK_US without
 // lengthening the plan, by longest paths over a rough cost model of each
 // launch (a fixed latency plus a term in its CTAs; bulk nodes cost nothing
@@ -825,7 +848,7 @@ void mark_slack(CompiledPlan &cp) {
   for (int q = 0; q < nd; q++) cp.dn[q].slack = T - (head[q] + tail[q]) > SLACK_US;
 }
 
-int build_graph(CompiledPlan &cp, bool pdl) {
+int build_graph(CompiledPlan &cp, bool pdl, const cudaAccessPolicyWindow *win = nullptr) {
   mark_slack(cp);
   MB_CUDA(cudaGraphCreate(&cp.graph, 0));
   std::vector<cudaGraphNode_t> gn(cp.dn.size(), nullptr);
@@ -848,6 +871,11 @@ int build_graph(CompiledPlan &cp, bool pdl) {
     if (!pdl) {
       MB_CUDA(cudaGraphAddKernelNode(&gn[q], cp.graph, deps.data(), deps.size(), &kp));
       if (int e = set_priority(gn[q], d.background, d.slack)) return e;
+      if (win && !d.background) {  // chain kernels keep the fine levels' lines in the set-aside L2
+        cudaKernelNodeAttrValue v{};
+        v.accessPolicyWindow = *win;
+        MB_CUDA(cudaGraphKernelNodeSetAttribute(gn[q], cudaKernelNodeAttributeAccessPolicyWindow, &v));
+      }
       continue;
     }
     // programmatic edges between kernels of the fine-level chain: this kernel
@@ -1099,6 +1127,36 @@ CompiledPlan *get_diag_plan(mb_ctx *c, int n, int *err) {
   return raw;
 }
 
+// Coarse steps of the next plan a call of `remaining` more steps replays, and
+// whether it is the call's last (rho/u of every cell written in its last
+// step).  Graphs and direct launches take plans of a whole number of
+// scheduler periods, at least plan_steps long, so that one compiled plan
+// serves every repetition and the next step's level-0 interior overlaps the
+// chain everywhere except across the few graph boundaries; the call's tail
+// is one plan of the remaining steps.  The executor keeps its launches of
+// prg_periods periods and single final-state steps.  Diagnostic plans write
+// rho/u every step, so they have no final flag.
+int next_chunk(const mb_ctx *c, int remaining, bool diag, bool *fin) {
+  if (c->use_graph == 3) {
+    const int G = c->period * c->prg_periods;
+    *fin = diag || remaining == 1;
+    if (diag) return 1;
+    return remaining - 1 >= G ? G : 1;
+  }
+  const int per = std::max(c->period, 1);
+  const int G = (std::max(c->plan_steps, 1) + per - 1) / per * per;
+  if (diag) {
+    *fin = true;
+    return std::min(remaining, G);
+  }
+  if (remaining > G) {
+    *fin = false;
+    return G;
+  }
+  *fin = true;
+  return remaining;
+}
+
 int exec_plan(mb_ctx *c, CompiledPlan *cp, cudaStream_t s) {
   int e;
   if (c->use_graph == 3) {
@@ -1111,7 +1169,8 @@ int exec_plan(mb_ctx *c, CompiledPlan *cp, cudaStream_t s) {
   }
   if (c->use_graph) {
     if (!cp->exec) {
-      e = build_graph(*cp, c->use_graph == 2);
+      cudaAccessPolicyWindow w{};
+      e = build_graph(*cp, c->use_graph == 2, l2_window(c, &w) ? &w : nullptr);
       if (e) return e;
     }
     MB_CUDA(cudaGraphLaunch(cp->exec, s));
@@ -1195,6 +1254,11 @@ extern "C" int mb_create(const mb_geometry *geo, int precision, mb_ctx **out) {
   }
   c->shift_mode = default_shift(precision);
   c->shift = make_shift(c.get(), c->shift_mode);
+  // measured on config 2's developed shedding against FP64 storage (mean Cd,
+  // rms Cl, St): stochastic rounding +9e-5, -4.6e-3, -6.9e-4 in FP16 storage
+  // (round to nearest -8.7e-3, -0.36, -7.1e-2) for 4 % more time per step;
+  // h16c -5.3e-4, -4.2e-3, -5.1e-4 (round to nearest -6.2e-3, -8.9e-2, -2.6e-3)
+  c->shift.sr = precision == MB_PREC_F16C || precision == MB_PREC_F16S ? MB_ROUND_STOCHASTIC : MB_ROUND_NEAREST;
 
   // block layouts and flags
   c->bl.resize(c->nblk);
@@ -1277,20 +1341,50 @@ extern "C" int mb_create(const mb_geometry *geo, int precision, mb_ctx **out) {
     }
   }
 
-  // device allocations (Multi-block-LBM.cu:26-113, without x/y/force/f arrays)
+  // device allocations (Multi-block-LBM.cu:26-113, without x/y/force/f arrays).
+  // F and rho/u of the fine blocks (m > 1) and the interface slots are carved
+  // from one arena, the range an L2 access-policy window can keep resident.
   int e;
+  auto a256 = [](size_t n) { return (std::max<size_t>(n, 1) + 255) & ~(size_t)255; };
+  const size_t slot_bytes = (size_t)std::max<long long>(slot_pts, 1) * 27 * rb;
+  size_t fine = a256(slot_bytes);
+  for (int a = 0; a < c->nblk; a++)
+    if (geo->Areas[a].m > 1) fine += 2 * a256((size_t)9 * c->bl[a].plane * sb) + 3 * a256((size_t)c->bl[a].plane * rb);
+  {
+    void *p;
+    if (cudaMalloc(&p, fine) != cudaSuccess) return MB_ERR_NOMEM;
+    c->allocs.push_back(p);
+    c->fine_arena = p;
+    c->fine_bytes = fine;
+  }
+  size_t fine_off = 0;
+  auto take = [&](size_t n) {
+    void *p = (char *)c->fine_arena + fine_off;
+    fine_off += a256(n);
+    return p;
+  };
+  c->d_slots = take(slot_bytes);
   c->blk.resize(c->nblk);
   for (int a = 0; a < c->nblk; a++) {
     IfBlk &B = c->blk[a];
     const BlockLayout &b = c->bl[a];
+    const bool in_arena = geo->Areas[a].m > 1;
     for (int q = 0; q < 2; q++) {
       void *p;
-      if (cudaMalloc(&p, (size_t)9 * b.plane * sb) != cudaSuccess) return MB_ERR_NOMEM;
-      c->allocs.push_back(p);
+      if (in_arena) {
+        p = take((size_t)9 * b.plane * sb);
+      } else {
+        if (cudaMalloc(&p, (size_t)9 * b.plane * sb) != cudaSuccess) return MB_ERR_NOMEM;
+        c->allocs.push_back(p);
+      }
       B.F[q] = p;
     }
     void *m[5];
     for (int q = 0; q < 5; q++) {
+      if (in_arena && q < 3) {
+        m[q] = take((size_t)b.plane * rb);
+        continue;
+      }
       if (cudaMalloc(&m[q], (size_t)b.plane * rb) != cudaSuccess) return MB_ERR_NOMEM;
       c->allocs.push_back(m[q]);
     }
@@ -1316,12 +1410,6 @@ extern "C" int mb_create(const mb_geometry *geo, int precision, mb_ctx **out) {
     }
     if ((e = dalloc(c.get(), &c->d_cclist[l], ents.size()))) return e;
     MB_CUDA(cudaMemcpy(c->d_cclist[l], ents.data(), ents.size() * sizeof(CcEntry), cudaMemcpyHostToDevice));
-  }
-  {
-    void *p;
-    if (cudaMalloc(&p, std::max<long long>(slot_pts, 1) * 27 * rb) != cudaSuccess) return MB_ERR_NOMEM;
-    c->allocs.push_back(p);
-    c->d_slots = p;
   }
   if (L.number_line) {
     // LU coefficients of each line's system (init_tri_A rows): c'_i = u_i / den_i,
@@ -1438,6 +1526,10 @@ extern "C" int mb_destroy(mb_ctx *c) {
   if (!c) return MB_ERR_INVALID;
   cudaDeviceSynchronize();
   c->plans.clear();
+  if (c->l2_persist) {  // the set-aside goes back to normal lines
+    cudaCtxResetPersistingL2Cache();
+    cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, 0);
+  }
   for (void *p : c->allocs) cudaFree(p);
   if (c->h_drag_out) cudaFreeHost(c->h_drag_out);
   if (c->h_l2_out) cudaFreeHost(c->h_l2_out);
@@ -1464,8 +1556,40 @@ extern "C" int mb_set_shift(mb_ctx *c, int mode) {
   cudaDeviceSynchronize();
   c->plans.clear();
   c->shift_mode = mode;
+  const int sr = c->shift.sr;
   c->shift = make_shift(c, mode);
+  c->shift.sr = sr;
   c->inited = false;  // the stored words mean something else now: mb_init (or a restore) comes next
+  return MB_OK;
+}
+
+extern "C" int mb_set_rounding(mb_ctx *c, int mode) {
+  if (!c || (mode != MB_ROUND_NEAREST && mode != MB_ROUND_STOCHASTIC)) return MB_ERR_INVALID;
+  if (mode == MB_ROUND_STOCHASTIC && c->prec != MB_PREC_F16C && c->prec != MB_PREC_F16S) return MB_ERR_INVALID;
+  if (mode == c->shift.sr) return MB_OK;
+  cudaDeviceSynchronize();
+  c->plans.clear();  // the kernels read the mode from their parameters
+  c->shift.sr = mode;
+  return MB_OK;
+}
+
+extern "C" int mb_set_l2_persist(mb_ctx *c, int mb) {
+  if (!c || mb < 0) return MB_ERR_INVALID;
+  cudaDeviceSynchronize();
+  c->plans.clear();
+  int dev = 0, maxp = 0;
+  MB_CUDA(cudaGetDevice(&dev));
+  MB_CUDA(cudaDeviceGetAttribute(&maxp, cudaDevAttrMaxPersistingL2CacheSize, dev));
+  const size_t want = std::min(std::min((size_t)mb << 20, (size_t)std::max(maxp, 0)), c->fine_bytes);
+  MB_CUDA(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want));
+  if (!want) MB_CUDA(cudaCtxResetPersistingL2Cache());
+  c->l2_persist = want;
+  return MB_OK;
+}
+
+extern "C" int mb_set_plan_steps(mb_ctx *c, int n) {
+  if (!c || n < 1 || n > 4096) return MB_ERR_INVALID;
+  c->plan_steps = n;
   return MB_OK;
 }
 
@@ -1796,13 +1920,9 @@ extern "C" int mb_step(mb_ctx *c, int n, mb_stream stream) {
   cudaStream_t s = (cudaStream_t)stream;
   c->kernels_last_call = 0;
   int remaining = n;
-  const int G = c->use_graph == 3 ? c->period * c->prg_periods : c->period;
   while (remaining > 0) {
-    int chunk;
     bool fin;
-    if (remaining - 1 >= G) { chunk = G; fin = false; }
-    else if (remaining > 1) { chunk = 1; fin = false; }
-    else { chunk = 1; fin = true; }
+    const int chunk = next_chunk(c, remaining, false, &fin);
     int err = 0;
     CompiledPlan *cp = get_plan(c, chunk, fin, &err);
     if (!cp) return err ? err : MB_ERR_INVALID;
@@ -1820,7 +1940,8 @@ namespace {
 int ready_plan(mb_ctx *c, CompiledPlan *cp, cudaStream_t up) {
   if (c->use_graph == 3) return cp->prg_built ? MB_OK : build_program(c, *cp);
   if (!c->use_graph || cp->exec) return MB_OK;
-  if (int e = build_graph(*cp, c->use_graph == 2)) return e;
+  cudaAccessPolicyWindow w{};
+  if (int e = build_graph(*cp, c->use_graph == 2, l2_window(c, &w) ? &w : nullptr)) return e;
   MB_CUDA(cudaGraphUpload(cp->exec, up));
   return MB_OK;
 }
@@ -1832,23 +1953,12 @@ int prepare_chunks(mb_ctx *c, int n, bool diag) {
   MB_CUDA(cudaStreamCreateWithFlags(&up, cudaStreamNonBlocking));
   const SchedState save = c->state;
   int remaining = n, err = MB_OK;
-  const int G = c->use_graph == 3 ? c->period * c->prg_periods : c->period;
   while (remaining > 0 && err == MB_OK) {
-    CompiledPlan *cp = nullptr;
-    int chunk;
-    if (diag && c->use_graph != 3) {  // mb_step_diag: plans of `period` steps, else single steps
-      chunk = remaining >= c->period ? c->period : 1;
-      cp = get_diag_plan(c, chunk, &err);
-    } else if (diag) {  // executor: one final-state step per plan, drag and L2 launched apart
-      chunk = 1;
-      cp = get_plan(c, 1, true, &err);
-    } else {
-      bool fin;
-      if (remaining - 1 >= G) { chunk = G; fin = false; }
-      else if (remaining > 1) { chunk = 1; fin = false; }
-      else { chunk = 1; fin = true; }
-      cp = get_plan(c, chunk, fin, &err);
-    }
+    bool fin;
+    const int chunk = next_chunk(c, remaining, diag, &fin);
+    // mb_step_diag's plans carry their diagnostics; the executor's are
+    // final-state steps with drag and L2 launched apart
+    CompiledPlan *cp = diag && c->use_graph != 3 ? get_diag_plan(c, chunk, &err) : get_plan(c, chunk, fin, &err);
     if (!cp) { err = err ? err : MB_ERR_INVALID; break; }
     if ((err = ready_plan(c, cp, up))) break;
     c->state = cp->end;
@@ -1903,10 +2013,11 @@ extern "C" int mb_prepare_diag(mb_ctx *c, int n) {
 extern "C" int mb_plan_describe(mb_ctx *c, int n, char *buf, long long cap, long long *len) {
   if (!c || n < 1 || (!buf && cap > 0)) return MB_ERR_INVALID;
   if (!c->inited) return MB_ERR_STATE;
-  const int G = c->use_graph == 3 ? c->period * c->prg_periods : c->period;
   int err = 0;
   const SchedState save = c->state;
-  CompiledPlan *cp = get_plan(c, n - 1 >= G ? G : 1, n == 1, &err);
+  bool fin;
+  const int chunk = next_chunk(c, n, false, &fin);
+  CompiledPlan *cp = get_plan(c, chunk, fin, &err);
   c->state = save;
   if (!cp) return err ? err : MB_ERR_INVALID;
   if (c->use_graph && c->use_graph != 3) mark_slack(*cp);
@@ -2081,10 +2192,11 @@ extern "C" int mb_step_diag(mb_ctx *c, int n, double *cd, double *cl, double *er
   if (int e = ensure_diag(c, (size_t)n, s)) return e;
   c->kernels_last_call = 0;
   if (c->use_graph != 3) {
-    // plans of `period` steps with their diagnostics; each plan's results go
+    // plans of whole periods with their diagnostics; each plan's results go
     // to the host with one copy
     for (int q = 0; q < n;) {
-      const int chunk = (n - q >= c->period) ? c->period : 1;
+      bool fin;
+      const int chunk = next_chunk(c, n - q, true, &fin);
       int e = 0;
       CompiledPlan *cp = get_diag_plan(c, chunk, &e);
       if (!cp) return e ? e : MB_ERR_INVALID;

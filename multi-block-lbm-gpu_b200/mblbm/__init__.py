@@ -28,6 +28,7 @@ PREC_F64, PREC_F32, PREC_F16S, PREC_F32U, PREC_F16C = 0, 1, 2, 3, 4
 # 3-bit exponent and 12-bit fraction (a quarter of FP16's spacing for |f - w| < 1/4)
 PRECISIONS = {"f64": PREC_F64, "f32": PREC_F32, "f16s": PREC_F16S, "f32u": PREC_F32U, "f16c": PREC_F16C}
 SHIFT_W, SHIFT_FEQ0 = 0, 1  # mb_set_shift modes
+ROUND_NEAREST, ROUND_STOCHASTIC = 0, 1  # mb_set_rounding modes
 FLUID, SOLID_SBB, C_BOUNDARY = 0, 1, 9
 OBST_CIRCLE, OBST_ELLIPSE, OBST_NONE = 0, 1, 2
 PERIODIC_X, PERIODIC_Y, DIR_PERIODIC = 1, 2, 8  # mb_config.periodic bits, NeborCC code of ghost lines
@@ -184,6 +185,9 @@ SIGNATURES = {
     "mb_prepare_diag": ([_vp, C.c_int], C.c_int),
     "mb_set_bulk_spread": ([_vp, C.c_int], C.c_int),
     "mb_set_shift": ([_vp, C.c_int], C.c_int),
+    "mb_set_rounding": ([_vp, C.c_int], C.c_int),
+    "mb_set_l2_persist": ([_vp, C.c_int], C.c_int),
+    "mb_set_plan_steps": ([_vp, C.c_int], C.c_int),
     "mb_plan_describe": ([_vp, C.c_int, C.c_char_p, C.c_longlong, _pll], C.c_int),
     "mb_block_step": ([_vp, C.c_int, _vp], C.c_int),
     "mb_c_c_boundary_transfer": ([_vp, C.c_int, _vp], C.c_int),
@@ -469,12 +473,14 @@ def _stream_ptr(stream):
 class MultiBlockLBM:
     """One multi-block simulation on the current CUDA device."""
 
-    def __init__(self, geo, precision="f32", graph=True, shift=None):
+    def __init__(self, geo, precision="f32", graph=True, shift=None, rounding=None):
         """graph: False launches kernels one by one, True replays CUDA graphs,
         "pdl" replays graphs with programmatic kernel-to-kernel edges,
         "program" runs each plan as one persistent executor launch.
         shift: "w" or "feq0" for the stored distributions of the shifted
-        precisions (None: the precision's default, feq0 for f32, w otherwise)."""
+        precisions (None: the precision's default, feq0 for f32 and f16c, w for f16s).
+        rounding: "nearest" or "stochastic" (f16c, f16s) for the stored words (None: the
+        precision's default, stochastic for f16c and f16s, nearest otherwise)."""
         self.lib = load()
         self.geo = geo
         self.precision = precision
@@ -486,6 +492,8 @@ class MultiBlockLBM:
             _check(self.lib.mb_set_graph_mode(self.h, mode), "mb_set_graph_mode")
         if shift is not None:
             _check(self.lib.mb_set_shift(self.h, {"w": SHIFT_W, "feq0": SHIFT_FEQ0}[shift]), "mb_set_shift")
+        if rounding is not None:
+            self.set_rounding(rounding)
         self.n = 0
 
     def close(self):
@@ -537,6 +545,19 @@ class MultiBlockLBM:
     def set_cta_spread(self, spline_kb, records_kb):
         """Minimum shared memory per spline / record CTA (KB): caps their CTAs per SM."""
         _check(self.lib.mb_set_cta_spread(self.h, int(spline_kb), int(records_kb)), "mb_set_cta_spread")
+
+    def set_rounding(self, mode):
+        """"nearest" or "stochastic" (f16c, f16s): how the collision rounds the stored words."""
+        m = {"nearest": ROUND_NEAREST, "stochastic": ROUND_STOCHASTIC}[mode]
+        _check(self.lib.mb_set_rounding(self.h, m), "mb_set_rounding")
+
+    def set_plan_steps(self, n):
+        """Coarse steps per replayed graph (rounded up to whole scheduler periods)."""
+        _check(self.lib.mb_set_plan_steps(self.h, int(n)), "mb_set_plan_steps")
+
+    def set_l2_persist(self, mb):
+        """L2 set aside (MB) for the fine levels' state, kept resident for the chain kernels (0: off)."""
+        _check(self.lib.mb_set_l2_persist(self.h, int(mb)), "mb_set_l2_persist")
 
     def set_bulk_spread(self, kb):
         """Unused shared memory (KB) reserved by each bulk (interior) block-step CTA (0: none)."""

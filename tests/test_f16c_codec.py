@@ -71,7 +71,7 @@ def test_device_codec_matches(mb, cuda_device):
     import make_ref
 
     g = mb.geo_init(*make_ref.case("g11")[:2])
-    m = mb.MultiBlockLBM(g, "f16c")
+    m = mb.MultiBlockLBM(g, "f16c", shift="w")
     m.init()
     A = g.Areas[0]
     n = A.nx * A.ny

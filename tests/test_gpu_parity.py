@@ -459,3 +459,49 @@ def test_shift_modes(mb, orc, cuda_device, prec):
         other.restore(ck["feq0"])
     other.restore(ck["w"])
     other.close()
+
+
+@pytest.mark.parametrize("prec", ["f16c", "f16s"])
+@pytest.mark.parametrize("split", [0, 10**12])
+def test_stochastic_rounding_variants_bitwise(mb, orc, cuda_device, split, prec):
+    """16-bit storage with stochastic rounding: every block-step variant and execution
+    mode gives bitwise the same state (the dither is a function of the cell and
+    its inputs), the state differs from round-to-nearest's and stays within
+    the 16-bit bound of the FP64 oracle; the other precisions refuse it."""
+    g = mb.geo_init(*make_ref.case("n3")[:2])
+    steps = 60
+    sims = []
+    for variant, graph in ((0, True), (1, True), (3, True), (5, False), (2, "program")):
+        s = mb.MultiBlockLBM(g, prec, graph=graph, rounding="stochastic")
+        for lvl in range(g.layout.LEVEL):
+            s.set_stb_variant(lvl, variant)
+        s.set_split_cells(split)
+        s.init()
+        s.evolution(steps)
+        sims.append(s)
+    ref = [sims[0].fields(k) for k in range(g.layout.number_area)]
+    for s in sims[1:]:
+        for k in range(g.layout.number_area):
+            f = s.fields(k)
+            for key in ("F", "rho", "ux", "uy"):
+                assert np.array_equal(f[key], ref[k][key]), (k, key)
+    rn = mb.MultiBlockLBM(g, prec, rounding="nearest")
+    rn.init()
+    rn.evolution(steps)
+    assert any(not np.array_equal(rn.fields(k)["F"], ref[k]["F"]) for k in range(g.layout.number_area))
+    o = orc.Oracle(g)
+    o.init()
+    o.evolution(steps)
+    fo = all_fields(o, g)
+    for s in (rn, sims[0]):
+        fm = all_fields(s, g)
+        eu, er = rel_l2(g, fo, fm, "u"), rel_l2(g, fo, fm, "rho")
+        print(f"{prec} {'stochastic' if s is sims[0] else 'nearest'}: relL2 u {eu:.3e} rho {er:.3e}")
+        assert eu <= (2e-3 if prec == "f16c" else 5e-3) and er <= (2e-3 if prec == "f16c" else 5e-3)
+    for s in sims + [rn]:
+        s.close()
+    f32 = mb.MultiBlockLBM(g, "f32")
+    with pytest.raises(mb.MBError):
+        f32.set_rounding("stochastic")
+    f32.set_rounding("nearest")
+    f32.close()
