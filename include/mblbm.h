@@ -223,8 +223,13 @@ int mb_step(mb_ctx *ctx, int n_coarse, mb_stream stream);
  * consumer is scheduled while its producers drain; 3: one persistent
  * executor launch per plan, which tracks the DAG on the device (CTAs claim
  * work items of ready nodes; bulk interior work fills the fine-level chain's
- * waits).  Results are identical in every mode. */
+ * waits); 4: hybrid graphs, whose bulk interior nodes (and drag and L2 nodes)
+ * are kernel nodes and whose fine-level chain runs as persistent executor
+ * launches between them, each capped at mb_set_hybrid_ctas CTAs per SM.
+ * Results are identical in every mode. */
 int mb_set_graph_mode(mb_ctx *ctx, int mode);
+/* Executor CTAs per SM of the chain launches of graph mode 4 (default 2). */
+int mb_set_hybrid_ctas(mb_ctx *ctx, int per_sm);
 /* Mode 3: a CTA that finds no ready work for this long sets the context's
  * error word and the launch ends; the next synchronising call (mb_sync,
  * mb_drag, mb_error_L2, mb_check_finite, mb_copy_fields) returns

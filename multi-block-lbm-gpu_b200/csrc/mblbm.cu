@@ -75,6 +75,18 @@ struct DevPlanNode {
   std::vector<int> deps;
 };
 
+// One executor launch: its arguments, the claim | done | pending state and
+// the state's values at launch (copied over it before every launch), grid and
+// dynamic shared memory.
+struct PrgLaunch {
+  PrgArgs prg{};
+  unsigned int *state = nullptr;
+  const unsigned int *init = nullptr;
+  size_t state_bytes = 0;
+  int grid = 0;
+  size_t smem = 0;
+};
+
 struct CompiledPlan {
   std::vector<PlanNode> nodes;
   std::vector<DevPlanNode> dn;
@@ -85,14 +97,11 @@ struct CompiledPlan {
   long long kernels = 0;
   double *d_diag_res = nullptr;  // diagnostic plans: Fx, Fy and the two L2 sums of every part, per coarse step
   int diag_steps = 0;
-  // persistent executor (graph mode 3)
+  // persistent executor: the whole plan (graph mode 3), or the chain
+  // segments of a hybrid graph (mode 4)
   bool prg_built = false;
-  PrgArgs prg{};
-  unsigned int *prg_state = nullptr;       // claim | done | pending
-  const unsigned int *prg_init = nullptr;  // their values at launch
-  size_t prg_state_bytes = 0;
-  int prg_grid = 0;
-  size_t prg_smem = 0;
+  PrgLaunch prgm;
+  std::vector<PrgLaunch> segs;
   ~CompiledPlan() {
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
@@ -174,6 +183,7 @@ struct mb_ctx {
   int prg_bulk_cells = 512;             // cells per item of bulk block-step nodes
   int prg_urgent_cells = 256;           // cells per item of the other block-step nodes
   int prg_periods = 2;                  // scheduler periods per executor launch
+  int hyb_ctas_per_sm = 2;              // executor CTAs per SM of a hybrid graph's chain segments
   int plan_steps = 24;                  // coarse steps per replayed graph (rounded up to periods)
   int prg_bulk_limit = 0;               // CTAs allowed on bulk items at once (0: no limit)
   int rec_points = 32;                  // interface points per record CTA / executor item
@@ -455,7 +465,8 @@ StbParams make_stb(mb_ctx *c, int a0, int a1, uint64_t parity, int macro_all, in
 
 // the rim is always stepped one cell per thread
 bool stb_uses_quads(const mb_ctx *c, int level, int region) {
-  return region != STB_RIM && c->stb_variant[level] == 1 && c->use_graph != 3 && !options_on(c);
+  return region != STB_RIM && c->stb_variant[level] == 1 && c->use_graph != 3 &&
+         !(c->use_graph == 4 && region != STB_INTERIOR) && !options_on(c);
 }
 
 bool background_capped(const mb_ctx *c, bool background) { return background && c->bulk_ctas_per_sm > 0; }
@@ -926,76 +937,82 @@ int set_smem_limits(int prec) {
 }
 
 // ---- persistent executor ------------------------------------------------------
-// Lays the lowered nodes out as an executor program: nodes without work are
-// dropped (their successors inherit their dependencies), urgent nodes come
-// first and bulk (interior block-step) nodes after them, each class in plan
-// order, which is a topological order.
-int build_program(mb_ctx *c, CompiledPlan &cp) {
-  const int nd = (int)cp.dn.size();
-  std::vector<long long> units(nd, 0);
-  std::vector<int> per(nd, 1), kind(nd, 0);
-  for (int q = 0; q < nd; q++) {
-    const DevPlanNode &d = cp.dn[q];
-    if (d.kind == NK_STB) {
-      kind[q] = PK_STB;
-      units[q] = d.stb.total;
-      per[q] = d.background ? c->prg_bulk_cells : c->prg_urgent_cells;
-    } else if (d.kind == NK_REC) {
-      kind[q] = PK_REC;
-      units[q] = d.rec.total;
-      per[q] = c->rec_points;
-    } else {
-      kind[q] = PK_SPL;
-      units[q] = d.spl.nseg;
-      per[q] = c->spl_segs;
-    }
+// Item counts of a lowered node in the executor, and its work kind.
+void program_units(const mb_ctx *c, const DevPlanNode &d, int *kind, long long *units, int *per) {
+  if (d.kind == NK_STB) {
+    *kind = PK_STB;
+    *units = d.stb.total;
+    *per = d.background ? c->prg_bulk_cells : c->prg_urgent_cells;
+  } else if (d.kind == NK_REC) {
+    *kind = PK_REC;
+    *units = d.rec.total;
+    *per = c->rec_points;
+  } else {
+    *kind = PK_SPL;
+    *units = d.spl.nseg;
+    *per = c->spl_segs;
   }
-  // effective dependencies over non-empty nodes
+}
+
+// Dependencies of every node over the nodes that have work (a node without
+// work passes its own on to its successors).
+std::vector<std::vector<int>> effective_deps(const CompiledPlan &cp, const std::vector<char> &has_work) {
+  const int nd = (int)cp.dn.size();
   std::vector<std::vector<int>> eff(nd);
   for (int q = 0; q < nd; q++) {
     std::vector<int> out;
     for (int p : cp.dn[q].deps) {
-      if (units[p] > 0) out.push_back(p);
+      if (has_work[p]) out.push_back(p);
       else out.insert(out.end(), eff[p].begin(), eff[p].end());
     }
     std::sort(out.begin(), out.end());
     out.erase(std::unique(out.begin(), out.end()), out.end());
     eff[q] = std::move(out);
   }
-  std::vector<int> order;
-  for (int pass = 0; pass < 2; pass++)
-    for (int q = 0; q < nd; q++)
-      if (units[q] > 0 && cp.dn[q].background == (pass == 1)) order.push_back(q);
+  return eff;
+}
+
+// Lays out the nodes `order` (plan indices, a topological order) of a plan
+// as one executor program: node table, successor lists over these nodes
+// only, parameter blob and the claim / done / pending state with its launch
+// values, in one device allocation owned by the plan.  `nurgent` leading
+// nodes are urgent, the rest bulk.  `ctas_per_sm` caps the grid (0: as many
+// CTAs as fit).
+int program_from(mb_ctx *c, CompiledPlan &cp, const std::vector<int> &order, const std::vector<std::vector<int>> &eff,
+                 int nurgent, int ctas_per_sm, PrgLaunch &L) {
+  const int nd = (int)cp.dn.size();
   const int nn = (int)order.size();
   if (nn > PRG_MAX_NODES) return MB_ERR_UNSUPPORTED;
-  for (int q = 0; q < nd; q++)
-    if (units[q] >= (1LL << 31) - (1LL << 25)) return MB_ERR_UNSUPPORTED;  // item bounds are 32-bit
-  int nurgent = 0;
-  for (int q : order) nurgent += cp.dn[q].background ? 0 : 1;
   std::vector<int> pos(nd, -1);
   for (int i = 0; i < nn; i++) pos[order[i]] = i;
   std::vector<std::vector<int>> succ(nn);
   std::vector<unsigned int> pending(nn, 0);
   for (int i = 0; i < nn; i++)
     for (int p : eff[order[i]]) {
+      if (pos[p] < 0) continue;  // outside this program: ordered by the launch
       succ[pos[p]].push_back(i);
       pending[i]++;
     }
-  // node table, successor lists and parameter blob
   std::vector<PrgNode> nodes(nn);
   std::vector<int> sl;
   std::vector<unsigned char> blob;
+  long long items = 0;
   for (int i = 0; i < nn; i++) {
     const int q = order[i];
     const DevPlanNode &d = cp.dn[q];
+    int kind = 0, per = 1;
+    long long units = 0;
+    program_units(c, d, &kind, &units, &per);
+    if (units >= (1LL << 31) - (1LL << 25)) return MB_ERR_UNSUPPORTED;  // item bounds are 32-bit
     PrgNode &N = nodes[i];
     N = PrgNode{};
-    N.kind = kind[q];
-    N.units = units[q];
-    N.per_item = per[q];
-    N.items = (int)((units[q] + per[q] - 1) / per[q]);
-    const void *src = kind[q] == PK_STB ? (const void *)&d.stb : kind[q] == PK_REC ? (const void *)&d.rec : (const void *)&d.spl;
-    const size_t sz = kind[q] == PK_STB ? sizeof(StbParams) : kind[q] == PK_REC ? sizeof(RecOpsParams) : sizeof(SplParamsP);
+    N.kind = kind;
+    N.units = units;
+    N.per_item = per;
+    N.items = (int)((units + per - 1) / per);
+    items += N.items;
+    const void *src = kind == PK_STB ? (const void *)&d.stb : kind == PK_REC ? (const void *)&d.rec : (const void *)&d.spl;
+    const size_t sz = kind == PK_STB ? sizeof(StbParams) : kind == PK_REC ? sizeof(RecOpsParams) : sizeof(SplParamsP);
     const size_t padded = (sz + 15) / 16 * 16;
     N.param_off = (int)blob.size();
     N.param_bytes = (int)padded;
@@ -1008,60 +1025,172 @@ int build_program(mb_ctx *c, CompiledPlan &cp) {
   }
   // one allocation: nodes | succ | blob | init state | state
   auto al = [](size_t v) { return (v + 255) / 256 * 256; };
-  const size_t o_nodes = 0, o_succ = al(nn * sizeof(PrgNode)), o_blob = o_succ + al(std::max<size_t>(sl.size(), 1) * sizeof(int));
+  const size_t o_nodes = 0, o_succ = al(std::max(nn, 1) * sizeof(PrgNode)),
+               o_blob = o_succ + al(std::max<size_t>(sl.size(), 1) * sizeof(int));
   const size_t st_bytes = (3 * (size_t)nn + 2) * sizeof(unsigned int);  // claim, done, pending, generation, bulk
   const size_t o_init = o_blob + al(std::max<size_t>(blob.size(), 16)), o_state = o_init + al(st_bytes);
   const size_t total = o_state + al(st_bytes);
   std::vector<unsigned char> host(total, 0);
-  std::memcpy(host.data() + o_nodes, nodes.data(), nn * sizeof(PrgNode));
+  if (nn) std::memcpy(host.data() + o_nodes, nodes.data(), nn * sizeof(PrgNode));
   if (!sl.empty()) std::memcpy(host.data() + o_succ, sl.data(), sl.size() * sizeof(int));
   if (!blob.empty()) std::memcpy(host.data() + o_blob, blob.data(), blob.size());
-  std::memcpy(host.data() + o_init + 2 * nn * sizeof(unsigned int), pending.data(), nn * sizeof(unsigned int));
+  if (nn) std::memcpy(host.data() + o_init + 2 * nn * sizeof(unsigned int), pending.data(), nn * sizeof(unsigned int));
   unsigned char *dp = nullptr;
   if (cudaMalloc(&dp, total) != cudaSuccess) return MB_ERR_NOMEM;
   cp.dev_allocs.push_back(dp);
   MB_CUDA(cudaMemcpy(dp, host.data(), total, cudaMemcpyHostToDevice));
-  cp.prg_state = (unsigned int *)(dp + o_state);
-  cp.prg_init = (const unsigned int *)(dp + o_init);
-  cp.prg_state_bytes = st_bytes;
-  PrgArgs &a = cp.prg;
+  L.state = (unsigned int *)(dp + o_state);
+  L.init = (const unsigned int *)(dp + o_init);
+  L.state_bytes = st_bytes;
+  PrgArgs &a = L.prg;
+  a = PrgArgs{};
   a.nodes = (const PrgNode *)(dp + o_nodes);
   a.succ = (const int *)(dp + o_succ);
   a.blob = dp + o_blob;
-  a.claim = cp.prg_state;
-  a.done = cp.prg_state + nn;
-  a.pending = cp.prg_state + 2 * nn;
-  a.gen = cp.prg_state + 3 * nn;
-  a.bulk_active = cp.prg_state + 3 * nn + 1;
+  a.claim = L.state;
+  a.done = L.state + nn;
+  a.pending = L.state + 2 * nn;
+  a.gen = L.state + 3 * nn;
+  a.bulk_active = L.state + 3 * nn + 1;
   a.bulk_limit = c->prg_bulk_limit;
   a.err = c->d_prg_err;
   a.host_err = c->d_prg_err_host;
   a.nnodes = nn;
   a.nurgent = nurgent;
   a.timeout_ns = c->prg_timeout_ns;
-  cp.prg_smem = program_smem(c->prec);
+  L.smem = program_smem(c->prec);
   int per_sm = 0;
-  MB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfunc<KPrg>(c->prec), PRG_THREADS, cp.prg_smem));
+  MB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfunc<KPrg>(c->prec), PRG_THREADS, L.smem));
   if (per_sm < 1) return MB_ERR_UNSUPPORTED;
-  long long items = 0;
-  for (auto &N : nodes) items += N.items;
-  cp.prg_grid = (int)std::max<long long>(1, std::min<long long>((long long)per_sm * c->num_sms, items));
+  if (ctas_per_sm > 0) per_sm = std::min(per_sm, ctas_per_sm);
+  L.grid = (int)std::max<long long>(1, std::min<long long>((long long)per_sm * c->num_sms, items));
+  return MB_OK;
+}
+
+// Lays the lowered nodes out as an executor program: nodes without work are
+// dropped (their successors inherit their dependencies), urgent nodes come
+// first and bulk (interior block-step) nodes after them, each class in plan
+// order, which is a topological order.
+int build_program(mb_ctx *c, CompiledPlan &cp) {
+  const int nd = (int)cp.dn.size();
+  std::vector<char> has_work(nd, 0);
+  for (int q = 0; q < nd; q++) {
+    int kind = 0, per = 1;
+    long long units = 0;
+    program_units(c, cp.dn[q], &kind, &units, &per);
+    has_work[q] = units > 0;
+  }
+  const std::vector<std::vector<int>> eff = effective_deps(cp, has_work);
+  std::vector<int> order;
+  for (int pass = 0; pass < 2; pass++)
+    for (int q = 0; q < nd; q++)
+      if (has_work[q] && cp.dn[q].background == (pass == 1)) order.push_back(q);
+  int nurgent = 0;
+  for (int q : order) nurgent += cp.dn[q].background ? 0 : 1;
+  if (int e = program_from(c, cp, order, eff, nurgent, 0, cp.prgm)) return e;
+  cp.prg_built = true;
+  return MB_OK;
+}
+
+// Graph mode 4: the bulk nodes (interiors of split levels) and the nodes the
+// executor does not run (drag, L2, same-level pulls) stay graph kernel nodes;
+// the other nodes of the fine levels' chain run as executor programs, one
+// per segment: the chain nodes with the same number of bulk nodes on their
+// longest path from the plan's start.  A segment's program is one graph
+// node (after a copy that resets its state) that waits for every node its
+// members wait for outside it; inside, the executor orders its members by
+// their dependencies.  Its grid is capped so that the bulk node beside it
+// keeps most of every SM.
+int build_hybrid(mb_ctx *c, CompiledPlan &cp) {
+  const int nd = (int)cp.dn.size();
+  std::vector<char> has_work(nd, 0), alone(nd, 0);
+  for (int q = 0; q < nd; q++) {
+    const DevPlanNode &d = cp.dn[q];
+    alone[q] = d.background || (d.kind != NK_STB && d.kind != NK_REC && d.kind != NK_SPL);
+    if (alone[q]) {
+      has_work[q] = d.grid.x > 0;
+    } else {
+      int kind = 0, per = 1;
+      long long units = 0;
+      program_units(c, d, &kind, &units, &per);
+      has_work[q] = units > 0;
+    }
+  }
+  const std::vector<std::vector<int>> eff = effective_deps(cp, has_work);
+  std::vector<int> rank(nd, 0);
+  int maxr = 0;
+  for (int q = 0; q < nd; q++) {
+    for (int p : eff[q]) rank[q] = std::max(rank[q], rank[p] + (alone[p] ? 1 : 0));
+    maxr = std::max(maxr, rank[q]);
+  }
+  std::vector<std::vector<int>> seg(maxr + 1), solo(maxr + 1);
+  for (int q = 0; q < nd; q++) {
+    if (!has_work[q]) continue;
+    (alone[q] ? solo : seg)[rank[q]].push_back(q);
+  }
+  MB_CUDA(cudaGraphCreate(&cp.graph, 0));
+  std::vector<cudaGraphNode_t> gnode(nd, nullptr);  // graph node each plan node completes in
+  cp.segs.assign(maxr + 1, PrgLaunch{});
+  for (int r = 0; r <= maxr; r++) {
+    if (!seg[r].empty()) {
+      PrgLaunch &L = cp.segs[r];
+      if (int e = program_from(c, cp, seg[r], eff, (int)seg[r].size(), c->hyb_ctas_per_sm, L)) return e;
+      std::vector<cudaGraphNode_t> deps;
+      for (int q : seg[r])
+        for (int p : eff[q])
+          if (rank[p] != r || alone[p]) deps.push_back(gnode[p]);
+      std::sort(deps.begin(), deps.end());
+      deps.erase(std::unique(deps.begin(), deps.end()), deps.end());
+      cudaGraphNode_t cpy = nullptr, run = nullptr;
+      MB_CUDA(cudaGraphAddMemcpyNode1D(&cpy, cp.graph, deps.data(), deps.size(), L.state, L.init, L.state_bytes,
+                                       cudaMemcpyDeviceToDevice));
+      cudaKernelNodeParams kp{};
+      kp.func = kfunc<KPrg>(c->prec);
+      kp.gridDim = dim3(L.grid);
+      kp.blockDim = dim3(PRG_THREADS);
+      kp.sharedMemBytes = (unsigned)L.smem;
+      void *args[1] = {&L.prg};
+      kp.kernelParams = args;
+      MB_CUDA(cudaGraphAddKernelNode(&run, cp.graph, &cpy, 1, &kp));
+      if (int e = set_priority(run, false)) return e;
+      for (int q : seg[r]) gnode[q] = run;
+    }
+    for (int q : solo[r]) {
+      DevPlanNode &d = cp.dn[q];
+      std::vector<cudaGraphNode_t> deps;
+      for (int p : eff[q]) deps.push_back(gnode[p]);
+      std::sort(deps.begin(), deps.end());
+      deps.erase(std::unique(deps.begin(), deps.end()), deps.end());
+      cudaKernelNodeParams kp{};
+      kp.func = d.func;
+      kp.gridDim = d.grid;
+      kp.blockDim = d.block;
+      kp.sharedMemBytes = (unsigned)d.smem;
+      kp.kernelParams = d.args;
+      MB_CUDA(cudaGraphAddKernelNode(&gnode[q], cp.graph, deps.data(), deps.size(), &kp));
+      if (int e = set_priority(gnode[q], d.background)) return e;
+    }
+  }
+  MB_CUDA(cudaGraphInstantiateWithFlags(&cp.exec, cp.graph, cudaGraphInstantiateFlagUseNodePriority));
+  cp.kernels = 0;
+  for (int r = 0; r <= maxr; r++) cp.kernels += (seg[r].empty() ? 0 : 1) + (long long)solo[r].size();
   cp.prg_built = true;
   return MB_OK;
 }
 
 int launch_program(mb_ctx *c, CompiledPlan &cp, cudaStream_t s) {
-  if (cp.prg.nnodes == 0) return MB_OK;
-  cp.prg.timeout_ns = c->prg_timeout_ns;
-  cp.prg.trace = c->d_trace;
-  cp.prg.trace_n = c->d_trace_n;
-  cp.prg.trace_cap = c->trace_cap;
-  cp.prg.launch = c->prg_launches++;
-  cp.prg.bulk_limit = c->prg_bulk_limit;
-  MB_CUDA(cudaMemcpyAsync(cp.prg_state, cp.prg_init, cp.prg_state_bytes, cudaMemcpyDeviceToDevice, s));
-  void *args[1] = {&cp.prg};
+  PrgLaunch &L = cp.prgm;
+  if (L.prg.nnodes == 0) return MB_OK;
+  L.prg.timeout_ns = c->prg_timeout_ns;
+  L.prg.trace = c->d_trace;
+  L.prg.trace_n = c->d_trace_n;
+  L.prg.trace_cap = c->trace_cap;
+  L.prg.launch = c->prg_launches++;
+  L.prg.bulk_limit = c->prg_bulk_limit;
+  MB_CUDA(cudaMemcpyAsync(L.state, L.init, L.state_bytes, cudaMemcpyDeviceToDevice, s));
+  void *args[1] = {&L.prg};
   void *fn = c->d_trace ? kfunc<KPrgT>(c->prec) : kfunc<KPrg>(c->prec);
-  MB_CUDA(cudaLaunchKernel(fn, dim3(cp.prg_grid), dim3(PRG_THREADS), args, cp.prg_smem, s));
+  MB_CUDA(cudaLaunchKernel(fn, dim3(L.grid), dim3(PRG_THREADS), args, L.smem, s));
   return MB_OK;
 }
 
@@ -1076,8 +1205,9 @@ int program_status(mb_ctx *c) {
 
 CompiledPlan *get_plan(mb_ctx *c, int n, bool final_macros, int *err, bool batch = false) {
   // batches and the persistent executor run the plain node kinds only
-  const bool fuse = c->fuse_cc && !options_on(c) && !batch && c->use_graph != 3;
-  const bool early = c->fuse_early && !options_on(c) && !batch && c->use_graph != 3;
+  // batches and the executor run the plain node kinds only
+  const bool fuse = c->fuse_cc && !options_on(c) && !batch && c->use_graph < 3;
+  const bool early = c->fuse_early && !options_on(c) && !batch && c->use_graph < 3;
   std::string key = c->state.key() + "/" + std::to_string(n) + (final_macros ? "F" : "P") + (fuse ? "c" : "") +
                     (c->fuse_tmp ? "t" : "") + (early ? "e" : "");
   auto it = c->plans.find(key);
@@ -1103,8 +1233,8 @@ CompiledPlan *get_plan(mb_ctx *c, int n, bool final_macros, int *err, bool batch
 // error_L2 each step) as one plan: the drag and the L2 change of a step run
 // beside the rest of the plan where their reads and writes allow.
 CompiledPlan *get_diag_plan(mb_ctx *c, int n, int *err) {
-  const bool fuse = c->fuse_cc && !options_on(c);
-  const bool early = c->fuse_early && !options_on(c) && c->use_graph != 3;
+  const bool fuse = c->fuse_cc && !options_on(c) && c->use_graph < 3;
+  const bool early = c->fuse_early && !options_on(c) && c->use_graph < 3;
   const std::string key =
       c->state.key() + "/" + std::to_string(n) + "D" + (fuse ? "c" : "") + (c->fuse_tmp ? "t" : "") + (early ? "e" : "");
   auto it = c->plans.find(key);
@@ -1167,10 +1297,11 @@ int exec_plan(mb_ctx *c, CompiledPlan *cp, cudaStream_t s) {
     c->kernels_last_call += 1;
     return MB_OK;
   }
+  if (c->use_graph == 4 && options_on(c)) return MB_ERR_UNSUPPORTED;
   if (c->use_graph) {
     if (!cp->exec) {
       cudaAccessPolicyWindow w{};
-      e = build_graph(*cp, c->use_graph == 2, l2_window(c, &w) ? &w : nullptr);
+      e = c->use_graph == 4 ? build_hybrid(c, *cp) : build_graph(*cp, c->use_graph == 2, l2_window(c, &w) ? &w : nullptr);
       if (e) return e;
     }
     MB_CUDA(cudaGraphLaunch(cp->exec, s));
@@ -1587,6 +1718,14 @@ extern "C" int mb_set_l2_persist(mb_ctx *c, int mb) {
   return MB_OK;
 }
 
+extern "C" int mb_set_hybrid_ctas(mb_ctx *c, int per_sm) {
+  if (!c || per_sm < 1 || per_sm > 32) return MB_ERR_INVALID;
+  cudaDeviceSynchronize();
+  c->plans.clear();
+  c->hyb_ctas_per_sm = per_sm;
+  return MB_OK;
+}
+
 extern "C" int mb_set_plan_steps(mb_ctx *c, int n) {
   if (!c || n < 1 || n > 4096) return MB_ERR_INVALID;
   c->plan_steps = n;
@@ -1828,7 +1967,7 @@ extern "C" int mb_program_selftest(mb_ctx *c, int stall, mb_stream stream) {
 }
 
 extern "C" int mb_set_graph_mode(mb_ctx *c, int mode) {
-  if (!c || mode < 0 || mode > 3) return MB_ERR_INVALID;
+  if (!c || mode < 0 || mode > 4) return MB_ERR_INVALID;
   if (mode != c->use_graph) {
     cudaDeviceSynchronize();
     c->plans.clear();
@@ -1940,8 +2079,10 @@ namespace {
 int ready_plan(mb_ctx *c, CompiledPlan *cp, cudaStream_t up) {
   if (c->use_graph == 3) return cp->prg_built ? MB_OK : build_program(c, *cp);
   if (!c->use_graph || cp->exec) return MB_OK;
+  if (c->use_graph == 4 && options_on(c)) return MB_ERR_UNSUPPORTED;
   cudaAccessPolicyWindow w{};
-  if (int e = build_graph(*cp, c->use_graph == 2, l2_window(c, &w) ? &w : nullptr)) return e;
+  if (int e = c->use_graph == 4 ? build_hybrid(c, *cp) : build_graph(*cp, c->use_graph == 2, l2_window(c, &w) ? &w : nullptr))
+    return e;
   MB_CUDA(cudaGraphUpload(cp->exec, up));
   return MB_OK;
 }

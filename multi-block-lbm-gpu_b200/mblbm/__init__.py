@@ -188,6 +188,7 @@ SIGNATURES = {
     "mb_set_rounding": ([_vp, C.c_int], C.c_int),
     "mb_set_l2_persist": ([_vp, C.c_int], C.c_int),
     "mb_set_plan_steps": ([_vp, C.c_int], C.c_int),
+    "mb_set_hybrid_ctas": ([_vp, C.c_int], C.c_int),
     "mb_plan_describe": ([_vp, C.c_int, C.c_char_p, C.c_longlong, _pll], C.c_int),
     "mb_block_step": ([_vp, C.c_int, _vp], C.c_int),
     "mb_c_c_boundary_transfer": ([_vp, C.c_int, _vp], C.c_int),
@@ -476,7 +477,8 @@ class MultiBlockLBM:
     def __init__(self, geo, precision="f32", graph=True, shift=None, rounding=None):
         """graph: False launches kernels one by one, True replays CUDA graphs,
         "pdl" replays graphs with programmatic kernel-to-kernel edges,
-        "program" runs each plan as one persistent executor launch.
+        "program" runs each plan as one persistent executor launch, "hybrid" runs the
+        fine-level chain as executor launches beside the bulk interior kernels.
         shift: "w" or "feq0" for the stored distributions of the shifted
         precisions (None: the precision's default, feq0 for f32 and f16c, w for f16s).
         rounding: "nearest" or "stochastic" (f16c, f16s) for the stored words (None: the
@@ -487,7 +489,8 @@ class MultiBlockLBM:
         h = C.c_void_p()
         _check(self.lib.mb_create(C.byref(geo), PRECISIONS[precision], C.byref(h)), "mb_create")
         self.h = h
-        mode = {"pdl": 2, "program": 3}.get(graph, 1 if graph else 0) if isinstance(graph, str) else (1 if graph else 0)
+        mode = ({"pdl": 2, "program": 3, "hybrid": 4}.get(graph, 1 if graph else 0) if isinstance(graph, str)
+                else (1 if graph else 0))
         if mode != 1:
             _check(self.lib.mb_set_graph_mode(self.h, mode), "mb_set_graph_mode")
         if shift is not None:
@@ -550,6 +553,10 @@ class MultiBlockLBM:
         """"nearest" or "stochastic" (f16c, f16s): how the collision rounds the stored words."""
         m = {"nearest": ROUND_NEAREST, "stochastic": ROUND_STOCHASTIC}[mode]
         _check(self.lib.mb_set_rounding(self.h, m), "mb_set_rounding")
+
+    def set_hybrid_ctas(self, per_sm):
+        """Executor CTAs per SM of the chain launches (graph="hybrid")."""
+        _check(self.lib.mb_set_hybrid_ctas(self.h, int(per_sm)), "mb_set_hybrid_ctas")
 
     def set_plan_steps(self, n):
         """Coarse steps per replayed graph (rounded up to whole scheduler periods)."""

@@ -125,3 +125,32 @@ def test_program_trace(mb, cuda_device):
     assert len(np.unique(keys, axis=0)) == len(tr)
     assert_same_state(g, a, b)
     assert len(b.program_trace()) == 0  # emptied by the read
+
+
+@pytest.mark.parametrize("prec", ["f32", "f16s", "f64", "f16c"])
+@pytest.mark.parametrize("name,split", [("n3", 0), ("g49", 0), ("c1", 0), ("n3", None)])
+def test_hybrid_equals_graph_bitwise(mb, cuda_device, name, split, prec):
+    """Graph mode "hybrid": the chain as executor launches between the bulk
+    interior kernels (split levels) gives the graph path's state bitwise, with
+    single steps, multi-step plans and the diagnostics loop."""
+    g = mb.geo_init(*make_ref.case(name)[:2])
+    a = run(mb, g, prec, True, 19, split=split)
+    b = run(mb, g, prec, "hybrid", 19, split=split)
+    assert_same_state(g, a, b)
+    da = a.evolution_diag(7)
+    db = b.evolution_diag(7)
+    for x, y in zip(da, db):
+        assert np.array_equal(x, y)
+    assert_same_state(g, a, b)
+
+
+@pytest.mark.parametrize("per_sm", [1, 3])
+def test_hybrid_grid_caps_bitwise(mb, cuda_device, per_sm):
+    g = mb.geo_init(*make_ref.case("n3")[:2])
+    a = run(mb, g, "f32", True, 13, split=0)
+    b = mb.MultiBlockLBM(g, "f32", graph="hybrid")
+    b.set_hybrid_ctas(per_sm)
+    b.set_split_cells(0)
+    b.init()
+    b.evolution(13)
+    assert_same_state(g, a, b)
