@@ -350,7 +350,18 @@ int mb_set_bulk_occupancy(mb_ctx *ctx, int ctas_per_sm);
  * block step.  Bit 2 takes the lines it applies to before bit 1.  On the
  * 3-level cylinder bit 2 measured the same step time as without it (the
  * spline's longer tail takes what the dropped launch saved), so it is off by
- * default.  Results are identical. */
+ * default.  Bit 3: the f_c points (f_c_boundary_transfer,
+ * multi/FH/assit_multi.h:273-314) whose fine cell the fine level's last
+ * substep has just updated run in a small launch beside that block step,
+ * which updates those fine cells itself (the step leaves them alone), when
+ * no operation in between touches their cells: the coarse level's next
+ * substep then waits for that launch, not for the fine step and a record
+ * launch after it (levels stepped by the two-cell kernel, and MB_PREC_F32U,
+ * keep the records).
+ * Bit 4: consecutive record ops share a launch only when all or none of them
+ * wait for the latest block step.  Bits 3 and 4 measured within run-to-run
+ * noise on the 3-level cylinder and are off by default.  Results are
+ * identical. */
 int mb_set_fusion(mb_ctx *ctx, int flags);
 
 /* ---- collision and boundary options ----------------------------------------

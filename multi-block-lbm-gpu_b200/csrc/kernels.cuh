@@ -262,6 +262,34 @@ struct StbOptions {
   double force[2];  // forcex, forcey of every cell
 };
 
+// ----------------------------------------------------------------------------
+// Per-block table used by the interface, drag and diagnostic kernels.
+// ----------------------------------------------------------------------------
+struct IfBlk {
+  void *F[2];
+  void *rho, *ux, *uy;
+  void *upx, *upy;
+  const uint8_t *flags;
+  int nx, ny, pitch, m;
+  long long plane;
+  double tau;
+};
+
+// An f_c point (f_c_boundary_transfer, multi/FH/assit_multi.h:273-314) done
+// beside the block step that updates its fine cell (k_fc_pull): block gid's
+// cell `cell` (flagged FL_FCSRC) gives coarse cell dcell of block dblk, F in
+// buffer dbuf, feq + para (f - feq) of its new values, and its rho/u.
+struct StbFc {
+  int gid, cell, dblk, dcell;
+  int bits, dbuf;  // bits: 4 write F, 8 write rho/u
+  double para;
+};
+constexpr uint8_t FL_FCSRC = 16;  // FLUID: fine point of an f_c line (on SOLID cells the bit marks a half-way wall)
+// A cell k_fc_pull updates: block gid, (i, j), and its f_c points fc[e0, e1).
+struct FcCell {
+  int gid, i, j, e0, e1, pad_;
+};
+
 struct StbParams {
   int nblk;
   int macro_all;     // write rho/u of every FLUID cell (else only CF_MACRO cells)
@@ -281,7 +309,13 @@ struct StbParams {
   double rho0, u0x, u0y;
   StbOptions opt;
   int tskip;         // leave cells flagged FL_TSKIP alone: a spline writes their next values
-  int pad_t;
+  int fcskip;        // leave FLUID cells flagged FL_FCSRC alone: k_fc_pull updates them
+  int fc_n;          // k_fc_pull: f_c points (fc, sorted by cell), targets in the block table fcblk
+  int fc_cells;      // k_fc_pull: the FL_FCSRC cells it updates (fccell)
+  int pad_fc;
+  const StbFc *fc;
+  const FcCell *fccell;
+  const IfBlk *fcblk;
   Shift sh;          // shift of the stored words (shifted precisions)
   StbBlk b[STB_MAX_BLOCKS];
 };
@@ -397,6 +431,39 @@ __device__ __forceinline__ void stb_pull(const StbBlk &B, int i, int j, typename
   }
 }
 
+// The f_c points fc[e0, e1) of a fine cell, from its new values out[] and its
+// rho/u m[] (f_c_boundary_transfer, multi/FH/assit_multi.h:273-314): what the
+// record kernel computes from the same values read back through the stored
+// type.
+template <int P>
+__device__ __forceinline__ void stb_fc_points(const StbParams &p, int e0, int e1, const typename Prec<P>::R *out,
+                                              const typename Prec<P>::R *m) {
+  using R = typename Prec<P>::R;
+  using S = typename Prec<P>::S;
+  for (int q = e0; q < e1; q++) {
+    const StbFc &e = p.fc[q];
+    const IfBlk &D = p.fcblk[e.dblk];
+    const R rh = m[0], ux = m[1], uy = m[2];
+    if (e.bits & 8) {
+      ((R *)D.rho)[e.dcell] = rh;
+      ((R *)D.ux)[e.dcell] = ux;
+      ((R *)D.uy)[e.dcell] = uy;
+    }
+    if (e.bits & 4) {
+      S *Fd = (S *)D.F[e.dbuf];
+      const R para = (R)e.para;
+#pragma unroll
+      for (int k = 0; k < 9; k++) {
+        R ft;  // the stored word read back, as ld_f does
+        if constexpr (Prec<P>::shifted) ft = to_r(from_r<S>(out[k])) + p.sh.v.s[k];
+        else ft = to_r(from_r<S>(out[k]));
+        const R fe = feq<R>(k, rh, ux, uy);
+        st_f<P>(Fd, k * D.plane + e.dcell, k, fe + para * (ft - fe), p.sh.v);
+      }
+    }
+  }
+}
+
 // The block step of cell (i, j) of block B (stb_finish below) with its new
 // values stored at cell cd of block D: a same-level copy target's values.
 // cc: the values are a c_c_boundary_transfer copy (multi/FH/assit_multi.h:38-44),
@@ -477,6 +544,7 @@ __device__ __forceinline__ void stb_finish(const StbParams &p, const StbBlk &B, 
   const bool wm = p.write_macros && (p.macro_all || (fl & 8));
 
   if (type == 0) {  // FLUID
+    if (p.fcskip && (fl & FL_FCSRC)) return;  // k_fc_pull updates it beside this step
     if (fl & 4) {   // block edge: equilibrium at rho0, U0 (stb2 :47-57), collide keeps it
 #pragma unroll
       for (int k = 0; k < 9; k++) {
@@ -544,6 +612,8 @@ __global__ void __launch_bounds__(128) k_cc_pull(const __grid_constant__ StbPara
   stb_finish_at<P, false>(p, B, e.si, e.sj, raw, B.flags[(long long)e.sj * B.pitch + e.si], D, e.tcell, true);
 }
 
+
+
 // Pulled values of a cell at least one cell from the block edge: every
 // neighbour is inside the block (constant offsets).
 template <int P, bool EF>
@@ -569,6 +639,34 @@ __device__ __forceinline__ void stb_cell_h(const StbParams &p, const StbBlk &B, 
 template <int P>
 __device__ __forceinline__ void stb_cell(const StbParams &p, const StbBlk &B, int i, int j) {
   stb_cell_h<P, false>(p, B, i, j);
+}
+
+// The FL_FCSRC cells of a fine level's block step, updated beside it (the
+// step leaves them alone: StbParams::fcskip) by the step's own per-cell
+// code, then their f_c points from the values read back: what reads the
+// coarse cells of those points waits for this small launch instead of the
+// whole fine step.  One thread per cell.
+template <int P>
+__global__ void __launch_bounds__(128) k_fc_pull(const __grid_constant__ StbParams p) {
+  using R = typename Prec<P>::R;
+  using S = typename Prec<P>::S;
+  pdl_trigger();
+  pdl_wait();
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= p.fc_cells) return;
+  const FcCell e = p.fccell[t];
+  const StbBlk &B = p.b[e.gid - p.a0];
+  stb_cell_h<P, false>(p, B, e.i, e.j);  // the step's own code (this launch's fcskip is 0)
+  // its points read the cell back, as the record kernel does
+  const long long c = (long long)e.j * B.pitch + e.i;
+  const S *Fo = (const S *)B.Fout;
+  R out[9], m[3];
+#pragma unroll
+  for (int k = 0; k < 9; k++) out[k] = to_r(Fo[k * B.plane + c]);
+  m[0] = ((const R *)B.rho)[c];
+  m[1] = ((const R *)B.ux)[c];
+  m[2] = ((const R *)B.uy)[c];
+  stb_fc_points<P>(p, e.e0, e.e1, out, m);
 }
 
 // Cell g (0 <= g < p.total) of a block-step launch: its block t and its
@@ -883,7 +981,7 @@ __device__ __forceinline__ void stb_cell_rows(const StbParams &p, const StbBlk &
 #pragma unroll
     for (int k = 0; k < 9; k++) raw[k] = ld_ef<EF>(Fin + (k * plane + c - (ey(k) * B.pitch + ex(k))));
     const uint8_t fl = B.flags[c];
-    if ((fl & 7) == 0) {  // FLUID away from the block edge
+    if ((fl & (7 | FL_FCSRC)) == 0) {  // FLUID away from the block edge, no f_c point
       R f[9];
 #pragma unroll
       for (int k = 0; k < 9; k++) f[k] = to_r(raw[k]);
@@ -973,7 +1071,7 @@ __device__ __forceinline__ void stb_pair(const StbParams &p, const StbBlk &B, in
     }
     const unsigned short fl2 = *(const unsigned short *)(B.flags + c);
     const uint8_t fa = uint8_t(fl2 & 0xff), fb = uint8_t(fl2 >> 8);
-    if (((fa | fb) & 7) == 0) {  // both FLUID away from the block edge
+    if (((fa | fb) & (7 | FL_FCSRC)) == 0) {  // both FLUID away from the block edge, no f_c point
       R f[9], oa[9], ob[9], ma[3], mb[3];
 #pragma unroll
       for (int k = 0; k < 9; k++) f[k] = to_r(a[k]);
@@ -1175,7 +1273,7 @@ __global__ void __launch_bounds__(TB_THREADS, 1) k_block_step_tb(const __grid_co
     const int i = x0 + tid;
     if (i >= 2 && i <= B.nx - 3) {
       const uint8_t fl = st[9 * C::SEG_BYTES + 16 + tid];
-      if ((fl & 7) == 0) {
+      if ((fl & (7 | FL_FCSRC)) == 0) {
         R f[9];
 #pragma unroll
         for (int k = 0; k < 9; k++) f[k] = to_r(((const S *)(st + k * C::SEG_BYTES))[tid + C::A - ex(k)]);
@@ -1271,7 +1369,7 @@ __device__ __forceinline__ void stb_quad_body(const StbParams &p, long long wt, 
   const bool inrow = i0 < B.pitch;
   const long long rowc = (long long)j * B.pitch;
   const uint32_t fl4 = inrow ? *(const uint32_t *)(B.flags + rowc + i0) : 0x03030303u;
-  const bool fast = inrow && (fl4 & 0x07070707u) == 0u && i0 >= clo && i0 + 3 <= chi;
+  const bool fast = inrow && (fl4 & 0x17171717u) == 0u && i0 >= clo && i0 + 3 <= chi;  // FLUID, off the edge, no f_c point
   const S *Fin = (const S *)B.Fin;
   // issue every load before any shuffle consumes one: nine quads and, for the
   // six directions with a column shift, the cell just outside the warp's span
@@ -1337,18 +1435,6 @@ __global__ void __launch_bounds__(256) k_block_step_q(const __grid_constant__ St
   else stb_quad_body<P, false>(p, wt, lane);
 }
 
-// ----------------------------------------------------------------------------
-// Per-block table used by the interface, drag and diagnostic kernels.
-// ----------------------------------------------------------------------------
-struct IfBlk {
-  void *F[2];
-  void *rho, *ux, *uy;
-  void *upx, *upy;
-  const uint8_t *flags;
-  int nx, ny, pitch, m;
-  long long plane;
-  double tau;
-};
 
 // ----------------------------------------------------------------------------
 // Interface point records: c_c_boundary_transfer, temporal_interpolation,

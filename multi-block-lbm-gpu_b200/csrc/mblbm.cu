@@ -161,6 +161,11 @@ struct mb_ctx {
   int fuse_cc = 1;
   int fuse_tmp = 0;  // splines do the next temporal interpolation of their line (mb_set_fusion bit 1)
   int fuse_early = 0;  // ... in place, beside the fine level's substep (mb_set_fusion bit 2)
+  // f_c points beside the fine level's last block step (mb_set_fusion bit 3)
+  // and record launches split by what they wait for (bit 4): both measured
+  // within run-to-run noise of the defaults on config 2, so off
+  int fuse_fc = 0;
+  int split_waits = 0;
   unsigned early_levels = 0;  // levels whose temporal edge cells carry CF_TSKIP
   // scheduler
   SchedState state;
@@ -349,6 +354,7 @@ template <int P> struct KStbPI { static void *ptr() { return (void *)k_block_ste
 template <int P> struct KStbQ { static void *ptr() { return (void *)k_block_step_q<P>; } };
 template <int P> struct KStbX { static void *ptr() { return (void *)k_block_step_x<P>; } };
 template <int P> struct KCcp { static void *ptr() { return (void *)k_cc_pull<P>; } };
+template <int P> struct KFcp { static void *ptr() { return (void *)k_fc_pull<P>; } };
 template <int P> struct KStbTb { static void *ptr() { return (void *)k_block_step_tb<P>; } };
 int tb_smem(int prec) {
   switch (prec) {
@@ -629,6 +635,7 @@ int lower_plan(mb_ctx *c, CompiledPlan &cp) {
       const bool quads = stb_uses_quads(c, n.level, n.region);
       d.stb = make_stb(c, n.a0, n.a1, n.parity, n.macro_all, 1, n.region, quads, n.ccpull);
       d.stb.tskip = n.tskip;
+      d.stb.fcskip = n.fcskip;
       // bulk: interiors of split levels, and whole levels streamed with
       // evict-first hints when bulk_levels is set
       d.background = (n.region == STB_INTERIOR) || (c->bulk_levels && n.region == STB_ALL && d.stb.evict_first);
@@ -668,6 +675,59 @@ int lower_plan(mb_ctx *c, CompiledPlan &cp) {
       d.block = dim3(DRAG_THREADS);
       d.grid = dim3(1);
       d.args[0] = &d.drag;
+    } else if (n.kind == NK_FCP) {
+      // the CF_FCSRC cells of the step's blocks and their f_c points
+      d.stb = make_stb(c, n.a0, n.a1, n.parity, n.macro_all, 1, STB_ALL, false, 0);
+      std::vector<StbFc> fc;
+      for (const FcFuse &e : n.fc) {
+        if (!(e.bits & (RB_WRITE_F | RB_WRITE_M))) continue;
+        StbFc x{};
+        x.gid = e.src_block;
+        x.cell = e.src_cell;
+        x.dblk = e.dst_block;
+        x.dcell = e.dst_cell;
+        x.bits = e.bits & (RB_WRITE_F | RB_WRITE_M);
+        x.dbuf = e.dst_buf;
+        x.para = e.para;
+        fc.push_back(x);
+      }
+      std::stable_sort(fc.begin(), fc.end(), [](const StbFc &u, const StbFc &v) {
+        return u.gid != v.gid ? u.gid < v.gid : u.cell < v.cell;
+      });
+      std::vector<FcCell> cells;
+      size_t e = 0;
+      for (int a = n.a0; a < n.a1; a++) {
+        const BlockLayout &b = c->bl[a];
+        for (int j = 0; j < b.ny; j++)
+          for (int i = 0; i < b.nx; i++) {
+            const long long cell = (long long)j * b.pitch + i;
+            if ((c->hflags[a][(size_t)cell] & (3 | CF_FCSRC)) != (CT_FLUID | CF_FCSRC)) continue;
+            FcCell fcl{};
+            fcl.gid = a;
+            fcl.i = i;
+            fcl.j = j;
+            while (e < fc.size() && (fc[e].gid < a || (fc[e].gid == a && fc[e].cell < cell))) e++;
+            fcl.e0 = (int)e;
+            while (e < fc.size() && fc[e].gid == a && fc[e].cell == cell) e++;
+            fcl.e1 = (int)e;
+            cells.push_back(fcl);
+          }
+      }
+      const size_t b1 = fc.size() * sizeof(StbFc), b2 = cells.size() * sizeof(FcCell);
+      unsigned char *dp = nullptr;
+      if (cudaMalloc(&dp, std::max<size_t>(b1 + b2, 16)) != cudaSuccess) return MB_ERR_NOMEM;
+      cp.dev_allocs.push_back(dp);
+      if (b1) MB_CUDA(cudaMemcpy(dp, fc.data(), b1, cudaMemcpyHostToDevice));
+      if (b2) MB_CUDA(cudaMemcpy(dp + b1, cells.data(), b2, cudaMemcpyHostToDevice));
+      d.stb.fc = (const StbFc *)dp;
+      d.stb.fc_n = (int)fc.size();
+      d.stb.fccell = (const FcCell *)(dp + b1);
+      d.stb.fc_cells = (int)cells.size();
+      d.stb.fcblk = c->d_blk;
+      d.func = kfunc<KFcp>(c->prec);
+      d.block = dim3(128);
+      d.grid = dim3((unsigned)((cells.size() + 127) / 128));
+      d.args[0] = &d.stb;
     } else if (n.kind == NK_CCP) {
       d.stb = make_stb(c, n.a0, n.a1, n.parity, 0, 1, STB_ALL, false, 0);
       d.stb.cc_list = c->d_cclist[n.level];
@@ -1203,13 +1263,28 @@ int program_status(mb_ctx *c) {
   return MB_ERR_TIMEOUT;
 }
 
+// Levels whose block-step kernel computes CF_FCSRC cells with the per-cell
+// code that k_fc_pull runs (every kernel but the two-cell one, variant 2), so
+// that an NK_FCP node gives bitwise the step's values.  In unshifted FP32
+// storage the per-cell code compiled into k_fc_pull rounds a few values
+// differently from the block-step kernels' copy: no level there.
+unsigned fc_levels(const mb_ctx *c) {
+  if (c->prec == MB_PREC_F32U) return 0;
+  unsigned m = 0;
+  for (int l = 0; l < MB_MAX_LEVEL; l++)
+    if (c->stb_variant[l] != 2) m |= 1u << l;
+  return m;
+}
+
 CompiledPlan *get_plan(mb_ctx *c, int n, bool final_macros, int *err, bool batch = false) {
   // batches and the persistent executor run the plain node kinds only
   // batches and the executor run the plain node kinds only
   const bool fuse = c->fuse_cc && !options_on(c) && !batch && c->use_graph < 3;
   const bool early = c->fuse_early && !options_on(c) && !batch && c->use_graph < 3;
+  const bool ffc = c->fuse_fc && !options_on(c) && !batch && c->use_graph < 3;
   std::string key = c->state.key() + "/" + std::to_string(n) + (final_macros ? "F" : "P") + (fuse ? "c" : "") +
-                    (c->fuse_tmp ? "t" : "") + (early ? "e" : "");
+                    (c->fuse_tmp ? "t" : "") + (early ? "e" : "") + (ffc ? "f" : "") +
+                    (c->split_waits ? "w" : "");
   auto it = c->plans.find(key);
   if (it != c->plans.end()) return it->second.get();
   auto cp = std::make_unique<CompiledPlan>();
@@ -1219,6 +1294,9 @@ CompiledPlan *get_plan(mb_ctx *c, int n, bool final_macros, int *err, bool batch
   if (fuse) pc.cc = &c->cc;
   pc.fuse_tmp = c->fuse_tmp != 0;
   if (early) pc.early_levels = c->early_levels;
+  pc.fuse_fc = ffc;
+  pc.fc_levels = fc_levels(c);
+  pc.split_waits = c->split_waits != 0;
   SchedState s = c->state;
   cp->nodes = pc.compile(s, n, final_macros);
   cp->end = s;
@@ -1235,8 +1313,10 @@ CompiledPlan *get_plan(mb_ctx *c, int n, bool final_macros, int *err, bool batch
 CompiledPlan *get_diag_plan(mb_ctx *c, int n, int *err) {
   const bool fuse = c->fuse_cc && !options_on(c) && c->use_graph < 3;
   const bool early = c->fuse_early && !options_on(c) && c->use_graph < 3;
-  const std::string key =
-      c->state.key() + "/" + std::to_string(n) + "D" + (fuse ? "c" : "") + (c->fuse_tmp ? "t" : "") + (early ? "e" : "");
+  const bool ffc = c->fuse_fc && !options_on(c) && c->use_graph < 3;
+  const std::string key = c->state.key() + "/" + std::to_string(n) + "D" + (fuse ? "c" : "") +
+                          (c->fuse_tmp ? "t" : "") + (early ? "e" : "") + (ffc ? "f" : "") +
+                    (c->split_waits ? "w" : "");
   auto it = c->plans.find(key);
   if (it != c->plans.end()) return it->second.get();
   auto cp = std::make_unique<CompiledPlan>();
@@ -1247,6 +1327,9 @@ CompiledPlan *get_diag_plan(mb_ctx *c, int n, int *err) {
   if (fuse) pc.cc = &c->cc;
   pc.fuse_tmp = c->fuse_tmp != 0;
   if (early) pc.early_levels = c->early_levels;
+  pc.fuse_fc = ffc;
+  pc.fc_levels = fc_levels(c);
+  pc.split_waits = c->split_waits != 0;
   SchedState s = c->state;
   cp->nodes = pc.compile_diag(s, n);
   cp->end = s;
@@ -1414,6 +1497,7 @@ extern "C" int mb_create(const mb_geometry *geo, int precision, mb_ctx **out) {
       }
   }
   mark_macro_sources(*geo, c->bl, c->hflags);
+  mark_fc_sources(*geo, c->bl, c->hflags);
   // same-level copies the block step of their level can perform: flag the
   // targets and keep, per target cell, where its source is
   c->cc = cc_levels(*geo, c->bl, c->hflags);
@@ -1819,14 +1903,16 @@ extern "C" int mb_set_cell_types(mb_ctx *c, int a, const int *types) {
       uint8_t &f = fl[(size_t)j * b.pitch + i];
       const int was = flag_code(f), t = types[(size_t)j * b.nx + i];
       if (movable(was) != movable(t) || (!movable(was) && t != was)) return MB_ERR_INVALID;
-      if (f & (CF_HBB | CF_SLIP)) alt_before++;
+      if ((f & 3) == CT_SOLID && (f & (CF_HBB | CF_SLIP))) alt_before++;  // on FLUID cells bit 16 is CF_FCSRC
       if (!movable(t)) continue;
       f = uint8_t((f & ~(3 | CF_HBB | CF_SLIP)) | (t == MB_FLUID ? CT_FLUID : CT_SOLID) |
                   (t == MB_SOLID_HBB ? CF_HBB : 0) | (t == MB_SOLID_SLIP ? CF_SLIP : 0));
-      if (f & (CF_HBB | CF_SLIP)) alt_after++;
+      if ((f & 3) == CT_SOLID && (f & (CF_HBB | CF_SLIP))) alt_after++;
     }
   cudaDeviceSynchronize();
   c->hflags[a] = fl;
+  mark_fc_sources(c->geo, c->bl, c->hflags);  // f_c points of FLUID cells only
+  fl = c->hflags[a];
   MB_CUDA(cudaMemcpy((void *)c->blk[a].flags, fl.data(), fl.size(), cudaMemcpyHostToDevice));
   c->n_alt_walls += alt_after - alt_before;
   int e;
@@ -1836,11 +1922,13 @@ extern "C" int mb_set_cell_types(mb_ctx *c, int a, const int *types) {
 }
 
 extern "C" int mb_set_fusion(mb_ctx *c, int flags) {
-  if (!c || flags < 0 || flags > 7) return MB_ERR_INVALID;
+  if (!c || flags < 0 || flags > 31) return MB_ERR_INVALID;
   cudaDeviceSynchronize();
   c->fuse_cc = flags & 1;
   c->fuse_tmp = (flags >> 1) & 1;
   c->fuse_early = (flags >> 2) & 1;
+  c->fuse_fc = (flags >> 3) & 1;
+  c->split_waits = (flags >> 4) & 1;
   c->plans.clear();
   return MB_OK;
 }
@@ -2163,7 +2251,7 @@ extern "C" int mb_plan_describe(mb_ctx *c, int n, char *buf, long long cap, long
   if (!cp) return err ? err : MB_ERR_INVALID;
   if (c->use_graph && c->use_graph != 3) mark_slack(*cp);
   std::string out;
-  static const char *kinds[] = {"stb", "rec", "spl", "ccp", "?", "drag", "l2"};
+  static const char *kinds[] = {"stb", "rec", "spl", "ccp", "fcp", "drag", "l2"};
   for (size_t q = 0; q < cp->dn.size(); q++) {
     const DevPlanNode &d = cp->dn[q];
     const PlanNode &nd = cp->nodes[q];
@@ -2173,6 +2261,7 @@ extern "C" int mb_plan_describe(mb_ctx *c, int n, char *buf, long long cap, long
                   d.background ? "bulk" : (d.slack ? "slack" : "chain"), nd.label.c_str());
     out += line;
     for (int p : d.deps) out += " " + std::to_string(p);
+    if (d.kind == NK_FCP) out += " ; fc " + std::to_string(d.stb.fc_n);
     out += "\n";
   }
   if (len) *len = (long long)out.size();

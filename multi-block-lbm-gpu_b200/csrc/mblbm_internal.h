@@ -19,6 +19,8 @@ enum : uint8_t {
   CF_EDGE = 4,  // i==0 || j==0 || i==nx-1 || j==ny-1
   CF_MACRO = 8, // rho/ux/uy of this FLUID cell are read by an interface op
   CF_HBB = 16,  // CT_SOLID cell that is a half-way bounce-back wall (MB_SOLID_HBB)
+  CF_FCSRC = 16, // CT_FLUID cell (not on the block edge) that is the fine point of an f_c line: a
+                 // block step may do that f_c point itself (PlanNode::fc); same bit as CF_HBB
   CF_SLIP = 32, // CT_SOLID cell that is an on-node free-slip wall (MB_SOLID_SLIP)
   CF_CCPULL = 64, // C_BOUNDARY target of a same-level copy run beside its level's block step (NK_CCP)
   CF_TSKIP = 128, // fine edge cell of a temporal interpolation that a spline may do early: a block step
@@ -89,10 +91,22 @@ struct SplTask {
 // a coarse step; NK_L2: one part of its error_L2 (region STB_INTERIOR: the
 // interiors of the split levels in a0's bit mask, else every other cell);
 // `level` holds the step's index within the plan for both.
-enum NodeKind { NK_STB = 0, NK_REC = 1, NK_SPL = 2, NK_CCP = 3, NK_DRAG = 5, NK_L2 = 6 };
+// NK_FCP: the CF_FCSRC cells of a block step and their f_c points, beside it.
+enum NodeKind { NK_STB = 0, NK_REC = 1, NK_SPL = 2, NK_CCP = 3, NK_FCP = 4, NK_DRAG = 5, NK_L2 = 6 };
 // cells a block-step node updates: all, those at distance >= 2 from the block
 // edge (they read nothing an interface op writes), or the distance <= 1 rim
 enum StbRegion { STB_ALL = 0, STB_INTERIOR = 1, STB_RIM = 2 };
+
+// An f_c point (f_c_boundary_transfer, multi/FH/assit_multi.h:273-314) done
+// by an NK_FCP node beside the block step that updates its fine cell: coarse
+// cell dst_cell of dst_block, F in buffer dst_buf, gets feq + para (f - feq)
+// of the fine cell's new values, and its rho/u.
+struct FcFuse {
+  int src_block, src_cell, dst_block, dst_cell;
+  uint8_t bits;     // RB_WRITE_F | RB_WRITE_M still live
+  uint8_t dst_buf;
+  double para;      // r (tau_c - 1) / (tau_f - 1), as the record kernel computes it
+};
 
 struct PlanNode {
   NodeKind kind;
@@ -104,6 +118,8 @@ struct PlanNode {
   int ccpull = 0;             // STB: skips CF_CCPULL cells (an NK_CCP node of the same level writes them)
   int part = 0;               // L2: the error_L2 part (L2_NPARTS)
   int tskip = 0;              // STB: leaves CF_TSKIP cells alone (a spline writes them)
+  int fcskip = 0;             // STB: leaves CF_FCSRC cells alone (an NK_FCP node updates them)
+  std::vector<FcFuse> fc;     // FCP: the f_c points it does
   std::vector<Rec> recs;      // REC
   std::vector<std::pair<int, int>> ops;  // REC: (first record, count) of each reference line op
   double tw[4][3] = {};       // REC: temporal weight triples (a, b, c)
@@ -184,6 +200,14 @@ struct PlanCompiler {
   // level's substep between them leaving the edge cells alone (fuse_early);
   // their edge cells carry CF_TSKIP
   unsigned early_levels = 0;
+  // f_c points whose fine cell the level's last block step has just updated
+  // run in an NK_FCP node beside that step (FcFuse), which updates the
+  // CF_FCSRC cells of the step, when no op between them touches their cells
+  bool fuse_fc = false;
+  unsigned fc_levels = ~0u;  // fine levels (bit per level) whose f_c points may fuse
+  // record launches keep ops that wait for the latest block step apart from
+  // ops that do not
+  bool split_waits = false;
   PlanCompiler(const mb_geometry &g_, const std::vector<BlockLayout> &bl_,
                const std::vector<std::vector<uint8_t>> &fl, const std::vector<SplLine> &sl)
       : g(g_), bl(bl_), flags(fl), spl_lines(sl) {}
@@ -205,5 +229,9 @@ struct PlanCompiler {
 // Cells whose rho/ux/uy an interface op reads (the CF_MACRO attribute).
 void mark_macro_sources(const mb_geometry &g, const std::vector<BlockLayout> &bl,
                         std::vector<std::vector<uint8_t>> &flags);
+// FLUID cells off the block edge that are fine points of f_c lines (CF_FCSRC);
+// the bit is cleared on every other FLUID cell.
+void mark_fc_sources(const mb_geometry &g, const std::vector<BlockLayout> &bl,
+                     std::vector<std::vector<uint8_t>> &flags);
 
 }  // namespace mblbm

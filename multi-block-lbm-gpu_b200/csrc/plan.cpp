@@ -56,6 +56,7 @@ struct Whole {
   uint8_t dlo, dhi;
   bool skip_cc = false;  // CF_CCPULL cells excluded (written by an NK_CCP node instead)
   bool skip_t = false;   // CF_TSKIP cells excluded (written by a spline instead)
+  bool skip_fc = false;  // FLUID CF_FCSRC cells excluded (written by an NK_FCP node instead)
 };
 constexpr uint8_t DMAX = 255;
 
@@ -67,8 +68,8 @@ struct Access {
   void write(uint64_t k) { w.insert(k); ws.insert(summ(k)); }
   void read_whole(uint32_t s, uint8_t dlo = 0, uint8_t dhi = DMAX) { wr.push_back({s, false, dlo, dhi}); rs.insert(s); }
   void write_whole(uint32_t s, bool fo, uint8_t dlo = 0, uint8_t dhi = DMAX, bool skip_cc = false,
-                   bool skip_t = false) {
-    ww.push_back({s, fo, dlo, dhi, skip_cc, skip_t});
+                   bool skip_t = false, bool skip_fc = false) {
+    ww.push_back({s, fo, dlo, dhi, skip_cc, skip_t, skip_fc});
     ws.insert(s);
   }
   void merge(const Access &o) {
@@ -129,6 +130,27 @@ void mark_macro_sources(const mb_geometry &g, const std::vector<BlockLayout> &bl
     const mb_line &lf = g.Line_Inf_F[b];
     const int r = g.Areas[lf.areaf_n].m / g.Areas[lf.areac_n].m;
     mark_line(g, bl, flags, lf.areaf_n, lf.line_F, lf.Nc, r);
+  }
+}
+
+void mark_fc_sources(const mb_geometry &g, const std::vector<BlockLayout> &bl,
+                     std::vector<std::vector<uint8_t>> &flags) {
+  const mb_layout &L = g.layout;
+  for (size_t a = 0; a < flags.size(); a++)
+    for (auto &f : flags[a])
+      if ((f & 3) == CT_FLUID) f = uint8_t(f & ~CF_FCSRC);
+  for (int b = 0; b < L.number_line; b++) {
+    const mb_line &lf = g.Line_Inf_F[b];
+    const int a = lf.areaf_n;
+    const int r = g.Areas[a].m / g.Areas[lf.areac_n].m;
+    for (int ip = 0; ip < lf.Nc; ip++) {
+      int i, j;
+      if (lf.line_C.xstart == lf.line_C.xend) { i = lf.line_F.xstart; j = lf.line_F.ystart + ip * r; }
+      else { i = lf.line_F.xstart + ip * r; j = lf.line_F.ystart; }
+      if (i < 0 || j < 0 || i >= bl[a].nx || j >= bl[a].ny) continue;
+      uint8_t &f = flags[a][(size_t)j * bl[a].pitch + i];
+      if ((f & (3 | CF_EDGE)) == CT_FLUID) f = uint8_t(f | CF_FCSRC);
+    }
   }
 }
 
@@ -469,8 +491,32 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
     if (d < wh.dlo || d > wh.dhi) return false;
     if (wh.skip_cc && (flags[blk][cell] & CF_CCPULL)) return false;
     if (wh.skip_t && (flags[blk][cell] & CF_TSKIP)) return false;
+    if (wh.skip_fc && (flags[blk][cell] & (3 | CF_FCSRC)) == (CT_FLUID | CF_FCSRC)) return false;
     return !wh.fluid_only || is_fluid(blk, cell);
   };
+
+  // CF_FCSRC cells of each block (the fine points of f_c lines that are FLUID
+  // and off the block edge): what an NK_FCP node updates beside the step
+  std::vector<std::vector<long long>> fcsrc(L.number_area);
+  if (fuse_fc) {
+    for (int b = 0; b < L.number_line; b++) {
+      const mb_line &lf = g.Line_Inf_F[b];
+      const int a = lf.areaf_n;
+      const int r = g.Areas[a].m / g.Areas[lf.areac_n].m;
+      for (int ip = 0; ip < lf.Nc; ip++) {
+        int i, j;
+        if (lf.line_C.xstart == lf.line_C.xend) { i = lf.line_F.xstart; j = lf.line_F.ystart + ip * r; }
+        else { i = lf.line_F.xstart + ip * r; j = lf.line_F.ystart; }
+        if (i < 0 || j < 0 || i >= bl[a].nx || j >= bl[a].ny) continue;
+        const long long cell = pitch_cell(a, i, j);
+        if ((flags[a][(size_t)cell] & (3 | CF_FCSRC)) == (CT_FLUID | CF_FCSRC)) fcsrc[a].push_back(cell);
+      }
+    }
+    for (auto &v : fcsrc) {
+      std::sort(v.begin(), v.end());
+      v.erase(std::unique(v.begin(), v.end()), v.end());
+    }
+  }
 
   // One write of an op (the F part or the M part of a record, or the rho/u
   // write of a spline point) with the reads it needs.
@@ -480,6 +526,7 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
     uint64_t wkey;
     std::vector<uint64_t> rkeys;
     bool live = true;
+    bool fc = false;  // an f_c point done by block-step node `node` (its fc entry idx)
   };
   struct OpInfo {
     bool stb = false;
@@ -487,18 +534,22 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
     bool tskip = false;         // STB: leaves CF_TSKIP cells alone
     std::vector<int> stb_nodes; // STB: its nodes
     std::vector<int> cc_nodes;  // STB: NK_CCP nodes, one per launch chunk with copies
+    std::vector<int> fc_nodes;  // STB: NK_FCP node of each launch chunk with CF_FCSRC cells (-1: none)
     int diag = -1;              // SNAP / DRAG / L2 op: its Op::Kind
     int level = -1;
     std::vector<int> parity;
     std::vector<Part> parts;
     std::vector<uint64_t> always_r, always_w;  // spline: gathered cells / written slot
     int node = -1;
+    Access ac;            // point accesses of a line op (records, splines)
+    bool has_ac = false;
   };
   std::vector<OpInfo> info(ops.size());
   std::vector<PlanNode> nodes;
   std::vector<Access> acc;  // forward (unpruned) sets: used only to decide batching
   int open = -1;
   int last_stb = -1;  // latest STB op; same-level copies right after it can fuse into it
+  bool open_after_stb = false;  // the open launch's ops touch blocks of the latest step's level
   // Reads of a C_BOUNDARY cell's F that no op has written since its block's
   // last step may read the step's input buffer instead: the step copies
   // C_BOUNDARY cells unchanged, so both buffers hold the same value there,
@@ -516,6 +567,49 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
     if ((f & 3) != CT_COPY || (f & CF_CCPULL) || stb_op[b] < 0) return p;
     auto it = lastw.find(fkey(p, b, cell));
     return (it == lastw.end() || it->second.op < stb_op[b]) ? p ^ 1 : p;
+  };
+
+  // NK_FCP node that can do f_c point (fine cell cf of block Fb, coarse
+  // target in block Cb; keys of its reads and writes) for op oi, or -1: the
+  // fine block's latest step updates cf (an off-edge FLUID cell whose rho/u
+  // it writes), and no op since that step writes what the point reads or
+  // touches what it writes.  The node updates the step's CF_FCSRC cells
+  // beside it (the step leaves them alone) and then does its points.
+  auto level_of = [&](int a) {
+    for (int l = 0; l < L.LEVEL; l++)
+      if (a >= L.ASP[l] && a < L.ASP[l + 1]) return l;
+    return -1;
+  };
+  auto fc_host = [&](size_t oi, int Fb, int Cb, long long cf, uint64_t kSF, uint64_t kSM, uint64_t kDF,
+                     uint64_t kDM) -> int {
+    const int so = stb_op[Fb];
+    if (!fuse_fc || so < 0 || !((fc_levels >> level_of(Fb)) & 1u)) return -1;
+    const uint8_t f = flags[Fb][(size_t)cf];
+    if ((f & (3 | CF_EDGE | CF_FCSRC | CF_MACRO)) != (CT_FLUID | CF_FCSRC | CF_MACRO)) return -1;
+    const int lf = level_of(Fb), lc = level_of(Cb);
+    for (size_t q = size_t(so) + 1; q < oi; q++) {
+      const OpInfo &Q = info[q];
+      if (Q.stb) {
+        if (ops[q].level == lf || ops[q].level == lc) return -1;
+        continue;
+      }
+      if (Q.diag >= 0) return -1;
+      if (!Q.has_ac) {  // same-level copies run beside their step: targets are C_BOUNDARY cells of their level
+        if (ops[q].level == lc || ops[q].level == lf) return -1;
+        continue;
+      }
+      if (Q.ac.w.count(kSF) || Q.ac.w.count(kSM) || Q.ac.w.count(kDF) || Q.ac.w.count(kDM) || Q.ac.r.count(kDF) ||
+          Q.ac.r.count(kDM))
+        return -1;
+    }
+    const OpInfo &S = info[so];
+    const size_t chunk = size_t((Fb - L.ASP[lf]) / 16);
+    if (chunk >= S.fc_nodes.size() || S.fc_nodes[chunk] < 0) return -1;
+    const int q = S.fc_nodes[chunk];
+    if (nodes[q].fc.empty())  // first point: the chunk's step nodes leave the CF_FCSRC cells to it
+      for (int sn : S.stb_nodes)
+        if (nodes[sn].a0 == nodes[q].a0) nodes[sn].fcskip = 1;
+    return q;
   };
 
   // ---- forward: expand ops into records and batch them ---------------------
@@ -580,6 +674,24 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
           nodes.push_back(nd);
           acc.push_back(Access());
         }
+        int fcn = -1;  // the chunk's NK_FCP node, used only if an f_c point fuses into it
+        bool any = false;
+        for (int a = a0; a < a1; a++) any = any || !fcsrc[a].empty();
+        if (fuse_fc && any) {
+          PlanNode nd;
+          nd.kind = NK_FCP;
+          nd.level = o.level;
+          nd.macro_all = o.macro_all;
+          nd.a0 = a0;
+          nd.a1 = a1;
+          for (int a = a0; a < a1; a++)
+            if (o.parity[a]) nd.parity |= (1ull << a);
+          nd.label = "fcp L" + std::to_string(o.level);
+          fcn = int(nodes.size());
+          nodes.push_back(nd);
+          acc.push_back(Access());
+        }
+        I.fc_nodes.push_back(fcn);
       }
       continue;
     }
@@ -722,8 +834,34 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
           rr.m2 = uint8_t(lw->second.marker);
           rF = key(RK_SLOT, lw->second.line, lw->second.marker);
         }
+        const uint64_t kDF = fkey(pC, Cb, cc), kDM = key(RK_M, Cb, cc), kSF = rF, kSM = key(RK_M, Fb, cf);
+        const int sn = rr.type == REC_FC ? fc_host(oi, Fb, Cb, cf, kSF, kSM, kDF, kDM) : -1;
+        if (sn >= 0) {  // done by the fine level's last block step
+          FcFuse e{};
+          e.src_block = Fb;
+          e.src_cell = int(cf);
+          e.dst_block = Cb;
+          e.dst_cell = int(cc);
+          e.bits = RB_WRITE_F | RB_WRITE_M;
+          e.dst_buf = uint8_t(pC);
+          e.para = (double)(g.Areas[Fb].m / g.Areas[Cb].m) * (g.Areas[Cb].tau - 1.0) / (g.Areas[Fb].tau - 1.0);
+          const int idx = int(nodes[sn].fc.size());
+          nodes[sn].fc.push_back(e);
+          Part pf{sn, idx, RB_WRITE_F, kDF, {kSF, kSM}};
+          pf.fc = true;
+          Part pm{sn, idx, RB_WRITE_M, kDM, {kSM}};
+          pm.fc = true;
+          I.parts.push_back(pf);
+          I.parts.push_back(pm);
+          lastw[kDF] = LastWrite{int(oi)};
+          ac.read(kSF);
+          ac.read(kSM);
+          ac.write(kDF);
+          ac.write(kDM);
+          continue;
+        }
         recs.push_back(rr);
-        rparts.push_back({fkey(pC, Cb, cc), key(RK_M, Cb, cc), {rF, key(RK_M, Fb, cf)}, {key(RK_M, Fb, cf)}});
+        rparts.push_back({kDF, kDM, {rF, kSM}, {kSM}});
       }
     } else if (is_spl) {
       const mb_line &l = g.Line_Inf_C[o.line];
@@ -787,15 +925,47 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
     for (auto k : spl_wM) ac.write(k);
     for (auto k : tmp_w) ac.write(k);
     for (auto k : tmp_r) ac.read(k);
+    I.ac = ac;
+    I.has_ac = true;
+    if (!is_spl && recs.empty()) continue;  // every point runs inside a block step (f_c fused)
 
     const NodeKind want = is_spl ? NK_SPL : NK_REC;
-    bool join = (open >= 0 && nodes[open].kind == want);
+    // whether this op touches a block the latest block step updated: a launch
+    // mixing ops that wait for that step with ops that do not would hold the
+    // latter back (a temporal interpolation of the coarser level behind the
+    // finer level's c_f, say)
+    bool after_stb = false;
+    if (last_stb >= 0 && split_waits) {
+      const int ls = ops[last_stb].level;
+      auto hits = [&](uint64_t k) {
+        const uint64_t kind = k >> 56;
+        if (kind != RK_F0 && kind != RK_F1 && kind != RK_M) return false;
+        const int a = int((k >> 48) & 0xff);
+        return a >= L.ASP[ls] && a < L.ASP[ls + 1];
+      };
+      for (auto k : ac.r) after_stb = after_stb || hits(k);
+      for (auto k : ac.w) after_stb = after_stb || hits(k);
+    }
+    bool join = (open >= 0 && nodes[open].kind == want && open_after_stb == after_stb);
     int nruns = 0;
+    // a run of records shares type and buffer bits and is affine in the point
+    // index (an f_c line whose points partly moved into an NK_FCP node has gaps)
+    auto breaks = [&](size_t q0, size_t q) {
+      if (cc_points || run_key(recs[q]) != run_key(recs[q0]) || recs[q].type == REC_FC_SLOT ||
+          recs[q0].type == REC_FC_SLOT)
+        return true;
+      if (q - q0 < 2) return false;
+      const long long dd = (long long)recs[q0 + 1].dst_cell - recs[q0].dst_cell,
+                      ds = (long long)recs[q0 + 1].src - recs[q0].src;
+      return (long long)recs[q].dst_cell - recs[q - 1].dst_cell != dd || (long long)recs[q].src - recs[q - 1].src != ds;
+    };
     if (want == NK_REC) {
       nruns = recs.empty() ? 0 : 1;
-      for (size_t q = 1; q < recs.size(); q++)
-        nruns += cc_points || run_key(recs[q]) != run_key(recs[q - 1]) || recs[q].type == REC_FC_SLOT ||
-                 recs[q - 1].type == REC_FC_SLOT;
+      for (size_t q = 1, q0 = 0; q < recs.size(); q++)
+        if (breaks(q0, q)) {
+          nruns++;
+          q0 = q;
+        }
     }
     if (join && want == NK_REC && int(nodes[open].ops.size()) + nruns > PLAN_MAX_REC_OPS) join = false;
     if (join && want == NK_SPL && int(nodes[open].spl.size()) >= PLAN_MAX_SPL_TASKS) join = false;
@@ -822,6 +992,7 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
       nodes.push_back(nd);
       acc.push_back(Access());
       open = int(nodes.size()) - 1;
+      open_after_stb = after_stb;
     }
     PlanNode &nd = nodes[open];
     I.node = open;
@@ -843,8 +1014,7 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
       } else {  // runs of records with the same type and buffer bits (each run is affine)
         size_t q0 = 0;
         for (size_t q = 1; q <= recs.size(); q++)
-          if (q == recs.size() || run_key(recs[q]) != run_key(recs[q0]) || recs[q].type == REC_FC_SLOT ||
-              recs[q0].type == REC_FC_SLOT) {
+          if (q == recs.size() || breaks(q0, q)) {
             nd.ops.push_back({int(nd.recs.size() + q0), int(q - q0)});
             q0 = q;
           }
@@ -927,12 +1097,23 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
     }
     if (I.stb) {
       // the op's nodes together write F of buffer 1-p and rho/u of FLUID
-      // cells and read F of buffer p, over the whole block
+      // cells and read F of buffer p, over the whole block; CF_FCSRC cells of
+      // chunks with a used NK_FCP node are that node's
+      auto fcp_used = [&](int a) {
+        const size_t chunk = size_t((a - L.ASP[I.level]) / 16);
+        return chunk < I.fc_nodes.size() && I.fc_nodes[chunk] >= 0 && !nodes[I.fc_nodes[chunk]].fc.empty();
+      };
       for (int a = L.ASP[I.level]; a < L.ASP[I.level + 1]; a++) {
         const int p = I.parity[a];
-        apply_layer({uint32_t(((p ? RK_F0 : RK_F1) << 8) | a), false, 0, DMAX, I.cc_fused, I.tskip}, true);
-        apply_layer({uint32_t((RK_M << 8) | a), true, 0, DMAX, I.cc_fused}, true);
+        const bool fs = fcp_used(a);
+        apply_layer({uint32_t(((p ? RK_F0 : RK_F1) << 8) | a), false, 0, DMAX, I.cc_fused, I.tskip, fs}, true);
+        apply_layer({uint32_t((RK_M << 8) | a), true, 0, DMAX, I.cc_fused, false, fs}, true);
         apply_layer({uint32_t(((p ? RK_F1 : RK_F0) << 8) | a), false, 0, DMAX}, false);
+        if (fs)
+          for (long long cell : fcsrc[a]) {
+            set_state(fkey(p ^ 1, a, cell), true);
+            set_state(key(RK_M, a, cell), true);
+          }
       }
       if (I.cc_fused)  // the copies beside the step write F and rho/u of their targets
         for (const CcLink &lk : (*cc)[I.level].links) {
@@ -952,7 +1133,8 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
     for (Part &pt : I.parts) {
       if (pt.live) continue;
       PlanNode &nd = nodes[pt.node];
-      if (pt.bit) nd.recs[pt.idx].bits &= uint8_t(~pt.bit);
+      if (pt.fc) nd.fc[pt.idx].bits &= uint8_t(~pt.bit);
+      else if (pt.bit) nd.recs[pt.idx].bits &= uint8_t(~pt.bit);
       else nd.spl_mask.at(pt.idx) = 0;
     }
   }
@@ -967,8 +1149,23 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
       const int p = int((nodes[q].parity >> a) & 1);
       fin[q].read_whole(uint32_t(((p ? RK_F1 : RK_F0) << 8) | a), rlo, rhi);
       fin[q].write_whole(uint32_t(((p ? RK_F0 : RK_F1) << 8) | a), false, wlo, whi, nodes[q].ccpull != 0,
-                         nodes[q].tskip != 0);
-      fin[q].write_whole(uint32_t((RK_M << 8) | a), true, wlo, whi, nodes[q].ccpull != 0);
+                         nodes[q].tskip != 0, nodes[q].fcskip != 0);
+      fin[q].write_whole(uint32_t((RK_M << 8) | a), true, wlo, whi, nodes[q].ccpull != 0, false,
+                         nodes[q].fcskip != 0);
+    }
+  }
+  for (size_t q = 0; q < nodes.size(); q++) {  // NK_FCP: the CF_FCSRC cells, pulled from the step's input
+    if (nodes[q].kind != NK_FCP || nodes[q].fc.empty()) continue;
+    for (int a = nodes[q].a0; a < nodes[q].a1; a++) {
+      const int p = int((nodes[q].parity >> a) & 1);
+      for (long long cell : fcsrc[a]) {
+        fin[q].write(fkey(p ^ 1, a, cell));
+        fin[q].write(key(RK_M, a, cell));
+        for (int k = 0; k < 9; k++) {
+          static const int EX[9] = {0, 1, 0, -1, 0, 1, -1, -1, 1}, EY[9] = {0, 0, 1, 0, -1, 1, 1, -1, -1};
+          fin[q].read(fkey(p, a, cell - ((long long)EY[k] * bl[a].pitch + EX[k])));
+        }
+      }
     }
   }
   for (auto &I : info) {
@@ -1016,13 +1213,15 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
     }
   }
   for (auto &I : info) {
-    if (I.stb || I.node < 0 || I.diag >= 0) continue;
-    Access &A = fin[I.node];
-    for (auto &pt : I.parts) {
+    if (I.stb || I.diag >= 0) continue;
+    for (auto &pt : I.parts) {  // a fused f_c point belongs to its block-step node
       if (!pt.live) continue;
+      Access &A = fin[pt.node];
       A.write(pt.wkey);
       for (auto k : pt.rkeys) A.read(k);
     }
+    if (I.node < 0) continue;
+    Access &A = fin[I.node];
     for (auto k : I.always_r) A.read(k);
     for (auto k : I.always_w) A.write(k);
   }
@@ -1032,6 +1231,7 @@ std::vector<PlanNode> PlanCompiler::build(const std::vector<Op> &ops) const {
   std::vector<Access> kacc;
   for (size_t q = 0; q < nodes.size(); q++) {
     PlanNode &nd = nodes[q];
+    if (nd.kind == NK_FCP && nd.fc.empty()) continue;  // no f_c point fused: its step updates the cells
     if (nd.kind == NK_REC) {
       // ops keep their point ranges (each is affine in the point index); an op
       // whose every write died is dropped whole

@@ -383,12 +383,14 @@ def test_step_diag_equals_step_by_step(mb, cuda_device, prec, split, graph):
 @pytest.mark.parametrize("split,variant", [(10**12, 0), (0, 0), (10**12, 4), (0, 4), (0, 3), (0, 5)])
 @pytest.mark.parametrize("name,prec", [("n3", "f32"), ("g49", "f64"), ("g25", "f16s"), ("n3", "f16c")])
 def test_fused_copies_bitwise(mb, cuda_device, name, prec, split, variant, graph):
-    """Same-level copies done inside the block step (mb_set_fusion bit 0) and
-    temporal interpolations done by the splines (bits 1 and 2), alone and
-    together, give bitwise the state of separate launches."""
+    """Same-level copies done inside the block step (mb_set_fusion bit 0),
+    temporal interpolations done by the splines (bits 1 and 2), f_c points
+    inside the fine steps (bit 3) and record launches split by what they wait
+    for (bit 4), alone and together, give bitwise the state of separate
+    launches."""
     g = mb.geo_init(*make_ref.case(name)[:2])
     sims = []
-    for fuse in (0, 1, 2, 3, 4, 5, 7):
+    for fuse in (0, 1, 2, 3, 4, 5, 7, 9, 17, 25, 31):
         s = mb.MultiBlockLBM(g, prec, graph=graph)
         s.set_fusion(fuse)
         s.set_split_cells(split)
@@ -505,3 +507,69 @@ def test_stochastic_rounding_variants_bitwise(mb, orc, cuda_device, split, prec)
         f32.set_rounding("stochastic")
     f32.set_rounding("nearest")
     f32.close()
+
+
+@pytest.mark.parametrize("name,prec,variant,split,graph", [
+    ("n3", "f32", 0, None, True), ("n3", "f32", 1, 0, True), ("n3", "f16s", 4, None, True),
+    ("n3", "f16c", 3, 0, False), ("n3", "f64", 0, None, True), ("g49", "f32", 5, 0, True),
+    ("c1", "f32", 0, None, True), ("g25", "f16s", 4, 0, False), ("n3", "f32u", 0, None, True),
+    ("n3", "f32u", 2, None, True)])
+def test_fc_fusion_bitwise(mb, cuda_device, name, prec, variant, split, graph):
+    """f_c points done inside the fine level's last block step (mb_set_fusion
+    bit 3) give bitwise the state, drag and L2 series of the record launches,
+    for every block-step kernel; the plan of the nested layout carries them."""
+    g = mb.geo_init(*make_ref.case(name)[:2])
+    sims = []
+    for flags in (1, 9, 25):
+        s = mb.MultiBlockLBM(g, prec, graph=graph)
+        s.set_fusion(flags)
+        for lvl in range(g.layout.LEVEL):
+            s.set_stb_variant(lvl, variant)
+        if split is not None:
+            s.set_split_cells(split)
+        s.init()
+        s.evolution(13)
+        sims.append(s)
+    if name == "n3" and split is None:  # split fine levels keep f_c sources in their bulk interiors: records
+        # the two-cell kernel (variant 2) computes cells in its own paired code: records
+        # and in unshifted FP32 the per-cell code compiled into k_fc_pull rounds differently: records
+        assert (" ; fc " in sims[1].plan_description(6)) == (variant != 2 and prec != "f32u")
+        assert " ; fc " not in sims[0].plan_description(6)
+    a = sims[0]
+    for b in sims[1:]:
+        for k in range(g.layout.number_area):
+            fa, fb = a.fields(k), b.fields(k)
+            for key in ("F", "rho", "ux", "uy"):
+                assert np.array_equal(fa[key], fb[key]), (k, key)
+    da = a.evolution_diag(8)
+    for b in sims[1:]:
+        db = b.evolution_diag(8)
+        for x, y in zip(da, db):
+            assert np.array_equal(x, y)
+        for k in range(g.layout.number_area):
+            assert np.array_equal(a.fields(k)["F"], b.fields(k)["F"]), k
+    for s in sims:
+        s.close()
+
+
+def test_fc_fusion_after_cell_type_change(mb, cuda_device):
+    """Cell types changed through mb_set_cell_types keep the f_c source marks:
+    fused and record f_c points still agree bitwise."""
+    g = mb.geo_init(*make_ref.case("n3")[:2])
+    sims = []
+    for flags in (1, 9):
+        s = mb.MultiBlockLBM(g, "f32")
+        s.set_fusion(flags)
+        s.init()
+        a = g.layout.number_area - 1
+        A = g.Areas[a]
+        t = s.fields(a)["solid"].copy()
+        t[A.ny // 2, A.nx // 2 - 3] = 1  # one more solid cell inside the finest block
+        s.set_cell_types(a, t)
+        s.init()
+        s.evolution(11)
+        sims.append(s)
+    for k in range(g.layout.number_area):
+        assert np.array_equal(sims[0].fields(k)["F"], sims[1].fields(k)["F"]), k
+    for s in sims:
+        s.close()
