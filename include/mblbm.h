@@ -326,9 +326,11 @@ int mb_set_stream_cells(mb_ctx *ctx, long long cells, int bulk);
  * shared addresses and vector accesses, 256 pairs per CTA (same coverage as 3),
  * 5 = bulk asynchronous copies: persistent CTAs stage the nine input row
  * segments of 256 cells in shared memory with cp.async.bulk and mbarriers
- * (interiors of split levels; the other regions use 0).
- * Default 0; every level uses 4 in MB_PREC_F16S, level 0 uses 1 in
- * MB_PREC_F32 and MB_PREC_F32U.  Results are identical. */
+ * (interiors of split levels; the other regions use 0), 6 = octets (16-bit
+ * stored forms only; other precisions run 0): a lane steps eight cells of a
+ * row with one 16-byte load and store per direction.
+ * Default 0; every level uses 4 in MB_PREC_F16S and MB_PREC_F16C, level 0
+ * uses 4 in MB_PREC_F32 and MB_PREC_F32U.  Results are identical. */
 int mb_set_stb_variant(mb_ctx *ctx, int level, int variant);
 /* Caps the grid of interior (bulk) block-step launches at ctas_per_sm CTAs of
  * 256 threads per SM (0 = uncapped), leaving CTA slots on every SM for the

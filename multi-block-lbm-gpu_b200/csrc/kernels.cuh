@@ -1435,6 +1435,167 @@ __global__ void __launch_bounds__(256) k_block_step_q(const __grid_constant__ St
   else stb_quad_body<P, false>(p, wt, lane);
 }
 
+// Two 16-bit stored words packed in one 32-bit word (the lower cell in the
+// low half), as arithmetic values, and back.  The collision has already
+// rounded its outputs to values of the stored type (stochastic rounding), so
+// packing them rounds nothing further.
+__device__ __forceinline__ void unpack_h2(unsigned int w, float &lo, float &hi, const __half *) {
+  const float2 v = __half22float2(*(const __half2 *)&w);
+  lo = v.x;
+  hi = v.y;
+}
+__device__ __forceinline__ void unpack_h2(unsigned int w, float &lo, float &hi, const h16c *) {
+  lo = h16c_decode(w & 0xffffu);
+  hi = h16c_decode(w >> 16);
+}
+__device__ __forceinline__ unsigned int pack_h2(float lo, float hi, const __half *) {
+  const __half2 v = __floats2half2_rn(lo, hi);
+  return *(const unsigned int *)&v;
+}
+__device__ __forceinline__ unsigned int pack_h2(float lo, float hi, const h16c *) {
+  return h16c_encode(lo) | (h16c_encode(hi) << 16);
+}
+template <bool EF> __device__ __forceinline__ uint4 ld_oct(const void *p) {
+  if constexpr (EF) return __ldcs((const uint4 *)p);
+  else return *(const uint4 *)p;
+}
+template <bool EF> __device__ __forceinline__ void st_oct(void *p, uint4 v) {
+  if constexpr (EF) __stcs((uint4 *)p, v);
+  else *(uint4 *)p = v;
+}
+
+// The block step on octets, for the 16-bit stored forms: a warp owns 256
+// consecutive cells of one row and each lane eight of them, moved with one
+// 16-byte load and store per direction (four packed pairs of words).  The
+// +-1 shift of the pulled column is a byte permutation of neighbouring
+// pairs, with the word beyond the lane's octet from the neighbouring lane
+// (shuffle) or, at the two ends of the warp's span, from one scalar load.
+// Each pair of cells is unpacked, collided cell by cell with the per-cell
+// code (same values and the same stochastic rounding as every other
+// variant) and packed back in place.  Octets that are not all FLUID
+// interior cells of the region run the per-cell stb_cell_h for their cells.
+template <int P, bool EF>
+__device__ __forceinline__ void stb_oct_body(const StbParams &p, long long wt, int lane) {
+  using S = typename Prec<P>::S;
+  static_assert(sizeof(S) == 2, "octets are for the 16-bit stored forms");
+  int t = 0;
+#pragma unroll 1
+  while (t + 1 < p.nblk && wt >= p.b[t + 1].wt0) t++;
+  const StbBlk &B = p.b[t];
+  const int local = int(wt - B.wt0);
+  const int rr = local / B.tiles_x;
+  const int j = B.row0 + rr;
+  const int i0 = (local - rr * B.tiles_x) * 256 + 8 * lane;
+  const int clo = p.region == 1 ? 2 : 0, chi = p.region == 1 ? B.nx - 3 : B.nx - 1;
+  if (j == 0 || j == B.ny - 1) {  // no row on one side: per-cell path for the whole warp
+    for (int q = 0; q < 8; q++) {
+      const int i = i0 + q;
+      if (i >= clo && i <= chi) stb_cell_h<P, EF>(p, B, i, j);
+    }
+    return;
+  }
+  // the pitch is a multiple of 64 words, so every row and octet start is
+  // 16-byte aligned; a lane past the row's pitch loads nothing
+  const bool inrow = i0 < B.pitch;
+  const long long rowc = (long long)j * B.pitch;
+  uint2 fl8 = make_uint2(0x03030303u, 0x03030303u);
+  if (inrow) fl8 = *(const uint2 *)(B.flags + rowc + i0);
+  const bool fast = inrow && ((fl8.x | fl8.y) & 0x17171717u) == 0u && i0 >= clo && i0 + 7 <= chi;
+  const S *Fin = (const S *)B.Fin;
+  // every load before any shuffle consumes one: nine octets and, for the six
+  // directions with a column shift, the word just outside the warp's span
+  uint4 w[9];
+  unsigned int halo[9];
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    const S *rowp = Fin + k * B.plane + (long long)(j - ey(k)) * B.pitch;
+    w[k] = make_uint4(0u, 0u, 0u, 0u);
+    if (inrow) w[k] = ld_oct<EF>(rowp + i0);
+    halo[k] = 0u;
+    if (ex(k) == 1 && lane == 0 && inrow && i0 > 0)
+      halo[k] = (unsigned int)(*(const unsigned short *)(rowp + i0 - 1)) << 16;
+    if (ex(k) == -1 && lane == 31 && i0 + 8 < B.pitch) halo[k] = *(const unsigned short *)(rowp + i0 + 8);
+  }
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    if (ex(k) == 1) {  // cells i0..i0+7 pull from i0-1..i0+6: the high word of the previous pair leads
+      unsigned int pw = __shfl_up_sync(0xffffffffu, w[k].w, 1);
+      if (lane == 0) pw = halo[k];
+      w[k].w = __byte_perm(w[k].z, w[k].w, 0x5432);
+      w[k].z = __byte_perm(w[k].y, w[k].z, 0x5432);
+      w[k].y = __byte_perm(w[k].x, w[k].y, 0x5432);
+      w[k].x = __byte_perm(pw, w[k].x, 0x5432);
+    } else if (ex(k) == -1) {  // pull from i0+1..i0+8: the low word of the next pair trails
+      unsigned int nw = __shfl_down_sync(0xffffffffu, w[k].x, 1);
+      if (lane == 31) nw = halo[k];
+      w[k].x = __byte_perm(w[k].x, w[k].y, 0x5432);
+      w[k].y = __byte_perm(w[k].y, w[k].z, 0x5432);
+      w[k].z = __byte_perm(w[k].z, w[k].w, 0x5432);
+      w[k].w = __byte_perm(w[k].w, nw, 0x5432);
+    }
+  }
+  if (fast) {
+    const float rv = (float)B.rv_tau;
+    const bool wm = p.write_macros != 0;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      float fa[9], fb[9], oa[9], ob[9], ma[3], mb[3];
+#pragma unroll
+      for (int k = 0; k < 9; k++) {
+        const unsigned int v = q == 0 ? w[k].x : q == 1 ? w[k].y : q == 2 ? w[k].z : w[k].w;
+        unpack_h2(v, fa[k], fb[k], (const S *)nullptr);
+      }
+      const int ia = i0 + 2 * q;
+      stb_collide<P>(fa, rv, oa, ma, p.sh, cell_key(B, ia, j));
+      stb_collide<P>(fb, rv, ob, mb, p.sh, cell_key(B, ia + 1, j));
+#pragma unroll
+      for (int k = 0; k < 9; k++) {
+        const unsigned int v = pack_h2(oa[k], ob[k], (const S *)nullptr);
+        if (q == 0) w[k].x = v;
+        else if (q == 1) w[k].y = v;
+        else if (q == 2) w[k].z = v;
+        else w[k].w = v;
+      }
+      if (wm) {
+        const unsigned int fq = (q < 2 ? fl8.x : fl8.y) >> (16 * (q & 1));
+        if (p.macro_all || (fq & 8u)) {
+          st_ef<EF>((float *)B.rho + rowc + ia, ma[0]);
+          st_ef<EF>((float *)B.ux + rowc + ia, ma[1]);
+          st_ef<EF>((float *)B.uy + rowc + ia, ma[2]);
+        }
+        if (p.macro_all || ((fq >> 8) & 8u)) {
+          st_ef<EF>((float *)B.rho + rowc + ia + 1, mb[0]);
+          st_ef<EF>((float *)B.ux + rowc + ia + 1, mb[1]);
+          st_ef<EF>((float *)B.uy + rowc + ia + 1, mb[2]);
+        }
+      }
+    }
+    S *Fout = (S *)B.Fout;
+#pragma unroll
+    for (int k = 0; k < 9; k++) st_oct<EF>(Fout + k * B.plane + rowc + i0, w[k]);
+  } else {
+    for (int q = 0; q < 8; q++) {
+      const int i = i0 + q;
+      if (i < B.nx && i >= clo && i <= chi) stb_cell_h<P, EF>(p, B, i, j);
+    }
+  }
+}
+
+// Octet kernel (16-bit stored forms): 8 warps per CTA, one warp tile of 256
+// cells each (StbBlk::wt0 and tiles_x count 256-cell tiles for it).
+template <int P>
+__global__ void __launch_bounds__(256, 3) k_block_step_o(const __grid_constant__ StbParams p) {
+  pdl_trigger();
+  const long long wt = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (wt >= p.total) return;  // warp-uniform
+  pdl_wait();
+  if constexpr (sizeof(typename Prec<P>::S) == 2) {
+    if (p.evict_first) stb_oct_body<P, true>(p, wt, lane);
+    else stb_oct_body<P, false>(p, wt, lane);
+  }
+}
+
 
 // ----------------------------------------------------------------------------
 // Interface point records: c_c_boundary_transfer, temporal_interpolation,

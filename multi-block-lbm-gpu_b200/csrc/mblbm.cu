@@ -352,6 +352,12 @@ template <int P> struct KStbRI { static void *ptr() { return (void *)k_block_ste
 template <int P> struct KStbP { static void *ptr() { return (void *)k_block_step_p<P, false>; } };
 template <int P> struct KStbPI { static void *ptr() { return (void *)k_block_step_p<P, true>; } };
 template <int P> struct KStbQ { static void *ptr() { return (void *)k_block_step_q<P>; } };
+template <int P> struct KStbO {
+  static void *ptr() {
+    if constexpr (sizeof(typename Prec<P>::S) == 2) return (void *)k_block_step_o<P>;
+    else return nullptr;  // octets exist for the 16-bit stored forms only
+  }
+};
 template <int P> struct KStbX { static void *ptr() { return (void *)k_block_step_x<P>; } };
 template <int P> struct KCcp { static void *ptr() { return (void *)k_cc_pull<P>; } };
 template <int P> struct KFcp { static void *ptr() { return (void *)k_fc_pull<P>; } };
@@ -394,6 +400,7 @@ long long region_cells(int nx, int ny, int region) {
 }
 
 bool stb_uses_quads(const mb_ctx *c, int level, int region);
+int stb_tile(const mb_ctx *c, int level, int region);
 
 // any collision or boundary option on: every block step runs k_block_step_x
 bool options_on(const mb_ctx *c) { return c->opt.coll != MB_COLL_BGK || c->opt.has_force || c->n_alt_walls > 0; }
@@ -401,7 +408,8 @@ bool options_on(const mb_ctx *c) { return c->opt.coll != MB_COLL_BGK || c->opt.h
 // Launch parameters of a block-step node.  total counts cells for the
 // one-cell-per-thread kernel and warp tiles for the quad kernel (quads).
 StbParams make_stb(mb_ctx *c, int a0, int a1, uint64_t parity, int macro_all, int write_macros, int region,
-                   bool quads, int ccpull) {
+                   int tile, int ccpull) {
+  const bool quads = tile > 0;
   StbParams p{};
   p.nblk = a1 - a0;
   p.a0 = a0;
@@ -438,8 +446,10 @@ StbParams make_stb(mb_ctx *c, int a0, int a1, uint64_t parity, int macro_all, in
     s.rv_tau = c->geo.Areas[a].rv_tau;
     s.dt = 1.0 / c->geo.Areas[a].m;
     cell += region_cells(B.nx, B.ny, region);
-    // quad kernel: rows of the region in tiles of 128 cells
-    s.tiles_x = (B.nx + 127) / 128;
+    // quad and octet kernels: rows of the region in warp tiles of 128 (quads)
+    // or 256 (octets) cells
+    const int tw = tile > 0 ? tile : 128;
+    s.tiles_x = (B.nx + tw - 1) / tw;
     s.row0 = region == STB_INTERIOR ? 2 : 0;
     const int nrows = region == STB_INTERIOR ? std::max(0, B.ny - 4) : B.ny;
     s.wt0 = wt;
@@ -470,9 +480,18 @@ StbParams make_stb(mb_ctx *c, int a0, int a1, uint64_t parity, int macro_all, in
 }
 
 // the rim is always stepped one cell per thread
+// octet kernel: variant 6 on a level of a 16-bit stored form (others run 0)
+bool stb_uses_octets(const mb_ctx *c, int level) { return c->stb_variant[level] == 6 && prec_bytes(c->prec) == 2; }
+
 bool stb_uses_quads(const mb_ctx *c, int level, int region) {
-  return region != STB_RIM && c->stb_variant[level] == 1 && c->use_graph != 3 &&
+  return region != STB_RIM && (c->stb_variant[level] == 1 || stb_uses_octets(c, level)) && c->use_graph != 3 &&
          !(c->use_graph == 4 && region != STB_INTERIOR) && !options_on(c);
+}
+
+// warp-tile width of a launch: 128 cells (quads), 256 (octets), 0 (others)
+int stb_tile(const mb_ctx *c, int level, int region) {
+  if (!stb_uses_quads(c, level, region)) return 0;
+  return stb_uses_octets(c, level) ? 256 : 128;
 }
 
 bool background_capped(const mb_ctx *c, bool background) { return background && c->bulk_ctas_per_sm > 0; }
@@ -497,8 +516,8 @@ void stb_launch_shape(const mb_ctx *c, int level, int region, bool background, c
     *grid = dim3((unsigned)std::max<long long>((p.total + 255) / 256, 0));
     return;
   }
-  if (stb_uses_quads(c, level, region)) {  // the quad grid is never capped
-    *func = kfunc<KStbQ>(c->prec);
+  if (stb_uses_quads(c, level, region)) {  // the quad and octet grids are never capped
+    *func = stb_uses_octets(c, level) ? kfunc<KStbO>(c->prec) : kfunc<KStbQ>(c->prec);
     *grid = dim3((unsigned)((p.total + 7) / 8));  // 8 warp tiles per CTA
     return;
   }
@@ -632,8 +651,7 @@ int lower_plan(mb_ctx *c, CompiledPlan &cp) {
     d.kind = n.kind;
     d.deps = n.deps;
     if (n.kind == NK_STB) {
-      const bool quads = stb_uses_quads(c, n.level, n.region);
-      d.stb = make_stb(c, n.a0, n.a1, n.parity, n.macro_all, 1, n.region, quads, n.ccpull);
+      d.stb = make_stb(c, n.a0, n.a1, n.parity, n.macro_all, 1, n.region, stb_tile(c, n.level, n.region), n.ccpull);
       d.stb.tskip = n.tskip;
       d.stb.fcskip = n.fcskip;
       // bulk: interiors of split levels, and whole levels streamed with
@@ -677,7 +695,7 @@ int lower_plan(mb_ctx *c, CompiledPlan &cp) {
       d.args[0] = &d.drag;
     } else if (n.kind == NK_FCP) {
       // the CF_FCSRC cells of the step's blocks and their f_c points
-      d.stb = make_stb(c, n.a0, n.a1, n.parity, n.macro_all, 1, STB_ALL, false, 0);
+      d.stb = make_stb(c, n.a0, n.a1, n.parity, n.macro_all, 1, STB_ALL, 0, 0);
       std::vector<StbFc> fc;
       for (const FcFuse &e : n.fc) {
         if (!(e.bits & (RB_WRITE_F | RB_WRITE_M))) continue;
@@ -729,7 +747,7 @@ int lower_plan(mb_ctx *c, CompiledPlan &cp) {
       d.grid = dim3((unsigned)((cells.size() + 127) / 128));
       d.args[0] = &d.stb;
     } else if (n.kind == NK_CCP) {
-      d.stb = make_stb(c, n.a0, n.a1, n.parity, 0, 1, STB_ALL, false, 0);
+      d.stb = make_stb(c, n.a0, n.a1, n.parity, 0, 1, STB_ALL, 0, 0);
       d.stb.cc_list = c->d_cclist[n.level];
       d.stb.cc_n = (int)c->cc[n.level].links.size();
       d.func = kfunc<KCcp>(c->prec);
@@ -980,8 +998,9 @@ int set_smem_limits(int prec) {
   // memory up to the spread limit (mb_set_bulk_spread)
   {
     void *fns[] = {kfunc<KStb>(prec), kfunc<KStb2>(prec), kfunc<KStbQ>(prec), kfunc<KStbPI>(prec),
-                   kfunc<KStbP>(prec), kfunc<KStbRI>(prec), kfunc<KStbR>(prec)};
-    for (void *f : fns) MB_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, MB_CTA_SMEM_MAX));
+                   kfunc<KStbP>(prec), kfunc<KStbRI>(prec), kfunc<KStbR>(prec), kfunc<KStbO>(prec)};
+    for (void *f : fns)
+      if (f) MB_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, MB_CTA_SMEM_MAX));
   }
   MB_CUDA(cudaFuncSetAttribute(kfunc<KSpl>(prec), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)std::max(spline_smem(prec), (size_t)MB_CTA_SMEM_MAX)));
@@ -1432,18 +1451,18 @@ extern "C" int mb_create(const mb_geometry *geo, int precision, mb_ctx **out) {
   // cell pairs on every level, whose shared addresses and paired accesses
   // cut its issue-bound instruction count (85.4 against 86.7 us with cell
   // ranges on level 0 and one cell per thread elsewhere; level 0 alone 39.7
-  // against 46.0 us); FP32 storage gains from the quads' vector accesses on
-  // level 0 (112 against 117 us with the split level 0)
+  // against 46.0 us); FP32 storage steps level 0 in cell pairs too (104.3
+  // against 109.9 us per step with quads; level 0 alone 52.8 against 61.0 us)
   if (precision == MB_PREC_F16S || precision == MB_PREC_F16C)
     for (int l = 0; l < MB_MAX_LEVEL; l++) c->stb_variant[l] = 4;
-  if (precision == MB_PREC_F32 || precision == MB_PREC_F32U) c->stb_variant[0] = 1;
+  if (precision == MB_PREC_F32 || precision == MB_PREC_F32U) c->stb_variant[0] = 4;
   // measured on config 2 (sweeps of both): the interior CTAs reserve shared
-  // memory they do not use, so an SM holds two of them (FP32 quads, 80 KB)
-  // or three (FP16 pairs, 60 KB) and keeps room for the fine levels' chain,
-  // and the splines ask for 48 / 64 KB: 104.8 against 112.6 us per step in
-  // FP32, 84.4 against 85.5 in FP16 storage
+  // memory they do not use, so an SM holds three of them (cell pairs, 60 KB)
+  // and keeps room for the fine levels' chain, and the splines ask for
+  // 48 / 64 KB: FP32 104.3 against 111.2 us per step without the reserve
+  // and 115.8 with two CTAs per SM; FP16 storage 84.4 against 85.5
   if (precision == MB_PREC_F32 || precision == MB_PREC_F32U) {
-    c->bulk_cta_smem = 80 * 1024;
+    c->bulk_cta_smem = 60 * 1024;
     c->spl_cta_smem = 48 * 1024;
   } else if (precision == MB_PREC_F16S || precision == MB_PREC_F16C) {
     c->bulk_cta_smem = 60 * 1024;
@@ -1862,7 +1881,7 @@ extern "C" int mb_set_stream_cells(mb_ctx *c, long long cells, int bulk) {
 }
 
 extern "C" int mb_set_stb_variant(mb_ctx *c, int level, int variant) {
-  if (!c || level < 0 || level >= c->geo.layout.LEVEL || variant < 0 || variant > 5) return MB_ERR_INVALID;
+  if (!c || level < 0 || level >= c->geo.layout.LEVEL || variant < 0 || variant > 6) return MB_ERR_INVALID;
   cudaDeviceSynchronize();
   c->stb_variant[level] = variant;
   c->plans.clear();
@@ -2736,7 +2755,7 @@ extern "C" int mb_time_block_step(mb_ctx *c, int level, int n, mb_stream stream,
   long long tot = 0;
   for (int a0 = L.ASP[level]; a0 < L.ASP[level + 1]; a0 += STB_MAX_BLOCKS) {
     const int a1 = std::min(L.ASP[level + 1], a0 + STB_MAX_BLOCKS);
-    ps.push_back(make_stb(c, a0, a1, par, 0, 0, STB_ALL, stb_uses_quads(c, level, STB_ALL), 0));
+    ps.push_back(make_stb(c, a0, a1, par, 0, 0, STB_ALL, stb_tile(c, level, STB_ALL), 0));
     for (int a = a0; a < a1; a++) tot += (long long)c->blk[a].nx * c->blk[a].ny;
   }
   void *fn = nullptr;

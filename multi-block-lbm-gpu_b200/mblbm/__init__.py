@@ -524,7 +524,9 @@ class MultiBlockLBM:
         _check(self.lib.mb_set_split_cells(self.h, int(cells)), "mb_set_split_cells")
 
     def set_stb_variant(self, level, variant):
-        """Block-step kernel of a level: 0 one cell per thread, 1 four cells per thread."""
+        """Block-step kernel of a level: 0 one cell per thread, 1 four cells per thread,
+        2 two cells per thread, 3 cell ranges, 4 cell pairs, 5 bulk-copy row staging,
+        6 eight cells per thread (16-bit stored forms; others run 0).  Results are identical."""
         _check(self.lib.mb_set_stb_variant(self.h, int(level), int(variant)), "mb_set_stb_variant")
 
     def set_split_levels(self, level_mask):

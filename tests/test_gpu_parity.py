@@ -286,7 +286,7 @@ def test_interior_rim_split(mb, orc, cuda_device, name):
 
 
 @pytest.mark.parametrize("split", [0, 10**12])
-@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5])
+@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5, 6])
 @pytest.mark.parametrize("prec", ["f32", "f16s", "f64", "f16c"])
 def test_quad_kernel_equals_cell_kernel(mb, cuda_device, prec, variant, split):
     """Every block-step variant gives bitwise the same state, on whole levels
@@ -380,7 +380,7 @@ def test_step_diag_equals_step_by_step(mb, cuda_device, prec, split, graph):
 
 
 @pytest.mark.parametrize("graph", [True, False, "program"])
-@pytest.mark.parametrize("split,variant", [(10**12, 0), (0, 0), (10**12, 4), (0, 4), (0, 3), (0, 5)])
+@pytest.mark.parametrize("split,variant", [(10**12, 0), (0, 0), (10**12, 4), (0, 4), (0, 3), (0, 5), (0, 6)])
 @pytest.mark.parametrize("name,prec", [("n3", "f32"), ("g49", "f64"), ("g25", "f16s"), ("n3", "f16c")])
 def test_fused_copies_bitwise(mb, cuda_device, name, prec, split, variant, graph):
     """Same-level copies done inside the block step (mb_set_fusion bit 0),
@@ -473,7 +473,7 @@ def test_stochastic_rounding_variants_bitwise(mb, orc, cuda_device, split, prec)
     g = mb.geo_init(*make_ref.case("n3")[:2])
     steps = 60
     sims = []
-    for variant, graph in ((0, True), (1, True), (3, True), (5, False), (2, "program")):
+    for variant, graph in ((0, True), (1, True), (3, True), (5, False), (2, "program"), (6, True), (6, False)):
         s = mb.MultiBlockLBM(g, prec, graph=graph, rounding="stochastic")
         for lvl in range(g.layout.LEVEL):
             s.set_stb_variant(lvl, variant)
@@ -513,7 +513,7 @@ def test_stochastic_rounding_variants_bitwise(mb, orc, cuda_device, split, prec)
     ("n3", "f32", 0, None, True), ("n3", "f32", 1, 0, True), ("n3", "f16s", 4, None, True),
     ("n3", "f16c", 3, 0, False), ("n3", "f64", 0, None, True), ("g49", "f32", 5, 0, True),
     ("c1", "f32", 0, None, True), ("g25", "f16s", 4, 0, False), ("n3", "f32u", 0, None, True),
-    ("n3", "f32u", 2, None, True)])
+    ("n3", "f32u", 2, None, True), ("n3", "f16s", 6, None, True), ("g25", "f16c", 6, 0, False)])
 def test_fc_fusion_bitwise(mb, cuda_device, name, prec, variant, split, graph):
     """f_c points done inside the fine level's last block step (mb_set_fusion
     bit 3) give bitwise the state, drag and L2 series of the record launches,
