@@ -600,6 +600,9 @@ def main():
                          "graph (untimed, then timed; an ncu capture of that kernel takes -k regex:k_block_step "
                          "-s 3 with N >= 2); prints its roofline")
     ap.add_argument("--level", type=int, default=0, help="level of --roofline-only")
+    ap.add_argument("--no-in-step", action="store_true",
+                    help="leave out the CUPTI record of the level-0 interior inside the step (after the timed "
+                         "region; for runs under ncu, which holds CUPTI itself)")
     ap.add_argument("--variant", type=int, default=None, help="block-step variant of every level (mb_set_stb_variant)")
     ap.add_argument("--workload", default="cylinder3",
                     choices=["cylinder3", "batch256", "timetocd", "warmstart", "forces", "tgv"],
@@ -690,7 +693,7 @@ def main():
     # ---- dominant kernel alone: level-0 block step, CUDA events on its stream
     kms, kbytes, kcells = sim.time_block_step(0, 50, stream)
     # ---- the same kernel inside the step: CUPTI kernel records of one plan
-    in_step = level0_in_step(sim, stream)
+    in_step = None if args.no_in_step else level0_in_step(sim, stream)
     # ---- end to end through the C ABI with host buffers ----------------------
     import numpy as np
 
