@@ -173,6 +173,32 @@ def level0_in_step(sim, stream):
     return name, float(sum(d) / len(d)), float(BYTES_PER_UPDATE[sim.precision]) * cells
 
 
+def step_timeline(sim, stream, n=48):
+    """CUPTI kernel records (torch.profiler) of an n-step call after 30 warm-up
+    steps: every launch of the two coarse steps that start at the 21st
+    level-0 interior launch, as (start us from that launch, duration us,
+    kernel), and the period and duration of the interior launches around it."""
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+
+    sim.evolution(30, stream)
+    sim.prepare(n)
+    torch.cuda.synchronize()
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        sim.evolution(n, stream)
+        torch.cuda.synchronize()
+    ev = sorted((e.time_range.start, e.time_range.end, e.name.split("(")[0].replace("void mblbm::dev::", ""))
+                for e in prof.events() if e.device_type == torch.autograd.DeviceType.CUDA)
+    ints = [e for e in ev if ("block_step_p<" in e[2] and ", true>" in e[2]) or "block_step_q<" in e[2]
+            or ("block_step_r<" in e[2] and ", true>" in e[2]) or "block_step_tb<" in e[2] or "block_step_o<" in e[2]]
+    if len(ints) < 24:
+        return None
+    t0, t1 = ints[20][0], ints[22][0]
+    return {"launches": [(round(a - t0, 1), round(b - a, 1), nm) for a, b, nm in ev if t0 - 5 <= a < t1 + 5],
+            "interior_period_us": [round(ints[i + 1][0] - ints[i][0], 1) for i in range(18, 23)],
+            "interior_us": [round(e[1] - e[0], 1) for e in ints[18:23]]}
+
+
 def run_reference(args):
     """The reference's own CUDA build (oracle/_ref/ref_c2) on WORKLOAD.  Loads
     nothing of this repository's library: the update count comes from the
@@ -383,13 +409,13 @@ def run_warmstart(args):
     chunk = 50
     cold, tc = sg.drag_series(eval_ids, args.eval_per_d, "f32", chunk)
     t2 = time.perf_counter()
-    warm, tw = sg.drag_series(eval_ids, args.eval_per_d, args.warm_precision, chunk, net=net)
+    warm, tw = sg.drag_series(eval_ids, args.eval_per_d, args.warm_precision, chunk, net=net, kick=args.kick)
     t_warm_total = time.perf_counter() - t2
     res = []
     for i in eval_ids:
         sc, prm, key, lc = cold[i]
         sw, lw = warm[i][0], warm[i][3]
-        win = 10 if prm["Re"] < 47 else max(10, int(np.ceil(150 * prm["D"] / chunk)))
+        win = 10 if prm["Re"] < sg.RE_SHEDDING else max(10, int(np.ceil(150 * prm["D"] / chunk)))
         kern = np.ones(win) / win
         rc, rw = np.convolve(sc, kern, "valid"), np.convolve(sw, kern, "valid")
         ref = rc[-1]
@@ -398,7 +424,7 @@ def run_warmstart(args):
         # shedding cases: the Strouhal number of the second half of the run
         # (lift sampled every `chunk` steps) must also agree within 1 %
         st_c = st_w = None
-        if prm["Re"] >= 47:
+        if prm["Re"] >= sg.RE_SHEDDING:
             half = len(lc) // 2
             st_c = mblbm.strouhal(lc, prm["D"], 0.04 * chunk, skip=half)
             st_w = mblbm.strouhal(lw, prm["D"], 0.04 * chunk, skip=half)
@@ -412,16 +438,19 @@ def run_warmstart(args):
                     "ms_cold": steps_c * tc[key], "ms_warm": steps_w * tw[key] if ok else steps_c * tc[key]})
     acc = [r for r in res if r["accepted"]]
     ratio = sum(r["ms_warm"] for r in res) / sum(r["ms_cold"] for r in res)
-    steady = [r for r in res if r["Re"] < 47]
+    steady = [r for r in res if r["Re"] < sg.RE_SHEDDING]
+    shedding = [r for r in res if r["Re"] >= sg.RE_SHEDDING]
     line = {"metric": "time to Cd within 0.5% (warm start vs plain FP32 cold start)", "unit": "ratio",
             "higher_is_better": False, "value": round(ratio, 4), "n_gpus": 1, "data": "synthetic",
             "dtype": f"bf16 surrogate, {args.warm_precision} warm / f32 cold solver",
             "config": {"workload": "held-out cases of the batched distribution (mblbm.batch_case ids 100000+)",
                        "train_cases": len(ids), "snap_steps_per_D": args.snap_per_d, "epochs": args.epochs,
-                       "eval_cases": len(res), "eval_steps_per_D": args.eval_per_d, "cd_sample_every": chunk},
+                       "eval_cases": len(res), "eval_steps_per_D": args.eval_per_d, "cd_sample_every": chunk,
+                       "kick": args.kick},
             "accepted": len(acc),
             "steady_cases": len(steady),
             "steady_ratio": round(sum(r["ms_warm"] for r in steady) / max(1e-9, sum(r["ms_cold"] for r in steady)), 4),
+            "shedding_ratio": round(sum(r["ms_warm"] for r in shedding) / max(1e-9, sum(r["ms_cold"] for r in shedding)), 4),
             "median_cold_steps": float(np.median([r["cold_steps"] for r in res])),
             "median_warm_steps_accepted": float(np.median([r["warm_steps"] for r in acc])) if acc else None,
             "loss_first_last": [round(hist[0], 5), round(hist[-1], 5)], "train_s": round(t_train, 1),
@@ -600,6 +629,8 @@ def main():
                          "graph (untimed, then timed; an ncu capture of that kernel takes -k regex:k_block_step "
                          "-s 3 with N >= 2); prints its roofline")
     ap.add_argument("--level", type=int, default=0, help="level of --roofline-only")
+    ap.add_argument("--timeline", action="store_true",
+                    help="print the CUPTI kernel records of two coarse steps (step_timeline) and exit")
     ap.add_argument("--no-in-step", action="store_true",
                     help="leave out the CUPTI record of the level-0 interior inside the step (after the timed "
                          "region; for runs under ncu, which holds CUPTI itself)")
@@ -617,6 +648,9 @@ def main():
     ap.add_argument("--eval-per-d", type=float, default=900.0, help="coarse steps per unit D of a warm-start evaluation run")
     ap.add_argument("--warm-precision", default="f16s", choices=["f16s", "f16c", "f32"], help="solver storage of warm starts")
     ap.add_argument("--epochs", type=int, default=40, help="training epochs of --workload warmstart")
+    ap.add_argument("--kick", type=float, default=0.0,
+                    help="--workload warmstart: transverse velocity kick (x U0) behind the obstacle in the warm "
+                         "starts of shedding cases (surrogate.warm_start)")
     ap.add_argument("--save", default=None, metavar="DIR", help="--workload forces: write Cd and Cl per step to DIR")
     ap.add_argument("--spinup", type=int, default=0,
                     help="--workload forces: FP64 coarse steps from rest before every precision continues from "
@@ -662,6 +696,9 @@ def main():
         for lvl in range(geo.layout.LEVEL):
             sim.set_stb_variant(lvl, args.variant)
     sim.init(stream)
+    if args.timeline:
+        print(json.dumps({"precision": args.precision, "timeline": step_timeline(sim, stream)}))
+        return 0
     if args.roofline_only:
         kms, kbytes, kcells = sim.time_block_step(args.level, args.roofline_only, stream)
         peak, src = peaks()

@@ -95,11 +95,21 @@ def case_targets(sim, geo, h=H, w=W):
     return t.astype(np.float32)
 
 
-def warm_start(sim, geo, pred, stream=None):
+# Reynolds number above which the wake of the workload's obstacles sheds
+RE_SHEDDING = 47.0
+
+
+def warm_start(sim, geo, pred, stream=None, kick=0.0):
     """Initialise every block of sim from a prediction (h, w, 3): f = feq +
     (1 - 1/tau) f_neq with f_neq_k = -3 w_k rho tau (e_k e_k - I/3) : grad u
     (Chapman-Enskog, lattice units of the block's level), obstacle cells at
-    rest; then ring slots and u_prev follow the new fields."""
+    rest; then ring slots and u_prev follow the new fields.
+
+    kick > 0 (shedding cases, Re >= RE_SHEDDING, only): the surrogate
+    predicts the mean wake, which is symmetric, and shedding would have to
+    grow out of round-off again; a transverse velocity kick * U0 in a
+    Gaussian of radius R centred 3R behind the obstacle breaks the symmetry
+    so the wake starts shedding at once."""
     c = geo.config
     U0 = c.U0[0]
     h, w = pred.shape[:2]
@@ -107,6 +117,10 @@ def warm_start(sim, geo, pred, stream=None):
     v = pred[..., 1].astype(np.float64) * U0
     rho = 1.0 + pred[..., 2].astype(np.float64) / 100.0
     gx, gy = (c.LX - 1.0) / (w - 1), (c.LY - 1.0) / (h - 1)
+    if kick > 0.0 and c.Re >= RE_SHEDDING:
+        yy, xx = np.meshgrid(np.arange(h) * gy, np.arange(w) * gx, indexing="ij")
+        r2 = ((xx - (c.CX + 3.0 * c.R)) ** 2 + (yy - c.CY) ** 2) / float(c.R) ** 2
+        v = v + kick * U0 * np.exp(-r2)
     dudy, dudx = np.gradient(u, gy, gx)
     dvdy, dvdx = np.gradient(v, gy, gx)
     L = geo.layout
@@ -176,11 +190,12 @@ def generate(case_ids, steps_per_d, precision="f32", h=H, w=W, stream=None, d_ra
     return np.stack(xs), np.stack(ts), np.stack(ms), ids
 
 
-def drag_series(case_ids, steps_per_d, precision, chunk=50, net=None, d_range=(10.0, 40.0), stream=None):
+def drag_series(case_ids, steps_per_d, precision, chunk=50, net=None, d_range=(10.0, 40.0), stream=None, kick=0.0):
     """Cd and Cl every `chunk` coarse steps of each case, cold-started (net
-    None) or warm-started from the surrogate, batched by level count and D
-    bin.  Returns {id: (cd series, params, batch key, cl series)} and the
-    device time per coarse step of each batch {(levels, steps): ms}."""
+    None) or warm-started from the surrogate (with warm_start's kick for
+    shedding cases), batched by level count and D bin.  Returns {id: (cd
+    series, params, batch key, cl series)} and the device time per coarse
+    step of each batch {(levels, steps): ms}."""
     import torch
 
     out, times = {}, {}
@@ -195,7 +210,7 @@ def drag_series(case_ids, steps_per_d, precision, chunk=50, net=None, d_range=(1
             xin = torch.from_numpy(np.stack([case_inputs(g, net.H, net.W)[0] for _, g, _ in items])).cuda()
             pred = predict(net, xin).cpu().numpy()
             for (i, g, _), s, p in zip(items, sims, pred):
-                warm_start(s, g, p, stream)
+                warm_start(s, g, p, stream, kick=kick)
         b = Batch(sims)
         b.prepare(chunk)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
