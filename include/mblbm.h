@@ -516,13 +516,20 @@ int mb_batch_set_interface_shape(mb_batch *batch, int rec_points, int spline_seg
  * of k CTAs per SM, each CTA taking an equal share of the tiles, in order.
  * Results are identical. */
 int mb_batch_set_schedule(mb_batch *batch, int stb_ctas_per_sm);
-/* Autotuner: times the block-step schedules (0, 2, 4, 8 CTAs per SM), then
- * with the fastest the interface shapes (points per record CTA, spline
- * segments per CTA), each over `steps` coarse steps, and keeps the fastest;
- * reports the choice and its time per coarse step (any pointer may be NULL).
- * The timing steps advance the cases. */
+/* Block-step kernel of the batch: 0 one cell per thread (default), 1 cell
+ * pairs (a thread steps cells i, i+1 of a row, the single-case variant 4),
+ * tiles of 256 pairs under the same schedule; nodes where a case's launch
+ * does not fit the pair form (block rims, 32-bit offsets exceeded) keep one
+ * cell per thread.  Results are identical. */
+int mb_batch_set_kernel(mb_batch *batch, int kernel);
+/* Autotuner: times the block-step kernels and schedules (one cell per
+ * thread at 0, 2, 4, 8 CTAs per SM; cell pairs at 0, 2, 4), then with the
+ * fastest the interface shapes (points per record CTA, spline segments per
+ * CTA), each over `steps` coarse steps, and keeps the fastest; reports the
+ * choice and its time per coarse step (any pointer may be NULL).  The timing
+ * steps advance the cases. */
 int mb_batch_autotune(mb_batch *batch, int steps, mb_stream stream, int *rec_points, int *spline_segments,
-                      int *stb_ctas_per_sm, double *ms_per_step);
+                      int *stb_ctas_per_sm, double *ms_per_step, int *stb_kernel);
 
 /* ---- learned warm start (no reference counterpart) ----------------------- */
 /* A 4-level convolutional U-Net (3x3 convolutions with ReLU, 32, 64, 128,

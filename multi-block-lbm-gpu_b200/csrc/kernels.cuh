@@ -1102,11 +1102,9 @@ __device__ __forceinline__ void stb_pair(const StbParams &p, const StbBlk &B, in
   if (two) stb_cell_slow<P, EF>(p, B, i + 1, j);
 }
 
+// CTA `cta` of a cell-pair launch: 256 consecutive pairs of one block's region.
 template <int P, bool INTERIOR>
-__global__ void __launch_bounds__(256, P == MB_PREC_F64 ? 2 : 5) k_block_step_p(const __grid_constant__ StbParams p) {
-  pdl_trigger();
-  pdl_wait();
-  const int cta = blockIdx.x;
+__device__ __forceinline__ void stb_pair_cta(const StbParams &p, int cta) {
   int t = 0;
 #pragma unroll 1
   while (t + 1 < p.nblk && cta >= p.b[t + 1].pcta0) t++;
@@ -1122,6 +1120,13 @@ __global__ void __launch_bounds__(256, P == MB_PREC_F64 ? 2 : 5) k_block_step_p(
   const bool two = 2 * q + 1 < B.rw;
   if (p.evict_first) stb_pair<P, true, INTERIOR>(p, B, i, j, two);
   else stb_pair<P, false, INTERIOR>(p, B, i, j, two);
+}
+
+template <int P, bool INTERIOR>
+__global__ void __launch_bounds__(256, P == MB_PREC_F64 ? 2 : 5) k_block_step_p(const __grid_constant__ StbParams p) {
+  pdl_trigger();
+  pdl_wait();
+  stb_pair_cta<P, INTERIOR>(p, blockIdx.x);
 }
 
 // ----------------------------------------------------------------------------
@@ -2014,6 +2019,48 @@ __global__ void __launch_bounds__(256, P == MB_PREC_F64 ? 4 : 8) kb_block_step_p
     }
     const long long g = (long long)(t - __ldg(a.cta0 + lo)) * 256 + threadIdx.x;
     if (g < p.total) stb_at<P>(p, g);
+  }
+}
+
+// Cell-pair form of kb_block_step: one CTA per CTA of the cell-pair kernel
+// (256 pairs of one block's region), cases in order.
+template <int P>
+__global__ void __launch_bounds__(256, P == MB_PREC_F64 ? 2 : 5) kb_block_step_pt(const __grid_constant__ BatchArgs a) {
+  __shared__ __align__(16) unsigned char sp[(sizeof(StbParams) + 15) / 16 * 16];
+  const int c = batch_case(a, sp, (int)sizeof(sp));
+  const StbParams &p = *(const StbParams *)sp;
+  const int cta = (int)blockIdx.x - __ldg(a.cta0 + c);
+  if (cta < p.pctas) stb_pair_cta<P, false>(p, cta);
+}
+
+// Cell-pair form of kb_block_step_ps: the tiles are the cell-pair kernel's
+// CTAs (256 pairs of one block's region, cta0 holding each case's first),
+// split evenly over a persistent grid.  Whole levels and interiors only (the
+// pair code also serves an interior region).
+template <int P>
+__global__ void __launch_bounds__(256, P == MB_PREC_F64 ? 2 : 5) kb_block_step_pp(const __grid_constant__ BatchArgs a) {
+  __shared__ __align__(16) unsigned char sp[(sizeof(StbParams) + 15) / 16 * 16];
+  const StbParams &p = *(const StbParams *)sp;
+  const long long T = __ldg(a.cta0 + a.ncases), G = gridDim.x;
+  const int t0 = (int)(T * blockIdx.x / G), t1 = (int)(T * (blockIdx.x + 1) / G);
+  int lo = 0, hi = a.ncases - 1;  // case of the first tile
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(a.cta0 + mid) <= t0) lo = mid; else hi = mid - 1;
+  }
+  int cur = -1;
+#pragma unroll 1
+  for (int t = t0; t < t1; t++) {
+    while (lo + 1 < a.ncases && __ldg(a.cta0 + lo + 1) <= t) lo++;
+    if (lo != cur) {
+      __syncthreads();  // every thread is done with the previous case's parameters
+      const int4 *src = (const int4 *)(a.params + (size_t)lo * a.pstride);
+      for (int q = threadIdx.x; q < (int)sizeof(sp) / 16; q += blockDim.x) ((int4 *)sp)[q] = __ldg(src + q);
+      __syncthreads();
+      cur = lo;
+    }
+    const int cta = t - __ldg(a.cta0 + lo);
+    if (cta < p.pctas) stb_pair_cta<P, false>(p, cta);
   }
 }
 

@@ -377,6 +377,8 @@ template <int P> struct KL2 { static void *ptr() { return (void *)k_error_l2<P>;
 template <int P> struct KPrg { static void *ptr() { return (void *)k_program<P, false>; } };
 template <int P> struct KBStb { static void *ptr() { return (void *)kb_block_step<P>; } };
 template <int P> struct KBStbPs { static void *ptr() { return (void *)kb_block_step_ps<P>; } };
+template <int P> struct KBStbPp { static void *ptr() { return (void *)kb_block_step_pp<P>; } };
+template <int P> struct KBStbPt { static void *ptr() { return (void *)kb_block_step_pt<P>; } };
 template <int P> struct KBRec { static void *ptr() { return (void *)kb_records<P>; } };
 template <int P> struct KBSpl { static void *ptr() { return (void *)kb_spline<P>; } };
 template <int P> struct KPrgT { static void *ptr() { return (void *)k_program<P, true>; } };
@@ -2843,6 +2845,11 @@ struct mb_batch {
   // k > 0 a persistent grid of k CTAs per SM over equal shares of the
   // tiles (kb_block_step_ps)
   int stb_ctas_per_sm = 0;
+  // block-step kernel: 0 one cell per thread, 1 cell pairs (one CTA per
+  // pair-kernel CTA, kb_block_step_pt, or with a schedule k > 0 a persistent
+  // grid over them, kb_block_step_pp) on the nodes where every case's launch
+  // fits the pair form
+  int stb_kernel = 0;
   int num_sms = 148;
   long long steps_done = 0;  // coarse steps of mb_batch_step calls (the autotuner's included)
 };
@@ -2890,9 +2897,15 @@ int batch_plan(mb_batch *b, int n, bool fin, BatchPlan **out) {
     void *func;
     unsigned block = n0.block.x;
     size_t smem = 0;
+    // cell pairs on this node: every case's launch covers a whole level or an
+    // interior with 32-bit offsets
+    bool pairs = n0.kind == NK_STB && b->stb_kernel == 1;
+    for (int c = 0; c < nc && pairs; c++)
+      pairs = parts[c]->dn[q].stb.region != STB_RIM && rows_fit(b->cases[c], parts[c]->dn[q].stb);
     if (n0.kind == NK_STB) {
       psz = sizeof(StbParams);
-      func = b->stb_ctas_per_sm > 0 ? kfunc<KBStbPs>(b->prec) : kfunc<KBStb>(b->prec);
+      if (pairs) func = b->stb_ctas_per_sm > 0 ? kfunc<KBStbPp>(b->prec) : kfunc<KBStbPt>(b->prec);
+      else func = b->stb_ctas_per_sm > 0 ? kfunc<KBStbPs>(b->prec) : kfunc<KBStb>(b->prec);
       block = 256;
     } else if (n0.kind == NK_REC) {
       psz = sizeof(RecOpsParams);
@@ -2912,7 +2925,8 @@ int batch_plan(mb_batch *b, int n, bool fin, BatchPlan **out) {
                                                                                       : (const void *)&dn.spl;
       std::memcpy(host.data() + stride * c, src, psz);
       cta0[c] = (int)ctas;
-      if (n0.kind == NK_STB) ctas += (dn.stb.total + 255) / 256;
+      if (pairs) ctas += dn.stb.pctas;
+      else if (n0.kind == NK_STB) ctas += (dn.stb.total + 255) / 256;
       else ctas += dn.grid.x;
       if (ctas >= (1LL << 31)) return MB_ERR_UNSUPPORTED;
     }
@@ -3114,6 +3128,14 @@ extern "C" int mb_batch_set_schedule(mb_batch *b, int stb_ctas_per_sm) {
   return MB_OK;
 }
 
+extern "C" int mb_batch_set_kernel(mb_batch *b, int kernel) {
+  if (!b || kernel < 0 || kernel > 1) return MB_ERR_INVALID;
+  cudaDeviceSynchronize();
+  b->plans.clear();
+  b->stb_kernel = kernel;
+  return MB_OK;
+}
+
 namespace {
 // Mean device time of one coarse step of the batch with its current shapes:
 // one untimed chunk (period + 1 steps) builds the graphs, then `steps` timed
@@ -3132,29 +3154,34 @@ int batch_time(mb_batch *b, int steps, cudaStream_t s, cudaEvent_t e0, cudaEvent
 }
 }  // namespace
 
-// Coordinate search: first the block-step schedule (one CTA per tile, or a
-// persistent grid of 2, 4 or 8 CTAs per SM over equal shares of the tiles)
-// with the default interface shape, then, with the best schedule, the
-// interface shapes (points per record CTA, spline segments per CTA).  Each
-// candidate is timed over `steps` coarse steps after one untimed chunk that
-// builds its graphs; the fastest is kept.  The timing steps advance the cases.
+// Coordinate search: first the block-step kernel and schedule (one cell per
+// thread, and cell pairs, each with one CTA per tile or a persistent grid of
+// 2, 4 (or 8, one cell per thread) CTAs per SM over equal shares of the
+// tiles) with the default interface shape, then, with the best of
+// those, the interface shapes (points per record CTA, spline segments per
+// CTA).  Each candidate is timed over `steps` coarse steps after one untimed
+// chunk that builds its graphs; the fastest is kept.  The timing steps
+// advance the cases.
 extern "C" int mb_batch_autotune(mb_batch *b, int steps, mb_stream stream, int *rec_points, int *spline_segments,
-                                 int *stb_ctas_per_sm, double *ms_per_step) {
+                                 int *stb_ctas_per_sm, double *ms_per_step, int *stb_kernel) {
   if (!b || steps < 1) return MB_ERR_INVALID;
   cudaStream_t s = (cudaStream_t)stream;
-  static const int sched[] = {0, 2, 4, 8};
+  static const int sched[][2] = {{0, 0}, {0, 2}, {0, 4}, {0, 8}, {1, 0}, {1, 2}, {1, 4}};  // (kernel, CTAs per SM)
   static const int cand[][2] = {{64, 1}, {32, 2}, {64, 2}, {64, 4}};
   cudaEvent_t e0, e1;
   MB_CUDA(cudaEventCreate(&e0));
   MB_CUDA(cudaEventCreate(&e1));
   double best = 1e30, ms = 0;
-  int bk = 0, br = 32, bs = 1, err = MB_OK;
+  int bk = 0, bkern = 0, br = 32, bs = 1, err = MB_OK;
   if ((err = mb_batch_set_interface_shape(b, 32, 1))) return err;
-  for (int k : sched) {
-    if (b->prec == MB_PREC_F64 && k > 4) continue;
-    if ((err = mb_batch_set_schedule(b, k)) || (err = batch_time(b, steps, s, e0, e1, &ms))) break;
-    if (ms < best) { best = ms; bk = k; }
+  for (const auto &ks : sched) {
+    if (b->prec == MB_PREC_F64 && ks[1] > 4) continue;
+    if ((err = mb_batch_set_kernel(b, ks[0])) || (err = mb_batch_set_schedule(b, ks[1])) ||
+        (err = batch_time(b, steps, s, e0, e1, &ms)))
+      break;
+    if (ms < best) { best = ms; bkern = ks[0]; bk = ks[1]; }
   }
+  if (!err) err = mb_batch_set_kernel(b, bkern);
   if (!err) err = mb_batch_set_schedule(b, bk);
   for (int q = 0; q < 4 && !err; q++) {
     if ((err = mb_batch_set_interface_shape(b, cand[q][0], cand[q][1])) || (err = batch_time(b, steps, s, e0, e1, &ms)))
@@ -3168,6 +3195,7 @@ extern "C" int mb_batch_autotune(mb_batch *b, int steps, mb_stream stream, int *
   if (rec_points) *rec_points = br;
   if (spline_segments) *spline_segments = bs;
   if (stb_ctas_per_sm) *stb_ctas_per_sm = bk;
+  if (stb_kernel) *stb_kernel = bkern;
   if (ms_per_step) *ms_per_step = best;
   return MB_OK;
 }

@@ -176,8 +176,9 @@ SIGNATURES = {
     "mb_unet_train_step": ([_vp, _vp, _vp, _vp, C.c_int, C.c_float, C.c_int, C.POINTER(C.c_float), _vp], C.c_int),
     "mb_batch_stats": ([_vp, _pll, _pll, _pll], C.c_int),
     "mb_batch_set_interface_shape": ([_vp, C.c_int, C.c_int], C.c_int),
-    "mb_batch_autotune": ([_vp, C.c_int, _vp, _pi, _pi, _pi, _pd], C.c_int),
+    "mb_batch_autotune": ([_vp, C.c_int, _vp, _pi, _pi, _pi, _pd, _pi], C.c_int),
     "mb_batch_set_schedule": ([_vp, C.c_int], C.c_int),
+    "mb_batch_set_kernel": ([_vp, C.c_int], C.c_int),
     "mb_set_program_trace": ([_vp, C.c_longlong], C.c_int),
     "mb_program_trace": ([_vp, _vp, C.c_longlong, C.POINTER(C.c_longlong)], C.c_int),
     "mb_program_selftest": ([_vp, C.c_int, _vp], C.c_int),
@@ -839,13 +840,17 @@ class Batch:
         grid of k CTAs per SM over equal shares of the tiles."""
         _check(self.lib.mb_batch_set_schedule(self.h, int(stb_ctas_per_sm)), "mb_batch_set_schedule")
 
+    def set_kernel(self, kernel):
+        """Block-step kernel: 0 one cell per thread, 1 cell pairs on a persistent grid."""
+        _check(self.lib.mb_batch_set_kernel(self.h, int(kernel)), "mb_batch_set_kernel")
+
     def autotune(self, steps=12, stream=None):
-        """Times the block-step schedules, then the interface shapes; keeps the fastest."""
-        r, sg, k, ms = C.c_int(), C.c_int(), C.c_int(), C.c_double()
+        """Times the block-step kernels and schedules, then the interface shapes; keeps the fastest."""
+        r, sg, k, ms, kern = C.c_int(), C.c_int(), C.c_int(), C.c_double(), C.c_int()
         _check(self.lib.mb_batch_autotune(self.h, int(steps), _stream_ptr(stream), C.byref(r), C.byref(sg), C.byref(k),
-                                          C.byref(ms)), "mb_batch_autotune")
+                                          C.byref(ms), C.byref(kern)), "mb_batch_autotune")
         return {"rec_points": r.value, "spline_segments": sg.value, "stb_ctas_per_sm": k.value,
-                "ms_per_step": ms.value}
+                "stb_kernel": kern.value, "ms_per_step": ms.value}
 
 
 # ---------------------------------------------------------------------------

@@ -47,10 +47,11 @@ def test_batch_autotune_keeps_results(mb, cuda_device):
     batch = mb.Batch(sims)
     choice = batch.autotune(steps=3)
     assert choice["rec_points"] in (32, 64) and 1 <= choice["spline_segments"] <= 4 and choice["ms_per_step"] > 0
-    assert choice["stb_ctas_per_sm"] in (0, 2, 4, 8)
+    assert choice["stb_ctas_per_sm"] in (0, 2, 4, 8) and choice["stb_kernel"] in (0, 1)
     batch.evolution(5)
-    # 4 schedules + 4 interface shapes, each (one untimed chunk of period + 1 = 7 steps, then 3 timed), then 5 more
-    steps_done = 8 * (7 + 3) + 5
+    # 7 kernel/schedule pairs + 4 interface shapes, each (one untimed chunk of
+    # period + 1 = 7 steps, then 3 timed), then 5 more
+    steps_done = 11 * (7 + 3) + 5
     for g, a, s in zip(geos, alone, sims):
         a.evolution(steps_done)
         assert_same(g, s, a)
@@ -69,13 +70,17 @@ def test_batch_rejects_diverged_state(mb, cuda_device):
     batch.close()
 
 
-@pytest.mark.parametrize("sched", [1, 2, 4, 8])
-@pytest.mark.parametrize("prec", ["f32", "f64"])
-def test_batch_persistent_schedule_bitwise(mb, cuda_device, prec, sched):
+@pytest.mark.parametrize("kernel", [0, 1])
+@pytest.mark.parametrize("sched", [0, 1, 2, 4, 8])
+@pytest.mark.parametrize("prec", ["f32", "f64", "f16s"])
+def test_batch_persistent_schedule_bitwise(mb, cuda_device, prec, sched, kernel):
     """The persistent block-step schedule (k CTAs per SM over equal shares of
-    the 256-cell tiles of all cases) gives the state of one CTA per tile."""
+    the 256-cell tiles of all cases), and the cell-pair kernel on such a grid,
+    give the state of one CTA per tile of one cell per thread."""
     if prec == "f64" and sched > 4:
         pytest.skip("FP64 block steps run at most 4 CTAs per SM")
+    if kernel == 0 and sched == 0:
+        pytest.skip("the reference schedule itself")
     geos = cases(mb, range(6), 3, d_range=(10.0, 30.0))
     a = [mb.MultiBlockLBM(g, prec) for g in geos]
     b = [mb.MultiBlockLBM(g, prec) for g in geos]
@@ -83,6 +88,7 @@ def test_batch_persistent_schedule_bitwise(mb, cuda_device, prec, sched):
         s.init()
     ba, bb = mb.Batch(a), mb.Batch(b)
     bb.set_schedule(sched)
+    bb.set_kernel(kernel)
     ba.evolution(9)
     bb.evolution(9)
     for g, x, y in zip(geos, a, b):
