@@ -115,5 +115,9 @@ def test_tcgen05_convolutions_match_mma_sync(mb, cuda_device):
         a, b = g1[off:off + n], g0[off:off + n]
         errs.append(float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)))
         off += n + cout
-    print("tcgen05 vs mma.sync weight-gradient differences", errs)
-    assert max(errs) < 5e-2, errs
+    print("tcgen05 vs mma.sync weight-gradient differences", errs,
+          "forward", float(np.linalg.norm(o1 - o0) / np.linalg.norm(o0)))
+    # both paths accumulate in FP32 and round to BF16 at the same points: the
+    # gradients agree to FP32 summation order (measured 1.4e-7), where a wrong
+    # index or layout in either would give errors of order one
+    assert max(errs) < 1e-4, errs
