@@ -336,7 +336,7 @@ int mb_set_stb_variant(mb_ctx *ctx, int level, int variant);
  * 256 threads per SM (0 = uncapped), leaving CTA slots on every SM for the
  * fine-level kernels that run beside them. */
 int mb_set_bulk_occupancy(mb_ctx *ctx, int ctas_per_sm);
-/* Kernel fusions of the plan (bit mask; default 1).  Bit 0: the same-level
+/* Kernel fusions of the plan (bit mask; default 5: bits 0 and 2).  Bit 0: the same-level
  * copies (c_c_boundary_transfer, multi/FH/assit_multi.h:2-46) of a level run
  * inside its block-step launch: each target cell computes its source's new
  * values itself.  Bit 1: the spline of a coarse-fine line
@@ -350,10 +350,11 @@ int mb_set_bulk_occupancy(mb_ctx *ctx, int ctas_per_sm);
  * buffer the level's next block step reads, and the level's block step in
  * between leaves those edge cells alone; the spline then runs beside that
  * block step.  Bit 2 takes the lines it applies to before bit 1.  On the
- * 3-level cylinder bit 2 measured the same step time as without it (the
- * spline's longer tail takes what the dropped launch saved), so it is off by
- * default.  Bit 3: the f_c points (f_c_boundary_transfer,
- * multi/FH/assit_multi.h:273-314) whose fine cell the fine level's last
+ * 3-level cylinder bit 2 takes 2 of 20 launches per coarse step off the
+ * fine levels' chain and the step 1 % shorter (103.1 against 104.3 us in
+ * FP32, 93.3 against 93.8 in FP16 storage), so it is on by default.  Batches
+ * and the persistent executor leave it out.  Bit 3: the f_c points
+ * (f_c_boundary_transfer, multi/FH/assit_multi.h:273-314) whose fine cell the fine level's last
  * substep has just updated run in a small launch beside that block step,
  * which updates those fine cells itself (the step leaves them alone), when
  * no operation in between touches their cells: the coarse level's next

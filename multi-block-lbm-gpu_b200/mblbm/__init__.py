@@ -578,8 +578,8 @@ class MultiBlockLBM:
         interpolations inside the splines, moved to the interpolation's place; bit 2: the
         same at the spline's place, the fine substep in between leaving those edge cells
         alone; bit 3: f_c points inside the fine level's last block step; bit 4: record
-        launches split by whether they wait for the latest block step); results are
-        identical."""
+        launches split by whether they wait for the latest block step); default 5 (bits 0
+        and 2); results are identical."""
         _check(self.lib.mb_set_fusion(self.h, int(flags)), "mb_set_fusion")
 
     def set_collision(self, kind, s_e=0.0, s_eps=0.0, s_q=0.0):
