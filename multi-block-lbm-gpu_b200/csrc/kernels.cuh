@@ -1821,9 +1821,27 @@ __device__ __forceinline__ void spl_gather_p(const SplTaskP &T, int ip, typename
 // shared memory of one spline warp: the gathered fields, the forward sweep
 // (then the moments) and the window's c' and 1/den
 template <typename R> __host__ __device__ constexpr size_t spl_warp_smem() { return (size_t)26 * spl_win<R>() * sizeof(R); }
+// ... and, for the spline launches (UNROLL), the slot values each lane's
+// first fine point reads for a fused temporal interpolation (27 per lane)
+template <typename R> __host__ __device__ constexpr size_t spl_warp_smem_pf() {
+  return spl_warp_smem<R>() + (size_t)27 * 32 * sizeof(R);
+}
+
+// Asynchronous 4- or 8-byte copy from global to shared memory (cp.async,
+// completes into shared memory without holding registers).
+template <typename R> __device__ __forceinline__ void cp_async_val(R *dst, const R *src) {
+  static_assert(sizeof(R) == 4 || sizeof(R) == 8, "cp.async value size");
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(d), "l"(src), "n"((int)sizeof(R)) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
 
 // Segment sid (0 <= sid < p.nseg) of a spline launch, by one warp, with its
-// window arrays at wsm (spl_warp_smem bytes, 16-byte aligned).
+// window arrays at wsm (spl_warp_smem bytes, 16-byte aligned; with UNROLL,
+// spl_warp_smem_pf bytes).
 template <int P, bool UNROLL>
 __device__ __forceinline__ void spl_segment(const SplParamsP &p, int sid, int lane, unsigned char *wsm) {
   using R = typename Prec<P>::R;
@@ -1845,6 +1863,27 @@ __device__ __forceinline__ void spl_segment(const SplParamsP &p, int sid, int la
   const int Ilo = 1 + seg * SPL_SEG, Ihi = min(N - 1, (seg + 1) * SPL_SEG);
   const int w0 = max(0, Ilo - 1 - H), w1 = min(N - 1, Ihi + H);  // rows solved
   const int g0 = max(0, w0 - 1), g1 = min(N - 1, w1 + 1);        // rows gathered
+  // fine points of the segment (evaluated below)
+  const int ip0 = (seg == 0) ? 0 : T.r * (Ilo - 1) + 1;
+  const int ip1 = min(T.Nf - 1, T.r * Ihi);
+  R *slots = (R *)p.slots;
+  // fused temporal interpolation: the slot values of the lane's first point
+  // that this launch does not write (markers other than m0) are copied to
+  // shared memory now, beside the gather, instead of read after the slot
+  // stores (no other op of the launch writes them)
+  R *pf = (R *)(wsm + spl_warp_smem<R>()) + lane * 27;
+  const int ipf = ip0 + lane;
+  const bool pre = UNROLL && T.tmp && ipf <= ip1;
+  if constexpr (UNROLL) {
+    if (pre) {
+      const R *s3 = slots + (long long)(T.slot0 + ipf) * 27;
+#pragma unroll
+      for (int q = 0; q < 3; q++)
+        if (T.tm[q] != T.m0)
+#pragma unroll
+          for (int k = 0; k < 9; k++) cp_async_val<R>(pf + T.tm[q] * 9 + k, s3 + T.tm[q] * 9 + k);
+    }
+  }
   if constexpr (UNROLL) {
     // at most 3 x 32 rows (the window is below 96 rows): every load of the
     // gather in flight at once
@@ -1904,10 +1943,10 @@ __device__ __forceinline__ void spl_segment(const SplParamsP &p, int sid, int la
   __syncwarp();
 
   // evaluate the fine points of the segment (calculate_Spline3_gpu :136-185)
-  R *slots = (R *)p.slots;
   const R para = (R)T.para;
-  const int ip0 = (seg == 0) ? 0 : T.r * (Ilo - 1) + 1;
-  const int ip1 = min(T.Nf - 1, T.r * Ihi);
+  if constexpr (UNROLL) {
+    if (pre) cp_async_wait_all();  // the lane's own copies
+  }
   for (int ip = ip0 + lane; ip <= ip1; ip += 32) {
     const R xx = (R)ip / (R)T.r;
     int I = (int)ceil(xx);
@@ -1924,19 +1963,26 @@ __device__ __forceinline__ void spl_segment(const SplParamsP &p, int sid, int la
       ((R *)T.Mf[2])[fc] = out[2];
     }
     R *sl = slots + ((long long)(T.slot0 + ip) * 3 + T.m0) * 9;
+    R slv[9];  // the slot values this launch writes (marker m0)
 #pragma unroll
     for (int k = 0; k < 9; k++) {
       const R fe = feq<R>(k, out[0], out[1], out[2]);
-      sl[k] = fe + para * (out[3 + k] - fe);
+      slv[k] = fe + para * (out[3 + k] - fe);
+      sl[k] = slv[k];
     }
-    if (T.tmp && p.mask[T.tmask_off + ip]) {  // the fused temporal interpolation, from the slots just written
-      const R *s3 = slots + (long long)(T.slot0 + ip) * 27;
+    if (T.tmp && p.mask[T.tmask_off + ip]) {  // the fused temporal interpolation of the slots
+      // marker m0 from the values just computed, the others from the
+      // prefetched copies (the lane's first point) or from global memory
+      const R *s3 = (pre && ip == ipf) ? pf : slots + (long long)(T.slot0 + ip) * 27;
       const R a = (R)T.tw[0], b = (R)T.tw[1], cc = (R)T.tw[2];
       typename Prec<P>::S *Fd = (typename Prec<P>::S *)T.Ft;
 #pragma unroll
-      for (int k = 0; k < 9; k++)
-        st_f<P>(Fd, k * T.fplane + fc, k, temporal3<R>(a, b, cc, s3[T.tm[0] * 9 + k], s3[T.tm[1] * 9 + k], s3[T.tm[2] * 9 + k]),
-                p.sh);
+      for (int k = 0; k < 9; k++) {
+        const R s0 = T.tm[0] == T.m0 ? slv[k] : s3[T.tm[0] * 9 + k];
+        const R s1 = T.tm[1] == T.m0 ? slv[k] : s3[T.tm[1] * 9 + k];
+        const R s2 = T.tm[2] == T.m0 ? slv[k] : s3[T.tm[2] * 9 + k];
+        st_f<P>(Fd, k * T.fplane + fc, k, temporal3<R>(a, b, cc, s0, s1, s2), p.sh);
+      }
     }
   }
 }
@@ -1950,7 +1996,7 @@ __global__ void __launch_bounds__(32 * SPL_WARPS) k_spline(const __grid_constant
   const int sid = blockIdx.x * (int)(blockDim.x >> 5) + warp;  // blockDim: 1 to SPL_WARPS warps
   if (sid >= p.nseg) return;
   pdl_wait();
-  spl_segment<P, true>(p, sid, lane, smem_raw + warp * spl_warp_smem<R>());
+  spl_segment<P, true>(p, sid, lane, smem_raw + warp * spl_warp_smem_pf<R>());
 }
 
 // ----------------------------------------------------------------------------
@@ -2082,7 +2128,7 @@ __global__ void __launch_bounds__(32 * SPL_WARPS) kb_spline(const __grid_constan
   const SplParamsP &p = *(const SplParamsP *)smem_raw;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int sid = ((int)blockIdx.x - __ldg(a.cta0 + c)) * (int)(blockDim.x >> 5) + warp;
-  if (sid < p.nseg) spl_segment<P, true>(p, sid, lane, smem_raw + PB + warp * spl_warp_smem<R>());
+  if (sid < p.nseg) spl_segment<P, true>(p, sid, lane, smem_raw + PB + warp * spl_warp_smem_pf<R>());
 }
 
 // ----------------------------------------------------------------------------

@@ -392,8 +392,7 @@ size_t program_smem(int prec) { return prec == MB_PREC_F64 ? prg_smem<double>() 
 constexpr int MB_CTA_SMEM_MAX = 200 * 1024;  // largest spread request (B200: 227 KB per CTA)
 
 size_t spline_smem(int prec) {
-  return prec == MB_PREC_F64 ? (size_t)26 * SPL_WARPS * spl_win<double>() * sizeof(double)
-                             : (size_t)26 * SPL_WARPS * spl_win<float>() * sizeof(float);
+  return prec == MB_PREC_F64 ? SPL_WARPS * spl_warp_smem_pf<double>() : SPL_WARPS * spl_warp_smem_pf<float>();
 }
 
 // ---- node lowering ------------------------------------------------------------
