@@ -1874,6 +1874,13 @@ __device__ __forceinline__ void spl_segment(const SplParamsP &p, int sid, int la
   R *pf = (R *)(wsm + spl_warp_smem<R>()) + lane * 27;
   const int ipf = ip0 + lane;
   const bool pre = UNROLL && T.tmp && ipf <= ip1;
+  // the write masks of the lane's first point, loaded now as well (plan
+  // data, constant during the launch)
+  bool mk_first = true, tk_first = false;
+  if (ipf <= ip1) {
+    mk_first = T.mask_off < 0 || p.mask[T.mask_off + ipf];
+    tk_first = T.tmp && p.mask[T.tmask_off + ipf];
+  }
   if constexpr (UNROLL) {
     if (pre) {
       const R *s3 = slots + (long long)(T.slot0 + ipf) * 27;
@@ -1957,7 +1964,7 @@ __device__ __forceinline__ void spl_segment(const SplParamsP &p, int sid, int la
       out[f] = spline3_s<R>(xx, (R)(I - 1), (R)1.0, sfw[f][I - 1 - g0], sfw[f][I - g0],
                             sxw[f][I - 1 - g0], sxw[f][I - g0]);
     const long long fc = (long long)(T.fj0 + ip * T.fdj) * T.fpitch + (T.fi0 + ip * T.fdi);
-    if (T.mask_off < 0 || p.mask[T.mask_off + ip]) {
+    if (ip == ipf ? mk_first : (T.mask_off < 0 || p.mask[T.mask_off + ip])) {
       ((R *)T.Mf[0])[fc] = out[0];
       ((R *)T.Mf[1])[fc] = out[1];
       ((R *)T.Mf[2])[fc] = out[2];
@@ -1970,7 +1977,7 @@ __device__ __forceinline__ void spl_segment(const SplParamsP &p, int sid, int la
       slv[k] = fe + para * (out[3 + k] - fe);
       sl[k] = slv[k];
     }
-    if (T.tmp && p.mask[T.tmask_off + ip]) {  // the fused temporal interpolation of the slots
+    if (ip == ipf ? tk_first : (T.tmp && p.mask[T.tmask_off + ip])) {  // the fused temporal interpolation of the slots
       // marker m0 from the values just computed, the others from the
       // prefetched copies (the lane's first point) or from global memory
       const R *s3 = (pre && ip == ipf) ? pf : slots + (long long)(T.slot0 + ip) * 27;
