@@ -99,6 +99,18 @@ def case_targets(sim, geo, h=H, w=W):
 RE_SHEDDING = 47.0
 
 
+def wake_kick(cfg, h, w, kick):
+    """Transverse velocity (h, w) added to a prediction on the h x w grid of
+    warm_start: kick * U0 in a Gaussian of radius R centred 3R behind the
+    obstacle at (CX, CY); zero when kick <= 0 or Re < RE_SHEDDING."""
+    if kick <= 0.0 or cfg.Re < RE_SHEDDING:
+        return np.zeros((h, w))
+    gx, gy = (cfg.LX - 1.0) / (w - 1), (cfg.LY - 1.0) / (h - 1)
+    yy, xx = np.meshgrid(np.arange(h) * gy, np.arange(w) * gx, indexing="ij")
+    r2 = ((xx - (cfg.CX + 3.0 * cfg.R)) ** 2 + (yy - cfg.CY) ** 2) / float(cfg.R) ** 2
+    return kick * cfg.U0[0] * np.exp(-r2)
+
+
 def warm_start(sim, geo, pred, stream=None, kick=0.0):
     """Initialise every block of sim from a prediction (h, w, 3): f = feq +
     (1 - 1/tau) f_neq with f_neq_k = -3 w_k rho tau (e_k e_k - I/3) : grad u
@@ -117,10 +129,7 @@ def warm_start(sim, geo, pred, stream=None, kick=0.0):
     v = pred[..., 1].astype(np.float64) * U0
     rho = 1.0 + pred[..., 2].astype(np.float64) / 100.0
     gx, gy = (c.LX - 1.0) / (w - 1), (c.LY - 1.0) / (h - 1)
-    if kick > 0.0 and c.Re >= RE_SHEDDING:
-        yy, xx = np.meshgrid(np.arange(h) * gy, np.arange(w) * gx, indexing="ij")
-        r2 = ((xx - (c.CX + 3.0 * c.R)) ** 2 + (yy - c.CY) ** 2) / float(c.R) ** 2
-        v = v + kick * U0 * np.exp(-r2)
+    v = v + wake_kick(c, h, w, kick)
     dudy, dudx = np.gradient(u, gy, gx)
     dvdy, dvdx = np.gradient(v, gy, gx)
     L = geo.layout
