@@ -483,10 +483,10 @@ StbParams make_stb(mb_ctx *c, int a0, int a1, uint64_t parity, int macro_all, in
   return p;
 }
 
-// the rim is always stepped one cell per thread
 // octet kernel: variant 6 on a level of a 16-bit stored form (others run 0)
 bool stb_uses_octets(const mb_ctx *c, int level) { return c->stb_variant[level] == 6 && prec_bytes(c->prec) == 2; }
 
+// the rim is always stepped one cell per thread
 bool stb_uses_quads(const mb_ctx *c, int level, int region) {
   return region != STB_RIM && (c->stb_variant[level] == 1 || stb_uses_octets(c, level)) && c->use_graph != 3 &&
          !(c->use_graph == 4 && region != STB_INTERIOR) && !options_on(c);
