@@ -210,16 +210,20 @@ def run_reference(args):
     js, why = None, "reference build absent (oracle/_ref/ref_c2)"
     if os.path.exists(exe):
         wd = tempfile.mkdtemp()
-        r = subprocess.run([exe, "bench", str(args.steps), str(args.warmup)], cwd=wd, capture_output=True, text=True,
-                           timeout=1800)
-        lines = r.stdout.strip().splitlines()
         try:
-            js = json.loads(lines[-1]) if r.returncode == 0 and lines else None
-        except ValueError:
-            js = None
-        if js is None:
-            err = (r.stderr.strip().splitlines() or ["no output"])[-1]
-            why = f"reference build failed (exit {r.returncode}): {err[:200]}"
+            r = subprocess.run([exe, "bench", str(args.steps), str(args.warmup)], cwd=wd, capture_output=True,
+                               text=True, timeout=1800)
+        except subprocess.TimeoutExpired:
+            r, why = None, "reference build did not finish within 1800 s"
+        if r is not None:
+            lines = r.stdout.strip().splitlines()
+            try:
+                js = json.loads(lines[-1]) if r.returncode == 0 and lines else None
+            except ValueError:
+                js = None
+            if js is None:
+                err = (r.stderr.strip().splitlines() or ["no output"])[-1]
+                why = f"reference build failed (exit {r.returncode}): {err[:200]}"
     if js is not None:
         upd = int(js["cell_updates_per_step"])
         if upd != UPDATES_PER_STEP:
